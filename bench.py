@@ -1,0 +1,330 @@
+"""Benchmark: second-order Trotter evolution of the XXZ chain on one B200.
+
+Workload (the Trotter configuration of the reference's state-vector path):
+XXZ chain N=28, open boundary, J=1, Delta=0.5, on-site fields h_i ~ U[-1,1]
+(seed 42), Neel initial state, Strang splitting S2(dt) = S1(dt/2) then
+reversed S1(dt/2) with S1 = [Rz fields; per bond Rxx, Ryy, Rzz]
+(218 gate applications per step), dt = 0.05, 200 steps, <Z_i> recorded every
+10 steps (21 records); complex64 amplitudes, FP64 reductions.
+
+One bench step = one whole 200-step evolution from the initial state,
+43,600 gate applications.  metric = gate applications per second (whole job).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank runs an independent replica (the path does
+not shard: one state per GPU); value = all ranks' gate applications / the
+max over ranks of the device time.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "smoq.jl_b200"))
+
+N_QUBITS = 28
+DT = 0.05
+STEPS = 200
+RECORD_EVERY = 10
+J, DELTA = 1.0, 0.5
+SEED = 42
+GATES_PER_STEP = 2 * (N_QUBITS + 3 * (N_QUBITS - 1))  # 218
+GATE_APPS = STEPS * GATES_PER_STEP                    # 43,600 per bench step
+WORKLOAD = "xxz_chain_trotter2_n28_c64_200steps"
+
+
+def rz(t):
+    return np.diag([np.exp(-0.5j * t), np.exp(0.5j * t)])
+
+
+def rpp(P, t):
+    PP = np.kron(P, P)
+    return np.cos(t / 2) * np.eye(4) - 1j * np.sin(t / 2) * PP
+
+
+X = np.array([[0, 1], [1, 0]], complex)
+Y = np.array([[0, -1j], [1j, 0]], complex)
+Z = np.array([[1, 0], [0, -1]], complex)
+
+
+def s1_gates(N, tau):
+    """S1(tau) as (1-based indices, U): Rz(2 h_i tau) on every site, then per bond
+    Rxx(2 J tau), Ryy(2 J tau), Rzz(2 J Delta tau)."""
+    h = np.random.default_rng(SEED).uniform(-1, 1, size=N)
+    g = [([i + 1], rz(2 * h[i] * tau)) for i in range(N)]
+    for i in range(1, N):
+        g += [([i, i + 1], rpp(X, 2 * J * tau)), ([i, i + 1], rpp(Y, 2 * J * tau)),
+              ([i, i + 1], rpp(Z, 2 * J * DELTA * tau))]
+    return g
+
+
+def neel_index(N):
+    return sum(1 << (k - 1) for k in range(1, N + 1, 2))
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampler during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv") \
+            if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/smoq_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        for ln in open(self.path):
+            c = [x.strip() for x in ln.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1]))
+                mx = float(c[2])
+            except ValueError:
+                continue
+            for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], c[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    p = os.path.join(ROOT, "profiles", "tile_pass_xxz_n28_c64.json")
+    if os.path.exists(p):
+        try:
+            return float(json.load(open(p))["traffic_bytes_per_launch"])
+        except Exception:
+            return None
+    return None
+
+
+def cpu_baseline_sample(n_gates=12, N=N_QUBITS):
+    """The oracle (CPU restatement of the reference's loops, one thread) on the
+    first n_gates of one Strang step at full N, complex128."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    gl = s1_gates(N, DT / 2)
+    both = gl + gl[::-1]
+    sample = both[:n_gates]
+    arr = O.make_gates([([q for q in idx], U) for idx, U in sample])
+    psi = O.zero_state(N, neel_index(N))
+    t0 = O.wtime()
+    O.trotter_step(psi, arr, len(sample), N)
+    dt = O.wtime() - t0
+    return len(sample) / dt, dt
+
+
+def reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    n_gates = 8
+    for _ in range(args.warmup):
+        cpu_baseline_sample(n_gates)
+    rates, tot = [], 0.0
+    for _ in range(args.steps):
+        r, t = cpu_baseline_sample(n_gates)
+        rates.append(r)
+        tot += t
+    v = float(np.mean(rates))
+    line = {"impl": "reference", "metric": "gate_apps_per_s", "value": v, "unit": "gate-apps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * GATE_APPS / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "N": N_QUBITS, "dtype_reference": "complex128",
+                       "sample": f"first {n_gates} gates of one Strang step at N=28 per step"},
+            "cpu_baseline": {"value": v, "unit": "gate-apps/s", "cores": 1, "kind": "port",
+                             "sample": f"{n_gates} of the 218 gate applications of one step at N=28, complex128, "
+                                       "single thread (the reference's kernels are single-threaded per state)"},
+            "e2e": {"value": v, "unit": "gate-apps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    ws, rank, local = dist_env()
+    import torch
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    import build as _b
+    if rank == 0 and not os.path.exists(_b.LIB):
+        _b.build_cuda()
+    if ws > 1:
+        dist.barrier()
+    import pysmoq as S
+
+    ctx = S.Context(local)
+    N = N_QUBITS
+    gl = s1_gates(N, DT / 2)
+    gates = [S.FastTrotterGate(idx, U) for idx, U in gl]
+    plan = S.TrotterPlan(ctx, N, gates, order=2, dtype=S.C64)
+    st = S.CuState(ctx, N, S.C64, basis=None)
+    neel = neel_index(N)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+
+    def device_step():
+        st.set_basis(neel)                      # make_initial_psi on the device
+        return plan.run(st, STEPS, RECORD_EVERY)
+
+    # e2e input: the initial state in pinned host memory (what a caller holding
+    # psi on the host passes), uploaded every step; output: the <Z> records.
+    host_psi = torch.zeros(1 << N, dtype=torch.complex64, pin_memory=True)
+    host_psi[neel] = 1.0
+    hp = host_psi.numpy()
+
+    def e2e_step():
+        S.lib.smoq_state_upload(st.h, hp.ctypes.data_as(S._lib.C.c_void_p), hp.nbytes)
+        return plan.run(st, STEPS, RECORD_EVERY)
+
+    def timed(fn, k):
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+        ctx.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        ctx.synchronize()
+        ms = e0.elapsed_time(e1)
+        if ws > 1:
+            t = torch.tensor([ms], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    for _ in range(args.warmup):
+        rec = device_step()
+    ctx.reset_counters()
+    clocks = Clocks(local)
+    clocks.start()
+    ms = timed(device_step, args.steps)
+    clk = clocks.stop()
+    launches = ctx.counters()["launches"]
+    rec = device_step()
+    # sanity of the result: the Neel state's <Z> at t=0 and bounded magnetisation after
+    assert np.allclose(rec[0, 0, :], [(-1.0 if (neel >> k) & 1 else 1.0) for k in range(N)], atol=1e-6)
+    assert np.all(np.abs(rec) <= 1 + 1e-5)
+
+    # roofline of the dominant kernel: the fused tile pass, timed per launch with
+    # CUDA events on the library's stream (graphs off so every launch is bracketed)
+    for _ in range(1):
+        e2e_step()
+    ctx.set_option(S._lib.OPT_USE_GRAPHS, 0)
+    ctx.set_option(S._lib.OPT_KERNEL_TIMING, 1)
+    ctx.reset_counters()
+    timed(device_step, 1)
+    kc = ctx.counters()
+    ctx.set_option(S._lib.OPT_KERNEL_TIMING, 0)
+    ctx.set_option(S._lib.OPT_USE_GRAPHS, 1)
+    passes = kc["tile_passes"]
+    avg_ms = kc["tile_ms"] / max(1, passes)
+    bytes_per_launch = kc["tile_bytes"] / max(1, passes)
+    achieved = bytes_per_launch / (avg_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+
+    # e2e through the C ABI with host buffers
+    e2e_ms = timed(e2e_step, args.steps)
+
+    per_rank_apps = GATE_APPS * args.steps
+    value = ws * per_rank_apps / (ms * 1e-3)
+    e2e_value = ws * per_rank_apps / (e2e_ms * 1e-3)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        r, t = cpu_baseline_sample(12)
+        cpu = {"value": r, "unit": "gate-apps/s", "cores": 1, "kind": "port",
+               "sample": f"first 12 of the 218 gate applications of one Strang step at N=28, complex128, "
+                         f"single thread, {t:.1f} s (oracle restating the reference's loops)"}
+
+    if rank == 0:
+        line = {"metric": "gate_apps_per_s", "value": value, "unit": "gate-apps/s", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "N": N, "dt": DT, "trotter_steps": STEPS,
+                           "record_every": RECORD_EVERY, "gate_apps_per_step": GATE_APPS,
+                           "state_bytes": (1 << N) * 8, "l2_policy": "inputs larger than L2 (2 GiB state)",
+                           "parallelism": "replicas" if ws > 1 else "single_gpu",
+                           "tile_passes_per_step": passes, "hbm_gbs_effective":
+                               2.0 * (1 << N) * 8 * passes / (ms / args.steps * 1e-3) / 1e9},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": ncu_traffic(), "peak_kind": peak_kind,
+                             "kernel": "tile_pass_kernel<float>", "avg_launch_ms": avg_ms,
+                             "algorithmic_bytes_per_launch": bytes_per_launch},
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": "gate-apps/s", "h2d_bytes_per_step": int(hp.nbytes),
+                        "d2h_bytes_per_step": int(8 * N * (STEPS // RECORD_EVERY + 1))},
+                "gpu_launches": int(launches),
+                "clocks": clk}
+        print(json.dumps(line))
+    st.close()
+    plan.close()
+    ctx.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

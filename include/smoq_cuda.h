@@ -1,0 +1,241 @@
+/*
+ * smoq_cuda.h -- C ABI of libsmoq_cuda.so, the B200 (sm_100a) state-vector
+ * engine behind SmoQ.jl's matrix-free gate / observable / evolution API.
+ *
+ * Every entry point below replaces one reference function (cited as
+ * file:line inside the SmoQ.jl tree).  Conventions:
+ *   - qubits are 0-based bit positions (the Julia wrapper passes k-1 for the
+ *     reference's 1-based k; bit k-1 of the index is qubit k, little-endian,
+ *     utils/cpu/cpuQuantumChannelGates.jl:48-51);
+ *   - a state holds `batch` independent states of 2^N amplitudes, state-major,
+ *     interleaved complex (ComplexF32 for SMOQ_C64, ComplexF64 for
+ *     SMOQ_C128); every gate acts on all states of the batch;
+ *   - matrices are column-major interleaved complex doubles (Julia Matrix
+ *     memory order); gate coefficients are always computed in FP64 on the
+ *     host, expectation values and norms are accumulated in FP64;
+ *   - every call returns smoq_status and never aborts, exits or traps;
+ *     smoq_last_error() gives the message.  Calls are asynchronous on the
+ *     context's stream; calls that return host values synchronise it.  A
+ *     context is not re-entrant: use one per host thread.
+ */
+#ifndef SMOQ_CUDA_H
+#define SMOQ_CUDA_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SMOQ_OK = 0,
+    SMOQ_ERR_BADINPUT = 1,    /* replaces error()/@assert in the reference, e.g.
+                                 utils/cpu/cpuQuantumStateObservables.jl:183 */
+    SMOQ_ERR_OOM = 2,
+    SMOQ_ERR_CUDA = 3,
+    SMOQ_ERR_TIMEOUT = 4,     /* a bounded device-side wait ran out */
+    SMOQ_ERR_UNSUPPORTED = 5,
+    SMOQ_ERR_NOGPU = 6
+} smoq_status;
+
+typedef enum { SMOQ_C64 = 0, SMOQ_C128 = 1 } smoq_dtype;
+
+typedef struct smoq_ctx smoq_ctx;
+typedef struct smoq_state smoq_state;
+typedef struct smoq_plan smoq_plan;
+
+/* ---------------------------------------------------------------- context */
+smoq_status smoq_ctx_create(int device, smoq_ctx** out);
+smoq_status smoq_ctx_destroy(smoq_ctx* ctx);
+const char* smoq_last_error(smoq_ctx* ctx);
+smoq_status smoq_ctx_synchronize(smoq_ctx* ctx);
+/* the cudaStream_t every call of this context is ordered on */
+void* smoq_ctx_stream(smoq_ctx* ctx);
+enum {
+    SMOQ_OPT_TILE_BITS_C64 = 1,   /* tile width (qubits) of fused passes, complex64 */
+    SMOQ_OPT_TILE_BITS_C128 = 2,
+    SMOQ_OPT_LOW_BITS_C64 = 3,    /* minimum contiguous low qubits per tile segment */
+    SMOQ_OPT_LOW_BITS_C128 = 4,
+    SMOQ_OPT_USE_GRAPHS = 5,      /* capture Trotter blocks as CUDA graphs (default 1) */
+    SMOQ_OPT_KERNEL_TIMING = 6    /* bracket fused passes with CUDA events (default 0) */
+};
+smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long value);
+/* launches: kernels launched by this context; tile_passes/tile_ms/tile_bytes:
+ * fused passes, their summed event time and algorithmic bytes (timing on) */
+smoq_status smoq_ctx_counters(smoq_ctx* ctx, long long* launches, long long* tile_passes,
+                              double* tile_ms, double* tile_bytes);
+smoq_status smoq_ctx_reset_counters(smoq_ctx* ctx);
+/* the library's build identification, e.g. "smoq_cuda sm_100a" */
+const char* smoq_version(void);
+
+/* ----------------------------------------------------------------- states */
+/* Vector{ComplexF64}(undef, 2^N) per state; zero-initialised */
+smoq_status smoq_state_create(smoq_ctx* ctx, int N, smoq_dtype dtype, int batch, smoq_state** out);
+/* borrow a device buffer (e.g. a CuArray's pointer, 16-byte aligned); never freed here */
+smoq_status smoq_state_wrap(smoq_ctx* ctx, void* devptr, int N, smoq_dtype dtype, int batch,
+                            smoq_state** out);
+smoq_status smoq_state_destroy(smoq_state* st);
+void* smoq_state_device_ptr(smoq_state* st);
+/* host <-> device copies of the whole batch in the state's own dtype */
+smoq_status smoq_state_upload(smoq_state* st, const void* host, size_t bytes);
+smoq_status smoq_state_download(smoq_state* st, void* host, size_t bytes);
+/* make_initial_psi (utils/cpu/cpuQuantumStatePreparation.jl:1211): every
+ * state of the batch becomes the basis state |index> */
+smoq_status smoq_state_set_basis(smoq_state* st, uint64_t index);
+/* dst <- src with dtype conversion (c128 <-> c64), same N and batch */
+smoq_status smoq_state_copy(smoq_state* dst, smoq_state* src);
+
+/* ---------------------------------------------- gates: utils/cpu/cpuQuantumChannelGates.jl */
+smoq_status smoq_apply_rx(smoq_state* st, int q, double theta);   /* apply_rx_psi! :142 */
+smoq_status smoq_apply_ry(smoq_state* st, int q, double theta);   /* apply_ry_psi! :172 */
+smoq_status smoq_apply_rz(smoq_state* st, int q, double theta);   /* apply_rz_psi! :201 */
+smoq_status smoq_apply_h(smoq_state* st, int q);                  /* apply_hadamard_psi! :222 */
+smoq_status smoq_apply_x(smoq_state* st, int q);                  /* apply_pauli_x_psi! :245 */
+smoq_status smoq_apply_y(smoq_state* st, int q);                  /* apply_pauli_y_psi! :265 */
+smoq_status smoq_apply_z(smoq_state* st, int q);                  /* apply_pauli_z_psi! :286;
+                                                                     apply_sigma_z! MCWF.jl:170 */
+smoq_status smoq_apply_s(smoq_state* st, int q);                  /* apply_s_psi! :307 */
+smoq_status smoq_apply_sdg(smoq_state* st, int q);                /* apply_sdagger_psi! :328 */
+smoq_status smoq_apply_t(smoq_state* st, int q);                  /* apply_t_psi! :360 */
+smoq_status smoq_apply_tdg(smoq_state* st, int q);                /* apply_tdagger_psi! :380 */
+smoq_status smoq_apply_ccz(smoq_state* st, int q1, int q2, int q3);      /* apply_ccz_psi! :448 */
+smoq_status smoq_apply_toffoli(smoq_state* st, int c1, int c2, int t);   /* apply_toffoli_psi! :471 */
+smoq_status smoq_apply_cnot(smoq_state* st, int control, int target);    /* apply_cnot_psi! :870 */
+smoq_status smoq_apply_cz(smoq_state* st, int q1, int q2);               /* apply_cz_psi! :889 */
+smoq_status smoq_apply_cry(smoq_state* st, int control, int target, double theta); /* apply_cry_psi! :914 */
+smoq_status smoq_apply_rxx(smoq_state* st, int q1, int q2, double theta);  /* apply_rxx_psi! :992 */
+smoq_status smoq_apply_ryy(smoq_state* st, int q1, int q2, double theta);  /* apply_ryy_psi! :1039 */
+smoq_status smoq_apply_rzz(smoq_state* st, int q1, int q2, double theta);  /* apply_rzz_psi! :1084 */
+smoq_status smoq_apply_sigma_minus(smoq_state* st, int q);       /* apply_sigma_minus_psi! :739 */
+smoq_status smoq_apply_sigma_plus(smoq_state* st, int q);        /* apply_sigma_plus_psi! :762 */
+/* generic 2x2: apply_one_qubit_gate_bitwise_cpu! (cpuQuantumChannelUnitaryEvolutionTrotter.jl:77),
+ * apply_gate! (cpuQuantumChannelRandomUnitaries.jl:230) */
+smoq_status smoq_apply_u1(smoq_state* st, int q, const double* U);
+/* generic 4x4 on (q1, q2), basis |00>,|q_lo=1>,|q_hi=1>,|11>.
+ * convention 0: apply_two_qubit_gate_bitwise_cpu! (Trotter.jl:107) -- when
+ *   q1 > q2 the qubits are swapped and U is used as given;
+ * convention 1: apply_2qubit_gate! (RandomUnitaries.jl:317) -- when q1 > q2
+ *   U is conjugated by SWAP first. */
+smoq_status smoq_apply_u2(smoq_state* st, int q1, int q2, const double* U, int convention);
+
+/* ----------------------------------------------------- fused gate sequences */
+/* gate types of smoq_op (the CircuitOperation symbols of
+ * utils/cpu/cpuVariationalQuantumCircuitBuilder.jl:82 GATE_TYPES, plus the
+ * generic matrices) */
+enum {
+    SMOQ_G_RX = 0, SMOQ_G_RY, SMOQ_G_RZ, SMOQ_G_H, SMOQ_G_X, SMOQ_G_Y, SMOQ_G_Z, SMOQ_G_S,
+    SMOQ_G_SDG, SMOQ_G_T, SMOQ_G_TDG, SMOQ_G_CZ, SMOQ_G_CNOT, SMOQ_G_RXX, SMOQ_G_RYY,
+    SMOQ_G_RZZ, SMOQ_G_CRY, SMOQ_G_CCZ, SMOQ_G_TOFFOLI, SMOQ_G_U1, SMOQ_G_U2
+};
+typedef struct {
+    int32_t type;     /* SMOQ_G_* */
+    int32_t q[3];     /* 0-based qubits */
+    int32_t param;    /* -1: fixed `angle`; >= 0: theta[param] (CircuitOperation.param_idx - 1) */
+    int32_t pad;
+    double angle;
+    double U[32];     /* SMOQ_G_U1 / SMOQ_G_U2 (convention 0), column-major interleaved */
+} smoq_op;
+/* apply_circuit! (cpuVariationalQuantumCircuitExecutor.jl:95) for gate-only
+ * circuits: the sequence is planned into fused tile passes (gates on a
+ * tile's qubits are applied in shared memory between one HBM read and one
+ * HBM write of the tile).  theta may be NULL when no op has param >= 0. */
+smoq_status smoq_apply_sequence(smoq_state* st, const smoq_op* ops, int n, const double* theta);
+/* the same, one launch per gate (the plain, unfused path) */
+smoq_status smoq_apply_sequence_unfused(smoq_state* st, const smoq_op* ops, int n,
+                                        const double* theta);
+
+/* ----------------------------------- observables: utils/cpu/cpuQuantumStateObservables.jl */
+/* each writes `batch` doubles to the host array out (one per state) */
+smoq_status smoq_expect_x(smoq_state* st, int q, double* out);   /* expect_local :175 -> _expect_X :230 */
+smoq_status smoq_expect_y(smoq_state* st, int q, double* out);   /* _expect_Y :256 */
+smoq_status smoq_expect_z(smoq_state* st, int q, double* out);   /* _expect_Z :201 */
+smoq_status smoq_expect_xx(smoq_state* st, int q1, int q2, double* out); /* expect_corr :306 -> :385 */
+smoq_status smoq_expect_yy(smoq_state* st, int q1, int q2, double* out); /* _expect_YY :427 */
+smoq_status smoq_expect_zz(smoq_state* st, int q1, int q2, double* out); /* _expect_ZZ :341 */
+/* get_expectation_pauli_string :840 (ops letters 'X','Y','Z' on 0-based qubits) */
+smoq_status smoq_expect_pauli_string(smoq_state* st, int n, const char* ops, const int* qubits,
+                                     double* out);
+/* diagonal batch in ONE pass: out[b * nobs + o] = <Z-string zmasks[o]> of state b
+ * (zmask 0 gives the squared norm); the Z/ZZ part of
+ * measure_all_observables_one_pass :1532 */
+smoq_status smoq_expect_zstrings(smoq_state* st, const uint64_t* zmasks, int nobs, double* out);
+/* population_excited_psi (Gates.jl:784) */
+smoq_status smoq_population_excited(smoq_state* st, int q, double* out);
+/* squared norm per state; get_norm (cpuQuantumStatePreparation.jl:377) is its sqrt */
+smoq_status smoq_norm2(smoq_state* st, double* out);
+/* normalize_state! (cpuQuantumStatePreparation.jl:307) */
+smoq_status smoq_normalize(smoq_state* st);
+
+/* ------------------------ Hamiltonian IR and Trotter (cpuHamiltonianBuilder.jl,
+ *                          cpuQuantumChannelUnitaryEvolutionTrotter.jl) */
+typedef struct {           /* FastTrotterGate (Trotter.jl:62) with 0-based indices */
+    int32_t nq;            /* 1 or 2 */
+    int32_t q[2];
+    int32_t pad;
+    double U[32];          /* column-major interleaved; 2x2 gates use U[0..7] */
+} smoq_trotter_gate;
+/* precompute_trotter_gates_bitwise_cpu (Trotter.jl:322): bonds are
+ * CouplingTerm (cpuHamiltonianBuilder.jl:42) rows (i, j, Jxx, Jyy, Jzz) and
+ * fields FieldTerm (:51) rows (idx, hx, hy, hz), 0-based sites; gates are
+ * exp(-i H_local dt) in closed form.  *n_out receives the gate count. */
+smoq_status smoq_precompute_trotter_gates(const double* bonds, int nb, const double* fields,
+                                          int nf, double dt, smoq_trotter_gate* out, int* n_out);
+/* A Trotter plan: order 1 applies the gates once per step (apply_fast_trotter_step_cpu!,
+ * Trotter.jl:150); order 2 applies them, then the same list reversed (Strang
+ * splitting; the caller passes gates computed for dt/2). */
+smoq_status smoq_trotter_plan_create(smoq_ctx* ctx, int N, smoq_dtype dtype,
+                                     const smoq_trotter_gate* gates, int n, int order,
+                                     smoq_plan** out);
+smoq_status smoq_plan_destroy(smoq_plan* plan);
+/* evolve_trotter_psi_cpu! (Trotter.jl:250): n_steps steps in place */
+smoq_status smoq_trotter_step(smoq_plan* plan, smoq_state* st, int n_steps);
+/* solve_trotter_bitwise_cpu (Trotter.jl:293) with <Z_i> records: runs `steps`
+ * steps and records <Z_i> of every state at t = 0, record_every, ... into
+ * z_out[r][b][i] (host, (steps/record_every + 1) * batch * N doubles). */
+smoq_status smoq_trotter_run(smoq_plan* plan, smoq_state* st, int steps, int record_every,
+                             double* z_out);
+
+/* ------------------ MCWF (cpuQuantumChannelLindbladianEvolutionMonteCarloWaveFunction.jl) */
+typedef struct {           /* JumpOperator (cpuQuantumChannelLindbladianEvolution.jl:65) */
+    int32_t type;          /* 0 sigma_minus, 1 sigma_plus, 2 sigma_z, 3 sigma_x */
+    int32_t qubit;         /* 0-based */
+    double gamma;
+} smoq_jump_op;
+/* Batched quantum-jump evolution (lindblad_mcwf_batched_step! :340,
+ * evolve_mcwf_batched_trotter! :412, generalised to any mix of the four jump
+ * types): every state of `st` is one trajectory, starting from whatever st
+ * holds (normalised).  The plan must be order 1 (the coherent step).
+ * Trajectory b uses Philox4x32-10 stream (key = seed, counter = (step, traj_offset + b)).
+ * Records at t = 0, record_every, ...: the trajectory means of <Z_i>
+ * (z_mean[r][i]) and <Z_i Z_{i+1}> (zz_mean[r][i]); optional per-trajectory
+ * values z_traj[r][b][i], zz_traj[r][b][i] (NULL to skip); jumps[b] counts the
+ * jumps per trajectory (NULL to skip). */
+smoq_status smoq_mcwf_run(smoq_plan* plan, smoq_state* st, const smoq_jump_op* ops, int nops,
+                          double dt, uint64_t seed, uint64_t traj_offset, int steps,
+                          int record_every, double* z_mean, double* zz_mean, double* z_traj,
+                          double* zz_traj, int* jumps);
+
+/* ------------------------------------------- VQE energy and adjoint gradient */
+typedef struct {           /* one Pauli-sum term: coef * prod of letters */
+    double coef;
+    uint64_t xmask;        /* qubits carrying X or Y */
+    uint64_t zmask;        /* qubits carrying Z or Y */
+} smoq_pauli_term;
+/* E(theta) = <0|U^dag H U|0> and dE/dtheta for `batch` parameter sets at once
+ * (theta[b * n_params + p]).  Gradient by the adjoint method (one forward
+ * sweep, then an uncompute sweep in reverse); replaces the gradient backends
+ * of calculate_gradients (cpuVariationalQuantumCircuitGradients.jl:88) for
+ * gate-only circuits whose parameterised gates are RX/RY/RZ/RXX/RYY/RZZ.
+ * energies[b], grads[b * n_params + p] are host arrays. */
+smoq_status smoq_energy_grad(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* ops, int n,
+                             int n_params, const smoq_pauli_term* H, int nterms, int batch,
+                             const double* theta, double* energies, double* grads);
+/* energy only (forward + reduction), same arguments */
+smoq_status smoq_energy(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* ops, int n,
+                        int n_params, const smoq_pauli_term* H, int nterms, int batch,
+                        const double* theta, double* energies);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,777 @@
+/*
+ * smoq_oracle.c -- CPU restatement of SmoQ.jl's state-vector hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker, never the product; see the header).
+ * Each function names the reference file:line whose loop it restates.  The
+ * loops deliberately keep the reference's shape (a scan over all 2^N
+ * indices with a branch on the qubit bit, single-threaded per state) so the
+ * CPU baseline built from this file times the work the Julia kernels do.
+ */
+#include "smoq_oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#include <pthread.h>
+
+#define I_ _Complex_I
+typedef so_cplx C;
+
+static inline C ld(const double* m, int idx) { return m[2 * idx] + I_ * m[2 * idx + 1]; }
+/* column-major element (r, c) of an n x n matrix */
+static inline C mat(const double* m, int n, int r, int c) { return ld(m, c * n + r); }
+
+double so_wtime(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+/* ========================================================================
+ * Single-qubit gates -- utils/cpu/cpuQuantumChannelGates.jl
+ * ======================================================================== */
+void so_apply_rx_psi(C* psi, int k, double theta, int N) { /* :142-161 */
+    double c = cos(theta / 2), s = sin(theta / 2);
+    C is = -I_ * s;
+    int64_t step = 1LL << (k - 1), dim = 1LL << N;
+    for (int64_t i = 0; i < dim; i++) {
+        if (((i >> (k - 1)) & 1) == 0) {
+            int64_t j = i + step;
+            C a = psi[i], b = psi[j];
+            psi[i] = c * a + is * b;
+            psi[j] = is * a + c * b;
+        }
+    }
+}
+void so_apply_ry_psi(C* psi, int k, double theta, int N) { /* :172-190 */
+    double c = cos(theta / 2), s = sin(theta / 2);
+    int64_t step = 1LL << (k - 1), dim = 1LL << N;
+    for (int64_t i = 0; i < dim; i++) {
+        if (((i >> (k - 1)) & 1) == 0) {
+            int64_t j = i + step;
+            C a = psi[i], b = psi[j];
+            psi[i] = c * a - s * b;
+            psi[j] = s * a + c * b;
+        }
+    }
+}
+void so_apply_rz_psi(C* psi, int k, double theta, int N) { /* :201-212 */
+    C ph[2] = {cexp(-I_ * theta / 2), cexp(I_ * theta / 2)};
+    int64_t dim = 1LL << N;
+    for (int64_t i = 0; i < dim; i++) psi[i] *= ph[(i >> (k - 1)) & 1];
+}
+void so_apply_hadamard_psi(C* psi, int k, int N) { /* :222-238 */
+    double s = 1 / sqrt(2.0);
+    int64_t step = 1LL << (k - 1), dim = 1LL << N;
+    for (int64_t i = 0; i < dim; i++) {
+        if (((i >> (k - 1)) & 1) == 0) {
+            int64_t j = i + step;
+            C a = psi[i], b = psi[j];
+            psi[i] = s * (a + b);
+            psi[j] = s * (a - b);
+        }
+    }
+}
+void so_apply_pauli_x_psi(C* psi, int k, int N) { /* :245-257 */
+    int64_t step = 1LL << (k - 1), dim = 1LL << N;
+    for (int64_t i = 0; i < dim; i++) {
+        if (((i >> (k - 1)) & 1) == 0) {
+            int64_t j = i + step;
+            C t = psi[i]; psi[i] = psi[j]; psi[j] = t;
+        }
+    }
+}
+void so_apply_pauli_y_psi(C* psi, int k, int N) { /* :265-280 */
+    int64_t step = 1LL << (k - 1), dim = 1LL << N;
+    for (int64_t i = 0; i < dim; i++) {
+        if (((i >> (k - 1)) & 1) == 0) {
+            int64_t j = i + step;
+            C v0 = psi[i], v1 = psi[j];
+            psi[i] = -I_ * v1;
+            psi[j] = I_ * v0;
+        }
+    }
+}
+static void phase_on_set_bit(C* psi, int k, int N, C ph) {
+    int64_t dim = 1LL << N;
+    for (int64_t i = 0; i < dim; i++)
+        if (((i >> (k - 1)) & 1) == 1) psi[i] *= ph;
+}
+void so_apply_pauli_z_psi(C* psi, int k, int N) { /* :286-296 */
+    int64_t dim = 1LL << N;
+    for (int64_t i = 0; i < dim; i++)
+        if (((i >> (k - 1)) & 1) == 1) psi[i] = -psi[i];
+}
+void so_apply_s_psi(C* psi, int k, int N) { phase_on_set_bit(psi, k, N, I_); }        /* :307 */
+void so_apply_sdagger_psi(C* psi, int k, int N) { phase_on_set_bit(psi, k, N, -I_); } /* :328 */
+void so_apply_t_psi(C* psi, int k, int N) { /* :360 */
+    phase_on_set_bit(psi, k, N, cexp(I_ * M_PI / 4));
+}
+void so_apply_tdagger_psi(C* psi, int k, int N) { /* :380 */
+    phase_on_set_bit(psi, k, N, cexp(-I_ * M_PI / 4));
+}
+
+/* ========================================================================
+ * Multi-qubit gates
+ * ======================================================================== */
+void so_apply_ccz_psi(C* psi, int q1, int q2, int q3, int N) { /* :448-461 */
+    int64_t dim = 1LL << N;
+    for (int64_t i = 0; i < dim; i++) {
+        int b1 = (i >> (q1 - 1)) & 1, b2 = (i >> (q2 - 1)) & 1, b3 = (i >> (q3 - 1)) & 1;
+        if (b1 && b2 && b3) psi[i] = -psi[i];
+    }
+}
+void so_apply_toffoli_psi(C* psi, int c1, int c2, int t, int N) { /* :471-489 */
+    int64_t dim = 1LL << N, ts = 1LL << (t - 1);
+    for (int64_t i = 0; i < dim; i++) {
+        int b1 = (i >> (c1 - 1)) & 1, b2 = (i >> (c2 - 1)) & 1, bt = (i >> (t - 1)) & 1;
+        if (b1 && b2 && !bt) {
+            int64_t j = i + ts;
+            C x = psi[i]; psi[i] = psi[j]; psi[j] = x;
+        }
+    }
+}
+void so_apply_cnot_psi(C* psi, int control, int target, int N) { /* :870-882 */
+    int64_t dim = 1LL << N, ts = 1LL << (target - 1);
+    for (int64_t i = 0; i < dim; i++) {
+        if (((i >> (control - 1)) & 1) == 1 && ((i >> (target - 1)) & 1) == 0) {
+            int64_t j = i + ts;
+            C x = psi[i]; psi[i] = psi[j]; psi[j] = x;
+        }
+    }
+}
+void so_apply_cz_psi(C* psi, int qi, int qj, int N) { /* :889-900 (branchless sign) */
+    int64_t dim = 1LL << N;
+    for (int64_t idx = 0; idx < dim; idx++) {
+        int bi = (idx >> (qi - 1)) & 1, bj = (idx >> (qj - 1)) & 1;
+        psi[idx] *= (double)(1 - 2 * (bi & bj));
+    }
+}
+void so_apply_cry_psi(C* psi, int control, int target, double theta, int N) { /* :914-943 */
+    double c = cos(theta / 2), s = sin(theta / 2);
+    int64_t dim = 1LL << N, ts = 1LL << (target - 1);
+    for (int64_t i = 0; i < dim; i++) {
+        if (((i >> (control - 1)) & 1) == 1 && ((i >> (target - 1)) & 1) == 0) {
+            int64_t j = i + ts;
+            C a = psi[i], b = psi[j];
+            psi[i] = c * a - s * b;
+            psi[j] = s * a + c * b;
+        }
+    }
+}
+/* :992-1028 and :1039-1073: quartet loops over "base" with both bits 0 */
+static void rpp_quartet(C* psi, int qi, int qj, C m00_11, C m01_10, C m10_01, C m11_00,
+                        double c, int N) {
+    int64_t dim = 1LL << N, si = 1LL << (qi - 1), sj = 1LL << (qj - 1);
+    for (int64_t base = 0; base < dim; base++) {
+        if (((base >> (qi - 1)) & 1) != 0 || ((base >> (qj - 1)) & 1) != 0) continue;
+        int64_t i00 = base, i01 = base + sj, i10 = base + si, i11 = base + si + sj;
+        C p00 = psi[i00], p01 = psi[i01], p10 = psi[i10], p11 = psi[i11];
+        psi[i00] = c * p00 + m00_11 * p11;
+        psi[i01] = c * p01 + m01_10 * p10;
+        psi[i10] = m10_01 * p01 + c * p10;
+        psi[i11] = m11_00 * p00 + c * p11;
+    }
+}
+void so_apply_rxx_psi(C* psi, int qi, int qj, double theta, int N) { /* :992 */
+    double c = cos(theta / 2), s = sin(theta / 2);
+    C is = -I_ * s;
+    rpp_quartet(psi, qi, qj, is, is, is, is, c, N);
+}
+void so_apply_ryy_psi(C* psi, int qi, int qj, double theta, int N) { /* :1039 */
+    double c = cos(theta / 2), s = sin(theta / 2);
+    C is = -I_ * s, isn = I_ * s;
+    rpp_quartet(psi, qi, qj, isn, is, is, isn, c, N);
+}
+void so_apply_rzz_psi(C* psi, int qi, int qj, double theta, int N) { /* :1084-1100 */
+    C same = cexp(-I_ * theta / 2), diff = cexp(I_ * theta / 2);
+    int64_t dim = 1LL << N;
+    for (int64_t idx = 0; idx < dim; idx++) {
+        int bi = (idx >> (qi - 1)) & 1, bj = (idx >> (qj - 1)) & 1;
+        psi[idx] *= (bi == bj) ? same : diff;
+    }
+}
+
+/* ========================================================================
+ * Jump operators
+ * ======================================================================== */
+void so_apply_sigma_minus_psi(C* psi, int k, int N) { /* :739-752 */
+    int64_t dim = 1LL << N, mask = 1LL << (k - 1);
+    for (int64_t i = 0; i < dim; i++) {
+        if (i & mask) {
+            int64_t j = i ^ mask;
+            psi[j] = psi[i];
+            psi[i] = 0;
+        }
+    }
+}
+void so_apply_sigma_plus_psi(C* psi, int k, int N) { /* :762-775 */
+    int64_t dim = 1LL << N, mask = 1LL << (k - 1);
+    for (int64_t i = 0; i < dim; i++) {
+        if ((i & mask) == 0) {
+            int64_t j = i | mask;
+            psi[j] = psi[i];
+            psi[i] = 0;
+        }
+    }
+}
+double so_population_excited_psi(const C* psi, int k, int N) { /* :784-796 */
+    int64_t dim = 1LL << N, mask = 1LL << (k - 1);
+    double r = 0;
+    for (int64_t i = 0; i < dim; i++)
+        if (i & mask) r += creal(psi[i]) * creal(psi[i]) + cimag(psi[i]) * cimag(psi[i]);
+    return r;
+}
+
+/* ========================================================================
+ * Generic bitwise gates
+ * ======================================================================== */
+void so_apply_one_qubit_gate(C* psi, const double* U, int qubit, int N) {
+    /* cpuQuantumChannelUnitaryEvolutionTrotter.jl:77-99 */
+    int64_t dim = 1LL << N, step = 1LL << (qubit - 1);
+    C u00 = mat(U, 2, 0, 0), u01 = mat(U, 2, 0, 1), u10 = mat(U, 2, 1, 0), u11 = mat(U, 2, 1, 1);
+    for (int64_t b = 0; b < dim; b++) {
+        if ((b & step) == 0) {
+            C a0 = psi[b], a1 = psi[b + step];
+            psi[b] = u00 * a0 + u01 * a1;
+            psi[b + step] = u10 * a0 + u11 * a1;
+        }
+    }
+}
+static void two_qubit_core(C* psi, const C u[4][4], int q1, int q2, int N) {
+    /* cpuQuantumChannelUnitaryEvolutionTrotter.jl:123-139: basis order
+     * |00>, |q1=1>, |q2=1>, |11> with q1 < q2 */
+    int64_t dim = 1LL << N, s1 = 1LL << (q1 - 1), s2 = 1LL << (q2 - 1);
+    for (int64_t b = 0; b < dim; b++) {
+        if ((b & s1) == 0 && (b & s2) == 0) {
+            int64_t i0 = b, i1 = b + s1, i2 = b + s2, i3 = b + s1 + s2;
+            C a[4] = {psi[i0], psi[i1], psi[i2], psi[i3]};
+            C o[4];
+            for (int r = 0; r < 4; r++)
+                o[r] = u[r][0] * a[0] + u[r][1] * a[1] + u[r][2] * a[2] + u[r][3] * a[3];
+            psi[i0] = o[0]; psi[i1] = o[1]; psi[i2] = o[2]; psi[i3] = o[3];
+        }
+    }
+}
+void so_apply_two_qubit_gate(C* psi, const double* U, int q1, int q2, int N) {
+    /* :107-142 -- if q1 > q2 the qubits are swapped, U is NOT permuted */
+    if (q1 > q2) { int t = q1; q1 = q2; q2 = t; }
+    C u[4][4];
+    for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++) u[r][c] = mat(U, 4, r, c);
+    two_qubit_core(psi, u, q1, q2, N);
+}
+void so_apply_2qubit_gate_ru(C* psi, const double* U, int q1, int q2, int N) {
+    /* cpuQuantumChannelRandomUnitaries.jl:317-360 -- if q1 > q2, U <- SWAP U SWAP */
+    C u[4][4];
+    int perm[4] = {0, 1, 2, 3};
+    if (q1 > q2) {
+        int t = q1; q1 = q2; q2 = t;
+        perm[1] = 2; perm[2] = 1;
+    }
+    for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++) u[r][c] = mat(U, 4, perm[r], perm[c]);
+    two_qubit_core(psi, u, q1, q2, N);
+}
+
+/* ========================================================================
+ * Observables -- utils/cpu/cpuQuantumStateObservables.jl
+ * ======================================================================== */
+static inline double abs2(C z) { return creal(z) * creal(z) + cimag(z) * cimag(z); }
+double so_expect_z(const C* psi, int k, int N) { /* :201-210 */
+    int64_t dim = 1LL << N;
+    double r = 0;
+    for (int64_t i = 0; i < dim; i++) r += abs2(psi[i]) * (double)(1 - 2 * ((i >> (k - 1)) & 1));
+    return r;
+}
+double so_expect_x(const C* psi, int k, int N) { /* :230-240 */
+    int64_t dim = 1LL << N, step = 1LL << (k - 1);
+    double r = 0;
+    for (int64_t i = 0; i < dim; i++)
+        if (((i >> (k - 1)) & 1) == 0) r += 2 * creal(conj(psi[i]) * psi[i + step]);
+    return r;
+}
+double so_expect_y(const C* psi, int k, int N) { /* :256-267 (code sign: +2 Im) */
+    int64_t dim = 1LL << N, step = 1LL << (k - 1);
+    double r = 0;
+    for (int64_t i = 0; i < dim; i++)
+        if (((i >> (k - 1)) & 1) == 0) r += 2 * cimag(conj(psi[i]) * psi[i + step]);
+    return r;
+}
+double so_expect_zz(const C* psi, int i, int j, int N) { /* :341-352 */
+    int64_t dim = 1LL << N;
+    double r = 0;
+    for (int64_t s = 0; s < dim; s++) {
+        int bi = (s >> (i - 1)) & 1, bj = (s >> (j - 1)) & 1;
+        r += abs2(psi[s]) * (double)(1 - 2 * (bi ^ bj));
+    }
+    return r;
+}
+static double corr_pairs(const C* psi, int i, int j, int N, double s0011) {
+    int64_t dim = 1LL << N, si = 1LL << (i - 1), sj = 1LL << (j - 1);
+    double r = 0;
+    for (int64_t s = 0; s < dim; s++) {
+        if (((s >> (i - 1)) & 1) == 0 && ((s >> (j - 1)) & 1) == 0) {
+            r += s0011 * 2 * creal(conj(psi[s]) * psi[s + si + sj]);
+            r += 2 * creal(conj(psi[s + sj]) * psi[s + si]);
+        }
+    }
+    return r;
+}
+double so_expect_xx(const C* psi, int i, int j, int N) { return corr_pairs(psi, i, j, N, 1.0); }  /* :385 */
+double so_expect_yy(const C* psi, int i, int j, int N) { return corr_pairs(psi, i, j, N, -1.0); } /* :427 */
+
+double so_norm2(const C* psi, int N) {
+    int64_t dim = 1LL << N;
+    double r = 0;
+    for (int64_t i = 0; i < dim; i++) r += abs2(psi[i]);
+    return r;
+}
+
+/* Pauli string expectation.  Z-only strings: _expect_pauli_Z_string (:900).
+ * Mixed strings: _expect_pauli_mixed_string (:948) visits each base with all
+ * X/Y bits 0 and each flip pattern once and adds Re(coeff psi_bra^* psi_ket),
+ * i.e. only the (bra<ket) half of the Hermitian sum -- its own docstring
+ * example (GHZ <XXX> = 1, :835) comes out 0.5 from that loop.  This oracle
+ * (and the CUDA library) returns the full expectation
+ *     <P> = sum_i conj(psi_i) * phase(i) * psi_{i ^ flipmask}
+ * which equals _expect_X/_expect_XX/_expect_YY (:230/:385/:427) on 1- and
+ * 2-body strings, where the reference is self-consistent. */
+double so_expect_pauli_string(const C* psi, int n, const char* ops, const int* qubits, int N) {
+    int64_t dim = 1LL << N, xmask = 0, zmask = 0;
+    int ny = 0;
+    for (int t = 0; t < n; t++) {
+        int64_t b = 1LL << (qubits[t] - 1);
+        char o = ops[t];
+        if (o == 'X' || o == 'x') xmask |= b;
+        else if (o == 'Y' || o == 'y') { xmask |= b; zmask |= b; ny++; }
+        else if (o == 'Z' || o == 'z') zmask |= b;
+    }
+    if (xmask == 0) { /* :900-930 */
+        double r = 0;
+        for (int64_t i = 0; i < dim; i++)
+            r += abs2(psi[i]) * (double)(1 - 2 * (__builtin_popcountll(i & zmask) & 1));
+        return r;
+    }
+    /* P|i> = i^{ny} (-1)^{popc(i & zmask)} |i ^ xmask>  with Y = i X Z */
+    C iy = 1;
+    for (int t = 0; t < ny; t++) iy *= I_;
+    C acc = 0;
+    for (int64_t i = 0; i < dim; i++) {
+        int64_t j = i ^ xmask;
+        double sg = (double)(1 - 2 * (__builtin_popcountll(i & zmask) & 1));
+        acc += conj(psi[j]) * iy * sg * psi[i];
+    }
+    return creal(acc);
+}
+
+/* ========================================================================
+ * Trotter -- utils/cpu/cpuQuantumChannelUnitaryEvolutionTrotter.jl
+ * ======================================================================== */
+static void put(double* U, int n, int r, int c, C v) {
+    U[2 * (c * n + r)] = creal(v);
+    U[2 * (c * n + r) + 1] = cimag(v);
+}
+int so_precompute_trotter_gates(const double* bonds, int nb, const double* fields, int nf,
+                                double dt, so_trotter_gate* out) {
+    /* :322-354.  exp(-i dt (Jx XX + Jy YY + Jz ZZ)): XX, YY, ZZ commute, so the
+     * exponential is the product of the three, and in the basis
+     * |00>,|01>,|10>,|11> (kron(A_hi, B_lo), Julia's kron order) it is block
+     * diagonal on {|00>,|11>} and {|01>,|10>}:
+     *   XX: |00><->|11>, |01><->|10> with +1;  YY: |00><->|11> with -1,
+     *   |01><->|10> with +1;  ZZ: +1 on 00/11, -1 on 01/10.
+     * even block {00,11}: H = Jz I + (Jx - Jy) sx  -> e^{-i Jz dt}(cos a I - i sin a sx), a=(Jx-Jy)dt
+     * odd  block {01,10}: H = -Jz I + (Jx + Jy) sx -> e^{+i Jz dt}(cos b I - i sin b sx), b=(Jx+Jy)dt */
+    int n = 0;
+    for (int t = 0; t < nb; t++) {
+        const double* b = bonds + 5 * t;
+        double Jx = b[2], Jy = b[3], Jz = b[4];
+        so_trotter_gate* g = out + n++;
+        memset(g, 0, sizeof(*g));
+        g->nq = 2; g->q[0] = (int)b[0]; g->q[1] = (int)b[1];
+        double a = (Jx - Jy) * dt, bb = (Jx + Jy) * dt;
+        C pe = cexp(-I_ * Jz * dt), po = cexp(I_ * Jz * dt);
+        put(g->U, 4, 0, 0, pe * cos(a)); put(g->U, 4, 3, 3, pe * cos(a));
+        put(g->U, 4, 0, 3, pe * (-I_ * sin(a))); put(g->U, 4, 3, 0, pe * (-I_ * sin(a)));
+        put(g->U, 4, 1, 1, po * cos(bb)); put(g->U, 4, 2, 2, po * cos(bb));
+        put(g->U, 4, 1, 2, po * (-I_ * sin(bb))); put(g->U, 4, 2, 1, po * (-I_ * sin(bb)));
+    }
+    for (int t = 0; t < nf; t++) {
+        const double* f = fields + 4 * t;
+        double hx = f[1], hy = f[2], hz = f[3];
+        if (!(fabs(hx) > 1e-14 || fabs(hy) > 1e-14 || fabs(hz) > 1e-14)) continue; /* :346 */
+        /* exp(-i dt h.sigma) = cos(|h|dt) I - i sin(|h|dt) (h.sigma)/|h| */
+        double h = sqrt(hx * hx + hy * hy + hz * hz), c = cos(h * dt), s = sin(h * dt) / h;
+        so_trotter_gate* g = out + n++;
+        memset(g, 0, sizeof(*g));
+        g->nq = 1; g->q[0] = (int)f[0];
+        put(g->U, 2, 0, 0, c - I_ * s * hz);
+        put(g->U, 2, 1, 1, c + I_ * s * hz);
+        put(g->U, 2, 0, 1, -I_ * s * (hx - I_ * hy));
+        put(g->U, 2, 1, 0, -I_ * s * (hx + I_ * hy));
+    }
+    return n;
+}
+void so_trotter_step(C* psi, const so_trotter_gate* g, int n, int N) { /* :150-162 */
+    for (int t = 0; t < n; t++) {
+        if (g[t].nq == 1) so_apply_one_qubit_gate(psi, g[t].U, g[t].q[0], N);
+        else so_apply_two_qubit_gate(psi, g[t].U, g[t].q[0], g[t].q[1], N);
+    }
+}
+
+/* ========================================================================
+ * Circuits -- cpuVariationalQuantumCircuitExecutor.jl:95-180
+ * ======================================================================== */
+void so_apply_circuit(C* psi, const so_op* ops, int n, const double* theta, int N) {
+    for (int t = 0; t < n; t++) {
+        const so_op* o = ops + t;
+        double a = o->param > 0 ? theta[o->param - 1] : o->angle; /* :147 */
+        const int* q = o->q;
+        switch (o->type) {
+        case SO_G_RX: so_apply_rx_psi(psi, q[0], a, N); break;
+        case SO_G_RY: so_apply_ry_psi(psi, q[0], a, N); break;
+        case SO_G_RZ: so_apply_rz_psi(psi, q[0], a, N); break;
+        case SO_G_H: so_apply_hadamard_psi(psi, q[0], N); break;
+        case SO_G_X: so_apply_pauli_x_psi(psi, q[0], N); break;
+        case SO_G_Y: so_apply_pauli_y_psi(psi, q[0], N); break;
+        case SO_G_Z: so_apply_pauli_z_psi(psi, q[0], N); break;
+        case SO_G_S: so_apply_s_psi(psi, q[0], N); break;
+        case SO_G_SDG: so_apply_sdagger_psi(psi, q[0], N); break;
+        case SO_G_T: so_apply_t_psi(psi, q[0], N); break;
+        case SO_G_TDG: so_apply_tdagger_psi(psi, q[0], N); break;
+        case SO_G_CZ: so_apply_cz_psi(psi, q[0], q[1], N); break;
+        case SO_G_CNOT: so_apply_cnot_psi(psi, q[0], q[1], N); break;
+        case SO_G_RXX: so_apply_rxx_psi(psi, q[0], q[1], a, N); break;
+        case SO_G_RYY: so_apply_ryy_psi(psi, q[0], q[1], a, N); break;
+        case SO_G_RZZ: so_apply_rzz_psi(psi, q[0], q[1], a, N); break;
+        case SO_G_CRY: so_apply_cry_psi(psi, q[0], q[1], a, N); break;
+        case SO_G_CCZ: so_apply_ccz_psi(psi, q[0], q[1], q[2], N); break;
+        case SO_G_TOFFOLI: so_apply_toffoli_psi(psi, q[0], q[1], q[2], N); break;
+        default: break;
+        }
+    }
+}
+
+double so_pauli_sum_expect(const C* psi, int nterms, const double* coef, const char* paulis, int N) {
+    double e = 0;
+    char ops[64];
+    int qs[64];
+    for (int t = 0; t < nterms; t++) {
+        int n = 0;
+        for (int q = 0; q < N; q++) {
+            char p = paulis[(size_t)t * N + q];
+            if (p == 'X' || p == 'Y' || p == 'Z') { ops[n] = p; qs[n] = q + 1; n++; }
+        }
+        e += coef[t] * (n ? so_expect_pauli_string(psi, n, ops, qs, N) : so_norm2(psi, N));
+    }
+    return e;
+}
+
+double so_energy(const so_op* ops, int n, const double* theta, int N, int nterms,
+                 const double* coef, const char* paulis) {
+    int64_t dim = 1LL << N;
+    C* psi = (C*)calloc(dim, sizeof(C));
+    psi[0] = 1;
+    so_apply_circuit(psi, ops, n, theta, N);
+    double e = so_pauli_sum_expect(psi, nterms, coef, paulis, N);
+    free(psi);
+    return e;
+}
+
+void so_grad_parameter_shift(const so_op* ops, int n, const double* theta, int P, int N,
+                             int nterms, const double* coef, const char* paulis, double shift,
+                             const int* which, int nwhich, double* grad) {
+    /* cpuVariationalQuantumCircuitGradients.jl:138-163 */
+    double* tp = (double*)malloc(P * sizeof(double));
+    memcpy(tp, theta, P * sizeof(double));
+    for (int w = 0; w < nwhich; w++) {
+        int k = which[w];
+        tp[k] = theta[k] + shift;
+        double cp = so_energy(ops, n, tp, N, nterms, coef, paulis);
+        tp[k] = theta[k] - shift;
+        double cm = so_energy(ops, n, tp, N, nterms, coef, paulis);
+        grad[w] = (cp - cm) / (2 * sin(shift));
+        tp[k] = theta[k];
+    }
+    free(tp);
+}
+
+void so_grad_finite_difference(const so_op* ops, int n, const double* theta, int P, int N,
+                               int nterms, const double* coef, const char* paulis, double eps,
+                               const int* which, int nwhich, double* grad) {
+    /* cpuVariationalQuantumCircuitGradients.jl:250-269 */
+    double* tw = (double*)malloc(P * sizeof(double));
+    memcpy(tw, theta, P * sizeof(double));
+    for (int w = 0; w < nwhich; w++) {
+        int k = which[w];
+        tw[k] = theta[k] + eps;
+        double cp = so_energy(ops, n, tw, N, nterms, coef, paulis);
+        tw[k] = theta[k] - eps;
+        double cm = so_energy(ops, n, tw, N, nterms, coef, paulis);
+        grad[w] = (cp - cm) / (2 * eps);
+        tw[k] = theta[k];
+    }
+    free(tw);
+}
+
+/* ========================================================================
+ * Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+ * easy as 1, 2, 3", SC'11): 10 rounds of the 4x32 S-box with multipliers
+ * 0xD2511F53 / 0xCD9E8D57 and Weyl key increments 0x9E3779B9 / 0xBB67AE85,
+ * all as published in the paper.
+ * ======================================================================== */
+void so_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3], k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; r++) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+double so_u01_from_words(uint32_t hi, uint32_t lo) {
+    /* 53-bit uniform in [0,1): 27 bits of hi, 26 bits of lo */
+    uint64_t a = hi >> 5, b = lo >> 6;
+    return (double)(a * 67108864ull + b) * (1.0 / 9007199254740992.0);
+}
+
+/* ========================================================================
+ * MCWF step -- the rule shared with the CUDA library.
+ *
+ * 1. coherent step: the first-order Trotter gate list (lindblad_mcwf_step_trotter!,
+ *    cpuQuantumChannelLindbladianEvolutionMonteCarloWaveFunction.jl:282);
+ * 2. no-jump decay, amplitude-wise
+ *      psi_i *= sqrt(1 - dt * sum_{sigma_z, sigma_x ops} gamma)          (:285, L^dag L = I)
+ *             * prod_{sigma_minus on k, bit k set}   sqrt(1 - gamma dt)  (:353-358, decay^popcount)
+ *             * prod_{sigma_plus  on k, bit k clear} sqrt(1 - gamma dt);
+ * 3. norm_sq = ||psi~||^2 in FP64, dp = 1 - norm_sq (:289-290);
+ * 4. u1, u2 = two 53-bit uniforms from Philox4x32-10 with counter
+ *    (step_lo, step_hi, traj_lo, traj_hi) and key (seed_lo, seed_hi);
+ * 5. jump iff u1 < dp && dp > 0 (:293).  The channel is chosen with the
+ *    independent u2 (the reference reuses r, caveat at :364-377) by weights
+ *    w_c = gamma_c dt <L_c^dag L_c>_{psi~} / norm_sq, walking the op list in
+ *    order and taking the first c with cumulative > u2 * sum(w);
+ * 6. renormalise (:303 / :381-384): the post-jump norm^2 is the excited (ground)
+ *    population for sigma_minus (sigma_plus) and norm_sq for sigma_z/sigma_x.
+ * ======================================================================== */
+static double pop_bit(const C* psi, int64_t dim, int64_t mask, int set) {
+    double r = 0;
+    for (int64_t i = 0; i < dim; i++)
+        if (((i & mask) != 0) == set) r += abs2(psi[i]);
+    return r;
+}
+int so_mcwf_step(C* psi, int N, const so_trotter_gate* g, int ng, const so_jump_op* ops,
+                 int nops, double dt, uint64_t seed, uint64_t traj, uint64_t step) {
+    int64_t dim = 1LL << N;
+    so_trotter_step(psi, g, ng, N);
+    double gz = 0;
+    for (int o = 0; o < nops; o++)
+        if (ops[o].type == 2 || ops[o].type == 3) gz += ops[o].gamma;
+    double fu = sqrt(1.0 - dt * gz);
+    for (int64_t i = 0; i < dim; i++) {
+        double f = fu;
+        for (int o = 0; o < nops; o++) {
+            int bit = (int)((i >> (ops[o].qubit - 1)) & 1);
+            if ((ops[o].type == 0 && bit) || (ops[o].type == 1 && !bit))
+                f *= sqrt(1.0 - ops[o].gamma * dt);
+        }
+        psi[i] *= f;
+    }
+    double norm_sq = so_norm2(psi, N), dp = 1.0 - norm_sq;
+    uint32_t ctr[4] = {(uint32_t)step, (uint32_t)(step >> 32), (uint32_t)traj, (uint32_t)(traj >> 32)};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t w[4];
+    so_philox4x32_10(ctr, key, w);
+    double u1 = so_u01_from_words(w[0], w[1]), u2 = so_u01_from_words(w[2], w[3]);
+    int chosen = -1;
+    double new_norm_sq = norm_sq;
+    if (u1 < dp && dp > 0) {
+        double wsum = 0;
+        double* wt = (double*)malloc((nops > 0 ? nops : 1) * sizeof(double));
+        double* pops = (double*)malloc((nops > 0 ? nops : 1) * sizeof(double));
+        for (int o = 0; o < nops; o++) {
+            int64_t mask = 1LL << (ops[o].qubit - 1);
+            double ev;
+            if (ops[o].type == 0) pops[o] = ev = pop_bit(psi, dim, mask, 1);
+            else if (ops[o].type == 1) pops[o] = ev = pop_bit(psi, dim, mask, 0);
+            else { pops[o] = norm_sq; ev = norm_sq; }
+            wt[o] = ops[o].gamma * dt * ev / norm_sq;
+            wsum += wt[o];
+        }
+        if (wsum > 0) {
+            double target = u2 * wsum, cum = 0;
+            chosen = nops - 1;
+            for (int o = 0; o < nops; o++) {
+                cum += wt[o];
+                if (target < cum) { chosen = o; break; }
+            }
+            int k = ops[chosen].qubit;
+            switch (ops[chosen].type) {
+            case 0: so_apply_sigma_minus_psi(psi, k, N); break;
+            case 1: so_apply_sigma_plus_psi(psi, k, N); break;
+            case 2: so_apply_pauli_z_psi(psi, k, N); break;
+            case 3: so_apply_pauli_x_psi(psi, k, N); break;
+            }
+            new_norm_sq = pops[chosen];
+        }
+        free(wt);
+        free(pops);
+    }
+    double inv = 1.0 / sqrt(new_norm_sq);
+    for (int64_t i = 0; i < dim; i++) psi[i] *= inv;
+    return chosen;
+}
+
+typedef struct {
+    int N, ng, nops, steps, record_every, ntraj, nthreads, tid;
+    const so_trotter_gate* g;
+    const so_jump_op* ops;
+    double dt;
+    uint64_t seed, t0, init_index;
+    double *z_out, *zz_out;
+    int* njumps;
+} mcwf_job;
+
+static void* mcwf_worker(void* arg) {
+    mcwf_job* J = (mcwf_job*)arg;
+    int N = J->N;
+    int64_t dim = 1LL << N;
+    C* psi = (C*)malloc(dim * sizeof(C));
+    for (int t = J->tid; t < J->ntraj; t += J->nthreads) { /* static round-robin */
+        memset(psi, 0, dim * sizeof(C));
+        psi[J->init_index] = 1;
+        int jumps = 0, r = 0;
+        for (int s = 0; s <= J->steps; s++) {
+            if (s > 0 && so_mcwf_step(psi, N, J->g, J->ng, J->ops, J->nops, J->dt, J->seed,
+                                      J->t0 + t, (uint64_t)(s - 1)) >= 0)
+                jumps++;
+            if (s % J->record_every == 0) {
+                for (int q = 1; q <= N; q++)
+                    J->z_out[((size_t)r * J->ntraj + t) * N + q - 1] = so_expect_z(psi, q, N);
+                for (int q = 1; q < N; q++)
+                    J->zz_out[((size_t)r * J->ntraj + t) * (N - 1) + q - 1] = so_expect_zz(psi, q, q + 1, N);
+                r++;
+            }
+        }
+        if (J->njumps) J->njumps[t] = jumps;
+    }
+    free(psi);
+    return NULL;
+}
+
+void so_mcwf_run(int N, const so_trotter_gate* g, int ng, const so_jump_op* ops, int nops,
+                 double dt, uint64_t seed, uint64_t t0, int ntraj, int steps, int record_every,
+                 uint64_t init_index, double* z_out, double* zz_out, int* njumps, int nthreads) {
+    /* trajectories are independent: spread them over host threads, as the
+     * reference's Threads.@threads over trajectories does */
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > ntraj) nthreads = ntraj > 0 ? ntraj : 1;
+    mcwf_job* jobs = (mcwf_job*)calloc(nthreads, sizeof(mcwf_job));
+    pthread_t* th = (pthread_t*)calloc(nthreads, sizeof(pthread_t));
+    for (int i = 0; i < nthreads; i++) {
+        mcwf_job J = {N, ng, nops, steps, record_every, ntraj, nthreads, i, g, ops, dt,
+                      seed, t0, init_index, z_out, zz_out, njumps};
+        jobs[i] = J;
+    }
+    for (int i = 1; i < nthreads; i++) pthread_create(&th[i], NULL, mcwf_worker, &jobs[i]);
+    mcwf_worker(&jobs[0]);
+    for (int i = 1; i < nthreads; i++) pthread_join(th[i], NULL);
+    free(jobs);
+    free(th);
+}
+
+/* ========================================================================
+ * Density-matrix oracle (column-major rho[(j * dim) + i] = rho_ij)
+ * ======================================================================== */
+static void rows_apply(C* rho, int64_t dim, const so_trotter_gate* g, const C u[4][4], int nq) {
+    /* right-multiply by U^dag on rows, as apply_fast_trotter_gates_to_matrix_rows_cpu!
+     * (:178-230) does with the conjugated gates: M[i, c] = sum conj(U)[c, c'] M[i, c'] */
+    if (nq == 1) {
+        int64_t step = 1LL << (g->q[0] - 1);
+        for (int64_t k = 0; k < dim; k++) {
+            if (k & step) continue;
+            for (int64_t i = 0; i < dim; i++) {
+                C a0 = rho[k * dim + i], a1 = rho[(k + step) * dim + i];
+                rho[k * dim + i] = conj(u[0][0]) * a0 + conj(u[0][1]) * a1;
+                rho[(k + step) * dim + i] = conj(u[1][0]) * a0 + conj(u[1][1]) * a1;
+            }
+        }
+    } else {
+        int q1 = g->q[0], q2 = g->q[1];
+        int64_t s1 = 1LL << (q1 - 1), s2 = 1LL << (q2 - 1);
+        for (int64_t k = 0; k < dim; k++) {
+            if ((k & s1) || (k & s2)) continue;
+            int64_t c[4] = {k, k + s1, k + s2, k + s1 + s2};
+            for (int64_t i = 0; i < dim; i++) {
+                C v[4], o[4];
+                for (int a = 0; a < 4; a++) v[a] = rho[c[a] * dim + i];
+                for (int r = 0; r < 4; r++)
+                    o[r] = conj(u[r][0]) * v[0] + conj(u[r][1]) * v[1] + conj(u[r][2]) * v[2] + conj(u[r][3]) * v[3];
+                for (int a = 0; a < 4; a++) rho[c[a] * dim + i] = o[a];
+            }
+        }
+    }
+}
+void so_trotter_step_rho(C* rho, const so_trotter_gate* g, int n, int N) {
+    /* evolve_trotter_rho_cpu! (:266-285): U on every column, then U^dag on rows */
+    int64_t dim = 1LL << N;
+    for (int64_t j = 0; j < dim; j++) so_trotter_step(rho + j * dim, g, n, N);
+    for (int t = 0; t < n; t++) {
+        C u[4][4];
+        int nn = g[t].nq == 1 ? 2 : 4;
+        for (int r = 0; r < nn; r++)
+            for (int c = 0; c < nn; c++) u[r][c] = mat(g[t].U, nn, r, c);
+        /* 2-qubit row gates: the reference row kernel does not swap q1>q2;
+         * gates built by the precompute have q1 < q2 */
+        rows_apply(rho, dim, g + t, u, g[t].nq);
+    }
+}
+void so_dissipator_dm(C* rho, const so_jump_op* op, double dt, int N) {
+    /* _apply_dissipator_dm! (cpuQuantumChannelLindbladianEvolution.jl:377-460),
+     * same in-place loop order (j outer, i inner) */
+    int64_t dim = 1LL << N, mask = 1LL << (op->qubit - 1);
+    double f = op->gamma * dt;
+    int qb = op->qubit - 1;
+    for (int64_t j = 0; j < dim; j++) {
+        for (int64_t i = 0; i < dim; i++) {
+            int bi = (int)((i >> qb) & 1), bj = (int)((j >> qb) & 1);
+            C* rij = rho + j * dim + i;
+            if (op->type == 0) {
+                if (bi && bj) {
+                    rho[(j ^ mask) * dim + (i ^ mask)] += f * (*rij);
+                    *rij *= (1 - f);
+                } else if (bi || bj) *rij *= (1 - 0.5 * f);
+            } else if (op->type == 1) {
+                if (!bi && !bj) {
+                    rho[(j ^ mask) * dim + (i ^ mask)] += f * (*rij);
+                    *rij *= (1 - f);
+                } else if (!bi || !bj) *rij *= (1 - 0.5 * f);
+            } else if (op->type == 2) {
+                if (bi != bj) *rij *= (1 - 2 * f);
+            } else {
+                int64_t ifl = i ^ mask, jfl = j ^ mask;
+                if (i < ifl || (i == ifl && j < jfl)) {
+                    C vo = *rij, vf = rho[jfl * dim + ifl];
+                    *rij += f * (vf - vo);
+                    rho[jfl * dim + ifl] += f * (vo - vf);
+                }
+            }
+        }
+    }
+}
+double so_expect_z_rho(const C* rho, int k, int N) {
+    int64_t dim = 1LL << N;
+    double r = 0;
+    for (int64_t i = 0; i < dim; i++) r += creal(rho[i * dim + i]) * (double)(1 - 2 * ((i >> (k - 1)) & 1));
+    return r;
+}
+double so_expect_zz_rho(const C* rho, int a, int b, int N) {
+    int64_t dim = 1LL << N;
+    double r = 0;
+    for (int64_t i = 0; i < dim; i++)
+        r += creal(rho[i * dim + i]) * (double)(1 - 2 * (((i >> (a - 1)) ^ (i >> (b - 1))) & 1));
+    return r;
+}

@@ -1,0 +1,169 @@
+/*
+ * smoq_oracle.h -- CPU restatement of SmoQ.jl's matrix-free state-vector path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA
+ * library (libsmoq_cuda.so): only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / --impl reference legs of bench.py may load it.  It is never
+ * the thing measured on the GPU path and never shipped behind the C-ABI.
+ *
+ * Conventions follow the reference exactly:
+ *   - states are complex128 (C99 double complex == Julia ComplexF64 layout),
+ *     length 2^N, little-endian: qubit k (1-based) <-> bit k-1;
+ *   - every gate/observable entry point takes 1-based qubits like the Julia
+ *     functions it restates (the utils/cpu Julia files), and the loops keep the
+ *     reference's shape (scan all 2^N indices, branch on the bit) so that the
+ *     CPU baseline times the same work the reference does;
+ *   - 2x2 / 4x4 matrices are passed column-major (Julia Matrix memory order)
+ *     as interleaved (re, im) doubles.
+ *
+ * Parity pins: tests/test_oracle_golden.py checks this restatement against
+ * the known-answer tests the reference's own demo suites hold
+ * (scripts_variational_quantum_circuits/demo_parametrized_gates.jl, the
+ * docstring examples in utils/cpu/cpuQuantumStateObservables.jl, the
+ * PS-vs-FD check of demo_VQC_base_test.jl) and against an independent dense
+ * kron-product restatement written in numpy.
+ */
+#ifndef SMOQ_ORACLE_H
+#define SMOQ_ORACLE_H
+#include <complex.h>
+#include <stdint.h>
+
+typedef double _Complex so_cplx;
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- single-qubit gates: utils/cpu/cpuQuantumChannelGates.jl ---- */
+void so_apply_rx_psi(so_cplx* psi, int k, double theta, int N);   /* :142 */
+void so_apply_ry_psi(so_cplx* psi, int k, double theta, int N);   /* :172 */
+void so_apply_rz_psi(so_cplx* psi, int k, double theta, int N);   /* :201 */
+void so_apply_hadamard_psi(so_cplx* psi, int k, int N);           /* :222 */
+void so_apply_pauli_x_psi(so_cplx* psi, int k, int N);            /* :245 */
+void so_apply_pauli_y_psi(so_cplx* psi, int k, int N);            /* :265 */
+void so_apply_pauli_z_psi(so_cplx* psi, int k, int N);            /* :286 */
+void so_apply_s_psi(so_cplx* psi, int k, int N);                  /* :307 */
+void so_apply_sdagger_psi(so_cplx* psi, int k, int N);            /* :328 */
+void so_apply_t_psi(so_cplx* psi, int k, int N);                  /* :360 */
+void so_apply_tdagger_psi(so_cplx* psi, int k, int N);            /* :380 */
+/* ---- multi-qubit gates ---- */
+void so_apply_ccz_psi(so_cplx* psi, int q1, int q2, int q3, int N);     /* :448 */
+void so_apply_toffoli_psi(so_cplx* psi, int c1, int c2, int t, int N);  /* :471 */
+void so_apply_cnot_psi(so_cplx* psi, int control, int target, int N);   /* :870 */
+void so_apply_cz_psi(so_cplx* psi, int qi, int qj, int N);              /* :889 */
+void so_apply_cry_psi(so_cplx* psi, int control, int target, double theta, int N); /* :914 */
+void so_apply_rxx_psi(so_cplx* psi, int qi, int qj, double theta, int N); /* :992 */
+void so_apply_ryy_psi(so_cplx* psi, int qi, int qj, double theta, int N); /* :1039 */
+void so_apply_rzz_psi(so_cplx* psi, int qi, int qj, double theta, int N); /* :1084 */
+/* ---- jump operators ---- */
+void so_apply_sigma_minus_psi(so_cplx* psi, int k, int N);   /* :739 */
+void so_apply_sigma_plus_psi(so_cplx* psi, int k, int N);    /* :762 */
+double so_population_excited_psi(const so_cplx* psi, int k, int N); /* :784 */
+
+/* ---- generic bitwise gates ---- */
+/* utils/cpu/cpuQuantumChannelUnitaryEvolutionTrotter.jl:77 */
+void so_apply_one_qubit_gate(so_cplx* psi, const double* U, int qubit, int N);
+/* utils/cpu/cpuQuantumChannelUnitaryEvolutionTrotter.jl:107 (q1/q2 swapped
+ * without permuting U when q1 > q2) */
+void so_apply_two_qubit_gate(so_cplx* psi, const double* U, int q1, int q2, int N);
+/* utils/cpu/cpuQuantumChannelRandomUnitaries.jl:317 (U conjugated by SWAP
+ * when q1 > q2) */
+void so_apply_2qubit_gate_ru(so_cplx* psi, const double* U, int q1, int q2, int N);
+
+/* ---- observables: utils/cpu/cpuQuantumStateObservables.jl ---- */
+double so_expect_z(const so_cplx* psi, int k, int N);   /* :201 */
+double so_expect_x(const so_cplx* psi, int k, int N);   /* :230 */
+double so_expect_y(const so_cplx* psi, int k, int N);   /* :256 */
+double so_expect_zz(const so_cplx* psi, int i, int j, int N); /* :341 */
+double so_expect_xx(const so_cplx* psi, int i, int j, int N); /* :385 */
+double so_expect_yy(const so_cplx* psi, int i, int j, int N); /* :427 */
+/* Pauli string <P>, ops[i] in {'X','Y','Z'} on 1-based qubits[i].  Z-only
+ * strings follow _expect_pauli_Z_string (:900).  Mixed strings sum the full
+ * Hermitian pair (bra,ket)+(ket,bra); see the Q1 note in the .c file. */
+double so_expect_pauli_string(const so_cplx* psi, int n, const char* ops,
+                              const int* qubits, int N);
+double so_norm2(const so_cplx* psi, int N);
+
+/* ---- Trotter: utils/cpu/cpuQuantumChannelUnitaryEvolutionTrotter.jl ---- */
+typedef struct {
+    int32_t nq;       /* 1 or 2 */
+    int32_t q[2];     /* 1-based qubits (FastTrotterGate.indices) */
+    int32_t pad;
+    double U[32];     /* column-major interleaved complex; 2x2 uses U[0..7] */
+} so_trotter_gate;
+/* closed-form restatement of precompute_trotter_gates_bitwise_cpu (:322):
+ * bonds (i, j, Jxx, Jyy, Jzz) then fields (idx, hx, hy, hz); gates with
+ * |h| <= 1e-14 are dropped as in :346.  Returns the number of gates. */
+int so_precompute_trotter_gates(const double* bonds, int nb, const double* fields,
+                                int nf, double dt, so_trotter_gate* out);
+/* apply_fast_trotter_step_cpu! (:150) */
+void so_trotter_step(so_cplx* psi, const so_trotter_gate* g, int n, int N);
+
+/* ---- circuits: utils/cpu/cpuVariationalQuantumCircuitExecutor.jl ---- */
+typedef struct {
+    int32_t type;     /* SO_G_* */
+    int32_t q[3];     /* 1-based */
+    int32_t param;    /* 0 = fixed angle, >0 = theta[param-1] (CircuitOperation.param_idx) */
+    int32_t pad;
+    double angle;
+} so_op;
+enum { SO_G_RX = 0, SO_G_RY, SO_G_RZ, SO_G_H, SO_G_X, SO_G_Y, SO_G_Z, SO_G_S,
+       SO_G_SDG, SO_G_T, SO_G_TDG, SO_G_CZ, SO_G_CNOT, SO_G_RXX, SO_G_RYY,
+       SO_G_RZZ, SO_G_CRY, SO_G_CCZ, SO_G_TOFFOLI };
+/* apply_circuit! (:95) -> apply_gate_psi! (:146) */
+void so_apply_circuit(so_cplx* psi, const so_op* ops, int n, const double* theta, int N);
+
+/* Pauli-sum observable: term t has coefficient coef[t] and, for each 1-based
+ * qubit, a letter in paulis[t*N + q-1] ('I','X','Y','Z'). */
+double so_pauli_sum_expect(const so_cplx* psi, int nterms, const double* coef,
+                           const char* paulis, int N);
+/* E(theta) = <0|U(theta)^dag H U(theta)|0> (the VQE cost closures of
+ * scripts_variational_quantum_circuits/demo_vqe_dm_vs_mcwf.jl:189-202) */
+double so_energy(const so_op* ops, int n, const double* theta, int N, int nterms,
+                 const double* coef, const char* paulis);
+/* calculate_gradients_parameter_shift (cpuVariationalQuantumCircuitGradients.jl:138) */
+void so_grad_parameter_shift(const so_op* ops, int n, const double* theta, int P, int N,
+                             int nterms, const double* coef, const char* paulis,
+                             double shift, const int* which, int nwhich, double* grad);
+/* calculate_gradients_finite_difference (:250) */
+void so_grad_finite_difference(const so_op* ops, int n, const double* theta, int P, int N,
+                               int nterms, const double* coef, const char* paulis,
+                               double eps, const int* which, int nwhich, double* grad);
+
+/* ---- counter-based RNG (Philox4x32-10, Salmon et al., SC'11) ---- */
+void so_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+double so_u01_from_words(uint32_t hi, uint32_t lo);
+
+/* ---- MCWF (batched trajectories) ----
+ * jump op types: 0 = sigma_minus, 1 = sigma_plus, 2 = sigma_z, 3 = sigma_x
+ * (JumpOperator, utils/cpu/cpuQuantumChannelLindbladianEvolution.jl:65). */
+typedef struct { int32_t type; int32_t qubit; double gamma; } so_jump_op;
+/* One first-order quantum-jump step on one trajectory (see the .c file for
+ * the exact rule and the reference lines each part follows).  Returns the
+ * index of the jump channel taken, or -1. */
+int so_mcwf_step(so_cplx* psi, int N, const so_trotter_gate* g, int ng,
+                 const so_jump_op* ops, int nops, double dt, uint64_t seed,
+                 uint64_t traj, uint64_t step);
+/* Runs trajectories [t0, t0+ntraj) of a batch from |init_index>, recording
+ * per-trajectory <Z_i> and <Z_i Z_{i+1}> every record_every steps
+ * (z_out[(r*ntraj + t)*N + i], zz_out[(r*ntraj + t)*(N-1) + i]).  OpenMP over
+ * pthreads over trajectories when nthreads > 1 (mirrors Threads.@threads). */
+void so_mcwf_run(int N, const so_trotter_gate* g, int ng, const so_jump_op* ops, int nops,
+                 double dt, uint64_t seed, uint64_t t0, int ntraj, int steps,
+                 int record_every, uint64_t init_index, double* z_out, double* zz_out,
+                 int* njumps, int nthreads);
+
+/* ---- density-matrix oracle (N <= 10) ----
+ * rho is column-major dim x dim complex128. */
+void so_trotter_step_rho(so_cplx* rho, const so_trotter_gate* g, int n, int N); /* evolve_trotter_rho_cpu! :266 */
+void so_dissipator_dm(so_cplx* rho, const so_jump_op* op, double dt, int N);    /* _apply_dissipator_dm! :377 */
+double so_expect_z_rho(const so_cplx* rho, int k, int N);
+double so_expect_zz_rho(const so_cplx* rho, int i, int j, int N);
+
+/* timing helper for the CPU baseline */
+double so_wtime(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,900 @@
+// capi.cu -- the extern "C" entry points of libsmoq_cuda.so (include/smoq_cuda.h).
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include "smoq_internal.h"
+#include "k_common.cuh"
+
+using namespace smoq;
+
+// ------------------------------------------------------------------ helpers
+static smoq_status fail(smoq_ctx* ctx, smoq_status s, const std::string& msg) {
+    if (ctx) ctx->last_error = msg;
+    return s;
+}
+static smoq_status cuda_fail(smoq_ctx* ctx, cudaError_t e, const char* where) {
+    char buf[256];
+    snprintf(buf, sizeof(buf), "%s: %s", where, cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation) return fail(ctx, SMOQ_ERR_OOM, buf);
+    return fail(ctx, SMOQ_ERR_CUDA, buf);
+}
+#define CK(ctx, call)                                              \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call); \
+    } while (0)
+
+static smoq_status check_state(smoq_state* st) {
+    if (!st || !st->ctx) return SMOQ_ERR_BADINPUT;
+    return SMOQ_OK;
+}
+static smoq_status check_q(smoq_state* st, int q, const char* what) {
+    if (q < 0 || q >= st->N) {
+        char b[160];
+        snprintf(b, sizeof(b), "%s: qubit %d out of range for N=%d", what, q, st->N);
+        return fail(st->ctx, SMOQ_ERR_BADINPUT, b);
+    }
+    return SMOQ_OK;
+}
+static smoq_status ensure_scratch(smoq_ctx* ctx, size_t doubles) {
+    const size_t bytes = doubles * sizeof(double);
+    if (bytes <= ctx->scratch_bytes) return SMOQ_OK;
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->d_scratch) cudaFree(ctx->d_scratch);
+    ctx->d_scratch = nullptr;
+    ctx->scratch_bytes = 0;
+    size_t nb = std::max(bytes, (size_t)1 << 20);
+    CK(ctx, cudaMalloc(&ctx->d_scratch, nb));
+    ctx->scratch_bytes = nb;
+    return SMOQ_OK;
+}
+static smoq_status ensure_pinned(smoq_ctx* ctx, size_t bytes) {
+    if (bytes <= ctx->pinned_bytes) return SMOQ_OK;
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    ctx->h_pinned = nullptr;
+    ctx->pinned_bytes = 0;
+    size_t nb = std::max(bytes, (size_t)1 << 20);
+    CK(ctx, cudaMallocHost((void**)&ctx->h_pinned, nb));
+    ctx->pinned_bytes = nb;
+    return SMOQ_OK;
+}
+// sync the ctx stream and turn a device error word into a status
+static smoq_status sync_check(smoq_ctx* ctx) {
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    int32_t h = 0;
+    CK(ctx, cudaMemcpy(&h, ctx->d_err, sizeof(h), cudaMemcpyDeviceToHost));
+    if (h != 0) {
+        CK(ctx, cudaMemset(ctx->d_err, 0, sizeof(int32_t)));
+        if (h == DEVERR_TIMEOUT) return fail(ctx, SMOQ_ERR_TIMEOUT, "a bounded device wait ran out");
+        return fail(ctx, SMOQ_ERR_BADINPUT, "device-side input check failed");
+    }
+    return SMOQ_OK;
+}
+
+static int tile_bits(smoq_ctx* ctx, int dtype) {
+    return dtype == SMOQ_C64 ? ctx->tile_bits_c64 : ctx->tile_bits_c128;
+}
+static int low_bits(smoq_ctx* ctx, int dtype) {
+    return dtype == SMOQ_C64 ? ctx->low_bits_c64 : ctx->low_bits_c128;
+}
+
+// ------------------------------------------------------------ pass runner
+namespace {
+struct DevProgram {
+    std::vector<Pass> passes;
+    std::vector<size_t> offs;  // first op of each pass in d_ops
+    DevOp* d_ops = nullptr;
+    size_t nops = 0;
+    int epi_pass = -1;
+    ~DevProgram() {
+        if (d_ops) cudaFree(d_ops);
+    }
+};
+}  // namespace
+
+static smoq_status upload_program(smoq_ctx* ctx, DevProgram& P) {
+    std::vector<DevOp> all;
+    P.offs.clear();
+    for (size_t i = 0; i < P.passes.size(); ++i) {
+        P.offs.push_back(all.size());
+        all.insert(all.end(), P.passes[i].ops.begin(), P.passes[i].ops.end());
+        if (P.passes[i].epilogue) P.epi_pass = (int)i;
+    }
+    P.nops = all.size();
+    if (all.empty()) return SMOQ_OK;
+    CK(ctx, cudaMalloc(&P.d_ops, all.size() * sizeof(DevOp)));
+    CK(ctx, cudaMemcpy(P.d_ops, all.data(), all.size() * sizeof(DevOp), cudaMemcpyHostToDevice));
+    return SMOQ_OK;
+}
+
+struct EventPair {
+    cudaEvent_t a, b;
+    double bytes;
+};
+
+static smoq_status run_program(smoq_ctx* ctx, smoq_state* st, const DevProgram& P, const Epilogue* ep,
+                               std::vector<EventPair>* timing) {
+    for (size_t i = 0; i < P.passes.size(); ++i) {
+        const Pass& p = P.passes[i];
+        if (p.ops.empty()) continue;
+        EventPair ev{};
+        if (timing) {
+            cudaEventCreate(&ev.a);
+            cudaEventCreate(&ev.b);
+            cudaEventRecord(ev.a, ctx->stream);
+        }
+        cudaError_t e = launch_tile_pass(ctx, st, p, P.d_ops + P.offs[i], p.epilogue ? ep : nullptr);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "tile pass launch");
+        ctx->tile_passes++;
+        if (timing) {
+            cudaEventRecord(ev.b, ctx->stream);
+            ev.bytes = 2.0 * (double)st->bytes();
+            timing->push_back(ev);
+        }
+    }
+    return SMOQ_OK;
+}
+
+static void harvest_timing(smoq_ctx* ctx, std::vector<EventPair>& timing) {
+    for (auto& ev : timing) {
+        float ms = 0;
+        cudaEventSynchronize(ev.b);
+        cudaEventElapsedTime(&ms, ev.a, ev.b);
+        ctx->tile_ms += ms;
+        ctx->tile_bytes += ev.bytes;
+        cudaEventDestroy(ev.a);
+        cudaEventDestroy(ev.b);
+    }
+    timing.clear();
+}
+
+// ================================================================= context
+extern "C" {
+
+const char* smoq_version(void) { return "smoq_cuda 0.1 sm_100a"; }
+
+smoq_status smoq_ctx_create(int device, smoq_ctx** out) {
+    if (!out) return SMOQ_ERR_BADINPUT;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return SMOQ_ERR_NOGPU;
+    if (device < 0 || device >= n) return SMOQ_ERR_BADINPUT;
+    std::unique_ptr<smoq_ctx> ctx(new smoq_ctx());
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) return SMOQ_ERR_CUDA;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return SMOQ_ERR_CUDA;
+    ctx->num_sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return SMOQ_ERR_CUDA;
+    if (cudaMalloc(&ctx->d_err, sizeof(int32_t)) != cudaSuccess) return SMOQ_ERR_OOM;
+    if (cudaMemset(ctx->d_err, 0, sizeof(int32_t)) != cudaSuccess) return SMOQ_ERR_CUDA;
+    if (ensure_scratch(ctx.get(), 1 << 17) != SMOQ_OK) return SMOQ_ERR_OOM;
+    if (ensure_pinned(ctx.get(), 1 << 20) != SMOQ_OK) return SMOQ_ERR_OOM;
+    *out = ctx.release();
+    return SMOQ_OK;
+}
+
+smoq_status smoq_ctx_destroy(smoq_ctx* ctx) {
+    if (!ctx) return SMOQ_ERR_BADINPUT;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->d_scratch) cudaFree(ctx->d_scratch);
+    if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+    if (ctx->d_err) cudaFree(ctx->d_err);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return SMOQ_OK;
+}
+
+const char* smoq_last_error(smoq_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+smoq_status smoq_ctx_synchronize(smoq_ctx* ctx) {
+    if (!ctx) return SMOQ_ERR_BADINPUT;
+    return sync_check(ctx);
+}
+
+void* smoq_ctx_stream(smoq_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long v) {
+    if (!ctx) return SMOQ_ERR_BADINPUT;
+    switch (option) {
+        case SMOQ_OPT_TILE_BITS_C64:
+            if (v < 1 || v > 14) return fail(ctx, SMOQ_ERR_BADINPUT, "tile bits (c64) must be 1..14");
+            ctx->tile_bits_c64 = (int)v;
+            break;
+        case SMOQ_OPT_TILE_BITS_C128:
+            if (v < 1 || v > 13) return fail(ctx, SMOQ_ERR_BADINPUT, "tile bits (c128) must be 1..13");
+            ctx->tile_bits_c128 = (int)v;
+            break;
+        case SMOQ_OPT_LOW_BITS_C64:
+            if (v < 1 || v > 14) return fail(ctx, SMOQ_ERR_BADINPUT, "low bits (c64) must be 1..14");
+            ctx->low_bits_c64 = (int)v;
+            break;
+        case SMOQ_OPT_LOW_BITS_C128:
+            if (v < 0 || v > 13) return fail(ctx, SMOQ_ERR_BADINPUT, "low bits (c128) must be 0..13");
+            ctx->low_bits_c128 = (int)v;
+            break;
+        case SMOQ_OPT_USE_GRAPHS: ctx->use_graphs = v != 0; break;
+        case SMOQ_OPT_KERNEL_TIMING: ctx->kernel_timing = v != 0; break;
+        default: return fail(ctx, SMOQ_ERR_BADINPUT, "unknown option");
+    }
+    return SMOQ_OK;
+}
+
+smoq_status smoq_ctx_counters(smoq_ctx* ctx, long long* launches, long long* tile_passes, double* tile_ms,
+                              double* tile_bytes) {
+    if (!ctx) return SMOQ_ERR_BADINPUT;
+    if (launches) *launches = ctx->launches;
+    if (tile_passes) *tile_passes = ctx->tile_passes;
+    if (tile_ms) *tile_ms = ctx->tile_ms;
+    if (tile_bytes) *tile_bytes = ctx->tile_bytes;
+    return SMOQ_OK;
+}
+
+smoq_status smoq_ctx_reset_counters(smoq_ctx* ctx) {
+    if (!ctx) return SMOQ_ERR_BADINPUT;
+    ctx->launches = 0;
+    ctx->tile_passes = 0;
+    ctx->tile_ms = 0;
+    ctx->tile_bytes = 0;
+    return SMOQ_OK;
+}
+
+// ================================================================== states
+smoq_status smoq_state_create(smoq_ctx* ctx, int N, smoq_dtype dtype, int batch, smoq_state** out) {
+    if (!ctx || !out) return SMOQ_ERR_BADINPUT;
+    *out = nullptr;
+    if (N < 1 || N > 40) return fail(ctx, SMOQ_ERR_BADINPUT, "N must be in 1..40");
+    if (dtype != SMOQ_C64 && dtype != SMOQ_C128) return fail(ctx, SMOQ_ERR_BADINPUT, "bad dtype");
+    if (batch < 1) return fail(ctx, SMOQ_ERR_BADINPUT, "batch must be >= 1");
+    std::unique_ptr<smoq_state> st(new smoq_state());
+    st->ctx = ctx;
+    st->N = N;
+    st->dtype = dtype;
+    st->batch = batch;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaMalloc(&st->ptr, st->bytes());
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "smoq_state_create");
+    e = cudaMemsetAsync(st->ptr, 0, st->bytes(), ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "smoq_state_create memset");
+    *out = st.release();
+    return SMOQ_OK;
+}
+
+smoq_status smoq_state_wrap(smoq_ctx* ctx, void* devptr, int N, smoq_dtype dtype, int batch,
+                            smoq_state** out) {
+    if (!ctx || !out || !devptr) return SMOQ_ERR_BADINPUT;
+    if (((uintptr_t)devptr & 15) != 0) return fail(ctx, SMOQ_ERR_BADINPUT, "device pointer must be 16-byte aligned");
+    if (N < 1 || N > 40 || batch < 1 || (dtype != SMOQ_C64 && dtype != SMOQ_C128))
+        return fail(ctx, SMOQ_ERR_BADINPUT, "bad state shape");
+    smoq_state* st = new smoq_state();
+    st->ctx = ctx;
+    st->N = N;
+    st->dtype = dtype;
+    st->batch = batch;
+    st->ptr = devptr;
+    st->owned = false;
+    *out = st;
+    return SMOQ_OK;
+}
+
+smoq_status smoq_state_destroy(smoq_state* st) {
+    if (!st) return SMOQ_ERR_BADINPUT;
+    if (st->owned && st->ptr) {
+        cudaStreamSynchronize(st->ctx->stream);
+        cudaFree(st->ptr);
+    }
+    delete st;
+    return SMOQ_OK;
+}
+
+void* smoq_state_device_ptr(smoq_state* st) { return st ? st->ptr : nullptr; }
+
+smoq_status smoq_state_upload(smoq_state* st, const void* host, size_t bytes) {
+    if (check_state(st) || !host) return SMOQ_ERR_BADINPUT;
+    if (bytes != st->bytes()) return fail(st->ctx, SMOQ_ERR_BADINPUT, "upload size mismatch");
+    CK(st->ctx, cudaMemcpyAsync(st->ptr, host, bytes, cudaMemcpyHostToDevice, st->ctx->stream));
+    return SMOQ_OK;
+}
+
+smoq_status smoq_state_download(smoq_state* st, void* host, size_t bytes) {
+    if (check_state(st) || !host) return SMOQ_ERR_BADINPUT;
+    if (bytes != st->bytes()) return fail(st->ctx, SMOQ_ERR_BADINPUT, "download size mismatch");
+    CK(st->ctx, cudaMemcpyAsync(host, st->ptr, bytes, cudaMemcpyDeviceToHost, st->ctx->stream));
+    return sync_check(st->ctx);
+}
+
+smoq_status smoq_state_set_basis(smoq_state* st, uint64_t index) {
+    if (check_state(st)) return SMOQ_ERR_BADINPUT;
+    if (st->N < 64 && index >= (1ull << st->N)) return fail(st->ctx, SMOQ_ERR_BADINPUT, "basis index out of range");
+    CK(st->ctx, launch_set_basis(st, index));
+    return SMOQ_OK;
+}
+
+smoq_status smoq_state_copy(smoq_state* dst, smoq_state* src) {
+    if (check_state(dst) || check_state(src)) return SMOQ_ERR_BADINPUT;
+    if (dst->N != src->N || dst->batch != src->batch) return fail(src->ctx, SMOQ_ERR_BADINPUT, "shape mismatch");
+    CK(src->ctx, launch_convert(dst, src));
+    return SMOQ_OK;
+}
+
+// =================================================================== gates
+static smoq_status apply_gate_ir(smoq_state* st, const GateIR& g) {
+    DevOp op;
+    try {
+        build_devop(g, nullptr, op);
+    } catch (const std::exception& ex) {
+        return fail(st->ctx, SMOQ_ERR_BADINPUT, ex.what());
+    }
+    CK(st->ctx, launch_direct_op(st, op));
+    return SMOQ_OK;
+}
+
+static smoq_status gate_common(smoq_state* st, int type, int nq, const int* q, double theta) {
+    if (check_state(st)) return SMOQ_ERR_BADINPUT;
+    for (int t = 0; t < nq; ++t) {
+        if (smoq_status s = check_q(st, q[t], "gate")) return s;
+        for (int u = 0; u < t; ++u)
+            if (q[u] == q[t]) return fail(st->ctx, SMOQ_ERR_BADINPUT, "gate qubits must be distinct");
+    }
+    if (!std::isfinite(theta)) return fail(st->ctx, SMOQ_ERR_BADINPUT, "gate angle is not finite");
+    return apply_gate_ir(st, gate_named(type, q, theta));
+}
+
+#define G1(name, TYPE)                                        \
+    smoq_status name(smoq_state* st, int q) {                 \
+        return gate_common(st, TYPE, 1, &q, 0.0);             \
+    }
+#define G1T(name, TYPE)                                       \
+    smoq_status name(smoq_state* st, int q, double theta) {   \
+        return gate_common(st, TYPE, 1, &q, theta);           \
+    }
+G1T(smoq_apply_rx, SMOQ_G_RX)
+G1T(smoq_apply_ry, SMOQ_G_RY)
+G1T(smoq_apply_rz, SMOQ_G_RZ)
+G1(smoq_apply_h, SMOQ_G_H)
+G1(smoq_apply_x, SMOQ_G_X)
+G1(smoq_apply_y, SMOQ_G_Y)
+G1(smoq_apply_z, SMOQ_G_Z)
+G1(smoq_apply_s, SMOQ_G_S)
+G1(smoq_apply_sdg, SMOQ_G_SDG)
+G1(smoq_apply_t, SMOQ_G_T)
+G1(smoq_apply_tdg, SMOQ_G_TDG)
+
+smoq_status smoq_apply_cnot(smoq_state* st, int c, int t) {
+    int q[2] = {c, t};
+    return gate_common(st, SMOQ_G_CNOT, 2, q, 0.0);
+}
+smoq_status smoq_apply_cz(smoq_state* st, int a, int b) {
+    int q[2] = {a, b};
+    return gate_common(st, SMOQ_G_CZ, 2, q, 0.0);
+}
+smoq_status smoq_apply_cry(smoq_state* st, int c, int t, double theta) {
+    int q[2] = {c, t};
+    return gate_common(st, SMOQ_G_CRY, 2, q, theta);
+}
+smoq_status smoq_apply_rxx(smoq_state* st, int a, int b, double theta) {
+    int q[2] = {a, b};
+    return gate_common(st, SMOQ_G_RXX, 2, q, theta);
+}
+smoq_status smoq_apply_ryy(smoq_state* st, int a, int b, double theta) {
+    int q[2] = {a, b};
+    return gate_common(st, SMOQ_G_RYY, 2, q, theta);
+}
+smoq_status smoq_apply_rzz(smoq_state* st, int a, int b, double theta) {
+    int q[2] = {a, b};
+    return gate_common(st, SMOQ_G_RZZ, 2, q, theta);
+}
+smoq_status smoq_apply_ccz(smoq_state* st, int a, int b, int c) {
+    int q[3] = {a, b, c};
+    return gate_common(st, SMOQ_G_CCZ, 3, q, 0.0);
+}
+smoq_status smoq_apply_toffoli(smoq_state* st, int c1, int c2, int t) {
+    int q[3] = {c1, c2, t};
+    return gate_common(st, SMOQ_G_TOFFOLI, 3, q, 0.0);
+}
+
+// sigma- = |0><1| (moves the |1> amplitude to |0>, zeroes the source);
+// sigma+ = |1><0|; both are monomial 2x2 with a zero row.
+smoq_status smoq_apply_sigma_minus(smoq_state* st, int q) {
+    if (check_state(st)) return SMOQ_ERR_BADINPUT;
+    if (smoq_status s = check_q(st, q, "sigma_minus")) return s;
+    cd m[4] = {0, 1, 0, 0};
+    return apply_gate_ir(st, gate_1q(q, m));
+}
+smoq_status smoq_apply_sigma_plus(smoq_state* st, int q) {
+    if (check_state(st)) return SMOQ_ERR_BADINPUT;
+    if (smoq_status s = check_q(st, q, "sigma_plus")) return s;
+    cd m[4] = {0, 0, 1, 0};
+    return apply_gate_ir(st, gate_1q(q, m));
+}
+
+static void load_colmajor(const double* U, int n, cd* row_major) {
+    for (int r = 0; r < n; ++r)
+        for (int c = 0; c < n; ++c) row_major[r * n + c] = cd(U[2 * (c * n + r)], U[2 * (c * n + r) + 1]);
+}
+
+smoq_status smoq_apply_u1(smoq_state* st, int q, const double* U) {
+    if (check_state(st) || !U) return SMOQ_ERR_BADINPUT;
+    if (smoq_status s = check_q(st, q, "u1")) return s;
+    cd m[4];
+    load_colmajor(U, 2, m);
+    return apply_gate_ir(st, gate_1q(q, m));
+}
+
+static GateIR u2_gate(int q1, int q2, const double* U, int convention) {
+    cd m[16];
+    load_colmajor(U, 4, m);
+    if (convention == 0) {
+        // Trotter.jl:110-112: the smaller qubit is bit 0 of U's index whatever the order
+        return gate_2q(std::min(q1, q2), std::max(q1, q2), m);
+    }
+    // RandomUnitaries.jl:327-333: U's bit 0 is q1 (SWAP-conjugated when q1 > q2)
+    return gate_2q(q1, q2, m);
+}
+
+smoq_status smoq_apply_u2(smoq_state* st, int q1, int q2, const double* U, int convention) {
+    if (check_state(st) || !U) return SMOQ_ERR_BADINPUT;
+    if (smoq_status s = check_q(st, q1, "u2")) return s;
+    if (smoq_status s = check_q(st, q2, "u2")) return s;
+    if (q1 == q2) return fail(st->ctx, SMOQ_ERR_BADINPUT, "u2 qubits must differ");
+    if (convention != 0 && convention != 1) return fail(st->ctx, SMOQ_ERR_BADINPUT, "bad u2 convention");
+    return apply_gate_ir(st, u2_gate(q1, q2, U, convention));
+}
+
+// ================================================================ sequences
+static smoq_status ops_to_ir(smoq_state* st, int N, const smoq_op* ops, int n, const double* theta,
+                             std::vector<GateIR>& out) {
+    smoq_ctx* ctx = st ? st->ctx : nullptr;
+    out.clear();
+    out.reserve(n);
+    for (int i = 0; i < n; ++i) {
+        const smoq_op& o = ops[i];
+        int nq = 1;
+        switch (o.type) {
+            case SMOQ_G_CZ: case SMOQ_G_CNOT: case SMOQ_G_RXX: case SMOQ_G_RYY: case SMOQ_G_RZZ:
+            case SMOQ_G_CRY: case SMOQ_G_U2: nq = 2; break;
+            case SMOQ_G_CCZ: case SMOQ_G_TOFFOLI: nq = 3; break;
+            default: nq = 1;
+        }
+        if (o.type < 0 || o.type > SMOQ_G_U2) return fail(ctx, SMOQ_ERR_BADINPUT, "unknown op type");
+        for (int t = 0; t < nq; ++t) {
+            if (o.q[t] < 0 || o.q[t] >= N) return fail(ctx, SMOQ_ERR_BADINPUT, "op qubit out of range");
+            for (int u = 0; u < t; ++u)
+                if (o.q[u] == o.q[t]) return fail(ctx, SMOQ_ERR_BADINPUT, "op qubits must be distinct");
+        }
+        double a = o.angle;
+        if (o.param >= 0) {
+            if (!theta) return fail(ctx, SMOQ_ERR_BADINPUT, "op needs theta but theta is NULL");
+            a = theta[o.param];
+        }
+        if (!std::isfinite(a)) return fail(ctx, SMOQ_ERR_BADINPUT, "op angle is not finite");
+        GateIR g;
+        if (o.type == SMOQ_G_U1) {
+            cd m[4];
+            load_colmajor(o.U, 2, m);
+            g = gate_1q(o.q[0], m);
+        } else if (o.type == SMOQ_G_U2) {
+            g = u2_gate(o.q[0], o.q[1], o.U, 0);
+        } else {
+            g = gate_named(o.type, o.q, a);
+        }
+        g.tag = o.param;
+        out.push_back(g);
+    }
+    return SMOQ_OK;
+}
+
+smoq_status smoq_apply_sequence(smoq_state* st, const smoq_op* ops, int n, const double* theta) {
+    if (check_state(st) || (!ops && n > 0) || n < 0) return SMOQ_ERR_BADINPUT;
+    if (n == 0) return SMOQ_OK;
+    smoq_ctx* ctx = st->ctx;
+    std::vector<GateIR> ir;
+    if (smoq_status s = ops_to_ir(st, st->N, ops, n, theta, ir)) return s;
+    DevProgram P;
+    try {
+        P.passes = plan_passes(ir, st->N, tile_bits(ctx, st->dtype), low_bits(ctx, st->dtype));
+    } catch (const std::exception& ex) {
+        return fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
+    }
+    CK(ctx, cudaStreamSynchronize(ctx->stream));  // P.d_ops is freed when P goes out of scope
+    if (smoq_status s = upload_program(ctx, P)) return s;
+    std::vector<EventPair> timing;
+    smoq_status s = run_program(ctx, st, P, nullptr, ctx->kernel_timing ? &timing : nullptr);
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    harvest_timing(ctx, timing);
+    if (s) return s;
+    return sync_check(ctx);
+}
+
+smoq_status smoq_apply_sequence_unfused(smoq_state* st, const smoq_op* ops, int n, const double* theta) {
+    if (check_state(st) || (!ops && n > 0) || n < 0) return SMOQ_ERR_BADINPUT;
+    std::vector<GateIR> ir;
+    if (smoq_status s = ops_to_ir(st, st->N, ops, n, theta, ir)) return s;
+    for (const GateIR& g : ir)
+        if (smoq_status s = apply_gate_ir(st, g)) return s;
+    return SMOQ_OK;
+}
+
+// ============================================================= observables
+static smoq_status fetch(smoq_ctx* ctx, const double* d, size_t n, double* host) {
+    if (smoq_status s = ensure_pinned(ctx, n * sizeof(double))) return s;
+    CK(ctx, cudaMemcpyAsync(ctx->h_pinned, d, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (smoq_status s = sync_check(ctx)) return s;
+    std::memcpy(host, ctx->h_pinned, n * sizeof(double));
+    return SMOQ_OK;
+}
+
+// out region for reductions lives after the partials in the scratch buffer
+static smoq_status diag_reduce_host(smoq_state* st, const uint64_t* zmasks, int nobs, double* out) {
+    smoq_ctx* ctx = st->ctx;
+    const int per = 32;
+    std::vector<double> all((size_t)st->batch * nobs);
+    for (int o0 = 0; o0 < nobs; o0 += per) {
+        const int k = std::min(per, nobs - o0);
+        const size_t part = diag_reduce_scratch_doubles(st, k);
+        const size_t outn = (size_t)st->batch * k;
+        if (smoq_status s = ensure_scratch(ctx, part + outn)) return s;
+        double* d_out = ctx->d_scratch + part;
+        CK(ctx, launch_diag_reduce(ctx, st, zmasks + o0, k, d_out));
+        std::vector<double> tmp(outn);
+        if (smoq_status s = fetch(ctx, d_out, outn, tmp.data())) return s;
+        for (int b = 0; b < st->batch; ++b)
+            for (int j = 0; j < k; ++j) all[(size_t)b * nobs + o0 + j] = tmp[(size_t)b * k + j];
+    }
+    std::memcpy(out, all.data(), all.size() * sizeof(double));
+    return SMOQ_OK;
+}
+
+static smoq_status pauli_reduce_host(smoq_state* st, uint64_t xmask, uint64_t zmask, int ny, double* out) {
+    smoq_ctx* ctx = st->ctx;
+    if (xmask == 0) return diag_reduce_host(st, &zmask, 1, out);
+    const size_t part = diag_reduce_scratch_doubles(st, 1);
+    const size_t outn = (size_t)st->batch;
+    if (smoq_status s = ensure_scratch(ctx, part + outn)) return s;
+    double* d_out = ctx->d_scratch + part;
+    CK(ctx, launch_pauli_reduce(ctx, st, xmask, zmask, ny, d_out));
+    return fetch(ctx, d_out, outn, out);
+}
+
+smoq_status smoq_expect_z(smoq_state* st, int q, double* out) {
+    if (check_state(st) || !out) return SMOQ_ERR_BADINPUT;
+    if (smoq_status s = check_q(st, q, "expect_z")) return s;
+    uint64_t m = 1ull << q;
+    return diag_reduce_host(st, &m, 1, out);
+}
+smoq_status smoq_expect_x(smoq_state* st, int q, double* out) {
+    if (check_state(st) || !out) return SMOQ_ERR_BADINPUT;
+    if (smoq_status s = check_q(st, q, "expect_x")) return s;
+    return pauli_reduce_host(st, 1ull << q, 0, 0, out);
+}
+smoq_status smoq_expect_y(smoq_state* st, int q, double* out) {
+    if (check_state(st) || !out) return SMOQ_ERR_BADINPUT;
+    if (smoq_status s = check_q(st, q, "expect_y")) return s;
+    return pauli_reduce_host(st, 1ull << q, 1ull << q, 1, out);
+}
+static smoq_status corr(smoq_state* st, int a, int b, double* out, char p) {
+    if (check_state(st) || !out) return SMOQ_ERR_BADINPUT;
+    if (smoq_status s = check_q(st, a, "expect_corr")) return s;
+    if (smoq_status s = check_q(st, b, "expect_corr")) return s;
+    if (a == b) return fail(st->ctx, SMOQ_ERR_BADINPUT, "correlator qubits must differ");
+    const uint64_t m = (1ull << a) | (1ull << b);
+    if (p == 'z') return diag_reduce_host(st, &m, 1, out);
+    if (p == 'x') return pauli_reduce_host(st, m, 0, 0, out);
+    return pauli_reduce_host(st, m, m, 2, out);
+}
+smoq_status smoq_expect_xx(smoq_state* st, int a, int b, double* out) { return corr(st, a, b, out, 'x'); }
+smoq_status smoq_expect_yy(smoq_state* st, int a, int b, double* out) { return corr(st, a, b, out, 'y'); }
+smoq_status smoq_expect_zz(smoq_state* st, int a, int b, double* out) { return corr(st, a, b, out, 'z'); }
+
+smoq_status smoq_expect_pauli_string(smoq_state* st, int n, const char* ops, const int* qubits, double* out) {
+    if (check_state(st) || !out || n < 0 || (n > 0 && (!ops || !qubits))) return SMOQ_ERR_BADINPUT;
+    uint64_t x = 0, z = 0, seen = 0;
+    int ny = 0;
+    for (int t = 0; t < n; ++t) {
+        if (smoq_status s = check_q(st, qubits[t], "pauli_string")) return s;
+        const uint64_t b = 1ull << qubits[t];
+        if (seen & b) return fail(st->ctx, SMOQ_ERR_BADINPUT, "qubits must be unique");
+        seen |= b;
+        switch (ops[t]) {
+            case 'X': case 'x': x |= b; break;
+            case 'Y': case 'y': x |= b; z |= b; ny++; break;
+            case 'Z': case 'z': z |= b; break;
+            default: return fail(st->ctx, SMOQ_ERR_BADINPUT, "pauli letters must be X, Y or Z");
+        }
+    }
+    return pauli_reduce_host(st, x, z, ny, out);
+}
+
+smoq_status smoq_expect_zstrings(smoq_state* st, const uint64_t* zmasks, int nobs, double* out) {
+    if (check_state(st) || !out || !zmasks || nobs < 1) return SMOQ_ERR_BADINPUT;
+    const uint64_t lim = st->N >= 64 ? ~0ull : ((1ull << st->N) - 1);
+    for (int o = 0; o < nobs; ++o)
+        if (zmasks[o] & ~lim) return fail(st->ctx, SMOQ_ERR_BADINPUT, "zmask has bits beyond N");
+    return diag_reduce_host(st, zmasks, nobs, out);
+}
+
+smoq_status smoq_population_excited(smoq_state* st, int q, double* out) {
+    if (check_state(st) || !out) return SMOQ_ERR_BADINPUT;
+    if (smoq_status s = check_q(st, q, "population_excited")) return s;
+    uint64_t m[2] = {0, 1ull << q};
+    std::vector<double> v((size_t)st->batch * 2);
+    if (smoq_status s = diag_reduce_host(st, m, 2, v.data())) return s;
+    for (int b = 0; b < st->batch; ++b) out[b] = 0.5 * (v[2 * b] - v[2 * b + 1]);
+    return SMOQ_OK;
+}
+
+smoq_status smoq_norm2(smoq_state* st, double* out) {
+    if (check_state(st) || !out) return SMOQ_ERR_BADINPUT;
+    uint64_t m = 0;
+    return diag_reduce_host(st, &m, 1, out);
+}
+
+smoq_status smoq_normalize(smoq_state* st) {
+    if (check_state(st)) return SMOQ_ERR_BADINPUT;
+    smoq_ctx* ctx = st->ctx;
+    std::vector<double> n2(st->batch);
+    if (smoq_status s = smoq_norm2(st, n2.data())) return s;
+    for (int b = 0; b < st->batch; ++b) {
+        if (!(n2[b] > 0)) return fail(ctx, SMOQ_ERR_BADINPUT, "Cannot normalize zero vector");
+        n2[b] = 1.0 / std::sqrt(n2[b]);
+    }
+    double* d = nullptr;
+    CK(ctx, cudaMallocAsync((void**)&d, n2.size() * sizeof(double), ctx->stream));
+    CK(ctx, cudaMemcpyAsync(d, n2.data(), n2.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx, launch_scale(st, d, 1.0));
+    CK(ctx, cudaFreeAsync(d, ctx->stream));
+    return sync_check(ctx);
+}
+
+}  // extern "C"
+
+// ================================================================== plans
+struct smoq_plan {
+    smoq_ctx* ctx = nullptr;
+    int N = 0;
+    int dtype = SMOQ_C64;
+    int order = 1;
+    std::vector<GateIR> step;  // gates of one step (order 2: list + reversed list)
+    struct Block {
+        DevProgram prog;
+        cudaGraphExec_t gexec = nullptr;
+        void* gptr = nullptr;
+        int gbatch = 0;
+        long long kernels = 0;
+        ~Block() {
+            if (gexec) cudaGraphExecDestroy(gexec);
+        }
+    };
+    std::map<int, std::unique_ptr<Block>> blocks;  // keyed by steps per block
+};
+
+static smoq_status get_block(smoq_plan* P, int nsteps, smoq_plan::Block** out) {
+    auto it = P->blocks.find(nsteps);
+    if (it != P->blocks.end()) {
+        *out = it->second.get();
+        return SMOQ_OK;
+    }
+    std::unique_ptr<smoq_plan::Block> B(new smoq_plan::Block());
+    std::vector<GateIR> all;
+    all.reserve(P->step.size() * nsteps);
+    for (int s = 0; s < nsteps; ++s) all.insert(all.end(), P->step.begin(), P->step.end());
+    try {
+        B->prog.passes = plan_passes(all, P->N, tile_bits(P->ctx, P->dtype), low_bits(P->ctx, P->dtype));
+    } catch (const std::exception& ex) {
+        return fail(P->ctx, SMOQ_ERR_BADINPUT, ex.what());
+    }
+    if (smoq_status s = upload_program(P->ctx, B->prog)) return s;
+    for (auto& p : B->prog.passes)
+        if (!p.ops.empty()) B->kernels++;
+    *out = B.get();
+    P->blocks[nsteps] = std::move(B);
+    return SMOQ_OK;
+}
+
+static smoq_status run_block(smoq_plan* P, smoq_state* st, smoq_plan::Block* B, std::vector<EventPair>* timing) {
+    smoq_ctx* ctx = P->ctx;
+    if (ctx->use_graphs && !timing) {
+        if (!B->gexec || B->gptr != st->ptr || B->gbatch != st->batch) {
+            if (B->gexec) cudaGraphExecDestroy(B->gexec);
+            B->gexec = nullptr;
+            cudaGraph_t g;
+            CK(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            smoq_status s = run_program(ctx, st, B->prog, nullptr, nullptr);
+            cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+            if (s) return s;
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "graph capture");
+            e = cudaGraphInstantiate(&B->gexec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "graph instantiate");
+            B->gptr = st->ptr;
+            B->gbatch = st->batch;
+            // capture counted launches that did not run
+            ctx->launches -= B->kernels;
+            ctx->tile_passes -= B->kernels;
+        }
+        CK(ctx, cudaGraphLaunch(B->gexec, ctx->stream));
+        ctx->launches += B->kernels;
+        ctx->tile_passes += B->kernels;
+        return SMOQ_OK;
+    }
+    return run_program(ctx, st, B->prog, nullptr, timing);
+}
+
+extern "C" {
+
+smoq_status smoq_precompute_trotter_gates(const double* bonds, int nb, const double* fields, int nf, double dt,
+                                          smoq_trotter_gate* out, int* n_out) {
+    // exp(-i dt (Jx XX + Jy YY + Jz ZZ)) is block diagonal on {00,11} and
+    // {01,10} because XX, YY, ZZ commute: even block e^{-i Jz dt} exp(-i (Jx-Jy) dt sx),
+    // odd block e^{+i Jz dt} exp(-i (Jx+Jy) dt sx); fields: exp(-i dt h.sigma)
+    // = cos(|h| dt) I - i sin(|h| dt) h.sigma/|h|.
+    if ((nb > 0 && !bonds) || (nf > 0 && !fields) || !out || !n_out) return SMOQ_ERR_BADINPUT;
+    int n = 0;
+    auto put = [](double* U, int dim, int r, int c, cd v) {
+        U[2 * (c * dim + r)] = v.real();
+        U[2 * (c * dim + r) + 1] = v.imag();
+    };
+    for (int t = 0; t < nb; ++t) {
+        const double* b = bonds + 5 * t;
+        smoq_trotter_gate& g = out[n++];
+        std::memset(&g, 0, sizeof(g));
+        g.nq = 2;
+        g.q[0] = (int)b[0];
+        g.q[1] = (int)b[1];
+        const double a = (b[2] - b[3]) * dt, bb = (b[2] + b[3]) * dt;
+        const cd pe = std::exp(cd(0, -b[4] * dt)), po = std::exp(cd(0, b[4] * dt));
+        put(g.U, 4, 0, 0, pe * std::cos(a));
+        put(g.U, 4, 3, 3, pe * std::cos(a));
+        put(g.U, 4, 0, 3, pe * cd(0, -std::sin(a)));
+        put(g.U, 4, 3, 0, pe * cd(0, -std::sin(a)));
+        put(g.U, 4, 1, 1, po * std::cos(bb));
+        put(g.U, 4, 2, 2, po * std::cos(bb));
+        put(g.U, 4, 1, 2, po * cd(0, -std::sin(bb)));
+        put(g.U, 4, 2, 1, po * cd(0, -std::sin(bb)));
+    }
+    for (int t = 0; t < nf; ++t) {
+        const double* f = fields + 4 * t;
+        const double hx = f[1], hy = f[2], hz = f[3];
+        if (!(std::fabs(hx) > 1e-14 || std::fabs(hy) > 1e-14 || std::fabs(hz) > 1e-14)) continue;
+        const double h = std::sqrt(hx * hx + hy * hy + hz * hz), c = std::cos(h * dt), s = std::sin(h * dt) / h;
+        smoq_trotter_gate& g = out[n++];
+        std::memset(&g, 0, sizeof(g));
+        g.nq = 1;
+        g.q[0] = (int)f[0];
+        put(g.U, 2, 0, 0, cd(c, -s * hz));
+        put(g.U, 2, 1, 1, cd(c, s * hz));
+        put(g.U, 2, 0, 1, cd(0, -s) * cd(hx, -hy));
+        put(g.U, 2, 1, 0, cd(0, -s) * cd(hx, hy));
+    }
+    *n_out = n;
+    return SMOQ_OK;
+}
+
+smoq_status smoq_trotter_plan_create(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_trotter_gate* gates, int n,
+                                     int order, smoq_plan** out) {
+    if (!ctx || !out || (n > 0 && !gates) || n < 0) return SMOQ_ERR_BADINPUT;
+    if (order != 1 && order != 2) return fail(ctx, SMOQ_ERR_BADINPUT, "order must be 1 or 2");
+    if (N < 1 || N > 40) return fail(ctx, SMOQ_ERR_BADINPUT, "N must be in 1..40");
+    std::unique_ptr<smoq_plan> P(new smoq_plan());
+    P->ctx = ctx;
+    P->N = N;
+    P->dtype = dtype;
+    P->order = order;
+    std::vector<GateIR> one;
+    for (int i = 0; i < n; ++i) {
+        const smoq_trotter_gate& g = gates[i];
+        if (g.nq == 1) {
+            if (g.q[0] < 0 || g.q[0] >= N) return fail(ctx, SMOQ_ERR_BADINPUT, "trotter gate qubit out of range");
+            cd m[4];
+            load_colmajor(g.U, 2, m);
+            one.push_back(gate_1q(g.q[0], m));
+        } else if (g.nq == 2) {
+            if (g.q[0] < 0 || g.q[0] >= N || g.q[1] < 0 || g.q[1] >= N || g.q[0] == g.q[1])
+                return fail(ctx, SMOQ_ERR_BADINPUT, "trotter gate qubits out of range");
+            one.push_back(u2_gate(g.q[0], g.q[1], g.U, 0));
+        } else {
+            return fail(ctx, SMOQ_ERR_BADINPUT, "Gates with more than 2 qubits not supported");  // Trotter.jl:157
+        }
+    }
+    P->step = one;
+    if (order == 2) P->step.insert(P->step.end(), one.rbegin(), one.rend());
+    *out = P.release();
+    return SMOQ_OK;
+}
+
+smoq_status smoq_plan_destroy(smoq_plan* plan) {
+    if (!plan) return SMOQ_ERR_BADINPUT;
+    cudaStreamSynchronize(plan->ctx->stream);
+    delete plan;
+    return SMOQ_OK;
+}
+
+static const int kMaxBlockSteps = 10;
+
+static smoq_status trotter_steps(smoq_plan* P, smoq_state* st, int n_steps, std::vector<EventPair>* timing) {
+    while (n_steps > 0) {
+        const int k = std::min(n_steps, kMaxBlockSteps);
+        smoq_plan::Block* B = nullptr;
+        if (smoq_status s = get_block(P, k, &B)) return s;
+        if (smoq_status s = run_block(P, st, B, timing)) return s;
+        n_steps -= k;
+    }
+    return SMOQ_OK;
+}
+
+static smoq_status check_plan_state(smoq_plan* P, smoq_state* st) {
+    if (!P || check_state(st)) return SMOQ_ERR_BADINPUT;
+    if (st->N != P->N || st->dtype != P->dtype) return fail(P->ctx, SMOQ_ERR_BADINPUT, "plan/state shape mismatch");
+    if (st->ctx != P->ctx) return fail(P->ctx, SMOQ_ERR_BADINPUT, "plan and state belong to different contexts");
+    return SMOQ_OK;
+}
+
+smoq_status smoq_trotter_step(smoq_plan* P, smoq_state* st, int n_steps) {
+    if (smoq_status s = check_plan_state(P, st)) return s;
+    if (n_steps < 0) return fail(P->ctx, SMOQ_ERR_BADINPUT, "n_steps < 0");
+    std::vector<EventPair> timing;
+    smoq_status s = trotter_steps(P, st, n_steps, P->ctx->kernel_timing ? &timing : nullptr);
+    if (!timing.empty()) harvest_timing(P->ctx, timing);
+    return s;
+}
+
+smoq_status smoq_trotter_run(smoq_plan* P, smoq_state* st, int steps, int record_every, double* z_out) {
+    if (smoq_status s = check_plan_state(P, st)) return s;
+    smoq_ctx* ctx = P->ctx;
+    if (steps < 0 || record_every < 1 || !z_out) return fail(ctx, SMOQ_ERR_BADINPUT, "bad steps/record_every/z_out");
+    const int N = P->N;
+    const int nrec = steps / record_every + 1;
+    const size_t per_rec = (size_t)st->batch * N;
+    std::vector<uint64_t> zm(N);
+    for (int i = 0; i < N; ++i) zm[i] = 1ull << i;
+    // device record buffer, then the reduction partials
+    const int per = 32;
+    const size_t part = diag_reduce_scratch_doubles(st, std::min(N, per));
+    if (smoq_status s = ensure_scratch(ctx, part + nrec * per_rec + (size_t)st->batch * per)) return s;
+    double* d_rec = ctx->d_scratch + part;
+    double* d_tmp = d_rec + nrec * per_rec;
+    std::vector<EventPair> timing;
+    std::vector<EventPair>* tp = ctx->kernel_timing ? &timing : nullptr;
+    auto record = [&](int r) -> smoq_status {
+        // <Z_i> of every state into d_rec[r][b][i]: 32 observables per reduction
+        if (N <= per) {  // [b][i] layout straight into the record slot
+            cudaError_t e = launch_diag_reduce(ctx, st, zm.data(), N, d_rec + r * per_rec);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "record reduction");
+            return SMOQ_OK;
+        }
+        for (int o0 = 0; o0 < N; o0 += per) {
+            const int k = std::min(per, N - o0);
+            cudaError_t e = launch_diag_reduce(ctx, st, zm.data() + o0, k, d_tmp);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "record reduction");
+            for (int b = 0; b < st->batch; ++b) {
+                e = cudaMemcpyAsync(d_rec + r * per_rec + (size_t)b * N + o0, d_tmp + (size_t)b * k,
+                                    k * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+                if (e != cudaSuccess) return cuda_fail(ctx, e, "record copy");
+            }
+        }
+        return SMOQ_OK;
+    };
+    if (smoq_status s = record(0)) return s;
+    int done = 0;
+    for (int r = 1; r < nrec; ++r) {
+        if (smoq_status s = trotter_steps(P, st, record_every, tp)) return s;
+        done += record_every;
+        if (smoq_status s = record(r)) return s;
+    }
+    if (steps > done)
+        if (smoq_status s = trotter_steps(P, st, steps - done, tp)) return s;
+    if (smoq_status s = fetch(ctx, d_rec, nrec * per_rec, z_out)) return s;
+    harvest_timing(ctx, timing);
+    return SMOQ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,189 @@
+// k_common.cuh -- device helpers: complex arithmetic, bit insertion, PTX
+// wrappers for the Blackwell bulk-copy engine (cp.async.bulk + mbarrier) and
+// bounded waits.  No wait in this library spins without an iteration limit.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "smoq_internal.h"
+
+namespace smoq {
+
+enum : int32_t { DEVERR_TIMEOUT = 1, DEVERR_BADINPUT = 2 };
+
+template <typename R> struct CT;
+template <> struct CT<float> { using T = float2; };
+template <> struct CT<double> { using T = double2; };
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a*b + c
+__device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {
+    return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, c.y)));
+}
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
+    return make_double2(fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y)));
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 czero(float2) { return make_float2(0.f, 0.f); }
+__device__ __forceinline__ double2 czero(double2) { return make_double2(0.0, 0.0); }
+__device__ __forceinline__ double cabs2d(float2 a) { return (double)a.x * a.x + (double)a.y * a.y; }
+__device__ __forceinline__ double cabs2d(double2 a) { return a.x * a.x + a.y * a.y; }
+
+template <typename R> __device__ __forceinline__ typename CT<R>::T coef(const DevOp& op, int i);
+template <> __device__ __forceinline__ float2 coef<float>(const DevOp& op, int i) { return op.cf[i]; }
+template <> __device__ __forceinline__ double2 coef<double>(const DevOp& op, int i) { return op.cd[i]; }
+
+// insert a zero bit at position p
+template <typename I> __device__ __forceinline__ I ins0(I x, int p) {
+    I lo = x & ((I(1) << p) - 1);
+    return ((x >> p) << (p + 1)) | lo;
+}
+
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait on an mbarrier phase: gives up after 2^24 polls (each poll may
+// suspend the thread for a hardware time slice, so the bound is far above any
+// legitimate copy), records DEVERR_TIMEOUT and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int32_t* err) {
+    for (int it = 0; it < (1 << 24); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    if (err) atomicExch(err, DEVERR_TIMEOUT);
+    return false;
+}
+// bulk global -> shared copy, completion counted on the mbarrier (no multicast)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+// bulk shared -> global copy (bulk async-group completion)
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+                 "r"(smem_u32(src)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() {
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// ------------------------------------------------------------ op application
+// Apply one fused op to the amplitude array `psi` indexed by I.  `bits` are
+// the op's qubit positions in that index space.  `nthr`/`tid` stride the
+// groups.  Used on a shared-memory tile (I = uint32_t, local bits) and on a
+// whole state in HBM (I = uint64_t, global bits).
+template <typename R, typename I>
+__device__ __forceinline__ void sweep_op(const DevOp& op, typename CT<R>::T* psi, int nbits,
+                                         const int* bits, I tid, I nthr) {
+    using C = typename CT<R>::T;
+    const int kind = op.kind;
+    if (kind == OPK_DENSE1) {
+        const int a = bits[0];
+        const C m0 = coef<R>(op, 0), m1 = coef<R>(op, 1), m2 = coef<R>(op, 2), m3 = coef<R>(op, 3);
+        const I n = I(1) << (nbits - 1);
+        for (I g = tid; g < n; g += nthr) {
+            I i0 = ins0(g, a), i1 = i0 | (I(1) << a);
+            C x = psi[i0], y = psi[i1];
+            psi[i0] = cfma(m0, x, cmul(m1, y));
+            psi[i1] = cfma(m2, x, cmul(m3, y));
+        }
+    } else if (kind == OPK_DENSE2 || kind == OPK_PARITY2) {
+        const int a = bits[0], b = bits[1];
+        const int lo = a < b ? a : b, hi = a < b ? b : a;
+        const I sa = I(1) << a, sb = I(1) << b;
+        const I n = I(1) << (nbits - 2);
+        if (kind == OPK_DENSE2) {
+            C m[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) m[k] = coef<R>(op, k);
+            for (I g = tid; g < n; g += nthr) {
+                I i0 = ins0(ins0(g, lo), hi);
+                I ix[4] = {i0, i0 | sa, i0 | sb, i0 | sa | sb};
+                C v[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) v[k] = psi[ix[k]];
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    C acc = cmul(m[4 * r], v[0]);
+                    acc = cfma(m[4 * r + 1], v[1], acc);
+                    acc = cfma(m[4 * r + 2], v[2], acc);
+                    acc = cfma(m[4 * r + 3], v[3], acc);
+                    psi[ix[r]] = acc;
+                }
+            }
+        } else {
+            // even block (00,11): e0 e1 / e2 e3 ; odd block (01,10): o0 o1 / o2 o3
+            const C e0 = coef<R>(op, 0), e1 = coef<R>(op, 1), e2 = coef<R>(op, 2), e3 = coef<R>(op, 3);
+            const C o0 = coef<R>(op, 4), o1 = coef<R>(op, 5), o2 = coef<R>(op, 6), o3 = coef<R>(op, 7);
+            for (I g = tid; g < n; g += nthr) {
+                I i0 = ins0(ins0(g, lo), hi);
+                I i1 = i0 | sa, i2 = i0 | sb, i3 = i0 | sa | sb;
+                C v0 = psi[i0], v1 = psi[i1], v2 = psi[i2], v3 = psi[i3];
+                psi[i0] = cfma(e0, v0, cmul(e1, v3));
+                psi[i3] = cfma(e2, v0, cmul(e3, v3));
+                psi[i1] = cfma(o0, v1, cmul(o1, v2));
+                psi[i2] = cfma(o2, v1, cmul(o3, v2));
+            }
+        }
+    } else if (kind == OPK_MONO) {
+        const int nq = op.nq;
+        int sorted[3] = {bits[0], nq > 1 ? bits[1] : 0, nq > 2 ? bits[2] : 0};
+        // insertion sort of the nq positions
+        for (int i = 1; i < nq; ++i)
+            for (int j = i; j > 0 && sorted[j] < sorted[j - 1]; --j) {
+                int t = sorted[j]; sorted[j] = sorted[j - 1]; sorted[j - 1] = t;
+            }
+        const int dim = 1 << nq;
+        const I n = I(1) << (nbits - nq);
+        for (I g = tid; g < n; g += nthr) {
+            I i0 = g;
+            for (int i = 0; i < nq; ++i) i0 = ins0(i0, sorted[i]);
+            I ix[8];
+            C v[8];
+            for (int m = 0; m < dim; ++m) {
+                I x = i0;
+                for (int t = 0; t < nq; ++t) x |= (I)((m >> t) & 1) << bits[t];
+                ix[m] = x;
+                v[m] = psi[x];
+            }
+            for (int r = 0; r < dim; ++r) psi[ix[r]] = cmul(coef<R>(op, r), v[op.perm[r]]);
+        }
+    }
+}
+
+}  // namespace smoq

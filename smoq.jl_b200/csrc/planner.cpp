@@ -1,0 +1,390 @@
+// planner.cpp -- gate IR, gate matrices, and the fused-pass planner.
+//
+// The planner turns an ordered gate list into tile passes.  It generalises
+// the reference's own fusion (fuse_gates, SmoQ.jl_benchmarks/
+// benchmark_random_circuit_sampling/run_benchmark_smoq_Float64.jl:167, which
+// merges runs of single-qubit gates into one 2x2 and flushes at two-qubit
+// gates) from "one qubit" to "one tile of T qubits":
+//   1. greedy pass building: scan the remaining gates in order; a
+//      non-diagonal gate joins the pass if none of its qubits is blocked and
+//      the pass's tile (the low Lmin qubits + the qubits taken so far) can
+//      hold its qubits within T; a diagonal gate joins whenever none of its
+//      qubits is blocked by a skipped NON-diagonal gate (diagonals commute
+//      with each other and need no tile membership: their phase depends only
+//      on the amplitude's global index).  A skipped gate blocks its qubits
+//      (hard for non-diagonal, soft for diagonal) so no later gate that does
+//      not commute with it can overtake it.
+//   2. fusion inside the pass: runs of 1-qubit gates on a qubit collapse to
+//      one 2x2; a 2-qubit gate absorbs the pending 2x2s of its qubits;
+//      consecutive 2-qubit gates on the same pair multiply into one 4x4.
+//   3. classification of every fused matrix (diagonal, monomial, parity
+//      block, dense) so the kernel runs the cheapest sweep for it.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include "smoq_internal.h"
+
+namespace smoq {
+
+static const cd I1(0.0, 1.0);
+
+GateIR gate_1q(int q, const cd m[4]) {
+    GateIR g;
+    g.nq = 1;
+    g.q[0] = q;
+    for (int k = 0; k < 4; ++k) g.m[k] = m[k];
+    g.diag = (m[1] == 0.0 && m[2] == 0.0);
+    return g;
+}
+
+GateIR gate_2q(int q0, int q1, const cd m[16]) {
+    GateIR g;
+    g.nq = 2;
+    g.q[0] = q0;
+    g.q[1] = q1;
+    bool d = true;
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            g.m[r * 4 + c] = m[r * 4 + c];
+            if (r != c && m[r * 4 + c] != 0.0) d = false;
+        }
+    g.diag = d;
+    return g;
+}
+
+static GateIR diag_nq(int nq, const int* q, const cd* d) {
+    GateIR g;
+    g.nq = nq;
+    for (int t = 0; t < nq; ++t) g.q[t] = q[t];
+    const int dim = 1 << nq;
+    for (int k = 0; k < dim * dim; ++k) g.m[k] = 0.0;
+    for (int k = 0; k < dim; ++k) g.m[k * dim + k] = d[k];
+    g.diag = true;
+    return g;
+}
+
+// Gate matrices as defined in utils/cpu/cpuQuantumChannelGates.jl:53-71
+// (header) and in each apply_*_psi! body; two-qubit local index
+// m = bit(q[0]) + 2 bit(q[1]).
+GateIR gate_named(int type, const int* q, double th) {
+    const double c = std::cos(th / 2), s = std::sin(th / 2);
+    switch (type) {
+        case SMOQ_G_RX: { cd m[4] = {c, -I1 * s, -I1 * s, c}; return gate_1q(q[0], m); }
+        case SMOQ_G_RY: { cd m[4] = {c, -s, s, c}; return gate_1q(q[0], m); }
+        case SMOQ_G_RZ: { cd m[4] = {std::exp(-I1 * th / 2.0), 0, 0, std::exp(I1 * th / 2.0)}; return gate_1q(q[0], m); }
+        case SMOQ_G_H: { const double r = 1 / std::sqrt(2.0); cd m[4] = {r, r, r, -r}; return gate_1q(q[0], m); }
+        case SMOQ_G_X: { cd m[4] = {0, 1, 1, 0}; return gate_1q(q[0], m); }
+        case SMOQ_G_Y: { cd m[4] = {0, -I1, I1, 0}; return gate_1q(q[0], m); }
+        case SMOQ_G_Z: { cd m[4] = {1, 0, 0, -1}; return gate_1q(q[0], m); }
+        case SMOQ_G_S: { cd m[4] = {1, 0, 0, I1}; return gate_1q(q[0], m); }
+        case SMOQ_G_SDG: { cd m[4] = {1, 0, 0, -I1}; return gate_1q(q[0], m); }
+        case SMOQ_G_T: { cd m[4] = {1, 0, 0, std::exp(I1 * (M_PI / 4))}; return gate_1q(q[0], m); }
+        case SMOQ_G_TDG: { cd m[4] = {1, 0, 0, std::exp(-I1 * (M_PI / 4))}; return gate_1q(q[0], m); }
+        case SMOQ_G_CZ: { cd d[4] = {1, 1, 1, -1}; return diag_nq(2, q, d); }
+        case SMOQ_G_RZZ: {
+            const cd same = std::exp(-I1 * th / 2.0), diff = std::exp(I1 * th / 2.0);
+            cd d[4] = {same, diff, diff, same};
+            return diag_nq(2, q, d);
+        }
+        case SMOQ_G_CCZ: { cd d[8] = {1, 1, 1, 1, 1, 1, 1, -1}; return diag_nq(3, q, d); }
+        case SMOQ_G_CNOT: {  // q[0] control, q[1] target: swap m=1 <-> m=3
+            cd m[16] = {};
+            m[0 * 4 + 0] = 1; m[2 * 4 + 2] = 1; m[1 * 4 + 3] = 1; m[3 * 4 + 1] = 1;
+            return gate_2q(q[0], q[1], m);
+        }
+        case SMOQ_G_RXX: {  // c I - i s XX, XX: m -> m ^ 3
+            cd m[16] = {};
+            for (int k = 0; k < 4; ++k) { m[k * 4 + k] = c; m[k * 4 + (k ^ 3)] = -I1 * s; }
+            return gate_2q(q[0], q[1], m);
+        }
+        case SMOQ_G_RYY: {  // c I - i s YY, YY: 00<->11 with -1, 01<->10 with +1
+            cd m[16] = {};
+            for (int k = 0; k < 4; ++k) m[k * 4 + k] = c;
+            m[0 * 4 + 3] = I1 * s; m[3 * 4 + 0] = I1 * s;
+            m[1 * 4 + 2] = -I1 * s; m[2 * 4 + 1] = -I1 * s;
+            return gate_2q(q[0], q[1], m);
+        }
+        case SMOQ_G_CRY: {  // q[0] control, q[1] target; Ry on (m=1, m=3)
+            cd m[16] = {};
+            m[0] = 1; m[2 * 4 + 2] = 1;
+            m[1 * 4 + 1] = c; m[1 * 4 + 3] = -s; m[3 * 4 + 1] = s; m[3 * 4 + 3] = c;
+            return gate_2q(q[0], q[1], m);
+        }
+        case SMOQ_G_TOFFOLI: {  // q = (c1, c2, t): swap m=3 <-> m=7
+            GateIR g;
+            g.nq = 3;
+            for (int t = 0; t < 3; ++t) g.q[t] = q[t];
+            for (int k = 0; k < 64; ++k) g.m[k] = 0.0;
+            for (int k = 0; k < 8; ++k) g.m[k * 8 + k] = 1;
+            g.m[3 * 8 + 3] = 0; g.m[7 * 8 + 7] = 0;
+            g.m[3 * 8 + 7] = 1; g.m[7 * 8 + 3] = 1;
+            g.diag = false;
+            return g;
+        }
+        default: throw std::invalid_argument("unknown gate type");
+    }
+}
+
+// ---------------------------------------------------------------- matrices
+static void matmul(int dim, const cd* A, const cd* B, cd* out) {  // out = A * B
+    cd tmp[64];
+    for (int r = 0; r < dim; ++r)
+        for (int c = 0; c < dim; ++c) {
+            cd s = 0;
+            for (int k = 0; k < dim; ++k) s += A[r * dim + k] * B[k * dim + c];
+            tmp[r * dim + c] = s;
+        }
+    std::memcpy(out, tmp, sizeof(cd) * dim * dim);
+}
+// kron for the 2-qubit local basis m = bit(q0) + 2 bit(q1): (P1 (x) P0)
+static void kron2(const cd* P0, const cd* P1, cd* out) {
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c)
+            out[r * 4 + c] = P1[(r >> 1) * 2 + (c >> 1)] * P0[(r & 1) * 2 + (c & 1)];
+}
+// the same 4x4 with its two qubits' roles exchanged
+static void swap_roles(const cd* M, cd* out) {
+    auto sw = [](int m) { return ((m & 1) << 1) | (m >> 1); };
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) out[sw(r) * 4 + sw(c)] = M[r * 4 + c];
+}
+
+static void fill_coeffs(DevOp& op, const cd* v, int n) {
+    for (int k = 0; k < 16; ++k) {
+        cd x = k < n ? v[k] : cd(0.0);
+        op.cd[k] = make_double2(x.real(), x.imag());
+        op.cf[k] = make_float2((float)x.real(), (float)x.imag());
+    }
+}
+
+// classify and encode a k-qubit matrix (k = 1..3) as a DevOp
+static void encode_matrix(int nq, const cd* M, DevOp& op) {
+    const int dim = 1 << nq;
+    bool diag = true, mono = true;
+    int perm[8];
+    for (int r = 0; r < dim; ++r) {
+        int nz = 0;
+        perm[r] = r;
+        for (int c = 0; c < dim; ++c)
+            if (M[r * dim + c] != 0.0) {
+                ++nz;
+                perm[r] = c;
+                if (r != c) diag = false;
+            }
+        if (nz > 1) { mono = false; diag = false; }
+        if (nz == 0) diag = false, perm[r] = r;  // a zero row: monomial with phase 0
+    }
+    op.nq = nq;
+    if (diag) {
+        cd d[8];
+        for (int k = 0; k < dim; ++k) d[k] = M[k * dim + k];
+        op.kind = OPK_DIAG;
+        fill_coeffs(op, d, dim);
+        return;
+    }
+    if (mono) {
+        cd ph[8];
+        for (int r = 0; r < dim; ++r) {
+            ph[r] = M[r * dim + perm[r]];
+            op.perm[r] = perm[r];
+        }
+        op.kind = OPK_MONO;
+        fill_coeffs(op, ph, dim);
+        return;
+    }
+    if (nq == 1) {
+        op.kind = OPK_DENSE1;
+        fill_coeffs(op, M, 4);
+        return;
+    }
+    if (nq == 2) {
+        const bool parity = M[0 * 4 + 1] == 0.0 && M[0 * 4 + 2] == 0.0 && M[3 * 4 + 1] == 0.0 &&
+                            M[3 * 4 + 2] == 0.0 && M[1 * 4 + 0] == 0.0 && M[1 * 4 + 3] == 0.0 &&
+                            M[2 * 4 + 0] == 0.0 && M[2 * 4 + 3] == 0.0;
+        if (parity) {
+            cd v[8] = {M[0], M[3], M[12], M[15], M[5], M[6], M[9], M[10]};
+            op.kind = OPK_PARITY2;
+            fill_coeffs(op, v, 8);
+            return;
+        }
+        op.kind = OPK_DENSE2;
+        fill_coeffs(op, M, 16);
+        return;
+    }
+    throw std::invalid_argument("3-qubit gates must be diagonal or monomial");
+}
+
+static int local_bit(const TileGeom* g, int q) {
+    if (!g) return q;
+    if (q < g->L) return q;
+    for (int m = 0; m < g->H; ++m)
+        if (g->hb[m] == q) return g->L + m;
+    return -1;
+}
+
+void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op) {
+    std::memset(&op, 0, sizeof(op));
+    for (int t = 0; t < 3; ++t) {
+        op.lb[t] = -1;
+        op.gb[t] = 0;
+    }
+    for (int r = 0; r < 8; ++r) op.perm[r] = r;
+    if (gt.special) {
+        op.kind = gt.special;
+        op.aux = gt.aux;
+        op.aux2 = gt.aux2;
+        op.nq = 0;
+        return;
+    }
+    for (int t = 0; t < gt.nq; ++t) {
+        op.gb[t] = gt.q[t];
+        op.lb[t] = local_bit(g, gt.q[t]);
+    }
+    encode_matrix(gt.nq, gt.m, op);
+    op.nq = gt.nq;
+}
+
+// -------------------------------------------------------------------- plan
+namespace {
+struct Fuser {
+    const TileGeom* g;
+    std::vector<DevOp> ops;
+    bool have_pending[64] = {};
+    cd pending[64][4];
+    int last2q = -1;  // index in ops of the last op if it is a mergeable 2-qubit op
+    cd last_m[16];
+    int last_q[2] = {-1, -1};
+
+    explicit Fuser(const TileGeom* geom) : g(geom) {}
+
+    void emit(const GateIR& gt) {
+        DevOp op;
+        build_devop(gt, g, op);
+        ops.push_back(op);
+        last2q = -1;
+    }
+    void flush(int q) {
+        if (!have_pending[q]) return;
+        GateIR p = gate_1q(q, pending[q]);
+        have_pending[q] = false;
+        emit(p);
+    }
+    void flush_all() {
+        for (int q = 0; q < 64; ++q) flush(q);
+    }
+    void add(const GateIR& gt) {
+        if (gt.special) {
+            if (gt.special == OPK_REALTAB) flush_all();  // diagonal over every qubit
+            emit(gt);
+            return;
+        }
+        bool all_tile = true;
+        for (int t = 0; t < gt.nq; ++t)
+            if (local_bit(g, gt.q[t]) < 0) all_tile = false;
+        if (gt.nq == 1 && all_tile) {
+            const int q = gt.q[0];
+            if (have_pending[q]) {
+                cd out[4];
+                matmul(2, gt.m, pending[q], out);
+                std::memcpy(pending[q], out, sizeof(out));
+            } else {
+                std::memcpy(pending[q], gt.m, sizeof(cd) * 4);
+                have_pending[q] = true;
+            }
+            return;
+        }
+        if (gt.nq == 2 && all_tile) {
+            const int a = gt.q[0], b = gt.q[1];
+            cd M[16];
+            std::memcpy(M, gt.m, sizeof(M));
+            if (have_pending[a] || have_pending[b]) {
+                static const cd Id[4] = {1, 0, 0, 1};
+                cd K[16];
+                kron2(have_pending[a] ? pending[a] : Id, have_pending[b] ? pending[b] : Id, K);
+                matmul(4, M, K, M);
+                have_pending[a] = have_pending[b] = false;
+            }
+            if (last2q >= 0 && ((last_q[0] == a && last_q[1] == b) || (last_q[0] == b && last_q[1] == a))) {
+                cd Mal[16];
+                if (last_q[0] == a) std::memcpy(Mal, M, sizeof(Mal));
+                else swap_roles(M, Mal);
+                matmul(4, Mal, last_m, last_m);
+                GateIR merged = gate_2q(last_q[0], last_q[1], last_m);
+                build_devop(merged, g, ops[last2q]);
+                return;
+            }
+            GateIR fused = gate_2q(a, b, M);
+            emit(fused);
+            last2q = (int)ops.size() - 1;
+            std::memcpy(last_m, M, sizeof(M));
+            last_q[0] = a;
+            last_q[1] = b;
+            return;
+        }
+        // diagonal gates touching non-tile qubits, and 3-qubit gates
+        for (int t = 0; t < gt.nq; ++t)
+            if (local_bit(g, gt.q[t]) >= 0) flush(gt.q[t]);
+        if (!all_tile && !gt.diag) throw std::logic_error("planner placed a non-diagonal gate off-tile");
+        emit(gt);
+    }
+};
+}  // namespace
+
+std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, int Lmin,
+                              int epilogue_after_special) {
+    if (T > N) T = N;
+    if (Lmin > T) Lmin = T;
+    std::vector<int> remaining(gates.size());
+    for (size_t i = 0; i < gates.size(); ++i) remaining[i] = (int)i;
+    const uint64_t allq = (N >= 64) ? ~0ull : ((1ull << N) - 1);
+    std::vector<Pass> passes;
+    while (!remaining.empty()) {
+        uint64_t tileset = (Lmin > 0) ? ((1ull << Lmin) - 1) : 0;
+        uint64_t hard = 0, soft = 0;
+        std::vector<int> taken, rest;
+        for (int idx : remaining) {
+            const GateIR& gt = gates[idx];
+            uint64_t qm = 0;
+            if (gt.special == OPK_REALTAB) qm = allq;
+            for (int t = 0; t < gt.nq; ++t) qm |= 1ull << gt.q[t];
+            if (gt.diag || gt.special) {
+                if ((qm & hard) == 0) taken.push_back(idx);
+                else { soft |= qm; rest.push_back(idx); }
+            } else {
+                const uint64_t ns = tileset | qm;
+                if ((qm & (hard | soft)) == 0 && __builtin_popcountll(ns) <= T) {
+                    tileset = ns;
+                    taken.push_back(idx);
+                } else {
+                    hard |= qm;
+                    rest.push_back(idx);
+                }
+            }
+        }
+        // widen the tile with the lowest free qubits: longer contiguous segments
+        for (int b = 0; b < N && __builtin_popcountll(tileset) < T; ++b) tileset |= 1ull << b;
+        Pass p;
+        std::memset(&p.g, 0, sizeof(p.g));
+        p.g.N = N;
+        p.g.T = __builtin_popcountll(tileset);
+        int L = 0;
+        while (L < N && ((tileset >> L) & 1)) ++L;
+        p.g.L = L;
+        p.g.H = 0;
+        for (int b = L; b < N; ++b)
+            if ((tileset >> b) & 1) p.g.hb[p.g.H++] = b;
+        Fuser f(&p.g);
+        for (int idx : taken) {
+            f.add(gates[idx]);
+            if (epilogue_after_special >= 0 && gates[idx].special == epilogue_after_special) p.epilogue = true;
+        }
+        f.flush_all();
+        p.ops = std::move(f.ops);
+        passes.push_back(std::move(p));
+        remaining.swap(rest);
+    }
+    return passes;
+}
+
+}  // namespace smoq

@@ -1,0 +1,161 @@
+// smoq_internal.h -- shared definitions of libsmoq_cuda.so (host + device).
+//
+// Layout in HBM: a state object holds B states ("batch", e.g. MCWF
+// trajectories or VQE parameter sets) of 2^N amplitudes each, state-major
+// (state b at offset b * 2^N), amplitudes interleaved (re, im) exactly like
+// Julia's Vector{ComplexF32/ComplexF64}.  Little-endian qubits: qubit k
+// (0-based at this ABI) is bit k of the amplitude index.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <complex>
+#include <string>
+#include <vector>
+#include "../../include/smoq_cuda.h"
+
+namespace smoq {
+
+using cd = std::complex<double>;
+
+// ----------------------------------------------------------------------------
+// Device op program.  One DevOp is one fused operation applied to every
+// amplitude group of a tile (tile kernel) or of the whole state (direct
+// kernel).  Matrix element (r, c) of a k-qubit op lives in c[r * 2^k + c];
+// bit t of a local matrix index is the value of the op's qubit t.
+// ----------------------------------------------------------------------------
+enum OpKind : int32_t {
+    OPK_DENSE1 = 0,   // 2x2 dense on qubit 0
+    OPK_DENSE2 = 1,   // 4x4 dense on qubits (0, 1)
+    OPK_PARITY2 = 2,  // 4x4 that keeps parity: even block {00,11}, odd block {01,10}
+    OPK_MONO = 3,     // monomial (permutation x phase) on 1..3 qubits
+    OPK_DIAG = 4,     // diagonal on 0..3 qubits; qubits need not be tile bits
+    OPK_STATESCALE = 5,  // amp *= scale[b] (per state, real, from aux pointer)
+    OPK_REALTAB = 6,  // amp *= prod_j tab[j][byte j of global index] (real factors)
+    OPK_JUMP = 7,     // per-state jump (sigma-/sigma+/sigma_z/sigma_x) from aux list
+};
+
+struct alignas(16) DevOp {
+    int32_t kind;
+    int32_t nq;
+    int32_t lb[3];      // tile-local bit of qubit t, -1 when the qubit is not a tile bit
+    int32_t gb[3];      // global bit of qubit t
+    int32_t perm[8];    // OPK_MONO: out[r] = ph[r] * in[perm[r]]
+    int32_t pad[2];
+    const void* aux;    // OPK_STATESCALE: const double* scale[B]; OPK_REALTAB: const double* tabs
+    int64_t aux2;       // OPK_REALTAB: number of byte tables
+    double2 cd[16];     // coefficients, double precision
+    float2 cf[16];      // the same, rounded to float (complex64 kernels)
+};
+
+// Tile geometry of one pass: the tile is the set of amplitudes whose index
+// varies over the low L bits and over the high bits hb[0..H-1]; every other
+// index bit is fixed by the tile number.
+struct TileGeom {
+    int32_t N, T, L, H;
+    int32_t hb[24];
+};
+
+// Per-pass epilogue: per-tile partial sums of |psi|^2 and of |psi|^2 over
+// amplitudes with bit q set (q in pop_mask order), written to
+// partials[(tile_global) * (1 + npop) + j].
+struct Epilogue {
+    double* partials;   // nullptr: no epilogue
+    int32_t npop;
+    int32_t popq[40];
+};
+
+struct TileArgs {
+    void* psi;
+    int64_t state_len;       // 2^N
+    int64_t tiles_per_state; // 2^(N-T)
+    int64_t ntiles;          // B * tiles_per_state
+    const DevOp* ops;
+    int32_t nops;
+    int32_t* err;
+    TileGeom g;
+    Epilogue ep;
+};
+
+// ----------------------------------------------------------------------------
+// Host-side gate IR consumed by the planner.
+// ----------------------------------------------------------------------------
+struct GateIR {
+    int nq = 0;             // 0..3 qubits
+    int q[3] = {0, 0, 0};   // 0-based global qubits
+    bool diag = false;      // diagonal in the computational basis (commutes with diagonals)
+    int special = 0;        // 0: matrix gate; OPK_STATESCALE / OPK_REALTAB / OPK_JUMP
+    const void* aux = nullptr;
+    int64_t aux2 = 0;
+    cd m[64];               // row-major 2^nq x 2^nq; bit t of an index = qubit q[t]
+    int tag = -1;           // caller tag (e.g. parameter index) carried through
+};
+
+struct Pass {
+    TileGeom g;
+    std::vector<DevOp> ops;
+    bool epilogue = false;
+};
+
+// planner.cpp
+std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, int Lmin,
+                              int epilogue_after_special = -1);
+void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op);
+
+// gate library (planner.cpp)
+GateIR gate_1q(int q, const cd m[4]);
+GateIR gate_2q(int q0, int q1, const cd m[16]);
+GateIR gate_named(int type, const int* q, double angle);
+
+}  // namespace smoq
+
+// ----------------------------------------------------------------------------
+// Objects behind the opaque C handles.
+// ----------------------------------------------------------------------------
+struct smoq_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    int32_t* d_err = nullptr;          // device error word (timeouts, bad input)
+    double* d_scratch = nullptr;       // reduction partials
+    size_t scratch_bytes = 0;
+    double* h_pinned = nullptr;        // pinned host staging for small results
+    size_t pinned_bytes = 0;
+    int tile_bits_c64 = 13;
+    int tile_bits_c128 = 12;
+    int low_bits_c64 = 5;
+    int low_bits_c128 = 4;
+    int use_graphs = 1;
+    int kernel_timing = 0;             // bracket tile passes with events
+    long long launches = 0;            // kernels launched by this ctx
+    long long tile_passes = 0;
+    double tile_ms = 0;                // summed tile-pass time when kernel_timing
+    double tile_bytes = 0;             // algorithmic bytes of the timed tile passes
+    int num_sms = 148;
+};
+
+struct smoq_state {
+    smoq_ctx* ctx = nullptr;
+    int N = 0;
+    int dtype = SMOQ_C64;
+    int batch = 1;
+    void* ptr = nullptr;
+    bool owned = true;
+    size_t amp_bytes() const { return dtype == SMOQ_C64 ? 8 : 16; }
+    size_t bytes() const { return ((size_t)1 << N) * (size_t)batch * amp_bytes(); }
+};
+
+// kernels (k_*.cu)
+namespace smoq {
+cudaError_t launch_direct_op(smoq_state* st, const DevOp& op);
+cudaError_t launch_tile_pass(smoq_ctx* ctx, smoq_state* st, const Pass& p, const DevOp* d_ops,
+                             const Epilogue* ep);
+cudaError_t launch_diag_reduce(smoq_ctx* ctx, smoq_state* st, const uint64_t* zmasks, int nobs,
+                               double* d_out);
+cudaError_t launch_pauli_reduce(smoq_ctx* ctx, smoq_state* st, uint64_t xmask, uint64_t zmask,
+                                int ny, double* d_out);
+cudaError_t launch_set_basis(smoq_state* st, uint64_t index);
+cudaError_t launch_scale(smoq_state* st, const double* d_scale_per_state, double scalar);
+cudaError_t launch_convert(smoq_state* dst, smoq_state* src);
+size_t diag_reduce_scratch_doubles(smoq_state* st, int nobs);
+size_t tile_max_smem(int amp_bytes, int T);
+}  // namespace smoq
