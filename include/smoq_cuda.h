@@ -235,6 +235,27 @@ smoq_status smoq_energy(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* o
                         int n_params, const smoq_pauli_term* H, int nterms, int batch,
                         const double* theta, double* energies);
 
+/* ------------------------------------------------- host-only introspection */
+/* No counterpart in the reference.  Runs the fused-pass planner (host code,
+ * no GPU or context needed) on a gate sequence exactly as
+ * smoq_apply_sequence would and reports, per pass, the tile geometry and the
+ * fused ops (kind = 0 dense 2x2, 1 dense 4x4, 2 parity 4x4, 3 monomial,
+ * 4 diagonal; coefficients as the kernels read them).  Counts are written
+ * even when the output arrays are too small (NULL arrays allowed). */
+typedef struct {
+    int32_t T, L, H, nops;
+    int32_t hb[24];
+} smoq_pass_info;
+typedef struct {
+    int32_t kind, nq;
+    int32_t lb[4], gb[4];
+    int32_t perm[8];
+    double c[32];          /* 16 interleaved complex coefficients */
+} smoq_fused_op_info;
+smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops,
+                                     int n, const double* theta, smoq_pass_info* passes, int max_passes,
+                                     smoq_fused_op_info* fused, int max_fused, int* n_passes, int* n_fused);
+
 #ifdef __cplusplus
 }
 #endif

@@ -176,6 +176,7 @@ smoq_status smoq_ctx_create(int device, smoq_ctx** out) {
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (cudaMalloc(&ctx->d_err, sizeof(int32_t)) != cudaSuccess) return SMOQ_ERR_OOM;
     if (cudaMemset(ctx->d_err, 0, sizeof(int32_t)) != cudaSuccess) return SMOQ_ERR_CUDA;
+    if (tile_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (ensure_scratch(ctx.get(), 1 << 17) != SMOQ_OK) return SMOQ_ERR_OOM;
     if (ensure_pinned(ctx.get(), 1 << 20) != SMOQ_OK) return SMOQ_ERR_OOM;
     *out = ctx.release();
@@ -207,11 +208,11 @@ smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long v) {
     if (!ctx) return SMOQ_ERR_BADINPUT;
     switch (option) {
         case SMOQ_OPT_TILE_BITS_C64:
-            if (v < 1 || v > 14) return fail(ctx, SMOQ_ERR_BADINPUT, "tile bits (c64) must be 1..14");
+            if (v < 4 || v > 14) return fail(ctx, SMOQ_ERR_BADINPUT, "tile bits (c64) must be 4..14");
             ctx->tile_bits_c64 = (int)v;
             break;
         case SMOQ_OPT_TILE_BITS_C128:
-            if (v < 1 || v > 13) return fail(ctx, SMOQ_ERR_BADINPUT, "tile bits (c128) must be 1..13");
+            if (v < 3 || v > 13) return fail(ctx, SMOQ_ERR_BADINPUT, "tile bits (c128) must be 3..13");
             ctx->tile_bits_c128 = (int)v;
             break;
         case SMOQ_OPT_LOW_BITS_C64:
@@ -501,7 +502,8 @@ smoq_status smoq_apply_sequence(smoq_state* st, const smoq_op* ops, int n, const
     if (smoq_status s = ops_to_ir(st, st->N, ops, n, theta, ir)) return s;
     DevProgram P;
     try {
-        P.passes = plan_passes(ir, st->N, tile_bits(ctx, st->dtype), low_bits(ctx, st->dtype));
+        P.passes = plan_passes(ir, st->N, tile_bits(ctx, st->dtype), low_bits(ctx, st->dtype), -1,
+                               st->dtype == SMOQ_C64 ? 1 : 0);
     } catch (const std::exception& ex) {
         return fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
     }
@@ -513,6 +515,55 @@ smoq_status smoq_apply_sequence(smoq_state* st, const smoq_op* ops, int n, const
     harvest_timing(ctx, timing);
     if (s) return s;
     return sync_check(ctx);
+}
+
+smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tbits, int lbits, const smoq_op* ops, int n,
+                                     const double* theta, smoq_pass_info* passes, int max_passes,
+                                     smoq_fused_op_info* fused, int max_fused, int* n_passes, int* n_fused) {
+    if (N < 1 || N > 40 || n < 0 || (n > 0 && !ops) || !n_passes || !n_fused) return SMOQ_ERR_BADINPUT;
+    if (dtype != SMOQ_C64 && dtype != SMOQ_C128) return SMOQ_ERR_BADINPUT;
+    std::vector<GateIR> ir;
+    if (smoq_status s = ops_to_ir(nullptr, N, ops, n, theta, ir)) return s;
+    std::vector<Pass> pl;
+    try {
+        pl = plan_passes(ir, N, tbits, lbits, -1, dtype == SMOQ_C64 ? 1 : 0);
+    } catch (const std::exception&) {
+        return SMOQ_ERR_BADINPUT;
+    }
+    int np = 0, no = 0;
+    for (const Pass& p : pl) {
+        if (passes && np < max_passes) {
+            smoq_pass_info& pi = passes[np];
+            std::memset(&pi, 0, sizeof(pi));
+            pi.T = p.g.T;
+            pi.L = p.g.L;
+            pi.H = p.g.H;
+            pi.nops = (int32_t)p.ops.size();
+            for (int m = 0; m < p.g.H; ++m) pi.hb[m] = p.g.hb[m];
+        }
+        ++np;
+        for (const DevOp& op : p.ops) {
+            if (fused && no < max_fused) {
+                smoq_fused_op_info& fi = fused[no];
+                std::memset(&fi, 0, sizeof(fi));
+                fi.kind = op.kind;
+                fi.nq = op.nq;
+                for (int t = 0; t < 4; ++t) {
+                    fi.lb[t] = op.lb[t];
+                    fi.gb[t] = op.gb[t];
+                }
+                for (int r = 0; r < 8; ++r) fi.perm[r] = op.perm[r];
+                for (int k = 0; k < 16; ++k) {
+                    fi.c[2 * k] = op.cd[k].x;
+                    fi.c[2 * k + 1] = op.cd[k].y;
+                }
+            }
+            ++no;
+        }
+    }
+    *n_passes = np;
+    *n_fused = no;
+    return SMOQ_OK;
 }
 
 smoq_status smoq_apply_sequence_unfused(smoq_state* st, const smoq_op* ops, int n, const double* theta) {
@@ -688,7 +739,8 @@ static smoq_status get_block(smoq_plan* P, int nsteps, smoq_plan::Block** out) {
     all.reserve(P->step.size() * nsteps);
     for (int s = 0; s < nsteps; ++s) all.insert(all.end(), P->step.begin(), P->step.end());
     try {
-        B->prog.passes = plan_passes(all, P->N, tile_bits(P->ctx, P->dtype), low_bits(P->ctx, P->dtype));
+        B->prog.passes = plan_passes(all, P->N, tile_bits(P->ctx, P->dtype), low_bits(P->ctx, P->dtype), -1,
+                                     P->dtype == SMOQ_C64 ? 1 : 0);
     } catch (const std::exception& ex) {
         return fail(P->ctx, SMOQ_ERR_BADINPUT, ex.what());
     }

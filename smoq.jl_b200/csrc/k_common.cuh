@@ -70,12 +70,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait on an mbarrier phase: gives up after 2^24 polls (each poll may
-// suspend the thread for a hardware time slice, so the bound is far above any
-// legitimate copy), records DEVERR_TIMEOUT and returns false.
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait on an mbarrier phase: gives up after kWaitLimitNs of wall time
+// (a legitimate tile copy completes in microseconds) or 2^22 polls, whichever
+// comes first, records DEVERR_TIMEOUT and returns false.
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int32_t* err) {
-    for (int it = 0; it < (1 << 24); ++it)
+    const uint64_t t0 = globaltimer_ns();
+    for (int it = 0; it < (1 << 22); ++it) {
         if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 63) == 63 && globaltimer_ns() - t0 > kWaitLimitNs) break;
+    }
     if (err) atomicExch(err, DEVERR_TIMEOUT);
     return false;
 }

@@ -33,27 +33,19 @@ struct DiagBits {
 template <typename R>
 __device__ __forceinline__ void tile_diag(const DevOp& op, typename CT<R>::T* tile, uint32_t amps,
                                           uint64_t base) {
-    using C = typename CT<R>::T;
     const int nq = op.nq;
-    int sh[3] = {-1, -1, -1};
+    int sh[4] = {-1, -1, -1, -1};
     int cm = 0;  // constant part of the matrix index
     for (int t = 0; t < nq; ++t) {
         if (op.lb[t] >= 0) sh[t] = op.lb[t];
         else cm |= (int)((base >> op.gb[t]) & 1) << t;
     }
-    C ph[8];
-#pragma unroll
-    for (int m = 0; m < 8; ++m) ph[m] = coef<R>(op, m);
     for (uint32_t j = threadIdx.x; j < amps; j += blockDim.x) {
         int m = cm;
 #pragma unroll
-        for (int t = 0; t < 3; ++t)
+        for (int t = 0; t < 4; ++t)
             if (sh[t] >= 0) m |= (int)((j >> sh[t]) & 1) << t;
-        C p = ph[0];
-#pragma unroll
-        for (int k = 1; k < 8; ++k)
-            if (m == k) p = ph[k];
-        tile[j] = cmul(p, tile[j]);
+        tile[j] = cmul(coef<R>(op, m), tile[j]);  // op lives in global memory: a cached load
     }
 }
 
@@ -200,9 +192,9 @@ __global__ void __launch_bounds__(256) direct_op_kernel(typename CT<R>::T* psi, 
     const uint64_t nthr = (uint64_t)gridDim.x * blockDim.x;
     const int kind = op.kind;
     if (kind == OPK_DIAG || kind == OPK_STATESCALE) {
-        C ph[8];
+        C ph[16];
 #pragma unroll
-        for (int m = 0; m < 8; ++m) ph[m] = coef<R>(op, m);
+        for (int m = 0; m < 16; ++m) ph[m] = coef<R>(op, m);
         const uint64_t total = (uint64_t)B * len;
         for (uint64_t i = tid; i < total; i += nthr) {
             C p;
@@ -211,7 +203,7 @@ __global__ void __launch_bounds__(256) direct_op_kernel(typename CT<R>::T* psi, 
                 for (int t = 0; t < op.nq; ++t) m |= (int)((i >> op.gb[t]) & 1) << t;
                 p = ph[0];
 #pragma unroll
-                for (int k = 1; k < 8; ++k)
+                for (int k = 1; k < 16; ++k)
                     if (m == k) p = ph[k];
             } else {
                 p = czero(ph[0]);
@@ -385,20 +377,39 @@ cudaError_t launch_direct_op(smoq_state* st, const DevOp& op) {
 
 size_t tile_max_smem(int amp_bytes, int T) { return (size_t)amp_bytes << T; }
 
+// Opt the tile kernels in to large dynamic shared memory and record their
+// occupancy for every tile width, once per context (never during capture).
 template <typename R, bool EPI>
-static cudaError_t launch_tile_t(smoq_ctx* ctx, const TileArgs& a, size_t smem) {
-    static bool configured[2] = {false, false};
+static cudaError_t init_tile_t(smoq_ctx* ctx, int dt) {
     auto kern = tile_pass_kernel<R, EPI>;
-    // opt in to >48 KB dynamic shared memory once per instantiation
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)tile_max_smem((int)sizeof(typename CT<R>::T), dt == 0 ? 14 : 13));
     if (e != cudaSuccess) return e;
-    (void)configured;
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TILE_THREADS, smem);
+    for (int T = 1; T <= (dt == 0 ? 14 : 13); ++T) {
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TILE_THREADS,
+                                                          tile_max_smem((int)sizeof(typename CT<R>::T), T));
+        if (e != cudaSuccess) return e;
+        ctx->tile_occ[dt][EPI ? 1 : 0][T] = per_sm < 1 ? 1 : per_sm;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t tile_kernels_init(smoq_ctx* ctx) {
+    cudaError_t e;
+    if ((e = init_tile_t<float, false>(ctx, 0)) != cudaSuccess) return e;
+    if ((e = init_tile_t<float, true>(ctx, 0)) != cudaSuccess) return e;
+    if ((e = init_tile_t<double, false>(ctx, 1)) != cudaSuccess) return e;
+    return init_tile_t<double, true>(ctx, 1);
+}
+
+template <typename R, bool EPI>
+static cudaError_t launch_tile_t(smoq_ctx* ctx, const TileArgs& a, size_t smem, int dt) {
+    int per_sm = ctx->tile_occ[dt][EPI ? 1 : 0][a.g.T];
     if (per_sm < 1) per_sm = 1;
     int64_t grid = (int64_t)ctx->num_sms * per_sm;
     if (grid > a.ntiles) grid = a.ntiles;
-    kern<<<(unsigned)grid, TILE_THREADS, smem, ctx->stream>>>(a);
+    tile_pass_kernel<R, EPI><<<(unsigned)grid, TILE_THREADS, smem, ctx->stream>>>(a);
     return cudaGetLastError();
 }
 
@@ -419,9 +430,9 @@ cudaError_t launch_tile_pass(smoq_ctx* ctx, smoq_state* st, const Pass& p, const
     cudaError_t e;
     const bool epi = ep && ep->partials;
     if (st->dtype == SMOQ_C64)
-        e = epi ? launch_tile_t<float, true>(ctx, a, smem) : launch_tile_t<float, false>(ctx, a, smem);
+        e = epi ? launch_tile_t<float, true>(ctx, a, smem, 0) : launch_tile_t<float, false>(ctx, a, smem, 0);
     else
-        e = epi ? launch_tile_t<double, true>(ctx, a, smem) : launch_tile_t<double, false>(ctx, a, smem);
+        e = epi ? launch_tile_t<double, true>(ctx, a, smem, 1) : launch_tile_t<double, false>(ctx, a, smem, 1);
     ctx->launches++;
     return e;
 }

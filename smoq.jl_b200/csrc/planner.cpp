@@ -158,11 +158,11 @@ static void fill_coeffs(DevOp& op, const cd* v, int n) {
     }
 }
 
-// classify and encode a k-qubit matrix (k = 1..3) as a DevOp
+// classify and encode a k-qubit matrix (k = 1..3; diagonals up to 4) as a DevOp
 static void encode_matrix(int nq, const cd* M, DevOp& op) {
     const int dim = 1 << nq;
-    bool diag = true, mono = true;
-    int perm[8];
+    bool diag = true, mono = nq <= 3;
+    int perm[16];
     for (int r = 0; r < dim; ++r) {
         int nz = 0;
         perm[r] = r;
@@ -177,7 +177,7 @@ static void encode_matrix(int nq, const cd* M, DevOp& op) {
     }
     op.nq = nq;
     if (diag) {
-        cd d[8];
+        cd d[16];
         for (int k = 0; k < dim; ++k) d[k] = M[k * dim + k];
         op.kind = OPK_DIAG;
         fill_coeffs(op, d, dim);
@@ -225,7 +225,7 @@ static int local_bit(const TileGeom* g, int q) {
 
 void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op) {
     std::memset(&op, 0, sizeof(op));
-    for (int t = 0; t < 3; ++t) {
+    for (int t = 0; t < 4; ++t) {
         op.lb[t] = -1;
         op.gb[t] = 0;
     }
@@ -247,28 +247,100 @@ void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op) {
 
 // -------------------------------------------------------------------- plan
 namespace {
+// diagonal of a diagonal gate, index bit t = qubit q[t]
+static void diag_of(const GateIR& g, cd* d) {
+    const int dim = 1 << g.nq;
+    for (int k = 0; k < dim; ++k) d[k] = g.m[k * dim + k];
+}
+
+// Fusion inside one pass.  Ops are kept in host (matrix) form until the pass
+// is complete so that later gates can still be folded into earlier ops:
+//  * 1-qubit gates on a tile qubit accumulate in a pending 2x2 per qubit;
+//  * a 2-qubit gate absorbs the pending 2x2s of its qubits, and merges into
+//    the last op on the same pair when no op since has touched either qubit;
+//  * a pending 2x2 that is flushed (end of pass, or a diagonal on a non-tile
+//    qubit) is folded into the last 2-qubit op on its qubit when nothing
+//    after that op touched the qubit;
+//  * consecutive diagonal ops merge into one phase table (up to 4 qubits).
 struct Fuser {
     const TileGeom* g;
-    std::vector<DevOp> ops;
+    std::vector<GateIR> ops;
     bool have_pending[64] = {};
     cd pending[64][4];
-    int last2q = -1;  // index in ops of the last op if it is a mergeable 2-qubit op
-    cd last_m[16];
-    int last_q[2] = {-1, -1};
+    int last_touch[64];
 
-    explicit Fuser(const TileGeom* geom) : g(geom) {}
-
-    void emit(const GateIR& gt) {
-        DevOp op;
-        build_devop(gt, g, op);
-        ops.push_back(op);
-        last2q = -1;
+    explicit Fuser(const TileGeom* geom) : g(geom) {
+        for (int q = 0; q < 64; ++q) last_touch[q] = -1;
+    }
+    bool is_tile(int q) const { return local_bit(g, q) >= 0; }
+    bool tile_2q(const GateIR& o) const {
+        return o.nq == 2 && !o.special && is_tile(o.q[0]) && is_tile(o.q[1]);
+    }
+    void touch(int idx) {
+        const GateIR& o = ops[idx];
+        if (o.special == OPK_REALTAB) {
+            for (int q = 0; q < 64; ++q) last_touch[q] = idx;
+            return;
+        }
+        for (int t = 0; t < o.nq; ++t) last_touch[o.q[t]] = idx;
+    }
+    static bool merge_diag(GateIR& A, const GateIR& B) {
+        int uq[4], u = 0;
+        for (int t = 0; t < A.nq; ++t) uq[u++] = A.q[t];
+        for (int t = 0; t < B.nq; ++t) {
+            bool seen = false;
+            for (int s = 0; s < u; ++s) seen |= (uq[s] == B.q[t]);
+            if (!seen) {
+                if (u == 4) return false;
+                uq[u++] = B.q[t];
+            }
+        }
+        cd da[16], db[16], d[16];
+        diag_of(A, da);
+        diag_of(B, db);
+        for (int m = 0; m < (1 << u); ++m) {
+            int ia = 0, ib = 0;
+            for (int t = 0; t < A.nq; ++t)
+                for (int s = 0; s < u; ++s)
+                    if (uq[s] == A.q[t]) ia |= ((m >> s) & 1) << t;
+            for (int t = 0; t < B.nq; ++t)
+                for (int s = 0; s < u; ++s)
+                    if (uq[s] == B.q[t]) ib |= ((m >> s) & 1) << t;
+            d[m] = da[ia] * db[ib];
+        }
+        GateIR r;
+        r.nq = u;
+        for (int s = 0; s < u; ++s) r.q[s] = uq[s];
+        const int dim = 1 << u;
+        for (int k = 0; k < dim * dim; ++k) r.m[k] = 0.0;
+        for (int k = 0; k < dim; ++k) r.m[k * dim + k] = d[k];
+        r.diag = true;
+        A = r;
+        return true;
+    }
+    void push(const GateIR& gt) {
+        if (gt.diag && !gt.special && !ops.empty() && ops.back().diag && !ops.back().special &&
+            merge_diag(ops.back(), gt)) {
+            touch((int)ops.size() - 1);
+            return;
+        }
+        ops.push_back(gt);
+        touch((int)ops.size() - 1);
     }
     void flush(int q) {
         if (!have_pending[q]) return;
-        GateIR p = gate_1q(q, pending[q]);
         have_pending[q] = false;
-        emit(p);
+        const int j = last_touch[q];
+        if (j >= 0 && tile_2q(ops[j])) {
+            static const cd Id[4] = {1, 0, 0, 1};
+            cd P4[16], out[16];
+            if (ops[j].q[0] == q) kron2(pending[q], Id, P4);
+            else kron2(Id, pending[q], P4);
+            matmul(4, P4, ops[j].m, out);  // the pending gates act after op j
+            ops[j] = gate_2q(ops[j].q[0], ops[j].q[1], out);
+            return;
+        }
+        push(gate_1q(q, pending[q]));
     }
     void flush_all() {
         for (int q = 0; q < 64; ++q) flush(q);
@@ -276,12 +348,13 @@ struct Fuser {
     void add(const GateIR& gt) {
         if (gt.special) {
             if (gt.special == OPK_REALTAB) flush_all();  // diagonal over every qubit
-            emit(gt);
+            ops.push_back(gt);
+            touch((int)ops.size() - 1);
             return;
         }
         bool all_tile = true;
         for (int t = 0; t < gt.nq; ++t)
-            if (local_bit(g, gt.q[t]) < 0) all_tile = false;
+            if (!is_tile(gt.q[t])) all_tile = false;
         if (gt.nq == 1 && all_tile) {
             const int q = gt.q[0];
             if (have_pending[q]) {
@@ -305,35 +378,45 @@ struct Fuser {
                 matmul(4, M, K, M);
                 have_pending[a] = have_pending[b] = false;
             }
-            if (last2q >= 0 && ((last_q[0] == a && last_q[1] == b) || (last_q[0] == b && last_q[1] == a))) {
-                cd Mal[16];
-                if (last_q[0] == a) std::memcpy(Mal, M, sizeof(Mal));
+            const int j = last_touch[a];
+            if (j >= 0 && j == last_touch[b] && tile_2q(ops[j]) &&
+                ((ops[j].q[0] == a && ops[j].q[1] == b) || (ops[j].q[0] == b && ops[j].q[1] == a))) {
+                cd Mal[16], out[16];
+                if (ops[j].q[0] == a) std::memcpy(Mal, M, sizeof(Mal));
                 else swap_roles(M, Mal);
-                matmul(4, Mal, last_m, last_m);
-                GateIR merged = gate_2q(last_q[0], last_q[1], last_m);
-                build_devop(merged, g, ops[last2q]);
+                matmul(4, Mal, ops[j].m, out);
+                ops[j] = gate_2q(ops[j].q[0], ops[j].q[1], out);
                 return;
             }
-            GateIR fused = gate_2q(a, b, M);
-            emit(fused);
-            last2q = (int)ops.size() - 1;
-            std::memcpy(last_m, M, sizeof(M));
-            last_q[0] = a;
-            last_q[1] = b;
+            push(gate_2q(a, b, M));
             return;
         }
         // diagonal gates touching non-tile qubits, and 3-qubit gates
         for (int t = 0; t < gt.nq; ++t)
-            if (local_bit(g, gt.q[t]) >= 0) flush(gt.q[t]);
+            if (is_tile(gt.q[t])) flush(gt.q[t]);
         if (!all_tile && !gt.diag) throw std::logic_error("planner placed a non-diagonal gate off-tile");
-        emit(gt);
+        push(gt);
+    }
+    std::vector<DevOp> finish() {
+        flush_all();
+        std::vector<DevOp> out(ops.size());
+        for (size_t i = 0; i < ops.size(); ++i) build_devop(ops[i], g, out[i]);
+        return out;
     }
 };
 }  // namespace
 
 std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, int Lmin,
-                              int epilogue_after_special) {
+                              int epilogue_after_special, int Lreq) {
+    // Lreq: contiguous low qubits every tile must hold (complex64 needs 1 so a
+    // segment is >= 16 bytes, the bulk-copy granule).  A tile must keep room
+    // for a 3-qubit gate next to its reserved low qubits, or some gates could
+    // never be placed.
     if (T > N) T = N;
+    if (Lreq > T) Lreq = T;
+    if (T < N && T < Lreq + 3) throw std::invalid_argument("tile too narrow for 3-qubit gates");
+    if (Lmin > T - 3) Lmin = T - 3;
+    if (Lmin < Lreq) Lmin = Lreq;
     if (Lmin > T) Lmin = T;
     std::vector<int> remaining(gates.size());
     for (size_t i = 0; i < gates.size(); ++i) remaining[i] = (int)i;
@@ -362,6 +445,7 @@ std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, in
                 }
             }
         }
+        if (taken.empty()) throw std::logic_error("planner made no progress");
         // widen the tile with the lowest free qubits: longer contiguous segments
         for (int b = 0; b < N && __builtin_popcountll(tileset) < T; ++b) tileset |= 1ull << b;
         Pass p;
@@ -379,8 +463,7 @@ std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, in
             f.add(gates[idx]);
             if (epilogue_after_special >= 0 && gates[idx].special == epilogue_after_special) p.epilogue = true;
         }
-        f.flush_all();
-        p.ops = std::move(f.ops);
+        p.ops = f.finish();
         passes.push_back(std::move(p));
         remaining.swap(rest);
     }

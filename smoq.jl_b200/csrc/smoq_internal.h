@@ -36,11 +36,10 @@ enum OpKind : int32_t {
 
 struct alignas(16) DevOp {
     int32_t kind;
-    int32_t nq;
-    int32_t lb[3];      // tile-local bit of qubit t, -1 when the qubit is not a tile bit
-    int32_t gb[3];      // global bit of qubit t
+    int32_t nq;         // 1..3 qubits (OPK_DIAG: 0..4)
+    int32_t lb[4];      // tile-local bit of qubit t, -1 when the qubit is not a tile bit
+    int32_t gb[4];      // global bit of qubit t
     int32_t perm[8];    // OPK_MONO: out[r] = ph[r] * in[perm[r]]
-    int32_t pad[2];
     const void* aux;    // OPK_STATESCALE: const double* scale[B]; OPK_REALTAB: const double* tabs
     int64_t aux2;       // OPK_REALTAB: number of byte tables
     double2 cd[16];     // coefficients, double precision
@@ -80,13 +79,13 @@ struct TileArgs {
 // Host-side gate IR consumed by the planner.
 // ----------------------------------------------------------------------------
 struct GateIR {
-    int nq = 0;             // 0..3 qubits
-    int q[3] = {0, 0, 0};   // 0-based global qubits
+    int nq = 0;             // 0..3 qubits (diagonals merged by the fuser: up to 4)
+    int q[4] = {0, 0, 0, 0};  // 0-based global qubits
     bool diag = false;      // diagonal in the computational basis (commutes with diagonals)
     int special = 0;        // 0: matrix gate; OPK_STATESCALE / OPK_REALTAB / OPK_JUMP
     const void* aux = nullptr;
     int64_t aux2 = 0;
-    cd m[64];               // row-major 2^nq x 2^nq; bit t of an index = qubit q[t]
+    cd m[256];              // row-major 2^nq x 2^nq; bit t of an index = qubit q[t]
     int tag = -1;           // caller tag (e.g. parameter index) carried through
 };
 
@@ -98,7 +97,7 @@ struct Pass {
 
 // planner.cpp
 std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, int Lmin,
-                              int epilogue_after_special = -1);
+                              int epilogue_after_special = -1, int Lreq = 0);
 void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op);
 
 // gate library (planner.cpp)
@@ -131,6 +130,7 @@ struct smoq_ctx {
     double tile_ms = 0;                // summed tile-pass time when kernel_timing
     double tile_bytes = 0;             // algorithmic bytes of the timed tile passes
     int num_sms = 148;
+    int tile_occ[2][2][16] = {};       // CTAs per SM of tile_pass_kernel [dtype][epilogue][T]
 };
 
 struct smoq_state {
@@ -158,4 +158,5 @@ cudaError_t launch_scale(smoq_state* st, const double* d_scale_per_state, double
 cudaError_t launch_convert(smoq_state* dst, smoq_state* src);
 size_t diag_reduce_scratch_doubles(smoq_state* st, int nobs);
 size_t tile_max_smem(int amp_bytes, int T);
+cudaError_t tile_kernels_init(smoq_ctx* ctx);
 }  // namespace smoq

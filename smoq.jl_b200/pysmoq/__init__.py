@@ -33,7 +33,7 @@ __all__ = [
     "precompute_trotter_gates_bitwise", "TrotterPlan", "apply_fast_trotter_step", "evolve_trotter_psi",
     "CircuitOperation", "gate", "ParameterizedCircuit", "single_qubit_rotation_layer", "entangling_layer",
     "repeat_layer", "apply_circuit", "JumpOperator", "create_jump_operator", "mcwf_run", "PauliSum",
-    "energy", "energy_and_gradient",
+    "energy", "energy_and_gradient", "debug_plan",
 ]
 
 
@@ -634,3 +634,30 @@ def energy_and_gradient(ctx: Context, circuit: ParameterizedCircuit, H: PauliSum
     ck(lib.smoq_energy_grad(ctx.h, circuit.N, dtype, ops, len(circuit.operations), circuit.n_params, H.c_terms(),
                             len(H.terms), B, dptr(th), dptr(e), dptr(g)), ctx.h, "energy_grad")
     return e, g
+
+
+# ------------------------------------------------------ planner introspection
+def debug_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtype: int = C128, tile_bits: int = 12,
+               low_bits: int = 4):
+    """Host-only view of how smoq_apply_sequence splits `ops` into tile passes.
+    Returns a list of passes: {"T","L","H","hb","ops":[{"kind","nq","lb","gb","perm","c"}]}."""
+    arr = circuit_to_c_ops(ops)
+    th = np.ascontiguousarray(theta if theta is not None else np.zeros(1), dtype=np.float64)
+    npass, nops = C.c_int(), C.c_int()
+    ck(lib.smoq_debug_plan_sequence(N, dtype, tile_bits, low_bits, arr, len(ops), dptr(th), None, 0, None, 0,
+                                    C.byref(npass), C.byref(nops)), None, "debug_plan")
+    P = (_lib.SmoqPassInfo * max(1, npass.value))()
+    F = (_lib.SmoqFusedOpInfo * max(1, nops.value))()
+    ck(lib.smoq_debug_plan_sequence(N, dtype, tile_bits, low_bits, arr, len(ops), dptr(th), P, npass.value, F,
+                                    nops.value, C.byref(npass), C.byref(nops)), None, "debug_plan")
+    out, k = [], 0
+    for i in range(npass.value):
+        p = P[i]
+        d = {"T": p.T, "L": p.L, "H": p.H, "hb": list(p.hb[:p.H]), "ops": []}
+        for _ in range(p.nops):
+            f = F[k]
+            k += 1
+            d["ops"].append({"kind": f.kind, "nq": f.nq, "lb": list(f.lb), "gb": list(f.gb), "perm": list(f.perm),
+                             "c": np.array(f.c[:]).view(np.complex128).copy()})
+        out.append(d)
+    return out

@@ -38,6 +38,15 @@ class SmoqPauliTerm(C.Structure):
     _fields_ = [("coef", C.c_double), ("xmask", C.c_uint64), ("zmask", C.c_uint64)]
 
 
+class SmoqPassInfo(C.Structure):
+    _fields_ = [("T", C.c_int32), ("L", C.c_int32), ("H", C.c_int32), ("nops", C.c_int32), ("hb", C.c_int32 * 24)]
+
+
+class SmoqFusedOpInfo(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("nq", C.c_int32), ("lb", C.c_int32 * 4), ("gb", C.c_int32 * 4),
+                ("perm", C.c_int32 * 8), ("c", C.c_double * 32)]
+
+
 class SmoqError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"smoq status {STATUS_NAMES.get(status, status)}: {msg}")
@@ -117,6 +126,8 @@ _SIGS = {
                       C.c_int, _dp, _dp, _dp, _dp, _ip],
     "smoq_energy_grad": [_vp, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, C.c_int, C.POINTER(SmoqPauliTerm),
                          C.c_int, C.c_int, _dp, _dp, _dp],
+    "smoq_debug_plan_sequence": [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, _dp,
+                                 C.POINTER(SmoqPassInfo), C.c_int, C.POINTER(SmoqFusedOpInfo), C.c_int, _ip, _ip],
     "smoq_energy": [_vp, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, C.c_int, C.POINTER(SmoqPauliTerm),
                     C.c_int, C.c_int, _dp, _dp],
 }

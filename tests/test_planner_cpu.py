@@ -1,0 +1,149 @@
+"""Host logic of the fused-pass planner, checked on CPU: smoq_debug_plan_sequence
+returns the exact pass geometry and fused op program the GPU would run; a numpy
+replay of that program must reproduce the oracle's gate-by-gate state, every
+pass must be a legal tile (contiguous low segment >= 16 bytes, ops on tile
+bits), and fusion must produce the op kinds the kernels specialise on."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def apply_local(psi, M, bits, N):
+    """apply a 2^k x 2^k matrix whose index bit t is global qubit bits[t]"""
+    k = len(bits)
+    t = psi.reshape([2] * N)
+    axes = [N - 1 - b for b in bits]            # C-order axis of index bit b
+    t = np.moveaxis(t, axes[::-1], list(range(k)))  # axis 0 = bits[k-1] (most significant)
+    sh = t.shape
+    t = (M @ t.reshape(1 << k, -1)).reshape(sh)
+    t = np.moveaxis(t, list(range(k)), axes[::-1])
+    return t.reshape(-1)
+
+
+def op_matrix(op):
+    c = op["c"]
+    nq = op["nq"]
+    dim = 1 << nq
+    k = op["kind"]
+    if k == 0:
+        return c[:4].reshape(2, 2)
+    if k == 1:
+        return c[:16].reshape(4, 4)
+    if k == 2:
+        M = np.zeros((4, 4), complex)
+        M[0, 0], M[0, 3], M[3, 0], M[3, 3] = c[0], c[1], c[2], c[3]
+        M[1, 1], M[1, 2], M[2, 1], M[2, 2] = c[4], c[5], c[6], c[7]
+        return M
+    if k == 3:
+        M = np.zeros((dim, dim), complex)
+        for r in range(dim):
+            M[r, op["perm"][r]] = c[r]
+        return M
+    if k == 4:
+        return np.diag(c[:dim])
+    raise AssertionError(k)
+
+
+def replay(plan, N, psi):
+    for p in plan:
+        for op in p["ops"]:
+            psi = apply_local(psi, op_matrix(op), op["gb"][:op["nq"]], N)
+    return psi
+
+
+def check_geometry(plan, N, dtype, tile_bits):
+    import pysmoq as S
+    for p in plan:
+        assert len(p["ops"]) >= 1
+        assert p["T"] <= max(tile_bits, 1) or p["T"] == N
+        assert p["T"] == p["L"] + p["H"]
+        if dtype == S.C64:
+            assert p["L"] >= 1                 # segment >= 16 bytes
+        assert all(p["L"] <= b < N for b in p["hb"]) and p["hb"] == sorted(p["hb"])
+        for op in p["ops"]:
+            for t in range(op["nq"]):
+                g, lb = op["gb"][t], op["lb"][t]
+                if lb >= 0:
+                    assert (lb < p["L"] and g == lb) or (lb >= p["L"] and p["hb"][lb - p["L"]] == g)
+                else:
+                    assert op["kind"] == 4, "only diagonal ops may touch non-tile qubits"
+
+
+def circuit(N, n=None):
+    import pysmoq as S
+    lines = json.load(open(os.path.join(GOLD, "circuits.json")))[str(N)]
+    name = {"H": "h", "X": "x", "Y": "y", "Z": "z", "S": "s", "T": "t", "RX": "rx", "RY": "ry", "RZ": "rz",
+            "CNOT": "cnot", "CZ": "cz"}
+    g, o = [], []
+    for ln in lines[:n]:
+        p = ln.split()
+        t = name[p[0]]
+        qs = [int(p[1]) + 1] + ([int(p[2]) + 1] if t in ("cnot", "cz") else [])
+        a = float(p[2]) if t in ("rx", "ry", "rz") else 0.0
+        g.append(S.gate(t, qs, angle=a))
+        o.append((t, qs, 0, a))
+    return g, o
+
+
+@pytest.mark.parametrize("N", [2, 4, 8, 10, 12])
+@pytest.mark.parametrize("tile_bits,low_bits", [(4, 1), (6, 3), (8, 5), (12, 4), (14, 5)])
+def test_replay_of_fused_plan_matches_oracle(built, N, tile_bits, low_bits):
+    import pysmoq as S
+    g, o = circuit(N, 300)
+    want = O.zero_state(N)
+    O.apply_circuit(want, O.make_ops(o), len(o), np.zeros(1), N)
+    for dtype in (S.C64, S.C128):
+        tb = tile_bits if dtype == S.C64 else min(tile_bits, 13)
+        plan = S.debug_plan(N, g, dtype=dtype, tile_bits=tb, low_bits=low_bits)
+        check_geometry(plan, N, dtype, tb)
+        got = replay(plan, N, O.zero_state(N))
+        assert np.max(np.abs(got - want)) < 1e-12
+
+
+def test_narrow_tiles_are_rejected_not_hung(built):
+    import pysmoq as S
+    g, _ = circuit(10, 50)
+    with pytest.raises(S.SmoqError):
+        S.debug_plan(10, g, dtype=S.C64, tile_bits=3, low_bits=3)
+
+
+def test_xxz_strang_step_fuses_to_parity_ops(built):
+    """A Strang step of the XXZ chain (Rz fields; Rxx, Ryy, Rzz per bond) must
+    fuse every bond into one parity-block op and absorb the fields."""
+    import pysmoq as S
+    N = 16
+    rng = np.random.default_rng(42)
+    h = rng.uniform(-1, 1, size=N)
+    s1 = [S.gate("rz", [i + 1], angle=2 * h[i] * 0.025) for i in range(N)]
+    for i in range(1, N):
+        s1 += [S.gate("rxx", [i, i + 1], angle=0.05), S.gate("ryy", [i, i + 1], angle=0.05),
+               S.gate("rzz", [i, i + 1], angle=0.025)]
+    ops = s1 + s1[::-1]
+    plan = S.debug_plan(N, ops, dtype=S.C64, tile_bits=13, low_bits=5)
+    kinds = [op["kind"] for p in plan for op in p["ops"]]
+    assert set(kinds) <= {2, 4}, kinds
+    assert len(kinds) <= 2 * (N - 1) + 2
+    assert len(plan) <= 3
+    # replay vs the oracle on the same gates
+    o = [(op.type, op.qubits, 0, op.fixed_angle) for op in ops]
+    want = O.zero_state(N, 0b0101010101010101)
+    O.apply_circuit(want, O.make_ops(o), len(o), np.zeros(1), N)
+    got = replay(plan, N, O.zero_state(N, 0b0101010101010101))
+    assert np.max(np.abs(got - want)) < 1e-12
+
+
+def test_diagonal_gates_need_no_tile_membership(built):
+    """Rzz on far-apart qubits is diagonal: it rides along in the low-qubit pass."""
+    import pysmoq as S
+    N = 20
+    ops = [S.gate("rx", [q], angle=0.1 * q) for q in range(1, 9)] + [S.gate("rzz", [1, 20], angle=0.3),
+                                                                    S.gate("cz", [3, 17])]
+    plan = S.debug_plan(N, ops, dtype=S.C64, tile_bits=12, low_bits=5)
+    assert len(plan) == 1
+    assert any(op["kind"] == 4 and -1 in op["lb"][:op["nq"]] for op in plan[0]["ops"])
