@@ -159,6 +159,22 @@ smoq_status smoq_expect_pauli_string(smoq_state* st, int n, const char* ops, con
  * (zmask 0 gives the squared norm); the Z/ZZ part of
  * measure_all_observables_one_pass :1532 */
 smoq_status smoq_expect_zstrings(smoq_state* st, const uint64_t* zmasks, int nobs, double* out);
+/* No counterpart in the reference.  The same diagonal batch as
+ * smoq_expect_zstrings for callers that cannot allocate device memory at
+ * call time (fixed-footprint hosts, callers that already hold most of HBM,
+ * code that must not wait on the allocator, callers without a smoq_ctx):
+ * it allocates nothing.  psi points to batch * 2^N caller-owned device
+ * amplitudes (16-byte aligned), out to batch * nobs caller-owned device
+ * doubles (out[b * nobs + o]); kernels run on `stream` (a cudaStream_t,
+ * NULL = default stream) and the call returns without synchronising.  Limits:
+ * nobs <= 32, batch <= 65535 and batch * nobs <= 65536 (the fixed scratch of
+ * 512 KiB per GPU); larger requests return SMOQ_ERR_BADINPUT with a message
+ * in errbuf (may be NULL).  The first call on each device looks up the
+ * scratch array's device address (make it before any stream capture); calls
+ * that can overlap on one device race on the shared scratch. */
+smoq_status smoq_expect_zstrings_noalloc(const void* psi, int N, smoq_dtype dtype, int batch,
+                                         const uint64_t* zmasks, int nobs, double* out, void* stream,
+                                         char* errbuf, size_t errlen);
 /* population_excited_psi (Gates.jl:784) */
 smoq_status smoq_population_excited(smoq_state* st, int q, double* out);
 /* squared norm per state; get_norm (cpuQuantumStatePreparation.jl:377) is its sqrt */

@@ -113,6 +113,8 @@ _SIGS = {
     "smoq_expect_zz": [_vp, C.c_int, C.c_int, _dp],
     "smoq_expect_pauli_string": [_vp, C.c_int, C.c_char_p, _ip, _dp],
     "smoq_expect_zstrings": [_vp, _u64p, C.c_int, _dp],
+    "smoq_expect_zstrings_noalloc": [_vp, C.c_int, C.c_int, C.c_int, _u64p, C.c_int, _vp, _vp, C.c_char_p,
+                                     C.c_size_t],
     "smoq_population_excited": [_vp, C.c_int, _dp],
     "smoq_norm2": [_vp, _dp],
     "smoq_normalize": [_vp],
