@@ -190,6 +190,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # smaller cases of the same kernel (profiling, sweeps); the defaults are the workload
+    ap.add_argument("--n-qubits", type=int, default=N_QUBITS)
+    ap.add_argument("--trotter-steps", type=int, default=STEPS)
+    ap.add_argument("--tile-bits", type=int, default=0, help="complex64 tile width (0 = library default)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -210,7 +214,12 @@ def main():
     import pysmoq as S
 
     ctx = S.Context(local)
-    N = N_QUBITS
+    if args.tile_bits:
+        ctx.set_option(S._lib.OPT_TILE_BITS_C64, args.tile_bits)
+    N = args.n_qubits
+    tsteps = args.trotter_steps
+    gate_apps = tsteps * 2 * (N + 3 * (N - 1))
+    workload = WORKLOAD if (N, tsteps) == (N_QUBITS, 200) else f"xxz_chain_trotter2_n{N}_c64_{tsteps}steps"
     gl = s1_gates(N, DT / 2)
     gates = [S.FastTrotterGate(idx, U) for idx, U in gl]
     plan = S.TrotterPlan(ctx, N, gates, order=2, dtype=S.C64)
@@ -220,7 +229,7 @@ def main():
 
     def device_step():
         st.set_basis(neel)                      # make_initial_psi on the device
-        return plan.run(st, STEPS, RECORD_EVERY)
+        return plan.run(st, tsteps, RECORD_EVERY)
 
     # e2e input: the initial state in pinned host memory (what a caller holding
     # psi on the host passes), uploaded every step; output: the <Z> records.
@@ -230,7 +239,7 @@ def main():
 
     def e2e_step():
         S.lib.smoq_state_upload(st.h, hp.ctypes.data_as(S._lib.C.c_void_p), hp.nbytes)
-        return plan.run(st, STEPS, RECORD_EVERY)
+        return plan.run(st, tsteps, RECORD_EVERY)
 
     def timed(fn, k):
         if ws > 1:
@@ -285,12 +294,12 @@ def main():
     # e2e through the C ABI with host buffers
     e2e_ms = timed(e2e_step, args.steps)
 
-    per_rank_apps = GATE_APPS * args.steps
+    per_rank_apps = gate_apps * args.steps
     value = ws * per_rank_apps / (ms * 1e-3)
     e2e_value = ws * per_rank_apps / (e2e_ms * 1e-3)
 
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and N == N_QUBITS:
         r, t = cpu_baseline_sample(12)
         cpu = {"value": r, "unit": "gate-apps/s", "cores": 1, "kind": "port",
                "sample": f"first 12 of the 218 gate applications of one Strang step at N=28, complex128, "
@@ -301,8 +310,9 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
                 "data": "synthetic",
-                "config": {"workload": WORKLOAD, "N": N, "dt": DT, "trotter_steps": STEPS,
-                           "record_every": RECORD_EVERY, "gate_apps_per_step": GATE_APPS,
+                "config": {"workload": workload, "N": N, "dt": DT, "trotter_steps": tsteps,
+                           "tile_bits_c64": args.tile_bits or 13,
+                           "record_every": RECORD_EVERY, "gate_apps_per_step": gate_apps,
                            "state_bytes": (1 << N) * 8, "l2_policy": "inputs larger than L2 (2 GiB state)",
                            "parallelism": "replicas" if ws > 1 else "single_gpu",
                            "tile_passes_per_step": passes, "hbm_gbs_effective":
@@ -313,7 +323,7 @@ def main():
                              "algorithmic_bytes_per_launch": bytes_per_launch},
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": "gate-apps/s", "h2d_bytes_per_step": int(hp.nbytes),
-                        "d2h_bytes_per_step": int(8 * N * (STEPS // RECORD_EVERY + 1))},
+                        "d2h_bytes_per_step": int(8 * N * (tsteps // RECORD_EVERY + 1))},
                 "gpu_launches": int(launches),
                 "clocks": clk}
         print(json.dumps(line))

@@ -57,7 +57,8 @@ enum {
     SMOQ_OPT_LOW_BITS_C64 = 3,    /* minimum contiguous low qubits per tile segment */
     SMOQ_OPT_LOW_BITS_C128 = 4,
     SMOQ_OPT_USE_GRAPHS = 5,      /* capture Trotter blocks as CUDA graphs (default 1) */
-    SMOQ_OPT_KERNEL_TIMING = 6    /* bracket fused passes with CUDA events (default 0) */
+    SMOQ_OPT_KERNEL_TIMING = 6,   /* bracket fused passes with CUDA events (default 0) */
+    SMOQ_OPT_ENGINE = 7           /* fused-pass engine: 0 shared-memory sweeps (default), 1 register tiles */
 };
 smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long value);
 /* launches: kernels launched by this context; tile_passes/tile_ms/tile_bytes:
@@ -256,7 +257,8 @@ smoq_status smoq_energy(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* o
  * no GPU or context needed) on a gate sequence exactly as
  * smoq_apply_sequence would and reports, per pass, the tile geometry and the
  * fused ops (kind = 0 dense 2x2, 1 dense 4x4, 2 parity 4x4, 3 monomial,
- * 4 diagonal; coefficients as the kernels read them).  Counts are written
+ * 4 diagonal, 8 register-tile layout change; coefficients as the kernels read
+ * them), scheduled for the default register-tile engine.  Counts are written
  * even when the output arrays are too small (NULL arrays allowed). */
 typedef struct {
     int32_t T, L, H, nops;
@@ -265,7 +267,9 @@ typedef struct {
 typedef struct {
     int32_t kind, nq;
     int32_t lb[4], gb[4];
-    int32_t perm[8];
+    int32_t perm[8];       /* monomial permutation; kind 8 (register layout): register / warp bits */
+    int32_t slot[4];       /* register-tile placement of each qubit: type << 8 | index */
+    int32_t mode;          /* 1 = applied through shared memory */
     double c[32];          /* 16 interleaved complex coefficients */
 } smoq_fused_op_info;
 smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops,

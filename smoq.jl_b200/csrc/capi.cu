@@ -86,6 +86,17 @@ static int low_bits(smoq_ctx* ctx, int dtype) {
     return dtype == SMOQ_C64 ? ctx->low_bits_c64 : ctx->low_bits_c128;
 }
 
+// plan a gate list into fused passes; with the register engine every pass
+// wide enough for it gets a register-tile schedule
+static std::vector<Pass> plan_for(int engine, const std::vector<GateIR>& ir, int N, int dtype, int tbits, int lbits,
+                                  int epilogue_special = -1) {
+    std::vector<Pass> pl = plan_passes(ir, N, tbits, lbits, epilogue_special, dtype == SMOQ_C64 ? 1 : 0);
+    if (engine == 1)
+        for (Pass& p : pl)
+            if (p.g.T >= RT_MIN_T && p.g.T - RT_MIN_T <= (dtype == SMOQ_C64 ? 5 : 4)) schedule_regtile(p);
+    return pl;
+}
+
 // ------------------------------------------------------------ pass runner
 namespace {
 struct DevProgram {
@@ -177,6 +188,7 @@ smoq_status smoq_ctx_create(int device, smoq_ctx** out) {
     if (cudaMalloc(&ctx->d_err, sizeof(int32_t)) != cudaSuccess) return SMOQ_ERR_OOM;
     if (cudaMemset(ctx->d_err, 0, sizeof(int32_t)) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (tile_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
+    if (regtile_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (ensure_scratch(ctx.get(), 1 << 17) != SMOQ_OK) return SMOQ_ERR_OOM;
     if (ensure_pinned(ctx.get(), 1 << 20) != SMOQ_OK) return SMOQ_ERR_OOM;
     *out = ctx.release();
@@ -225,6 +237,10 @@ smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long v) {
             break;
         case SMOQ_OPT_USE_GRAPHS: ctx->use_graphs = v != 0; break;
         case SMOQ_OPT_KERNEL_TIMING: ctx->kernel_timing = v != 0; break;
+        case SMOQ_OPT_ENGINE:
+            if (v != 0 && v != 1) return fail(ctx, SMOQ_ERR_BADINPUT, "engine must be 0 or 1");
+            ctx->engine = (int)v;
+            break;
         default: return fail(ctx, SMOQ_ERR_BADINPUT, "unknown option");
     }
     return SMOQ_OK;
@@ -502,8 +518,7 @@ smoq_status smoq_apply_sequence(smoq_state* st, const smoq_op* ops, int n, const
     if (smoq_status s = ops_to_ir(st, st->N, ops, n, theta, ir)) return s;
     DevProgram P;
     try {
-        P.passes = plan_passes(ir, st->N, tile_bits(ctx, st->dtype), low_bits(ctx, st->dtype), -1,
-                               st->dtype == SMOQ_C64 ? 1 : 0);
+        P.passes = plan_for(ctx->engine, ir, st->N, st->dtype, tile_bits(ctx, st->dtype), low_bits(ctx, st->dtype));
     } catch (const std::exception& ex) {
         return fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
     }
@@ -526,7 +541,7 @@ smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tbits, int lbi
     if (smoq_status s = ops_to_ir(nullptr, N, ops, n, theta, ir)) return s;
     std::vector<Pass> pl;
     try {
-        pl = plan_passes(ir, N, tbits, lbits, -1, dtype == SMOQ_C64 ? 1 : 0);
+        pl = plan_for(1, ir, N, dtype, tbits, lbits);
     } catch (const std::exception&) {
         return SMOQ_ERR_BADINPUT;
     }
@@ -553,6 +568,8 @@ smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tbits, int lbi
                     fi.gb[t] = op.gb[t];
                 }
                 for (int r = 0; r < 8; ++r) fi.perm[r] = op.perm[r];
+                for (int t = 0; t < 4; ++t) fi.slot[t] = op.slot[t];
+                fi.mode = op.mode;
                 for (int k = 0; k < 16; ++k) {
                     fi.c[2 * k] = op.cd[k].x;
                     fi.c[2 * k + 1] = op.cd[k].y;
@@ -739,8 +756,8 @@ static smoq_status get_block(smoq_plan* P, int nsteps, smoq_plan::Block** out) {
     all.reserve(P->step.size() * nsteps);
     for (int s = 0; s < nsteps; ++s) all.insert(all.end(), P->step.begin(), P->step.end());
     try {
-        B->prog.passes = plan_passes(all, P->N, tile_bits(P->ctx, P->dtype), low_bits(P->ctx, P->dtype), -1,
-                                     P->dtype == SMOQ_C64 ? 1 : 0);
+        B->prog.passes = plan_for(P->ctx->engine, all, P->N, P->dtype, tile_bits(P->ctx, P->dtype),
+                                  low_bits(P->ctx, P->dtype));
     } catch (const std::exception& ex) {
         return fail(P->ctx, SMOQ_ERR_BADINPUT, ex.what());
     }

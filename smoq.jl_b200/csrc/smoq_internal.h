@@ -32,13 +32,22 @@ enum OpKind : int32_t {
     OPK_STATESCALE = 5,  // amp *= scale[b] (per state, real, from aux pointer)
     OPK_REALTAB = 6,  // amp *= prod_j tab[j][byte j of global index] (real factors)
     OPK_JUMP = 7,     // per-state jump (sigma-/sigma+/sigma_z/sigma_x) from aux list
+    OPK_LAYOUT = 8,   // register-tile layout change: perm[0..KR-1] = register bits,
+                      // perm[5..7] = warp bits (tile-local bit positions)
 };
+
+// Placement of an op qubit in the register-tile engine: slot = type << 8 | index
+enum SlotType : int32_t { SLOT_LANE = 0, SLOT_REG = 1, SLOT_WARP = 2, SLOT_OFF = 3 };
 
 struct alignas(16) DevOp {
     int32_t kind;
     int32_t nq;         // 1..3 qubits (OPK_DIAG: 0..4)
     int32_t lb[4];      // tile-local bit of qubit t, -1 when the qubit is not a tile bit
     int32_t gb[4];      // global bit of qubit t
+    int32_t slot[4];    // register-tile placement of qubit t (SlotType << 8 | index)
+    int32_t mode;       // register-tile engine: 0 = in registers, 1 = through shared memory
+    int32_t flags;      // OPK_PARITY2: bit 0 even block diagonal, bit 1 odd block diagonal
+    int32_t pad0[2];
     int32_t perm[8];    // OPK_MONO: out[r] = ph[r] * in[perm[r]]
     const void* aux;    // OPK_STATESCALE: const double* scale[B]; OPK_REALTAB: const double* tabs
     int64_t aux2;       // OPK_REALTAB: number of byte tables
@@ -93,11 +102,21 @@ struct Pass {
     TileGeom g;
     std::vector<DevOp> ops;
     bool epilogue = false;
+    bool regtile = false;   // scheduled for the register-tile engine (ops[0] is OPK_LAYOUT)
 };
+
+// register-tile engine geometry: 256 threads = 8 warps x 32 lanes; lanes hold
+// tile-local bits 0..4, 3 warp bits, KR = T - 8 register bits per thread
+constexpr int RT_THREADS = 256;
+constexpr int RT_LANE_BITS = 5;
+constexpr int RT_WARP_BITS = 3;
+constexpr int RT_MIN_T = 8;
 
 // planner.cpp
 std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, int Lmin,
                               int epilogue_after_special = -1, int Lreq = 0);
+// turn a planned pass into a register-tile program (layout ops + slots)
+void schedule_regtile(Pass& p);
 void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op);
 
 // gate library (planner.cpp)
@@ -124,6 +143,8 @@ struct smoq_ctx {
     int low_bits_c64 = 5;
     int low_bits_c128 = 4;
     int use_graphs = 1;
+    int engine = 0;                    // fused passes: 0 = shared-memory sweeps, 1 = register tiles
+    int rt_occ[2][2][8] = {};          // CTAs per SM of the register-tile kernel [dtype][epilogue][KR]
     int kernel_timing = 0;             // bracket tile passes with events
     long long launches = 0;            // kernels launched by this ctx
     long long tile_passes = 0;
@@ -159,4 +180,6 @@ cudaError_t launch_convert(smoq_state* dst, smoq_state* src);
 size_t diag_reduce_scratch_doubles(smoq_state* st, int nobs);
 size_t tile_max_smem(int amp_bytes, int T);
 cudaError_t tile_kernels_init(smoq_ctx* ctx);
+cudaError_t regtile_kernels_init(smoq_ctx* ctx);
+cudaError_t launch_regtile(smoq_ctx* ctx, const TileArgs& a, int dtype, bool epi);
 }  // namespace smoq

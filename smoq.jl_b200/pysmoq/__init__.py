@@ -658,6 +658,7 @@ def debug_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtype: int =
             f = F[k]
             k += 1
             d["ops"].append({"kind": f.kind, "nq": f.nq, "lb": list(f.lb), "gb": list(f.gb), "perm": list(f.perm),
+                             "slot": list(f.slot), "mode": f.mode,
                              "c": np.array(f.c[:]).view(np.complex128).copy()})
         out.append(d)
     return out

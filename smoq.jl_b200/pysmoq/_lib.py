@@ -18,7 +18,8 @@ C64, C128 = 0, 1
 (G_RX, G_RY, G_RZ, G_H, G_X, G_Y, G_Z, G_S, G_SDG, G_T, G_TDG, G_CZ, G_CNOT, G_RXX, G_RYY, G_RZZ,
  G_CRY, G_CCZ, G_TOFFOLI, G_U1, G_U2) = range(21)
 
-OPT_TILE_BITS_C64, OPT_TILE_BITS_C128, OPT_LOW_BITS_C64, OPT_LOW_BITS_C128, OPT_USE_GRAPHS, OPT_KERNEL_TIMING = range(1, 7)
+(OPT_TILE_BITS_C64, OPT_TILE_BITS_C128, OPT_LOW_BITS_C64, OPT_LOW_BITS_C128, OPT_USE_GRAPHS, OPT_KERNEL_TIMING,
+ OPT_ENGINE) = range(1, 8)
 
 
 class SmoqOp(C.Structure):
@@ -44,7 +45,7 @@ class SmoqPassInfo(C.Structure):
 
 class SmoqFusedOpInfo(C.Structure):
     _fields_ = [("kind", C.c_int32), ("nq", C.c_int32), ("lb", C.c_int32 * 4), ("gb", C.c_int32 * 4),
-                ("perm", C.c_int32 * 8), ("c", C.c_double * 32)]
+                ("perm", C.c_int32 * 8), ("slot", C.c_int32 * 4), ("mode", C.c_int32), ("c", C.c_double * 32)]
 
 
 class SmoqError(RuntimeError):

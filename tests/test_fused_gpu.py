@@ -72,6 +72,32 @@ def test_tile_width_variations(ctx, tile_bits):
         ctx.set_option(S._lib.OPT_LOW_BITS_C128, 4)
 
 
+@pytest.mark.parametrize("engine", [0, 1])
+@pytest.mark.parametrize("N,tile_bits", [(9, 8), (12, 9), (16, 10), (18, 13), (20, 11)])
+def test_both_engines_and_register_widths(ctx, engine, N, tile_bits):
+    """shared-memory sweeps (engine 0) and register tiles (engine 1, every register
+    width KR = tile_bits - 8) give the oracle's state on a benchmark circuit"""
+    lines = json.load(open(os.path.join(GOLD, "circuits.json")))[str(N - N % 2)]
+    g_ops, o_ops = circuit_ops(lines[:600])
+    g_ops = [op for op in g_ops if max(op.qubits) <= N]
+    o_ops = [op for op in o_ops if max(op[1]) <= N]
+    want = O.zero_state(N)
+    O.apply_circuit(want, O.make_ops(o_ops), len(o_ops), np.zeros(1), N)
+    ctx.set_option(S._lib.OPT_ENGINE, engine)
+    try:
+        for dtype, tol, opt, default in ((S.C128, 1e-12, S._lib.OPT_TILE_BITS_C128, 12),
+                                         (S.C64, 5e-5, S._lib.OPT_TILE_BITS_C64, 13)):
+            ctx.set_option(opt, min(tile_bits, 13 if dtype == S.C64 else 12))
+            try:
+                st = S.CuState(ctx, N, dtype)
+                S.apply_circuit(st, S.ParameterizedCircuit(N, g_ops), np.zeros(1))
+                assert rel(st.download().astype(complex), want) < tol, (engine, N, tile_bits, dtype)
+            finally:
+                ctx.set_option(opt, default)
+    finally:
+        ctx.set_option(S._lib.OPT_ENGINE, 0)
+
+
 def hea_ops(N, L, theta_seed=42):
     """10 layers of [Ry all; Rz all; CZ ladder], gate-major params (Builder.jl:341-346)"""
     ops, idx = [], 1
