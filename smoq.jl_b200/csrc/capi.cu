@@ -967,3 +967,54 @@ smoq_status smoq_trotter_run(smoq_plan* P, smoq_state* st, int steps, int record
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------
+// Internal entry points shared with the other translation units (MCWF, VQE).
+// ------------------------------------------------------------------------
+smoq_status smoq_internal_fail(smoq_ctx* ctx, smoq_status s, const char* msg) { return fail(ctx, s, msg); }
+smoq_status smoq_internal_cuda(smoq_ctx* ctx, cudaError_t e, const char* where) { return cuda_fail(ctx, e, where); }
+
+smoq_status smoq_internal_plan_step(smoq_plan* plan, std::vector<GateIR>& out, int& N, int& dtype, int& order) {
+    out = plan->step;
+    N = plan->N;
+    dtype = plan->dtype;
+    order = plan->order;
+    return SMOQ_OK;
+}
+
+// plan + upload a gate program for `st` (no launch); the handle owns it
+smoq_status smoq_internal_prepare(smoq_ctx* ctx, smoq_state* st, const std::vector<GateIR>& gates,
+                                  int epilogue_special, void** handle) {
+    std::unique_ptr<DevProgram> P(new DevProgram());
+    try {
+        P->passes = plan_for(ctx->engine, gates, st->N, st->dtype, tile_bits(ctx, st->dtype),
+                             low_bits(ctx, st->dtype), epilogue_special);
+    } catch (const std::exception& ex) {
+        return fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
+    }
+    if (smoq_status s = upload_program(ctx, *P)) return s;
+    *handle = P.release();
+    return SMOQ_OK;
+}
+
+smoq_status smoq_internal_rerun(smoq_ctx* ctx, smoq_state* st, void* handle, const Epilogue* ep) {
+    return run_program(ctx, st, *(DevProgram*)handle, ep, nullptr);
+}
+
+void smoq_internal_free_prog(void* handle) { delete (DevProgram*)handle; }
+
+// tiles per state of the pass that carries the epilogue (else of the last pass)
+int64_t smoq_internal_tiles_per_state(void* handle) {
+    const DevProgram* P = (const DevProgram*)handle;
+    for (const Pass& p : P->passes)
+        if (p.epilogue) return (int64_t)1 << (p.g.N - p.g.T);
+    return P->passes.empty() ? 1 : (int64_t)1 << (P->passes.back().g.N - P->passes.back().g.T);
+}
+
+// up to 32 Z-string sums of every state into d_out[b * nobs + o] (device)
+smoq_status smoq_internal_zreduce(smoq_ctx* ctx, smoq_state* st, const uint64_t* zmasks, int nobs, double* d_out) {
+    if (nobs < 1 || nobs > 32) return fail(ctx, SMOQ_ERR_BADINPUT, "at most 32 observables per reduction");
+    if (smoq_status s = ensure_scratch(ctx, diag_reduce_scratch_doubles(st, nobs))) return s;
+    CK(ctx, launch_diag_reduce(ctx, st, zmasks, nobs, d_out));
+    return SMOQ_OK;
+}

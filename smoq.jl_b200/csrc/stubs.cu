@@ -1,11 +1,6 @@
 // stubs.cu -- entry points whose implementation is not built yet.
 #include "smoq_internal.h"
 extern "C" {
-smoq_status smoq_mcwf_run(smoq_plan*, smoq_state* st, const smoq_jump_op*, int, double, uint64_t, uint64_t, int, int,
-                          double*, double*, double*, double*, int*) {
-    if (st && st->ctx) st->ctx->last_error = "smoq_mcwf_run: not implemented";
-    return SMOQ_ERR_UNSUPPORTED;
-}
 smoq_status smoq_energy_grad(smoq_ctx* ctx, int, smoq_dtype, const smoq_op*, int, int, const smoq_pauli_term*, int,
                              int, const double*, double*, double*) {
     if (ctx) ctx->last_error = "smoq_energy_grad: not implemented";
