@@ -1018,3 +1018,9 @@ smoq_status smoq_internal_zreduce(smoq_ctx* ctx, smoq_state* st, const uint64_t*
     CK(ctx, launch_diag_reduce(ctx, st, zmasks, nobs, d_out));
     return SMOQ_OK;
 }
+
+smoq_status smoq_internal_ops_to_ir(int N, const smoq_op* ops, int n, const double* theta, std::vector<GateIR>& out) {
+    return ops_to_ir(nullptr, N, ops, n, theta, out);
+}
+int smoq_internal_tile_bits(smoq_ctx* ctx, int dtype) { return tile_bits(ctx, dtype); }
+int smoq_internal_low_bits(smoq_ctx* ctx, int dtype) { return low_bits(ctx, dtype); }

@@ -233,6 +233,18 @@ void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op) {
         op.gb[t] = 0;
     }
     for (int r = 0; r < 8; ++r) op.perm[r] = r;
+    if (gt.special == OPK_INNER) {
+        // generator G as a dense row-major matrix on the op's qubits
+        op.kind = OPK_INNER;
+        op.nq = gt.nq;
+        for (int t = 0; t < gt.nq; ++t) {
+            op.gb[t] = gt.q[t];
+            op.lb[t] = local_bit(g, gt.q[t]);
+        }
+        fill_coeffs(op, gt.m, 1 << (2 * gt.nq));
+        op.perm[0] = (int32_t)gt.aux2;  // slot in the pass's partials (set by the caller)
+        return;
+    }
     if (gt.special) {
         op.kind = gt.special;
         op.aux = gt.aux;
@@ -351,6 +363,8 @@ struct Fuser {
     void add(const GateIR& gt) {
         if (gt.special) {
             if (gt.special == OPK_REALTAB) flush_all();  // diagonal over every qubit
+            if (gt.special == OPK_INNER)                 // measures the state as it is at this point
+                for (int t = 0; t < gt.nq; ++t) flush(gt.q[t]);
             ops.push_back(gt);
             touch((int)ops.size() - 1);
             return;
@@ -434,7 +448,8 @@ std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, in
             uint64_t qm = 0;
             if (gt.special == OPK_REALTAB) qm = allq;
             for (int t = 0; t < gt.nq; ++t) qm |= 1ull << gt.q[t];
-            if (gt.diag || gt.special) {
+            // an inner-product op needs its generator's qubits in the tile, like a gate
+            if (gt.diag || (gt.special && gt.special != OPK_INNER)) {
                 if ((qm & hard) == 0) taken.push_back(idx);
                 else { soft |= qm; rest.push_back(idx); }
             } else {

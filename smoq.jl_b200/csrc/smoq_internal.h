@@ -32,6 +32,8 @@ enum OpKind : int32_t {
     OPK_STATESCALE = 5,  // amp *= scale[b] (per state, real, from aux pointer)
     OPK_REALTAB = 6,  // amp *= prod_j tab[j][byte j of global index] (real factors)
     OPK_JUMP = 7,     // per-state jump (sigma-/sigma+/sigma_z/sigma_x) from aux list
+    OPK_INNER = 9,    // adjoint sweep: per-tile Im<lambda|G|phi> with G = cd (dense, 1-2
+                      // qubits), written to partials slot perm[0] of the pass
     OPK_LAYOUT = 8,   // register-tile layout change: perm[0..KR-1] = register bits,
                       // perm[5..7] = warp bits (tile-local bit positions)
 };

@@ -1,0 +1,488 @@
+// vqe.cu -- VQE energy and adjoint gradient.
+//
+// E(theta) = <phi|H|phi>, phi = U_P ... U_1 |0>, H = sum_t c_t P_t (Pauli strings).
+// For a rotation U_k = exp(-i theta G_k / 2) (RX/RY/RZ/RXX/RYY/RZZ, and CRY
+// with G = |1><1| (x) Y), dE/dtheta_k = Im <lambda_k| G_k |phi_k>, where
+// phi_k = U_k ... U_1 |0> and lambda_k = U_{k+1}^dag ... U_P^dag H phi.
+// The gradient therefore needs one forward sweep, one application of H and
+// ONE backward sweep that carries the pair (phi, lambda): walking the gates
+// in reverse, measure Im<lambda|G|phi> at a parameterised gate, then apply
+// U_k^dag to both.  Nothing is stored per layer (the gates are unitary and
+// are uncomputed), so memory is three states whatever the depth.
+//
+//  * ham_apply_kernel: lambda = H phi and the energy partials in one read of
+//    phi per term;
+//  * adj_tile_kernel: the backward sweep as fused passes over (phi, lambda)
+//    tile pairs: both tiles come into shared memory by bulk copy, the pass's
+//    program (U^dag ops and OPK_INNER measurements, in order) runs on both,
+//    every OPK_INNER writes its FP64 per-tile partial.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <vector>
+#include "smoq_internal.h"
+#include "k_common.cuh"
+
+namespace smoq {
+
+struct HamTerm {
+    double coef;
+    uint64_t x, z;
+    int32_t ny;
+    int32_t pad;
+};
+
+// lambda_k = sum_t c_t i^{ny} (-1)^{popc((k ^ x) & z)} phi_{k ^ x}; partial
+// sums of conj(phi_k) lambda_k (real part) per block
+template <typename R>
+__global__ void __launch_bounds__(256) ham_apply_kernel(const typename CT<R>::T* phi, typename CT<R>::T* lam, int N,
+                                                        const HamTerm* terms, int nterms, double* partials) {
+    using C = typename CT<R>::T;
+    const int64_t len = (int64_t)1 << N;
+    double acc = 0;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < len; k += (int64_t)gridDim.x * blockDim.x) {
+        double lr = 0, li = 0;
+        for (int t = 0; t < nterms; ++t) {
+            const uint64_t j = (uint64_t)k ^ terms[t].x;
+            const C p = phi[j];
+            double s = terms[t].coef * ((__popcll(j & terms[t].z) & 1) ? -1.0 : 1.0);
+            const int yk = terms[t].ny & 3;
+            double pr = p.x, pi = p.y;
+            // multiply by i^yk
+            if (yk == 1) { const double tr = -pi; pi = pr; pr = tr; }
+            else if (yk == 2) { pr = -pr; pi = -pi; }
+            else if (yk == 3) { const double tr = pi; pi = -pr; pr = tr; }
+            lr += s * pr;
+            li += s * pi;
+        }
+        C o;
+        o.x = (R)lr;
+        o.y = (R)li;
+        lam[k] = o;
+        const C f = phi[k];
+        acc += (double)f.x * lr + (double)f.y * li;  // Re(conj(phi) lambda)
+    }
+    __shared__ double red[8];
+    for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, d);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        partials[blockIdx.x] = s;
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void adj_diag(const DevOp& op, typename CT<R>::T* tile, uint32_t amps, uint64_t base) {
+    int sh[4] = {-1, -1, -1, -1};
+    int cm = 0;
+    for (int t = 0; t < op.nq; ++t) {
+        if (op.lb[t] >= 0) sh[t] = op.lb[t];
+        else cm |= (int)((base >> op.gb[t]) & 1) << t;
+    }
+    for (uint32_t j = threadIdx.x; j < amps; j += blockDim.x) {
+        int m = cm;
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+            if (sh[t] >= 0) m |= (int)((j >> sh[t]) & 1) << t;
+        tile[j] = cmul(coef<R>(op, m), tile[j]);
+    }
+}
+
+// Im sum_i conj(lam_i) (G phi)_i over the tile, G dense on 1 or 2 tile bits
+template <typename R>
+__device__ __forceinline__ double adj_inner(const DevOp& op, const typename CT<R>::T* P,
+                                            const typename CT<R>::T* L, int T) {
+    using C = typename CT<R>::T;
+    double acc = 0;
+    if (op.nq == 1) {
+        const int a = op.lb[0];
+        const C g00 = coef<R>(op, 0), g01 = coef<R>(op, 1), g10 = coef<R>(op, 2), g11 = coef<R>(op, 3);
+        for (uint32_t g = threadIdx.x; g < (1u << (T - 1)); g += blockDim.x) {
+            const uint32_t i0 = ins0<uint32_t>(g, a), i1 = i0 | (1u << a);
+            const C p0 = P[i0], p1 = P[i1], l0 = L[i0], l1 = L[i1];
+            const C q0 = cfma(g00, p0, cmul(g01, p1)), q1 = cfma(g10, p0, cmul(g11, p1));
+            acc += (double)l0.x * q0.y - (double)l0.y * q0.x + (double)l1.x * q1.y - (double)l1.y * q1.x;
+        }
+    } else {
+        const int a = op.lb[0], b = op.lb[1];
+        const int lo = a < b ? a : b, hi = a < b ? b : a;
+        C G[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) G[k] = coef<R>(op, k);
+        for (uint32_t g = threadIdx.x; g < (1u << (T - 2)); g += blockDim.x) {
+            const uint32_t i0 = ins0<uint32_t>(ins0<uint32_t>(g, lo), hi);
+            const uint32_t ix[4] = {i0, i0 | (1u << a), i0 | (1u << b), i0 | (1u << a) | (1u << b)};
+            C p[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) p[k] = P[ix[k]];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                C q = cmul(G[4 * r], p[0]);
+                q = cfma(G[4 * r + 1], p[1], q);
+                q = cfma(G[4 * r + 2], p[2], q);
+                q = cfma(G[4 * r + 3], p[3], q);
+                const C l = L[ix[r]];
+                acc += (double)l.x * q.y - (double)l.y * q.x;
+            }
+        }
+    }
+    return acc;
+}
+
+struct AdjArgs {
+    TileArgs a;      // a.psi = phi
+    void* lam;
+    double* partials;
+    int32_t n_inner;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) adj_tile_kernel(const AdjArgs A) {
+    using C = typename CT<R>::T;
+    const TileArgs& a = A.a;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int T = a.g.T, L = a.g.L, H = a.g.H;
+    const uint32_t amps = 1u << T;
+    C* tP = reinterpret_cast<C*>(smem_raw);
+    C* tL = tP + amps;
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ double red[8];
+    const int tid = threadIdx.x;
+    const uint32_t nseg = 1u << H;
+    const uint32_t seg_bytes = (uint32_t)sizeof(C) << L;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    for (int64_t t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+        uint64_t base = (uint64_t)t << L;
+        for (int m = 0; m < H; ++m) base = ins0<uint64_t>(base, a.g.hb[m]);
+        C* gP = reinterpret_cast<C*>(a.psi);
+        C* gL = reinterpret_cast<C*>(A.lam);
+        if (tid == 0) mbar_arrive_expect_tx(&bar, 2u * amps * (uint32_t)sizeof(C));
+        for (uint32_t s = tid; s < 2 * nseg; s += blockDim.x) {
+            const uint32_t sg = s < nseg ? s : s - nseg;
+            uint64_t off = base;
+            for (int m = 0; m < H; ++m) off |= (uint64_t)((sg >> m) & 1) << a.g.hb[m];
+            if (s < nseg) bulk_g2s(tP + ((size_t)sg << L), gP + off, seg_bytes, &bar);
+            else bulk_g2s(tL + ((size_t)sg << L), gL + off, seg_bytes, &bar);
+        }
+        const bool ok = mbar_wait_bounded(&bar, phase, a.err);
+        if (!__syncthreads_and(ok)) {
+            mbar_wait_bounded(&bar, phase, nullptr);
+            return;
+        }
+        phase ^= 1;
+        for (int o = 0; o < a.nops; ++o) {
+            const DevOp& op = a.ops[o];
+            if (op.kind == OPK_INNER) {
+                double x = adj_inner<R>(op, tP, tL, T);
+                for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
+                if ((tid & 31) == 0) red[tid >> 5] = x;
+                __syncthreads();
+                if (tid == 0) {
+                    double s = 0;
+                    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+                    A.partials[(size_t)t * A.n_inner + op.perm[0]] = s;
+                }
+            } else if (op.kind == OPK_DIAG) {
+                adj_diag<R>(op, tP, amps, base);
+                adj_diag<R>(op, tL, amps, base);
+            } else {
+                sweep_op<R, uint32_t>(op, tP, T, op.lb, (uint32_t)tid, (uint32_t)blockDim.x);
+                sweep_op<R, uint32_t>(op, tL, T, op.lb, (uint32_t)tid, (uint32_t)blockDim.x);
+            }
+            __syncthreads();
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+        for (uint32_t s = tid; s < 2 * nseg; s += blockDim.x) {
+            const uint32_t sg = s < nseg ? s : s - nseg;
+            uint64_t off = base;
+            for (int m = 0; m < H; ++m) off |= (uint64_t)((sg >> m) & 1) << a.g.hb[m];
+            if (s < nseg) bulk_s2g(gP + off, tP + ((size_t)sg << L), seg_bytes);
+            else bulk_s2g(gL + off, tL + ((size_t)sg << L), seg_bytes);
+        }
+        bulk_commit();
+        bulk_wait_read0();
+        __syncthreads();
+    }
+    bulk_wait0();
+}
+
+}  // namespace smoq
+
+using namespace smoq;
+
+smoq_status smoq_internal_fail(smoq_ctx* ctx, smoq_status s, const char* msg);
+smoq_status smoq_internal_cuda(smoq_ctx* ctx, cudaError_t e, const char* where);
+smoq_status smoq_internal_ops_to_ir(int N, const smoq_op* ops, int n, const double* theta, std::vector<GateIR>& out);
+smoq_status smoq_internal_prepare(smoq_ctx* ctx, smoq_state* st, const std::vector<GateIR>& gates,
+                                  int epilogue_special, void** prog_handle);
+smoq_status smoq_internal_rerun(smoq_ctx* ctx, smoq_state* st, void* prog_handle, const Epilogue* ep);
+void smoq_internal_free_prog(void* prog_handle);
+int smoq_internal_tile_bits(smoq_ctx* ctx, int dtype);
+int smoq_internal_low_bits(smoq_ctx* ctx, int dtype);
+
+#define VCK(call)                                                         \
+    do {                                                                  \
+        cudaError_t e_ = (call);                                          \
+        if (e_ != cudaSuccess) return smoq_internal_cuda(ctx, e_, #call); \
+    } while (0)
+
+namespace {
+
+// generator G of a parameterised gate, as a dense matrix on the gate's qubits
+// (index bit t = the gate's qubit t); false if the gate type has no generator
+bool generator(int type, GateIR& g) {
+    const cd I(0.0, 1.0);
+    const int dim = g.nq == 1 ? 2 : 4;
+    for (int k = 0; k < dim * dim; ++k) g.m[k] = 0.0;
+    switch (type) {
+        case SMOQ_G_RX: g.m[1] = 1; g.m[2] = 1; return true;
+        case SMOQ_G_RY: g.m[1] = -I; g.m[2] = I; return true;
+        case SMOQ_G_RZ: g.m[0] = 1; g.m[3] = -1; return true;
+        case SMOQ_G_RXX:
+            for (int m = 0; m < 4; ++m) g.m[m * 4 + (m ^ 3)] = 1;
+            return true;
+        case SMOQ_G_RYY:
+            g.m[0 * 4 + 3] = -1; g.m[3 * 4 + 0] = -1; g.m[1 * 4 + 2] = 1; g.m[2 * 4 + 1] = 1;
+            return true;
+        case SMOQ_G_RZZ:
+            g.m[0] = 1; g.m[5] = -1; g.m[10] = -1; g.m[15] = 1;
+            return true;
+        case SMOQ_G_CRY:  // |1><1| on the control (bit 0) times Y on the target (bit 1)
+            g.m[1 * 4 + 3] = -I; g.m[3 * 4 + 1] = I;
+            return true;
+        default: return false;
+    }
+}
+
+GateIR dagger(const GateIR& g) {
+    GateIR d = g;
+    const int dim = 1 << g.nq;
+    for (int r = 0; r < dim; ++r)
+        for (int c = 0; c < dim; ++c) d.m[r * dim + c] = std::conj(g.m[c * dim + r]);
+    return d;
+}
+
+struct Work {
+    smoq_state phi, lam;
+    std::vector<void*> owned;
+    cudaStream_t s;
+    ~Work() {
+        for (void* p : owned) cudaFreeAsync(p, s);
+    }
+};
+
+}  // namespace
+
+static smoq_status check_vqe_args(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* ops, int n, int n_params,
+                                  const smoq_pauli_term* H, int nterms, int batch, const double* theta) {
+    if (!ctx) return SMOQ_ERR_BADINPUT;
+    if (N < 1 || N > 34) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "N must be in 1..34");
+    if (dtype != SMOQ_C64 && dtype != SMOQ_C128) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "bad dtype");
+    if (n < 0 || (n > 0 && !ops) || n_params < 0 || (n_params > 0 && !theta) || nterms < 1 || !H || batch < 1)
+        return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "bad VQE arguments");
+    const uint64_t lim = (1ull << N) - 1;
+    for (int t = 0; t < nterms; ++t)
+        if ((H[t].xmask | H[t].zmask) & ~lim)
+            return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "Hamiltonian term acts beyond N");
+    for (int i = 0; i < n; ++i)
+        if (ops[i].param >= n_params) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "op param index >= n_params");
+    return SMOQ_OK;
+}
+
+// forward state into w.phi, lambda = H phi into w.lam; returns E
+static smoq_status forward_and_h(smoq_ctx* ctx, Work& w, const std::vector<GateIR>& ir, const std::vector<HamTerm>& ht,
+                                 HamTerm* d_terms, double* d_epart, int eblocks, double* E) {
+    VCK(launch_set_basis(&w.phi, 0));
+    if (!ir.empty()) {
+        void* h = nullptr;
+        if (smoq_status s = smoq_internal_prepare(ctx, &w.phi, ir, -1, &h)) return s;
+        std::unique_ptr<void, void (*)(void*)> hold(h, smoq_internal_free_prog);
+        if (smoq_status s = smoq_internal_rerun(ctx, &w.phi, h, nullptr)) return s;
+        VCK(cudaStreamSynchronize(ctx->stream));  // the program is freed at scope exit
+    }
+    if (w.phi.dtype == SMOQ_C64)
+        ham_apply_kernel<float><<<eblocks, 256, 0, ctx->stream>>>((const float2*)w.phi.ptr, (float2*)w.lam.ptr,
+                                                                  w.phi.N, d_terms, (int)ht.size(), d_epart);
+    else
+        ham_apply_kernel<double><<<eblocks, 256, 0, ctx->stream>>>((const double2*)w.phi.ptr, (double2*)w.lam.ptr,
+                                                                   w.phi.N, d_terms, (int)ht.size(), d_epart);
+    ctx->launches++;
+    VCK(cudaGetLastError());
+    std::vector<double> ep(eblocks);
+    VCK(cudaMemcpyAsync(ep.data(), d_epart, eblocks * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    VCK(cudaStreamSynchronize(ctx->stream));
+    double e = 0;
+    for (double x : ep) e += x;
+    *E = e;
+    return SMOQ_OK;
+}
+
+static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* ops, int n, int n_params,
+                           const smoq_pauli_term* H, int nterms, int batch, const double* theta, double* energies,
+                           double* grads) {
+    if (smoq_status s = check_vqe_args(ctx, N, dtype, ops, n, n_params, H, nterms, batch, theta)) return s;
+    Work w;
+    w.s = ctx->stream;
+    for (smoq_state* st : {&w.phi, &w.lam}) {
+        st->ctx = ctx;
+        st->N = N;
+        st->dtype = dtype;
+        st->batch = 1;
+        st->owned = false;
+        VCK(cudaMallocAsync(&st->ptr, st->bytes(), ctx->stream));
+        w.owned.push_back(st->ptr);
+    }
+    std::vector<HamTerm> ht(nterms);
+    for (int t = 0; t < nterms; ++t) {
+        ht[t].coef = H[t].coef;
+        ht[t].x = H[t].xmask;
+        ht[t].z = H[t].zmask;
+        ht[t].ny = __builtin_popcountll(H[t].xmask & H[t].zmask);
+    }
+    HamTerm* d_terms;
+    VCK(cudaMallocAsync((void**)&d_terms, ht.size() * sizeof(HamTerm), ctx->stream));
+    w.owned.push_back(d_terms);
+    VCK(cudaMemcpyAsync(d_terms, ht.data(), ht.size() * sizeof(HamTerm), cudaMemcpyHostToDevice, ctx->stream));
+    const int64_t len = (int64_t)1 << N;
+    const int eblocks = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, (int64_t)ctx->num_sms * 8));
+    double* d_epart;
+    VCK(cudaMallocAsync((void**)&d_epart, eblocks * sizeof(double), ctx->stream));
+    w.owned.push_back(d_epart);
+
+    for (int b = 0; b < batch; ++b) {
+        const double* th = theta ? theta + (size_t)b * n_params : nullptr;
+        std::vector<GateIR> ir;
+        if (smoq_status s = smoq_internal_ops_to_ir(N, ops, n, th, ir)) return smoq_internal_fail(ctx, s, "bad op list");
+        double E = 0;
+        if (smoq_status s = forward_and_h(ctx, w, ir, ht, d_terms, d_epart, eblocks, &E)) return s;
+        energies[b] = E;
+        if (!grads) continue;
+        double* g = grads + (size_t)b * n_params;
+        for (int p = 0; p < n_params; ++p) g[p] = 0.0;
+
+        // the backward program: for k = n-1 .. 0: [inner(G_k)] then U_k^dag
+        std::vector<GateIR> back;
+        std::vector<int> inner_param;
+        for (int k = n - 1; k >= 0; --k) {
+            if (ops[k].param >= 0) {
+                GateIR gi;
+                gi.nq = ir[k].nq;
+                for (int t = 0; t < gi.nq; ++t) gi.q[t] = ir[k].q[t];
+                if (!generator(ops[k].type, gi))
+                    return smoq_internal_fail(ctx, SMOQ_ERR_UNSUPPORTED,
+                                              "adjoint gradient: parameterised gate type has no generator");
+                gi.special = OPK_INNER;
+                gi.aux2 = (int64_t)inner_param.size();
+                inner_param.push_back(ops[k].param);
+                back.push_back(gi);
+            }
+            back.push_back(dagger(ir[k]));
+        }
+        if (inner_param.empty()) continue;
+        // tiles for two states in shared memory: one qubit narrower than the single-state passes
+        int T = std::max(smoq_internal_tile_bits(ctx, dtype) - 1, 6);
+        std::vector<Pass> passes;
+        try {
+            passes = plan_passes(back, N, T, smoq_internal_low_bits(ctx, dtype), -1, dtype == SMOQ_C64 ? 1 : 0);
+        } catch (const std::exception& ex) {
+            return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
+        }
+        // per pass: local inner slots -> global inner index
+        std::vector<std::vector<int>> slot_global(passes.size());
+        std::vector<size_t> off(passes.size() + 1, 0), opoff(passes.size() + 1, 0);
+        std::vector<DevOp> all;
+        for (size_t i = 0; i < passes.size(); ++i) {
+            for (DevOp& op : passes[i].ops)
+                if (op.kind == OPK_INNER) {
+                    slot_global[i].push_back(op.perm[0]);
+                    op.perm[0] = (int32_t)slot_global[i].size() - 1;
+                }
+            const int64_t ntiles = (int64_t)1 << (N - passes[i].g.T);
+            off[i + 1] = off[i] + (size_t)ntiles * std::max<size_t>(1, slot_global[i].size());
+            opoff[i + 1] = opoff[i] + passes[i].ops.size();
+            all.insert(all.end(), passes[i].ops.begin(), passes[i].ops.end());
+        }
+        double* d_part;
+        DevOp* d_ops;
+        VCK(cudaMallocAsync((void**)&d_part, off.back() * sizeof(double), ctx->stream));
+        VCK(cudaMallocAsync((void**)&d_ops, std::max<size_t>(1, all.size()) * sizeof(DevOp), ctx->stream));
+        VCK(cudaMemcpyAsync(d_ops, all.data(), all.size() * sizeof(DevOp), cudaMemcpyHostToDevice, ctx->stream));
+        for (size_t i = 0; i < passes.size(); ++i) {
+            const Pass& p = passes[i];
+            if (p.ops.empty()) continue;
+            AdjArgs A;
+            A.a.psi = w.phi.ptr;
+            A.a.state_len = len;
+            A.a.tiles_per_state = (int64_t)1 << (N - p.g.T);
+            A.a.ntiles = A.a.tiles_per_state;
+            A.a.ops = d_ops + opoff[i];
+            A.a.nops = (int32_t)p.ops.size();
+            A.a.err = ctx->d_err;
+            A.a.g = p.g;
+            A.a.ep.partials = nullptr;
+            A.a.ep.npop = 0;
+            A.lam = w.lam.ptr;
+            A.partials = d_part + off[i];
+            A.n_inner = (int32_t)std::max<size_t>(1, slot_global[i].size());
+            const size_t smem = (size_t)2 * w.phi.amp_bytes() << p.g.T;
+            int grid = (int)std::min<int64_t>(A.a.ntiles, (int64_t)ctx->num_sms * 2);
+            if (dtype == SMOQ_C64) {
+                VCK(cudaFuncSetAttribute(adj_tile_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                adj_tile_kernel<float><<<grid, 256, smem, ctx->stream>>>(A);
+            } else {
+                VCK(cudaFuncSetAttribute(adj_tile_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                adj_tile_kernel<double><<<grid, 256, smem, ctx->stream>>>(A);
+            }
+            ctx->launches++;
+            ctx->tile_passes++;
+            VCK(cudaGetLastError());
+        }
+        std::vector<double> part(off.back());
+        VCK(cudaMemcpyAsync(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        VCK(cudaFreeAsync(d_part, ctx->stream));
+        VCK(cudaFreeAsync(d_ops, ctx->stream));
+        VCK(cudaStreamSynchronize(ctx->stream));
+        int32_t herr = 0;
+        VCK(cudaMemcpy(&herr, ctx->d_err, sizeof(herr), cudaMemcpyDeviceToHost));
+        if (herr) {
+            VCK(cudaMemset(ctx->d_err, 0, sizeof(int32_t)));
+            return smoq_internal_fail(ctx, SMOQ_ERR_TIMEOUT, "a bounded device wait ran out");
+        }
+        for (size_t i = 0; i < passes.size(); ++i) {
+            const size_t ns = slot_global[i].size();
+            if (!ns) continue;
+            const int64_t ntiles = (int64_t)1 << (N - passes[i].g.T);
+            for (size_t sl = 0; sl < ns; ++sl) {
+                double s = 0;
+                for (int64_t t = 0; t < ntiles; ++t) s += part[off[i] + (size_t)t * ns + sl];
+                g[inner_param[slot_global[i][sl]]] += s;
+            }
+        }
+    }
+    return SMOQ_OK;
+}
+
+extern "C" smoq_status smoq_energy_grad(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* ops, int n,
+                                        int n_params, const smoq_pauli_term* H, int nterms, int batch,
+                                        const double* theta, double* energies, double* grads) {
+    if (!energies || !grads) return ctx ? smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "null output") : SMOQ_ERR_BADINPUT;
+    return vqe_run(ctx, N, dtype, ops, n, n_params, H, nterms, batch, theta, energies, grads);
+}
+
+extern "C" smoq_status smoq_energy(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* ops, int n, int n_params,
+                                   const smoq_pauli_term* H, int nterms, int batch, const double* theta,
+                                   double* energies) {
+    if (!energies) return ctx ? smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "null output") : SMOQ_ERR_BADINPUT;
+    return vqe_run(ctx, N, dtype, ops, n, n_params, H, nterms, batch, theta, energies, nullptr);
+}

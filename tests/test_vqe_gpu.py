@@ -1,0 +1,108 @@
+"""GPU parity of the VQE energy and the adjoint gradient.
+
+The oracle's energy (so_energy) and its gradients -- the parameter-shift rule
+(calculate_gradients_parameter_shift, cpuVariationalQuantumCircuitGradients.jl:138)
+and central finite differences (calculate_gradients_finite_difference, :250) --
+are the references.  The gradient configuration: TFIM H = -sum Z_i Z_{i+1} -
+sum X_i, 12 layers of [Ry all; Rz all; CZ ladder] on N=24 (576 parameters),
+complex64 and complex128."""
+import numpy as np
+import pytest
+
+import oracle as O
+import pysmoq as S
+
+pytestmark = pytest.mark.gpu
+
+
+def hea(N, L, seed=42):
+    ops, idx = [], 1
+    for _ in range(L):
+        rot, idx = S.single_qubit_rotation_layer(N, idx, gates=("ry", "rz"))
+        ops += rot + S.entangling_layer(N, "chain", "cz")
+    theta = np.random.default_rng(seed).uniform(0, 2 * np.pi, size=idx - 1)
+    return S.ParameterizedCircuit(N, ops), theta
+
+
+def tfim_terms(N):
+    return [(-1.0, {i: "Z", i + 1: "Z"}) for i in range(1, N)] + [(-1.0, {i: "X"}) for i in range(1, N + 1)]
+
+
+def oracle_ops(circ):
+    return [(op.type, op.qubits, op.param_idx, op.fixed_angle) for op in circ.operations]
+
+
+@pytest.mark.parametrize("N,L", [(4, 2), (8, 3), (11, 2)])
+def test_energy_and_adjoint_gradient_vs_oracle(ctx, N, L):
+    circ, theta = hea(N, L)
+    terms = tfim_terms(N)
+    H = S.PauliSum(terms)
+    oo = oracle_ops(circ)
+    arr = O.make_ops(oo)
+    e_ref = O.energy(arr, len(oo), theta, N, terms)
+    ps = O.grad(arr, len(oo), theta, N, terms, method="ps")
+    fd = O.grad(arr, len(oo), theta, N, terms, method="fd", eps=1e-4)
+    assert np.max(np.abs(ps - fd)) < 1e-6           # the two oracle gradients agree
+    e, g = S.energy_and_gradient(ctx, circ, H, theta, dtype=S.C128)
+    assert abs(e[0] - e_ref) < 1e-11
+    assert np.max(np.abs(g[0] - ps)) < 1e-10
+    e64, g64 = S.energy_and_gradient(ctx, circ, H, theta, dtype=S.C64)
+    assert abs(e64[0] - e_ref) < 1e-5
+    assert np.max(np.abs(g64[0] - ps)) < 1e-4
+    assert abs(S.energy(ctx, circ, H, theta, dtype=S.C128)[0] - e_ref) < 1e-11
+
+
+def test_all_generator_types_and_shared_parameters(ctx):
+    """RX, RY, RZ, RXX, RYY, RZZ, CRY with parameters (one shared by two gates),
+    mixed with fixed H, CNOT, S, T, CZ; Pauli terms with X, Y and Z."""
+    N = 7
+    g = S.gate
+    ops = [g("h", 1), g("rx", 2, param_idx=1), g("ry", 3, param_idx=2), g("cnot", [1, 4]),
+           g("rz", 4, param_idx=3), g("rxx", [2, 5], param_idx=4), g("s", 6), g("ryy", [5, 6], param_idx=5),
+           g("t", 7), g("rzz", [3, 7], param_idx=6), g("cry", [2, 6], param_idx=7), g("cz", [1, 7]),
+           g("rx", 5, param_idx=1), g("ry", 1, param_idx=8), g("cnot", [7, 2]), g("rz", 3, param_idx=2)]
+    circ = S.ParameterizedCircuit(N, ops)
+    theta = np.random.default_rng(3).uniform(-2, 2, size=circ.n_params)
+    terms = [(0.7, {1: "X", 2: "Y"}), (-1.1, {3: "Z", 7: "Z"}), (0.4, {4: "Y"}), (0.25, {2: "X", 5: "Z", 6: "Y"}),
+             (-0.3, {1: "Z"})]
+    oo = oracle_ops(circ)
+    arr = O.make_ops(oo)
+    e_ref = O.energy(arr, len(oo), theta, N, terms)
+    fd = O.grad(arr, len(oo), theta, N, terms, method="fd", eps=1e-5)
+    e, gr = S.energy_and_gradient(ctx, circ, S.PauliSum(terms), theta, dtype=S.C128)
+    assert abs(e[0] - e_ref) < 1e-12
+    assert np.max(np.abs(gr[0] - fd)) < 1e-7
+
+
+def test_batch_of_parameter_sets(ctx):
+    N, L, B = 9, 2, 4
+    circ, _ = hea(N, L)
+    rng = np.random.default_rng(5)
+    thetas = rng.uniform(0, 2 * np.pi, size=(B, circ.n_params))
+    H = S.PauliSum(tfim_terms(N))
+    e, g = S.energy_and_gradient(ctx, circ, H, thetas, dtype=S.C128)
+    for b in range(B):
+        e1, g1 = S.energy_and_gradient(ctx, circ, H, thetas[b], dtype=S.C128)
+        assert abs(e[b] - e1[0]) < 1e-13 and np.max(np.abs(g[b] - g1[0])) < 1e-13
+
+
+def test_gradient_configuration_n24(ctx):
+    """N=24, 12 layers, 576 parameters: the complex64 adjoint agrees with the
+    complex128 adjoint, and the complex128 adjoint with a GPU complex128
+    parameter-shift gradient on a fixed subset of 16 parameters."""
+    N, L = 24, 12
+    circ, theta = hea(N, L)
+    assert circ.n_params == 576 and len(circ.operations) == 852
+    H = S.PauliSum(tfim_terms(N))
+    e128, g128 = S.energy_and_gradient(ctx, circ, H, theta, dtype=S.C128)
+    e64, g64 = S.energy_and_gradient(ctx, circ, H, theta, dtype=S.C64)
+    assert abs(e64[0] - e128[0]) < 1e-4, abs(e64[0] - e128[0])
+    assert np.max(np.abs(g64[0] - g128[0])) < 1e-4
+    idx = np.linspace(0, 575, 16).astype(int)
+    shifted = np.repeat(theta[None, :], 32, axis=0)
+    for k, p in enumerate(idx):
+        shifted[2 * k, p] += np.pi / 2
+        shifted[2 * k + 1, p] -= np.pi / 2
+    es = S.energy(ctx, circ, H, shifted, dtype=S.C128)
+    ps = (es[0::2] - es[1::2]) / 2
+    assert np.max(np.abs(g128[0][idx] - ps)) < 1e-9
