@@ -183,6 +183,125 @@ def reference_arm(args):
     return 0
 
 
+def _events(torch, stream):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    return e0, e1
+
+
+def vqe_workload(args):
+    """VQE gradient throughput on the gradient configuration: TFIM N=24, 12 layers of
+    [Ry all; Rz all; CZ ladder] (852 gates, 576 parameters).  Batched complex64
+    adjoint gradients against the plain complex128 path (one kernel per gate,
+    per-term reductions, parameter-shift gradient); the plain path is timed on
+    one parameter's two shifted energies and scaled to 576 parameters."""
+    import torch
+    import pysmoq as S
+    ctx = S.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    N, L, B = 24, 12, 8
+    ops, idx = [], 1
+    for _ in range(L):
+        rot, idx = S.single_qubit_rotation_layer(N, idx, gates=("ry", "rz"))
+        ops += rot + S.entangling_layer(N, "chain", "cz")
+    circ = S.ParameterizedCircuit(N, ops)
+    P = circ.n_params
+    thetas = np.random.default_rng(SEED).uniform(0, 2 * np.pi, size=(B, P))
+    H = S.PauliSum.tfim(N)
+    res = {}
+    for name, dt in (("c64", S.C64), ("c128", S.C128)):
+        for _ in range(max(1, args.warmup)):
+            S.energy_and_gradient(ctx, circ, H, thetas[:1], dtype=dt)
+        e0, e1 = _events(torch, stream)
+        e0.record(stream)
+        for _ in range(args.steps):
+            E, G = S.energy_and_gradient(ctx, circ, H, thetas, dtype=dt)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        res[name] = (B * args.steps / (ms * 1e-3), E, G)
+
+    def plain_energy(theta):
+        st = S.CuState(ctx, N, S.C128, basis=0)
+        S.apply_circuit(st, circ, theta, fused=False)
+        e = -sum(S.expect_corr(st, i, i + 1, N, "zz") for i in range(1, N)) - \
+            sum(S.expect_local(st, i, N, "x") for i in range(1, N + 1))
+        st.close()
+        return e
+
+    plain_energy(thetas[0])
+    e0, e1 = _events(torch, stream)
+    e0.record(stream)
+    th = thetas[0].copy()
+    th[0] += np.pi / 2
+    ep = plain_energy(th)
+    th[0] -= np.pi
+    em = plain_energy(th)
+    e1.record(stream)
+    e1.synchronize()
+    pair_ms = e0.elapsed_time(e1)
+    plain_gps = 1.0 / (P * pair_ms * 1e-3)
+    ps0 = (ep - em) / 2
+    err_e = float(np.max(np.abs(res["c64"][1] - res["c128"][1])))
+    err_g = float(np.max(np.abs(res["c64"][2] - res["c128"][2])))
+    line = {"metric": "vqe_gradients_per_s", "value": res["c64"][0], "unit": "gradients/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * B / res["c64"][0],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {"workload": "vqe_tfim_n24_hea12_576params", "N": N, "layers": L, "params": P,
+                       "gates": len(ops), "batch": B, "gradient": "adjoint"},
+            "c128_adjoint_gradients_per_s": res["c128"][0],
+            "plain_c128_ps_gradients_per_s": plain_gps,
+            "plain_c128_sample": "two shifted energies of one parameter, one kernel per gate; scaled to 576 parameters",
+            "speedup_c64_adjoint_vs_plain_c128": res["c64"][0] / plain_gps,
+            "energy_abs_err_c64_vs_c128": err_e, "grad_max_abs_err_c64_vs_c128": err_g,
+            "plain_ps_vs_adjoint_param0": abs(ps0 - res["c128"][2][0, 0])}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
+def bandwidth_workload(args):
+    """32 GiB single-state sweeps: N=32 complex64 and N=31 complex128, 20 layers of
+    [Rx, Ry, Rz on every qubit (seeded angles); Rzz on a seeded random perfect
+    matching], fused passes; every pass timed with CUDA events."""
+    import torch
+    import pysmoq as S
+    ctx = S.Context(0)
+    peak, peak_kind = measured_peak()
+    out = {}
+    for N, dt, name in ((32, S.C64, "n32_c64"), (31, S.C128, "n31_c128")):
+        rng = np.random.default_rng(SEED)
+        ops = []
+        for _ in range(20):
+            for g in ("rx", "ry", "rz"):
+                ops += [S.gate(g, q, angle=float(rng.uniform(0, 2 * np.pi))) for q in range(1, N + 1)]
+            perm = rng.permutation(N) + 1
+            ops += [S.gate("rzz", [int(perm[2 * i]), int(perm[2 * i + 1])], angle=float(rng.uniform(0, 2 * np.pi)))
+                    for i in range(N // 2)]
+        circ = S.ParameterizedCircuit(N, ops)
+        st = S.CuState(ctx, N, dt, basis=0)
+        S.apply_circuit(st, circ, np.zeros(1))  # warm-up (plans, first touch)
+        ctx.set_option(S._lib.OPT_KERNEL_TIMING, 1)
+        ctx.reset_counters()
+        st.set_basis(0)
+        S.apply_circuit(st, circ, np.zeros(1))
+        c = ctx.counters()
+        ctx.set_option(S._lib.OPT_KERNEL_TIMING, 0)
+        masks = [1 << q for q in range(N)] + [3 << q for q in range(N - 1)]
+        obs = S.expect_zstrings(st, masks[:32])
+        gbs = c["tile_bytes"] / (c["tile_ms"] * 1e-3) / 1e9
+        out[name] = {"gates": len(ops), "passes": c["tile_passes"], "ms": c["tile_ms"],
+                     "gate_apps_per_s": len(ops) / (c["tile_ms"] * 1e-3), "hbm_gbs": gbs, "frac": gbs / peak,
+                     "norm": float(S.get_norm(st)), "z1": float(obs[0, 0])}
+        st.close()
+    line = {"metric": "hbm_gbs_per_sweep", "value": out["n32_c64"]["hbm_gbs"], "unit": "GB/s", "n_gpus": 1,
+            "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64", "data": "synthetic", "config": {"workload": "random_rxryrz_rzz_depth20_32GiB"},
+            "peak": peak, "peak_kind": peak_kind, "runs": out}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -194,9 +313,16 @@ def main():
     ap.add_argument("--n-qubits", type=int, default=N_QUBITS)
     ap.add_argument("--trotter-steps", type=int, default=STEPS)
     ap.add_argument("--tile-bits", type=int, default=0, help="complex64 tile width (0 = library default)")
+    ap.add_argument("--engine", type=int, default=-1, help="fused-pass engine (-1 = library default)")
+    ap.add_argument("--workload", default="trotter", choices=["trotter", "vqe", "bandwidth"],
+                    help="trotter: the headline line; vqe / bandwidth: the gradient and 32 GiB sweep figures")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload == "vqe":
+        return vqe_workload(args)
+    if args.workload == "bandwidth":
+        return bandwidth_workload(args)
 
     ws, rank, local = dist_env()
     import torch
@@ -216,6 +342,8 @@ def main():
     ctx = S.Context(local)
     if args.tile_bits:
         ctx.set_option(S._lib.OPT_TILE_BITS_C64, args.tile_bits)
+    if args.engine >= 0:
+        ctx.set_option(S._lib.OPT_ENGINE, args.engine)
     N = args.n_qubits
     tsteps = args.trotter_steps
     gate_apps = tsteps * 2 * (N + 3 * (N - 1))
