@@ -58,7 +58,8 @@ enum {
     SMOQ_OPT_LOW_BITS_C128 = 4,
     SMOQ_OPT_USE_GRAPHS = 5,      /* capture Trotter blocks as CUDA graphs (default 1) */
     SMOQ_OPT_KERNEL_TIMING = 6,   /* bracket fused passes with CUDA events (default 0) */
-    SMOQ_OPT_ENGINE = 7           /* fused-pass engine: 0 shared-memory sweeps (default), 1 register tiles */
+    SMOQ_OPT_ENGINE = 7           /* fused-pass engine: 0 shared-memory sweeps (default), 1 register tiles,
+                                     2 stage sweeps (4-bit register stages, tile widths 12-13) */
 };
 smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long value);
 /* launches: kernels launched by this context; tile_passes/tile_ms/tile_bytes:
@@ -272,8 +273,8 @@ typedef struct {
     int32_t mode;          /* 1 = applied through shared memory */
     double c[32];          /* 16 interleaved complex coefficients */
 } smoq_fused_op_info;
-smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops,
-                                     int n, const double* theta, smoq_pass_info* passes, int max_passes,
+smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tile_bits, int low_bits, int engine,
+                                     const smoq_op* ops, int n, const double* theta, smoq_pass_info* passes, int max_passes,
                                      smoq_fused_op_info* fused, int max_fused, int* n_passes, int* n_fused);
 
 #ifdef __cplusplus

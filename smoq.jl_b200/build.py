@@ -5,14 +5,16 @@
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "lib", "libsmoq_cuda.so")
-SOURCES = ["capi.cu", "k_kernels.cu", "k_regtile.cu", "planner.cpp", "mcwf.cu", "vqe.cu", "stubs.cu", "noalloc.cu"]
+SOURCES = ["capi.cu", "k_kernels.cu", "k_regtile.cu", "k_stage.cu", "planner.cpp", "mcwf.cu", "vqe.cu", "noalloc.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared"]
+              "-Xcompiler", "-fPIC"]
+OBJDIR = os.path.join(PKG, "_build")
 
 
 def _sources():
@@ -26,21 +28,38 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build_cuda(force=False, verbose=False):
+def build_cuda(force=False, verbose=False, lib=LIB, defines=()):
+    """Compile every source to an object (in parallel), link the shared library.
+    `defines` (e.g. ["SMOQ_STAGE_MINB_C64=2"]) are passed as -D to every source."""
     srcs = _sources()
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     deps.append(os.path.join(ROOT, "include", "smoq_cuda.h"))
-    if not force and not _stale(LIB, deps):
-        return LIB
-    os.makedirs(os.path.dirname(LIB), exist_ok=True)
+    if not force and not defines and not _stale(lib, deps):
+        return lib
+    os.makedirs(os.path.dirname(lib), exist_ok=True)
+    os.makedirs(OBJDIR, exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", LIB] + srcs
-    r = subprocess.run(cmd, capture_output=True, text=True)
+    dflags = ["-D" + d for d in defines]
+    tag = "_".join(d.replace("=", "") for d in defines)
+
+    def compile_one(src):
+        obj = os.path.join(OBJDIR, os.path.basename(src) + (("." + tag) if tag else "") + ".o")
+        cmd = [nvcc] + NVCC_FLAGS + dflags + (["-Xptxas", "-v"] if verbose else []) + ["-c", "-o", obj, src]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return obj, r
+
+    with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 4)) as ex:
+        results = list(ex.map(compile_one, srcs))
+    for obj, r in results:
+        if r.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        if verbose:
+            sys.stderr.write(r.stderr)
+    r = subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", lib] +
+                       [o for o, _ in results], capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
-    if verbose:
-        sys.stderr.write(r.stderr)
-    return LIB
+        raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
+    return lib
 
 
 def build_oracle(force=False):

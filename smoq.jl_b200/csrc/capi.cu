@@ -94,6 +94,9 @@ static std::vector<Pass> plan_for(int engine, const std::vector<GateIR>& ir, int
     if (engine == 1)
         for (Pass& p : pl)
             if (p.g.T >= RT_MIN_T && p.g.T - RT_MIN_T <= (dtype == SMOQ_C64 ? 5 : 4)) schedule_regtile(p);
+    if (engine == 2)
+        for (Pass& p : pl)
+            if (p.g.T == 12 || (p.g.T == 13 && dtype == SMOQ_C64)) schedule_stages(p, dtype == SMOQ_C64 ? 8 : 16);
     return pl;
 }
 
@@ -189,6 +192,7 @@ smoq_status smoq_ctx_create(int device, smoq_ctx** out) {
     if (cudaMemset(ctx->d_err, 0, sizeof(int32_t)) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (tile_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (regtile_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
+    if (stage_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (ensure_scratch(ctx.get(), 1 << 17) != SMOQ_OK) return SMOQ_ERR_OOM;
     if (ensure_pinned(ctx.get(), 1 << 20) != SMOQ_OK) return SMOQ_ERR_OOM;
     *out = ctx.release();
@@ -238,7 +242,7 @@ smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long v) {
         case SMOQ_OPT_USE_GRAPHS: ctx->use_graphs = v != 0; break;
         case SMOQ_OPT_KERNEL_TIMING: ctx->kernel_timing = v != 0; break;
         case SMOQ_OPT_ENGINE:
-            if (v != 0 && v != 1) return fail(ctx, SMOQ_ERR_BADINPUT, "engine must be 0 or 1");
+            if (v < 0 || v > 2) return fail(ctx, SMOQ_ERR_BADINPUT, "engine must be 0, 1 or 2");
             ctx->engine = (int)v;
             break;
         default: return fail(ctx, SMOQ_ERR_BADINPUT, "unknown option");
@@ -532,16 +536,17 @@ smoq_status smoq_apply_sequence(smoq_state* st, const smoq_op* ops, int n, const
     return sync_check(ctx);
 }
 
-smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tbits, int lbits, const smoq_op* ops, int n,
+smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tbits, int lbits, int engine, const smoq_op* ops, int n,
                                      const double* theta, smoq_pass_info* passes, int max_passes,
                                      smoq_fused_op_info* fused, int max_fused, int* n_passes, int* n_fused) {
     if (N < 1 || N > 40 || n < 0 || (n > 0 && !ops) || !n_passes || !n_fused) return SMOQ_ERR_BADINPUT;
     if (dtype != SMOQ_C64 && dtype != SMOQ_C128) return SMOQ_ERR_BADINPUT;
+    if (engine < 0 || engine > 2) return SMOQ_ERR_BADINPUT;
     std::vector<GateIR> ir;
     if (smoq_status s = ops_to_ir(nullptr, N, ops, n, theta, ir)) return s;
     std::vector<Pass> pl;
     try {
-        pl = plan_for(1, ir, N, dtype, tbits, lbits);
+        pl = plan_for(engine, ir, N, dtype, tbits, lbits);
     } catch (const std::exception&) {
         return SMOQ_ERR_BADINPUT;
     }

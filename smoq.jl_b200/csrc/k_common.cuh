@@ -195,4 +195,30 @@ __device__ __forceinline__ void sweep_op(const DevOp& op, typename CT<R>::T* psi
     }
 }
 
+// ------------------------------------------------------- tile bulk loads
+// first global index of tile t and the state it belongs to
+__device__ __forceinline__ uint64_t tile_base(const TileArgs& a, int64_t t, int64_t& b) {
+    b = t / a.tiles_per_state;
+    const int64_t r0 = t - b * a.tiles_per_state;
+    uint64_t base = (uint64_t)r0 << a.g.L;
+    for (int m = 0; m < a.g.H; ++m) base = ins0<uint64_t>(base, a.g.hb[m]);
+    return base;
+}
+
+// issue the bulk copies that bring tile t into `buf` (completion on `bar`)
+template <typename C>
+__device__ __forceinline__ void issue_tile_load(const TileArgs& a, int64_t t, C* buf, uint64_t* bar) {
+    int64_t b;
+    const uint64_t base = tile_base(a, t, b);
+    const C* gs = reinterpret_cast<const C*>(a.psi) + b * a.state_len;
+    const uint32_t nseg = 1u << a.g.H;
+    const uint32_t seg_bytes = (uint32_t)sizeof(C) << a.g.L;
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, ((uint32_t)sizeof(C)) << a.g.T);
+    for (uint32_t s = threadIdx.x; s < nseg; s += blockDim.x) {
+        uint64_t off = base;
+        for (int m = 0; m < a.g.H; ++m) off |= (uint64_t)((s >> m) & 1) << a.g.hb[m];
+        bulk_g2s(buf + ((size_t)s << a.g.L), gs + off, seg_bytes, bar);
+    }
+}
+
 }  // namespace smoq

@@ -434,6 +434,11 @@ cudaError_t launch_tile_pass(smoq_ctx* ctx, smoq_state* st, const Pass& p, const
         ctx->launches++;
         return e;
     }
+    if (p.staged) {
+        e = launch_stage(ctx, a, st->dtype, epi);
+        ctx->launches++;
+        return e;
+    }
     if (st->dtype == SMOQ_C64)
         e = epi ? launch_tile_t<float, true>(ctx, a, smem, 0) : launch_tile_t<float, false>(ctx, a, smem, 0);
     else

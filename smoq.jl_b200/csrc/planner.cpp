@@ -640,4 +640,113 @@ void schedule_regtile(Pass& p) {
     p.regtile = true;
 }
 
+// ----------------------------------------------------------------------------
+// Stage-sweep scheduling (engine 2).  The tile stays in shared memory; the
+// pass's op list is cut into stages of consecutive ops whose non-diagonal
+// qubits fit in 4 tile bits S.  A stage is one conflict-free sweep: every
+// thread loads 16-amplitude groups (the 16 values of S for fixed other bits)
+// into registers, applies all the stage's ops there and stores them back.
+// Bank spreading: the tile bits below `LB` pick the shared-memory bank
+// (8-byte amplitudes: 16 per 128-byte row, LB = 4; 16-byte amplitudes:
+// LB = 3).  Lanes run over the lowest free (non-S) bits; every stage bit below
+// LB is XOR-rotated by one lane bit (perm[4 + k]), so the 32 lanes of a warp
+// always hit distinct banks.  The kernel folds the rotation into per-thread
+// coefficients, once per op.
+// ----------------------------------------------------------------------------
+void schedule_stages(Pass& p, int amp_bytes) {
+    const int T = p.g.T;
+    if (T < 12 || T > 13) return;
+    const int LB = amp_bytes == 8 ? 4 : 3;
+    for (const DevOp& op : p.ops)  // adjoint partials and layout ops belong to other kernels
+        if (op.kind == OPK_INNER || op.kind == OPK_LAYOUT || op.kind == OPK_JUMP || op.kind == OPK_STAGE) return;
+    std::vector<DevOp> in = std::move(p.ops);
+    // 1- and 2-qubit permutations run as dense matrices on the stage registers
+    for (DevOp& op : in) {
+        if (op.kind != OPK_MONO || op.nq > 2) continue;
+        const int dim = 1 << op.nq;
+        double2 d[4];
+        float2 f[4];
+        for (int r = 0; r < dim; ++r) d[r] = op.cd[r], f[r] = op.cf[r];
+        for (int k = 0; k < 16; ++k) {
+            op.cd[k] = make_double2(0.0, 0.0);
+            op.cf[k] = make_float2(0.f, 0.f);
+        }
+        for (int r = 0; r < dim; ++r) {
+            op.cd[r * dim + op.perm[r]] = d[r];
+            op.cf[r * dim + op.perm[r]] = f[r];
+        }
+        op.kind = op.nq == 1 ? OPK_DENSE1 : OPK_DENSE2;
+    }
+    std::vector<DevOp> out;
+    auto needs = [](const DevOp& op) {
+        std::vector<int> v;
+        if (op.kind == OPK_DIAG || op.kind == OPK_STATESCALE || op.kind == OPK_REALTAB) return v;
+        for (int t = 0; t < op.nq; ++t) v.push_back(op.lb[t]);
+        return v;
+    };
+    auto contains = [](const std::vector<int>& s, int b) { return std::find(s.begin(), s.end(), b) != s.end(); };
+    auto header = [&](std::vector<int> S, int nmembers) {
+        for (int b = LB; (int)S.size() < 4 && b < T; ++b)  // pad with bank-neutral bits first
+            if (!contains(S, b)) S.push_back(b);
+        for (int b = 0; (int)S.size() < 4 && b < T; ++b)
+            if (!contains(S, b)) S.push_back(b);
+        std::sort(S.begin(), S.end());
+        DevOp h;
+        std::memset(&h, 0, sizeof(h));
+        h.kind = OPK_STAGE;
+        h.nq = 4;
+        h.aux2 = nmembers;
+        int c = 0;  // free bits below LB: the lowest lane bits
+        for (int b = 0; b < LB; ++b)
+            if (!contains(S, b)) ++c;
+        int a = 0;
+        for (int k = 0; k < 4; ++k) {
+            h.perm[k] = S[k];
+            h.perm[4 + k] = S[k] < LB ? c + a++ : -1;
+        }
+        return h;
+    };
+    size_t i = 0;
+    while (i < in.size()) {
+        // a 3-qubit permutation (Toffoli) runs as a plain shared-memory sweep
+        if (in[i].kind != OPK_DIAG && in[i].nq > 2) {
+            DevOp h;
+            std::memset(&h, 0, sizeof(h));
+            h.kind = OPK_STAGE;
+            h.nq = 0;
+            h.aux2 = 1;
+            out.push_back(h);
+            out.push_back(in[i]);
+            ++i;
+            continue;
+        }
+        std::vector<int> S;
+        size_t j = i;
+        for (; j < in.size(); ++j) {
+            if (in[j].kind != OPK_DIAG && in[j].nq > 2) break;
+            std::vector<int> U = S;
+            for (int b : needs(in[j]))
+                if (!contains(U, b)) U.push_back(b);
+            if (U.size() > 4) break;
+            S = U;
+        }
+        DevOp h = header(S, (int)(j - i));
+        out.push_back(h);
+        for (size_t k = i; k < j; ++k) {
+            DevOp op = in[k];
+            for (int t = 0; t < 4; ++t) op.slot[t] = -1;
+            if (op.kind != OPK_DIAG && op.kind != OPK_STATESCALE && op.kind != OPK_REALTAB) {
+                for (int t = 0; t < op.nq; ++t)
+                    for (int q = 0; q < 4; ++q)
+                        if (h.perm[q] == op.lb[t]) op.slot[t] = q;
+                if (op.nq == 2 && op.slot[0] > op.slot[1]) swap_qubit_roles(op);
+            }
+            out.push_back(op);
+        }
+        i = j;
+    }
+    p.ops = std::move(out);
+    p.staged = true;
+}
+
 }  // namespace smoq

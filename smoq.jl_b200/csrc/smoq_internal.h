@@ -32,6 +32,10 @@ enum OpKind : int32_t {
     OPK_STATESCALE = 5,  // amp *= scale[b] (per state, real, from aux pointer)
     OPK_REALTAB = 6,  // amp *= prod_j tab[j][byte j of global index] (real factors)
     OPK_JUMP = 7,     // per-state jump (sigma-/sigma+/sigma_z/sigma_x) from aux list
+    OPK_STAGE = 10,   // stage-sweep engine: header of a stage; perm[0..3] = the stage's 4
+                      // tile bits (ascending), perm[4..7] = lane bit feeding the rotation of
+                      // each stage bit (-1 none), aux2 = number of member ops that follow;
+                      // nq = 0 marks a single op applied by a plain shared-memory sweep
     OPK_INNER = 9,    // adjoint sweep: per-tile Im<lambda|G|phi> with G = cd (dense, 1-2
                       // qubits), written to partials slot perm[0] of the pass
     OPK_LAYOUT = 8,   // register-tile layout change: perm[0..KR-1] = register bits,
@@ -105,6 +109,7 @@ struct Pass {
     std::vector<DevOp> ops;
     bool epilogue = false;
     bool regtile = false;   // scheduled for the register-tile engine (ops[0] is OPK_LAYOUT)
+    bool staged = false;    // scheduled for the stage-sweep engine (OPK_STAGE headers)
 };
 
 // register-tile engine geometry: 256 threads = 8 warps x 32 lanes; lanes hold
@@ -119,6 +124,8 @@ std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, in
                               int epilogue_after_special = -1, int Lreq = 0);
 // turn a planned pass into a register-tile program (layout ops + slots)
 void schedule_regtile(Pass& p);
+// turn a planned pass into stage sweeps (engine 2); amp_bytes selects the bank geometry
+void schedule_stages(Pass& p, int amp_bytes);
 void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op);
 
 // gate library (planner.cpp)
@@ -145,8 +152,10 @@ struct smoq_ctx {
     int low_bits_c64 = 5;
     int low_bits_c128 = 4;
     int use_graphs = 1;
-    int engine = 0;                    // fused passes: 0 = shared-memory sweeps, 1 = register tiles
+    int engine = 0;                    // fused passes: 0 = shared-memory sweeps, 1 = register tiles,
+                                       // 2 = stage sweeps
     int rt_occ[2][2][8] = {};          // CTAs per SM of the register-tile kernel [dtype][epilogue][KR]
+    int st_occ[2][2][2] = {};          // CTAs per SM of the stage kernel [dtype][epilogue][GP-1]
     int kernel_timing = 0;             // bracket tile passes with events
     long long launches = 0;            // kernels launched by this ctx
     long long tile_passes = 0;
@@ -184,4 +193,6 @@ size_t tile_max_smem(int amp_bytes, int T);
 cudaError_t tile_kernels_init(smoq_ctx* ctx);
 cudaError_t regtile_kernels_init(smoq_ctx* ctx);
 cudaError_t launch_regtile(smoq_ctx* ctx, const TileArgs& a, int dtype, bool epi);
+cudaError_t stage_kernels_init(smoq_ctx* ctx);
+cudaError_t launch_stage(smoq_ctx* ctx, const TileArgs& a, int dtype, bool epi);
 }  // namespace smoq

@@ -638,17 +638,18 @@ def energy_and_gradient(ctx: Context, circuit: ParameterizedCircuit, H: PauliSum
 
 # ------------------------------------------------------ planner introspection
 def debug_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtype: int = C128, tile_bits: int = 12,
-               low_bits: int = 4):
-    """Host-only view of how smoq_apply_sequence splits `ops` into tile passes.
+               low_bits: int = 4, engine: int = 1):
+    """Host-only view of how smoq_apply_sequence splits `ops` into tile passes
+    (as scheduled for fused-pass `engine`).
     Returns a list of passes: {"T","L","H","hb","ops":[{"kind","nq","lb","gb","perm","c"}]}."""
     arr = circuit_to_c_ops(ops)
     th = np.ascontiguousarray(theta if theta is not None else np.zeros(1), dtype=np.float64)
     npass, nops = C.c_int(), C.c_int()
-    ck(lib.smoq_debug_plan_sequence(N, dtype, tile_bits, low_bits, arr, len(ops), dptr(th), None, 0, None, 0,
+    ck(lib.smoq_debug_plan_sequence(N, dtype, tile_bits, low_bits, engine, arr, len(ops), dptr(th), None, 0, None, 0,
                                     C.byref(npass), C.byref(nops)), None, "debug_plan")
     P = (_lib.SmoqPassInfo * max(1, npass.value))()
     F = (_lib.SmoqFusedOpInfo * max(1, nops.value))()
-    ck(lib.smoq_debug_plan_sequence(N, dtype, tile_bits, low_bits, arr, len(ops), dptr(th), P, npass.value, F,
+    ck(lib.smoq_debug_plan_sequence(N, dtype, tile_bits, low_bits, engine, arr, len(ops), dptr(th), P, npass.value, F,
                                     nops.value, C.byref(npass), C.byref(nops)), None, "debug_plan")
     out, k = [], 0
     for i in range(npass.value):

@@ -53,7 +53,7 @@ def op_matrix(op):
 def replay(plan, N, psi):
     for p in plan:
         for op in p["ops"]:
-            if op["kind"] == 8:      # register-tile layout change: no arithmetic
+            if op["kind"] in (8, 10):  # layout change / stage header: no arithmetic
                 continue
             psi = apply_local(psi, op_matrix(op), op["gb"][:op["nq"]], N)
     return psi
@@ -149,3 +149,67 @@ def test_diagonal_gates_need_no_tile_membership(built):
     plan = S.debug_plan(N, ops, dtype=S.C64, tile_bits=12, low_bits=5)
     assert len(plan) == 1
     assert any(op["kind"] == 4 and -1 in op["lb"][:op["nq"]] for op in plan[0]["ops"])
+
+
+def check_stages(plan, lb_bank):
+    """stage-sweep schedule: every member op sits on its stage's 4 bits, 2-qubit
+    members in ascending stage positions, the bank rotation uses distinct lane
+    bits exactly for the stage bits below the bank boundary"""
+    for p in plan:
+        ops = p["ops"]
+        i = 0
+        while i < len(ops):
+            h = ops[i]
+            assert h["kind"] == 10
+            i += 1
+            if h["nq"] == 0:                      # single wide op, plain sweep
+                assert ops[i]["nq"] == 3 and ops[i]["kind"] == 3
+                i += 1
+                continue
+            S = h["perm"][:4]
+            assert S == sorted(S) and len(set(S)) == 4 and all(0 <= b < p["T"] for b in S)
+            rot = h["perm"][4:]
+            free_low = sum(1 for b in range(lb_bank) if b not in S)
+            lanes = [r for r in rot if r >= 0]
+            assert [r >= 0 for r in rot] == [b < lb_bank for b in S]
+            assert sorted(lanes) == list(range(free_low, free_low + len(lanes)))
+            while i < len(ops) and ops[i]["kind"] != 10:
+                op = ops[i]
+                if op["kind"] not in (4, 5, 6):
+                    assert op["kind"] in (0, 1, 2), "permutations of 1-2 qubits run as dense stage ops"
+                    pos = op["slot"][:op["nq"]]
+                    assert all(S[q] == op["lb"][t] for t, q in enumerate(pos))
+                    if op["nq"] == 2:
+                        assert pos[0] < pos[1]
+                i += 1
+
+
+@pytest.mark.parametrize("N", [12, 13, 15])
+@pytest.mark.parametrize("dtype,tile_bits", [("c64", 12), ("c64", 13), ("c128", 12)])
+def test_stage_schedule_replays_and_is_well_formed(built, N, dtype, tile_bits):
+    import pysmoq as S
+    dt = S.C64 if dtype == "c64" else S.C128
+    rng = np.random.default_rng(N)
+    g, o = circuit(N - N % 2, 400)
+    g = [x for x in g if max(x.qubits) <= N]
+    o = [x for x in o if max(x[1]) <= N]
+    # permutations, parity bonds and 3-qubit ops on top of the benchmark circuit
+    for _ in range(40):
+        a = int(rng.integers(1, N))
+        t = ["swap_like", "rxx", "ryy", "toffoli", "cnot"][int(rng.integers(5))]
+        if t == "toffoli":
+            qs = [int(x) + 1 for x in rng.choice(N, 3, replace=False)]
+        else:
+            qs = [a, a + 1]
+            t = "rzz" if t == "swap_like" else t
+        ang = float(rng.uniform(-3, 3))
+        g.append(S.gate(t, qs, angle=ang))
+        o.append((t, qs, 0, ang))
+    plan = S.debug_plan(N, g, dtype=dt, tile_bits=tile_bits, low_bits=5 if dt == S.C64 else 4, engine=2)
+    staged = [p for p in plan if p["T"] == 12 or (p["T"] == 13 and dt == S.C64)]
+    assert staged, "no pass wide enough for the stage engine"
+    check_stages(staged, 4 if dt == S.C64 else 3)
+    want = O.zero_state(N)
+    O.apply_circuit(want, O.make_ops(o), len(o), np.zeros(1), N)
+    got = replay(plan, N, O.zero_state(N))
+    assert np.max(np.abs(got - want)) < 1e-12
