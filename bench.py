@@ -131,8 +131,25 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    p = os.path.join(ROOT, "profiles", "tile_pass_xxz_n28_c64.json")
+ENGINE_KERNELS = {0: ("tile_pass_kernel<float>", "tile_pass_xxz_n28_c64.json"),
+                  1: ("regtile_kernel<float>", None),
+                  2: ("stage_kernel<float>", None),
+                  3: ("smoq_pass_e0 (compiled per pass)", "compiled_pass_xxz_n28_c64.json")}
+
+
+def resolve_engine(S, engine):
+    """the fused-pass engine a Trotter plan runs: the option, or the library's auto
+    choice (compiled pass kernels when NVRTC loads, else shared-memory sweeps)"""
+    if engine >= 0:
+        return engine
+    return 3 if S.jit_available() else 0
+
+
+def ncu_traffic(engine):
+    name = ENGINE_KERNELS[engine][1]
+    if name is None:
+        return None
+    p = os.path.join(ROOT, "profiles", name)
     if os.path.exists(p):
         try:
             return float(json.load(open(p))["traffic_bytes_per_launch"])
@@ -340,6 +357,7 @@ def main():
     import pysmoq as S
 
     ctx = S.Context(local)
+    eng = resolve_engine(S, args.engine)
     if args.tile_bits:
         ctx.set_option(S._lib.OPT_TILE_BITS_C64, args.tile_bits)
     if args.engine >= 0:
@@ -439,15 +457,15 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
                 "data": "synthetic",
                 "config": {"workload": workload, "N": N, "dt": DT, "trotter_steps": tsteps,
-                           "tile_bits_c64": args.tile_bits or 13,
+                           "tile_bits_c64": args.tile_bits or 13, "engine": eng,
                            "record_every": RECORD_EVERY, "gate_apps_per_step": gate_apps,
                            "state_bytes": (1 << N) * 8, "l2_policy": "inputs larger than L2 (2 GiB state)",
                            "parallelism": "replicas" if ws > 1 else "single_gpu",
                            "tile_passes_per_step": passes, "hbm_gbs_effective":
                                2.0 * (1 << N) * 8 * passes / (ms / args.steps * 1e-3) / 1e9},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": ncu_traffic(), "peak_kind": peak_kind,
-                             "kernel": "tile_pass_kernel<float>", "avg_launch_ms": avg_ms,
+                             "frac": achieved / peak, "traffic": ncu_traffic(eng), "peak_kind": peak_kind,
+                             "kernel": ENGINE_KERNELS[eng][0], "avg_launch_ms": avg_ms,
                              "algorithmic_bytes_per_launch": bytes_per_launch},
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": "gate-apps/s", "h2d_bytes_per_step": int(hp.nbytes),

@@ -58,8 +58,12 @@ enum {
     SMOQ_OPT_LOW_BITS_C128 = 4,
     SMOQ_OPT_USE_GRAPHS = 5,      /* capture Trotter blocks as CUDA graphs (default 1) */
     SMOQ_OPT_KERNEL_TIMING = 6,   /* bracket fused passes with CUDA events (default 0) */
-    SMOQ_OPT_ENGINE = 7           /* fused-pass engine: 0 shared-memory sweeps (default), 1 register tiles,
-                                     2 stage sweeps (4-bit register stages, tile widths 12-13) */
+    SMOQ_OPT_ENGINE = 7           /* fused-pass engine: -1 auto (default), 0 shared-memory sweeps,
+                                     1 register tiles, 2 stage sweeps (4-bit register stages, tile
+                                     widths 12-13), 3 compiled pass kernels (engine 2's schedule,
+                                     each complex64 pass compiled with NVRTC at upload; needs
+                                     libnvrtc).  Auto: reusable complex64 programs (Trotter plans,
+                                     MCWF) run engine 3 when NVRTC loads, everything else engine 0 */
 };
 smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long value);
 /* launches: kernels launched by this context; tile_passes/tile_ms/tile_bytes:
@@ -69,6 +73,8 @@ smoq_status smoq_ctx_counters(smoq_ctx* ctx, long long* launches, long long* til
 smoq_status smoq_ctx_reset_counters(smoq_ctx* ctx);
 /* the library's build identification, e.g. "smoq_cuda sm_100a" */
 const char* smoq_version(void);
+/* 1 when the plan compiler (engine 3) can run: NVRTC could be loaded */
+int smoq_jit_available(void);
 
 /* ----------------------------------------------------------------- states */
 /* Vector{ComplexF64}(undef, 2^N) per state; zero-initialised */
@@ -273,6 +279,13 @@ typedef struct {
     int32_t mode;          /* 1 = applied through shared memory */
     double c[32];          /* 16 interleaved complex coefficients */
 } smoq_fused_op_info;
+/* Host-only check of the plan compiler (engine 3): plans `ops` as smoq_apply_sequence
+ * would with engine 3 and compiles every complex64 pass kernel with NVRTC, without a GPU
+ * and without loading them.  *n_compiled = kernels compiled; msg gets "ok" (verbose: the
+ * compiler's register/spill report) or the first error.  SMOQ_ERR_UNSUPPORTED when NVRTC
+ * is not available. */
+smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops, int n,
+                                    const double* theta, int verbose, int* n_compiled, char* msg, int msg_len);
 smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tile_bits, int low_bits, int engine,
                                      const smoq_op* ops, int n, const double* theta, smoq_pass_info* passes, int max_passes,
                                      smoq_fused_op_info* fused, int max_fused, int* n_passes, int* n_fused);

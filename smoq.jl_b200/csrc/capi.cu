@@ -86,6 +86,14 @@ static int low_bits(smoq_ctx* ctx, int dtype) {
     return dtype == SMOQ_C64 ? ctx->low_bits_c64 : ctx->low_bits_c128;
 }
 
+// fused-pass engine of a program: the ctx option, or in auto mode (-1) the
+// compiled pass kernels for reusable complex64 programs (Trotter plans, MCWF)
+// when NVRTC is available and the shared-memory sweeps otherwise
+static int engine_for(smoq_ctx* ctx, bool reusable, int dtype) {
+    if (ctx->engine >= 0) return ctx->engine;
+    return (reusable && dtype == SMOQ_C64 && jit_available()) ? 3 : 0;
+}
+
 // plan a gate list into fused passes; with the register engine every pass
 // wide enough for it gets a register-tile schedule
 static std::vector<Pass> plan_for(int engine, const std::vector<GateIR>& ir, int N, int dtype, int tbits, int lbits,
@@ -94,9 +102,12 @@ static std::vector<Pass> plan_for(int engine, const std::vector<GateIR>& ir, int
     if (engine == 1)
         for (Pass& p : pl)
             if (p.g.T >= RT_MIN_T && p.g.T - RT_MIN_T <= (dtype == SMOQ_C64 ? 5 : 4)) schedule_regtile(p);
-    if (engine == 2)
+    if (engine == 2 || engine == 3)
         for (Pass& p : pl)
-            if (p.g.T == 12 || (p.g.T == 13 && dtype == SMOQ_C64)) schedule_stages(p, dtype == SMOQ_C64 ? 8 : 16);
+            if (p.g.T == 12 || (p.g.T == 13 && dtype == SMOQ_C64)) {
+                schedule_stages(p, dtype == SMOQ_C64 ? 8 : 16);
+                p.want_jit = engine == 3 && p.staged && dtype == SMOQ_C64;
+            }
     return pl;
 }
 
@@ -115,6 +126,12 @@ struct DevProgram {
 }  // namespace
 
 static smoq_status upload_program(smoq_ctx* ctx, DevProgram& P) {
+    for (Pass& p : P.passes) {
+        if (!p.want_jit || p.jit) continue;
+        std::string why;
+        p.jit = jit_pass_kernel(p, why);
+        if (!p.jit) return fail(ctx, SMOQ_ERR_UNSUPPORTED, "compiled pass kernel: " + why);
+    }
     std::vector<DevOp> all;
     P.offs.clear();
     for (size_t i = 0; i < P.passes.size(); ++i) {
@@ -174,6 +191,8 @@ static void harvest_timing(smoq_ctx* ctx, std::vector<EventPair>& timing) {
 extern "C" {
 
 const char* smoq_version(void) { return "smoq_cuda 0.1 sm_100a"; }
+
+int smoq_jit_available(void) { return jit_available() ? 1 : 0; }
 
 smoq_status smoq_ctx_create(int device, smoq_ctx** out) {
     if (!out) return SMOQ_ERR_BADINPUT;
@@ -242,7 +261,7 @@ smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long v) {
         case SMOQ_OPT_USE_GRAPHS: ctx->use_graphs = v != 0; break;
         case SMOQ_OPT_KERNEL_TIMING: ctx->kernel_timing = v != 0; break;
         case SMOQ_OPT_ENGINE:
-            if (v < 0 || v > 2) return fail(ctx, SMOQ_ERR_BADINPUT, "engine must be 0, 1 or 2");
+            if (v < -1 || v > 3) return fail(ctx, SMOQ_ERR_BADINPUT, "engine must be -1 (auto), 0, 1, 2 or 3");
             ctx->engine = (int)v;
             break;
         default: return fail(ctx, SMOQ_ERR_BADINPUT, "unknown option");
@@ -522,7 +541,8 @@ smoq_status smoq_apply_sequence(smoq_state* st, const smoq_op* ops, int n, const
     if (smoq_status s = ops_to_ir(st, st->N, ops, n, theta, ir)) return s;
     DevProgram P;
     try {
-        P.passes = plan_for(ctx->engine, ir, st->N, st->dtype, tile_bits(ctx, st->dtype), low_bits(ctx, st->dtype));
+        P.passes = plan_for(engine_for(ctx, false, st->dtype), ir, st->N, st->dtype, tile_bits(ctx, st->dtype),
+                            low_bits(ctx, st->dtype));
     } catch (const std::exception& ex) {
         return fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
     }
@@ -536,12 +556,47 @@ smoq_status smoq_apply_sequence(smoq_state* st, const smoq_op* ops, int n, const
     return sync_check(ctx);
 }
 
+smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tbits, int lbits, const smoq_op* ops, int n,
+                                   const double* theta, int verbose, int* n_compiled, char* msg, int msg_len) {
+    if (N < 1 || N > 40 || n < 0 || (n > 0 && !ops) || !n_compiled) return SMOQ_ERR_BADINPUT;
+    if (dtype != SMOQ_C64 && dtype != SMOQ_C128) return SMOQ_ERR_BADINPUT;
+    *n_compiled = 0;
+    auto say = [&](const std::string& m) {
+        if (msg && msg_len > 0) {
+            std::strncpy(msg, m.c_str(), (size_t)msg_len - 1);
+            msg[msg_len - 1] = 0;
+        }
+    };
+    std::vector<GateIR> ir;
+    if (smoq_status s = ops_to_ir(nullptr, N, ops, n, theta, ir)) return s;
+    std::vector<Pass> pl;
+    try {
+        pl = plan_for(3, ir, N, dtype, tbits, lbits);
+    } catch (const std::exception& e) {
+        say(e.what());
+        return SMOQ_ERR_BADINPUT;
+    }
+    std::string report;
+    for (const Pass& p : pl) {
+        if (!p.want_jit) continue;
+        std::string why, info;
+        if (!jit_check_pass(p, why, nullptr, verbose ? &info : nullptr)) {
+            say(why);
+            return why.rfind("NVRTC (", 0) == 0 ? SMOQ_ERR_UNSUPPORTED : SMOQ_ERR_BADINPUT;
+        }
+        report += info;
+        ++*n_compiled;
+    }
+    say(verbose ? report : std::string("ok"));
+    return SMOQ_OK;
+}
+
 smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tbits, int lbits, int engine, const smoq_op* ops, int n,
                                      const double* theta, smoq_pass_info* passes, int max_passes,
                                      smoq_fused_op_info* fused, int max_fused, int* n_passes, int* n_fused) {
     if (N < 1 || N > 40 || n < 0 || (n > 0 && !ops) || !n_passes || !n_fused) return SMOQ_ERR_BADINPUT;
     if (dtype != SMOQ_C64 && dtype != SMOQ_C128) return SMOQ_ERR_BADINPUT;
-    if (engine < 0 || engine > 2) return SMOQ_ERR_BADINPUT;
+    if (engine < 0 || engine > 3) return SMOQ_ERR_BADINPUT;
     std::vector<GateIR> ir;
     if (smoq_status s = ops_to_ir(nullptr, N, ops, n, theta, ir)) return s;
     std::vector<Pass> pl;
@@ -761,7 +816,7 @@ static smoq_status get_block(smoq_plan* P, int nsteps, smoq_plan::Block** out) {
     all.reserve(P->step.size() * nsteps);
     for (int s = 0; s < nsteps; ++s) all.insert(all.end(), P->step.begin(), P->step.end());
     try {
-        B->prog.passes = plan_for(P->ctx->engine, all, P->N, P->dtype, tile_bits(P->ctx, P->dtype),
+        B->prog.passes = plan_for(engine_for(P->ctx, true, P->dtype), all, P->N, P->dtype, tile_bits(P->ctx, P->dtype),
                                   low_bits(P->ctx, P->dtype));
     } catch (const std::exception& ex) {
         return fail(P->ctx, SMOQ_ERR_BADINPUT, ex.what());
@@ -989,10 +1044,10 @@ smoq_status smoq_internal_plan_step(smoq_plan* plan, std::vector<GateIR>& out, i
 
 // plan + upload a gate program for `st` (no launch); the handle owns it
 smoq_status smoq_internal_prepare(smoq_ctx* ctx, smoq_state* st, const std::vector<GateIR>& gates,
-                                  int epilogue_special, void** handle) {
+                                  int epilogue_special, bool reusable, void** handle) {
     std::unique_ptr<DevProgram> P(new DevProgram());
     try {
-        P->passes = plan_for(ctx->engine, gates, st->N, st->dtype, tile_bits(ctx, st->dtype),
+        P->passes = plan_for(engine_for(ctx, reusable, st->dtype), gates, st->N, st->dtype, tile_bits(ctx, st->dtype),
                              low_bits(ctx, st->dtype), epilogue_special);
     } catch (const std::exception& ex) {
         return fail(ctx, SMOQ_ERR_BADINPUT, ex.what());

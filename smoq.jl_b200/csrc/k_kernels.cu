@@ -434,6 +434,11 @@ cudaError_t launch_tile_pass(smoq_ctx* ctx, smoq_state* st, const Pass& p, const
         ctx->launches++;
         return e;
     }
+    if (p.jit) {
+        e = launch_jit(ctx, a, p.jit, epi);
+        ctx->launches++;
+        return e;
+    }
     if (p.staged) {
         e = launch_stage(ctx, a, st->dtype, epi);
         ctx->launches++;

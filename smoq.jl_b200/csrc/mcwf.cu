@@ -160,7 +160,7 @@ using namespace smoq;
 // pieces of capi.cu this file uses
 smoq_status smoq_internal_plan_step(smoq_plan* plan, std::vector<GateIR>& out, int& N, int& dtype, int& order);
 smoq_status smoq_internal_prepare(smoq_ctx* ctx, smoq_state* st, const std::vector<GateIR>& gates,
-                                  int epilogue_special, void** prog_handle);
+                                  int epilogue_special, bool reusable, void** prog_handle);
 smoq_status smoq_internal_rerun(smoq_ctx* ctx, smoq_state* st, void* prog_handle, const Epilogue* ep);
 void smoq_internal_free_prog(void* prog_handle);
 smoq_status smoq_internal_fail(smoq_ctx* ctx, smoq_status s, const char* msg);
@@ -291,7 +291,7 @@ extern "C" smoq_status smoq_mcwf_run(smoq_plan* plan, smoq_state* st, const smoq
     ep.npop = (int)popq.size();
     for (size_t k = 0; k < popq.size(); ++k) ep.popq[k] = popq[k];
     void* handle = nullptr;
-    if (smoq_status s = smoq_internal_prepare(ctx, st, prog, OPK_REALTAB, &handle)) return s;
+    if (smoq_status s = smoq_internal_prepare(ctx, st, prog, OPK_REALTAB, true, &handle)) return s;
     std::unique_ptr<void, void (*)(void*)> hold(handle, smoq_internal_free_prog);
     const int64_t tps = smoq_internal_tiles_per_state(handle);
     MCK(buf.alloc(&d_part, (size_t)B * tps * (1 + ep.npop)));

@@ -104,12 +104,22 @@ struct GateIR {
     int tag = -1;           // caller tag (e.g. parameter index) carried through
 };
 
+// a pass program compiled to its own kernel (engine 3, jit.cpp)
+struct JitKernel {
+    const void* fn[2] = {nullptr, nullptr};  // without / with the norm+population epilogue
+    int threads = 0;
+    int per_sm[2] = {1, 1};
+    size_t smem = 0;
+};
+
 struct Pass {
     TileGeom g;
     std::vector<DevOp> ops;
     bool epilogue = false;
     bool regtile = false;   // scheduled for the register-tile engine (ops[0] is OPK_LAYOUT)
     bool staged = false;    // scheduled for the stage-sweep engine (OPK_STAGE headers)
+    bool want_jit = false;  // engine 3: compile this staged pass to its own kernel at upload
+    const JitKernel* jit = nullptr;
 };
 
 // register-tile engine geometry: 256 threads = 8 warps x 32 lanes; lanes hold
@@ -127,6 +137,12 @@ void schedule_regtile(Pass& p);
 // turn a planned pass into stage sweeps (engine 2); amp_bytes selects the bank geometry
 void schedule_stages(Pass& p, int amp_bytes);
 void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op);
+// jit.cpp: compile (or fetch from the process cache) the kernel of a staged complex64 pass
+const JitKernel* jit_pass_kernel(const Pass& p, std::string& err);
+// jit.cpp: generate and compile a staged complex64 pass without a GPU (plan checks)
+bool jit_check_pass(const Pass& p, std::string& err, size_t* cubin_bytes, std::string* info);
+// jit.cpp: NVRTC could be loaded
+bool jit_available();
 
 // gate library (planner.cpp)
 GateIR gate_1q(int q, const cd m[4]);
@@ -152,8 +168,8 @@ struct smoq_ctx {
     int low_bits_c64 = 5;
     int low_bits_c128 = 4;
     int use_graphs = 1;
-    int engine = 0;                    // fused passes: 0 = shared-memory sweeps, 1 = register tiles,
-                                       // 2 = stage sweeps
+    int engine = -1;                   // fused passes: -1 = auto, 0 = shared-memory sweeps, 1 = register
+                                       // tiles, 2 = stage sweeps, 3 = compiled pass kernels
     int rt_occ[2][2][8] = {};          // CTAs per SM of the register-tile kernel [dtype][epilogue][KR]
     int st_occ[2][2][2] = {};          // CTAs per SM of the stage kernel [dtype][epilogue][GP-1]
     int kernel_timing = 0;             // bracket tile passes with events
@@ -195,4 +211,5 @@ cudaError_t regtile_kernels_init(smoq_ctx* ctx);
 cudaError_t launch_regtile(smoq_ctx* ctx, const TileArgs& a, int dtype, bool epi);
 cudaError_t stage_kernels_init(smoq_ctx* ctx);
 cudaError_t launch_stage(smoq_ctx* ctx, const TileArgs& a, int dtype, bool epi);
+cudaError_t launch_jit(smoq_ctx* ctx, const TileArgs& a, const JitKernel* k, bool epi);
 }  // namespace smoq

@@ -225,7 +225,7 @@ smoq_status smoq_internal_fail(smoq_ctx* ctx, smoq_status s, const char* msg);
 smoq_status smoq_internal_cuda(smoq_ctx* ctx, cudaError_t e, const char* where);
 smoq_status smoq_internal_ops_to_ir(int N, const smoq_op* ops, int n, const double* theta, std::vector<GateIR>& out);
 smoq_status smoq_internal_prepare(smoq_ctx* ctx, smoq_state* st, const std::vector<GateIR>& gates,
-                                  int epilogue_special, void** prog_handle);
+                                  int epilogue_special, bool reusable, void** prog_handle);
 smoq_status smoq_internal_rerun(smoq_ctx* ctx, smoq_state* st, void* prog_handle, const Epilogue* ep);
 void smoq_internal_free_prog(void* prog_handle);
 int smoq_internal_tile_bits(smoq_ctx* ctx, int dtype);
@@ -306,7 +306,7 @@ static smoq_status forward_and_h(smoq_ctx* ctx, Work& w, const std::vector<GateI
     VCK(launch_set_basis(&w.phi, 0));
     if (!ir.empty()) {
         void* h = nullptr;
-        if (smoq_status s = smoq_internal_prepare(ctx, &w.phi, ir, -1, &h)) return s;
+        if (smoq_status s = smoq_internal_prepare(ctx, &w.phi, ir, -1, false, &h)) return s;
         std::unique_ptr<void, void (*)(void*)> hold(h, smoq_internal_free_prog);
         if (smoq_status s = smoq_internal_rerun(ctx, &w.phi, h, nullptr)) return s;
         VCK(cudaStreamSynchronize(ctx->stream));  // the program is freed at scope exit

@@ -663,3 +663,22 @@ def debug_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtype: int =
                              "c": np.array(f.c[:]).view(np.complex128).copy()})
         out.append(d)
     return out
+
+
+def debug_compile_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtype: int = C64, tile_bits: int = 13,
+                       low_bits: int = 5, verbose: bool = False):
+    """Host-only: plan `ops` for the plan compiler (engine 3) and compile every pass
+    kernel with NVRTC (no GPU, nothing loaded).  Returns (status, n_compiled, message);
+    with verbose the message is the compiler's register/spill report."""
+    arr = circuit_to_c_ops(ops)
+    th = np.ascontiguousarray(theta if theta is not None else np.zeros(1), dtype=np.float64)
+    n = C.c_int()
+    msg = C.create_string_buffer(1 << 16)
+    st = lib.smoq_debug_compile_plan(N, dtype, tile_bits, low_bits, arr, len(ops), dptr(th), int(verbose), C.byref(n),
+                                     msg, 1 << 16)
+    return st, n.value, msg.value.decode(errors="replace")
+
+
+def jit_available() -> bool:
+    """True when the plan compiler (engine 3, NVRTC) can run in this process."""
+    return bool(lib.smoq_jit_available())

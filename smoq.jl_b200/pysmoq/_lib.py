@@ -129,6 +129,9 @@ _SIGS = {
                       C.c_int, _dp, _dp, _dp, _dp, _ip],
     "smoq_energy_grad": [_vp, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, C.c_int, C.POINTER(SmoqPauliTerm),
                          C.c_int, C.c_int, _dp, _dp, _dp],
+    "smoq_jit_available": [],
+    "smoq_debug_compile_plan": [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, _dp, C.c_int, _ip,
+                                C.c_char_p, C.c_int],
     "smoq_debug_plan_sequence": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, _dp,
                                  C.POINTER(SmoqPassInfo), C.c_int, C.POINTER(SmoqFusedOpInfo), C.c_int, _ip, _ip],
     "smoq_energy": [_vp, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, C.c_int, C.POINTER(SmoqPauliTerm),

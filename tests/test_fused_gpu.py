@@ -95,7 +95,7 @@ def test_both_engines_and_register_widths(ctx, engine, N, tile_bits):
             finally:
                 ctx.set_option(opt, default)
     finally:
-        ctx.set_option(S._lib.OPT_ENGINE, 0)
+        ctx.set_option(S._lib.OPT_ENGINE, -1)
 
 
 def hea_ops(N, L, theta_seed=42):

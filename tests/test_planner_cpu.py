@@ -213,3 +213,25 @@ def test_stage_schedule_replays_and_is_well_formed(built, N, dtype, tile_bits):
     O.apply_circuit(want, O.make_ops(o), len(o), np.zeros(1), N)
     got = replay(plan, N, O.zero_state(N))
     assert np.max(np.abs(got - want)) < 1e-12
+
+
+@pytest.mark.parametrize("N,tile_bits", [(13, 12), (16, 13), (20, 13)])
+def test_plan_compiler_generates_valid_kernels(built, N, tile_bits):
+    """engine 3 (host only): every complex64 stage pass of a circuit with every gate
+    kind compiles with NVRTC for sm_100a, without spills"""
+    import pysmoq as S
+    rng = np.random.default_rng(N)
+    kinds = ["h", "rx", "rz", "t", "cnot", "cz", "rxx", "ryy", "rzz", "cry", "toffoli", "ccz"]
+    g = []
+    for _ in range(120):
+        t = kinds[int(rng.integers(len(kinds)))]
+        k = 3 if t in ("toffoli", "ccz") else (2 if t in ("cnot", "cz", "rxx", "ryy", "rzz", "cry") else 1)
+        qs = [int(x) + 1 for x in rng.choice(N, k, replace=False)]
+        g.append(S.gate(t, qs, angle=float(rng.uniform(-3, 3))))
+    st, n, msg = S.debug_compile_plan(N, g, dtype=S.C64, tile_bits=tile_bits, verbose=True)
+    if st == 5:
+        pytest.skip("NVRTC not available: " + msg)
+    assert st == 0, msg
+    assert n >= 1
+    assert "0 bytes spill stores" in msg and "bytes spill stores" in msg
+    assert all(" 0 bytes spill" in line for line in msg.splitlines() if "spill stores" in line), msg

@@ -1,8 +1,11 @@
-"""GPU parity of the stage-sweep engine (fused-pass engine 2).
+"""GPU parity of the stage-sweep engine (fused-pass engine 2) and of the plan
+compiler (engine 3, the same stage schedule compiled per pass with NVRTC).
 
 The stage engine runs every fused pass of tile width 12 or 13 as 4-bit
 register stages with XOR-rotated bank mapping; every other width falls back to
-the shared-memory sweeps.  These tests switch the engine on and compare with
+the shared-memory sweeps.  Engine 3 compiles each complex64 stage pass into
+its own kernel (literal coefficients, compile-time addressing); complex128
+passes run engine 2's kernel.  These tests switch the engine on and compare with
 the oracle on the workloads that reach each op kind of a stage:
 dense and parity 2-qubit ops on rotated and unrotated stage bits, 1- and
 2-qubit permutations turned dense, 3-qubit permutations as plain sweeps,
@@ -21,6 +24,11 @@ pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
 
+@pytest.fixture(params=[2, 3], ids=["stage", "compiled"])
+def eng(request):
+    return request.param
+
+
 def rel(a, b):
     return np.max(np.abs(a - b)) / np.max(np.abs(b))
 
@@ -37,7 +45,7 @@ class engine:
         self.ctx.set_option(S._lib.OPT_TILE_BITS_C128, self.tb128)
 
     def __exit__(self, *a):
-        self.ctx.set_option(S._lib.OPT_ENGINE, 0)
+        self.ctx.set_option(S._lib.OPT_ENGINE, -1)
         self.ctx.set_option(S._lib.OPT_TILE_BITS_C64, 13)
         self.ctx.set_option(S._lib.OPT_TILE_BITS_C128, 12)
 
@@ -90,11 +98,11 @@ def random_circuit(N, n, seed):
 
 @pytest.mark.parametrize("N", [12, 14, 16, 20])
 @pytest.mark.parametrize("tb64", [12, 13])
-def test_benchmark_circuits(ctx, N, tb64):
+def test_benchmark_circuits(ctx, eng, N, tb64):
     g_ops, o_ops = bench_circuit(N, 800)
     want = O.zero_state(N)
     O.apply_circuit(want, O.make_ops(o_ops), len(o_ops), np.zeros(1), N)
-    with engine(ctx, 2, tb64=tb64):
+    with engine(ctx, eng, tb64=tb64):
         for dtype, tol in ((S.C128, 1e-12), (S.C64, 5e-5)):
             st = S.CuState(ctx, N, dtype)
             S.apply_circuit(st, S.ParameterizedCircuit(N, g_ops), np.zeros(1))
@@ -102,14 +110,16 @@ def test_benchmark_circuits(ctx, N, tb64):
 
 
 @pytest.mark.parametrize("N,seed", [(12, 1), (13, 2), (15, 3), (18, 4)])
-def test_random_circuits_every_gate_kind(ctx, N, seed):
-    g_ops, o_ops = random_circuit(N, 500, seed)
+def test_random_circuits_every_gate_kind(ctx, eng, N, seed):
+    # the plan compiler builds one kernel per distinct pass: a shorter circuit keeps
+    # its compile time in check while still reaching every gate kind
+    g_ops, o_ops = random_circuit(N, 500 if eng == 2 else 200, seed)
     rng = np.random.default_rng(seed + 100)
     psi = rng.normal(size=1 << N) + 1j * rng.normal(size=1 << N)
     psi /= np.linalg.norm(psi)
     want = psi.copy()
     O.apply_circuit(want, O.make_ops(o_ops), len(o_ops), np.zeros(1), N)
-    with engine(ctx, 2):
+    with engine(ctx, eng):
         for dtype, tol in ((S.C128, 1e-12), (S.C64, 5e-5)):
             st = S.CuState(ctx, N, dtype, basis=None)
             st.upload(psi.astype(np.complex128 if dtype == S.C128 else np.complex64))
@@ -128,7 +138,7 @@ def xxz(N, dt):
 
 @pytest.mark.parametrize("N,dtype,tb64,tol", [(14, S.C128, 13, 1e-12), (16, S.C64, 13, 1e-4),
                                               (17, S.C64, 12, 1e-4)])
-def test_strang_trotter(ctx, N, dtype, tb64, tol):
+def test_strang_trotter(ctx, eng, N, dtype, tb64, tol):
     dt, steps, rec = 0.05, 6, 3
     arr, n, gl = xxz(N, dt)
     neel = sum(1 << (k - 1) for k in range(1, N + 1, 2))
@@ -139,7 +149,7 @@ def test_strang_trotter(ctx, N, dtype, tb64, tol):
         O.trotter_step(psi, both, 2 * n, N)
         if s % rec == 0:
             want_rec.append([O.expect_local(psi, k, N, "z") for k in range(1, N + 1)])
-    with engine(ctx, 2, tb64=tb64):
+    with engine(ctx, eng, tb64=tb64):
         plan = S.TrotterPlan(ctx, N, [S.FastTrotterGate(i, U) for i, U in gl], order=2, dtype=dtype)
         st = S.CuState(ctx, N, dtype, basis=neel)
         recs = plan.run(st, steps, rec)
@@ -154,7 +164,7 @@ def test_engines_agree_on_trotter_n22(ctx):
     _, _, gl = xxz(N, 0.05)
     gates = [S.FastTrotterGate(i, U) for i, U in gl]
     out = {}
-    for e in (0, 2):
+    for e in (0, 2, 3):
         with engine(ctx, e):
             plan = S.TrotterPlan(ctx, N, gates, order=2, dtype=S.C64)
             st = S.CuState(ctx, N, S.C64, basis=5)
@@ -163,9 +173,10 @@ def test_engines_agree_on_trotter_n22(ctx):
             st.close()
             plan.close()
     assert np.max(np.abs(out[0] - out[2])) < 2e-6
+    assert np.max(np.abs(out[0] - out[3])) < 2e-6
 
 
-def test_mcwf_trajectory_exact(ctx):
+def test_mcwf_trajectory_exact(ctx, eng):
     """N=12 complex128 trajectories through stage passes (renormalise, decay
     table, norm/population epilogue) match the oracle's jump counts exactly"""
     N, dt, steps, rec, B, seed = 12, 0.05, 30, 5, 8, 99
@@ -176,7 +187,7 @@ def test_mcwf_trajectory_exact(ctx):
          [S.JumpOperator("sigma_z", q, 0.1) for q in range(1, N + 1)]
     oj = [(0, q, 0.3) for q in range(1, N + 1)] + [(2, q, 0.1) for q in range(1, N + 1)]
     idx = (1 << N) - 1
-    with engine(ctx, 2):
+    with engine(ctx, eng):
         plan = S.TrotterPlan(ctx, N, gates, order=1, dtype=S.C128)
         st = S.CuState(ctx, N, S.C128, B, basis=idx)
         res = S.mcwf_run(plan, st, gj, dt, seed, steps, rec, traj_offset=3, per_trajectory=True)
@@ -188,7 +199,7 @@ def test_mcwf_trajectory_exact(ctx):
     assert np.max(np.abs(res["zz_traj"] - zz)) < 1e-10
 
 
-def test_vqe_energy_and_gradient(ctx):
+def test_vqe_energy_and_gradient(ctx, eng):
     N, L = 13, 3
     ops, idx = [], 1
     for _ in range(L):
@@ -198,13 +209,31 @@ def test_vqe_energy_and_gradient(ctx):
     circ = S.ParameterizedCircuit(N, ops)
     H = S.PauliSum.tfim(N)
     e0, g0 = S.energy_and_gradient(ctx, circ, H, theta, dtype=S.C128)
-    with engine(ctx, 2):
+    with engine(ctx, eng):
         e2, g2 = S.energy_and_gradient(ctx, circ, H, theta, dtype=S.C128)
     assert abs(e2[0] - e0[0]) < 1e-11
     assert np.max(np.abs(g2 - g0)) < 1e-10
 
 
+def test_mcwf_complex64_epilogue_engines_agree(ctx, eng):
+    """N=13 complex64 trajectories: the compiled passes with the norm/population
+    epilogue give the stage engine's jump counts and records"""
+    N, dt, steps, rec, B, seed = 13, 0.05, 20, 5, 16, 7
+    arr, n = O.precompute_trotter_gates([(i, i + 1, 0.0, 0.0, 1.0) for i in range(1, N)],
+                                        [(i, 1.0, 0.0, 0.0) for i in range(1, N + 1)], dt)
+    gates = [S.FastTrotterGate(idx, U) for idx, U in O.gates_to_list(arr, n)]
+    gj = [S.JumpOperator("sigma_minus", q, 0.3) for q in range(1, N + 1)]
+    out = {}
+    for e in (0, eng):
+        with engine(ctx, e):
+            plan = S.TrotterPlan(ctx, N, gates, order=1, dtype=S.C64)
+            st = S.CuState(ctx, N, S.C64, B, basis=(1 << N) - 1)
+            out[e] = S.mcwf_run(plan, st, gj, dt, seed, steps, rec, per_trajectory=True)
+    assert np.array_equal(out[0]["jumps"], out[eng]["jumps"])
+    assert np.max(np.abs(out[0]["z_traj"] - out[eng]["z_traj"])) < 1e-4
+
+
 def test_engine_option_range(ctx):
     with pytest.raises(Exception):
-        ctx.set_option(S._lib.OPT_ENGINE, 3)
-    ctx.set_option(S._lib.OPT_ENGINE, 0)
+        ctx.set_option(S._lib.OPT_ENGINE, 4)
+    ctx.set_option(S._lib.OPT_ENGINE, -1)
