@@ -331,6 +331,7 @@ def main():
     ap.add_argument("--trotter-steps", type=int, default=STEPS)
     ap.add_argument("--tile-bits", type=int, default=0, help="complex64 tile width (0 = library default)")
     ap.add_argument("--engine", type=int, default=-1, help="fused-pass engine (-1 = library default)")
+    ap.add_argument("--jit-buffers", type=int, default=1, help="compiled pass kernels: tile buffers per CTA (1, 2)")
     ap.add_argument("--workload", default="trotter", choices=["trotter", "vqe", "bandwidth"],
                     help="trotter: the headline line; vqe / bandwidth: the gradient and 32 GiB sweep figures")
     args = ap.parse_args()
@@ -362,6 +363,8 @@ def main():
         ctx.set_option(S._lib.OPT_TILE_BITS_C64, args.tile_bits)
     if args.engine >= 0:
         ctx.set_option(S._lib.OPT_ENGINE, args.engine)
+    if args.jit_buffers != 1:
+        ctx.set_option(S._lib.OPT_JIT_BUFFERS, args.jit_buffers)
     N = args.n_qubits
     tsteps = args.trotter_steps
     gate_apps = tsteps * 2 * (N + 3 * (N - 1))

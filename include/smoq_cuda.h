@@ -63,7 +63,9 @@ enum {
                                      widths 12-13), 3 compiled pass kernels (engine 2's schedule,
                                      each complex64 pass compiled with NVRTC at upload; needs
                                      libnvrtc).  Auto: reusable complex64 programs (Trotter plans,
-                                     MCWF) run engine 3 when NVRTC loads, everything else engine 0 */
+                                     MCWF) run engine 3 when NVRTC loads, everything else engine 0 */,
+    SMOQ_OPT_JIT_BUFFERS = 8      /* compiled pass kernels: tile buffers per CTA, 1 (default) or 2 (the next
+                                     tile's bulk load runs under the current tile's stages) */
 };
 smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long value);
 /* launches: kernels launched by this context; tile_passes/tile_ms/tile_bytes:
@@ -281,11 +283,12 @@ typedef struct {
 } smoq_fused_op_info;
 /* Host-only check of the plan compiler (engine 3): plans `ops` as smoq_apply_sequence
  * would with engine 3 and compiles every complex64 pass kernel with NVRTC, without a GPU
- * and without loading them.  *n_compiled = kernels compiled; msg gets "ok" (verbose: the
- * compiler's register/spill report) or the first error.  SMOQ_ERR_UNSUPPORTED when NVRTC
- * is not available. */
+ * and without loading them.  flags: 1 = return the compiler's register/spill report in msg,
+ * 2 = two tile buffers per CTA (SMOQ_OPT_JIT_BUFFERS 2).  *n_compiled = kernels compiled; msg
+ * gets "ok" (or the report) or the first error.  SMOQ_ERR_UNSUPPORTED when NVRTC is not
+ * available. */
 smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops, int n,
-                                    const double* theta, int verbose, int* n_compiled, char* msg, int msg_len);
+                                    const double* theta, int flags, int* n_compiled, char* msg, int msg_len);
 smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tile_bits, int low_bits, int engine,
                                      const smoq_op* ops, int n, const double* theta, smoq_pass_info* passes, int max_passes,
                                      smoq_fused_op_info* fused, int max_fused, int* n_passes, int* n_fused);

@@ -129,7 +129,7 @@ static smoq_status upload_program(smoq_ctx* ctx, DevProgram& P) {
     for (Pass& p : P.passes) {
         if (!p.want_jit || p.jit) continue;
         std::string why;
-        p.jit = jit_pass_kernel(p, why);
+        p.jit = jit_pass_kernel(p, ctx->jit_buffers, why);
         if (!p.jit) return fail(ctx, SMOQ_ERR_UNSUPPORTED, "compiled pass kernel: " + why);
     }
     std::vector<DevOp> all;
@@ -263,6 +263,10 @@ smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long v) {
         case SMOQ_OPT_ENGINE:
             if (v < -1 || v > 3) return fail(ctx, SMOQ_ERR_BADINPUT, "engine must be -1 (auto), 0, 1, 2 or 3");
             ctx->engine = (int)v;
+            break;
+        case SMOQ_OPT_JIT_BUFFERS:
+            if (v != 1 && v != 2) return fail(ctx, SMOQ_ERR_BADINPUT, "compiled-kernel tile buffers must be 1 or 2");
+            ctx->jit_buffers = (int)v;
             break;
         default: return fail(ctx, SMOQ_ERR_BADINPUT, "unknown option");
     }
@@ -557,7 +561,8 @@ smoq_status smoq_apply_sequence(smoq_state* st, const smoq_op* ops, int n, const
 }
 
 smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tbits, int lbits, const smoq_op* ops, int n,
-                                   const double* theta, int verbose, int* n_compiled, char* msg, int msg_len) {
+                                   const double* theta, int flags, int* n_compiled, char* msg, int msg_len) {
+    const bool verbose = (flags & 1) != 0;
     if (N < 1 || N > 40 || n < 0 || (n > 0 && !ops) || !n_compiled) return SMOQ_ERR_BADINPUT;
     if (dtype != SMOQ_C64 && dtype != SMOQ_C128) return SMOQ_ERR_BADINPUT;
     *n_compiled = 0;
@@ -580,7 +585,7 @@ smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tbits, int lbit
     for (const Pass& p : pl) {
         if (!p.want_jit) continue;
         std::string why, info;
-        if (!jit_check_pass(p, why, nullptr, verbose ? &info : nullptr)) {
+        if (!jit_check_pass(p, (flags & 2) ? 2 : 1, why, nullptr, verbose ? &info : nullptr)) {
             say(why);
             return why.rfind("NVRTC (", 0) == 0 ? SMOQ_ERR_UNSUPPORTED : SMOQ_ERR_BADINPUT;
         }

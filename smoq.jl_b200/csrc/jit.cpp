@@ -428,7 +428,7 @@ struct Gen {
 };
 
 // full source of the kernels for one pass
-std::string generate(const Pass& p, bool need_epi, std::string& err) {
+std::string generate(const Pass& p, bool need_epi, int nbuf, std::string& err) {
     const int N = p.g.N;
     const TileGeom& g = p.g;
     const int T = g.T;
@@ -458,25 +458,54 @@ std::string generate(const Pass& p, bool need_epi, std::string& err) {
          "    for (int k = 0; k < (int)op.aux2; ++k) f *= tab[k * 256 + ((gi >> (8 * k)) & 255)];\n"
          "    return (float)f;\n}\n";
     // the body
+    // tile loop: one buffer (load, run, store), or two with the next tile's
+    // bulk load issued before the current tile's stages run
+    o << "__device__ __forceinline__ void issue_load(const TileArgs& a, i64 t, cf* buf, u64* bar) {\n"
+         "    i64 b;\n"
+         "    const u64 base = tile_base(t, b);\n"
+         "    const cf* gs = (const cf*)a.psi + b * a.state_len;\n"
+         "    if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, 8u << TB);\n"
+         "    for (u32 s = threadIdx.x; s < (1u << HB); s += NT)\n"
+         "        bulk_g2s(buf + ((u64)s << LB), gs + seg_off(base, s), 8u << LB, bar);\n"
+         "}\n";
     o << "template <bool EPI>\n__device__ __forceinline__ void body(const TileArgs& a) {\n"
          "    extern __shared__ __align__(128) unsigned char smem_raw[];\n"
-         "    cf* tile = (cf*)smem_raw;\n"
-         "    __shared__ __align__(8) u64 bar;\n"
+         "    cf* const buf0 = (cf*)smem_raw;\n"
+         "    __shared__ __align__(8) u64 bars[2];\n"
          "    __shared__ double red[NT / 32][16];\n"
          "    const u32 tid = threadIdx.x;\n"
          "    const u32 seg_bytes = 8u << LB;\n"
-         "    if (tid == 0) { mbar_init(&bar, 1); fence_mbar_init(); }\n"
+         "    if (tid == 0) { mbar_init(&bars[0], 1); mbar_init(&bars[1], 1); fence_mbar_init(); }\n"
          "    __syncthreads();\n"
-         "    u32 phase = 0;\n"
-         "    for (i64 t = blockIdx.x; t < a.ntiles; t += gridDim.x) {\n"
+         "    u32 phases = 0;\n";
+    if (nbuf == 2)
+        o << "    cf* const buf1 = buf0 + (1u << TB);\n"
+             "    if ((i64)blockIdx.x < a.ntiles) issue_load(a, blockIdx.x, buf0, &bars[0]);\n";
+    o << "    int k = 0;\n"
+         "    for (i64 t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++k) {\n"
          "    i64 b;\n"
          "    const u64 base = tile_base(t, b);\n"
-         "    cf* gs = (cf*)a.psi + b * a.state_len;\n"
-         "    if (tid == 0) mbar_arrive_expect_tx(&bar, 8u << TB);\n"
-         "    for (u32 s = tid; s < (1u << HB); s += NT) bulk_g2s(tile + ((u64)s << LB), gs + seg_off(base, s), seg_bytes, &bar);\n"
-         "    const bool ok = mbar_wait_bounded(&bar, phase, a.err);\n"
-         "    if (!__syncthreads_and(ok)) { mbar_wait_bounded(&bar, phase, nullptr); return; }\n"
-         "    phase ^= 1;\n";
+         "    cf* gs = (cf*)a.psi + b * a.state_len;\n";
+    if (nbuf == 2)
+        o << "    const int cur = k & 1;\n"
+             "    cf* const tile = cur ? buf1 : buf0;\n"
+             "    const bool have_next = t + gridDim.x < a.ntiles;\n"
+             "    if (have_next) issue_load(a, t + gridDim.x, cur ? buf0 : buf1, &bars[cur ^ 1]);\n"
+             "    const bool ok = mbar_wait_bounded(&bars[cur], (phases >> cur) & 1, a.err);\n"
+             "    if (!__syncthreads_and(ok)) {\n"
+             "        mbar_wait_bounded(&bars[cur], (phases >> cur) & 1, nullptr);\n"
+             "        if (have_next) mbar_wait_bounded(&bars[cur ^ 1], (phases >> (cur ^ 1)) & 1, nullptr);\n"
+             "        return;\n"
+             "    }\n"
+             "    phases ^= 1u << cur;\n";
+    else
+        o << "    const int cur = 0;\n"
+             "    cf* const tile = buf0;\n"
+             "    issue_load(a, t, tile, &bars[0]);\n"
+             "    const bool ok = mbar_wait_bounded(&bars[0], phases & 1, a.err);\n"
+             "    if (!__syncthreads_and(ok)) { mbar_wait_bounded(&bars[0], phases & 1, nullptr); return; }\n"
+             "    phases ^= 1;\n"
+             "    (void)cur; (void)k;\n";
     // stages
     const int LBk = 4;  // complex64 bank boundary
     size_t o_i = 0;
@@ -614,12 +643,12 @@ bool compile_cubin(const std::string& src, std::vector<char>& cubin, std::string
 
 // Generate and compile a staged complex64 pass without loading it (host only);
 // `info` (optional) receives the compiler's resource report.
-bool jit_check_pass(const Pass& p, std::string& err, size_t* cubin_bytes, std::string* info) {
+bool jit_check_pass(const Pass& p, int nbuf, std::string& err, size_t* cubin_bytes, std::string* info) {
     if (!p.staged || (p.g.T != 12 && p.g.T != 13)) {
         err = "jit: only stage-scheduled passes of tile width 12-13";
         return false;
     }
-    const std::string src = generate(p, p.epilogue, err);
+    const std::string src = generate(p, p.epilogue, nbuf, err);
     if (src.empty()) return false;
     std::vector<char> cubin;
     if (!compile_cubin(src, cubin, err, info)) return false;
@@ -629,12 +658,12 @@ bool jit_check_pass(const Pass& p, std::string& err, size_t* cubin_bytes, std::s
 
 // Compile (or fetch) the kernel of a stage-scheduled complex64 pass and load
 // it into the current device.  Returns nullptr and fills `err` on failure.
-const JitKernel* jit_pass_kernel(const Pass& p, std::string& err) {
+const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, std::string& err) {
     if (!p.staged || (p.g.T != 12 && p.g.T != 13)) {
         err = "jit: only stage-scheduled passes of tile width 12-13";
         return nullptr;
     }
-    std::string src = generate(p, p.epilogue, err);
+    std::string src = generate(p, p.epilogue, nbuf, err);
     if (src.empty()) return nullptr;
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_cache.find(src);
@@ -649,7 +678,7 @@ const JitKernel* jit_pass_kernel(const Pass& p, std::string& err) {
         return nullptr;
     }
     k->threads = 1 << (p.g.T - 5);
-    k->smem = (size_t)8 << p.g.T;
+    k->smem = (size_t)(nbuf == 2 ? 16 : 8) << p.g.T;
     const char* names[2] = {"smoq_pass_e0", "smoq_pass_e1"};
     for (int v = 0; v < (p.epilogue ? 2 : 1); ++v) {
         cudaKernel_t kern = nullptr;

@@ -237,3 +237,25 @@ def test_engine_option_range(ctx):
     with pytest.raises(Exception):
         ctx.set_option(S._lib.OPT_ENGINE, 4)
     ctx.set_option(S._lib.OPT_ENGINE, -1)
+
+
+@pytest.mark.parametrize("tb64", [12, 13])
+def test_compiled_two_tile_buffers(ctx, tb64):
+    """engine 3 with two tile buffers per CTA (next tile prefetched): Strang XXZ
+    N=16 complex64 equals the oracle"""
+    N, dt, steps = 16, 0.05, 4
+    arr, n, gl = xxz(N, dt)
+    neel = sum(1 << (k - 1) for k in range(1, N + 1, 2))
+    psi = O.zero_state(N, neel)
+    both = O.make_gates(gl + gl[::-1])
+    for _ in range(steps):
+        O.trotter_step(psi, both, 2 * n, N)
+    ctx.set_option(S._lib.OPT_JIT_BUFFERS, 2)
+    try:
+        with engine(ctx, 3, tb64=tb64):
+            plan = S.TrotterPlan(ctx, N, [S.FastTrotterGate(i, U) for i, U in gl], order=2, dtype=S.C64)
+            st = S.CuState(ctx, N, S.C64, basis=neel)
+            plan.step(st, steps)
+            assert rel(st.download().astype(complex), psi) < 1e-4
+    finally:
+        ctx.set_option(S._lib.OPT_JIT_BUFFERS, 1)
