@@ -276,6 +276,55 @@ def vqe_workload(args):
     return 0
 
 
+def vqe_jobs_workload(args):
+    """Batched uneven circuits: 256 circuits, N ~ U{10..20}, depth ~ U{4..16} layers of
+    [Ry all; Rz all; CZ ladder] (seeded), TFIM H = -sum ZZ - sum X each, one energy +
+    adjoint gradient per circuit, through smoq_energy_grad_jobs.  metric =
+    full gradients per second (one gradient = all of one circuit's parameters).
+    The jobs run in order on the library stream."""
+    import torch
+    import pysmoq as S
+    ctx = S.Context(0)
+    rng = np.random.default_rng(SEED)
+    jobs, nparams = [], 0
+    for _ in range(256):
+        N = int(rng.integers(10, 21))
+        L = int(rng.integers(4, 17))
+        ops, idx = [], 1
+        for _ in range(L):
+            rot, idx = S.single_qubit_rotation_layer(N, idx, gates=("ry", "rz"))
+            ops += rot + S.entangling_layer(N, "chain", "cz")
+        circ = S.ParameterizedCircuit(N, ops)
+        theta = rng.uniform(0, 2 * np.pi, size=circ.n_params)
+        jobs.append((circ, S.PauliSum.tfim(N), theta))
+        nparams += circ.n_params
+    res = {}
+    for name, dt in (("c64", S.C64), ("c128", S.C128)):
+        for _ in range(max(1, args.warmup)):
+            S.energy_and_gradient_jobs(ctx, jobs[:32], dtype=dt)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            E, G = S.energy_and_gradient_jobs(ctx, jobs, dtype=dt)
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        res[name] = (len(jobs) * args.steps / sec, E, G, sec)
+    err_e = float(np.max(np.abs(res["c64"][1] - res["c128"][1])))
+    err_g = float(max(np.max(np.abs(a - b)) for a, b in zip(res["c64"][2], res["c128"][2])))
+    line = {"metric": "vqe_gradients_per_s", "value": res["c64"][0], "unit": "gradients/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * res["c64"][3] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {"workload": "vqe_256_uneven_circuits_n10_20_depth4_16", "circuits": len(jobs),
+                       "params_total": nparams, "gradient": "adjoint",
+                       "timing": "host wall clock around the call (returns after all jobs synchronised)"},
+            "c128_gradients_per_s": res["c128"][0],
+            "param_gradients_per_s_c64": nparams * args.steps / res["c64"][3],
+            "energy_abs_err_c64_vs_c128": err_e, "grad_max_abs_err_c64_vs_c128": err_g}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
 def bandwidth_workload(args):
     """32 GiB single-state sweeps: N=32 complex64 and N=31 complex128, 20 layers of
     [Rx, Ry, Rz on every qubit (seeded angles); Rzz on a seeded random perfect
@@ -283,6 +332,8 @@ def bandwidth_workload(args):
     import torch
     import pysmoq as S
     ctx = S.Context(0)
+    if args.engine >= 0:
+        ctx.set_option(S._lib.OPT_ENGINE, args.engine)
     peak, peak_kind = measured_peak()
     out = {}
     for N, dt, name in ((32, S.C64, "n32_c64"), (31, S.C128, "n31_c128")):
@@ -312,7 +363,8 @@ def bandwidth_workload(args):
         st.close()
     line = {"metric": "hbm_gbs_per_sweep", "value": out["n32_c64"]["hbm_gbs"], "unit": "GB/s", "n_gpus": 1,
             "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "c64", "data": "synthetic", "config": {"workload": "random_rxryrz_rzz_depth20_32GiB"},
+            "dtype": "c64", "data": "synthetic",
+            "config": {"workload": "random_rxryrz_rzz_depth20_32GiB", "engine": args.engine},
             "peak": peak, "peak_kind": peak_kind, "runs": out}
     print(json.dumps(line))
     ctx.close()
@@ -332,7 +384,7 @@ def main():
     ap.add_argument("--tile-bits", type=int, default=0, help="complex64 tile width (0 = library default)")
     ap.add_argument("--engine", type=int, default=-1, help="fused-pass engine (-1 = library default)")
     ap.add_argument("--jit-buffers", type=int, default=1, help="compiled pass kernels: tile buffers per CTA (1, 2)")
-    ap.add_argument("--workload", default="trotter", choices=["trotter", "vqe", "bandwidth"],
+    ap.add_argument("--workload", default="trotter", choices=["trotter", "vqe", "vqe_jobs", "bandwidth"],
                     help="trotter: the headline line; vqe / bandwidth: the gradient and 32 GiB sweep figures")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -341,6 +393,8 @@ def main():
         return vqe_workload(args)
     if args.workload == "bandwidth":
         return bandwidth_workload(args)
+    if args.workload == "vqe_jobs":
+        return vqe_jobs_workload(args)
 
     ws, rank, local = dist_env()
     import torch

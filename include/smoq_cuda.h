@@ -261,6 +261,26 @@ smoq_status smoq_energy(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* o
                         int n_params, const smoq_pauli_term* H, int nterms, int batch,
                         const double* theta, double* energies);
 
+/* Many independent VQE circuits at once (a batch of different circuits, sizes and
+ * Hamiltonians: the reference evaluates such batches one circuit at a time with
+ * calculate_gradients, cpuVariationalQuantumCircuitGradients.jl:88, inside a
+ * Threads.@threads loop).  Each job is one circuit with one parameter vector;
+ * grad may be NULL (energy only).  The jobs run in submission order on the
+ * context's stream; the call returns when all are done.  The first failing
+ * job's status is returned, with its index in the message. */
+typedef struct {
+    int N;                        /* qubits of this circuit */
+    const smoq_op* ops;           /* its gate list */
+    int n;
+    int n_params;
+    const smoq_pauli_term* H;     /* its Hamiltonian */
+    int nterms;
+    const double* theta;          /* n_params values */
+    double* energy;               /* host, 1 value */
+    double* grad;                 /* host, n_params values, or NULL */
+} smoq_vqe_job;
+smoq_status smoq_energy_grad_jobs(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vqe_job* jobs, int njobs);
+
 /* ------------------------------------------------- host-only introspection */
 /* No counterpart in the reference.  Runs the fused-pass planner (host code,
  * no GPU or context needed) on a gate sequence exactly as

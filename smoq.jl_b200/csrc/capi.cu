@@ -74,6 +74,8 @@ static smoq_status sync_check(smoq_ctx* ctx) {
     if (h != 0) {
         CK(ctx, cudaMemset(ctx->d_err, 0, sizeof(int32_t)));
         if (h == DEVERR_TIMEOUT) return fail(ctx, SMOQ_ERR_TIMEOUT, "a bounded device wait ran out");
+        if ((h & 255) == DEVERR_BOUNDS)
+            return fail(ctx, SMOQ_ERR_CUDA, "device bounds check failed at site " + std::to_string(h >> 8));
         return fail(ctx, SMOQ_ERR_BADINPUT, "device-side input check failed");
     }
     return SMOQ_OK;
@@ -212,6 +214,7 @@ smoq_status smoq_ctx_create(int device, smoq_ctx** out) {
     if (tile_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (regtile_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (stage_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
+    if (vqe_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (ensure_scratch(ctx.get(), 1 << 17) != SMOQ_OK) return SMOQ_ERR_OOM;
     if (ensure_pinned(ctx.get(), 1 << 20) != SMOQ_OK) return SMOQ_ERR_OOM;
     *out = ctx.release();

@@ -8,7 +8,17 @@
 
 namespace smoq {
 
-enum : int32_t { DEVERR_TIMEOUT = 1, DEVERR_BADINPUT = 2 };
+enum : int32_t { DEVERR_TIMEOUT = 1, DEVERR_BADINPUT = 2, DEVERR_BOUNDS = 3 };
+
+// Diagnostic builds (-DSMOQ_DEVICE_CHECKS): kernels test the extent of every
+// bulk copy and partial-sum index they are about to issue, record a violation
+// as DEVERR_BOUNDS | site << 8 in the error word and skip the access.
+#ifdef SMOQ_DEVICE_CHECKS
+#define SMOQ_INBOUNDS(cond, err, site) \
+    ((cond) ? true : ((err) ? (atomicExch((err), DEVERR_BOUNDS | ((site) << 8)), false) : false))
+#else
+#define SMOQ_INBOUNDS(cond, err, site) true
+#endif
 
 template <typename R> struct CT;
 template <> struct CT<float> { using T = float2; };

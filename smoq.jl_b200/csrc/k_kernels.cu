@@ -98,7 +98,8 @@ __global__ void __launch_bounds__(TILE_THREADS) tile_pass_kernel(const TileArgs 
         for (uint32_t s = tid; s < nseg; s += blockDim.x) {
             uint64_t off = base;
             for (int m = 0; m < H; ++m) off |= (uint64_t)((s >> m) & 1) << a.g.hb[m];
-            bulk_g2s(tile + ((size_t)s << L), gs + off, seg_bytes, &bar);
+            if (SMOQ_INBOUNDS(b * a.tiles_per_state < a.ntiles && off + (1ull << L) <= (uint64_t)a.state_len, a.err, 1))
+                bulk_g2s(tile + ((size_t)s << L), gs + off, seg_bytes, &bar);
         }
         const bool ok = mbar_wait_bounded(&bar, phase, a.err);
         if (!__syncthreads_and(ok)) {
@@ -173,7 +174,8 @@ __global__ void __launch_bounds__(TILE_THREADS) tile_pass_kernel(const TileArgs 
         for (uint32_t s = tid; s < nseg; s += blockDim.x) {
             uint64_t off = base;
             for (int m = 0; m < H; ++m) off |= (uint64_t)((s >> m) & 1) << a.g.hb[m];
-            bulk_s2g(gs + off, tile + ((size_t)s << L), seg_bytes);
+            if (SMOQ_INBOUNDS(b * a.tiles_per_state < a.ntiles && off + (1ull << L) <= (uint64_t)a.state_len, a.err, 2))
+                bulk_s2g(gs + off, tile + ((size_t)s << L), seg_bytes);
         }
         bulk_commit();
         bulk_wait_read0();

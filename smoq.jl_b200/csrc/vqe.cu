@@ -22,6 +22,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <string>
 #include <vector>
 #include "smoq_internal.h"
 #include "k_common.cuh"
@@ -138,6 +139,7 @@ struct AdjArgs {
     TileArgs a;      // a.psi = phi
     void* lam;
     double* partials;
+    int64_t n_partials;  // entries of partials (diagnostic bounds checks)
     int32_t n_inner;
 };
 
@@ -171,6 +173,7 @@ __global__ void __launch_bounds__(256) adj_tile_kernel(const AdjArgs A) {
             const uint32_t sg = s < nseg ? s : s - nseg;
             uint64_t off = base;
             for (int m = 0; m < H; ++m) off |= (uint64_t)((sg >> m) & 1) << a.g.hb[m];
+            if (!SMOQ_INBOUNDS(off + (1ull << L) <= (uint64_t)a.state_len, a.err, 3)) continue;
             if (s < nseg) bulk_g2s(tP + ((size_t)sg << L), gP + off, seg_bytes, &bar);
             else bulk_g2s(tL + ((size_t)sg << L), gL + off, seg_bytes, &bar);
         }
@@ -190,7 +193,9 @@ __global__ void __launch_bounds__(256) adj_tile_kernel(const AdjArgs A) {
                 if (tid == 0) {
                     double s = 0;
                     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-                    A.partials[(size_t)t * A.n_inner + op.perm[0]] = s;
+                    const int64_t pi = t * A.n_inner + op.perm[0];
+                    if (SMOQ_INBOUNDS(pi >= 0 && pi < A.n_partials && op.perm[0] < A.n_inner, a.err, 4))
+                        A.partials[pi] = s;
                 }
             } else if (op.kind == OPK_DIAG) {
                 adj_diag<R>(op, tP, amps, base);
@@ -207,6 +212,7 @@ __global__ void __launch_bounds__(256) adj_tile_kernel(const AdjArgs A) {
             const uint32_t sg = s < nseg ? s : s - nseg;
             uint64_t off = base;
             for (int m = 0; m < H; ++m) off |= (uint64_t)((sg >> m) & 1) << a.g.hb[m];
+            if (!SMOQ_INBOUNDS(off + (1ull << L) <= (uint64_t)a.state_len, a.err, 5)) continue;
             if (s < nseg) bulk_s2g(gP + off, tP + ((size_t)sg << L), seg_bytes);
             else bulk_s2g(gL + off, tL + ((size_t)sg << L), seg_bytes);
         }
@@ -272,6 +278,11 @@ GateIR dagger(const GateIR& g) {
         for (int c = 0; c < dim; ++c) d.m[r * dim + c] = std::conj(g.m[c * dim + r]);
     return d;
 }
+
+// shared memory of the widest adjoint tile: two states of 2^13 complex64 or 2^12
+// complex128 amplitudes (tile widths up to 14 / 13, one bit narrower for two states)
+constexpr size_t kAdjMaxSmem = (size_t)2 * 8 << 13;
+static_assert(((size_t)2 * 16 << 12) == kAdjMaxSmem, "same limit for both precisions");
 
 struct Work {
     smoq_state phi, lam;
@@ -434,16 +445,15 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
             A.a.ep.npop = 0;
             A.lam = w.lam.ptr;
             A.partials = d_part + off[i];
+            A.n_partials = (int64_t)(off[i + 1] - off[i]);
             A.n_inner = (int32_t)std::max<size_t>(1, slot_global[i].size());
             const size_t smem = (size_t)2 * w.phi.amp_bytes() << p.g.T;
             int grid = (int)std::min<int64_t>(A.a.ntiles, (int64_t)ctx->num_sms * 2);
-            if (dtype == SMOQ_C64) {
-                VCK(cudaFuncSetAttribute(adj_tile_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                adj_tile_kernel<float><<<grid, 256, smem, ctx->stream>>>(A);
-            } else {
-                VCK(cudaFuncSetAttribute(adj_tile_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                adj_tile_kernel<double><<<grid, 256, smem, ctx->stream>>>(A);
-            }
+            // (the kernels' shared-memory limit is set once per context, vqe_kernels_init:
+            // setting it per launch would race between contexts driven from several threads)
+            if (smem > kAdjMaxSmem) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "adjoint tile too wide");
+            if (dtype == SMOQ_C64) adj_tile_kernel<float><<<grid, 256, smem, ctx->stream>>>(A);
+            else adj_tile_kernel<double><<<grid, 256, smem, ctx->stream>>>(A);
             ctx->launches++;
             ctx->tile_passes++;
             VCK(cudaGetLastError());
@@ -457,6 +467,9 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
         VCK(cudaMemcpy(&herr, ctx->d_err, sizeof(herr), cudaMemcpyDeviceToHost));
         if (herr) {
             VCK(cudaMemset(ctx->d_err, 0, sizeof(int32_t)));
+            if ((herr & 255) == DEVERR_BOUNDS)
+                return smoq_internal_fail(ctx, SMOQ_ERR_CUDA,
+                                          ("device bounds check failed at site " + std::to_string(herr >> 8)).c_str());
             return smoq_internal_fail(ctx, SMOQ_ERR_TIMEOUT, "a bounded device wait ran out");
         }
         for (size_t i = 0; i < passes.size(); ++i) {
@@ -485,4 +498,35 @@ extern "C" smoq_status smoq_energy(smoq_ctx* ctx, int N, smoq_dtype dtype, const
                                    double* energies) {
     if (!energies) return ctx ? smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "null output") : SMOQ_ERR_BADINPUT;
     return vqe_run(ctx, N, dtype, ops, n, n_params, H, nterms, batch, theta, energies, nullptr);
+}
+
+// once per context, before any launch (and never during capture)
+cudaError_t smoq::vqe_kernels_init(smoq_ctx* ctx) {
+    (void)ctx;
+    cudaError_t e = cudaFuncSetAttribute(adj_tile_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kAdjMaxSmem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(adj_tile_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kAdjMaxSmem);
+}
+
+// ---------------------------------------------------------------- many circuits
+// Independent VQE jobs (each its own circuit, size and Hamiltonian), run in
+// submission order on the context's stream; each job's passes fill the GPU by
+// themselves from N of about 16 up (smaller states leave most SMs idle).
+extern "C" smoq_status smoq_energy_grad_jobs(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vqe_job* jobs, int njobs) {
+    if (!ctx) return SMOQ_ERR_BADINPUT;
+    if (njobs < 0 || (njobs > 0 && !jobs)) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "bad job list");
+    for (int j = 0; j < njobs; ++j)
+        if (!jobs[j].energy) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "job without energy output");
+    for (int j = 0; j < njobs; ++j) {
+        const smoq_vqe_job& J = jobs[j];
+        const smoq_status s = vqe_run(ctx, J.N, dtype, J.ops, J.n, J.n_params, J.H, J.nterms, 1, J.theta, J.energy,
+                                      J.grad);
+        if (s != SMOQ_OK) {
+            const std::string why = "job " + std::to_string(j) + ": " + smoq_last_error(ctx);
+            return smoq_internal_fail(ctx, s, why.c_str());
+        }
+    }
+    return SMOQ_OK;
 }

@@ -636,6 +636,29 @@ def energy_and_gradient(ctx: Context, circuit: ParameterizedCircuit, H: PauliSum
     return e, g
 
 
+def energy_and_gradient_jobs(ctx: Context, jobs, dtype: int = C128, gradient: bool = True):
+    """Many independent circuits at once: jobs = [(circuit, PauliSum, theta), ...],
+    each its own size and Hamiltonian.  Returns (energies[njobs], [grad arrays])."""
+    keep, arr = [], (_lib.SmoqVqeJob * max(1, len(jobs)))()
+    e = np.empty(len(jobs))
+    grads = []
+    for j, (circ, H, theta) in enumerate(jobs):
+        ops = circuit_to_c_ops(circ.operations)
+        terms = H.c_terms()
+        th = np.ascontiguousarray(theta, dtype=np.float64).reshape(-1)
+        if th.size != circ.n_params:
+            raise ValueError(f"job {j}: theta has {th.size} values, the circuit {circ.n_params} parameters")
+        g = np.zeros(max(1, circ.n_params))
+        keep += [ops, terms, th, g]
+        grads.append(g[:circ.n_params])
+        arr[j] = _lib.SmoqVqeJob(circ.N, C.cast(ops, C.POINTER(_lib.SmoqOp)), len(circ.operations), circ.n_params,
+                                 C.cast(terms, C.POINTER(_lib.SmoqPauliTerm)), len(H.terms), dptr(th),
+                                 C.cast(C.c_void_p(e.ctypes.data + 8 * j), C.POINTER(C.c_double)),
+                                 dptr(g) if gradient else None)
+    ck(lib.smoq_energy_grad_jobs(ctx.h, dtype, arr, len(jobs)), ctx.h, "energy_grad_jobs")
+    return e, grads
+
+
 # ------------------------------------------------------ planner introspection
 def debug_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtype: int = C128, tile_bits: int = 12,
                low_bits: int = 4, engine: int = 1):

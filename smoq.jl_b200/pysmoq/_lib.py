@@ -39,6 +39,12 @@ class SmoqPauliTerm(C.Structure):
     _fields_ = [("coef", C.c_double), ("xmask", C.c_uint64), ("zmask", C.c_uint64)]
 
 
+class SmoqVqeJob(C.Structure):
+    _fields_ = [("N", C.c_int), ("ops", C.POINTER(SmoqOp)), ("n", C.c_int), ("n_params", C.c_int),
+                ("H", C.POINTER(SmoqPauliTerm)), ("nterms", C.c_int), ("theta", C.POINTER(C.c_double)),
+                ("energy", C.POINTER(C.c_double)), ("grad", C.POINTER(C.c_double))]
+
+
 class SmoqPassInfo(C.Structure):
     _fields_ = [("T", C.c_int32), ("L", C.c_int32), ("H", C.c_int32), ("nops", C.c_int32), ("hb", C.c_int32 * 24)]
 
@@ -130,6 +136,7 @@ _SIGS = {
     "smoq_energy_grad": [_vp, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, C.c_int, C.POINTER(SmoqPauliTerm),
                          C.c_int, C.c_int, _dp, _dp, _dp],
     "smoq_jit_available": [],
+    "smoq_energy_grad_jobs": [_vp, C.c_int, C.POINTER(SmoqVqeJob), C.c_int],
     "smoq_debug_compile_plan": [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, _dp, C.c_int, _ip,
                                 C.c_char_p, C.c_int],
     "smoq_debug_plan_sequence": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, _dp,

@@ -106,3 +106,29 @@ def test_gradient_configuration_n24(ctx):
     es = S.energy(ctx, circ, H, shifted, dtype=S.C128)
     ps = (es[0::2] - es[1::2]) / 2
     assert np.max(np.abs(g128[0][idx] - ps)) < 1e-9
+
+
+def test_many_independent_circuits_vs_oracle(ctx):
+    """a batch of different circuits (sizes 5-14, depths 1-4, own Hamiltonians and
+    parameters) through smoq_energy_grad_jobs: every energy and gradient equals
+    the oracle's (energy, parameter-shift gradient) for that circuit"""
+    rng = np.random.default_rng(7)
+    jobs, refs = [], []
+    for j in range(12):
+        N = int(rng.integers(5, 12)) if j < 10 else 13 + (j - 10)   # the last two span several tiles
+        L = int(rng.integers(1, 5)) if j < 10 else 2
+        circ, theta = hea(N, L, seed=100 + j)
+        terms = tfim_terms(N)
+        if j % 3 == 1:  # a different Hamiltonian for some jobs: XX bonds and Z fields
+            terms = [(0.7, {i: "X", i + 1: "X"}) for i in range(1, N)] + [(-0.3, {i: "Z"}) for i in range(1, N + 1)]
+        jobs.append((circ, S.PauliSum(terms), theta))
+        oo = oracle_ops(circ)
+        arr = O.make_ops(oo)
+        refs.append((O.energy(arr, len(oo), theta, N, terms), O.grad(arr, len(oo), theta, N, terms, method="ps")))
+    e, g = S.energy_and_gradient_jobs(ctx, jobs, dtype=S.C128)
+    for j, (er, gr) in enumerate(refs):
+        assert abs(e[j] - er) < 1e-10, j
+        assert np.max(np.abs(g[j] - gr)) < 1e-9, j
+    e64, g64 = S.energy_and_gradient_jobs(ctx, jobs, dtype=S.C64)
+    for j, (er, gr) in enumerate(refs):
+        assert abs(e64[j] - er) < 1e-4 and np.max(np.abs(g64[j] - gr)) < 1e-3
