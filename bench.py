@@ -334,6 +334,8 @@ def bandwidth_workload(args):
     ctx = S.Context(0)
     if args.engine >= 0:
         ctx.set_option(S._lib.OPT_ENGINE, args.engine)
+    if args.jit_packed:
+        ctx.set_option(S._lib.OPT_JIT_PACKED, args.jit_packed)
     peak, peak_kind = measured_peak()
     out = {}
     for N, dt, name in ((32, S.C64, "n32_c64"), (31, S.C128, "n31_c128")):
@@ -384,6 +386,7 @@ def main():
     ap.add_argument("--tile-bits", type=int, default=0, help="complex64 tile width (0 = library default)")
     ap.add_argument("--engine", type=int, default=-1, help="fused-pass engine (-1 = library default)")
     ap.add_argument("--jit-buffers", type=int, default=1, help="compiled pass kernels: tile buffers per CTA (1, 2)")
+    ap.add_argument("--jit-packed", type=int, default=0, help="compiled pass kernels: FP32x2 arithmetic (1) or scalar (0)")
     ap.add_argument("--workload", default="trotter", choices=["trotter", "vqe", "vqe_jobs", "bandwidth"],
                     help="trotter: the headline line; vqe / bandwidth: the gradient and 32 GiB sweep figures")
     args = ap.parse_args()
@@ -419,6 +422,8 @@ def main():
         ctx.set_option(S._lib.OPT_ENGINE, args.engine)
     if args.jit_buffers != 1:
         ctx.set_option(S._lib.OPT_JIT_BUFFERS, args.jit_buffers)
+    if args.jit_packed:
+        ctx.set_option(S._lib.OPT_JIT_PACKED, args.jit_packed)
     N = args.n_qubits
     tsteps = args.trotter_steps
     gate_apps = tsteps * 2 * (N + 3 * (N - 1))

@@ -259,3 +259,24 @@ def test_compiled_two_tile_buffers(ctx, tb64):
             assert rel(st.download().astype(complex), psi) < 1e-4
     finally:
         ctx.set_option(S._lib.OPT_JIT_BUFFERS, 1)
+
+
+def test_compiled_fp32x2_arithmetic(ctx):
+    """engine 3 with FP32x2 arithmetic (SMOQ_OPT_JIT_PACKED): random circuit on a
+    random state equals the oracle"""
+    N, seed = 14, 11
+    g_ops, o_ops = random_circuit(N, 200, seed)
+    rng = np.random.default_rng(seed)
+    psi = rng.normal(size=1 << N) + 1j * rng.normal(size=1 << N)
+    psi /= np.linalg.norm(psi)
+    want = psi.copy()
+    O.apply_circuit(want, O.make_ops(o_ops), len(o_ops), np.zeros(1), N)
+    ctx.set_option(S._lib.OPT_JIT_PACKED, 1)
+    try:
+        with engine(ctx, 3):
+            st = S.CuState(ctx, N, S.C64, basis=None)
+            st.upload(psi.astype(np.complex64))
+            S.apply_circuit(st, S.ParameterizedCircuit(N, g_ops), np.zeros(1))
+            assert rel(st.download().astype(complex), want) < 5e-5
+    finally:
+        ctx.set_option(S._lib.OPT_JIT_PACKED, 0)
