@@ -384,6 +384,7 @@ def main():
     ap.add_argument("--n-qubits", type=int, default=N_QUBITS)
     ap.add_argument("--trotter-steps", type=int, default=STEPS)
     ap.add_argument("--tile-bits", type=int, default=0, help="complex64 tile width (0 = library default)")
+    ap.add_argument("--low-bits", type=int, default=0, help="complex64 contiguous low qubits per tile segment (0 = default)")
     ap.add_argument("--engine", type=int, default=-1, help="fused-pass engine (-1 = library default)")
     ap.add_argument("--jit-buffers", type=int, default=1, help="compiled pass kernels: tile buffers per CTA (1, 2)")
     ap.add_argument("--jit-packed", type=int, default=0, help="compiled pass kernels: FP32x2 arithmetic (1) or scalar (0)")
@@ -418,6 +419,8 @@ def main():
     eng = resolve_engine(S, args.engine)
     if args.tile_bits:
         ctx.set_option(S._lib.OPT_TILE_BITS_C64, args.tile_bits)
+    if args.low_bits:
+        ctx.set_option(S._lib.OPT_LOW_BITS_C64, args.low_bits)
     if args.engine >= 0:
         ctx.set_option(S._lib.OPT_ENGINE, args.engine)
     if args.jit_buffers != 1:
@@ -519,7 +522,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
                 "data": "synthetic",
                 "config": {"workload": workload, "N": N, "dt": DT, "trotter_steps": tsteps,
-                           "tile_bits_c64": args.tile_bits or 13, "engine": eng,
+                           "tile_bits_c64": args.tile_bits or 13, "low_bits_c64": args.low_bits or 5, "engine": eng,
                            "record_every": RECORD_EVERY, "gate_apps_per_step": gate_apps,
                            "state_bytes": (1 << N) * 8, "l2_policy": "inputs larger than L2 (2 GiB state)",
                            "parallelism": "replicas" if ws > 1 else "single_gpu",

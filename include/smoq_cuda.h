@@ -284,6 +284,34 @@ typedef struct {
 } smoq_vqe_job;
 smoq_status smoq_energy_grad_jobs(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vqe_job* jobs, int njobs);
 
+/* out = H in for every state of the batch (H = sum of Pauli strings, smoq_pauli_term);
+ * expect[b] = Re <in_b|H|in_b> (host, may be NULL).  The Hamiltonian apply of
+ * apply_hamiltonian_bitwise! (cpuQuantumChannelUnitaryEvolutionChebyshev.jl:55) and
+ * apply_H_xxz! / apply_H_ising! (cpuQuantumStateLanczos.jl:157,220), for any Pauli sum:
+ * the building block of Chebyshev and Lanczos.  in and out: same shape, not aliased. */
+smoq_status smoq_apply_pauli_sum(smoq_state* in, smoq_state* out, const smoq_pauli_term* H, int nterms,
+                                 double* expect);
+
+/* ------------------------------------------------- sampling and measurement */
+/* Born-rule sampling from |psi|^2: out[b * nshots + s] = basis index of shot s of
+ * state b.  Replaces sample_from_probabilities (cpuQuantumStateMeasurements.jl:203)
+ * and the benchmark's cumsum + searchsortedfirst shot loop
+ * (run_benchmark_smoq_Float64.jl:424-435).  Uniforms from Philox4x32-10 with key =
+ * seed and counter = (shot, stream + b): the same seed and stream give the same
+ * shots.  N >= 8.  out is a host array. */
+smoq_status smoq_sample(smoq_state* st, long long nshots, unsigned long long seed, unsigned long long stream,
+                        long long* out);
+/* projective_measurement_all! (cpuQuantumStateMeasurements.jl:484): one shot per
+ * state (shot 0 of the stream above), each state collapsed onto its outcome;
+ * outcome[b] = basis index (bit k-1 = qubit k).  N >= 8. */
+smoq_status smoq_measure_all(smoq_state* st, unsigned long long seed, unsigned long long stream,
+                             long long* outcome);
+/* _measure_z_single! (cpuQuantumStateMeasurements.jl:224): Z measurement of qubit q
+ * (0-based) of every state, collapse and renormalise; outcome[b] in {0, 1}.  The
+ * uniform is shot 0 of (seed, stream + b). */
+smoq_status smoq_measure_qubit(smoq_state* st, int q, unsigned long long seed, unsigned long long stream,
+                               int* outcome);
+
 /* ------------------------------------------------- host-only introspection */
 /* No counterpart in the reference.  Runs the fused-pass planner (host code,
  * no GPU or context needed) on a gate sequence exactly as

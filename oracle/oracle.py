@@ -89,6 +89,9 @@ _sig("so_grad_parameter_shift", [C.POINTER(Op), C.c_int, _dp, C.c_int, C.c_int, 
 _sig("so_grad_finite_difference", [C.POINTER(Op), C.c_int, _dp, C.c_int, C.c_int, C.c_int, _dp, C.c_char_p,
                                    C.c_double, C.POINTER(C.c_int), C.c_int, _dp])
 _sig("so_philox4x32_10", [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)])
+_sig("so_sample", [_cp, C.c_int, C.c_int64, C.c_uint64, C.c_uint64, C.POINTER(C.c_int64)])
+_sig("so_measure_all", [_cp, C.c_int, C.c_uint64, C.c_uint64], C.c_int64)
+_sig("so_measure_qubit", [_cp, C.c_int, C.c_int, C.c_uint64, C.c_uint64], C.c_int)
 _sig("so_u01_from_words", [C.c_uint32, C.c_uint32], C.c_double)
 _sig("so_mcwf_step", [_cp, C.c_int, C.POINTER(TrotterGate), C.c_int, C.POINTER(JumpOp), C.c_int, C.c_double,
                       C.c_uint64, C.c_uint64, C.c_uint64], C.c_int)
@@ -352,3 +355,20 @@ def dm_expect_zz(rho, i, j, N):
 
 def wtime():
     return L.so_wtime()
+
+
+def sample(psi, N, nshots, seed, stream=0):
+    """Born sampling, shot loop of run_benchmark_smoq_Float64.jl:424-435 (Philox draws)"""
+    out = np.empty(nshots, dtype=np.int64)
+    L.so_sample(_p(psi), N, nshots, seed, stream, out.ctypes.data_as(C.POINTER(C.c_int64)))
+    return out
+
+
+def measure_all(psi, N, seed, stream=0):
+    """projective_measurement_all! (cpuQuantumStateMeasurements.jl:484), in place"""
+    return int(L.so_measure_all(_p(psi), N, seed, stream))
+
+
+def measure_qubit(psi, k, N, seed, stream=0):
+    """_measure_z_single! (cpuQuantumStateMeasurements.jl:224), in place, k 1-based"""
+    return int(L.so_measure_qubit(_p(psi), k, N, seed, stream))

@@ -775,3 +775,67 @@ double so_expect_zz_rho(const C* rho, int a, int b, int N) {
         r += creal(rho[i * dim + i]) * (double)(1 - 2 * (((i >> (a - 1)) ^ (i >> (b - 1))) & 1));
     return r;
 }
+
+/* ========================================================================
+ * Born sampling and projective Z measurements
+ * (utils/cpu/cpuQuantumStateMeasurements.jl), with the uniforms drawn from
+ * Philox4x32-10 -- counter (shot_lo, shot_hi, stream_lo, stream_hi), key
+ * (seed_lo, seed_hi), u from the first two words -- so that the CUDA library
+ * can be checked draw for draw.
+ * ======================================================================== */
+static double shot_u(uint64_t seed, uint64_t shot, uint64_t stream) {
+    uint32_t ctr[4] = {(uint32_t)shot, (uint32_t)(shot >> 32), (uint32_t)stream, (uint32_t)(stream >> 32)};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t w[4];
+    so_philox4x32_10(ctr, key, w);
+    return so_u01_from_words(w[0], w[1]);
+}
+/* the benchmark's shot loop: cumprobs = cumsum(abs2.(psi)), idx =
+ * searchsortedfirst(cumprobs, r) - 1 (run_benchmark_smoq_Float64.jl:424-435);
+ * an r above the total takes the last index, as sample_from_probabilities (:203) */
+void so_sample(const so_cplx* psi, int N, int64_t nshots, uint64_t seed, uint64_t stream, int64_t* out) {
+    int64_t dim = 1LL << N;
+    double* cum = (double*)malloc(dim * sizeof(double));
+    double run = 0;
+    for (int64_t i = 0; i < dim; i++) {
+        run += abs2(psi[i]);
+        cum[i] = run;
+    }
+    for (int64_t s = 0; s < nshots; s++) {
+        double r = shot_u(seed, (uint64_t)s, stream);
+        int64_t lo = 0, hi = dim - 1;
+        while (lo < hi) {
+            int64_t mid = (lo + hi) >> 1;
+            if (cum[mid] >= r) hi = mid;
+            else lo = mid + 1;
+        }
+        out[s] = lo;
+    }
+    free(cum);
+}
+/* projective_measurement_all! (:484): one sample, collapse onto it */
+int64_t so_measure_all(so_cplx* psi, int N, uint64_t seed, uint64_t stream) {
+    int64_t idx;
+    so_sample(psi, N, 1, seed, stream, &idx);
+    int64_t dim = 1LL << N;
+    for (int64_t i = 0; i < dim; i++) psi[i] = 0;
+    psi[idx] = 1.0;
+    return idx;
+}
+/* _measure_z_single! (:224), k 1-based */
+int so_measure_qubit(so_cplx* psi, int k, int N, uint64_t seed, uint64_t stream) {
+    int64_t dim = 1LL << N, mask = 1LL << (k - 1);
+    double prob_0 = 0;
+    for (int64_t i = 0; i < dim; i++)
+        if ((i & mask) == 0) prob_0 += abs2(psi[i]);
+    int outcome = shot_u(seed, 0, stream) < prob_0 ? 0 : 1;
+    double norm_sq = 0;
+    for (int64_t i = 0; i < dim; i++) {
+        int bit = (int)((i >> (k - 1)) & 1);
+        if (bit != outcome) psi[i] = 0;
+        else norm_sq += abs2(psi[i]);
+    }
+    double f = 1.0 / sqrt(norm_sq);
+    for (int64_t i = 0; i < dim; i++) psi[i] *= f;
+    return outcome;
+}

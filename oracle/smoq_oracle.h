@@ -163,6 +163,12 @@ double so_expect_zz_rho(const so_cplx* rho, int i, int j, int N);
 /* timing helper for the CPU baseline */
 double so_wtime(void);
 
+/* ---- Born sampling / projective Z measurement: utils/cpu/cpuQuantumStateMeasurements.jl ---- */
+/* u from Philox4x32-10, counter (shot, stream), key seed (the CUDA library's draws) */
+void so_sample(const so_cplx* psi, int N, int64_t nshots, uint64_t seed, uint64_t stream, int64_t* out); /* :203 */
+int64_t so_measure_all(so_cplx* psi, int N, uint64_t seed, uint64_t stream);                             /* :484 */
+int so_measure_qubit(so_cplx* psi, int k, int N, uint64_t seed, uint64_t stream);                         /* :224 */
+
 #ifdef __cplusplus
 }
 #endif

@@ -530,3 +530,66 @@ extern "C" smoq_status smoq_energy_grad_jobs(smoq_ctx* ctx, smoq_dtype dtype, co
     }
     return SMOQ_OK;
 }
+
+// ---------------------------------------------------------------- H psi
+// out = H in for every state of the batch, H = sum_t c_t P_t (Pauli strings);
+// expect[b] = Re <in_b|H|in_b> when expect != NULL.  The pull-pattern
+// Hamiltonian apply of apply_hamiltonian_bitwise!
+// (cpuQuantumChannelUnitaryEvolutionChebyshev.jl:55) and apply_H_xxz! /
+// apply_H_ising! (cpuQuantumStateLanczos.jl:157,220), for any Pauli sum.
+extern "C" smoq_status smoq_apply_pauli_sum(smoq_state* in, smoq_state* out, const smoq_pauli_term* H, int nterms,
+                                            double* expect) {
+    if (!in || !out || !in->ctx) return SMOQ_ERR_BADINPUT;
+    smoq_ctx* ctx = in->ctx;
+    if (out->ctx != ctx || out->N != in->N || out->dtype != in->dtype || out->batch != in->batch)
+        return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "apply_pauli_sum: in/out states differ in shape");
+    if (out->ptr == in->ptr) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "apply_pauli_sum: out must not alias in");
+    if (nterms < 1 || !H) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "apply_pauli_sum: no terms");
+    const int N = in->N;
+    const uint64_t lim = (N >= 64) ? ~0ull : ((1ull << N) - 1);
+    std::vector<HamTerm> ht(nterms);
+    for (int t = 0; t < nterms; ++t) {
+        if ((H[t].xmask | H[t].zmask) & ~lim)
+            return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "Hamiltonian term acts beyond N");
+        ht[t].coef = H[t].coef;
+        ht[t].x = H[t].xmask;
+        ht[t].z = H[t].zmask;
+        ht[t].ny = __builtin_popcountll(H[t].xmask & H[t].zmask);
+    }
+    const int64_t len = (int64_t)1 << N;
+    const int eblocks = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, (int64_t)ctx->num_sms * 8));
+    void* buf = nullptr;
+    const size_t tbytes = ht.size() * sizeof(HamTerm);
+    VCK(cudaMallocAsync(&buf, ((tbytes + 15) / 16) * 16 + (size_t)eblocks * in->batch * sizeof(double), ctx->stream));
+    HamTerm* d_terms = (HamTerm*)buf;
+    double* d_part = (double*)((char*)buf + ((tbytes + 15) / 16) * 16);
+    VCK(cudaMemcpyAsync(d_terms, ht.data(), tbytes, cudaMemcpyHostToDevice, ctx->stream));
+    const size_t amp = in->amp_bytes();
+    for (int b = 0; b < in->batch; ++b) {
+        const char* src = (const char*)in->ptr + (size_t)b * len * amp;
+        char* dst = (char*)out->ptr + (size_t)b * len * amp;
+        if (in->dtype == SMOQ_C64)
+            ham_apply_kernel<float><<<eblocks, 256, 0, ctx->stream>>>((const float2*)src, (float2*)dst, N, d_terms,
+                                                                      nterms, d_part + (size_t)b * eblocks);
+        else
+            ham_apply_kernel<double><<<eblocks, 256, 0, ctx->stream>>>((const double2*)src, (double2*)dst, N,
+                                                                       d_terms, nterms, d_part + (size_t)b * eblocks);
+        ctx->launches++;
+    }
+    cudaError_t e = cudaGetLastError();
+    std::vector<double> part;
+    if (e == cudaSuccess && expect) {
+        part.resize((size_t)eblocks * in->batch);
+        e = cudaMemcpyAsync(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    }
+    cudaFreeAsync(buf, ctx->stream);
+    if (e != cudaSuccess) return smoq_internal_cuda(ctx, e, "apply_pauli_sum");
+    VCK(cudaStreamSynchronize(ctx->stream));
+    if (expect)
+        for (int b = 0; b < in->batch; ++b) {
+            double s = 0;
+            for (int k = 0; k < eblocks; ++k) s += part[(size_t)b * eblocks + k];
+            expect[b] = s;
+        }
+    return SMOQ_OK;
+}

@@ -289,6 +289,33 @@ def expect_zstrings(psi: CuState, zmasks: Sequence[int]) -> np.ndarray:
     return out.reshape(psi.batch, len(m))
 
 
+def sample_bitstrings(psi: CuState, nshots: int, seed: int, stream: int = 0) -> np.ndarray:
+    """Born-rule shots (basis indices; bit k-1 = qubit k), [batch, nshots] or [nshots]."""
+    out = np.empty((psi.batch, nshots), dtype=np.int64)
+    ck(lib.smoq_sample(psi.h, nshots, seed, stream, out.ctypes.data_as(C.POINTER(C.c_longlong))), psi.ctx.h,
+       "sample")
+    return out[0] if psi.batch == 1 else out
+
+
+def projective_measurement_all(psi: CuState, N: int, seed: int, stream: int = 0):
+    """projective_measurement_all!(psi, N): (bitstring per qubit, collapsed psi)."""
+    _n(psi, N)
+    out = np.empty(psi.batch, dtype=np.int64)
+    ck(lib.smoq_measure_all(psi.h, seed, stream, out.ctypes.data_as(C.POINTER(C.c_longlong))), psi.ctx.h,
+       "projective_measurement_all")
+    bits = [[(int(o) >> (k - 1)) & 1 for k in range(1, N + 1)] for o in out]
+    return (bits[0] if psi.batch == 1 else bits), psi
+
+
+def measure_z(psi: CuState, k: int, N: int, seed: int, stream: int = 0):
+    """_measure_z_single!(psi, k, N): outcome 0/1 (per state), psi collapsed."""
+    _n(psi, N)
+    out = np.empty(psi.batch, dtype=np.int32)
+    ck(lib.smoq_measure_qubit(psi.h, k - 1, seed, stream, out.ctypes.data_as(C.POINTER(C.c_int))), psi.ctx.h,
+       "measure_z")
+    return int(out[0]) if psi.batch == 1 else out
+
+
 def population_excited_psi(psi: CuState, k: int, N: int):
     _n(psi, N)
     out = np.empty(psi.batch)
@@ -612,6 +639,15 @@ class PauliSum:
         for t, (c, x, z) in enumerate(self.terms):
             arr[t].coef, arr[t].xmask, arr[t].zmask = c, x, z
         return arr
+
+
+def apply_hamiltonian_bitwise(psi_out: CuState, psi_in: CuState, H: PauliSum):
+    """apply_hamiltonian_bitwise!(psi_out, psi_in, params): psi_out = H psi_in; returns
+    Re <psi_in|H|psi_in> (per state)."""
+    e = np.empty(psi_in.batch)
+    ck(lib.smoq_apply_pauli_sum(psi_in.h, psi_out.h, H.c_terms(), len(H.terms), dptr(e)), psi_in.ctx.h,
+       "apply_hamiltonian_bitwise")
+    return e[0] if psi_in.batch == 1 else e
 
 
 def energy(ctx: Context, circuit: ParameterizedCircuit, H: PauliSum, theta, dtype: int = C128):

@@ -136,6 +136,10 @@ _SIGS = {
     "smoq_energy_grad": [_vp, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, C.c_int, C.POINTER(SmoqPauliTerm),
                          C.c_int, C.c_int, _dp, _dp, _dp],
     "smoq_jit_available": [],
+    "smoq_apply_pauli_sum": [_vp, _vp, C.POINTER(SmoqPauliTerm), C.c_int, _dp],
+    "smoq_sample": [_vp, C.c_longlong, C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_longlong)],
+    "smoq_measure_all": [_vp, C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_longlong)],
+    "smoq_measure_qubit": [_vp, C.c_int, C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_int)],
     "smoq_energy_grad_jobs": [_vp, C.c_int, C.POINTER(SmoqVqeJob), C.c_int],
     "smoq_debug_compile_plan": [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, _dp, C.c_int, _ip,
                                 C.c_char_p, C.c_int],

@@ -282,3 +282,36 @@ def test_mcwf_converges_to_dm_small():
         m, s = z[-1, :, k - 1].mean(), z[-1, :, k - 1].std() / math.sqrt(ntraj)
         assert abs(m - O.dm_expect_z(rho, k, N)) < 5 * s + 2e-3, (k, m, O.dm_expect_z(rho, k, N), s)
     assert nj.sum() > 0
+
+
+def test_oracle_born_sampling_and_measurement():
+    """the oracle's Born sampling reproduces |psi|^2 (chi-square over 40k shots), its
+    draws are the Philox stream (u of shot s is the first uniform of counter (s, stream)),
+    and _measure_z_single! / projective_measurement_all! collapse as the reference does"""
+    N = 8
+    rng = np.random.default_rng(3)
+    psi = rng.normal(size=1 << N) + 1j * rng.normal(size=1 << N)
+    psi /= np.linalg.norm(psi)
+    p = np.abs(psi) ** 2
+    shots = O.sample(psi.copy(), N, 40000, seed=99, stream=5)
+    cnt = np.bincount(shots, minlength=1 << N)
+    chi2 = np.sum((cnt - 40000 * p) ** 2 / (40000 * p))
+    assert chi2 < (1 << N) + 6 * np.sqrt(2 * (1 << N))     # dof = 255, ~6 sigma
+    # shot s is the inverse CDF of the Philox uniform of (s, stream)
+    cum = np.cumsum(p)
+    for s in (0, 1, 7, 1234):
+        w = O.philox([s & 0xFFFFFFFF, s >> 32, 5, 0], [99, 0])
+        u = ((w[0] >> 5) * 67108864 + (w[1] >> 6)) / 9007199254740992.0
+        assert shots[s] == min(int(np.searchsorted(cum, u, side="left")), (1 << N) - 1)
+    # single-qubit measurement: outcome by u < P(0), collapse, renormalise
+    q = 3
+    phi = psi.copy()
+    o = O.measure_qubit(phi, q, N, seed=7, stream=2)
+    bits = (np.arange(1 << N) >> (q - 1)) & 1
+    want = np.where(bits == o, psi, 0)
+    want /= np.linalg.norm(want)
+    assert np.allclose(phi, want, atol=1e-14)
+    # all-qubit measurement: a basis state
+    phi = psi.copy()
+    idx = O.measure_all(phi, N, seed=7, stream=2)
+    assert phi[idx] == 1 and np.count_nonzero(phi) == 1
