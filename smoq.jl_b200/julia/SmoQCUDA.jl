@@ -14,7 +14,9 @@ export CuContext, CuState, apply_rx_psi!, apply_ry_psi!, apply_rz_psi!, apply_ha
        apply_rxx_psi!, apply_ryy_psi!, apply_rzz_psi!, apply_ccz_psi!, apply_toffoli_psi!,
        apply_sigma_minus_psi!, apply_sigma_plus_psi!, apply_sigma_z!, population_excited_psi,
        expect_local, expect_corr, get_expectation_pauli_string, get_norm, normalize_state!,
-       TrotterPlan, evolve_trotter_psi!, apply_fast_trotter_step_cpu!, energy_and_gradient
+       TrotterPlan, evolve_trotter_psi!, apply_fast_trotter_step_cpu!, energy_and_gradient,
+       energy_and_gradient_jobs, lindblad_mcwf_batched!, apply_hamiltonian_bitwise!, sample_bitstrings,
+       projective_measurement_all!, measure_z_single!, set_engine!
 
 const lib = joinpath(@__DIR__, "..", "lib", "libsmoq_cuda.so")
 const SMOQ_C64 = Cint(0)
@@ -184,5 +186,94 @@ end
 #       E, G = energy_and_gradient(ctx, N, ops, length(θ), H, reshape(θ, :, 1))
 #       return E[1], Δ -> (NoTangent(), Δ .* G[:, 1])
 #   end
+
+# ------------------------------------------------ many circuits (C4b)
+struct CVqeJob
+    N::Cint
+    ops::Ptr{COp}
+    n::Cint
+    n_params::Cint
+    H::Ptr{CPauliTerm}
+    nterms::Cint
+    theta::Ptr{Float64}
+    energy::Ptr{Float64}
+    grad::Ptr{Float64}
+end
+
+"jobs: Vector of (N, ops::Vector{COp}, n_params, H::Vector{CPauliTerm}, θ::Vector{Float64});
+returns (energies, grads) -- each circuit its own size and Hamiltonian"
+function energy_and_gradient_jobs(ctx::CuContext, jobs; dtype=SMOQ_C128)
+    E = Vector{Float64}(undef, length(jobs))
+    G = [Vector{Float64}(undef, j[3]) for j in jobs]
+    GC.@preserve jobs E G begin
+        cj = [CVqeJob(j[1], pointer(j[2]), length(j[2]), j[3], pointer(j[4]), length(j[4]), pointer(j[5]),
+                      pointer(E, i), pointer(G[i])) for (i, j) in enumerate(jobs)]
+        check(ccall((:smoq_energy_grad_jobs, lib), Cint, (Ptr{Cvoid}, Cint, Ptr{CVqeJob}, Cint),
+                    ctx.h, dtype, cj, length(cj)), ctx)
+    end
+    E, G
+end
+
+# ------------------------------------------------------------------ MCWF
+struct CJumpOp
+    type::Int32       # 0 sigma-, 1 sigma+, 2 sigma_z, 3 sigma_x
+    qubit::Int32      # 0-based
+    gamma::Float64
+end
+
+"evolve_mcwf_batched_trotter! (MonteCarloWaveFunction.jl:412) on the GPU: every state
+of ψ (batch = trajectories) evolves under `plan` (order 1) and `jumps`; returns the
+trajectory means of <Z_i> and <Z_i Z_{i+1}> every `record_every` steps and the jump counts."
+function lindblad_mcwf_batched!(ψ::CuState, plan::TrotterPlan, jumps::Vector{CJumpOp}, dt::Float64,
+                                seed::UInt64, steps::Int, record_every::Int)
+    nrec = steps ÷ record_every + 1
+    z = Matrix{Float64}(undef, ψ.N, nrec)
+    zz = Matrix{Float64}(undef, ψ.N - 1, nrec)
+    nj = Vector{Cint}(undef, ψ.batch)
+    check(ccall((:smoq_mcwf_run, lib), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{CJumpOp}, Cint, Cdouble, UInt64, UInt64, Cint, Cint,
+                 Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Cint}),
+                plan.h, ψ.h, jumps, length(jumps), dt, seed, 0, steps, record_every, z, zz, C_NULL, C_NULL, nj),
+          ψ.ctx)
+    z, zz, nj
+end
+
+# ------------------------------------------------ H ψ, sampling, measurement
+"apply_hamiltonian_bitwise!(ψ_out, ψ_in, params) -- Chebyshev.jl:55, for a Pauli sum; returns <ψ_in|H|ψ_in>"
+function apply_hamiltonian_bitwise!(ψout::CuState, ψin::CuState, H::Vector{CPauliTerm})
+    e = Vector{Float64}(undef, ψin.batch)
+    check(ccall((:smoq_apply_pauli_sum, lib), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{CPauliTerm}, Cint, Ptr{Float64}),
+                ψin.h, ψout.h, H, length(H), e), ψin.ctx)
+    ψin.batch == 1 ? e[1] : e
+end
+
+"Born shots (0-based basis indices), the benchmark's cumsum + searchsortedfirst loop"
+function sample_bitstrings(ψ::CuState, nshots::Int; seed::UInt64=UInt64(42), stream::UInt64=UInt64(0))
+    out = Matrix{Int64}(undef, nshots, ψ.batch)
+    check(ccall((:smoq_sample, lib), Cint, (Ptr{Cvoid}, Clonglong, Culonglong, Culonglong, Ptr{Int64}),
+                ψ.h, nshots, seed, stream, out), ψ.ctx)
+    out
+end
+
+"projective_measurement_all!(ψ, N) -- Measurements.jl:484: (bitstring, ψ collapsed)"
+function projective_measurement_all!(ψ::CuState, N::Int; seed::UInt64=UInt64(42), stream::UInt64=UInt64(0))
+    o = Vector{Int64}(undef, ψ.batch)
+    check(ccall((:smoq_measure_all, lib), Cint, (Ptr{Cvoid}, Culonglong, Culonglong, Ptr{Int64}),
+                ψ.h, seed, stream, o), ψ.ctx)
+    [(o[1] >> (k - 1)) & 1 for k in 1:N], ψ
+end
+
+"_measure_z_single!(ψ, k, N) -- Measurements.jl:224: outcome 0/1, ψ collapsed"
+function measure_z_single!(ψ::CuState, k::Int, N::Int; seed::UInt64=UInt64(42), stream::UInt64=UInt64(0))
+    o = Vector{Cint}(undef, ψ.batch)
+    check(ccall((:smoq_measure_qubit, lib), Cint, (Ptr{Cvoid}, Cint, Culonglong, Culonglong, Ptr{Cint}),
+                ψ.h, k - 1, seed, stream, o), ψ.ctx)
+    ψ.batch == 1 ? Int(o[1]) : Int.(o)
+end
+
+"fused-pass engine: -1 auto (default), 0 shared-memory sweeps, 1 register tiles, 2 stage
+sweeps, 3 compiled pass kernels"
+set_engine!(ctx::CuContext, e::Integer) =
+    check(ccall((:smoq_ctx_set_option, lib), Cint, (Ptr{Cvoid}, Cint, Clonglong), ctx.h, 7, e), ctx)
 
 end # module
