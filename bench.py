@@ -388,6 +388,7 @@ def main():
     ap.add_argument("--engine", type=int, default=-1, help="fused-pass engine (-1 = library default)")
     ap.add_argument("--jit-buffers", type=int, default=1, help="compiled pass kernels: tile buffers per CTA (1, 2)")
     ap.add_argument("--jit-packed", type=int, default=0, help="compiled pass kernels: FP32x2 arithmetic (1) or scalar (0)")
+    ap.add_argument("--jit-groups", type=int, default=2, help="compiled pass kernels: register groups per thread (1, 2)")
     ap.add_argument("--workload", default="trotter", choices=["trotter", "vqe", "vqe_jobs", "bandwidth"],
                     help="trotter: the headline line; vqe / bandwidth: the gradient and 32 GiB sweep figures")
     args = ap.parse_args()
@@ -427,6 +428,8 @@ def main():
         ctx.set_option(S._lib.OPT_JIT_BUFFERS, args.jit_buffers)
     if args.jit_packed:
         ctx.set_option(S._lib.OPT_JIT_PACKED, args.jit_packed)
+    if args.jit_groups != 2:
+        ctx.set_option(S._lib.OPT_JIT_GROUPS, args.jit_groups)
     N = args.n_qubits
     tsteps = args.trotter_steps
     gate_apps = tsteps * 2 * (N + 3 * (N - 1))

@@ -131,7 +131,7 @@ static smoq_status upload_program(smoq_ctx* ctx, DevProgram& P) {
     for (Pass& p : P.passes) {
         if (!p.want_jit || p.jit) continue;
         std::string why;
-        p.jit = jit_pass_kernel(p, ctx->jit_buffers, ctx->jit_packed != 0, why);
+        p.jit = jit_pass_kernel(p, ctx->jit_buffers, ctx->jit_packed != 0, ctx->jit_groups, why);
         if (!p.jit) return fail(ctx, SMOQ_ERR_UNSUPPORTED, "compiled pass kernel: " + why);
     }
     std::vector<DevOp> all;
@@ -268,6 +268,10 @@ smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long v) {
             ctx->engine = (int)v;
             break;
         case SMOQ_OPT_JIT_PACKED: ctx->jit_packed = v != 0; break;
+        case SMOQ_OPT_JIT_GROUPS:
+            if (v != 1 && v != 2) return fail(ctx, SMOQ_ERR_BADINPUT, "compiled-kernel register groups must be 1 or 2");
+            ctx->jit_groups = (int)v;
+            break;
         case SMOQ_OPT_JIT_BUFFERS:
             if (v != 1 && v != 2) return fail(ctx, SMOQ_ERR_BADINPUT, "compiled-kernel tile buffers must be 1 or 2");
             ctx->jit_buffers = (int)v;
@@ -589,7 +593,8 @@ smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tbits, int lbit
     for (const Pass& p : pl) {
         if (!p.want_jit) continue;
         std::string why, info;
-        if (!jit_check_pass(p, (flags & 2) ? 2 : 1, (flags & 4) != 0, why, nullptr, verbose ? &info : nullptr)) {
+        if (!jit_check_pass(p, (flags & 2) ? 2 : 1, (flags & 4) != 0, (flags & 8) ? 1 : 2, why, nullptr,
+                            verbose ? &info : nullptr)) {
             say(why);
             return why.rfind("NVRTC (", 0) == 0 ? SMOQ_ERR_UNSUPPORTED : SMOQ_ERR_BADINPUT;
         }

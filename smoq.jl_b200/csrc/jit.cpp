@@ -652,11 +652,13 @@ struct Gen {
 };
 
 // full source of the kernels for one pass
-std::string generate(const Pass& p, bool need_epi, int nbuf, bool packed, std::string& err) {
+std::string generate(const Pass& p, bool need_epi, int nbuf, bool packed, int groups, std::string& err) {
     const int N = p.g.N;
     const TileGeom& g = p.g;
     const int T = g.T;
-    const int G = 2, NT = 1 << (T - 5), MINB = T == 13 ? 2 : 4;
+    // G register groups of 16 amplitudes per thread, NT = 2^(T-4) / G threads
+    // register budget: 128 per thread with two groups, 64 with one
+    const int G = packed ? 2 : groups, NT = 1 << (T - 4 - (G - 1)), MINB = 65536 / (NT * (G == 2 ? 128 : 64));
     Gen gen(p, G, NT);
     std::ostringstream& o = gen.o;
     o << kPrelude;
@@ -771,7 +773,7 @@ std::string generate(const Pass& p, bool need_epi, int nbuf, bool packed, std::s
         else gen.stage(S, rl, members);
     }
     o << "    if (EPI) {\n"
-         "        constexpr int nb = NT == 128 ? 7 : 8;\n"
+         "        constexpr int nb = NT == 128 ? 7 : NT == 256 ? 8 : 9;\n"
          "        double acc[16];\n"
          "#pragma unroll\n"
          "        for (int q = 0; q < 16; ++q) acc[q] = 0.0;\n"
@@ -878,12 +880,13 @@ bool compile_cubin(const std::string& src, std::vector<char>& cubin, std::string
 
 // Generate and compile a staged complex64 pass without loading it (host only);
 // `info` (optional) receives the compiler's resource report.
-bool jit_check_pass(const Pass& p, int nbuf, bool packed, std::string& err, size_t* cubin_bytes, std::string* info) {
+bool jit_check_pass(const Pass& p, int nbuf, bool packed, int groups, std::string& err, size_t* cubin_bytes,
+                    std::string* info) {
     if (!p.staged || (p.g.T != 12 && p.g.T != 13)) {
         err = "jit: only stage-scheduled passes of tile width 12-13";
         return false;
     }
-    const std::string src = generate(p, p.epilogue, nbuf, packed, err);
+    const std::string src = generate(p, p.epilogue, nbuf, packed, groups, err);
     if (src.empty()) return false;
     std::vector<char> cubin;
     if (!compile_cubin(src, cubin, err, info)) return false;
@@ -893,12 +896,12 @@ bool jit_check_pass(const Pass& p, int nbuf, bool packed, std::string& err, size
 
 // Compile (or fetch) the kernel of a stage-scheduled complex64 pass and load
 // it into the current device.  Returns nullptr and fills `err` on failure.
-const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, std::string& err) {
+const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, int groups, std::string& err) {
     if (!p.staged || (p.g.T != 12 && p.g.T != 13)) {
         err = "jit: only stage-scheduled passes of tile width 12-13";
         return nullptr;
     }
-    std::string src = generate(p, p.epilogue, nbuf, packed, err);
+    std::string src = generate(p, p.epilogue, nbuf, packed, groups, err);
     if (src.empty()) return nullptr;
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_cache.find(src);
@@ -912,7 +915,7 @@ const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, std::stri
         err = std::string("cudaLibraryLoadData: ") + cudaGetErrorString(e);
         return nullptr;
     }
-    k->threads = 1 << (p.g.T - 5);
+    k->threads = 1 << (p.g.T - 4 - ((packed ? 2 : groups) - 1));
     k->smem = (size_t)(nbuf == 2 ? 16 : 8) << p.g.T;
     const char* names[2] = {"smoq_pass_e0", "smoq_pass_e1"};
     for (int v = 0; v < (p.epilogue ? 2 : 1); ++v) {

@@ -138,9 +138,10 @@ void schedule_regtile(Pass& p);
 void schedule_stages(Pass& p, int amp_bytes);
 void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op);
 // jit.cpp: compile (or fetch from the process cache) the kernel of a staged complex64 pass
-const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, std::string& err);
+const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, int groups, std::string& err);
 // jit.cpp: generate and compile a staged complex64 pass without a GPU (plan checks)
-bool jit_check_pass(const Pass& p, int nbuf, bool packed, std::string& err, size_t* cubin_bytes, std::string* info);
+bool jit_check_pass(const Pass& p, int nbuf, bool packed, int groups, std::string& err, size_t* cubin_bytes,
+                    std::string* info);
 // jit.cpp: NVRTC could be loaded
 bool jit_available();
 
@@ -175,6 +176,7 @@ struct smoq_ctx {
     int kernel_timing = 0;             // bracket tile passes with events
     int jit_buffers = 1;               // compiled pass kernels: tile buffers per CTA (1 or 2)
     int jit_packed = 0;                // compiled pass kernels: FP32x2 arithmetic on group pairs
+    int jit_groups = 2;                // compiled pass kernels: 16-amplitude register groups per thread
     long long launches = 0;            // kernels launched by this ctx
     long long tile_passes = 0;
     double tile_ms = 0;                // summed tile-pass time when kernel_timing
