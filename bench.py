@@ -383,6 +383,8 @@ def mcwf_workload(args):
                                    "= 503 trajectory-steps/s on a laptop (output.log:449)",
             "cpu_baseline": cpu}
     print(json.dumps(line))
+    st.close()
+    plan.close()
     ctx.close()
     return 0
 

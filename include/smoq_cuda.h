@@ -46,6 +46,7 @@ typedef struct smoq_plan smoq_plan;
 
 /* ---------------------------------------------------------------- context */
 smoq_status smoq_ctx_create(int device, smoq_ctx** out);
+/* States and plans refer to their context: destroy them before the context. */
 smoq_status smoq_ctx_destroy(smoq_ctx* ctx);
 const char* smoq_last_error(smoq_ctx* ctx);
 smoq_status smoq_ctx_synchronize(smoq_ctx* ctx);

@@ -11,6 +11,7 @@ C ABI in include/smoq_cuda.h.  `CuState` plays the role of the reference's
     expect_local(ψ, 1, N, "z")           # expect_local(ψ, 1, N, :z)
 """
 import ctypes as C
+import weakref
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
 
@@ -39,7 +40,9 @@ __all__ = [
 
 # ----------------------------------------------------------------- context
 class Context:
-    """Owns a CUDA stream, scratch buffers and the last-error string (smoq_ctx)."""
+    """Owns a CUDA stream, scratch buffers and the last-error string (smoq_ctx).
+    Closing it first closes the states and plans created on it (their C objects
+    refer to the context)."""
 
     def __init__(self, device: int = 0):
         h = C.c_void_p()
@@ -47,9 +50,12 @@ class Context:
         if s != 0:
             raise SmoqError(s, f"smoq_ctx_create(device={device}) failed")
         self.h = h
+        self._children = weakref.WeakSet()
 
     def close(self):
         if self.h:
+            for child in list(self._children):
+                child.close()
             lib.smoq_ctx_destroy(self.h)
             self.h = None
 
@@ -85,9 +91,11 @@ class CuState:
 
     def __init__(self, ctx: Context, N: int, dtype: int = C128, batch: int = 1, basis: Optional[int] = 0):
         self.ctx, self.N, self.dtype, self.batch = ctx, N, dtype, batch
+        self.h = None
         h = C.c_void_p()
         ck(lib.smoq_state_create(ctx.h, N, dtype, batch, C.byref(h)), ctx.h, "smoq_state_create")
         self.h = h
+        ctx._children.add(self)
         if basis is not None:
             self.set_basis(basis)
 
@@ -96,9 +104,9 @@ class CuState:
         return np.complex64 if self.dtype == C64 else np.complex128
 
     def close(self):
-        if self.h:
+        if self.h and self.ctx.h:  # a closed context has already closed this state
             lib.smoq_state_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -431,16 +439,18 @@ class TrotterPlan:
 
     def __init__(self, ctx: Context, N: int, gates: Sequence[FastTrotterGate], order: int = 1, dtype: int = C128):
         self.ctx, self.N, self.order, self.dtype = ctx, N, order, dtype
+        self.h = None
         arr = _to_c_gates(gates)
         h = C.c_void_p()
         ck(lib.smoq_trotter_plan_create(ctx.h, N, dtype, arr, len(gates), order, C.byref(h)), ctx.h,
            "trotter_plan_create")
         self.h = h
+        ctx._children.add(self)
 
     def close(self):
-        if self.h:
+        if self.h and self.ctx.h:  # a closed context has already closed this plan
             lib.smoq_plan_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:

@@ -144,3 +144,17 @@ def test_bad_input_is_reported(ctx):
         S.apply_rx_psi(st, 1, float("nan"), 4)
     with pytest.raises(S.SmoqError):
         S.expect_local(st, 1, 4, "w")
+
+
+def test_closing_a_context_closes_its_states_and_plans():
+    """closing a Context first closes the states and plans made on it, so objects
+    released later (e.g. at interpreter exit) never reach a destroyed context"""
+    import gc
+    c = S.Context(0)
+    st = S.CuState(c, 10, S.C64, basis=3)
+    plan = S.TrotterPlan(c, 10, [S.FastTrotterGate([1, 2], np.eye(4))], order=1, dtype=S.C64)
+    plan.step(st, 1)
+    c.close()
+    assert st.h is None and plan.h is None
+    del st, plan
+    gc.collect()
