@@ -76,6 +76,21 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(ms, dist, device):
+    """The slowest replica's device time: every rank passes its own CUDA-event time
+    and gets back the maximum (the job finishes when its slowest rank does)."""
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, ranks, ms):
+    """Whole-job throughput of independent replicas: all ranks' units over the
+    slowest rank's time (weak scaling: the work per rank is fixed)."""
+    return ranks * units_per_rank / (ms * 1e-3)
+
+
 class Clocks:
     """nvidia-smi sampler during the timed region."""
 
@@ -536,9 +551,7 @@ def main():
         ctx.synchronize()
         ms = e0.elapsed_time(e1)
         if ws > 1:
-            t = torch.tensor([ms], device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = max_over_ranks(ms, dist, f"cuda:{local}")
         return ms
 
     for _ in range(args.warmup):
@@ -575,8 +588,8 @@ def main():
     e2e_ms = timed(e2e_step, args.steps)
 
     per_rank_apps = gate_apps * args.steps
-    value = ws * per_rank_apps / (ms * 1e-3)
-    e2e_value = ws * per_rank_apps / (e2e_ms * 1e-3)
+    value = whole_job_rate(per_rank_apps, ws, ms)
+    e2e_value = whole_job_rate(per_rank_apps, ws, e2e_ms)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and N == N_QUBITS:
