@@ -415,6 +415,8 @@ def bandwidth_workload(args):
         ctx.set_option(S._lib.OPT_ENGINE, args.engine)
     if args.jit_packed:
         ctx.set_option(S._lib.OPT_JIT_PACKED, args.jit_packed)
+    if args.jit_stage_bits != 4:
+        ctx.set_option(S._lib.OPT_JIT_STAGE_BITS, args.jit_stage_bits)
     peak, peak_kind = measured_peak()
     out = {}
     for N, dt, name in ((32, S.C64, "n32_c64"), (31, S.C128, "n31_c128")):
@@ -468,6 +470,7 @@ def main():
     ap.add_argument("--jit-buffers", type=int, default=1, help="compiled pass kernels: tile buffers per CTA (1, 2)")
     ap.add_argument("--jit-packed", type=int, default=0, help="compiled pass kernels: FP32x2 arithmetic (1) or scalar (0)")
     ap.add_argument("--jit-groups", type=int, default=2, help="compiled pass kernels: register groups per thread (1, 2)")
+    ap.add_argument("--jit-stage-bits", type=int, default=4, help="compiled pass kernels: bits per register stage (4, 5)")
     ap.add_argument("--workload", default="trotter", choices=["trotter", "vqe", "vqe_jobs", "mcwf", "bandwidth"],
                     help="trotter: the headline line; vqe / bandwidth: the gradient and 32 GiB sweep figures")
     args = ap.parse_args()
@@ -511,6 +514,8 @@ def main():
         ctx.set_option(S._lib.OPT_JIT_PACKED, args.jit_packed)
     if args.jit_groups != 2:
         ctx.set_option(S._lib.OPT_JIT_GROUPS, args.jit_groups)
+    if args.jit_stage_bits != 4:
+        ctx.set_option(S._lib.OPT_JIT_STAGE_BITS, args.jit_stage_bits)
     N = args.n_qubits
     tsteps = args.trotter_steps
     gate_apps = tsteps * 2 * (N + 3 * (N - 1))

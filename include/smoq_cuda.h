@@ -70,8 +70,11 @@ enum {
     SMOQ_OPT_JIT_PACKED = 9       /* compiled pass kernels: 0 (default) = scalar FP32; 1 = FP32x2 arithmetic,
                                      a thread's two register groups as one 64-bit pair (more registers
                                      per thread; measured slower on B200) */,
-    SMOQ_OPT_JIT_GROUPS = 10      /* compiled pass kernels: 16-amplitude register groups per thread, 2
+    SMOQ_OPT_JIT_GROUPS = 10,     /* compiled pass kernels: 16-amplitude register groups per thread, 2
                                      (default; 2^(T-5) threads) or 1 (2^(T-4) threads) */
+    SMOQ_OPT_JIT_STAGE_BITS = 11  /* compiled pass kernels: tile bits per register stage, 4 (default) or 5
+                                     (32-amplitude stages: fewer shared-memory round trips per pass;
+                                     needs 2 groups per thread and scalar arithmetic) */
 };
 smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long value);
 /* launches: kernels launched by this context; tile_passes/tile_ms/tile_bytes:
@@ -339,7 +342,7 @@ typedef struct {
  * would with engine 3 and compiles every complex64 pass kernel with NVRTC, without a GPU
  * and without loading them.  flags: 1 = return the compiler's register/spill report in msg,
  * 2 = two tile buffers per CTA (SMOQ_OPT_JIT_BUFFERS 2), 4 = FP32x2 arithmetic (SMOQ_OPT_JIT_PACKED 1),
- * 8 = one register group per thread (SMOQ_OPT_JIT_GROUPS 1).  *n_compiled = kernels compiled; msg
+ * 8 = one register group per thread (SMOQ_OPT_JIT_GROUPS 1), 16 = 5-bit stages (SMOQ_OPT_JIT_STAGE_BITS 5).  *n_compiled = kernels compiled; msg
  * gets "ok" (or the report) or the first error.  SMOQ_ERR_UNSUPPORTED when NVRTC is not
  * available. */
 smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops, int n,

@@ -99,7 +99,7 @@ static int engine_for(smoq_ctx* ctx, bool reusable, int dtype) {
 // plan a gate list into fused passes; with the register engine every pass
 // wide enough for it gets a register-tile schedule
 static std::vector<Pass> plan_for(int engine, const std::vector<GateIR>& ir, int N, int dtype, int tbits, int lbits,
-                                  int epilogue_special = -1) {
+                                  int epilogue_special = -1, int stage_bits = 4) {
     std::vector<Pass> pl = plan_passes(ir, N, tbits, lbits, epilogue_special, dtype == SMOQ_C64 ? 1 : 0);
     if (engine == 1)
         for (Pass& p : pl)
@@ -107,7 +107,9 @@ static std::vector<Pass> plan_for(int engine, const std::vector<GateIR>& ir, int
     if (engine == 2 || engine == 3)
         for (Pass& p : pl)
             if (p.g.T == 12 || (p.g.T == 13 && dtype == SMOQ_C64)) {
-                schedule_stages(p, dtype == SMOQ_C64 ? 8 : 16);
+                // 5-bit stages exist only in compiled complex64 kernels
+                const bool k5 = engine == 3 && dtype == SMOQ_C64 && stage_bits == 5;
+                schedule_stages(p, dtype == SMOQ_C64 ? 8 : 16, k5 ? 5 : 4);
                 p.want_jit = engine == 3 && p.staged && dtype == SMOQ_C64;
             }
     return pl;
@@ -268,6 +270,10 @@ smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long v) {
             ctx->engine = (int)v;
             break;
         case SMOQ_OPT_JIT_PACKED: ctx->jit_packed = v != 0; break;
+        case SMOQ_OPT_JIT_STAGE_BITS:
+            if (v != 4 && v != 5) return fail(ctx, SMOQ_ERR_BADINPUT, "compiled-kernel stage bits must be 4 or 5");
+            ctx->jit_stage_bits = (int)v;
+            break;
         case SMOQ_OPT_JIT_GROUPS:
             if (v != 1 && v != 2) return fail(ctx, SMOQ_ERR_BADINPUT, "compiled-kernel register groups must be 1 or 2");
             ctx->jit_groups = (int)v;
@@ -554,7 +560,7 @@ smoq_status smoq_apply_sequence(smoq_state* st, const smoq_op* ops, int n, const
     DevProgram P;
     try {
         P.passes = plan_for(engine_for(ctx, false, st->dtype), ir, st->N, st->dtype, tile_bits(ctx, st->dtype),
-                            low_bits(ctx, st->dtype));
+                            low_bits(ctx, st->dtype), -1, ctx->jit_stage_bits);
     } catch (const std::exception& ex) {
         return fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
     }
@@ -584,7 +590,7 @@ smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tbits, int lbit
     if (smoq_status s = ops_to_ir(nullptr, N, ops, n, theta, ir)) return s;
     std::vector<Pass> pl;
     try {
-        pl = plan_for(3, ir, N, dtype, tbits, lbits);
+        pl = plan_for(3, ir, N, dtype, tbits, lbits, -1, (flags & 16) ? 5 : 4);
     } catch (const std::exception& e) {
         say(e.what());
         return SMOQ_ERR_BADINPUT;
@@ -831,7 +837,7 @@ static smoq_status get_block(smoq_plan* P, int nsteps, smoq_plan::Block** out) {
     for (int s = 0; s < nsteps; ++s) all.insert(all.end(), P->step.begin(), P->step.end());
     try {
         B->prog.passes = plan_for(engine_for(P->ctx, true, P->dtype), all, P->N, P->dtype, tile_bits(P->ctx, P->dtype),
-                                  low_bits(P->ctx, P->dtype));
+                                  low_bits(P->ctx, P->dtype), -1, P->ctx->jit_stage_bits);
     } catch (const std::exception& ex) {
         return fail(P->ctx, SMOQ_ERR_BADINPUT, ex.what());
     }
@@ -1062,7 +1068,7 @@ smoq_status smoq_internal_prepare(smoq_ctx* ctx, smoq_state* st, const std::vect
     std::unique_ptr<DevProgram> P(new DevProgram());
     try {
         P->passes = plan_for(engine_for(ctx, reusable, st->dtype), gates, st->N, st->dtype, tile_bits(ctx, st->dtype),
-                             low_bits(ctx, st->dtype), epilogue_special);
+                             low_bits(ctx, st->dtype), epilogue_special, ctx->jit_stage_bits);
     } catch (const std::exception& ex) {
         return fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
     }

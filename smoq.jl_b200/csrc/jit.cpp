@@ -179,13 +179,13 @@ std::string flit(float v) {
 
 // deposit of thread-index bits around the sorted stage bits S: segment masks
 struct Deposit {
-    uint32_t m[5];
+    uint32_t m[6];  // segment k of the thread index moves up by k (K + 1 segments)
 };
-Deposit deposit_masks(const int* S) {
+Deposit deposit_masks(const int* S, int K) {
     Deposit d;
     int lo = 0;
-    for (int k = 0; k < 5; ++k) {
-        const int hi = k < 4 ? S[k] - k : 32;
+    for (int k = 0; k <= K; ++k) {
+        const int hi = k < K ? S[k] - k : 32;
         uint32_t mask = 0;
         for (int b = lo; b < hi && b < 32; ++b) mask |= 1u << b;
         d.m[k] = mask;
@@ -193,19 +193,19 @@ Deposit deposit_masks(const int* S) {
     }
     return d;
 }
-uint32_t deposit_value(const int* S, uint32_t g) {
+uint32_t deposit_value(const int* S, int K, uint32_t g) {
     uint32_t x = g;
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < K; ++k) {
         const uint32_t lo = x & ((1u << S[k]) - 1);
         x = ((x >> S[k]) << (S[k] + 1)) | lo;
     }
     return x;
 }
-std::string deposit_expr(const int* S, const char* g) {
-    const Deposit d = deposit_masks(S);
+std::string deposit_expr(const int* S, int K, const char* g) {
+    const Deposit d = deposit_masks(S, K);
     std::ostringstream o;
     o << "((" << g << " & " << d.m[0] << "u)";
-    for (int k = 1; k < 5; ++k)
+    for (int k = 1; k <= K; ++k)
         if (d.m[k]) o << " | ((" << g << " & " << d.m[k] << "u) << " << k << ")";
     o << ")";
     return o.str();
@@ -300,7 +300,7 @@ struct Gen {
     std::string Qn(int r) { return "Q" + std::to_string(r); }
 
     void stage_packed(const int* S, const int* rl, const std::vector<int>& members) {
-        const uint32_t gstep = deposit_value(S, (uint32_t)NT);
+        const uint32_t gstep = deposit_value(S, 4, (uint32_t)NT);
         uint32_t off[16];
         for (int r = 0; r < 16; ++r) {
             off[r] = 0;
@@ -310,7 +310,7 @@ struct Gen {
         bool rotated = false;
         for (int q = 0; q < 4; ++q) rotated |= rl[q] >= 0;
         o << "    {  // stage S = {" << S[0] << "," << S[1] << "," << S[2] << "," << S[3] << "}, FP32x2\n";
-        o << "        const u32 g0 = " << deposit_expr(S, "tid") << ";\n";
+        o << "        const u32 g0 = " << deposit_expr(S, 4, "tid") << ";\n";
         if (rotated) {
             o << "        const u32 ga = g0";
             for (int q = 0; q < 4; ++q)
@@ -482,27 +482,37 @@ struct Gen {
 
     // one stage: S sorted 4 tile bits, rl[q] lane bit of the rotation at stage
     // position q (-1 none), members = indices into p.ops
-    void stage(const int* S, const int* rl, const std::vector<int>& members) {
-        const uint32_t gstep = deposit_value(S, (uint32_t)NT);
-        uint32_t off[16];
-        for (int r = 0; r < 16; ++r) {
+    // current stage: KB bits, GS register groups of 2^KB amplitudes per thread
+    int KB = 4, GS = 2;
+
+    // one stage: S sorted KB tile bits, rl[q] lane bit of the rotation at stage
+    // position q (-1 none), members = indices into p.ops
+    void stage(const int* S, int k_bits, const int* rl, const std::vector<int>& members) {
+        KB = k_bits;
+        GS = (G << 4) >> KB;  // the thread's 16 G amplitudes as GS groups of 2^KB
+        const int R = 1 << KB;
+        const uint32_t gstep = GS > 1 ? deposit_value(S, KB, (uint32_t)NT) : 0u;
+        uint32_t off[32];
+        for (int r = 0; r < R; ++r) {
             off[r] = 0;
-            for (int q = 0; q < 4; ++q)
+            for (int q = 0; q < KB; ++q)
                 if ((r >> q) & 1) off[r] |= 1u << S[q];
         }
         bool rotated = false;
-        for (int q = 0; q < 4; ++q) rotated |= rl[q] >= 0;
-        o << "    {  // stage S = {" << S[0] << "," << S[1] << "," << S[2] << "," << S[3] << "}\n";
-        o << "        const u32 g0 = " << deposit_expr(S, "tid") << ";\n";
+        for (int q = 0; q < KB; ++q) rotated |= rl[q] >= 0;
+        o << "    {  // stage S = {";
+        for (int q = 0; q < KB; ++q) o << (q ? "," : "") << S[q];
+        o << "}\n";
+        o << "        const u32 g0 = " << deposit_expr(S, KB, "tid") << ";\n";
         if (rotated) {
             o << "        const u32 ga = g0";
-            for (int q = 0; q < 4; ++q)
+            for (int q = 0; q < KB; ++q)
                 if (rl[q] >= 0) o << " ^ (((tid >> " << rl[q] << ") & 1u) << " << S[q] << ")";
             o << ";\n";
         }
-        const int nreg = 16 * G;
+        const int nreg = GS * R;
         for (int i = 0; i < nreg; ++i) {
-            const uint32_t c = off[i & 15] | ((i >> 4) ? gstep : 0u);
+            const uint32_t c = off[i & (R - 1)] | ((i >> KB) ? gstep : 0u);
             if (rotated) o << "        cf " << v(i) << " = tile[ga ^ " << c << "u];\n";
             else o << "        cf " << v(i) << " = tile[g0 + " << c << "u];\n";
         }
@@ -513,7 +523,7 @@ struct Gen {
             for (int i = 0; i < nreg; ++i) o << "        " << v(i) << " = cmul(sc, " << v(i) << ");\n";
         if (rotated) unrotate(rl);  // conditional swaps are involutions
         for (int i = 0; i < nreg; ++i) {
-            const uint32_t c = off[i & 15] | ((i >> 4) ? gstep : 0u);
+            const uint32_t c = off[i & (R - 1)] | ((i >> KB) ? gstep : 0u);
             if (rotated) o << "        tile[ga ^ " << c << "u] = " << v(i) << ";\n";
             else o << "        tile[g0 + " << c << "u] = " << v(i) << ";\n";
         }
@@ -522,10 +532,10 @@ struct Gen {
 
     // registers loaded at stage bits r ^ rot -> canonical order (and back)
     void unrotate(const int* rl) {
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < KB; ++q) {
             if (rl[q] < 0) continue;
             o << "        { const bool s = (tid >> " << rl[q] << ") & 1u;\n";
-            for (int i = 0; i < 16 * G; ++i) {
+            for (int i = 0; i < (GS << KB); ++i) {
                 if ((i >> q) & 1) continue;
                 const int k = i | (1 << q);
                 o << "          { const cf t = s ? " << v(k) << " : " << v(i) << "; " << v(k) << " = s ? " << v(i)
@@ -539,7 +549,7 @@ struct Gen {
     bool member(int m, const int* S, uint32_t gstep, bool have_scal) {
         const DevOp& op = p.ops[m];
         auto spos = [&](int lb) {
-            for (int q = 0; q < 4; ++q)
+            for (int q = 0; q < KB; ++q)
                 if (S[q] == lb) return q;
             return -1;
         };
@@ -552,9 +562,9 @@ struct Gen {
             return true;
         }
         if (op.kind == OPK_REALTAB) {
-            for (int i = 0; i < 16 * G; ++i) {
-                uint32_t c = (i >> 4) ? gstep : 0u;
-                for (int q = 0; q < 4; ++q)
+            for (int i = 0; i < (GS << KB); ++i) {
+                uint32_t c = (i >> KB) ? gstep : 0u;
+                for (int q = 0; q < KB; ++q)
                     if ((i >> q) & 1) c |= 1u << S[q];
                 o << "        " << v(i) << " = cscale(" << v(i) << ", realtab(a.ops[" << m << "], base, g0 | " << c
                   << "u));\n";
@@ -586,7 +596,7 @@ struct Gen {
             }
             if (!any_tile_nonstage && !any_off) {
                 // every qubit on a stage bit: literal factor per register
-                for (int i = 0; i < 16 * G; ++i) {
+                for (int i = 0; i < (GS << KB); ++i) {
                     int mi = 0;
                     for (int t = 0; t < op.nq; ++t) mi |= ((i >> pos[t]) & 1) << t;
                     const float re = op.cf[mi].x, im = op.cf[mi].y;
@@ -598,17 +608,17 @@ struct Gen {
                 return false;
             }
             // mixed: runtime index from non-stage tile bits (per group) and off-tile bits
-            for (int j = 0; j < G; ++j) {
+            for (int j = 0; j < GS; ++j) {
                 o << "        { const u32 gj = g0 | " << (j ? gstep : 0u) << "u; const u32 mr = " << rt.str();
                 for (int t = 0; t < op.nq; ++t)
                     if (op.lb[t] >= 0 && pos[t] < 0) o << " | (((gj >> " << op.lb[t] << ") & 1u) << " << t << ")";
                 o << ";\n";
-                for (int r = 0; r < 16; ++r) {
+                for (int r = 0; r < (1 << KB); ++r) {
                     int mi = 0;
                     for (int t = 0; t < op.nq; ++t)
                         if (pos[t] >= 0) mi |= ((r >> pos[t]) & 1) << t;
-                    o << "          " << v(16 * j + r) << " = cmul(a.ops[" << m << "].c[mr | " << mi << "u], "
-                      << v(16 * j + r) << ");\n";
+                    o << "          " << v((j << KB) + r) << " = cmul(a.ops[" << m << "].c[mr | " << mi << "u], "
+                      << v((j << KB) + r) << ");\n";
                 }
                 o << "        }\n";
             }
@@ -621,15 +631,15 @@ struct Gen {
         const std::vector<CplxF> M = op_matrix_f(op);
         int pmask = 0;
         for (int t = 0; t < op.nq; ++t) pmask |= 1 << pos[t];
-        for (int j = 0; j < G; ++j) {
-            for (int e = 0; e < 16; ++e) {
+        for (int j = 0; j < GS; ++j) {
+            for (int e = 0; e < (1 << KB); ++e) {
                 if (e & pmask) continue;
                 int ix[8];
                 for (int c = 0; c < dim; ++c) {
                     int r = e;
                     for (int t = 0; t < op.nq; ++t)
                         if ((c >> t) & 1) r |= 1 << pos[t];
-                    ix[c] = 16 * j + r;
+                    ix[c] = (j << KB) + r;
                 }
                 o << "        {";
                 for (int c = 0; c < dim; ++c) o << " const cf x" << c << " = " << v(ix[c]) << ";";
@@ -743,7 +753,7 @@ std::string generate(const Pass& p, bool need_epi, int nbuf, bool packed, int gr
             return "";
         }
         std::vector<int> members;
-        int S[4], rl[4];
+        int S[5], rl[5] = {-1, -1, -1, -1, -1}, kb = 4;
         if (h.nq == 0) {
             // one wide op: its 3 bits + one pad bit (bank-neutral first)
             const DevOp& op = p.ops[o_i + 1];
@@ -764,13 +774,24 @@ std::string generate(const Pass& p, bool need_epi, int nbuf, bool packed, int gr
             }
             members.push_back((int)o_i + 1);
             o_i += 2;
+        } else if (h.nq == 5) {
+            // 5-bit stage: bits in perm[0..4], rotation lanes of positions 0..3 in lb[0..3]
+            if (packed || G != 2) {
+                err = "jit: 5-bit stages need scalar arithmetic and two groups per thread";
+                return "";
+            }
+            kb = 5;
+            for (int q = 0; q < 5; ++q) S[q] = h.perm[q];
+            for (int q = 0; q < 4; ++q) rl[q] = h.lb[q];
+            for (int k = 1; k <= (int)h.aux2; ++k) members.push_back((int)(o_i + k));
+            o_i += 1 + (size_t)h.aux2;
         } else {
             for (int q = 0; q < 4; ++q) S[q] = h.perm[q], rl[q] = h.perm[4 + q];
             for (int k = 1; k <= (int)h.aux2; ++k) members.push_back((int)(o_i + k));
             o_i += 1 + (size_t)h.aux2;
         }
         if (packed) gen.stage_packed(S, rl, members);
-        else gen.stage(S, rl, members);
+        else gen.stage(S, kb, rl, members);
     }
     o << "    if (EPI) {\n"
          "        constexpr int nb = NT == 128 ? 7 : NT == 256 ? 8 : 9;\n"

@@ -653,8 +653,9 @@ void schedule_regtile(Pass& p) {
 // always hit distinct banks.  The kernel folds the rotation into per-thread
 // coefficients, once per op.
 // ----------------------------------------------------------------------------
-void schedule_stages(Pass& p, int amp_bytes) {
+void schedule_stages(Pass& p, int amp_bytes, int K) {
     const int T = p.g.T;
+    if (K != 5) K = 4;
     if (T < 12 || T > 13) return;
     const int LB = amp_bytes == 8 ? 4 : 3;
     for (const DevOp& op : p.ops)  // adjoint partials and layout ops belong to other kernels
@@ -686,23 +687,26 @@ void schedule_stages(Pass& p, int amp_bytes) {
     };
     auto contains = [](const std::vector<int>& s, int b) { return std::find(s.begin(), s.end(), b) != s.end(); };
     auto header = [&](std::vector<int> S, int nmembers) {
-        for (int b = LB; (int)S.size() < 4 && b < T; ++b)  // pad with bank-neutral bits first
+        for (int b = LB; (int)S.size() < K && b < T; ++b)  // pad with bank-neutral bits first
             if (!contains(S, b)) S.push_back(b);
-        for (int b = 0; (int)S.size() < 4 && b < T; ++b)
+        for (int b = 0; (int)S.size() < K && b < T; ++b)
             if (!contains(S, b)) S.push_back(b);
         std::sort(S.begin(), S.end());
         DevOp h;
         std::memset(&h, 0, sizeof(h));
         h.kind = OPK_STAGE;
-        h.nq = 4;
+        h.nq = K;
         h.aux2 = nmembers;
         int c = 0;  // free bits below LB: the lowest lane bits
         for (int b = 0; b < LB; ++b)
             if (!contains(S, b)) ++c;
         int a = 0;
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < 4; ++k) h.lb[k] = -1;
+        for (int k = 0; k < K; ++k) {
             h.perm[k] = S[k];
-            h.perm[4 + k] = S[k] < LB ? c + a++ : -1;
+            const int lane = S[k] < LB ? c + a++ : -1;
+            if (K == 4) h.perm[4 + k] = lane;
+            else if (k < 4) h.lb[k] = lane;  // 5-bit stage: bits in perm[0..4], lanes in lb[0..3]
         }
         return h;
     };
@@ -727,7 +731,7 @@ void schedule_stages(Pass& p, int amp_bytes) {
             std::vector<int> U = S;
             for (int b : needs(in[j]))
                 if (!contains(U, b)) U.push_back(b);
-            if (U.size() > 4) break;
+            if ((int)U.size() > K) break;
             S = U;
         }
         DevOp h = header(S, (int)(j - i));
@@ -737,7 +741,7 @@ void schedule_stages(Pass& p, int amp_bytes) {
             for (int t = 0; t < 4; ++t) op.slot[t] = -1;
             if (op.kind != OPK_DIAG && op.kind != OPK_STATESCALE && op.kind != OPK_REALTAB) {
                 for (int t = 0; t < op.nq; ++t)
-                    for (int q = 0; q < 4; ++q)
+                    for (int q = 0; q < K; ++q)
                         if (h.perm[q] == op.lb[t]) op.slot[t] = q;
                 if (op.nq == 2 && op.slot[0] > op.slot[1]) swap_qubit_roles(op);
             }

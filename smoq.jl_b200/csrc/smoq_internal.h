@@ -35,7 +35,9 @@ enum OpKind : int32_t {
     OPK_STAGE = 10,   // stage-sweep engine: header of a stage; perm[0..3] = the stage's 4
                       // tile bits (ascending), perm[4..7] = lane bit feeding the rotation of
                       // each stage bit (-1 none), aux2 = number of member ops that follow;
-                      // nq = 0 marks a single op applied by a plain shared-memory sweep
+                      // nq = 0 marks a single op applied by a plain shared-memory sweep;
+                      // nq = 5 a 5-bit stage (compiled kernels only): perm[0..4] = bits,
+                      // lb[0..3] = rotation lanes
     OPK_INNER = 9,    // adjoint sweep: per-tile Im<lambda|G|phi> with G = cd (dense, 1-2
                       // qubits), written to partials slot perm[0] of the pass
     OPK_LAYOUT = 8,   // register-tile layout change: perm[0..KR-1] = register bits,
@@ -134,8 +136,10 @@ std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, in
                               int epilogue_after_special = -1, int Lreq = 0);
 // turn a planned pass into a register-tile program (layout ops + slots)
 void schedule_regtile(Pass& p);
-// turn a planned pass into stage sweeps (engine 2); amp_bytes selects the bank geometry
-void schedule_stages(Pass& p, int amp_bytes);
+// turn a planned pass into stage sweeps (engines 2, 3); amp_bytes selects the bank
+// geometry; K = 4 bits per stage, or 5 (engine 3 only: header bits in perm[0..4],
+// rotation lanes of positions 0..3 in lb[0..3])
+void schedule_stages(Pass& p, int amp_bytes, int K = 4);
 void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op);
 // jit.cpp: compile (or fetch from the process cache) the kernel of a staged complex64 pass
 const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, int groups, std::string& err);
@@ -177,6 +181,7 @@ struct smoq_ctx {
     int jit_buffers = 1;               // compiled pass kernels: tile buffers per CTA (1 or 2)
     int jit_packed = 0;                // compiled pass kernels: FP32x2 arithmetic on group pairs
     int jit_groups = 2;                // compiled pass kernels: 16-amplitude register groups per thread
+    int jit_stage_bits = 4;            // compiled pass kernels: tile bits per register stage (4 or 5)
     long long launches = 0;            // kernels launched by this ctx
     long long tile_passes = 0;
     double tile_ms = 0;                // summed tile-pass time when kernel_timing

@@ -736,7 +736,7 @@ def debug_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtype: int =
 
 def debug_compile_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtype: int = C64, tile_bits: int = 13,
                        low_bits: int = 5, verbose: bool = False, buffers: int = 1, packed: bool = False,
-                       groups: int = 2):
+                       groups: int = 2, stage_bits: int = 4):
     """Host-only: plan `ops` for the plan compiler (engine 3) and compile every pass
     kernel with NVRTC (no GPU, nothing loaded).  Returns (status, n_compiled, message);
     with verbose the message is the compiler's register/spill report."""
@@ -744,7 +744,8 @@ def debug_compile_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtyp
     th = np.ascontiguousarray(theta if theta is not None else np.zeros(1), dtype=np.float64)
     n = C.c_int()
     msg = C.create_string_buffer(1 << 16)
-    flags = (1 if verbose else 0) | (2 if buffers == 2 else 0) | (4 if packed else 0) | (8 if groups == 1 else 0)
+    flags = (1 if verbose else 0) | (2 if buffers == 2 else 0) | (4 if packed else 0) | (8 if groups == 1 else 0) \
+        | (16 if stage_bits == 5 else 0)
     st = lib.smoq_debug_compile_plan(N, dtype, tile_bits, low_bits, arr, len(ops), dptr(th), flags, C.byref(n),
                                      msg, 1 << 16)
     return st, n.value, msg.value.decode(errors="replace")
