@@ -298,6 +298,26 @@ smoq_status smoq_energy_grad_jobs(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vq
 smoq_status smoq_apply_pauli_sum(smoq_state* in, smoq_state* out, const smoq_pauli_term* H, int nterms,
                                  double* expect);
 
+/* ------------------------------------------------------- density matrices */
+/* A density matrix of N qubits (N <= 16) is a smoq_state of 2N qubits holding
+ * rho column-major (rho[i, j] at i + j 2^N, the memory of Julia's
+ * Matrix{ComplexF64}): bits 0..N-1 index the row, bits N..2N-1 the column;
+ * |k><k| is smoq_state_set_basis(st, k + k * 2^N).
+ * smoq_dm_plan_create builds a plan whose one step is the reference's DM step:
+ * rho -> U rho U^dag for the gate list (evolve_trotter_rho_cpu!,
+ * cpuQuantumChannelUnitaryEvolutionTrotter.jl:266-285), then, for each jump in
+ * order, one Euler step rho += gamma dt (L rho L^dag - {L^dag L, rho}/2)
+ * (_apply_dissipator_dm!, cpuQuantumChannelLindbladianEvolution.jl:377-460).
+ * Run it with smoq_trotter_step / smoq_plan_destroy like any plan; the state
+ * passed must have 2N qubits.  2-qubit gates follow the smoq_trotter_gate
+ * convention on both sides (rows: U, columns: conj(U)). */
+smoq_status smoq_dm_plan_create(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_trotter_gate* gates, int ngates,
+                                const smoq_jump_op* jumps, int njumps, double dt, smoq_plan** out);
+/* out[b * nobs + o] = sum_i Re rho_ii (-1)^popc(i & zmasks[o]) for every matrix of
+ * the batch: <Z...> strings of a density matrix (cpuQuantumStateObservables.jl:1246-1420
+ * restricted to Z strings; mask 0 gives the trace).  1 <= nobs <= 32; out is host. */
+smoq_status smoq_dm_expect_zstrings(smoq_state* rho, int N, const uint64_t* zmasks, int nobs, double* out);
+
 /* ------------------------------------------------- sampling and measurement */
 /* Born-rule sampling from |psi|^2: out[b * nshots + s] = basis index of shot s of
  * state b.  Replaces sample_from_probabilities (cpuQuantumStateMeasurements.jl:203)

@@ -754,3 +754,40 @@ def debug_compile_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtyp
 def jit_available() -> bool:
     """True when the plan compiler (engine 3, NVRTC) can run in this process."""
     return bool(lib.smoq_jit_available())
+
+
+# ----------------------------------------------------------- density matrices
+class DensityMatrixPlan(TrotterPlan):
+    """One step of the reference's density-matrix evolution on a 2N-qubit state that
+    holds rho column-major: rho -> U rho U^dag for the gate list (evolve_trotter_rho_cpu!),
+    then one Euler dissipator step per jump (_apply_dissipator_dm!)."""
+
+    def __init__(self, ctx: Context, N: int, gates: Sequence[FastTrotterGate], jump_ops, dt: float,
+                 dtype: int = C128):
+        self.ctx, self.N, self.order, self.dtype = ctx, N, 1, dtype
+        self.h = None
+        arr = _to_c_gates(gates)
+        ops = (SmoqJumpOp * max(1, len(jump_ops)))()
+        for t, o in enumerate(jump_ops):
+            ops[t].type = _JUMP_CODES[o.type]
+            ops[t].qubit = o.qubit - 1
+            ops[t].gamma = o.gamma
+        h = C.c_void_p()
+        ck(lib.smoq_dm_plan_create(ctx.h, N, dtype, arr, len(gates), ops, len(jump_ops), float(dt), C.byref(h)),
+           ctx.h, "dm_plan_create")
+        self.h = h
+        ctx._children.add(self)
+
+
+def density_matrix_state(ctx: Context, N: int, basis: int = 0, dtype: int = C128, batch: int = 1) -> CuState:
+    """|basis><basis| as a 2N-qubit state (rho column-major)."""
+    return CuState(ctx, 2 * N, dtype, batch, basis=basis + (basis << N))
+
+
+def dm_expect_zstrings(rho: CuState, N: int, zmasks: Sequence[int]) -> np.ndarray:
+    """sum_i Re rho_ii (-1)^popc(i & mask) per mask (mask 0: trace), [batch, nobs]."""
+    m = np.ascontiguousarray(zmasks, dtype=np.uint64)
+    out = np.empty((rho.batch, len(m)))
+    ck(lib.smoq_dm_expect_zstrings(rho.h, N, m.ctypes.data_as(C.POINTER(C.c_uint64)), len(m), dptr(out)),
+       rho.ctx.h, "dm_expect_zstrings")
+    return out

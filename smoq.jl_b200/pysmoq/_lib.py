@@ -137,6 +137,9 @@ _SIGS = {
                          C.c_int, C.c_int, _dp, _dp, _dp],
     "smoq_jit_available": [],
     "smoq_apply_pauli_sum": [_vp, _vp, C.POINTER(SmoqPauliTerm), C.c_int, _dp],
+    "smoq_dm_plan_create": [_vp, C.c_int, C.c_int, C.POINTER(SmoqTrotterGate), C.c_int, C.POINTER(SmoqJumpOp),
+                            C.c_int, C.c_double, C.POINTER(C.c_void_p)],
+    "smoq_dm_expect_zstrings": [_vp, C.c_int, C.POINTER(C.c_uint64), C.c_int, _dp],
     "smoq_sample": [_vp, C.c_longlong, C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_longlong)],
     "smoq_measure_all": [_vp, C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_longlong)],
     "smoq_measure_qubit": [_vp, C.c_int, C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_int)],
