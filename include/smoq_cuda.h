@@ -174,6 +174,12 @@ smoq_status smoq_expect_zz(smoq_state* st, int q1, int q2, double* out); /* _exp
 /* get_expectation_pauli_string :840 (ops letters 'X','Y','Z' on 0-based qubits) */
 smoq_status smoq_expect_pauli_string(smoq_state* st, int n, const char* ops, const int* qubits,
                                      double* out);
+/* measure_all_observables_state_vector_cpu! (cpuQuantumStateObservables.jl:1483) for
+ * the multi-rail ladder of N = L * n_rails qubits: out[b * n_ops + k] in the
+ * reference's order -- (<X_q>, <Y_q>, <Z_q>) for every qubit, then (<XX>, <YY>, <ZZ>)
+ * for every bond along each rail, then for every rung between rails;
+ * n_ops = 3N + 3 (L-1) n_rails + 3 L (n_rails-1).  Z and ZZ share Z-string passes. */
+smoq_status smoq_measure_all_observables(smoq_state* st, int L, int n_rails, double* out);
 /* diagonal batch in ONE pass: out[b * nobs + o] = <Z-string zmasks[o]> of state b
  * (zmask 0 gives the squared norm); the Z/ZZ part of
  * measure_all_observables_one_pass :1532 */

@@ -770,6 +770,54 @@ smoq_status smoq_expect_zstrings(smoq_state* st, const uint64_t* zmasks, int nob
     return diag_reduce_host(st, zmasks, nobs, out);
 }
 
+smoq_status smoq_measure_all_observables(smoq_state* st, int L, int n_rails, double* out) {
+    if (check_state(st) || !out || L < 1 || n_rails < 1) return SMOQ_ERR_BADINPUT;
+    const int N = L * n_rails;
+    if (N != st->N) return fail(st->ctx, SMOQ_ERR_BADINPUT, "L * n_rails must equal the state's N");
+    // the reference's order: (X, Y, Z) per qubit, then (XX, YY, ZZ) per rail bond, then per rung
+    struct Obs { uint64_t x, z; int ny; };
+    std::vector<Obs> obs;
+    for (int k = 0; k < N; ++k) {
+        const uint64_t b = 1ull << k;
+        obs.push_back({b, 0, 0});
+        obs.push_back({b, b, 1});
+        obs.push_back({0, b, 0});
+    }
+    auto pair = [&](int i, int j) {
+        const uint64_t m = (1ull << i) | (1ull << j);
+        obs.push_back({m, 0, 0});
+        obs.push_back({m, m, 2});
+        obs.push_back({0, m, 0});
+    };
+    for (int r = 0; r < n_rails; ++r)
+        for (int s = 0; s < L - 1; ++s) pair(r * L + s, r * L + s + 1);
+    for (int r = 0; r < n_rails - 1; ++r)
+        for (int s = 0; s < L; ++s) pair(r * L + s, (r + 1) * L + s);
+    const int nops = (int)obs.size();
+    const int B = st->batch;
+    // diagonal ones (Z, ZZ) in Z-string reductions of up to 32 masks, the others one by one
+    std::vector<int> zi;
+    for (int o = 0; o < nops; ++o)
+        if (!obs[o].x) zi.push_back(o);
+    std::vector<double> v;
+    for (size_t a = 0; a < zi.size(); a += 32) {
+        const int k = (int)std::min<size_t>(32, zi.size() - a);
+        std::vector<uint64_t> m(k);
+        for (int t = 0; t < k; ++t) m[t] = obs[zi[a + t]].z;
+        v.assign((size_t)B * k, 0.0);
+        if (smoq_status s = diag_reduce_host(st, m.data(), k, v.data())) return s;
+        for (int b = 0; b < B; ++b)
+            for (int t = 0; t < k; ++t) out[(size_t)b * nops + zi[a + t]] = v[(size_t)b * k + t];
+    }
+    v.assign(B, 0.0);
+    for (int o = 0; o < nops; ++o) {
+        if (!obs[o].x) continue;
+        if (smoq_status s = pauli_reduce_host(st, obs[o].x, obs[o].z, obs[o].ny, v.data())) return s;
+        for (int b = 0; b < B; ++b) out[(size_t)b * nops + o] = v[b];
+    }
+    return SMOQ_OK;
+}
+
 smoq_status smoq_population_excited(smoq_state* st, int q, double* out) {
     if (check_state(st) || !out) return SMOQ_ERR_BADINPUT;
     if (smoq_status s = check_q(st, q, "population_excited")) return s;

@@ -324,6 +324,16 @@ def measure_z(psi: CuState, k: int, N: int, seed: int, stream: int = 0):
     return int(out[0]) if psi.batch == 1 else out
 
 
+def measure_all_observables_state_vector(psi: CuState, L: int, n_rails: int) -> np.ndarray:
+    """measure_all_observables_state_vector_cpu(psi, L, n_rails): local X, Y, Z, then
+    XX, YY, ZZ on rail bonds, then on rungs (reference order); [n_ops] or [batch, n_ops]."""
+    N = L * n_rails
+    n_ops = 3 * N + 3 * (L - 1) * n_rails + 3 * L * (n_rails - 1)
+    out = np.empty((psi.batch, n_ops))
+    ck(lib.smoq_measure_all_observables(psi.h, L, n_rails, dptr(out)), psi.ctx.h, "measure_all_observables")
+    return out[0] if psi.batch == 1 else out
+
+
 def population_excited_psi(psi: CuState, k: int, N: int):
     _n(psi, N)
     out = np.empty(psi.batch)

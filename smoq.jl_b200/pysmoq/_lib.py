@@ -140,6 +140,7 @@ _SIGS = {
     "smoq_dm_plan_create": [_vp, C.c_int, C.c_int, C.POINTER(SmoqTrotterGate), C.c_int, C.POINTER(SmoqJumpOp),
                             C.c_int, C.c_double, C.POINTER(C.c_void_p)],
     "smoq_dm_expect_zstrings": [_vp, C.c_int, C.POINTER(C.c_uint64), C.c_int, _dp],
+    "smoq_measure_all_observables": [_vp, C.c_int, C.c_int, _dp],
     "smoq_sample": [_vp, C.c_longlong, C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_longlong)],
     "smoq_measure_all": [_vp, C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_longlong)],
     "smoq_measure_qubit": [_vp, C.c_int, C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_int)],

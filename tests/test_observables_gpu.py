@@ -95,3 +95,29 @@ def test_many_observables_in_chunks(ctx):
     for o, m in enumerate(masks):
         sign = np.array([1 - 2 * (bin(i & m).count("1") & 1) for i in range(1 << N)])
         assert abs(got[o] - np.sum(p * sign)) < 1e-12
+
+
+@pytest.mark.parametrize("L,rails,dtype,tol", [(5, 2, S.C128, 1e-12), (4, 3, S.C64, 1e-5), (9, 1, S.C128, 1e-12)])
+def test_measure_all_observables_ladder(ctx, L, rails, dtype, tol):
+    """measure_all_observables_state_vector_cpu! order and values: local X, Y, Z per
+    qubit, then XX, YY, ZZ per rail bond, then per rung, against the oracle's
+    _expect_* restatements, for two states of a batch"""
+    N = L * rails
+    rng = np.random.default_rng(N + rails)
+    states = []
+    for _ in range(2):
+        v = rng.normal(size=1 << N) + 1j * rng.normal(size=1 << N)
+        states.append(v / np.linalg.norm(v))
+    st = S.CuState(ctx, N, dtype, 2, basis=None)
+    st.upload(np.concatenate(states).astype(np.complex128 if dtype == S.C128 else np.complex64))
+    got = S.measure_all_observables_state_vector(st, L, rails)
+    for b, psi in enumerate(states):
+        want = []
+        for k in range(1, N + 1):
+            want += [O.expect_local(psi, k, N, p) for p in "xyz"]
+        pairs = [(r * L + s, r * L + s + 1) for r in range(rails) for s in range(1, L)]
+        pairs += [(r * L + s, (r + 1) * L + s) for r in range(rails - 1) for s in range(1, L + 1)]
+        for i, j in pairs:
+            want += [O.expect_corr(psi, i, j, N, pp) for pp in ("xx", "yy", "zz")]
+        assert got.shape == (2, len(want))
+        assert np.max(np.abs(got[b] - np.array(want))) < tol
