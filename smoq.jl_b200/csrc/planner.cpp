@@ -234,15 +234,37 @@ void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op) {
     }
     for (int r = 0; r < 8; ++r) op.perm[r] = r;
     if (gt.special == OPK_INNER) {
-        // generator G as a dense row-major matrix on the op's qubits
+        // generator G (dense row-major on the op's qubits) re-encoded as a signed
+        // monomial: row r has at most one nonzero, i^code at column perm[1 + r]
         op.kind = OPK_INNER;
         op.nq = gt.nq;
+        if (gt.nq < 1 || gt.nq > 2) throw std::runtime_error("adjoint generator must act on 1 or 2 qubits");
         for (int t = 0; t < gt.nq; ++t) {
             op.gb[t] = gt.q[t];
             op.lb[t] = local_bit(g, gt.q[t]);
         }
-        fill_coeffs(op, gt.m, 1 << (2 * gt.nq));
-        op.perm[0] = (int32_t)gt.aux2;  // slot in the pass's partials (set by the caller)
+        const int dim = 1 << gt.nq;
+        bool diag = true;
+        for (int r = 0; r < dim; ++r) {
+            int col = r, code = INNER_ZERO, nz = 0;
+            for (int c = 0; c < dim; ++c) {
+                const cd x = gt.m[r * dim + c];
+                if (std::abs(x) == 0.0) continue;
+                ++nz;
+                col = c;
+                if (x == cd(1.0, 0.0)) code = 0;
+                else if (x == cd(0.0, 1.0)) code = 1;
+                else if (x == cd(-1.0, 0.0)) code = 2;
+                else if (x == cd(0.0, -1.0)) code = 3;
+                else throw std::runtime_error("adjoint generator entries must be +-1 or +-i");
+            }
+            if (nz > 1) throw std::runtime_error("adjoint generator must be a signed Pauli monomial");
+            op.perm[1 + r] = col;
+            op.slot[r] = code;
+            if (col != r || code == 1 || code == 3) diag = false;  // real diagonal only
+        }
+        op.flags = diag ? INNER_DIAGG : 0;
+        op.perm[0] = (int32_t)gt.aux2;  // the caller's index of this measurement
         return;
     }
     if (gt.special) {

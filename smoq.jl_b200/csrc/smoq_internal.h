@@ -38,14 +38,20 @@ enum OpKind : int32_t {
                       // nq = 0 marks a single op applied by a plain shared-memory sweep;
                       // nq = 5 a 5-bit stage (compiled kernels only): perm[0..4] = bits,
                       // lb[0..3] = rotation lanes
-    OPK_INNER = 9,    // adjoint sweep: per-tile Im<lambda|G|phi> with G = cd (dense, 1-2
-                      // qubits), written to partials slot perm[0] of the pass
+    OPK_INNER = 9,    // adjoint sweep: Im<lambda|G|phi> on 1-2 tile bits, accumulated into
+                      // partials column perm[0]; G is a signed monomial: row r holds i^slot[r]
+                      // at column perm[1 + r] (slot[r] = INNER_ZERO: an all-zero row);
+                      // flags: INNER_DIAGG (G real diagonal), INNER_PRE (cd/cf hold a dense
+                      // 2^nq x 2^nq matrix applied to both states first)
     OPK_LAYOUT = 8,   // register-tile layout change: perm[0..KR-1] = register bits,
                       // perm[5..7] = warp bits (tile-local bit positions)
 };
 
 // Placement of an op qubit in the register-tile engine: slot = type << 8 | index
 enum SlotType : int32_t { SLOT_LANE = 0, SLOT_REG = 1, SLOT_WARP = 2, SLOT_OFF = 3 };
+
+// OPK_INNER encoding details
+enum InnerBits : int32_t { INNER_ZERO = 4, INNER_DIAGG = 1, INNER_PRE = 2 };
 
 struct alignas(16) DevOp {
     int32_t kind;

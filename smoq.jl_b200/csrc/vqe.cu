@@ -14,8 +14,13 @@
 //    phi per term;
 //  * adj_tile_kernel: the backward sweep as fused passes over (phi, lambda)
 //    tile pairs: both tiles come into shared memory by bulk copy, the pass's
-//    program (U^dag ops and OPK_INNER measurements, in order) runs on both,
-//    every OPK_INNER writes its FP64 per-tile partial.
+//    program (U^dag ops and OPK_INNER measurements, in order) runs on both.
+//    Generators are signed Pauli monomials, so a measurement is a few FMAs
+//    per amplitude pair in the state's precision; a U^dag op directly before
+//    a measurement on the same qubits is applied in the same sweep, and runs
+//    of real-diagonal measurements (RZ, RZZ) share one read of the tiles.
+//    Each warp adds its FP64 sum of a measurement to its own row of the
+//    partials; adj_colsum_kernel reduces the rows.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -77,59 +82,159 @@ __global__ void __launch_bounds__(256) ham_apply_kernel(const typename CT<R>::T*
     }
 }
 
+// ---------------------------------------------------------------- backward sweep
+// The adjoint pass works on a PAIR of tiles in shared memory: P (phi) and Q
+// (lambda), 2^T amplitudes each, and applies every U^dag op to both in the
+// same loop iteration (one index decode, one coefficient load for both).
+
+// U^dag op on both tiles; dco: 16 shared-memory slots for diagonal tables
 template <typename R>
-__device__ __forceinline__ void adj_diag(const DevOp& op, typename CT<R>::T* tile, uint32_t amps, uint64_t base) {
-    int sh[4] = {-1, -1, -1, -1};
-    int cm = 0;
-    for (int t = 0; t < op.nq; ++t) {
-        if (op.lb[t] >= 0) sh[t] = op.lb[t];
-        else cm |= (int)((base >> op.gb[t]) & 1) << t;
-    }
-    for (uint32_t j = threadIdx.x; j < amps; j += blockDim.x) {
-        int m = cm;
+__device__ __forceinline__ void dual_apply(const DevOp& op, typename CT<R>::T* P, typename CT<R>::T* Q, int T,
+                                           uint64_t base, typename CT<R>::T* dco) {
+    using C = typename CT<R>::T;
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    if (op.kind == OPK_DENSE1) {
+        const int a = op.lb[0];
+        const C m0 = coef<R>(op, 0), m1 = coef<R>(op, 1), m2 = coef<R>(op, 2), m3 = coef<R>(op, 3);
+        for (uint32_t g = tid; g < (1u << (T - 1)); g += nthr) {
+            const uint32_t i0 = ins0<uint32_t>(g, a), i1 = i0 | (1u << a);
+            const C x = P[i0], y = P[i1], u = Q[i0], v = Q[i1];
+            P[i0] = cfma(m0, x, cmul(m1, y));
+            P[i1] = cfma(m2, x, cmul(m3, y));
+            Q[i0] = cfma(m0, u, cmul(m1, v));
+            Q[i1] = cfma(m2, u, cmul(m3, v));
+        }
+    } else if (op.kind == OPK_DENSE2) {
+        const int a = op.lb[0], b = op.lb[1];
+        const int lo = a < b ? a : b, hi = a < b ? b : a;
+        C m[16];
 #pragma unroll
-        for (int t = 0; t < 4; ++t)
-            if (sh[t] >= 0) m |= (int)((j >> sh[t]) & 1) << t;
-        tile[j] = cmul(coef<R>(op, m), tile[j]);
+        for (int k = 0; k < 16; ++k) m[k] = coef<R>(op, k);
+        for (uint32_t g = tid; g < (1u << (T - 2)); g += nthr) {
+            const uint32_t i0 = ins0<uint32_t>(ins0<uint32_t>(g, lo), hi);
+            const uint32_t ix[4] = {i0, i0 | (1u << a), i0 | (1u << b), i0 | (1u << a) | (1u << b)};
+            C x[4], y[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) x[k] = P[ix[k]], y[k] = Q[ix[k]];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                C s = cmul(m[4 * r], x[0]), t = cmul(m[4 * r], y[0]);
+#pragma unroll
+                for (int c = 1; c < 4; ++c) s = cfma(m[4 * r + c], x[c], s), t = cfma(m[4 * r + c], y[c], t);
+                P[ix[r]] = s;
+                Q[ix[r]] = t;
+            }
+        }
+    } else if (op.kind == OPK_PARITY2) {
+        const int a = op.lb[0], b = op.lb[1];
+        const int lo = a < b ? a : b, hi = a < b ? b : a;
+        const C e0 = coef<R>(op, 0), e1 = coef<R>(op, 1), e2 = coef<R>(op, 2), e3 = coef<R>(op, 3);
+        const C o0 = coef<R>(op, 4), o1 = coef<R>(op, 5), o2 = coef<R>(op, 6), o3 = coef<R>(op, 7);
+        for (uint32_t g = tid; g < (1u << (T - 2)); g += nthr) {
+            const uint32_t i0 = ins0<uint32_t>(ins0<uint32_t>(g, lo), hi);
+            const uint32_t i1 = i0 | (1u << a), i2 = i0 | (1u << b), i3 = i1 | (1u << b);
+            C v0 = P[i0], v1 = P[i1], v2 = P[i2], v3 = P[i3];
+            P[i0] = cfma(e0, v0, cmul(e1, v3));
+            P[i3] = cfma(e2, v0, cmul(e3, v3));
+            P[i1] = cfma(o0, v1, cmul(o1, v2));
+            P[i2] = cfma(o2, v1, cmul(o3, v2));
+            v0 = Q[i0], v1 = Q[i1], v2 = Q[i2], v3 = Q[i3];
+            Q[i0] = cfma(e0, v0, cmul(e1, v3));
+            Q[i3] = cfma(e2, v0, cmul(e3, v3));
+            Q[i1] = cfma(o0, v1, cmul(o1, v2));
+            Q[i2] = cfma(o2, v1, cmul(o3, v2));
+        }
+    } else if (op.kind == OPK_DIAG) {
+        // table index m = the op's qubit bits; qubits outside the tile are fixed by base
+        int sh[4] = {0, 0, 0, 0}, in = 0, cm = 0;
+        for (int t = 0; t < op.nq; ++t) {
+            if (op.lb[t] >= 0) sh[t] = op.lb[t], in |= 1 << t;
+            else cm |= (int)((base >> op.gb[t]) & 1) << t;
+        }
+        if (tid < 16) dco[tid] = coef<R>(op, (int)tid);
+        __syncthreads();
+        for (uint32_t j = tid; j < (1u << T); j += nthr) {
+            int m = cm;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) m |= (int)((j >> sh[t]) & (uint32_t)(in >> t) & 1u) << t;
+            const C c = dco[m];
+            P[j] = cmul(c, P[j]);
+            Q[j] = cmul(c, Q[j]);
+        }
+    } else {  // OPK_MONO
+        sweep_op<R, uint32_t>(op, P, T, op.lb, tid, nthr);
+        sweep_op<R, uint32_t>(op, Q, T, op.lb, tid, nthr);
     }
 }
 
-// Im sum_i conj(lam_i) (G phi)_i over the tile, G dense on 1 or 2 tile bits
+// weights of a monomial entry i^code: Im(conj(l) i^code p) = wi Im z + wr Re z, z = conj(l) p
 template <typename R>
-__device__ __forceinline__ double adj_inner(const DevOp& op, const typename CT<R>::T* P,
-                                            const typename CT<R>::T* L, int T) {
+__device__ __forceinline__ void code_weights(int code, R& wr, R& wi) {
+    wi = code == 0 ? R(1) : code == 2 ? R(-1) : R(0);
+    wr = code == 1 ? R(1) : code == 3 ? R(-1) : R(0);
+}
+
+template <typename R>
+__device__ __forceinline__ R im_term(typename CT<R>::T l, typename CT<R>::T p, R wr, R wi) {
+    const R zr = fma(l.x, p.x, l.y * p.y);
+    const R zi = fma(l.x, p.y, -l.y * p.x);
+    return fma(wi, zi, wr * zr);
+}
+
+template <typename C>
+__device__ __forceinline__ C pick4(const C* v, int c) {
+    return (c & 2) ? ((c & 1) ? v[3] : v[2]) : ((c & 1) ? v[1] : v[0]);
+}
+
+// this thread's share of Im<lambda|G|phi> over the tile pair, G a signed
+// monomial on 1 or 2 tile bits; PRE: the op's dense matrix is applied to both
+// tiles first (and written back)
+template <typename R, int NQ, bool PRE>
+__device__ __forceinline__ R inner_pairs(const DevOp& op, typename CT<R>::T* P, typename CT<R>::T* Q, int T) {
     using C = typename CT<R>::T;
-    double acc = 0;
-    if (op.nq == 1) {
-        const int a = op.lb[0];
-        const C g00 = coef<R>(op, 0), g01 = coef<R>(op, 1), g10 = coef<R>(op, 2), g11 = coef<R>(op, 3);
-        for (uint32_t g = threadIdx.x; g < (1u << (T - 1)); g += blockDim.x) {
-            const uint32_t i0 = ins0<uint32_t>(g, a), i1 = i0 | (1u << a);
-            const C p0 = P[i0], p1 = P[i1], l0 = L[i0], l1 = L[i1];
-            const C q0 = cfma(g00, p0, cmul(g01, p1)), q1 = cfma(g10, p0, cmul(g11, p1));
-            acc += (double)l0.x * q0.y - (double)l0.y * q0.x + (double)l1.x * q1.y - (double)l1.y * q1.x;
-        }
-    } else {
-        const int a = op.lb[0], b = op.lb[1];
-        const int lo = a < b ? a : b, hi = a < b ? b : a;
-        C G[16];
+    constexpr int D = 1 << NQ;
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    R wr[D], wi[D];
+    int col[D];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) G[k] = coef<R>(op, k);
-        for (uint32_t g = threadIdx.x; g < (1u << (T - 2)); g += blockDim.x) {
+    for (int r = 0; r < D; ++r) code_weights<R>(op.slot[r], wr[r], wi[r]), col[r] = op.perm[1 + r];
+    C m[D * D];
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) m[k] = PRE ? coef<R>(op, k) : C{};
+    const int a = op.lb[0], b = NQ == 2 ? op.lb[1] : 0;
+    const int lo = a < b ? a : b, hi = a < b ? b : a;
+    R acc = 0;
+    for (uint32_t g = tid; g < (1u << (T - NQ)); g += nthr) {
+        uint32_t ix[D];
+        if (NQ == 1) {
+            ix[0] = ins0<uint32_t>(g, a);
+            ix[D - 1] = ix[0] | (1u << a);
+        } else {
             const uint32_t i0 = ins0<uint32_t>(ins0<uint32_t>(g, lo), hi);
-            const uint32_t ix[4] = {i0, i0 | (1u << a), i0 | (1u << b), i0 | (1u << a) | (1u << b)};
-            C p[4];
+            ix[0] = i0;
+            ix[1 % D] = i0 | (1u << a);
+            ix[2 % D] = i0 | (1u << b);
+            ix[D - 1] = i0 | (1u << a) | (1u << b);
+        }
+        C p[D], l[D];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) p[k] = P[ix[k]];
+        for (int k = 0; k < D; ++k) p[k] = P[ix[k]], l[k] = Q[ix[k]];
+        if (PRE) {
+            C x[D], y[D];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                C q = cmul(G[4 * r], p[0]);
-                q = cfma(G[4 * r + 1], p[1], q);
-                q = cfma(G[4 * r + 2], p[2], q);
-                q = cfma(G[4 * r + 3], p[3], q);
-                const C l = L[ix[r]];
-                acc += (double)l.x * q.y - (double)l.y * q.x;
+            for (int r = 0; r < D; ++r) {
+                x[r] = cmul(m[r * D], p[0]);
+                y[r] = cmul(m[r * D], l[0]);
+#pragma unroll
+                for (int c = 1; c < D; ++c) x[r] = cfma(m[r * D + c], p[c], x[r]), y[r] = cfma(m[r * D + c], l[c], y[r]);
             }
+#pragma unroll
+            for (int k = 0; k < D; ++k) p[k] = x[k], l[k] = y[k], P[ix[k]] = x[k], Q[ix[k]] = y[k];
+        }
+#pragma unroll
+        for (int r = 0; r < D; ++r) {
+            const C pc = D == 2 ? (col[r] ? p[D - 1] : p[0]) : pick4(p, col[r]);
+            acc += im_term<R>(l[r], pc, wr[r], wi[r]);
         }
     }
     return acc;
@@ -138,13 +243,43 @@ __device__ __forceinline__ double adj_inner(const DevOp& op, const typename CT<R
 struct AdjArgs {
     TileArgs a;      // a.psi = phi
     void* lam;
-    double* partials;
-    int64_t n_partials;  // entries of partials (diagnostic bounds checks)
-    int32_t n_inner;
+    double* partials;  // [n_rows][n_cols]: row = CTA x warps + warp, column = measurement
+    int64_t n_rows;
+    int32_t n_cols;
 };
 
+// warp sum of one measurement, added to this warp's row of the partials
 template <typename R>
-__global__ void __launch_bounds__(256) adj_tile_kernel(const AdjArgs A) {
+__device__ __forceinline__ void inner_flush(R acc, const AdjArgs& A, int col) {
+    double x = (double)acc;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) x += __shfl_xor_sync(0xffffffffu, x, d);
+    if ((threadIdx.x & 31) == 0) {
+        const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        if (SMOQ_INBOUNDS(col >= 0 && col < A.n_cols && row < A.n_rows, A.a.err, 4))
+            atomicAdd(&A.partials[row * A.n_cols + col], x);
+    }
+}
+
+// descriptor of a real-diagonal measurement for the run sweep: lb0 | lb1 << 5 |
+// negative rows << 10 | zero rows << 14, rows indexed b(lb0) + 2 b(lb1) (a
+// 1-qubit op uses lb1 = lb0: rows 0 and 3)
+__device__ __forceinline__ uint32_t diag_desc(const DevOp& op) {
+    const uint32_t l0 = (uint32_t)op.lb[0], l1 = op.nq == 2 ? (uint32_t)op.lb[1] : l0;
+    uint32_t neg = 0, zero = 0;
+    for (int r = 0; r < (1 << op.nq); ++r) {
+        const int row = op.nq == 2 ? r : 3 * r;
+        if (op.slot[r] == 2) neg |= 1u << row;
+        if (op.slot[r] == INNER_ZERO) zero |= 1u << row;
+    }
+    return l0 | l1 << 5 | neg << 10 | zero << 14;
+}
+
+constexpr int kDiagRun = 8;  // real-diagonal measurements folded into one sweep
+
+// 2 (complex128) or 3 (complex64) CTAs per SM: one CTA's bulk copies overlap another's sweeps
+template <typename R>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) adj_tile_kernel(const AdjArgs A) {
     using C = typename CT<R>::T;
     const TileArgs& a = A.a;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -153,7 +288,7 @@ __global__ void __launch_bounds__(256) adj_tile_kernel(const AdjArgs A) {
     C* tP = reinterpret_cast<C*>(smem_raw);
     C* tL = tP + amps;
     __shared__ __align__(8) uint64_t bar;
-    __shared__ double red[8];
+    __shared__ C dco[16];
     const int tid = threadIdx.x;
     const uint32_t nseg = 1u << H;
     const uint32_t seg_bytes = (uint32_t)sizeof(C) << L;
@@ -183,28 +318,52 @@ __global__ void __launch_bounds__(256) adj_tile_kernel(const AdjArgs A) {
             return;
         }
         phase ^= 1;
-        for (int o = 0; o < a.nops; ++o) {
+        for (int o = 0; o < a.nops;) {
             const DevOp& op = a.ops[o];
-            if (op.kind == OPK_INNER) {
-                double x = adj_inner<R>(op, tP, tL, T);
-                for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
-                if ((tid & 31) == 0) red[tid >> 5] = x;
-                __syncthreads();
-                if (tid == 0) {
-                    double s = 0;
-                    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-                    const int64_t pi = t * A.n_inner + op.perm[0];
-                    if (SMOQ_INBOUNDS(pi >= 0 && pi < A.n_partials && op.perm[0] < A.n_inner, a.err, 4))
-                        A.partials[pi] = s;
+            bool writes = true;
+            if (op.kind == OPK_INNER && op.flags == INNER_DIAGG) {
+                // a run of real-diagonal measurements (RZ, RZZ generators): one read
+                // of both tiles, Im(conj(l) p) signed per measurement
+                int k = 1;
+                while (k < kDiagRun && o + k < a.nops && a.ops[o + k].kind == OPK_INNER &&
+                       a.ops[o + k].flags == INNER_DIAGG)
+                    ++k;
+                uint32_t d[kDiagRun];
+                R acc[kDiagRun];
+#pragma unroll
+                for (int u = 0; u < kDiagRun; ++u) acc[u] = 0, d[u] = u < k ? diag_desc(a.ops[o + u]) : 0u;
+                for (uint32_t j = tid; j < amps; j += blockDim.x) {
+                    const C p = tP[j], l = tL[j];
+                    const R zi = fma(l.x, p.y, -l.y * p.x);
+#pragma unroll
+                    for (int u = 0; u < kDiagRun; ++u) {
+                        if (u < k) {
+                            const uint32_t r = ((j >> (d[u] & 31)) & 1) | (((j >> ((d[u] >> 5) & 31)) & 1) << 1);
+                            const R x = ((d[u] >> (10 + r)) & 1) ? -zi : zi;
+                            acc[u] += ((d[u] >> (14 + r)) & 1) ? R(0) : x;
+                        }
+                    }
                 }
-            } else if (op.kind == OPK_DIAG) {
-                adj_diag<R>(op, tP, amps, base);
-                adj_diag<R>(op, tL, amps, base);
+#pragma unroll
+                for (int u = 0; u < kDiagRun; ++u)
+                    if (u < k) inner_flush<R>(acc[u], A, a.ops[o + u].perm[0]);
+                o += k;
+                writes = false;
+            } else if (op.kind == OPK_INNER) {
+                const bool pre = op.flags & INNER_PRE;
+                R acc;
+                if (op.nq == 1) acc = pre ? inner_pairs<R, 1, true>(op, tP, tL, T) : inner_pairs<R, 1, false>(op, tP, tL, T);
+                else acc = pre ? inner_pairs<R, 2, true>(op, tP, tL, T) : inner_pairs<R, 2, false>(op, tP, tL, T);
+                inner_flush<R>(acc, A, op.perm[0]);
+                writes = pre;
+                ++o;
             } else {
-                sweep_op<R, uint32_t>(op, tP, T, op.lb, (uint32_t)tid, (uint32_t)blockDim.x);
-                sweep_op<R, uint32_t>(op, tL, T, op.lb, (uint32_t)tid, (uint32_t)blockDim.x);
+                dual_apply<R>(op, tP, tL, T, base, dco);
+                ++o;
             }
-            __syncthreads();
+            // consecutive read-only measurements need no barrier between them
+            const bool next_writes = o < a.nops && !(a.ops[o].kind == OPK_INNER && !(a.ops[o].flags & INNER_PRE));
+            if (writes || next_writes) __syncthreads();
         }
         fence_proxy_async_smem();
         __syncthreads();
@@ -221,6 +380,25 @@ __global__ void __launch_bounds__(256) adj_tile_kernel(const AdjArgs A) {
         __syncthreads();
     }
     bulk_wait0();
+}
+
+// partial columns summed over rows: out[c] = sum_r part[r][c]; a block of
+// 32 x 32 threads takes 32 columns, its 32 row lanes stride over the rows
+__global__ void __launch_bounds__(1024) adj_colsum_kernel(const double* part, int64_t rows, int32_t cols, double* out) {
+    __shared__ double red[32][33];
+    const int lane = threadIdx.x & 31, rl = threadIdx.x >> 5;
+    const int c = blockIdx.x * 32 + lane;
+    double s = 0;
+    if (c < cols)
+#pragma unroll 4
+        for (int64_t r = rl; r < rows; r += 32) s += part[r * cols + c];
+    red[rl][lane] = s;
+    __syncthreads();
+    if (rl == 0 && c < cols) {
+        double t = 0;
+        for (int k = 0; k < 32; ++k) t += red[k][lane];
+        out[c] = t;
+    }
 }
 
 }  // namespace smoq
@@ -293,7 +471,83 @@ struct Work {
     }
 };
 
+constexpr int kAdjThreads = 256;  // the adjoint kernel's __launch_bounds__
+
+// dense row-major matrix of a 1- or 2-qubit U^dag op (false: not a dense/diagonal kind)
+bool op_dense(const DevOp& op, cd* M) {
+    const int dim = 1 << op.nq;
+    for (int k = 0; k < dim * dim; ++k) M[k] = 0.0;
+    auto c = [&](int k) { return cd(op.cd[k].x, op.cd[k].y); };
+    switch (op.kind) {
+        case OPK_DENSE1:
+        case OPK_DENSE2:
+            for (int k = 0; k < dim * dim; ++k) M[k] = c(k);
+            return true;
+        case OPK_DIAG:
+            for (int k = 0; k < dim; ++k) M[k * dim + k] = c(k);
+            return true;
+        case OPK_PARITY2:  // even block on local indices (0, 3), odd block on (1, 2)
+            M[0] = c(0); M[3] = c(1); M[12] = c(2); M[15] = c(3);
+            M[5] = c(4); M[6] = c(5); M[9] = c(6); M[10] = c(7);
+            return true;
+        default: return false;
+    }
+}
+
+// Fold a U^dag op that directly precedes a measurement on the same tile bits
+// into the measurement (INNER_PRE): one sweep of both tiles instead of two.
+smoq_status fuse_measurements(smoq_ctx* ctx, std::vector<DevOp>& ops) {
+    for (const DevOp& op : ops) {
+        const bool ok = op.kind == OPK_DENSE1 || op.kind == OPK_DENSE2 || op.kind == OPK_PARITY2 ||
+                        op.kind == OPK_MONO || op.kind == OPK_DIAG || op.kind == OPK_INNER;
+        if (!ok) return smoq_internal_fail(ctx, SMOQ_ERR_UNSUPPORTED, "adjoint pass holds an unsupported op kind");
+        if (op.kind == OPK_INNER)
+            for (int t = 0; t < op.nq; ++t)
+                if (op.lb[t] < 0) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "measurement qubit outside the tile");
+    }
+    std::vector<DevOp> out;
+    out.reserve(ops.size());
+    for (size_t i = 0; i < ops.size(); ++i) {
+        if (i + 1 < ops.size() && ops[i + 1].kind == OPK_INNER && ops[i].nq == ops[i + 1].nq) {
+            const DevOp& u = ops[i];
+            DevOp m = ops[i + 1];
+            const int nq = m.nq;
+            const bool same = u.lb[0] == m.lb[0] && (nq == 1 || u.lb[1] == m.lb[1]);
+            const bool swapped = nq == 2 && u.lb[0] == m.lb[1] && u.lb[1] == m.lb[0];
+            cd M[16];
+            if ((same || swapped) && u.lb[0] >= 0 && op_dense(u, M)) {
+                const int dim = 1 << nq;
+                auto sw = [&](int k) { return swapped ? (((k & 1) << 1) | (k >> 1)) : k; };
+                for (int r = 0; r < dim; ++r)
+                    for (int c = 0; c < dim; ++c) {
+                        const cd x = M[sw(r) * dim + sw(c)];
+                        m.cd[r * dim + c] = make_double2(x.real(), x.imag());
+                        m.cf[r * dim + c] = make_float2((float)x.real(), (float)x.imag());
+                    }
+                m.flags = INNER_PRE;
+                out.push_back(m);
+                ++i;
+                continue;
+            }
+        }
+        out.push_back(ops[i]);
+    }
+    ops.swap(out);
+    return SMOQ_OK;
+}
+
 }  // namespace
+
+// CTAs of the adjoint kernel: persistent grid, as many per SM as fit
+static int64_t adj_grid(smoq_ctx* ctx, smoq_dtype dtype, int64_t ntiles, size_t smem) {
+    int per_sm = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, dtype == SMOQ_C64 ? (const void*)adj_tile_kernel<float> : (const void*)adj_tile_kernel<double>,
+        kAdjThreads, smem);
+    if (e != cudaSuccess) (void)cudaGetLastError();
+    if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+    return std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)ctx->num_sms * per_sm));
+}
 
 static smoq_status check_vqe_args(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* ops, int n, int n_params,
                                   const smoq_pauli_term* H, int nterms, int batch, const double* theta) {
@@ -409,25 +663,28 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
         } catch (const std::exception& ex) {
             return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
         }
-        // per pass: local inner slots -> global inner index
-        std::vector<std::vector<int>> slot_global(passes.size());
-        std::vector<size_t> off(passes.size() + 1, 0), opoff(passes.size() + 1, 0);
+        std::vector<size_t> opoff(passes.size() + 1, 0);
+        std::vector<int64_t> grid(passes.size(), 0);
         std::vector<DevOp> all;
+        int64_t max_grid = 1;
         for (size_t i = 0; i < passes.size(); ++i) {
-            for (DevOp& op : passes[i].ops)
-                if (op.kind == OPK_INNER) {
-                    slot_global[i].push_back(op.perm[0]);
-                    op.perm[0] = (int32_t)slot_global[i].size() - 1;
-                }
-            const int64_t ntiles = (int64_t)1 << (N - passes[i].g.T);
-            off[i + 1] = off[i] + (size_t)ntiles * std::max<size_t>(1, slot_global[i].size());
+            if (smoq_status s = fuse_measurements(ctx, passes[i].ops)) return s;
             opoff[i + 1] = opoff[i] + passes[i].ops.size();
             all.insert(all.end(), passes[i].ops.begin(), passes[i].ops.end());
+            const size_t smem = (size_t)2 * w.phi.amp_bytes() << passes[i].g.T;
+            if (smem > kAdjMaxSmem) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "adjoint tile too wide");
+            grid[i] = adj_grid(ctx, dtype, (int64_t)1 << (N - passes[i].g.T), smem);
+            max_grid = std::max(max_grid, grid[i]);
         }
-        double* d_part;
+        // partials: one row per warp of the widest launch, one column per measurement
+        const int32_t ncols = (int32_t)inner_param.size();
+        const int64_t nrows = max_grid * (kAdjThreads / 32);
+        double *d_part, *d_sum;
         DevOp* d_ops;
-        VCK(cudaMallocAsync((void**)&d_part, off.back() * sizeof(double), ctx->stream));
+        VCK(cudaMallocAsync((void**)&d_part, (size_t)nrows * ncols * sizeof(double), ctx->stream));
+        VCK(cudaMallocAsync((void**)&d_sum, (size_t)ncols * sizeof(double), ctx->stream));
         VCK(cudaMallocAsync((void**)&d_ops, std::max<size_t>(1, all.size()) * sizeof(DevOp), ctx->stream));
+        VCK(cudaMemsetAsync(d_part, 0, (size_t)nrows * ncols * sizeof(double), ctx->stream));
         VCK(cudaMemcpyAsync(d_ops, all.data(), all.size() * sizeof(DevOp), cudaMemcpyHostToDevice, ctx->stream));
         for (size_t i = 0; i < passes.size(); ++i) {
             const Pass& p = passes[i];
@@ -444,23 +701,25 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
             A.a.ep.partials = nullptr;
             A.a.ep.npop = 0;
             A.lam = w.lam.ptr;
-            A.partials = d_part + off[i];
-            A.n_partials = (int64_t)(off[i + 1] - off[i]);
-            A.n_inner = (int32_t)std::max<size_t>(1, slot_global[i].size());
+            A.partials = d_part;
+            A.n_rows = nrows;
+            A.n_cols = ncols;
             const size_t smem = (size_t)2 * w.phi.amp_bytes() << p.g.T;
-            int grid = (int)std::min<int64_t>(A.a.ntiles, (int64_t)ctx->num_sms * 2);
             // (the kernels' shared-memory limit is set once per context, vqe_kernels_init:
             // setting it per launch would race between contexts driven from several threads)
-            if (smem > kAdjMaxSmem) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "adjoint tile too wide");
-            if (dtype == SMOQ_C64) adj_tile_kernel<float><<<grid, 256, smem, ctx->stream>>>(A);
-            else adj_tile_kernel<double><<<grid, 256, smem, ctx->stream>>>(A);
+            if (dtype == SMOQ_C64) adj_tile_kernel<float><<<(unsigned)grid[i], kAdjThreads, smem, ctx->stream>>>(A);
+            else adj_tile_kernel<double><<<(unsigned)grid[i], kAdjThreads, smem, ctx->stream>>>(A);
             ctx->launches++;
             ctx->tile_passes++;
             VCK(cudaGetLastError());
         }
-        std::vector<double> part(off.back());
-        VCK(cudaMemcpyAsync(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        adj_colsum_kernel<<<(unsigned)((ncols + 31) / 32), 1024, 0, ctx->stream>>>(d_part, nrows, ncols, d_sum);
+        ctx->launches++;
+        VCK(cudaGetLastError());
+        std::vector<double> colsum(ncols);
+        VCK(cudaMemcpyAsync(colsum.data(), d_sum, (size_t)ncols * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         VCK(cudaFreeAsync(d_part, ctx->stream));
+        VCK(cudaFreeAsync(d_sum, ctx->stream));
         VCK(cudaFreeAsync(d_ops, ctx->stream));
         VCK(cudaStreamSynchronize(ctx->stream));
         int32_t herr = 0;
@@ -472,16 +731,7 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
                                           ("device bounds check failed at site " + std::to_string(herr >> 8)).c_str());
             return smoq_internal_fail(ctx, SMOQ_ERR_TIMEOUT, "a bounded device wait ran out");
         }
-        for (size_t i = 0; i < passes.size(); ++i) {
-            const size_t ns = slot_global[i].size();
-            if (!ns) continue;
-            const int64_t ntiles = (int64_t)1 << (N - passes[i].g.T);
-            for (size_t sl = 0; sl < ns; ++sl) {
-                double s = 0;
-                for (int64_t t = 0; t < ntiles; ++t) s += part[off[i] + (size_t)t * ns + sl];
-                g[inner_param[slot_global[i][sl]]] += s;
-            }
-        }
+        for (int32_t c = 0; c < ncols; ++c) g[inner_param[c]] += colsum[c];
     }
     return SMOQ_OK;
 }

@@ -74,6 +74,54 @@ def test_all_generator_types_and_shared_parameters(ctx):
     assert np.max(np.abs(gr[0] - fd)) < 1e-7
 
 
+@pytest.mark.parametrize("seed", [11, 12])
+def test_all_generator_types_across_tiles(ctx, seed):
+    """N=14 (several tiles at both precisions): a random circuit of every
+    parameterised type on random qubits in both orders, fixed gates between,
+    and runs where a gate directly precedes another parameterised gate on the
+    same qubits (the measurement folds the gate into its sweep); gradient
+    against the oracle's central differences."""
+    N = 14
+    rng = np.random.default_rng(seed)
+    g = S.gate
+    ops, p = [], 1
+    one = ["rx", "ry", "rz"]
+    two = ["rxx", "ryy", "rzz", "cry"]
+    fixed1, fixed2 = ["h", "s", "t", "x"], ["cnot", "cz"]
+    for _ in range(60):
+        kind = rng.integers(0, 6)
+        q1 = int(rng.integers(1, N + 1))
+        q2 = int(rng.choice([q for q in range(1, N + 1) if q != q1]))
+        if kind == 0:
+            ops.append(g(str(rng.choice(one)), q1, param_idx=p)); p += 1
+        elif kind == 1:
+            ops.append(g(str(rng.choice(two)), [q1, q2], param_idx=p)); p += 1
+        elif kind == 2:   # two parameterised gates on the same qubit(s), back to back
+            ops.append(g(str(rng.choice(one)), q1, param_idx=p))
+            ops.append(g(str(rng.choice(one)), q1, param_idx=p + 1)); p += 2
+        elif kind == 3:
+            ops.append(g(str(rng.choice(two)), [q1, q2], param_idx=p))
+            ops.append(g(str(rng.choice(two)), [q2, q1], param_idx=p + 1)); p += 2
+        elif kind == 4:
+            ops.append(g(str(rng.choice(fixed1)), q1))
+        else:
+            ops.append(g(str(rng.choice(fixed2)), [q1, q2]))
+    circ = S.ParameterizedCircuit(N, ops)
+    theta = rng.uniform(-3, 3, size=circ.n_params)
+    terms = [(0.9, {1: "X", 9: "Y"}), (-0.6, {3: "Z", 14: "Z"}), (0.5, {12: "Y"}), (0.3, {2: "X", 7: "Z", 13: "Y"}),
+             (-0.4, {5: "Z"})]
+    oo = oracle_ops(circ)
+    arr = O.make_ops(oo)
+    e_ref = O.energy(arr, len(oo), theta, N, terms)
+    fd = O.grad(arr, len(oo), theta, N, terms, method="fd", eps=1e-5)  # (CRY has no two-term shift rule)
+    e, gr = S.energy_and_gradient(ctx, circ, S.PauliSum(terms), theta, dtype=S.C128)
+    assert abs(e[0] - e_ref) < 1e-11
+    assert np.max(np.abs(gr[0] - fd)) < 1e-7
+    e64, g64 = S.energy_and_gradient(ctx, circ, S.PauliSum(terms), theta, dtype=S.C64)
+    assert abs(e64[0] - e_ref) < 1e-5
+    assert np.max(np.abs(g64[0] - fd)) < 1e-4
+
+
 def test_batch_of_parameter_sets(ctx):
     N, L, B = 9, 2, 4
     circ, _ = hea(N, L)
