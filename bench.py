@@ -404,6 +404,75 @@ def mcwf_workload(args):
     return 0
 
 
+def qrc_workload(args):
+    """Quantum reservoir computing, the bitwise MCWF loop: two XXZ rails of L=6
+    qubits (N=12; rail bonds Jxx = Jyy = 1, Jzz = 0.5; rungs 0.7, 0.7, 0.3; x field
+    0.5 and seeded z fields), dt = 0.1, 5 Trotter steps per input, 100 seeded
+    inputs in [0, 1] (:batch window, :traceout_rail_1 reset), 4096 trajectories,
+    the 84 ladder features after every input.  metric = trajectory-inputs per
+    second through smoq_qrc_run (host inputs in, host feature means out: the
+    value is end to end).  CPU baseline: the oracle's restatement of the loop
+    (complex128, trajectories over all host cores) on a trajectory subset."""
+    import torch
+    import pysmoq as S
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    ctx = S.Context(0)
+    L, T, B, sub, dt = 6, 100, 4096, 5, 0.1
+    rng = np.random.default_rng(2026)
+    bonds = [(r * L + s + 1, r * L + s + 2, 1.0, 1.0, 0.5) for r in range(2) for s in range(L - 1)]
+    bonds += [(s + 1, L + s + 1, 0.7, 0.7, 0.3) for s in range(L)]
+    fields = [(q + 1, 0.5, 0.0, float(rng.uniform(-1, 1))) for q in range(2 * L)]
+    arr, n = O.precompute_trotter_gates(bonds, fields, dt)
+    gates = [S.FastTrotterGate(idx, U) for idx, U in O.gates_to_list(arr, n)]
+    u = rng.uniform(0, 1, T)
+    padded = np.concatenate([np.zeros(L), u])
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    res = {}
+    for name, dt_ in (("c64", S.C64), ("c128", S.C128)):
+        plan = S.TrotterPlan(ctx, 2 * L, gates, order=1, dtype=dt_)
+        for w in range(max(1, args.warmup)):
+            S.run_mcwf_simulation(None, None, plan, padded, L, 2, T, 256, n_substeps=sub, seed=100 + w)
+        e0, e1 = _events(torch, stream)
+        walls = []
+        e0.record(stream)
+        for k in range(args.steps):
+            t0 = time.perf_counter()
+            X = S.run_mcwf_simulation(None, None, plan, padded, L, 2, T, B, n_substeps=sub, seed=2026 + k)
+            walls.append(time.perf_counter() - t0)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        res[name] = (B * T * args.steps / (ms * 1e-3), ms / args.steps, B * T * args.steps / sum(walls), X,
+                     [round(w * 1e3, 1) for w in walls])
+        plan.close()
+    cpu = None
+    if not args.no_cpu_baseline:
+        ncpu = os.cpu_count() or 1
+        ntr = 4 * ncpu
+        t0 = time.perf_counter()
+        O.qrc_run(L, arr, n, u[:20], ntr, n_substeps=sub, seed=7, nthreads=ncpu)
+        sec = time.perf_counter() - t0
+        cpu = {"value": ntr * 20 / sec, "unit": "trajectory-inputs/s", "cores": ncpu, "kind": "port",
+               "sample": f"{ntr} trajectories x 20 inputs of the same configuration, complex128, {sec:.1f} s"}
+    X64, X128 = res["c64"][3], res["c128"][3]
+    line = {"metric": "qrc_trajectory_inputs_per_s", "value": res["c64"][0], "unit": "trajectory-inputs/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["c64"][1],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {"workload": "qrc_xxz_ladder_L6_4096traj_100inputs", "L": L, "N": 2 * L, "trajectories": B,
+                       "inputs": T, "n_substeps": sub, "features": S.qrc_n_ops(L), "encoding": "batch",
+                       "reset": "traceout_rail_1", "state_bytes_per_trajectory": (1 << (2 * L)) * 8},
+            "e2e": {"value": res["c64"][2], "unit": "trajectory-inputs/s",
+                    "h2d_bytes_per_step": int(padded.nbytes), "d2h_bytes_per_step": int(X64.nbytes)},
+            "e2e_ms_per_call": res["c64"][4],
+            "c128_trajectory_inputs_per_s": res["c128"][0],
+            "feature_mean_abs_diff_c64_vs_c128": float(np.mean(np.abs(X64 - X128))),
+            "gpu_launches": args.steps, "cpu_baseline": cpu}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
 def bandwidth_workload(args):
     """32 GiB single-state sweeps: N=32 complex64 and N=31 complex128, 20 layers of
     [Rx, Ry, Rz on every qubit (seeded angles); Rzz on a seeded random perfect
@@ -471,7 +540,7 @@ def main():
     ap.add_argument("--jit-packed", type=int, default=0, help="compiled pass kernels: FP32x2 arithmetic (1) or scalar (0)")
     ap.add_argument("--jit-groups", type=int, default=2, help="compiled pass kernels: register groups per thread (1, 2)")
     ap.add_argument("--jit-stage-bits", type=int, default=4, help="compiled pass kernels: bits per register stage (4, 5)")
-    ap.add_argument("--workload", default="trotter", choices=["trotter", "vqe", "vqe_jobs", "mcwf", "bandwidth"],
+    ap.add_argument("--workload", default="trotter", choices=["trotter", "vqe", "vqe_jobs", "mcwf", "bandwidth", "qrc"],
                     help="trotter: the headline line; vqe / bandwidth: the gradient and 32 GiB sweep figures")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -484,6 +553,8 @@ def main():
         return vqe_jobs_workload(args)
     if args.workload == "mcwf":
         return mcwf_workload(args)
+    if args.workload == "qrc":
+        return qrc_workload(args)
 
     ws, rank, local = dist_env()
     import torch

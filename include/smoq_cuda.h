@@ -256,6 +256,35 @@ smoq_status smoq_mcwf_run(smoq_plan* plan, smoq_state* st, const smoq_jump_op* o
                           int record_every, double* z_mean, double* zz_mean, double* z_traj,
                           double* zz_traj, int* jumps);
 
+/* ------------------------------------------- quantum reservoir computing (QRC) */
+/* The bitwise QRC trajectory loop: _run_traj_loop_bitwise! and the bitwise
+ * run_mcwf_simulation (utils/cpu/cpuQRCSimulationMonteCarloWaveFunction.jl:451,
+ * :531) with encode_input_ry_psi! and qrc_reset_psi! (utils/cpu/cpuQRCstep.jl:96,
+ * :332).  Two rails of L qubits (N = 2L; the reset reshapes the state as
+ * 2^L x 2^L).  Per input k: encode the window of inputs as Ry(pi u) rotations of
+ * the input rail (low L qubits), measure one rail by inverse-CDF sampling, keep
+ * the normalised state of the other rail as the new reservoir (high L qubits),
+ * run n_substeps steps of the plan's Trotter step, and measure the ladder's
+ * observable set (smoq_measure_all_observables order).  The draw r of
+ * trajectory traj_offset + t at input k is the 53-bit Philox4x32-10 uniform of
+ * smoq_sample with shot = k, stream = traj_offset + t, key = seed. */
+typedef struct {
+    int32_t L;             /* qubits per rail (N = 2L); <= 7 complex64, <= 6 complex128 */
+    int32_t n_substeps;    /* Trotter steps per input */
+    int32_t encoding;      /* 0 :batch (window u_{k-L+1..k}, zeros before the series), 1 :broadcast (u_k on every qubit) */
+    int32_t reset;         /* 1 :traceout_rail_1 (measure the input rail), 2 :traceout_rail_2 (measure the reservoir) */
+    uint64_t seed;
+    uint64_t traj_offset;
+} smoq_qrc_params;
+/* plan: a Trotter plan on N = 2L qubits (one step = the FastTrotterGate list);
+ * psi0: host 2^N complex128 (re, im interleaved), NULL = |0...0>; padded_u:
+ * T + L values, the input series after L leading zeros ([zeros(L); u], as
+ * run_mcwf_simulation builds it; values in [0, 1]); X (host, T * n_ops) receives the trajectory mean of every
+ * feature after every input, n_ops = 3N + 3 (L-1) 2 + 3 L; X_traj (host,
+ * n_traj * T * n_ops, or NULL) the per-trajectory features. */
+smoq_status smoq_qrc_run(smoq_plan* plan, const smoq_qrc_params* p, const double* psi0, const double* padded_u,
+                         int T, int64_t n_traj, double* X, double* X_traj);
+
 /* ------------------------------------------- VQE energy and adjoint gradient */
 typedef struct {           /* one Pauli-sum term: coef * prod of letters */
     double coef;

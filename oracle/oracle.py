@@ -103,6 +103,15 @@ _sig("so_dissipator_dm", [_cp, C.POINTER(JumpOp), C.c_double, C.c_int])
 _sig("so_expect_z_rho", [_cp, C.c_int, C.c_int], C.c_double)
 _sig("so_expect_zz_rho", [_cp, C.c_int, C.c_int, C.c_int], C.c_double)
 _sig("so_wtime", [], C.c_double)
+_sig("so_qrc_n_ops", [C.c_int, C.c_int], C.c_int)
+_sig("so_measure_all_observables", [_cp, C.c_int, C.c_int, _dp])
+_sig("so_qrc_window", [_dp, C.c_int, C.c_int, C.c_int, _dp])
+_sig("so_qrc_encode", [_dp, C.c_int, _cp])
+_sig("so_qrc_reset", [_cp, _cp, _cp, C.c_int, C.c_int, C.c_double], C.c_int)
+_sig("so_qrc_run", [C.c_int, C.POINTER(TrotterGate), C.c_int, C.c_int, C.c_int, C.c_int, _cp, _dp, C.c_int, C.c_int,
+                    C.c_uint64, C.c_uint64, _dp, _dp, C.c_int])
+_sig("so_qrc_dm_run", [C.c_int, C.POINTER(TrotterGate), C.c_int, C.c_int, C.c_int, C.c_int, _cp, _dp, C.c_int, _dp])
+_sig("so_expect_pauli_rho", [_cp, C.c_uint64, C.c_uint64, C.c_int], C.c_double)
 
 
 def zero_state(N, index=0):
@@ -372,3 +381,50 @@ def measure_all(psi, N, seed, stream=0):
 def measure_qubit(psi, k, N, seed, stream=0):
     """_measure_z_single! (cpuQuantumStateMeasurements.jl:224), in place, k 1-based"""
     return int(L.so_measure_qubit(_p(psi), k, N, seed, stream))
+
+
+# ---- quantum reservoir computing (bitwise MCWF path; two rails of L qubits)
+QRC_ENCODING = {"batch": 0, "batch_causal": 0, "broadcast": 1}
+QRC_RESET = {"traceout_rail_1": 1, "protocol1": 1, "traceout_rail_2": 2, "protocol2": 2}
+
+
+def qrc_n_ops(L, n_rails=2):
+    return 3 * L * n_rails + 3 * (L - 1) * n_rails + 3 * L * (n_rails - 1)
+
+
+def measure_all_observables(psi, L_, n_rails):
+    out = np.empty(qrc_n_ops(L_, n_rails))
+    L.so_measure_all_observables(_p(psi), L_, n_rails, out.ctypes.data_as(_dp))
+    return out
+
+
+def qrc_padded(inputs, L_):
+    return np.concatenate([np.zeros(L_), np.asarray(inputs, dtype=np.float64)])
+
+
+def qrc_run(L_, gates_arr, ng, inputs, n_traj, n_substeps=5, encoding="batch", reset="traceout_rail_1", seed=1234,
+            traj_offset=0, psi0=None, per_trajectory=False, nthreads=1):
+    """trajectory mean X[T, n_ops] (and, if asked, X_traj[n_traj, T, n_ops]) for the input series
+    `inputs` (padded with L zeros in front, as run_mcwf_simulation does)"""
+    T = len(inputs)
+    u = np.ascontiguousarray(qrc_padded(inputs, L_))
+    nops = qrc_n_ops(L_)
+    p0 = zero_state(2 * L_) if psi0 is None else np.ascontiguousarray(psi0, dtype=np.complex128)
+    X = np.empty(T * nops)
+    Xt = np.empty(n_traj * T * nops) if per_trajectory else None
+    L.so_qrc_run(L_, gates_arr, ng, n_substeps, QRC_ENCODING[encoding], QRC_RESET[reset], _p(p0),
+                 u.ctypes.data_as(_dp), T, n_traj, seed, traj_offset, X.ctypes.data_as(_dp),
+                 Xt.ctypes.data_as(_dp) if per_trajectory else None, nthreads)
+    X = X.reshape(T, nops)
+    return (X, Xt.reshape(n_traj, T, nops)) if per_trajectory else X
+
+
+def qrc_dm_run(L_, gates_arr, ng, inputs, n_substeps=5, encoding="batch", reset="traceout_rail_1", psi0=None):
+    T = len(inputs)
+    u = np.ascontiguousarray(qrc_padded(inputs, L_))
+    nops = qrc_n_ops(L_)
+    p0 = zero_state(2 * L_) if psi0 is None else np.ascontiguousarray(psi0, dtype=np.complex128)
+    X = np.empty(T * nops)
+    L.so_qrc_dm_run(L_, gates_arr, ng, n_substeps, QRC_ENCODING[encoding], QRC_RESET[reset], _p(p0),
+                    u.ctypes.data_as(_dp), T, X.ctypes.data_as(_dp))
+    return X.reshape(T, nops)

@@ -839,3 +839,212 @@ int so_measure_qubit(so_cplx* psi, int k, int N, uint64_t seed, uint64_t stream)
     for (int64_t i = 0; i < dim; i++) psi[i] *= f;
     return outcome;
 }
+
+/* ========================================================================
+ * Quantum reservoir computing, bitwise MCWF path
+ * (utils/cpu/cpuQRCSimulationMonteCarloWaveFunction.jl:451-530, :531-590;
+ * utils/cpu/cpuQRCstep.jl:96-113, :332-433, :457-475)
+ * ======================================================================== */
+int so_qrc_n_ops(int L, int n_rails) {
+    int N = L * n_rails;
+    return 3 * N + 3 * (L - 1) * n_rails + 3 * L * (n_rails - 1);
+}
+/* measure_all_observables_state_vector_cpu! (cpuQuantumStateObservables.jl:1483-1519) */
+void so_measure_all_observables(const C* psi, int L, int n_rails, double* out) {
+    int N = L * n_rails, idx = 0;
+    for (int k = 1; k <= N; k++) {
+        out[idx++] = so_expect_x(psi, k, N);
+        out[idx++] = so_expect_y(psi, k, N);
+        out[idx++] = so_expect_z(psi, k, N);
+    }
+    for (int rail = 1; rail <= n_rails; rail++)
+        for (int site = 1; site <= L - 1; site++) {
+            int i = (rail - 1) * L + site, j = i + 1;
+            out[idx++] = so_expect_xx(psi, i, j, N);
+            out[idx++] = so_expect_yy(psi, i, j, N);
+            out[idx++] = so_expect_zz(psi, i, j, N);
+        }
+    for (int rail = 1; rail <= n_rails - 1; rail++)
+        for (int site = 1; site <= L; site++) {
+            int i = (rail - 1) * L + site, j = rail * L + site;
+            out[idx++] = so_expect_xx(psi, i, j, N);
+            out[idx++] = so_expect_yy(psi, i, j, N);
+            out[idx++] = so_expect_zz(psi, i, j, N);
+        }
+}
+/* the input window of step k (0-based), :481-489, from padded_u (T + L values,
+ * [zeros(L); u] in run_mcwf_simulation): :batch -> win[q] = padded_u[k + q]
+ * (1-based k, q), :broadcast -> padded_u[k + L] */
+void so_qrc_window(const double* padded_u, int L, int k, int encoding, double* win) {
+    for (int q = 0; q < L; q++) win[q] = padded_u[encoding == 1 ? (int64_t)k + L : (int64_t)k + q + 1];
+}
+/* encode_input_ry_psi! (cpuQRCstep.jl:96): |0..0>, then Ry(pi u_q) on qubit q */
+void so_qrc_encode(const double* win, int L, C* psi_in) {
+    int64_t dim = 1LL << L;
+    for (int64_t i = 0; i < dim; i++) psi_in[i] = 0;
+    psi_in[0] = 1;
+    for (int k = 1; k <= L; k++) so_apply_ry_psi(psi_in, k, M_PI * win[k - 1], L);
+}
+/* qrc_reset_psi! (cpuQRCstep.jl:332-433) for L_in = L_res = L; returns the outcome */
+int so_qrc_reset(C* out, const C* psi, const C* psi_in, int L, int protocol, double r) {
+    int64_t d = 1LL << L;
+    double total = 0, cum = 0;
+    int64_t outcome = 0;
+    /* M[i, j] = psi[i + d j]: i the input rail (low bits), j the reservoir */
+    if (protocol == 1) {
+        for (int64_t i = 0; i < d; i++)
+            for (int64_t j = 0; j < d; j++) total += abs2(psi[i + d * j]);
+        for (int64_t i = 0; i < d; i++) {
+            double row = 0;
+            for (int64_t j = 0; j < d; j++) row += abs2(psi[i + d * j]);
+            cum += row / total;
+            if (r <= cum) { outcome = i; break; }
+        }
+    } else {
+        for (int64_t j = 0; j < d; j++)
+            for (int64_t i = 0; i < d; i++) total += abs2(psi[i + d * j]);
+        for (int64_t j = 0; j < d; j++) {
+            double col = 0;
+            for (int64_t i = 0; i < d; i++) col += abs2(psi[i + d * j]);
+            cum += col / total;
+            if (r <= cum) { outcome = j; break; }
+        }
+    }
+    C* phi = (C*)malloc(d * sizeof(C));
+    double nsq = 0;
+    for (int64_t y = 0; y < d; y++) {
+        phi[y] = protocol == 1 ? psi[outcome + d * y] : psi[y + d * outcome];
+        nsq += abs2(phi[y]);
+    }
+    double nrm = sqrt(nsq);
+    if (nrm > 1e-12) {
+        for (int64_t y = 0; y < d; y++) phi[y] /= nrm;
+    } else {
+        for (int64_t y = 0; y < d; y++) phi[y] = 0;
+        phi[0] = 1;
+    }
+    /* tensor_product_ket! (cpuQuantumStatePreparation.jl:1136): psi_in on the low bits */
+    for (int64_t a = 0; a < d; a++)
+        for (int64_t b = 0; b < d; b++) out[a + (b << L)] = psi_in[a] * phi[b];
+    free(phi);
+    return (int)outcome;
+}
+typedef struct {
+    int L, ng, n_substeps, encoding, protocol, T, n_traj, nthreads, tid;
+    const so_trotter_gate* g;
+    const C* psi0;
+    const double* u;
+    uint64_t seed, traj_offset;
+    double* X_traj; /* [n_traj][T][n_ops] */
+} qrc_job;
+static void* qrc_worker(void* arg) {
+    qrc_job* J = (qrc_job*)arg;
+    int L = J->L, N = 2 * L, nops = so_qrc_n_ops(L, 2);
+    int64_t dim = 1LL << N, d = 1LL << L;
+    C* psi = (C*)malloc(dim * sizeof(C));
+    C* nxt = (C*)malloc(dim * sizeof(C));
+    C* pin = (C*)malloc(d * sizeof(C));
+    double* win = (double*)malloc(L * sizeof(double));
+    for (int t = J->tid; t < J->n_traj; t += J->nthreads) {
+        memcpy(psi, J->psi0, dim * sizeof(C));
+        uint64_t traj = J->traj_offset + (uint64_t)t;
+        for (int k = 0; k < J->T; k++) {
+            so_qrc_window(J->u, L, k, J->encoding, win);
+            so_qrc_encode(win, L, pin);
+            so_qrc_reset(nxt, psi, pin, L, J->protocol, shot_u(J->seed, (uint64_t)k, traj));
+            for (int s = 0; s < J->n_substeps; s++) so_trotter_step(nxt, J->g, J->ng, N);
+            memcpy(psi, nxt, dim * sizeof(C));
+            so_measure_all_observables(psi, L, 2, J->X_traj + ((int64_t)t * J->T + k) * nops);
+        }
+    }
+    free(psi); free(nxt); free(pin); free(win);
+    return NULL;
+}
+void so_qrc_run(int L, const so_trotter_gate* g, int ng, int n_substeps, int encoding, int protocol,
+                const C* psi0, const double* u, int T, int n_traj, uint64_t seed, uint64_t traj_offset,
+                double* X, double* X_traj, int nthreads) {
+    int nops = so_qrc_n_ops(L, 2);
+    double* per = X_traj ? X_traj : (double*)malloc((size_t)n_traj * T * nops * sizeof(double));
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > n_traj) nthreads = n_traj > 0 ? n_traj : 1;
+    qrc_job* jobs = (qrc_job*)calloc(nthreads, sizeof(qrc_job));
+    pthread_t* th = (pthread_t*)calloc(nthreads, sizeof(pthread_t));
+    for (int i = 0; i < nthreads; i++) {
+        qrc_job J = {L, ng, n_substeps, encoding, protocol, T, n_traj, nthreads, i, g, psi0, u, seed, traj_offset, per};
+        jobs[i] = J;
+    }
+    for (int i = 1; i < nthreads; i++) pthread_create(&th[i], NULL, qrc_worker, &jobs[i]);
+    qrc_worker(&jobs[0]);
+    for (int i = 1; i < nthreads; i++) pthread_join(th[i], NULL);
+    /* X_sum ./ n_traj (:587-590), summed in trajectory order */
+    for (int64_t x = 0; x < (int64_t)T * nops; x++) {
+        double s = 0;
+        for (int t = 0; t < n_traj; t++) s += per[(int64_t)t * T * nops + x];
+        X[x] = s / n_traj;
+    }
+    if (!X_traj) free(per);
+    free(jobs); free(th);
+}
+/* Tr(rho P) for the Pauli string with X on xmask and Z on zmask (Y where both):
+ * P|j> = i^ny (-1)^popc(j & zmask) |j ^ xmask>; rho column-major */
+double so_expect_pauli_rho(const C* rho, uint64_t xmask, uint64_t zmask, int N) {
+    int64_t dim = 1LL << N;
+    int ny = __builtin_popcountll(xmask & zmask) & 3;
+    C ph = ny == 0 ? 1 : ny == 1 ? I_ : ny == 2 ? -1 : -I_;
+    C s = 0;
+    for (int64_t j = 0; j < dim; j++) {
+        C v = rho[j + (int64_t)(j ^ xmask) * dim];
+        s += (__builtin_popcountll((uint64_t)j & zmask) & 1) ? -v : v;
+    }
+    return creal(ph * s);
+}
+void so_qrc_dm_run(int L, const so_trotter_gate* g, int ng, int n_substeps, int encoding, int protocol,
+                   const C* psi0, const double* u, int T, double* X) {
+    int N = 2 * L, nops = so_qrc_n_ops(L, 2);
+    int64_t dim = 1LL << N, d = 1LL << L;
+    C* rho = (C*)malloc(dim * dim * sizeof(C));
+    C* red = (C*)malloc(d * d * sizeof(C));
+    C* pin = (C*)malloc(d * sizeof(C));
+    double* win = (double*)malloc(L * sizeof(double));
+    for (int64_t c = 0; c < dim; c++)
+        for (int64_t r = 0; r < dim; r++) rho[r + c * dim] = psi0[r] * conj(psi0[c]);
+    for (int k = 0; k < T; k++) {
+        so_qrc_window(u, L, k, encoding, win);
+        so_qrc_encode(win, L, pin);
+        /* reduced state of the kept rail (rail 1: reservoir = high bits; rail 2: input = low bits) */
+        for (int64_t a = 0; a < d; a++)
+            for (int64_t b = 0; b < d; b++) {
+                C s = 0;
+                for (int64_t x = 0; x < d; x++)
+                    s += protocol == 1 ? rho[(x + d * a) + (x + d * b) * dim] : rho[(a + d * x) + (b + d * x) * dim];
+                red[a + b * d] = s;
+            }
+        /* rho_in (x) rho_res: rho_in on the low bits, the kept state on the high bits */
+        for (int64_t i = 0; i < d; i++)
+            for (int64_t j = 0; j < d; j++)
+                for (int64_t i2 = 0; i2 < d; i2++)
+                    for (int64_t j2 = 0; j2 < d; j2++)
+                        rho[(i + d * j) + (i2 + d * j2) * dim] = pin[i] * conj(pin[i2]) * red[j + j2 * d];
+        for (int s = 0; s < n_substeps; s++) so_trotter_step_rho(rho, g, ng, N);
+        double* o = X + (int64_t)k * nops;
+        int idx = 0;
+        for (int q = 0; q < N; q++) {
+            uint64_t m = 1ULL << q;
+            o[idx++] = so_expect_pauli_rho(rho, m, 0, N);
+            o[idx++] = so_expect_pauli_rho(rho, m, m, N);
+            o[idx++] = so_expect_pauli_rho(rho, 0, m, N);
+        }
+        for (int pass = 0; pass < 2; pass++)
+            for (int rail = 0; rail < 2; rail++)
+                for (int site = 0; site < L; site++) {
+                    int i, j;
+                    if (pass == 0) { if (site == L - 1) continue; i = rail * L + site; j = i + 1; }
+                    else { if (rail == 1) continue; i = site; j = L + site; }
+                    uint64_t m = (1ULL << i) | (1ULL << j);
+                    o[idx++] = so_expect_pauli_rho(rho, m, 0, N);
+                    o[idx++] = so_expect_pauli_rho(rho, m, m, N);
+                    o[idx++] = so_expect_pauli_rho(rho, 0, m, N);
+                }
+    }
+    free(rho); free(red); free(pin); free(win);
+}

@@ -169,6 +169,31 @@ void so_sample(const so_cplx* psi, int N, int64_t nshots, uint64_t seed, uint64_
 int64_t so_measure_all(so_cplx* psi, int N, uint64_t seed, uint64_t stream);                             /* :484 */
 int so_measure_qubit(so_cplx* psi, int k, int N, uint64_t seed, uint64_t stream);                         /* :224 */
 
+/* ---- quantum reservoir computing, bitwise MCWF path ----
+ * utils/cpu/cpuQRCSimulationMonteCarloWaveFunction.jl:451 (_run_traj_loop_bitwise!),
+ * :531 (run_mcwf_simulation, bitwise), utils/cpu/cpuQRCstep.jl:96
+ * (encode_input_ry_psi!), :332 (qrc_reset_psi!).  Two rails of L qubits (N = 2L,
+ * the reset reshapes the state as 2^L x 2^L).  encoding: 0 :batch, 1 :broadcast;
+ * protocol: 1 :traceout_rail_1, 2 :traceout_rail_2.  The reset's rand() is the
+ * Philox draw u(seed, counter (step, trajectory)).  u is padded_u (T + L values,
+ * [zeros(L); inputs] as run_mcwf_simulation builds it).  X[k * n_ops + o] =
+ * trajectory mean of feature o after input k; X_traj (or NULL) per trajectory. */
+int so_qrc_n_ops(int L, int n_rails);
+void so_measure_all_observables(const so_cplx* psi, int L, int n_rails, double* out); /* :1483 */
+void so_qrc_window(const double* padded_u, int L, int k, int encoding, double* win);
+void so_qrc_encode(const double* win, int L, so_cplx* psi_in);
+int so_qrc_reset(so_cplx* out, const so_cplx* psi, const so_cplx* psi_in, int L, int protocol, double r);
+void so_qrc_run(int L, const so_trotter_gate* g, int ng, int n_substeps, int encoding, int protocol,
+                const so_cplx* psi0, const double* u, int T, int n_traj, uint64_t seed, uint64_t traj_offset,
+                double* X, double* X_traj, int nthreads);
+/* the density-matrix pipeline the trajectory mean converges to: run_dm_simulation
+ * (utils/cpu/cpuQRCSimulationDensityMatrix.jl:114, loop :186-244): the same window
+ * and encoding, qrc_reset_rho (cpuQRCstep.jl:457: partial trace, then
+ * rho_in (x) rho_res), U on columns and conj(U) on rows per Trotter step */
+void so_qrc_dm_run(int L, const so_trotter_gate* g, int ng, int n_substeps, int encoding, int protocol,
+                   const so_cplx* psi0, const double* u, int T, double* X);
+double so_expect_pauli_rho(const so_cplx* rho, uint64_t xmask, uint64_t zmask, int N);
+
 #ifdef __cplusplus
 }
 #endif

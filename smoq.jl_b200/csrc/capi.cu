@@ -217,6 +217,7 @@ smoq_status smoq_ctx_create(int device, smoq_ctx** out) {
     if (regtile_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (stage_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (vqe_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
+    if (qrc_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (ensure_scratch(ctx.get(), 1 << 17) != SMOQ_OK) return SMOQ_ERR_OOM;
     if (ensure_pinned(ctx.get(), 1 << 20) != SMOQ_OK) return SMOQ_ERR_OOM;
     *out = ctx.release();
@@ -1151,4 +1152,12 @@ smoq_status smoq_internal_ops_to_ir(int N, const smoq_op* ops, int n, const doub
     return ops_to_ir(nullptr, N, ops, n, theta, out);
 }
 int smoq_internal_tile_bits(smoq_ctx* ctx, int dtype) { return tile_bits(ctx, dtype); }
+smoq_status smoq_internal_plan_step(smoq_plan* P, smoq_ctx** ctx, int* N, int* dtype, const std::vector<GateIR>** step) {
+    if (!P || !P->ctx) return SMOQ_ERR_BADINPUT;
+    *ctx = P->ctx;
+    *N = P->N;
+    *dtype = P->dtype;
+    *step = &P->step;
+    return SMOQ_OK;
+}
 int smoq_internal_low_bits(smoq_ctx* ctx, int dtype) { return low_bits(ctx, dtype); }

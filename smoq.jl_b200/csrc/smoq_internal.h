@@ -228,4 +228,5 @@ cudaError_t stage_kernels_init(smoq_ctx* ctx);
 cudaError_t launch_stage(smoq_ctx* ctx, const TileArgs& a, int dtype, bool epi);
 cudaError_t launch_jit(smoq_ctx* ctx, const TileArgs& a, const JitKernel* k, bool epi);
 cudaError_t vqe_kernels_init(smoq_ctx* ctx);
+cudaError_t qrc_kernels_init(smoq_ctx* ctx);
 }  // namespace smoq

@@ -34,7 +34,7 @@ __all__ = [
     "precompute_trotter_gates_bitwise", "TrotterPlan", "apply_fast_trotter_step", "evolve_trotter_psi",
     "CircuitOperation", "gate", "ParameterizedCircuit", "single_qubit_rotation_layer", "entangling_layer",
     "repeat_layer", "apply_circuit", "JumpOperator", "create_jump_operator", "mcwf_run", "PauliSum",
-    "energy", "energy_and_gradient", "debug_plan",
+    "energy", "energy_and_gradient", "debug_plan", "run_mcwf_simulation", "qrc_n_ops",
 ]
 
 
@@ -801,3 +801,54 @@ def dm_expect_zstrings(rho: CuState, N: int, zmasks: Sequence[int]) -> np.ndarra
     ck(lib.smoq_dm_expect_zstrings(rho.h, N, m.ctypes.data_as(C.POINTER(C.c_uint64)), len(m), dptr(out)),
        rho.ctx.h, "dm_expect_zstrings")
     return out
+
+
+# ----------------------------------------------------------------- quantum reservoir computing
+_QRC_ENCODING = {"batch": 0, "batch_causal": 0, "broadcast": 1}
+_QRC_RESET = {"traceout_rail_1": 1, "protocol1": 1, "traceout_rail_2": 2, "protocol2": 2}
+
+
+def qrc_n_ops(L: int, n_rails: int = 2) -> int:
+    """features per input: 3N + 3 (L-1) n_rails + 3 L (n_rails-1)"""
+    return 3 * L * n_rails + 3 * (L - 1) * n_rails + 3 * L * (n_rails - 1)
+
+
+def run_mcwf_simulation(psi0, H_params, gates, padded_u, L: int, n_rails: int, T: int, n_traj: int,
+                        integrator_type: str = "trotter_cpu", T_evol: float = 0.0, encoding: str = "batch",
+                        reset_type: str = "traceout_rail_1", n_substeps: int = 5, *, ctx: "Context" = None,
+                        dtype: int = C128, seed: int = 1234, traj_offset: int = 0, per_trajectory: bool = False):
+    """The bitwise run_mcwf_simulation (cpuQRCSimulationMonteCarloWaveFunction.jl:531) on the GPU:
+    n_traj trajectories of the QRC loop (_run_traj_loop_bitwise! :451), each
+    trajectory's state in one CTA's shared memory for the whole series.  Returns
+    X[T, n_ops], the trajectory mean of the ladder features after every input
+    (and X_traj[n_traj, T, n_ops] with per_trajectory=True).
+
+    psi0: 2^N amplitudes or None (|0...0>); H_params: kept for the reference's
+    signature (the evolution is `gates`); gates: a TrotterPlan on N = 2L qubits or
+    a FastTrotterGate list (one Trotter step); padded_u: [zeros(L); inputs]
+    (T + L values).  Only the :trotter_cpu integrator runs here.  The reset's
+    rand() is the Philox draw (shot = input index, stream = trajectory id)."""
+    if integrator_type != "trotter_cpu":
+        raise ValueError(f"Unsupported integrator: {integrator_type}. Supported here: :trotter_cpu")
+    if n_rails != 2:
+        raise ValueError("the QRC reset reshapes the state as 2^L x 2^L: n_rails must be 2")
+    if ctx is None:
+        ctx = gates.ctx if isinstance(gates, TrotterPlan) else None
+    if ctx is None:
+        raise ValueError("a Context is needed (pass ctx=, or a TrotterPlan)")
+    N = L * n_rails
+    plan = gates if isinstance(gates, TrotterPlan) else TrotterPlan(ctx, N, gates, 1, dtype)
+    u = np.ascontiguousarray(padded_u, dtype=np.float64)
+    if u.size < T + L:
+        raise ValueError("padded_u must hold T + L values")
+    p = _lib.SmoqQrcParams(L, n_substeps, _QRC_ENCODING[encoding], _QRC_RESET[reset_type], seed, traj_offset)
+    nops = qrc_n_ops(L, n_rails)
+    X = np.empty(T * nops)
+    Xt = np.empty(n_traj * T * nops) if per_trajectory else None
+    p0 = None
+    if psi0 is not None:
+        p0 = np.ascontiguousarray(np.asarray(psi0, dtype=np.complex128).view(np.float64))
+    ck(lib.smoq_qrc_run(plan.h, C.byref(p), dptr(p0) if p0 is not None else None, dptr(u), T, n_traj, dptr(X),
+                        dptr(Xt) if per_trajectory else None), ctx.h, "qrc_run")
+    X = X.reshape(T, nops)
+    return (X, Xt.reshape(n_traj, T, nops)) if per_trajectory else X

@@ -45,6 +45,11 @@ class SmoqVqeJob(C.Structure):
                 ("energy", C.POINTER(C.c_double)), ("grad", C.POINTER(C.c_double))]
 
 
+class SmoqQrcParams(C.Structure):
+    _fields_ = [("L", C.c_int32), ("n_substeps", C.c_int32), ("encoding", C.c_int32), ("reset", C.c_int32),
+                ("seed", C.c_uint64), ("traj_offset", C.c_uint64)]
+
+
 class SmoqPassInfo(C.Structure):
     _fields_ = [("T", C.c_int32), ("L", C.c_int32), ("H", C.c_int32), ("nops", C.c_int32), ("hb", C.c_int32 * 24)]
 
@@ -145,6 +150,7 @@ _SIGS = {
     "smoq_measure_all": [_vp, C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_longlong)],
     "smoq_measure_qubit": [_vp, C.c_int, C.c_ulonglong, C.c_ulonglong, C.POINTER(C.c_int)],
     "smoq_energy_grad_jobs": [_vp, C.c_int, C.POINTER(SmoqVqeJob), C.c_int],
+    "smoq_qrc_run": [_vp, C.POINTER(SmoqQrcParams), _dp, _dp, C.c_int, C.c_int64, _dp, _dp],
     "smoq_debug_compile_plan": [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, _dp, C.c_int, _ip,
                                 C.c_char_p, C.c_int],
     "smoq_debug_plan_sequence": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, _dp,
