@@ -16,7 +16,7 @@ export CuContext, CuState, apply_rx_psi!, apply_ry_psi!, apply_rz_psi!, apply_ha
        expect_local, expect_corr, get_expectation_pauli_string, get_norm, normalize_state!,
        TrotterPlan, evolve_trotter_psi!, apply_fast_trotter_step_cpu!, energy_and_gradient,
        energy_and_gradient_jobs, lindblad_mcwf_batched!, apply_hamiltonian_bitwise!, sample_bitstrings,
-       projective_measurement_all!, measure_z_single!, set_engine!
+       projective_measurement_all!, measure_z_single!, set_engine!, run_mcwf_simulation
 
 const lib = joinpath(@__DIR__, "..", "lib", "libsmoq_cuda.so")
 const SMOQ_C64 = Cint(0)
@@ -269,6 +269,34 @@ function measure_z_single!(ψ::CuState, k::Int, N::Int; seed::UInt64=UInt64(42),
     check(ccall((:smoq_measure_qubit, lib), Cint, (Ptr{Cvoid}, Cint, Culonglong, Culonglong, Ptr{Cint}),
                 ψ.h, k - 1, seed, stream, o), ψ.ctx)
     ψ.batch == 1 ? Int(o[1]) : Int.(o)
+end
+
+struct CQrcParams
+    L::Int32; n_substeps::Int32; encoding::Int32; reset::Int32
+    seed::UInt64; traj_offset::UInt64
+end
+
+"""run_mcwf_simulation(psi0, H_params, gates, padded_u, L, n_rails, T, n_traj, :trotter_cpu,
+T_evol, encoding, reset_type, n_substeps) -- the bitwise QRC loop
+(cpuQRCSimulationMonteCarloWaveFunction.jl:531) on the GPU; `gates` is a TrotterPlan on
+N = 2L qubits.  Returns X (T x n_ops), the trajectory mean of the ladder features."""
+function run_mcwf_simulation(psi0, H_params, gates::TrotterPlan, padded_u::Vector{Float64}, L::Int,
+                             n_rails::Int, T::Int, n_traj::Int, integrator_type::Symbol, T_evol::Float64,
+                             encoding::Symbol, reset_type::Symbol, n_substeps::Int=5;
+                             seed::UInt64=UInt64(1234), traj_offset::UInt64=UInt64(0))
+    integrator_type == :trotter_cpu || error("Unsupported integrator: $integrator_type. Supported: :trotter_cpu")
+    n_rails == 2 || error("the QRC reset reshapes the state as 2^L x 2^L: n_rails must be 2")
+    enc = encoding == :broadcast ? 1 : 0
+    rst = reset_type in (:traceout_rail_1, :protocol1) ? 1 : reset_type in (:traceout_rail_2, :protocol2) ? 2 :
+          error("Unknown protocol: $reset_type. Use :traceout_rail_1 or :traceout_rail_2")
+    p = Ref(CQrcParams(L, n_substeps, enc, rst, seed, traj_offset))
+    n_ops = 3 * 2L + 3 * (L - 1) * 2 + 3 * L
+    X = Vector{Float64}(undef, T * n_ops)
+    p0 = psi0 === nothing ? C_NULL : reinterpret(Float64, Vector{ComplexF64}(psi0))
+    check(ccall((:smoq_qrc_run, lib), Cint,
+                (Ptr{Cvoid}, Ref{CQrcParams}, Ptr{Float64}, Ptr{Float64}, Cint, Int64, Ptr{Float64}, Ptr{Float64}),
+                gates.h, p, p0, padded_u, T, n_traj, X, C_NULL), gates.ctx)
+    permutedims(reshape(X, n_ops, T))   # X[k, f], as the reference's Matrix (T x n_ops)
 end
 
 "fused-pass engine: -1 auto (default), 0 shared-memory sweeps, 1 register tiles, 2 stage
