@@ -19,6 +19,9 @@
 // complex128), one CTA per trajectory, persistent over trajectories; HBM
 // sees only the initial state and the feature sums.  The Trotter steps are
 // the planner's fused op program for a tile that spans the whole state.
+// With the context's engine option at 3 the states stream through HBM
+// instead: per input, the plan's compiled passes (a CUDA graph), then one
+// kernel for the features of that input and the reset for the next.
 //
 // Randomness: r = 53-bit uniform of Philox4x32-10, key = seed, counter =
 // (step, trajectory id) -- the draw of smoq_sample for shot = step, stream =
@@ -37,9 +40,10 @@
 
 namespace smoq {
 
-// one observable group: q2 < 0 -> (X, Y, Z) of q1 at out..out+2; else (XX, YY, ZZ)
+// one group sweep over the amplitude quadruples of qubits (a, b): (XX, YY, ZZ) at
+// out, and, where out_a / out_b >= 0, (X, Y, Z) of a / b there
 struct QrcObs {
-    int32_t q1, q2, out, pad;
+    int32_t a, b, out, out_a, out_b, pad;
 };
 
 struct QrcArgs {
@@ -56,6 +60,20 @@ struct QrcArgs {
 };
 
 constexpr int kQrcThreads = 256;
+// CTAs per SM the register budget is sized for (shared memory allows up to 6 at L = 6 complex64)
+#ifndef SMOQ_QRC_MINB_C64
+#define SMOQ_QRC_MINB_C64 4
+#endif
+#ifndef SMOQ_QRC_MINB_C128
+#define SMOQ_QRC_MINB_C128 2
+#endif
+
+// warp sum of x added into this warp's feature row
+__device__ __forceinline__ void qrc_flush(double x, double* row, int f, int lane) {
+#pragma unroll
+    for (int dd = 16; dd > 0; dd >>= 1) x += __shfl_xor_sync(0xffffffffu, x, dd);
+    if (lane == 0) row[f] = x;
+}
 
 // the 53-bit uniform of counter (shot, stream) under key seed (Philox4x32-10)
 __device__ __forceinline__ double qrc_uniform(uint64_t seed, uint64_t shot, uint64_t stream) {
@@ -98,151 +116,218 @@ __device__ __forceinline__ void qrc_apply(const DevOp& op, typename CT<R>::T* ps
     }
 }
 
+// shared-memory scratch of a trajectory CTA, after the 2^N-amplitude state
 template <typename R>
-__global__ void __launch_bounds__(kQrcThreads) qrc_traj_kernel(const QrcArgs A) {
+struct QrcScratch {
+    typename CT<R>::T* phi;  // the kept rail's normalised state (2^L)
+    double* pin;             // encoded input amplitudes (real, 2^L)
+    double* prob;            // outcome probabilities (2^L)
+    double* part;            // one partial per thread
+    double* red;             // [warps][n_ops] feature rows
+};
+template <typename R>
+__device__ __forceinline__ QrcScratch<R> qrc_scratch(unsigned char* sm, uint32_t dim, uint32_t d) {
+    using C = typename CT<R>::T;
+    QrcScratch<R> S;
+    S.phi = reinterpret_cast<C*>(sm) + dim;
+    S.pin = reinterpret_cast<double*>(S.phi + d);
+    S.prob = S.pin + d;
+    S.part = S.prob + d;
+    S.red = S.part + kQrcThreads;
+    return S;
+}
+
+// A + B for input k: encode the window, measure the rail of psi (shared memory)
+// with the draw of (k, traj), write |psi_in> (x) |phi> to out (shared or global;
+// out may alias psi: every read of psi ends before the first write)
+template <typename R>
+__device__ __forceinline__ void qrc_reset(const QrcArgs& A, int k, uint64_t traj, const typename CT<R>::T* psi,
+                                          typename CT<R>::T* out, const QrcScratch<R>& S) {
+    using C = typename CT<R>::T;
+    __shared__ int s_out;
+    __shared__ double s_inv;
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const uint32_t dim = 1u << A.N, d = 1u << A.L;
+    // the encoded input, prod_q (bit q ? sin : cos)
+    const double* e = A.enc + (size_t)k * A.L * 2;
+    for (uint32_t i = tid; i < d; i += nthr) {
+        double v = 1.0;
+        for (int q = 0; q < A.L; ++q) v *= ((i >> q) & 1) ? e[2 * q + 1] : e[2 * q];
+        S.pin[i] = v;
+    }
+    // probabilities of the measured rail: x = the measured index, y = the kept one
+    {
+        const uint32_t x = tid & (d - 1), np = nthr / d;
+        double s = 0;
+        for (uint32_t y = tid / d; y < d; y += np) {
+            const C v = psi[A.protocol == 1 ? x + d * y : y + d * x];
+            s += (double)v.x * v.x + (double)v.y * v.y;
+        }
+        S.part[tid] = s;
+    }
+    __syncthreads();
+    for (uint32_t x = tid; x < d; x += nthr) {
+        double s = 0;
+        for (uint32_t p = 0; p < nthr / d; ++p) s += S.part[x + d * p];
+        S.prob[x] = s;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double total = 0;
+        for (uint32_t x = 0; x < d; ++x) total += S.prob[x];
+        const double r = qrc_uniform(A.seed, (uint64_t)k, traj);
+        int outcome = 0;  // (no crossing: the first outcome, as the reference)
+        double cum = 0;
+        for (uint32_t x = 0; x < d; ++x) {
+            cum += S.prob[x] / total;
+            if (r <= cum) {
+                outcome = (int)x;
+                break;
+            }
+        }
+        const double nrm = sqrt(S.prob[outcome]);
+        s_out = outcome;
+        s_inv = nrm > 1e-12 ? 1.0 / nrm : 0.0;  // 0: the reset falls back to |0>
+    }
+    __syncthreads();
+    const uint32_t o = (uint32_t)s_out;
+    const double inv = s_inv;
+    for (uint32_t y = tid; y < d; y += nthr) {
+        C v;
+        if (inv > 0) {
+            const C w = psi[A.protocol == 1 ? o + d * y : y + d * o];
+            v.x = (R)((double)w.x * inv);
+            v.y = (R)((double)w.y * inv);
+        } else {
+            v.x = (R)(y == 0 ? 1 : 0);
+            v.y = (R)0;
+        }
+        S.phi[y] = v;
+    }
+    __syncthreads();
+    for (uint32_t a = tid; a < dim; a += nthr) {
+        const C v = S.phi[a >> A.L];
+        const R w = (R)S.pin[a & (d - 1)];
+        C z;
+        z.x = w * v.x;
+        z.y = w * v.y;
+        out[a] = z;
+    }
+}
+
+// D: the features of input k of trajectory t (chunk-relative index tc for X_traj
+// is t itself) from psi in shared memory: one sweep per bond or rung, per-warp
+// rows, then one atomic add per feature into the trajectory sums
+template <typename R>
+__device__ __forceinline__ void qrc_features(const QrcArgs& A, int k, int64_t t, const typename CT<R>::T* psi,
+                                             const QrcScratch<R>& S) {
+    using C = typename CT<R>::T;
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
+    const uint32_t dim = 1u << A.N;
+    for (int g = 0; g < A.nobs; ++g) {
+        const QrcObs ob = A.obs[g];
+        const int a = ob.a, b = ob.b, lo = a < b ? a : b, hi = a < b ? b : a;
+        R xx = 0, yy = 0, zz = 0, xa = 0, ya = 0, za = 0, xb = 0, yb = 0, zb = 0;
+        for (uint32_t h = tid; h < dim / 4; h += nthr) {
+            const uint32_t i00 = ins0<uint32_t>(ins0<uint32_t>(h, lo), hi);
+            const uint32_t i10 = i00 | (1u << a), i01 = i00 | (1u << b), i11 = i10 | (1u << b);
+            const C v00 = psi[i00], v10 = psi[i10], v01 = psi[i01], v11 = psi[i11];
+            const R n00 = v00.x * v00.x + v00.y * v00.y, n10 = v10.x * v10.x + v10.y * v10.y;
+            const R n01 = v01.x * v01.x + v01.y * v01.y, n11 = v11.x * v11.x + v11.y * v11.y;
+            const R c0 = v00.x * v11.x + v00.y * v11.y;  // Re conj(v00) v11
+            const R c1 = v10.x * v01.x + v10.y * v01.y;  // Re conj(v10) v01
+            xx += c0 + c1;
+            yy += c1 - c0;
+            zz += (n00 + n11) - (n10 + n01);
+            // conj(v00) v10 + conj(v01) v11: the pairs of qubit a
+            xa += (v00.x * v10.x + v00.y * v10.y) + (v01.x * v11.x + v01.y * v11.y);
+            ya += (v00.x * v10.y - v00.y * v10.x) + (v01.x * v11.y - v01.y * v11.x);
+            za += (n00 + n01) - (n10 + n11);
+            // conj(v00) v01 + conj(v10) v11: the pairs of qubit b
+            xb += (v00.x * v01.x + v00.y * v01.y) + (v10.x * v11.x + v10.y * v11.y);
+            yb += (v00.x * v01.y - v00.y * v01.x) + (v10.x * v11.y - v10.y * v11.x);
+            zb += (n00 + n10) - (n01 + n11);
+        }
+        double* row = S.red + (size_t)warp * A.n_ops;
+        qrc_flush(2.0 * (double)xx, row, ob.out, lane);
+        qrc_flush(2.0 * (double)yy, row, ob.out + 1, lane);
+        qrc_flush((double)zz, row, ob.out + 2, lane);
+        if (ob.out_a >= 0) {
+            qrc_flush(2.0 * (double)xa, row, ob.out_a, lane);
+            qrc_flush(2.0 * (double)ya, row, ob.out_a + 1, lane);
+            qrc_flush((double)za, row, ob.out_a + 2, lane);
+        }
+        if (ob.out_b >= 0) {
+            qrc_flush(2.0 * (double)xb, row, ob.out_b, lane);
+            qrc_flush(2.0 * (double)yb, row, ob.out_b + 1, lane);
+            qrc_flush((double)zb, row, ob.out_b + 2, lane);
+        }
+    }
+    __syncthreads();
+    for (int f = tid; f < A.n_ops; f += nthr) {
+        double s = 0;
+        for (int w = 0; w < nwarps; ++w) s += S.red[(size_t)w * A.n_ops + f];
+        atomicAdd(&A.X[(size_t)k * A.n_ops + f], s);
+        if (A.X_traj) A.X_traj[((size_t)t * A.T + k) * A.n_ops + f] = s;
+    }
+}
+
+// The resident kernel: each trajectory's state stays in shared memory for the
+// whole series; the evolution runs as shared-memory sweeps of the fused ops.
+template <typename R>
+__global__ void __launch_bounds__(kQrcThreads, sizeof(R) == 4 ? SMOQ_QRC_MINB_C64 : SMOQ_QRC_MINB_C128)
+    qrc_traj_kernel(const QrcArgs A) {
     using C = typename CT<R>::T;
     extern __shared__ __align__(16) unsigned char sm[];
     const uint32_t dim = 1u << A.N, d = 1u << A.L;
     C* psi = reinterpret_cast<C*>(sm);
-    C* phi = psi + dim;
-    double* pin = reinterpret_cast<double*>(phi + d);  // encoded input amplitudes (real)
-    double* prob = pin + d;                            // outcome probabilities
-    double* part = prob + d;                           // one partial per thread
-    double* red = part + kQrcThreads;                  // [warps][n_ops]
+    const QrcScratch<R> S = qrc_scratch<R>(sm, dim, d);
     __shared__ C dco[16];
-    __shared__ int s_out;
-    __shared__ double s_inv;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nwarps = blockDim.x >> 5;
+    const int tid = threadIdx.x;
     const C* p0 = reinterpret_cast<const C*>(A.psi0);
     for (int64_t t = blockIdx.x; t < A.n_traj; t += gridDim.x) {
         for (uint32_t a = tid; a < dim; a += blockDim.x) psi[a] = p0[a];
+        __syncthreads();
         const uint64_t traj = A.traj_offset + (uint64_t)t;
         for (int k = 0; k < A.T; ++k) {
-            // A. the encoded input, prod_q (bit q ? sin : cos)
-            const double* e = A.enc + (size_t)k * A.L * 2;
-            for (uint32_t i = tid; i < d; i += blockDim.x) {
-                double v = 1.0;
-                for (int q = 0; q < A.L; ++q) v *= ((i >> q) & 1) ? e[2 * q + 1] : e[2 * q];
-                pin[i] = v;
-            }
+            qrc_reset<R>(A, k, traj, psi, psi, S);
             __syncthreads();
-            // B. probabilities of the measured rail: x = the measured index, y = the kept one
-            {
-                const uint32_t x = (uint32_t)tid & (d - 1), np = (uint32_t)blockDim.x / d;
-                double s = 0;
-                for (uint32_t y = (uint32_t)tid / d; y < d; y += np) {
-                    const C v = psi[A.protocol == 1 ? x + d * y : y + d * x];
-                    s += (double)v.x * v.x + (double)v.y * v.y;
-                }
-                part[tid] = s;
-            }
-            __syncthreads();
-            for (uint32_t x = tid; x < d; x += blockDim.x) {
-                double s = 0;
-                for (uint32_t p = 0; p < (uint32_t)blockDim.x / d; ++p) s += part[x + d * p];
-                prob[x] = s;
-            }
-            __syncthreads();
-            if (tid == 0) {
-                double total = 0;
-                for (uint32_t x = 0; x < d; ++x) total += prob[x];
-                const double r = qrc_uniform(A.seed, (uint64_t)k, traj);
-                int outcome = 0;  // (no crossing: the first outcome, as the reference)
-                double cum = 0;
-                for (uint32_t x = 0; x < d; ++x) {
-                    cum += prob[x] / total;
-                    if (r <= cum) {
-                        outcome = (int)x;
-                        break;
-                    }
-                }
-                const double nrm = sqrt(prob[outcome]);
-                s_out = outcome;
-                s_inv = nrm > 1e-12 ? 1.0 / nrm : 0.0;  // 0: the reset falls back to |0>
-            }
-            __syncthreads();
-            const uint32_t o = (uint32_t)s_out;
-            const double inv = s_inv;
-            for (uint32_t y = tid; y < d; y += blockDim.x) {
-                C v;
-                if (inv > 0) {
-                    const C w = psi[A.protocol == 1 ? o + d * y : y + d * o];
-                    v.x = (R)((double)w.x * inv);
-                    v.y = (R)((double)w.y * inv);
-                } else {
-                    v.x = (R)(y == 0 ? 1 : 0);
-                    v.y = (R)0;
-                }
-                phi[y] = v;
-            }
-            __syncthreads();
-            for (uint32_t a = tid; a < dim; a += blockDim.x) {
-                const C v = phi[a >> A.L];
-                const R w = (R)pin[a & (d - 1)];
-                C z;
-                z.x = w * v.x;
-                z.y = w * v.y;
-                psi[a] = z;
-            }
-            __syncthreads();
-            // C. n_substeps Trotter steps
-            for (int q = 0; q < A.nops; ++q) {
+            for (int q = 0; q < A.nops; ++q) {  // n_substeps Trotter steps
                 qrc_apply<R>(A.ops[q], psi, A.N, dco);
                 __syncthreads();
             }
-            // D. observables: each warp sums its share of every group into its row
-            for (int g = 0; g < A.nobs; ++g) {
-                const QrcObs ob = A.obs[g];
-                R s0 = 0, s1 = 0, s2 = 0;
-                if (ob.q2 < 0) {
-                    const int b = ob.q1;
-                    for (uint32_t h = tid; h < dim / 2; h += blockDim.x) {
-                        const uint32_t i0 = ins0<uint32_t>(h, b), i1 = i0 | (1u << b);
-                        const C u = psi[i0], v = psi[i1];
-                        s0 += u.x * v.x + u.y * v.y;                    // Re conj(u) v
-                        s1 += u.x * v.y - u.y * v.x;                    // Im conj(u) v
-                        s2 += (u.x * u.x + u.y * u.y) - (v.x * v.x + v.y * v.y);
-                    }
-                    s0 *= 2;
-                    s1 *= 2;
-                } else {
-                    const int a = ob.q1, b = ob.q2, lo = a < b ? a : b, hi = a < b ? b : a;
-                    for (uint32_t h = tid; h < dim / 4; h += blockDim.x) {
-                        const uint32_t i00 = ins0<uint32_t>(ins0<uint32_t>(h, lo), hi);
-                        const uint32_t i10 = i00 | (1u << a), i01 = i00 | (1u << b), i11 = i10 | (1u << b);
-                        const C v00 = psi[i00], v10 = psi[i10], v01 = psi[i01], v11 = psi[i11];
-                        const R c0 = v00.x * v11.x + v00.y * v11.y;     // Re conj(v00) v11
-                        const R c1 = v10.x * v01.x + v10.y * v01.y;     // Re conj(v10) v01
-                        s0 += c0 + c1;
-                        s1 += c1 - c0;
-                        s2 += (v00.x * v00.x + v00.y * v00.y) + (v11.x * v11.x + v11.y * v11.y) -
-                              (v10.x * v10.x + v10.y * v10.y) - (v01.x * v01.x + v01.y * v01.y);
-                    }
-                    s0 *= 2;
-                    s1 *= 2;
-                }
-                double w0 = s0, w1 = s1, w2 = s2;
-#pragma unroll
-                for (int dd = 16; dd > 0; dd >>= 1) {
-                    w0 += __shfl_xor_sync(0xffffffffu, w0, dd);
-                    w1 += __shfl_xor_sync(0xffffffffu, w1, dd);
-                    w2 += __shfl_xor_sync(0xffffffffu, w2, dd);
-                }
-                if (lane == 0) {
-                    double* row = red + (size_t)warp * A.n_ops + ob.out;
-                    row[0] = w0;
-                    row[1] = w1;
-                    row[2] = w2;
-                }
-            }
+            qrc_features<R>(A, k, t, psi, S);
             __syncthreads();
-            for (int f = tid; f < A.n_ops; f += blockDim.x) {
-                double s = 0;
-                for (int w = 0; w < nwarps; ++w) s += red[(size_t)w * A.n_ops + f];
-                atomicAdd(&A.X[(size_t)k * A.n_ops + f], s);
-                if (A.X_traj) A.X_traj[((size_t)t * A.T + k) * A.n_ops + f] = s;
-            }
+        }
+    }
+}
+
+// The streaming kernel, between the compiled evolution passes: for trajectories
+// t0 .. t0 + nchunk - 1 (state c at dst + c 2^N), the features of input k_obs
+// (k_obs >= 0) and the reset for input k_obs + 1 (< T).  src: the states to read
+// (src_stride 0: every trajectory starts from the same state).
+template <typename R>
+__global__ void __launch_bounds__(kQrcThreads, sizeof(R) == 4 ? SMOQ_QRC_MINB_C64 : SMOQ_QRC_MINB_C128)
+    qrc_obs_reset_kernel(const QrcArgs A, const void* src, int64_t src_stride, void* dst, int k_obs, int64_t t0,
+                         int64_t nchunk) {
+    using C = typename CT<R>::T;
+    extern __shared__ __align__(16) unsigned char sm[];
+    const uint32_t dim = 1u << A.N, d = 1u << A.L;
+    C* psi = reinterpret_cast<C*>(sm);
+    const QrcScratch<R> S = qrc_scratch<R>(sm, dim, d);
+    const int tid = threadIdx.x;
+    for (int64_t c = blockIdx.x; c < nchunk; c += gridDim.x) {
+        const C* in = reinterpret_cast<const C*>(src) + c * src_stride;
+        for (uint32_t a = tid; a < dim; a += blockDim.x) psi[a] = in[a];
+        __syncthreads();
+        if (k_obs >= 0) {
+            qrc_features<R>(A, k_obs, t0 + c, psi, S);
+            __syncthreads();
+        }
+        if (k_obs + 1 < A.T) {
+            qrc_reset<R>(A, k_obs + 1, A.traj_offset + (uint64_t)(t0 + c), psi,
+                         reinterpret_cast<C*>(dst) + c * (int64_t)dim, S);
             __syncthreads();
         }
     }
@@ -259,11 +344,12 @@ constexpr size_t kQrcMaxSmem = 200 * 1024;
 
 cudaError_t qrc_kernels_init(smoq_ctx* ctx) {
     (void)ctx;
-    cudaError_t e = cudaFuncSetAttribute(qrc_traj_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kQrcMaxSmem);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(qrc_traj_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kQrcMaxSmem);
+    const void* fns[4] = {(const void*)qrc_traj_kernel<float>, (const void*)qrc_traj_kernel<double>,
+                          (const void*)qrc_obs_reset_kernel<float>, (const void*)qrc_obs_reset_kernel<double>};
+    for (const void* f : fns)
+        if (cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQrcMaxSmem))
+            return e;
+    return cudaSuccess;
 }
 
 }  // namespace smoq
@@ -302,9 +388,15 @@ extern "C" smoq_status smoq_qrc_run(smoq_plan* plan, const smoq_qrc_params* p, c
                                   "Unknown protocol: use :traceout_rail_1 or :traceout_rail_2");
     const int n_ops = 3 * N + 3 * (L - 1) * 2 + 3 * L;
 
+    // the evolution: shared-memory sweeps inside the resident kernel, or, when the
+    // context's engine option is 3, the plan's compiled passes between streaming
+    // kernels (the states in HBM).  Both are FP32/FP64-issue-bound at about the same
+    // rate on the ladder workloads (dense 4x4 ops after field fusion), so the
+    // resident kernel, with no HBM traffic, is the default.
+    const bool streaming = ctx->engine == 3 && p->n_substeps > 0;
     // C. one input's evolution: n_substeps Trotter steps, fused on a tile spanning the state
     std::vector<GateIR> ev;
-    for (int s = 0; s < p->n_substeps; ++s) ev.insert(ev.end(), step->begin(), step->end());
+    for (int s = 0; !streaming && s < p->n_substeps; ++s) ev.insert(ev.end(), step->begin(), step->end());
     std::vector<DevOp> ops;
     if (!ev.empty()) {
         std::vector<Pass> passes;
@@ -324,13 +416,15 @@ extern "C" smoq_status smoq_qrc_run(smoq_plan* plan, const smoq_qrc_params* p, c
                 ops.push_back(op);
             }
     }
-    // D. observable groups in the reference's order
+    // D. one group sweep per rail bond (also carrying X, Y, Z of its lower qubit) and per
+    // rung (the last rung carries the rails' last qubits); outputs in the reference's
+    // order: (X, Y, Z) of qubit q at 3q, then the bonds of rail 0, rail 1, then the rungs
     std::vector<QrcObs> obs;
-    int out = 0;
-    for (int q = 0; q < N; ++q, out += 3) obs.push_back({q, -1, out, 0});
+    int out = 3 * N;
     for (int r = 0; r < 2; ++r)
-        for (int s = 0; s + 1 < L; ++s, out += 3) obs.push_back({r * L + s, r * L + s + 1, out, 0});
-    for (int s = 0; s < L; ++s, out += 3) obs.push_back({s, L + s, out, 0});
+        for (int s = 0; s + 1 < L; ++s, out += 3) obs.push_back({r * L + s, r * L + s + 1, out, 3 * (r * L + s), -1, 0});
+    for (int s = 0; s < L; ++s, out += 3)
+        obs.push_back({s, L + s, out, s == L - 1 ? 3 * s : -1, s == L - 1 ? 3 * (L + s) : -1, 0});
     // A. the input windows (encode_input_ry_psi!: Ry(pi u) on qubit q -> cos, sin of pi u / 2)
     std::vector<double> enc((size_t)T * L * 2);
     for (int k = 0; k < T; ++k)
@@ -392,17 +486,61 @@ extern "C" smoq_status smoq_qrc_run(smoq_plan* plan, const smoq_qrc_params* p, c
     A.L = L;
     A.T = T;
     A.protocol = p->reset;
-    const void* fn = dtype == SMOQ_C64 ? (const void*)qrc_traj_kernel<float> : (const void*)qrc_traj_kernel<double>;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kQrcThreads, smem) != cudaSuccess || per_sm < 1) {
-        (void)cudaGetLastError();
-        per_sm = 1;
+    auto per_sm = [&](const void* fn) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, kQrcThreads, smem) != cudaSuccess || n < 1) {
+            (void)cudaGetLastError();
+            n = 1;
+        }
+        return (int64_t)n;
+    };
+    std::unique_ptr<void, std::function<void(void*)>> hold_states(nullptr, [ctx](void* q) {
+        if (q) cudaFreeAsync(q, ctx->stream);
+    });
+    if (!streaming) {
+        const void* fn = dtype == SMOQ_C64 ? (const void*)qrc_traj_kernel<float> : (const void*)qrc_traj_kernel<double>;
+        const int grid = (int)std::min<int64_t>(n_traj, (int64_t)ctx->num_sms * per_sm(fn));
+        if (dtype == SMOQ_C64) qrc_traj_kernel<float><<<grid, kQrcThreads, smem, ctx->stream>>>(A);
+        else qrc_traj_kernel<double><<<grid, kQrcThreads, smem, ctx->stream>>>(A);
+        ctx->launches++;
+        QCK(cudaGetLastError());
+    } else {
+        // trajectories in chunks of at most 4 GiB of states; per input: the plan's
+        // compiled passes (n_substeps steps, one CUDA graph), then one kernel for the
+        // features of this input and the reset for the next
+        const size_t sbytes = dim * amp;
+        const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(n_traj, (int64_t)(((size_t)4 << 30) / sbytes)));
+        void* states = nullptr;
+        QCK(cudaMallocAsync(&states, (size_t)chunk * sbytes, ctx->stream));
+        hold_states.reset(states);
+        smoq_state st;
+        st.ctx = ctx;
+        st.N = N;
+        st.dtype = dtype;
+        st.owned = false;
+        st.ptr = states;
+        const void* fn = dtype == SMOQ_C64 ? (const void*)qrc_obs_reset_kernel<float>
+                                           : (const void*)qrc_obs_reset_kernel<double>;
+        const int64_t slots = (int64_t)ctx->num_sms * per_sm(fn);
+        auto obs_reset = [&](const void* src, int64_t stride, int k_obs, int64_t t0, int64_t nb) {
+            const int grid = (int)std::min<int64_t>(nb, slots);
+            if (dtype == SMOQ_C64)
+                qrc_obs_reset_kernel<float><<<grid, kQrcThreads, smem, ctx->stream>>>(A, src, stride, states, k_obs, t0, nb);
+            else
+                qrc_obs_reset_kernel<double><<<grid, kQrcThreads, smem, ctx->stream>>>(A, src, stride, states, k_obs, t0, nb);
+            ctx->launches++;
+            return cudaGetLastError();
+        };
+        for (int64_t t0 = 0; t0 < n_traj; t0 += chunk) {
+            const int64_t nb = std::min<int64_t>(chunk, n_traj - t0);
+            st.batch = (int)nb;
+            QCK(obs_reset(A.psi0, 0, -1, t0, nb));
+            for (int k = 0; k < T; ++k) {
+                if (smoq_status s = smoq_trotter_step(plan, &st, p->n_substeps)) return s;
+                QCK(obs_reset(states, (int64_t)dim, k, t0, nb));
+            }
+        }
     }
-    const int grid = (int)std::min<int64_t>(n_traj, (int64_t)ctx->num_sms * per_sm);
-    if (dtype == SMOQ_C64) qrc_traj_kernel<float><<<grid, kQrcThreads, smem, ctx->stream>>>(A);
-    else qrc_traj_kernel<double><<<grid, kQrcThreads, smem, ctx->stream>>>(A);
-    ctx->launches++;
-    QCK(cudaGetLastError());
     std::vector<double> sums((size_t)T * n_ops);
     QCK(cudaMemcpyAsync(sums.data(), A.X, sums.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
     if (X_traj) QCK(cudaMemcpyAsync(X_traj, A.X_traj, (size_t)n_traj * T * n_ops * 8, cudaMemcpyDeviceToHost, ctx->stream));

@@ -15,6 +15,17 @@ import pysmoq as S
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(scope="module", params=[-1, 0, 3], ids=["auto", "resident", "streaming"])
+def qctx(request, built):
+    """engine -1 (default) and 0: every trajectory's state resident in shared memory;
+    3: the states stream through HBM between the plan's compiled passes"""
+    c = S.Context(0)
+    if request.param >= 0:
+        c.set_option(S._lib.OPT_ENGINE, request.param)
+    yield c
+    c.close()
+
+
 def ladder(L, seed=1, dt=0.1):
     """XXZ rails plus rungs with random z fields: bonds (i, j, Jxx, Jyy, Jzz), fields (q, hx, hy, hz), 1-based"""
     rng = np.random.default_rng(seed)
@@ -39,7 +50,8 @@ def run_gpu(ctx, L, gl, u, n_traj, dtype, **kw):
 
 @pytest.mark.parametrize("reset", ["traceout_rail_1", "traceout_rail_2"])
 @pytest.mark.parametrize("encoding", ["batch", "broadcast"])
-def test_trajectories_equal_the_oracle(ctx, reset, encoding):
+def test_trajectories_equal_the_oracle(qctx, reset, encoding):
+    ctx = qctx
     L, T, n_traj = 3, 12, 16
     arr, n, gl = gates_both(L)
     u = np.random.default_rng(4).uniform(0, 1, T)
@@ -53,18 +65,19 @@ def test_trajectories_equal_the_oracle(ctx, reset, encoding):
 
 
 @pytest.mark.parametrize("L,dtype,tol", [(6, S.C128, 1e-9), (7, S.C64, 2e-4), (1, S.C128, 1e-12)])
-def test_sizes_and_precisions(ctx, L, dtype, tol):
+def test_sizes_and_precisions(qctx, L, dtype, tol):
     """the largest rails each precision holds in shared memory, and the smallest"""
     T, n_traj = 4, 6
     arr, n, gl = gates_both(L, seed=L)
     u = np.random.default_rng(L).uniform(0, 1, T)
-    X, Xt = run_gpu(ctx, L, gl, u, n_traj, dtype, n_substeps=2, seed=3, per_trajectory=True)
+    X, Xt = run_gpu(qctx, L, gl, u, n_traj, dtype, n_substeps=2, seed=3, per_trajectory=True)
     Xr, Xtr = O.qrc_run(L, arr, n, u, n_traj, n_substeps=2, seed=3, per_trajectory=True)
     assert np.max(np.abs(Xt - Xtr)) < tol
 
 
-def test_initial_state_and_zero_substeps(ctx):
+def test_initial_state_and_zero_substeps(qctx):
     """a random initial state, and n_substeps = 0 (reset and measurement only)"""
+    ctx = qctx
     L, T, n_traj = 2, 6, 10
     arr, n, gl = gates_both(L, seed=8)
     rng = np.random.default_rng(8)
