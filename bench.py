@@ -418,7 +418,7 @@ def qrc_workload(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     ctx = S.Context(0)
-    L, T, B, sub, dt = 6, 100, 4096, 5, 0.1
+    L, T, B, sub, dt = 6, args.inputs, args.trajectories, 5, 0.1
     rng = np.random.default_rng(2026)
     bonds = [(r * L + s + 1, r * L + s + 2, 1.0, 1.0, 0.5) for r in range(2) for s in range(L - 1)]
     bonds += [(s + 1, L + s + 1, 0.7, 0.7, 0.3) for s in range(L)]
@@ -449,17 +449,17 @@ def qrc_workload(args):
     cpu = None
     if not args.no_cpu_baseline:
         ncpu = os.cpu_count() or 1
-        ntr = 4 * ncpu
+        ntr, ti = 4 * ncpu, min(20, T)
         t0 = time.perf_counter()
-        O.qrc_run(L, arr, n, u[:20], ntr, n_substeps=sub, seed=7, nthreads=ncpu)
+        O.qrc_run(L, arr, n, u[:ti], ntr, n_substeps=sub, seed=7, nthreads=ncpu)
         sec = time.perf_counter() - t0
-        cpu = {"value": ntr * 20 / sec, "unit": "trajectory-inputs/s", "cores": ncpu, "kind": "port",
-               "sample": f"{ntr} trajectories x 20 inputs of the same configuration, complex128, {sec:.1f} s"}
+        cpu = {"value": ntr * ti / sec, "unit": "trajectory-inputs/s", "cores": ncpu, "kind": "port",
+               "sample": f"{ntr} trajectories x {ti} inputs of the same configuration, complex128, {sec:.1f} s"}
     X64, X128 = res["c64"][3], res["c128"][3]
     line = {"metric": "qrc_trajectory_inputs_per_s", "value": res["c64"][0], "unit": "trajectory-inputs/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["c64"][1],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
-            "config": {"workload": "qrc_xxz_ladder_L6_4096traj_100inputs", "L": L, "N": 2 * L, "trajectories": B,
+            "config": {"workload": f"qrc_xxz_ladder_L6_{B}traj_{T}inputs", "L": L, "N": 2 * L, "trajectories": B,
                        "inputs": T, "n_substeps": sub, "features": S.qrc_n_ops(L), "encoding": "batch",
                        "reset": "traceout_rail_1", "state_bytes_per_trajectory": (1 << (2 * L)) * 8},
             "e2e": {"value": res["c64"][2], "unit": "trajectory-inputs/s",
@@ -540,6 +540,8 @@ def main():
     ap.add_argument("--jit-packed", type=int, default=0, help="compiled pass kernels: FP32x2 arithmetic (1) or scalar (0)")
     ap.add_argument("--jit-groups", type=int, default=2, help="compiled pass kernels: register groups per thread (1, 2)")
     ap.add_argument("--jit-stage-bits", type=int, default=4, help="compiled pass kernels: bits per register stage (4, 5)")
+    ap.add_argument("--trajectories", type=int, default=4096, help="qrc workload: trajectories")
+    ap.add_argument("--inputs", type=int, default=100, help="qrc workload: length of the input series")
     ap.add_argument("--workload", default="trotter", choices=["trotter", "vqe", "vqe_jobs", "mcwf", "bandwidth", "qrc"],
                     help="trotter: the headline line; vqe / bandwidth: the gradient and 32 GiB sweep figures")
     args = ap.parse_args()

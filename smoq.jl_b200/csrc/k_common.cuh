@@ -125,18 +125,26 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 // Apply one fused op to the amplitude array `psi` indexed by I.  `bits` are
 // the op's qubit positions in that index space.  `nthr`/`tid` stride the
 // groups.  Used on a shared-memory tile (I = uint32_t, local bits) and on a
-// whole state in HBM (I = uint64_t, global bits).
-template <typename R, typename I>
+// whole state in HBM (I = uint64_t, global bits).  `mp` maps a logical index
+// to its storage position (identity, or a bank swizzle of a shared-memory
+// layout); it must be XOR-linear, mp(x ^ y) = mp(x) ^ mp(y), so that a group's
+// other members sit at fixed XOR offsets from its first.
+struct IdMap {
+    template <typename I>
+    __device__ __forceinline__ I operator()(I i) const { return i; }
+};
+template <typename R, typename I, typename Map = IdMap>
 __device__ __forceinline__ void sweep_op(const DevOp& op, typename CT<R>::T* psi, int nbits,
-                                         const int* bits, I tid, I nthr) {
+                                         const int* bits, I tid, I nthr, Map mp = Map()) {
     using C = typename CT<R>::T;
     const int kind = op.kind;
     if (kind == OPK_DENSE1) {
         const int a = bits[0];
         const C m0 = coef<R>(op, 0), m1 = coef<R>(op, 1), m2 = coef<R>(op, 2), m3 = coef<R>(op, 3);
         const I n = I(1) << (nbits - 1);
+        const I oa = mp(I(1) << a);
         for (I g = tid; g < n; g += nthr) {
-            I i0 = ins0(g, a), i1 = i0 | (I(1) << a);
+            const I i0 = mp(ins0(g, a)), i1 = i0 ^ oa;
             C x = psi[i0], y = psi[i1];
             psi[i0] = cfma(m0, x, cmul(m1, y));
             psi[i1] = cfma(m2, x, cmul(m3, y));
@@ -144,15 +152,15 @@ __device__ __forceinline__ void sweep_op(const DevOp& op, typename CT<R>::T* psi
     } else if (kind == OPK_DENSE2 || kind == OPK_PARITY2) {
         const int a = bits[0], b = bits[1];
         const int lo = a < b ? a : b, hi = a < b ? b : a;
-        const I sa = I(1) << a, sb = I(1) << b;
+        const I sa = mp(I(1) << a), sb = mp(I(1) << b);  // storage offsets of the op's bits
         const I n = I(1) << (nbits - 2);
         if (kind == OPK_DENSE2) {
             C m[16];
 #pragma unroll
             for (int k = 0; k < 16; ++k) m[k] = coef<R>(op, k);
             for (I g = tid; g < n; g += nthr) {
-                I i0 = ins0(ins0(g, lo), hi);
-                I ix[4] = {i0, i0 | sa, i0 | sb, i0 | sa | sb};
+                const I i0 = mp(ins0(ins0(g, lo), hi));
+                const I ix[4] = {i0, i0 ^ sa, i0 ^ sb, i0 ^ sa ^ sb};
                 C v[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) v[k] = psi[ix[k]];
@@ -170,8 +178,8 @@ __device__ __forceinline__ void sweep_op(const DevOp& op, typename CT<R>::T* psi
             const C e0 = coef<R>(op, 0), e1 = coef<R>(op, 1), e2 = coef<R>(op, 2), e3 = coef<R>(op, 3);
             const C o0 = coef<R>(op, 4), o1 = coef<R>(op, 5), o2 = coef<R>(op, 6), o3 = coef<R>(op, 7);
             for (I g = tid; g < n; g += nthr) {
-                I i0 = ins0(ins0(g, lo), hi);
-                I i1 = i0 | sa, i2 = i0 | sb, i3 = i0 | sa | sb;
+                const I i0 = mp(ins0(ins0(g, lo), hi));
+                const I i1 = i0 ^ sa, i2 = i0 ^ sb, i3 = i0 ^ sa ^ sb;
                 C v0 = psi[i0], v1 = psi[i1], v2 = psi[i2], v3 = psi[i3];
                 psi[i0] = cfma(e0, v0, cmul(e1, v3));
                 psi[i3] = cfma(e2, v0, cmul(e3, v3));
@@ -198,9 +206,9 @@ __device__ __forceinline__ void sweep_op(const DevOp& op, typename CT<R>::T* psi
                 I x = i0;
                 for (int t = 0; t < nq; ++t) x |= (I)((m >> t) & 1) << bits[t];
                 ix[m] = x;
-                v[m] = psi[x];
+                v[m] = psi[mp(x)];
             }
-            for (int r = 0; r < dim; ++r) psi[ix[r]] = cmul(coef<R>(op, r), v[op.perm[r]]);
+            for (int r = 0; r < dim; ++r) psi[mp(ix[r])] = cmul(coef<R>(op, r), v[op.perm[r]]);
         }
     }
 }

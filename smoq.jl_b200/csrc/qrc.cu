@@ -68,6 +68,21 @@ constexpr int kQrcThreads = 256;
 #define SMOQ_QRC_MINB_C128 2
 #endif
 
+// Bank swizzle of a trajectory's state in shared memory: amplitude j is stored
+// at j ^ M(j), M XORing the bits inside one 128-byte bank row (16 complex64 or 8
+// complex128 amplitudes) with masks keyed by the two bits above the row.  The
+// masks make the 16 (8) lanes of a half-warp (quarter-warp) phase hit distinct
+// banks in every pair sweep on a qubit inside the row and in the 2-qubit sweeps
+// of adjacent qubits there (without it, 42% of the shared-memory wavefronts of
+// the ladder workload were bank conflicts).  An involution on [0, 2^N).
+template <typename R>
+struct QrcSwizzle {
+    __device__ __forceinline__ uint32_t operator()(uint32_t j) const {
+        return sizeof(R) == 4 ? j ^ (((j >> 4) & 1u) * 15u) ^ (((j >> 5) & 1u) * 10u)
+                              : j ^ (((j >> 3) & 1u) * 7u) ^ (((j >> 4) & 1u) * 5u);
+    }
+};
+
 // warp sum of x added into this warp's feature row
 __device__ __forceinline__ void qrc_flush(double x, double* row, int f, int lane) {
 #pragma unroll
@@ -95,7 +110,7 @@ __device__ __forceinline__ double qrc_uniform(uint64_t seed, uint64_t shot, uint
     return (double)(a * 67108864ull + b) * (1.0 / 9007199254740992.0);
 }
 
-// one evolution op on the whole state in shared memory (qubit t at bit lb[t])
+// one evolution op on the whole (swizzled) state in shared memory (qubit t at bit lb[t])
 template <typename R>
 __device__ __forceinline__ void qrc_apply(const DevOp& op, typename CT<R>::T* psi, int N, typename CT<R>::T* dco) {
     using C = typename CT<R>::T;
@@ -109,10 +124,11 @@ __device__ __forceinline__ void qrc_apply(const DevOp& op, typename CT<R>::T* ps
             int m = 0;
 #pragma unroll
             for (int t = 0; t < 4; ++t) m |= (int)((j >> sh[t]) & (uint32_t)(in >> t) & 1u) << t;
-            psi[j] = cmul(dco[m], psi[j]);
+            const uint32_t js = QrcSwizzle<R>()(j);
+            psi[js] = cmul(dco[m], psi[js]);
         }
     } else {
-        sweep_op<R, uint32_t>(op, psi, N, op.lb, tid, nthr);
+        sweep_op<R, uint32_t>(op, psi, N, op.lb, tid, nthr, QrcSwizzle<R>());
     }
 }
 
@@ -138,11 +154,13 @@ __device__ __forceinline__ QrcScratch<R> qrc_scratch(unsigned char* sm, uint32_t
 }
 
 // A + B for input k: encode the window, measure the rail of psi (shared memory)
-// with the draw of (k, traj), write |psi_in> (x) |phi> to out (shared or global;
-// out may alias psi: every read of psi ends before the first write)
-template <typename R>
+// with the draw of (k, traj), write |psi_in> (x) |phi> to out (shared memory
+// through the swizzle, or global through the identity; out may alias psi: every
+// read of psi ends before the first write)
+template <typename R, typename OutMap>
 __device__ __forceinline__ void qrc_reset(const QrcArgs& A, int k, uint64_t traj, const typename CT<R>::T* psi,
-                                          typename CT<R>::T* out, const QrcScratch<R>& S) {
+                                          typename CT<R>::T* out, OutMap om, const QrcScratch<R>& S) {
+    const QrcSwizzle<R> sw;
     using C = typename CT<R>::T;
     __shared__ int s_out;
     __shared__ double s_inv;
@@ -160,7 +178,7 @@ __device__ __forceinline__ void qrc_reset(const QrcArgs& A, int k, uint64_t traj
         const uint32_t x = tid & (d - 1), np = nthr / d;
         double s = 0;
         for (uint32_t y = tid / d; y < d; y += np) {
-            const C v = psi[A.protocol == 1 ? x + d * y : y + d * x];
+            const C v = psi[sw(A.protocol == 1 ? x + d * y : y + d * x)];
             s += (double)v.x * v.x + (double)v.y * v.y;
         }
         S.part[tid] = s;
@@ -195,7 +213,7 @@ __device__ __forceinline__ void qrc_reset(const QrcArgs& A, int k, uint64_t traj
     for (uint32_t y = tid; y < d; y += nthr) {
         C v;
         if (inv > 0) {
-            const C w = psi[A.protocol == 1 ? o + d * y : y + d * o];
+            const C w = psi[sw(A.protocol == 1 ? o + d * y : y + d * o)];
             v.x = (R)((double)w.x * inv);
             v.y = (R)((double)w.y * inv);
         } else {
@@ -211,7 +229,7 @@ __device__ __forceinline__ void qrc_reset(const QrcArgs& A, int k, uint64_t traj
         C z;
         z.x = w * v.x;
         z.y = w * v.y;
-        out[a] = z;
+        out[om(a)] = z;
     }
 }
 
@@ -228,10 +246,12 @@ __device__ __forceinline__ void qrc_features(const QrcArgs& A, int k, int64_t t,
     for (int g = 0; g < A.nobs; ++g) {
         const QrcObs ob = A.obs[g];
         const int a = ob.a, b = ob.b, lo = a < b ? a : b, hi = a < b ? b : a;
+        const QrcSwizzle<R> sw;
+        const uint32_t oa = sw(1u << a), ob_ = sw(1u << b);
         R xx = 0, yy = 0, zz = 0, xa = 0, ya = 0, za = 0, xb = 0, yb = 0, zb = 0;
         for (uint32_t h = tid; h < dim / 4; h += nthr) {
-            const uint32_t i00 = ins0<uint32_t>(ins0<uint32_t>(h, lo), hi);
-            const uint32_t i10 = i00 | (1u << a), i01 = i00 | (1u << b), i11 = i10 | (1u << b);
+            const uint32_t i00 = sw(ins0<uint32_t>(ins0<uint32_t>(h, lo), hi));  // (XOR-linear swizzle)
+            const uint32_t i10 = i00 ^ oa, i01 = i00 ^ ob_, i11 = i10 ^ ob_;
             const C v00 = psi[i00], v10 = psi[i10], v01 = psi[i01], v11 = psi[i11];
             const R n00 = v00.x * v00.x + v00.y * v00.y, n10 = v10.x * v10.x + v10.y * v10.y;
             const R n01 = v01.x * v01.x + v01.y * v01.y, n11 = v11.x * v11.x + v11.y * v11.y;
@@ -287,11 +307,11 @@ __global__ void __launch_bounds__(kQrcThreads, sizeof(R) == 4 ? SMOQ_QRC_MINB_C6
     const int tid = threadIdx.x;
     const C* p0 = reinterpret_cast<const C*>(A.psi0);
     for (int64_t t = blockIdx.x; t < A.n_traj; t += gridDim.x) {
-        for (uint32_t a = tid; a < dim; a += blockDim.x) psi[a] = p0[a];
+        for (uint32_t a = tid; a < dim; a += blockDim.x) psi[QrcSwizzle<R>()(a)] = p0[a];
         __syncthreads();
         const uint64_t traj = A.traj_offset + (uint64_t)t;
         for (int k = 0; k < A.T; ++k) {
-            qrc_reset<R>(A, k, traj, psi, psi, S);
+            qrc_reset<R>(A, k, traj, psi, psi, QrcSwizzle<R>(), S);
             __syncthreads();
             for (int q = 0; q < A.nops; ++q) {  // n_substeps Trotter steps
                 qrc_apply<R>(A.ops[q], psi, A.N, dco);
@@ -319,7 +339,7 @@ __global__ void __launch_bounds__(kQrcThreads, sizeof(R) == 4 ? SMOQ_QRC_MINB_C6
     const int tid = threadIdx.x;
     for (int64_t c = blockIdx.x; c < nchunk; c += gridDim.x) {
         const C* in = reinterpret_cast<const C*>(src) + c * src_stride;
-        for (uint32_t a = tid; a < dim; a += blockDim.x) psi[a] = in[a];
+        for (uint32_t a = tid; a < dim; a += blockDim.x) psi[QrcSwizzle<R>()(a)] = in[a];
         __syncthreads();
         if (k_obs >= 0) {
             qrc_features<R>(A, k_obs, t0 + c, psi, S);
@@ -327,7 +347,7 @@ __global__ void __launch_bounds__(kQrcThreads, sizeof(R) == 4 ? SMOQ_QRC_MINB_C6
         }
         if (k_obs + 1 < A.T) {
             qrc_reset<R>(A, k_obs + 1, A.traj_offset + (uint64_t)(t0 + c), psi,
-                         reinterpret_cast<C*>(dst) + c * (int64_t)dim, S);
+                         reinterpret_cast<C*>(dst) + c * (int64_t)dim, IdMap(), S);
             __syncthreads();
         }
     }
