@@ -87,6 +87,30 @@ __global__ void __launch_bounds__(256) ham_apply_kernel(const typename CT<R>::T*
 // (lambda), 2^T amplitudes each, and applies every U^dag op to both in the
 // same loop iteration (one index decode, one coefficient load for both).
 
+// Bank spreading.  A shared-memory phase of 16 (complex64) or 8 (complex128)
+// lanes covers one 128-byte row; a sweep over an op on bits inside that row
+// has every phase hit each bank twice (one such bit) or four times (two).  The
+// lanes whose group index has the bits just above the row's free bits set read
+// their group with the op's low bits flipped: flip pattern s in the op's
+// matrix index space (bit 0 = qubit 0, bit 1 = qubit 1), group member k at
+// logical member k ^ s, matrix M'[k][j] = M[k ^ s][j ^ s].  s is fixed per
+// thread (groups stride by blockDim, a multiple of 16).
+template <typename R>
+__device__ __forceinline__ int lane_flip(uint32_t tid, int a, int b) {
+    constexpr int B = sizeof(R) == 4 ? 4 : 3;  // amplitude bits of one 128-byte row
+    const bool la = a < B, lb = b >= 0 && b < B;
+    if (la && lb) {
+        const int f = (int)(tid >> (B - 2)) & 3;  // bit 0 flips the lower of the two positions
+        return a < b ? f : ((f & 1) << 1) | (f >> 1);
+    }
+    if (la) return (int)(tid >> (B - 1)) & 1;
+    if (lb) return ((int)(tid >> (B - 1)) & 1) << 1;
+    return 0;
+}
+__device__ __forceinline__ uint32_t flip_bits(int s, int a, int b) {
+    return ((s & 1) ? 1u << a : 0u) | ((s & 2) ? 1u << b : 0u);
+}
+
 // U^dag op on both tiles; dco: 16 shared-memory slots for diagonal tables
 template <typename R>
 __device__ __forceinline__ void dual_apply(const DevOp& op, typename CT<R>::T* P, typename CT<R>::T* Q, int T,
@@ -95,9 +119,10 @@ __device__ __forceinline__ void dual_apply(const DevOp& op, typename CT<R>::T* P
     const uint32_t tid = threadIdx.x, nthr = blockDim.x;
     if (op.kind == OPK_DENSE1) {
         const int a = op.lb[0];
-        const C m0 = coef<R>(op, 0), m1 = coef<R>(op, 1), m2 = coef<R>(op, 2), m3 = coef<R>(op, 3);
+        const int f = lane_flip<R>(tid, a, -1);  // 0 or 1: M' = M with both indices flipped
+        const C m0 = coef<R>(op, 3 * f), m1 = coef<R>(op, 1 + f), m2 = coef<R>(op, 2 - f), m3 = coef<R>(op, 3 - 3 * f);
         for (uint32_t g = tid; g < (1u << (T - 1)); g += nthr) {
-            const uint32_t i0 = ins0<uint32_t>(g, a), i1 = i0 | (1u << a);
+            const uint32_t i0 = ins0<uint32_t>(g, a) ^ ((uint32_t)f << a), i1 = i0 ^ (1u << a);
             const C x = P[i0], y = P[i1], u = Q[i0], v = Q[i1];
             P[i0] = cfma(m0, x, cmul(m1, y));
             P[i1] = cfma(m2, x, cmul(m3, y));
@@ -107,12 +132,14 @@ __device__ __forceinline__ void dual_apply(const DevOp& op, typename CT<R>::T* P
     } else if (op.kind == OPK_DENSE2) {
         const int a = op.lb[0], b = op.lb[1];
         const int lo = a < b ? a : b, hi = a < b ? b : a;
+        const int f = lane_flip<R>(tid, a, b);
+        const uint32_t fb = flip_bits(f, a, b);
         C m[16];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) m[k] = coef<R>(op, k);
+        for (int k = 0; k < 16; ++k) m[k] = coef<R>(op, (((k >> 2) ^ f) << 2) | ((k & 3) ^ f));
         for (uint32_t g = tid; g < (1u << (T - 2)); g += nthr) {
-            const uint32_t i0 = ins0<uint32_t>(ins0<uint32_t>(g, lo), hi);
-            const uint32_t ix[4] = {i0, i0 | (1u << a), i0 | (1u << b), i0 | (1u << a) | (1u << b)};
+            const uint32_t i0 = ins0<uint32_t>(ins0<uint32_t>(g, lo), hi) ^ fb;
+            const uint32_t ix[4] = {i0, i0 ^ (1u << a), i0 ^ (1u << b), i0 ^ (1u << a) ^ (1u << b)};
             C x[4], y[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) x[k] = P[ix[k]], y[k] = Q[ix[k]];
@@ -128,11 +155,19 @@ __device__ __forceinline__ void dual_apply(const DevOp& op, typename CT<R>::T* P
     } else if (op.kind == OPK_PARITY2) {
         const int a = op.lb[0], b = op.lb[1];
         const int lo = a < b ? a : b, hi = a < b ? b : a;
-        const C e0 = coef<R>(op, 0), e1 = coef<R>(op, 1), e2 = coef<R>(op, 2), e3 = coef<R>(op, 3);
-        const C o0 = coef<R>(op, 4), o1 = coef<R>(op, 5), o2 = coef<R>(op, 6), o3 = coef<R>(op, 7);
+        // flipped members: s = 1, 2 exchange the even (00, 11) and odd (01, 10)
+        // blocks, s = 2, 3 reverse each block
+        const int f = lane_flip<R>(tid, a, b);
+        const uint32_t fb = flip_bits(f, a, b);
+        const int eb = (f == 1 || f == 2) ? 4 : 0, ob = 4 - eb;
+        const bool rv = f >= 2;
+        const C e0 = coef<R>(op, eb + (rv ? 3 : 0)), e1 = coef<R>(op, eb + (rv ? 2 : 1));
+        const C e2 = coef<R>(op, eb + (rv ? 1 : 2)), e3 = coef<R>(op, eb + (rv ? 0 : 3));
+        const C o0 = coef<R>(op, ob + (rv ? 3 : 0)), o1 = coef<R>(op, ob + (rv ? 2 : 1));
+        const C o2 = coef<R>(op, ob + (rv ? 1 : 2)), o3 = coef<R>(op, ob + (rv ? 0 : 3));
         for (uint32_t g = tid; g < (1u << (T - 2)); g += nthr) {
-            const uint32_t i0 = ins0<uint32_t>(ins0<uint32_t>(g, lo), hi);
-            const uint32_t i1 = i0 | (1u << a), i2 = i0 | (1u << b), i3 = i1 | (1u << b);
+            const uint32_t i0 = ins0<uint32_t>(ins0<uint32_t>(g, lo), hi) ^ fb;
+            const uint32_t i1 = i0 ^ (1u << a), i2 = i0 ^ (1u << b), i3 = i1 ^ (1u << b);
             C v0 = P[i0], v1 = P[i1], v2 = P[i2], v3 = P[i3];
             P[i0] = cfma(e0, v0, cmul(e1, v3));
             P[i3] = cfma(e2, v0, cmul(e3, v3));
@@ -194,27 +229,30 @@ __device__ __forceinline__ R inner_pairs(const DevOp& op, typename CT<R>::T* P, 
     using C = typename CT<R>::T;
     constexpr int D = 1 << NQ;
     const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const int a = op.lb[0], b = NQ == 2 ? op.lb[1] : 0;
+    const int lo = a < b ? a : b, hi = a < b ? b : a;
+    // member k of this thread's groups is logical member k ^ f (bank spreading)
+    const int f = lane_flip<R>(tid, a, NQ == 2 ? b : -1);
+    const uint32_t fb = flip_bits(f, a, b);
     R wr[D], wi[D];
     int col[D];
 #pragma unroll
-    for (int r = 0; r < D; ++r) code_weights<R>(op.slot[r], wr[r], wi[r]), col[r] = op.perm[1 + r];
+    for (int r = 0; r < D; ++r) code_weights<R>(op.slot[r ^ f], wr[r], wi[r]), col[r] = op.perm[1 + (r ^ f)] ^ f;
     C m[D * D];
 #pragma unroll
-    for (int k = 0; k < D * D; ++k) m[k] = PRE ? coef<R>(op, k) : C{};
-    const int a = op.lb[0], b = NQ == 2 ? op.lb[1] : 0;
-    const int lo = a < b ? a : b, hi = a < b ? b : a;
+    for (int k = 0; k < D * D; ++k) m[k] = PRE ? coef<R>(op, (((k / D) ^ f) * D) + ((k % D) ^ f)) : C{};
     R acc = 0;
     for (uint32_t g = tid; g < (1u << (T - NQ)); g += nthr) {
         uint32_t ix[D];
         if (NQ == 1) {
-            ix[0] = ins0<uint32_t>(g, a);
-            ix[D - 1] = ix[0] | (1u << a);
+            ix[0] = ins0<uint32_t>(g, a) ^ fb;
+            ix[D - 1] = ix[0] ^ (1u << a);
         } else {
-            const uint32_t i0 = ins0<uint32_t>(ins0<uint32_t>(g, lo), hi);
+            const uint32_t i0 = ins0<uint32_t>(ins0<uint32_t>(g, lo), hi) ^ fb;
             ix[0] = i0;
-            ix[1 % D] = i0 | (1u << a);
-            ix[2 % D] = i0 | (1u << b);
-            ix[D - 1] = i0 | (1u << a) | (1u << b);
+            ix[1 % D] = i0 ^ (1u << a);
+            ix[2 % D] = i0 ^ (1u << b);
+            ix[D - 1] = i0 ^ (1u << a) ^ (1u << b);
         }
         C p[D], l[D];
 #pragma unroll
