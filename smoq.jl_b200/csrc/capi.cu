@@ -536,18 +536,16 @@ static smoq_status ops_to_ir(smoq_state* st, int N, const smoq_op* ops, int n, c
             a = theta[o.param];
         }
         if (!std::isfinite(a)) return fail(ctx, SMOQ_ERR_BADINPUT, "op angle is not finite");
-        GateIR g;
         if (o.type == SMOQ_G_U1) {
             cd m[4];
             load_colmajor(o.U, 2, m);
-            g = gate_1q(o.q[0], m);
+            out.push_back(gate_1q(o.q[0], m));
         } else if (o.type == SMOQ_G_U2) {
-            g = u2_gate(o.q[0], o.q[1], o.U, 0);
+            out.push_back(u2_gate(o.q[0], o.q[1], o.U, 0));
         } else {
-            g = gate_named(o.type, o.q, a);
+            out.push_back(gate_named(o.type, o.q, a));
         }
-        g.tag = o.param;
-        out.push_back(g);
+        out.back().tag = o.param;
     }
     return SMOQ_OK;
 }

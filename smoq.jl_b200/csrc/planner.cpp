@@ -499,6 +499,7 @@ std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, in
         for (int b = L; b < N; ++b)
             if ((tileset >> b) & 1) p.g.hb[p.g.H++] = b;
         Fuser f(&p.g);
+        f.ops.reserve(taken.size() + 64);  // (a flush adds at most one op per qubit)
         for (int idx : taken) {
             f.add(gates[idx]);
             if (epilogue_after_special >= 0 && gates[idx].special == epilogue_after_special) p.epilogue = true;

@@ -101,6 +101,17 @@ struct TileArgs {
 // ----------------------------------------------------------------------------
 // Host-side gate IR consumed by the planner.
 // ----------------------------------------------------------------------------
+// Storage of a gate matrix (up to 16 x 16): complex entries that are NOT
+// initialised on construction -- a gate list holds thousands of these, and every
+// producer writes the 2^nq x 2^nq block it uses before anything reads it.
+struct GateMatrix {
+    alignas(16) double v[512];
+    cd& operator[](int i) { return reinterpret_cast<cd*>(v)[i]; }
+    const cd& operator[](int i) const { return reinterpret_cast<const cd*>(v)[i]; }
+    operator cd*() { return reinterpret_cast<cd*>(v); }
+    operator const cd*() const { return reinterpret_cast<const cd*>(v); }
+};
+
 struct GateIR {
     int nq = 0;             // 0..3 qubits (diagonals merged by the fuser: up to 4)
     int q[4] = {0, 0, 0, 0};  // 0-based global qubits
@@ -108,7 +119,7 @@ struct GateIR {
     int special = 0;        // 0: matrix gate; OPK_STATESCALE / OPK_REALTAB / OPK_JUMP
     const void* aux = nullptr;
     int64_t aux2 = 0;
-    cd m[256];              // row-major 2^nq x 2^nq; bit t of an index = qubit q[t]
+    GateMatrix m;           // row-major 2^nq x 2^nq; bit t of an index = qubit q[t]
     int tag = -1;           // caller tag (e.g. parameter index) carried through
 };
 

@@ -487,12 +487,19 @@ bool generator(int type, GateIR& g) {
     }
 }
 
-GateIR dagger(const GateIR& g) {
-    GateIR d = g;
+// d = g^dag, written into a freshly constructed d (only the 2^nq x 2^nq block of
+// the 256-entry matrix is touched: a gate list holds thousands of these)
+void dagger_into(const GateIR& g, GateIR& d) {
+    d.nq = g.nq;
+    for (int t = 0; t < 4; ++t) d.q[t] = g.q[t];
+    d.diag = g.diag;
+    d.special = g.special;
+    d.aux = g.aux;
+    d.aux2 = g.aux2;
+    d.tag = g.tag;
     const int dim = 1 << g.nq;
     for (int r = 0; r < dim; ++r)
         for (int c = 0; c < dim; ++c) d.m[r * dim + c] = std::conj(g.m[c * dim + r]);
-    return d;
 }
 
 // shared memory of the widest adjoint tile: two states of 2^13 complex64 or 2^12
@@ -677,9 +684,11 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
         // the backward program: for k = n-1 .. 0: [inner(G_k)] then U_k^dag
         std::vector<GateIR> back;
         std::vector<int> inner_param;
+        back.reserve(2 * (size_t)n);
         for (int k = n - 1; k >= 0; --k) {
             if (ops[k].param >= 0) {
-                GateIR gi;
+                back.emplace_back();
+                GateIR& gi = back.back();
                 gi.nq = ir[k].nq;
                 for (int t = 0; t < gi.nq; ++t) gi.q[t] = ir[k].q[t];
                 if (!generator(ops[k].type, gi))
@@ -688,9 +697,9 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
                 gi.special = OPK_INNER;
                 gi.aux2 = (int64_t)inner_param.size();
                 inner_param.push_back(ops[k].param);
-                back.push_back(gi);
             }
-            back.push_back(dagger(ir[k]));
+            back.emplace_back();
+            dagger_into(ir[k], back.back());
         }
         if (inner_param.empty()) continue;
         // tiles for two states in shared memory: one qubit narrower than the single-state passes
