@@ -72,9 +72,12 @@ enum {
                                      per thread; measured slower on B200) */,
     SMOQ_OPT_JIT_GROUPS = 10,     /* compiled pass kernels: 16-amplitude register groups per thread, 2
                                      (default; 2^(T-5) threads) or 1 (2^(T-4) threads) */
-    SMOQ_OPT_JIT_STAGE_BITS = 11  /* compiled pass kernels: tile bits per register stage, 4 (default) or 5
+    SMOQ_OPT_JIT_STAGE_BITS = 11, /* compiled pass kernels: tile bits per register stage, 4 (default) or 5
                                      (32-amplitude stages: fewer shared-memory round trips per pass;
                                      needs 2 groups per thread and scalar arithmetic) */
+    SMOQ_OPT_VQE_RESIDENT = 12    /* smoq_energy_grad_jobs: 1 (default) = circuits of N <= 13 (complex64)
+                                     or N <= 12 (complex128) run together in one launch, each in one
+                                     CTA's shared memory; 0 = every circuit through the tiled passes */
 };
 smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long value);
 /* launches: kernels launched by this context; tile_passes/tile_ms/tile_bytes:
@@ -309,9 +312,12 @@ smoq_status smoq_energy(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* o
  * Hamiltonians: the reference evaluates such batches one circuit at a time with
  * calculate_gradients, cpuVariationalQuantumCircuitGradients.jl:88, inside a
  * Threads.@threads loop).  Each job is one circuit with one parameter vector;
- * grad may be NULL (energy only).  The jobs run in submission order on the
- * context's stream; the call returns when all are done.  The first failing
- * job's status is returned, with its index in the message. */
+ * grad may be NULL (energy only).  Circuits whose two states fit one CTA's
+ * shared memory (N <= 13 complex64, N <= 12 complex128) run together in one
+ * launch, one CTA per circuit (SMOQ_OPT_VQE_RESIDENT); the others run in
+ * submission order on the context's stream; the call returns when all are
+ * done.  The first failing job's status is returned, with its index in the
+ * message. */
 typedef struct {
     int N;                        /* qubits of this circuit */
     const smoq_op* ops;           /* its gate list */

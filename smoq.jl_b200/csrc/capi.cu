@@ -283,6 +283,7 @@ smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long v) {
             if (v != 1 && v != 2) return fail(ctx, SMOQ_ERR_BADINPUT, "compiled-kernel tile buffers must be 1 or 2");
             ctx->jit_buffers = (int)v;
             break;
+        case SMOQ_OPT_VQE_RESIDENT: ctx->vqe_resident = v != 0; break;
         default: return fail(ctx, SMOQ_ERR_BADINPUT, "unknown option");
     }
     return SMOQ_OK;

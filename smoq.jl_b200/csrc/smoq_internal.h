@@ -199,6 +199,7 @@ struct smoq_ctx {
     int jit_packed = 0;                // compiled pass kernels: FP32x2 arithmetic on group pairs
     int jit_groups = 2;                // compiled pass kernels: 16-amplitude register groups per thread
     int jit_stage_bits = 4;            // compiled pass kernels: tile bits per register stage (4 or 5)
+    bool vqe_resident = true;          // many-circuit VQE: small circuits in one shared-memory launch
     long long launches = 0;            // kernels launched by this ctx
     long long tile_passes = 0;
     double tile_ms = 0;                // summed tile-pass time when kernel_timing

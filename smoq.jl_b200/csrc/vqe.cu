@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <string>
@@ -315,6 +316,63 @@ __device__ __forceinline__ uint32_t diag_desc(const DevOp& op) {
 
 constexpr int kDiagRun = 8;  // real-diagonal measurements folded into one sweep
 
+// The backward program of one tile pair (phi in tP, lambda in tL, 2^T amplitudes
+// each, in shared memory): U^dag ops on both, measurements through flush(acc, column)
+template <typename R, typename Flush>
+__device__ __forceinline__ void adj_program(const DevOp* ops, int nops, typename CT<R>::T* tP, typename CT<R>::T* tL,
+                                            int T, uint64_t base, typename CT<R>::T* dco, Flush flush) {
+    using C = typename CT<R>::T;
+    const int tid = threadIdx.x;
+    const uint32_t amps = 1u << T;
+    for (int o = 0; o < nops;) {
+        const DevOp& op = ops[o];
+        bool writes = true;
+        if (op.kind == OPK_INNER && op.flags == INNER_DIAGG) {
+            // a run of real-diagonal measurements (RZ, RZZ generators): one read
+            // of both tiles, Im(conj(l) p) signed per measurement
+            int k = 1;
+            while (k < kDiagRun && o + k < nops && ops[o + k].kind == OPK_INNER &&
+                   ops[o + k].flags == INNER_DIAGG)
+                ++k;
+            uint32_t d[kDiagRun];
+            R acc[kDiagRun];
+#pragma unroll
+            for (int u = 0; u < kDiagRun; ++u) acc[u] = 0, d[u] = u < k ? diag_desc(ops[o + u]) : 0u;
+            for (uint32_t j = tid; j < amps; j += blockDim.x) {
+                const C p = tP[j], l = tL[j];
+                const R zi = fma(l.x, p.y, -l.y * p.x);
+#pragma unroll
+                for (int u = 0; u < kDiagRun; ++u) {
+                    if (u < k) {
+                        const uint32_t r = ((j >> (d[u] & 31)) & 1) | (((j >> ((d[u] >> 5) & 31)) & 1) << 1);
+                        const R x = ((d[u] >> (10 + r)) & 1) ? -zi : zi;
+                        acc[u] += ((d[u] >> (14 + r)) & 1) ? R(0) : x;
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kDiagRun; ++u)
+                if (u < k) flush(acc[u], ops[o + u].perm[0]);
+            o += k;
+            writes = false;
+        } else if (op.kind == OPK_INNER) {
+            const bool pre = op.flags & INNER_PRE;
+            R acc;
+            if (op.nq == 1) acc = pre ? inner_pairs<R, 1, true>(op, tP, tL, T) : inner_pairs<R, 1, false>(op, tP, tL, T);
+            else acc = pre ? inner_pairs<R, 2, true>(op, tP, tL, T) : inner_pairs<R, 2, false>(op, tP, tL, T);
+            flush(acc, op.perm[0]);
+            writes = pre;
+            ++o;
+        } else {
+            dual_apply<R>(op, tP, tL, T, base, dco);
+            ++o;
+        }
+        // consecutive read-only measurements need no barrier between them
+        const bool next_writes = o < nops && !(ops[o].kind == OPK_INNER && !(ops[o].flags & INNER_PRE));
+        if (writes || next_writes) __syncthreads();
+    }
+}
+
 // 2 (complex128) or 3 (complex64) CTAs per SM: one CTA's bulk copies overlap another's sweeps
 template <typename R>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) adj_tile_kernel(const AdjArgs A) {
@@ -356,53 +414,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) adj_tile_kernel(c
             return;
         }
         phase ^= 1;
-        for (int o = 0; o < a.nops;) {
-            const DevOp& op = a.ops[o];
-            bool writes = true;
-            if (op.kind == OPK_INNER && op.flags == INNER_DIAGG) {
-                // a run of real-diagonal measurements (RZ, RZZ generators): one read
-                // of both tiles, Im(conj(l) p) signed per measurement
-                int k = 1;
-                while (k < kDiagRun && o + k < a.nops && a.ops[o + k].kind == OPK_INNER &&
-                       a.ops[o + k].flags == INNER_DIAGG)
-                    ++k;
-                uint32_t d[kDiagRun];
-                R acc[kDiagRun];
-#pragma unroll
-                for (int u = 0; u < kDiagRun; ++u) acc[u] = 0, d[u] = u < k ? diag_desc(a.ops[o + u]) : 0u;
-                for (uint32_t j = tid; j < amps; j += blockDim.x) {
-                    const C p = tP[j], l = tL[j];
-                    const R zi = fma(l.x, p.y, -l.y * p.x);
-#pragma unroll
-                    for (int u = 0; u < kDiagRun; ++u) {
-                        if (u < k) {
-                            const uint32_t r = ((j >> (d[u] & 31)) & 1) | (((j >> ((d[u] >> 5) & 31)) & 1) << 1);
-                            const R x = ((d[u] >> (10 + r)) & 1) ? -zi : zi;
-                            acc[u] += ((d[u] >> (14 + r)) & 1) ? R(0) : x;
-                        }
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < kDiagRun; ++u)
-                    if (u < k) inner_flush<R>(acc[u], A, a.ops[o + u].perm[0]);
-                o += k;
-                writes = false;
-            } else if (op.kind == OPK_INNER) {
-                const bool pre = op.flags & INNER_PRE;
-                R acc;
-                if (op.nq == 1) acc = pre ? inner_pairs<R, 1, true>(op, tP, tL, T) : inner_pairs<R, 1, false>(op, tP, tL, T);
-                else acc = pre ? inner_pairs<R, 2, true>(op, tP, tL, T) : inner_pairs<R, 2, false>(op, tP, tL, T);
-                inner_flush<R>(acc, A, op.perm[0]);
-                writes = pre;
-                ++o;
-            } else {
-                dual_apply<R>(op, tP, tL, T, base, dco);
-                ++o;
-            }
-            // consecutive read-only measurements need no barrier between them
-            const bool next_writes = o < a.nops && !(a.ops[o].kind == OPK_INNER && !(a.ops[o].flags & INNER_PRE));
-            if (writes || next_writes) __syncthreads();
-        }
+        adj_program<R>(a.ops, a.nops, tP, tL, T, base, dco,
+                       [&](R acc, int col) { inner_flush<R>(acc, A, col); });
         fence_proxy_async_smem();
         __syncthreads();
         for (uint32_t s = tid; s < 2 * nseg; s += blockDim.x) {
@@ -436,6 +449,109 @@ __global__ void __launch_bounds__(1024) adj_colsum_kernel(const double* part, in
         double t = 0;
         for (int k = 0; k < 32; ++k) t += red[k][lane];
         out[c] = t;
+    }
+}
+
+// ---------------------------------------------------------------- many small circuits, one launch
+// A circuit whose two states (phi, lambda) fit one CTA's shared memory runs
+// entirely there: forward program, lambda = H phi and the energy, then the
+// backward program; one CTA per circuit, persistent over the job list.
+struct ResJob {
+    int32_t N;
+    int32_t fwd_off, fwd_n;  // forward ops (whole-state tile)
+    int32_t bwd_off, bwd_n;  // backward ops (whole-state tile pair)
+    int32_t term_off, nterms;
+    int32_t col_off;         // first gradient column of the job
+};
+struct ResArgs {
+    const ResJob* jobs;
+    const DevOp* ops;
+    const HamTerm* terms;
+    double* energy;  // [njobs]
+    double* cols;    // [columns of all jobs], zeroed
+    int32_t njobs;
+};
+
+template <typename R>
+__device__ __forceinline__ void res_apply(const DevOp& op, typename CT<R>::T* psi, int N, typename CT<R>::T* dco) {
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    if (op.kind == OPK_DIAG) {
+        if (tid < 16) dco[tid] = coef<R>(op, (int)tid);
+        __syncthreads();
+        int sh[4] = {0, 0, 0, 0}, in = 0;
+        for (int t = 0; t < op.nq; ++t) sh[t] = op.lb[t], in |= 1 << t;
+        for (uint32_t j = tid; j < (1u << N); j += nthr) {
+            int m = 0;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) m |= (int)((j >> sh[t]) & (uint32_t)(in >> t) & 1u) << t;
+            psi[j] = cmul(dco[m], psi[j]);
+        }
+    } else {
+        sweep_op<R, uint32_t>(op, psi, N, op.lb, tid, nthr);
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) vqe_resident_kernel(const ResArgs A) {
+    using C = typename CT<R>::T;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ C dco[16];
+    __shared__ double red[8];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int j = blockIdx.x; j < A.njobs; j += gridDim.x) {
+        const ResJob J = A.jobs[j];
+        const uint32_t dim = 1u << J.N;
+        C* P = reinterpret_cast<C*>(smem_raw);
+        C* Q = P + dim;
+        for (uint32_t a = tid; a < dim; a += blockDim.x) {
+            C z;
+            z.x = (R)(a == 0 ? 1 : 0);
+            z.y = (R)0;
+            P[a] = z;
+        }
+        __syncthreads();
+        for (int o = 0; o < J.fwd_n; ++o) {
+            res_apply<R>(A.ops[J.fwd_off + o], P, J.N, dco);
+            __syncthreads();
+        }
+        // lambda = H phi and Re <phi|lambda> (the pull rule of ham_apply_kernel)
+        double acc = 0;
+        for (uint32_t k = tid; k < dim; k += blockDim.x) {
+            double lr = 0, li = 0;
+            for (int t = 0; t < J.nterms; ++t) {
+                const HamTerm& h = A.terms[J.term_off + t];
+                const uint32_t i = k ^ (uint32_t)h.x;
+                const C p = P[i];
+                const double sg = h.coef * ((__popc(i & (uint32_t)h.z) & 1) ? -1.0 : 1.0);
+                const int yk = h.ny & 3;
+                double pr = p.x, pi = p.y;
+                if (yk == 1) { const double tr = -pi; pi = pr; pr = tr; }
+                else if (yk == 2) { pr = -pr; pi = -pi; }
+                else if (yk == 3) { const double tr = pi; pi = -pr; pr = tr; }
+                lr += sg * pr;
+                li += sg * pi;
+            }
+            C o;
+            o.x = (R)lr;
+            o.y = (R)li;
+            Q[k] = o;
+            const C f = P[k];
+            acc += (double)f.x * lr + (double)f.y * li;
+        }
+        for (int d = 16; d > 0; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
+        if (lane == 0) red[warp] = acc;
+        __syncthreads();
+        if (tid == 0) {
+            double e = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) e += red[w];
+            A.energy[j] = e;
+        }
+        adj_program<R>(A.ops + J.bwd_off, J.bwd_n, P, Q, J.N, 0, dco, [&](R a, int col) {
+            double x = (double)a;
+            for (int d = 16; d > 0; d >>= 1) x += __shfl_xor_sync(0xffffffffu, x, d);
+            if (lane == 0) atomicAdd(&A.cols[J.col_off + col], x);
+        });
+        __syncthreads();
     }
 }
 
@@ -517,6 +633,11 @@ struct Work {
 };
 
 constexpr int kAdjThreads = 256;  // the adjoint kernel's __launch_bounds__
+// circuits with both states in one CTA's shared memory: 2 x 2^13 complex64 or
+// 2 x 2^12 complex128 = 128 KB
+constexpr int kResMaxN64 = 13, kResMaxN128 = 12;
+constexpr size_t kResMaxSmem = (size_t)2 * 8 << kResMaxN64;
+static_assert(((size_t)2 * 16 << kResMaxN128) == kResMaxSmem, "same limit for both precisions");
 
 // dense row-major matrix of a 1- or 2-qubit U^dag op (false: not a dense/diagonal kind)
 bool op_dense(const DevOp& op, cd* M) {
@@ -803,8 +924,156 @@ cudaError_t smoq::vqe_kernels_init(smoq_ctx* ctx) {
     cudaError_t e = cudaFuncSetAttribute(adj_tile_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)kAdjMaxSmem);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(adj_tile_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kAdjMaxSmem);
+    e = cudaFuncSetAttribute(adj_tile_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdjMaxSmem);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(vqe_resident_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kResMaxSmem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(vqe_resident_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kResMaxSmem);
+}
+
+// ---------------------------------------------------------------- many small circuits
+// the whole-state program of a circuit (one tile spanning every qubit), appended to out
+static smoq_status whole_state_ops(smoq_ctx* ctx, const std::vector<GateIR>& gates, int N, int dtype, bool backward,
+                                   std::vector<DevOp>& out) {
+    if (gates.empty()) return SMOQ_OK;
+    std::vector<Pass> passes;
+    try {
+        passes = plan_passes(gates, N, N, std::min(N, smoq_internal_low_bits(ctx, dtype)), -1, 0);
+    } catch (const std::exception& ex) {
+        return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
+    }
+    for (Pass& p : passes) {
+        if (backward)
+            if (smoq_status s = fuse_measurements(ctx, p.ops)) return s;
+        for (const DevOp& op : p.ops) {
+            const bool kind_ok = op.kind == OPK_DENSE1 || op.kind == OPK_DENSE2 || op.kind == OPK_PARITY2 ||
+                                 op.kind == OPK_MONO || op.kind == OPK_DIAG || (backward && op.kind == OPK_INNER);
+            bool bits_ok = op.nq >= 0 && op.nq <= 4;
+            for (int t = 0; bits_ok && t < op.nq; ++t) bits_ok = op.lb[t] == op.gb[t] && op.lb[t] >= 0 && op.lb[t] < N;
+            if (!kind_ok || !bits_ok)
+                return smoq_internal_fail(ctx, SMOQ_ERR_UNSUPPORTED, "whole-state program: op outside the tile");
+            out.push_back(op);
+        }
+    }
+    return SMOQ_OK;
+}
+
+// jobs[idx[*]] in one launch of vqe_resident_kernel
+static smoq_status run_resident(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vqe_job* jobs, const std::vector<int>& idx) {
+    std::vector<ResJob> rj;
+    std::vector<DevOp> ops;
+    std::vector<HamTerm> terms;
+    std::vector<std::vector<int>> inner_param(idx.size());
+    int32_t ncols = 0;
+    int nmax = 1;
+    for (size_t u = 0; u < idx.size(); ++u) {
+        const smoq_vqe_job& J = jobs[idx[u]];
+        auto job_fail = [&](smoq_status s) {
+            const std::string why = "job " + std::to_string(idx[u]) + ": " + smoq_last_error(ctx);
+            return smoq_internal_fail(ctx, s, why.c_str());
+        };
+        if (smoq_status s = check_vqe_args(ctx, J.N, dtype, J.ops, J.n, J.n_params, J.H, J.nterms, 1, J.theta))
+            return job_fail(s);
+        std::vector<GateIR> ir;
+        if (smoq_status s = smoq_internal_ops_to_ir(J.N, J.ops, J.n, J.theta, ir))
+            return job_fail(smoq_internal_fail(ctx, s, "bad op list"));
+        ResJob r;
+        r.N = J.N;
+        nmax = std::max(nmax, J.N);
+        r.fwd_off = (int32_t)ops.size();
+        if (smoq_status s = whole_state_ops(ctx, ir, J.N, dtype, false, ops)) return job_fail(s);
+        r.fwd_n = (int32_t)ops.size() - r.fwd_off;
+        r.bwd_off = (int32_t)ops.size();
+        if (J.grad) {
+            // the backward program, as vqe_run builds it
+            std::vector<GateIR> back;
+            back.reserve(2 * (size_t)J.n);
+            for (int k = J.n - 1; k >= 0; --k) {
+                if (J.ops[k].param >= 0) {
+                    back.emplace_back();
+                    GateIR& gi = back.back();
+                    gi.nq = ir[k].nq;
+                    for (int t = 0; t < gi.nq; ++t) gi.q[t] = ir[k].q[t];
+                    if (!generator(J.ops[k].type, gi))
+                        return job_fail(smoq_internal_fail(ctx, SMOQ_ERR_UNSUPPORTED,
+                                                           "adjoint gradient: parameterised gate type has no generator"));
+                    gi.special = OPK_INNER;
+                    gi.aux2 = (int64_t)inner_param[u].size();
+                    inner_param[u].push_back(J.ops[k].param);
+                }
+                back.emplace_back();
+                dagger_into(ir[k], back.back());
+            }
+            if (!inner_param[u].empty())
+                if (smoq_status s = whole_state_ops(ctx, back, J.N, dtype, true, ops)) return job_fail(s);
+        }
+        r.bwd_n = (int32_t)ops.size() - r.bwd_off;
+        r.term_off = (int32_t)terms.size();
+        r.nterms = J.nterms;
+        for (int t = 0; t < J.nterms; ++t) {
+            HamTerm h;
+            h.coef = J.H[t].coef;
+            h.x = J.H[t].xmask;
+            h.z = J.H[t].zmask;
+            h.ny = __builtin_popcountll(J.H[t].xmask & J.H[t].zmask);
+            h.pad = 0;
+            terms.push_back(h);
+        }
+        r.col_off = ncols;
+        ncols += (int32_t)inner_param[u].size();
+        rj.push_back(r);
+    }
+    const int n = (int)rj.size();
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t b_jobs = al(rj.size() * sizeof(ResJob)), b_ops = al(std::max<size_t>(1, ops.size()) * sizeof(DevOp)),
+                 b_terms = al(terms.size() * sizeof(HamTerm)), b_e = al((size_t)n * 8),
+                 b_c = al((size_t)std::max(1, ncols) * 8);
+    char* buf = nullptr;
+    VCK(cudaMallocAsync((void**)&buf, b_jobs + b_ops + b_terms + b_e + b_c, ctx->stream));
+    std::unique_ptr<char, std::function<void(char*)>> hold(buf, [ctx](char* q) { cudaFreeAsync(q, ctx->stream); });
+    ResArgs A;
+    char* c = buf;
+    A.jobs = (const ResJob*)c;
+    VCK(cudaMemcpyAsync(c, rj.data(), rj.size() * sizeof(ResJob), cudaMemcpyHostToDevice, ctx->stream));
+    c += b_jobs;
+    A.ops = (const DevOp*)c;
+    if (!ops.empty()) VCK(cudaMemcpyAsync(c, ops.data(), ops.size() * sizeof(DevOp), cudaMemcpyHostToDevice, ctx->stream));
+    c += b_ops;
+    A.terms = (const HamTerm*)c;
+    VCK(cudaMemcpyAsync(c, terms.data(), terms.size() * sizeof(HamTerm), cudaMemcpyHostToDevice, ctx->stream));
+    c += b_terms;
+    A.energy = (double*)c;
+    c += b_e;
+    A.cols = (double*)c;
+    VCK(cudaMemsetAsync(c, 0, (size_t)std::max(1, ncols) * 8, ctx->stream));
+    A.njobs = n;
+    const size_t amp = dtype == SMOQ_C64 ? 8 : 16;
+    const size_t smem = 2 * amp << nmax;
+    const void* fn = dtype == SMOQ_C64 ? (const void*)vqe_resident_kernel<float> : (const void*)vqe_resident_kernel<double>;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem) != cudaSuccess || per_sm < 1) {
+        (void)cudaGetLastError();
+        per_sm = 1;
+    }
+    const int grid = (int)std::min<int64_t>(n, (int64_t)ctx->num_sms * per_sm);
+    if (dtype == SMOQ_C64) vqe_resident_kernel<float><<<grid, 256, smem, ctx->stream>>>(A);
+    else vqe_resident_kernel<double><<<grid, 256, smem, ctx->stream>>>(A);
+    ctx->launches++;
+    VCK(cudaGetLastError());
+    std::vector<double> e(n), cols((size_t)std::max(1, ncols));
+    VCK(cudaMemcpyAsync(e.data(), A.energy, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    VCK(cudaMemcpyAsync(cols.data(), A.cols, cols.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    VCK(cudaStreamSynchronize(ctx->stream));
+    for (size_t u = 0; u < idx.size(); ++u) {
+        const smoq_vqe_job& J = jobs[idx[u]];
+        J.energy[0] = e[u];
+        if (!J.grad) continue;
+        for (int p = 0; p < J.n_params; ++p) J.grad[p] = 0.0;
+        for (size_t k = 0; k < inner_param[u].size(); ++k) J.grad[inner_param[u][k]] += cols[rj[u].col_off + k];
+    }
+    return SMOQ_OK;
 }
 
 // ---------------------------------------------------------------- many circuits
@@ -816,7 +1085,19 @@ extern "C" smoq_status smoq_energy_grad_jobs(smoq_ctx* ctx, smoq_dtype dtype, co
     if (njobs < 0 || (njobs > 0 && !jobs)) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "bad job list");
     for (int j = 0; j < njobs; ++j)
         if (!jobs[j].energy) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "job without energy output");
+    // circuits whose two states fit one CTA's shared memory: all in one launch
+    std::vector<int> small;
+    for (int j = 0; j < njobs; ++j)
+        if (ctx->vqe_resident && jobs[j].N >= 1 && jobs[j].N <= (dtype == SMOQ_C64 ? kResMaxN64 : kResMaxN128))
+            small.push_back(j);
+    if (!small.empty())
+        if (smoq_status s = run_resident(ctx, dtype, jobs, small)) return s;
+    size_t next_small = 0;
     for (int j = 0; j < njobs; ++j) {
+        if (next_small < small.size() && small[next_small] == j) {
+            ++next_small;
+            continue;
+        }
         const smoq_vqe_job& J = jobs[j];
         const smoq_status s = vqe_run(ctx, J.N, dtype, J.ops, J.n, J.n_params, J.H, J.nterms, 1, J.theta, J.energy,
                                       J.grad);

@@ -19,7 +19,7 @@ C64, C128 = 0, 1
  G_CRY, G_CCZ, G_TOFFOLI, G_U1, G_U2) = range(21)
 
 (OPT_TILE_BITS_C64, OPT_TILE_BITS_C128, OPT_LOW_BITS_C64, OPT_LOW_BITS_C128, OPT_USE_GRAPHS, OPT_KERNEL_TIMING,
- OPT_ENGINE, OPT_JIT_BUFFERS, OPT_JIT_PACKED, OPT_JIT_GROUPS, OPT_JIT_STAGE_BITS) = range(1, 12)
+ OPT_ENGINE, OPT_JIT_BUFFERS, OPT_JIT_PACKED, OPT_JIT_GROUPS, OPT_JIT_STAGE_BITS, OPT_VQE_RESIDENT) = range(1, 13)
 
 
 class SmoqOp(C.Structure):

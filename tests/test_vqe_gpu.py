@@ -180,3 +180,62 @@ def test_many_independent_circuits_vs_oracle(ctx):
     e64, g64 = S.energy_and_gradient_jobs(ctx, jobs, dtype=S.C64)
     for j, (er, gr) in enumerate(refs):
         assert abs(e64[j] - er) < 1e-4 and np.max(np.abs(g64[j] - gr)) < 1e-3
+
+
+def random_circuit(N, rng, n_gates=40):
+    """every parameterised type on random qubits (both orders) and fixed gates between"""
+    g = S.gate
+    ops, p = [], 1
+    for _ in range(n_gates):
+        kind = rng.integers(0, 5)
+        q1 = int(rng.integers(1, N + 1))
+        q2 = int(rng.choice([q for q in range(1, N + 1) if q != q1]))
+        if kind == 0:
+            ops.append(g(str(rng.choice(["rx", "ry", "rz"])), q1, param_idx=p)); p += 1
+        elif kind == 1:
+            ops.append(g(str(rng.choice(["rxx", "ryy", "rzz", "cry"])), [q1, q2], param_idx=p)); p += 1
+        elif kind == 2:
+            ops.append(g(str(rng.choice(["h", "s", "t", "x"])), q1))
+        elif kind == 3:
+            ops.append(g(str(rng.choice(["cnot", "cz"])), [q1, q2]))
+        else:   # a parameter shared by two gates
+            ops.append(g("ry", q1, param_idx=max(1, p - 1)))
+    return S.ParameterizedCircuit(N, ops)
+
+
+@pytest.mark.parametrize("dtype,tol", [(S.C128, 1e-11), (S.C64, 2e-5)])
+def test_jobs_in_one_launch_equal_the_tiled_path(built, dtype, tol):
+    """smoq_energy_grad_jobs runs circuits that fit one CTA's shared memory in one
+    launch; the same jobs with that path switched off (every circuit through the
+    tiled passes, one after another) give the same energies and gradients, and
+    a job list mixing both kinds keeps every job's outputs in place"""
+    rng = np.random.default_rng(21)
+    jobs, raw = [], []
+    for j in range(24):
+        N = [1, 2, 3, 5, 8, 11, 12, 13, 14][j % 9]
+        circ = random_circuit(N, rng, n_gates=int(rng.integers(1, 50))) if N > 1 else \
+            S.ParameterizedCircuit(1, [S.gate("rx", 1, param_idx=1), S.gate("ry", 1, param_idx=2)])
+        theta = rng.uniform(-3, 3, size=circ.n_params)
+        terms = [(float(rng.normal()), {int(q): str(rng.choice(["X", "Y", "Z"]))
+                                        for q in rng.choice(np.arange(1, N + 1), size=min(N, 2), replace=False)})
+                 for _ in range(3)]
+        jobs.append((circ, S.PauliSum(terms), theta))
+        raw.append(terms)
+    res = {}
+    for resident in (1, 0):
+        c = S.Context(0)
+        c.set_option(S._lib.OPT_VQE_RESIDENT, resident)
+        res[resident] = S.energy_and_gradient_jobs(c, jobs, dtype=dtype)
+        e_only, _ = S.energy_and_gradient_jobs(c, jobs, dtype=dtype, gradient=False)
+        assert np.max(np.abs(e_only - res[resident][0])) < tol
+        c.close()
+    (e1, g1), (e0, g0) = res[1], res[0]
+    assert np.max(np.abs(e1 - e0)) < tol
+    for a, b in zip(g1, g0):
+        assert a.shape == b.shape and (a.size == 0 or np.max(np.abs(a - b)) < tol)
+    # and one small job against the oracle's central differences
+    circ, H, theta = jobs[4]  # N = 8
+    oo = oracle_ops(circ)
+    arr = O.make_ops(oo)
+    fd = O.grad(arr, len(oo), theta, circ.N, raw[4], method="fd", eps=1e-5)
+    assert np.max(np.abs(g1[4] - fd)) < (1e-7 if dtype == S.C128 else 1e-4)
