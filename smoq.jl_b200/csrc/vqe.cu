@@ -23,12 +23,14 @@
 //    partials; adj_colsum_kernel reduces the rows.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <functional>
 #include <map>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 #include "smoq_internal.h"
 #include "k_common.cuh"
@@ -662,14 +664,20 @@ bool op_dense(const DevOp& op, cd* M) {
 
 // Fold a U^dag op that directly precedes a measurement on the same tile bits
 // into the measurement (INNER_PRE): one sweep of both tiles instead of two.
-smoq_status fuse_measurements(smoq_ctx* ctx, std::vector<DevOp>& ops) {
+smoq_status fuse_measurements(std::vector<DevOp>& ops, std::string& err) {
     for (const DevOp& op : ops) {
         const bool ok = op.kind == OPK_DENSE1 || op.kind == OPK_DENSE2 || op.kind == OPK_PARITY2 ||
                         op.kind == OPK_MONO || op.kind == OPK_DIAG || op.kind == OPK_INNER;
-        if (!ok) return smoq_internal_fail(ctx, SMOQ_ERR_UNSUPPORTED, "adjoint pass holds an unsupported op kind");
+        if (!ok) {
+            err = "adjoint pass holds an unsupported op kind";
+            return SMOQ_ERR_UNSUPPORTED;
+        }
         if (op.kind == OPK_INNER)
             for (int t = 0; t < op.nq; ++t)
-                if (op.lb[t] < 0) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "measurement qubit outside the tile");
+                if (op.lb[t] < 0) {
+                    err = "measurement qubit outside the tile";
+                    return SMOQ_ERR_BADINPUT;
+                }
     }
     std::vector<DevOp> out;
     out.reserve(ops.size());
@@ -759,9 +767,61 @@ static smoq_status forward_and_h(smoq_ctx* ctx, Work& w, const std::vector<GateI
     return SMOQ_OK;
 }
 
+// Host-only preparation of one parameter set: the gate IR and, for a gradient,
+// the backward program planned into fused tile passes.  Touches no context
+// state, so the many-circuit call prepares several circuits on host threads.
+struct GradPlan {
+    std::vector<GateIR> ir;
+    std::vector<Pass> passes;    // the backward passes, measurements fused
+    std::vector<int> inner_param;  // measurement -> parameter
+    smoq_status status = SMOQ_OK;
+    std::string error;
+};
+static void plan_gradient(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops, int n,
+                          const double* th, bool grad, GradPlan& gp) {
+    if ((gp.status = smoq_internal_ops_to_ir(N, ops, n, th, gp.ir))) {
+        gp.error = "bad op list";
+        return;
+    }
+    if (!grad) return;
+    // the backward program: for k = n-1 .. 0: [inner(G_k)] then U_k^dag
+    std::vector<GateIR> back;
+    back.reserve(2 * (size_t)n);
+    for (int k = n - 1; k >= 0; --k) {
+        if (ops[k].param >= 0) {
+            back.emplace_back();
+            GateIR& gi = back.back();
+            gi.nq = gp.ir[k].nq;
+            for (int t = 0; t < gi.nq; ++t) gi.q[t] = gp.ir[k].q[t];
+            if (!generator(ops[k].type, gi)) {
+                gp.status = SMOQ_ERR_UNSUPPORTED;
+                gp.error = "adjoint gradient: parameterised gate type has no generator";
+                return;
+            }
+            gi.special = OPK_INNER;
+            gi.aux2 = (int64_t)gp.inner_param.size();
+            gp.inner_param.push_back(ops[k].param);
+        }
+        back.emplace_back();
+        dagger_into(gp.ir[k], back.back());
+    }
+    if (gp.inner_param.empty()) return;
+    // tiles for two states in shared memory: one qubit narrower than the single-state passes
+    const int T = std::max(tile_bits - 1, 6);
+    try {
+        gp.passes = plan_passes(back, N, T, low_bits, -1, dtype == SMOQ_C64 ? 1 : 0);
+    } catch (const std::exception& ex) {
+        gp.status = SMOQ_ERR_BADINPUT;
+        gp.error = ex.what();
+        return;
+    }
+    for (Pass& p : gp.passes)
+        if ((gp.status = fuse_measurements(p.ops, gp.error))) return;
+}
+
 static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* ops, int n, int n_params,
                            const smoq_pauli_term* H, int nterms, int batch, const double* theta, double* energies,
-                           double* grads) {
+                           double* grads, GradPlan* pre = nullptr) {
     if (smoq_status s = check_vqe_args(ctx, N, dtype, ops, n, n_params, H, nterms, batch, theta)) return s;
     Work w;
     w.s = ctx->stream;
@@ -793,50 +853,26 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
 
     for (int b = 0; b < batch; ++b) {
         const double* th = theta ? theta + (size_t)b * n_params : nullptr;
-        std::vector<GateIR> ir;
-        if (smoq_status s = smoq_internal_ops_to_ir(N, ops, n, th, ir)) return smoq_internal_fail(ctx, s, "bad op list");
+        GradPlan own;
+        GradPlan& gp = (pre && batch == 1) ? *pre : own;
+        if (&gp == &own)
+            plan_gradient(N, dtype, smoq_internal_tile_bits(ctx, dtype), smoq_internal_low_bits(ctx, dtype), ops, n,
+                          th, grads != nullptr, gp);
+        if (gp.status) return smoq_internal_fail(ctx, gp.status, gp.error.c_str());
         double E = 0;
-        if (smoq_status s = forward_and_h(ctx, w, ir, ht, d_terms, d_epart, eblocks, &E)) return s;
+        if (smoq_status s = forward_and_h(ctx, w, gp.ir, ht, d_terms, d_epart, eblocks, &E)) return s;
         energies[b] = E;
         if (!grads) continue;
         double* g = grads + (size_t)b * n_params;
         for (int p = 0; p < n_params; ++p) g[p] = 0.0;
-
-        // the backward program: for k = n-1 .. 0: [inner(G_k)] then U_k^dag
-        std::vector<GateIR> back;
-        std::vector<int> inner_param;
-        back.reserve(2 * (size_t)n);
-        for (int k = n - 1; k >= 0; --k) {
-            if (ops[k].param >= 0) {
-                back.emplace_back();
-                GateIR& gi = back.back();
-                gi.nq = ir[k].nq;
-                for (int t = 0; t < gi.nq; ++t) gi.q[t] = ir[k].q[t];
-                if (!generator(ops[k].type, gi))
-                    return smoq_internal_fail(ctx, SMOQ_ERR_UNSUPPORTED,
-                                              "adjoint gradient: parameterised gate type has no generator");
-                gi.special = OPK_INNER;
-                gi.aux2 = (int64_t)inner_param.size();
-                inner_param.push_back(ops[k].param);
-            }
-            back.emplace_back();
-            dagger_into(ir[k], back.back());
-        }
-        if (inner_param.empty()) continue;
-        // tiles for two states in shared memory: one qubit narrower than the single-state passes
-        int T = std::max(smoq_internal_tile_bits(ctx, dtype) - 1, 6);
-        std::vector<Pass> passes;
-        try {
-            passes = plan_passes(back, N, T, smoq_internal_low_bits(ctx, dtype), -1, dtype == SMOQ_C64 ? 1 : 0);
-        } catch (const std::exception& ex) {
-            return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
-        }
+        if (gp.inner_param.empty()) continue;
+        const std::vector<int>& inner_param = gp.inner_param;
+        std::vector<Pass>& passes = gp.passes;
         std::vector<size_t> opoff(passes.size() + 1, 0);
         std::vector<int64_t> grid(passes.size(), 0);
         std::vector<DevOp> all;
         int64_t max_grid = 1;
         for (size_t i = 0; i < passes.size(); ++i) {
-            if (smoq_status s = fuse_measurements(ctx, passes[i].ops)) return s;
             opoff[i + 1] = opoff[i] + passes[i].ops.size();
             all.insert(all.end(), passes[i].ops.begin(), passes[i].ops.end());
             const size_t smem = (size_t)2 * w.phi.amp_bytes() << passes[i].g.T;
@@ -945,8 +981,9 @@ static smoq_status whole_state_ops(smoq_ctx* ctx, const std::vector<GateIR>& gat
         return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
     }
     for (Pass& p : passes) {
+        std::string err;
         if (backward)
-            if (smoq_status s = fuse_measurements(ctx, p.ops)) return s;
+            if (smoq_status s = fuse_measurements(p.ops, err)) return smoq_internal_fail(ctx, s, err.c_str());
         for (const DevOp& op : p.ops) {
             const bool kind_ok = op.kind == OPK_DENSE1 || op.kind == OPK_DENSE2 || op.kind == OPK_PARITY2 ||
                                  op.kind == OPK_MONO || op.kind == OPK_DIAG || (backward && op.kind == OPK_INNER);
@@ -1092,6 +1129,9 @@ extern "C" smoq_status smoq_energy_grad_jobs(smoq_ctx* ctx, smoq_dtype dtype, co
             small.push_back(j);
     if (!small.empty())
         if (smoq_status s = run_resident(ctx, dtype, jobs, small)) return s;
+    // the others: validated here, prepared on host threads a chunk at a time (the
+    // prepared gate IR takes 4 KB a gate), run on the GPU in submission order
+    std::vector<int> large;
     size_t next_small = 0;
     for (int j = 0; j < njobs; ++j) {
         if (next_small < small.size() && small[next_small] == j) {
@@ -1099,11 +1139,39 @@ extern "C" smoq_status smoq_energy_grad_jobs(smoq_ctx* ctx, smoq_dtype dtype, co
             continue;
         }
         const smoq_vqe_job& J = jobs[j];
-        const smoq_status s = vqe_run(ctx, J.N, dtype, J.ops, J.n, J.n_params, J.H, J.nterms, 1, J.theta, J.energy,
-                                      J.grad);
-        if (s != SMOQ_OK) {
+        if (smoq_status s = check_vqe_args(ctx, J.N, dtype, J.ops, J.n, J.n_params, J.H, J.nterms, 1, J.theta)) {
             const std::string why = "job " + std::to_string(j) + ": " + smoq_last_error(ctx);
             return smoq_internal_fail(ctx, s, why.c_str());
+        }
+        large.push_back(j);
+    }
+    const int tb = smoq_internal_tile_bits(ctx, dtype), lb = smoq_internal_low_bits(ctx, dtype);
+    // (half the host threads, at most 8: the planning is memory-bound on 4 KB gates)
+    const size_t nthreads = std::max<size_t>(1, std::min<size_t>(8, std::thread::hardware_concurrency() / 2));
+    const size_t chunk = 4 * nthreads;
+    for (size_t c0 = 0; c0 < large.size(); c0 += chunk) {
+        const size_t nc = std::min(chunk, large.size() - c0);
+        std::vector<GradPlan> plans(nc);
+        std::atomic<size_t> next(0);
+        auto work = [&]() {
+            for (size_t i; (i = next++) < nc;) {
+                const smoq_vqe_job& J = jobs[large[c0 + i]];
+                plan_gradient(J.N, dtype, tb, lb, J.ops, J.n, J.theta, J.grad != nullptr, plans[i]);
+            }
+        };
+        std::vector<std::thread> pool;
+        for (size_t t = 1; t < std::min(nthreads, nc); ++t) pool.emplace_back(work);
+        work();
+        for (std::thread& t : pool) t.join();
+        for (size_t i = 0; i < nc; ++i) {
+            const int j = large[c0 + i];
+            const smoq_vqe_job& J = jobs[j];
+            const smoq_status s = vqe_run(ctx, J.N, dtype, J.ops, J.n, J.n_params, J.H, J.nterms, 1, J.theta, J.energy,
+                                          J.grad, &plans[i]);
+            if (s != SMOQ_OK) {
+                const std::string why = "job " + std::to_string(j) + ": " + smoq_last_error(ctx);
+                return smoq_internal_fail(ctx, s, why.c_str());
+            }
         }
     }
     return SMOQ_OK;
