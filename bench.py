@@ -229,6 +229,8 @@ def vqe_workload(args):
     import torch
     import pysmoq as S
     ctx = S.Context(0)
+    if args.engine >= 0:
+        ctx.set_option(S._lib.OPT_ENGINE, args.engine)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
     N, L, B = 24, 12, 8
     ops, idx = [], 1
