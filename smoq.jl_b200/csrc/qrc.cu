@@ -59,13 +59,21 @@ struct QrcArgs {
     int32_t N, L, T, protocol;
 };
 
-constexpr int kQrcThreads = 256;
-// CTAs per SM the register budget is sized for (shared memory allows up to 6 at L = 6 complex64)
+// 128 threads per trajectory CTA (measured at L = 6: 143 ms against 157-171 ms with 256
+// threads and 205 ms with 512; 64 threads were no faster); the reset splits the
+// threads over the 2^L outcomes, so 2^L <= kQrcThreads (L <= 7)
+#ifndef SMOQ_QRC_THREADS
+#define SMOQ_QRC_THREADS 128
+#endif
+constexpr int kQrcThreads = SMOQ_QRC_THREADS;
+static_assert(kQrcThreads >= 128 && kQrcThreads % 32 == 0, "the reset needs 2^L <= threads for L <= 7");
+// CTAs per SM the register budget is sized for (64 and 128 registers a thread; shared
+// memory allows 6 at L = 6 complex64)
 #ifndef SMOQ_QRC_MINB_C64
-#define SMOQ_QRC_MINB_C64 4
+#define SMOQ_QRC_MINB_C64 8
 #endif
 #ifndef SMOQ_QRC_MINB_C128
-#define SMOQ_QRC_MINB_C128 2
+#define SMOQ_QRC_MINB_C128 4
 #endif
 
 // Bank swizzle of a trajectory's state in shared memory: amplitude j is stored
