@@ -193,9 +193,15 @@ static void encode_matrix(int nq, const cd* M, DevOp& op) {
         fill_coeffs(op, ph, dim);
         return;
     }
+    auto all_real = [&](int n) {
+        for (int k = 0; k < n; ++k)
+            if (M[k].imag() != 0.0) return false;
+        return true;
+    };
     if (nq == 1) {
         op.kind = OPK_DENSE1;
         fill_coeffs(op, M, 4);
+        op.flags = all_real(4) ? OPF_REAL : 0;
         return;
     }
     if (nq == 2) {
@@ -213,6 +219,7 @@ static void encode_matrix(int nq, const cd* M, DevOp& op) {
         }
         op.kind = OPK_DENSE2;
         fill_coeffs(op, M, 16);
+        op.flags = all_real(16) ? OPF_REAL : 0;
         return;
     }
     throw std::invalid_argument("3-qubit gates must be diagonal or monomial");

@@ -52,6 +52,9 @@ enum SlotType : int32_t { SLOT_LANE = 0, SLOT_REG = 1, SLOT_WARP = 2, SLOT_OFF =
 
 // OPK_INNER encoding details
 enum InnerBits : int32_t { INNER_ZERO = 4, INNER_DIAGG = 1, INNER_PRE = 2 };
+// OPK_DENSE1 / OPK_DENSE2 flag: every coefficient is real (Ry, CZ products): a
+// kernel may multiply with real scalars, half the FMAs of complex coefficients
+enum DenseBits : int32_t { OPF_REAL = 4 };
 
 struct alignas(16) DevOp {
     int32_t kind;

@@ -114,13 +114,64 @@ __device__ __forceinline__ uint32_t flip_bits(int s, int a, int b) {
     return ((s & 1) ? 1u << a : 0u) | ((s & 2) ? 1u << b : 0u);
 }
 
+// a x + b y for real a, b and complex x, y
+template <typename R, typename C>
+__device__ __forceinline__ C rmix(R a, C x, R b, C y) {
+    C z;
+    z.x = fma(a, x.x, b * y.x);
+    z.y = fma(a, x.y, b * y.y);
+    return z;
+}
+
 // U^dag op on both tiles; dco: 16 shared-memory slots for diagonal tables
 template <typename R>
 __device__ __forceinline__ void dual_apply(const DevOp& op, typename CT<R>::T* P, typename CT<R>::T* Q, int T,
                                            uint64_t base, typename CT<R>::T* dco) {
     using C = typename CT<R>::T;
     const uint32_t tid = threadIdx.x, nthr = blockDim.x;
-    if (op.kind == OPK_DENSE1) {
+    if (op.kind == OPK_DENSE1 && (op.flags & OPF_REAL)) {
+        // real 2x2 (Ry and its products): real scalars times complex amplitudes
+        const int a = op.lb[0];
+        const int f = lane_flip<R>(tid, a, -1);
+        const R m0 = coef<R>(op, 3 * f).x, m1 = coef<R>(op, 1 + f).x, m2 = coef<R>(op, 2 - f).x,
+                m3 = coef<R>(op, 3 - 3 * f).x;
+        for (uint32_t g = tid; g < (1u << (T - 1)); g += nthr) {
+            const uint32_t i0 = ins0<uint32_t>(g, a) ^ ((uint32_t)f << a), i1 = i0 ^ (1u << a);
+            const C x = P[i0], y = P[i1], u = Q[i0], v = Q[i1];
+            P[i0] = rmix(m0, x, m1, y);
+            P[i1] = rmix(m2, x, m3, y);
+            Q[i0] = rmix(m0, u, m1, v);
+            Q[i1] = rmix(m2, u, m3, v);
+        }
+    } else if (op.kind == OPK_DENSE2 && (op.flags & OPF_REAL)) {
+        const int a = op.lb[0], b = op.lb[1];
+        const int lo = a < b ? a : b, hi = a < b ? b : a;
+        const int f = lane_flip<R>(tid, a, b);
+        const uint32_t fb = flip_bits(f, a, b);
+        R m[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) m[k] = coef<R>(op, (((k >> 2) ^ f) << 2) | ((k & 3) ^ f)).x;
+        for (uint32_t g = tid; g < (1u << (T - 2)); g += nthr) {
+            const uint32_t i0 = ins0<uint32_t>(ins0<uint32_t>(g, lo), hi) ^ fb;
+            const uint32_t ix[4] = {i0, i0 ^ (1u << a), i0 ^ (1u << b), i0 ^ (1u << a) ^ (1u << b)};
+            C x[4], y[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) x[k] = P[ix[k]], y[k] = Q[ix[k]];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                C s, t;
+                s.x = m[4 * r] * x[0].x, s.y = m[4 * r] * x[0].y;
+                t.x = m[4 * r] * y[0].x, t.y = m[4 * r] * y[0].y;
+#pragma unroll
+                for (int c = 1; c < 4; ++c) {
+                    s.x = fma(m[4 * r + c], x[c].x, s.x), s.y = fma(m[4 * r + c], x[c].y, s.y);
+                    t.x = fma(m[4 * r + c], y[c].x, t.x), t.y = fma(m[4 * r + c], y[c].y, t.y);
+                }
+                P[ix[r]] = s;
+                Q[ix[r]] = t;
+            }
+        }
+    } else if (op.kind == OPK_DENSE1) {
         const int a = op.lb[0];
         const int f = lane_flip<R>(tid, a, -1);  // 0 or 1: M' = M with both indices flipped
         const C m0 = coef<R>(op, 3 * f), m1 = coef<R>(op, 1 + f), m2 = coef<R>(op, 2 - f), m3 = coef<R>(op, 3 - 3 * f);
