@@ -42,7 +42,8 @@ enum OpKind : int32_t {
                       // partials column perm[0]; G is a signed monomial: row r holds i^slot[r]
                       // at column perm[1 + r] (slot[r] = INNER_ZERO: an all-zero row);
                       // flags: INNER_DIAGG (G real diagonal), INNER_PRE (cd/cf hold a dense
-                      // 2^nq x 2^nq matrix applied to both states first)
+                      // 2^nq x 2^nq matrix applied to both states first), INNER_PREDIAG
+                      // (that matrix is diagonal)
     OPK_LAYOUT = 8,   // register-tile layout change: perm[0..KR-1] = register bits,
                       // perm[5..7] = warp bits (tile-local bit positions)
 };
@@ -51,7 +52,7 @@ enum OpKind : int32_t {
 enum SlotType : int32_t { SLOT_LANE = 0, SLOT_REG = 1, SLOT_WARP = 2, SLOT_OFF = 3 };
 
 // OPK_INNER encoding details
-enum InnerBits : int32_t { INNER_ZERO = 4, INNER_DIAGG = 1, INNER_PRE = 2 };
+enum InnerBits : int32_t { INNER_ZERO = 4, INNER_DIAGG = 1, INNER_PRE = 2, INNER_PREDIAG = 8 };
 // OPK_DENSE1 / OPK_DENSE2 flag: every coefficient is real (Ry, CZ products): a
 // kernel may multiply with real scalars, half the FMAs of complex coefficients
 enum DenseBits : int32_t { OPF_REAL = 4 };

@@ -278,7 +278,7 @@ __device__ __forceinline__ C pick4(const C* v, int c) {
 // this thread's share of Im<lambda|G|phi> over the tile pair, G a signed
 // monomial on 1 or 2 tile bits; PRE: the op's dense matrix is applied to both
 // tiles first (and written back)
-template <typename R, int NQ, bool PRE>
+template <typename R, int NQ, bool PRE, bool PREDIAG = false>
 __device__ __forceinline__ R inner_pairs(const DevOp& op, typename CT<R>::T* P, typename CT<R>::T* Q, int T) {
     using C = typename CT<R>::T;
     constexpr int D = 1 << NQ;
@@ -315,6 +315,11 @@ __device__ __forceinline__ R inner_pairs(const DevOp& op, typename CT<R>::T* P, 
             C x[D], y[D];
 #pragma unroll
             for (int r = 0; r < D; ++r) {
+                if (PREDIAG) {  // (a phase per member: the off-diagonal products are zero)
+                    x[r] = cmul(m[r * D + r], p[r]);
+                    y[r] = cmul(m[r * D + r], l[r]);
+                    continue;
+                }
                 x[r] = cmul(m[r * D], p[0]);
                 y[r] = cmul(m[r * D], l[0]);
 #pragma unroll
@@ -409,10 +414,14 @@ __device__ __forceinline__ void adj_program(const DevOp* ops, int nops, typename
             o += k;
             writes = false;
         } else if (op.kind == OPK_INNER) {
-            const bool pre = op.flags & INNER_PRE;
+            const bool pre = op.flags & INNER_PRE, pd = op.flags & INNER_PREDIAG;
             R acc;
-            if (op.nq == 1) acc = pre ? inner_pairs<R, 1, true>(op, tP, tL, T) : inner_pairs<R, 1, false>(op, tP, tL, T);
-            else acc = pre ? inner_pairs<R, 2, true>(op, tP, tL, T) : inner_pairs<R, 2, false>(op, tP, tL, T);
+            if (op.nq == 1)
+                acc = !pre ? inner_pairs<R, 1, false>(op, tP, tL, T)
+                           : pd ? inner_pairs<R, 1, true, true>(op, tP, tL, T) : inner_pairs<R, 1, true>(op, tP, tL, T);
+            else
+                acc = !pre ? inner_pairs<R, 2, false>(op, tP, tL, T)
+                           : pd ? inner_pairs<R, 2, true, true>(op, tP, tL, T) : inner_pairs<R, 2, true>(op, tP, tL, T);
             flush(acc, op.perm[0]);
             writes = pre;
             ++o;
@@ -749,7 +758,11 @@ smoq_status fuse_measurements(std::vector<DevOp>& ops, std::string& err) {
                         m.cd[r * dim + c] = make_double2(x.real(), x.imag());
                         m.cf[r * dim + c] = make_float2((float)x.real(), (float)x.imag());
                     }
-                m.flags = INNER_PRE;
+                bool diag = true;
+                for (int r = 0; r < dim; ++r)
+                    for (int c = 0; c < dim; ++c)
+                        if (r != c && std::abs(M[r * dim + c]) != 0.0) diag = false;
+                m.flags = INNER_PRE | (diag ? INNER_PREDIAG : 0);
                 out.push_back(m);
                 ++i;
                 continue;
