@@ -213,6 +213,118 @@ __device__ __forceinline__ void sweep_op(const DevOp& op, typename CT<R>::T* psi
     }
 }
 
+// Bank spreading.  A shared-memory phase of 16 (complex64) or 8 (complex128)
+// lanes covers one 128-byte row; a sweep over an op on bits inside that row
+// has every phase hit each bank twice (one such bit) or four times (two).  The
+// lanes whose group index has the bits just above the row's free bits set read
+// their group with the op's low bits flipped: flip pattern s in the op's
+// matrix index space (bit 0 = qubit 0, bit 1 = qubit 1), group member k at
+// logical member k ^ s, matrix M'[k][j] = M[k ^ s][j ^ s].  s is fixed per
+// thread (groups stride by blockDim, a multiple of 16).
+template <typename R>
+__device__ __forceinline__ int lane_flip(uint32_t tid, int a, int b) {
+    constexpr int B = sizeof(R) == 4 ? 4 : 3;  // amplitude bits of one 128-byte row
+    const bool la = a < B, lb = b >= 0 && b < B;
+    if (la && lb) {
+        const int f = (int)(tid >> (B - 2)) & 3;  // bit 0 flips the lower of the two positions
+        return a < b ? f : ((f & 1) << 1) | (f >> 1);
+    }
+    if (la) return (int)(tid >> (B - 1)) & 1;
+    if (lb) return ((int)(tid >> (B - 1)) & 1) << 1;
+    return 0;
+}
+__device__ __forceinline__ uint32_t flip_bits(int s, int a, int b) {
+    return ((s & 1) ? 1u << a : 0u) | ((s & 2) ? 1u << b : 0u);
+}
+
+// a x + b y for real a, b and complex x, y
+template <typename R, typename C>
+__device__ __forceinline__ C rmix(R a, C x, R b, C y) {
+    C z;
+    z.x = fma(a, x.x, b * y.x);
+    z.y = fma(a, x.y, b * y.y);
+    return z;
+}
+
+// The same op on a linear shared-memory tile with bank spreading (lane_flip);
+// dense ops with real coefficients (OPF_REAL) multiply by real scalars.
+template <typename R>
+__device__ __forceinline__ void sweep_op_spread(const DevOp& op, typename CT<R>::T* psi, int T, uint32_t tid,
+                                                uint32_t nthr) {
+    using C = typename CT<R>::T;
+    constexpr int B = sizeof(R) == 4 ? 4 : 3;  // amplitude bits of one 128-byte bank row
+    const bool low = (op.kind == OPK_DENSE1 || op.kind == OPK_DENSE2 || op.kind == OPK_PARITY2) &&
+                     (op.lb[0] < B || (op.kind != OPK_DENSE1 && op.lb[1] < B));
+    if (!low) {  // no member bit inside a bank row: nothing to spread, coefficients stay uniform
+        sweep_op<R, uint32_t>(op, psi, T, op.lb, tid, nthr);
+        return;
+    }
+    if (op.kind == OPK_DENSE1) {
+        const int a = op.lb[0];
+        const int f = lane_flip<R>(tid, a, -1);
+        const C c0 = coef<R>(op, 0), c1 = coef<R>(op, 1), c2 = coef<R>(op, 2), c3 = coef<R>(op, 3);
+        const C m0 = f ? c3 : c0, m1 = f ? c2 : c1, m2 = f ? c1 : c2, m3 = f ? c0 : c3;
+        const bool real = op.flags & OPF_REAL;
+        for (uint32_t g = tid; g < (1u << (T - 1)); g += nthr) {
+            const uint32_t i0 = ins0<uint32_t>(g, a) ^ ((uint32_t)f << a), i1 = i0 ^ (1u << a);
+            const C x = psi[i0], y = psi[i1];
+            if (real) {
+                psi[i0] = rmix(m0.x, x, m1.x, y);
+                psi[i1] = rmix(m2.x, x, m3.x, y);
+            } else {
+                psi[i0] = cfma(m0, x, cmul(m1, y));
+                psi[i1] = cfma(m2, x, cmul(m3, y));
+            }
+        }
+    } else if (op.kind == OPK_DENSE2) {
+        const int a = op.lb[0], b = op.lb[1];
+        const int lo = a < b ? a : b, hi = a < b ? b : a;
+        const int f = lane_flip<R>(tid, a, b);
+        const uint32_t fb = flip_bits(f, a, b);
+        C m[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) m[k] = coef<R>(op, (((k >> 2) ^ f) << 2) | ((k & 3) ^ f));
+        for (uint32_t g = tid; g < (1u << (T - 2)); g += nthr) {
+            const uint32_t i0 = ins0<uint32_t>(ins0<uint32_t>(g, lo), hi) ^ fb;
+            const uint32_t ix[4] = {i0, i0 ^ (1u << a), i0 ^ (1u << b), i0 ^ (1u << a) ^ (1u << b)};
+            C v[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) v[k] = psi[ix[k]];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                C acc = cmul(m[4 * r], v[0]);
+                acc = cfma(m[4 * r + 1], v[1], acc);
+                acc = cfma(m[4 * r + 2], v[2], acc);
+                acc = cfma(m[4 * r + 3], v[3], acc);
+                psi[ix[r]] = acc;
+            }
+        }
+    } else if (op.kind == OPK_PARITY2) {
+        const int a = op.lb[0], b = op.lb[1];
+        const int lo = a < b ? a : b, hi = a < b ? b : a;
+        // flipped members: s = 1, 2 exchange the even and odd blocks, s = 2, 3 reverse each block
+        const int f = lane_flip<R>(tid, a, b);
+        const uint32_t fb = flip_bits(f, a, b);
+        const int eb = (f == 1 || f == 2) ? 4 : 0, ob = 4 - eb;
+        const bool rv = f >= 2;
+        const C e0 = coef<R>(op, eb + (rv ? 3 : 0)), e1 = coef<R>(op, eb + (rv ? 2 : 1));
+        const C e2 = coef<R>(op, eb + (rv ? 1 : 2)), e3 = coef<R>(op, eb + (rv ? 0 : 3));
+        const C o0 = coef<R>(op, ob + (rv ? 3 : 0)), o1 = coef<R>(op, ob + (rv ? 2 : 1));
+        const C o2 = coef<R>(op, ob + (rv ? 1 : 2)), o3 = coef<R>(op, ob + (rv ? 0 : 3));
+        for (uint32_t g = tid; g < (1u << (T - 2)); g += nthr) {
+            const uint32_t i0 = ins0<uint32_t>(ins0<uint32_t>(g, lo), hi) ^ fb;
+            const uint32_t i1 = i0 ^ (1u << a), i2 = i0 ^ (1u << b), i3 = i1 ^ (1u << b);
+            const C v0 = psi[i0], v1 = psi[i1], v2 = psi[i2], v3 = psi[i3];
+            psi[i0] = cfma(e0, v0, cmul(e1, v3));
+            psi[i3] = cfma(e2, v0, cmul(e3, v3));
+            psi[i1] = cfma(o0, v1, cmul(o1, v2));
+            psi[i2] = cfma(o2, v1, cmul(o3, v2));
+        }
+    } else {
+        sweep_op<R, uint32_t>(op, psi, T, op.lb, tid, nthr);
+    }
+}
+
 // ------------------------------------------------------- tile bulk loads
 // first global index of tile t and the state it belongs to
 __device__ __forceinline__ uint64_t tile_base(const TileArgs& a, int64_t t, int64_t& b) {

@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(TILE_THREADS) tile_pass_kernel(const TileArgs 
             } else if (kind == OPK_REALTAB) {
                 tile_realtab<R>(op, tile, a.g, base);
             } else {
-                sweep_op<R, uint32_t>(op, tile, T, op.lb, (uint32_t)tid, (uint32_t)blockDim.x);
+                sweep_op_spread<R>(op, tile, T, (uint32_t)tid, (uint32_t)blockDim.x);
             }
             __syncthreads();
         }

@@ -90,39 +90,6 @@ __global__ void __launch_bounds__(256) ham_apply_kernel(const typename CT<R>::T*
 // (lambda), 2^T amplitudes each, and applies every U^dag op to both in the
 // same loop iteration (one index decode, one coefficient load for both).
 
-// Bank spreading.  A shared-memory phase of 16 (complex64) or 8 (complex128)
-// lanes covers one 128-byte row; a sweep over an op on bits inside that row
-// has every phase hit each bank twice (one such bit) or four times (two).  The
-// lanes whose group index has the bits just above the row's free bits set read
-// their group with the op's low bits flipped: flip pattern s in the op's
-// matrix index space (bit 0 = qubit 0, bit 1 = qubit 1), group member k at
-// logical member k ^ s, matrix M'[k][j] = M[k ^ s][j ^ s].  s is fixed per
-// thread (groups stride by blockDim, a multiple of 16).
-template <typename R>
-__device__ __forceinline__ int lane_flip(uint32_t tid, int a, int b) {
-    constexpr int B = sizeof(R) == 4 ? 4 : 3;  // amplitude bits of one 128-byte row
-    const bool la = a < B, lb = b >= 0 && b < B;
-    if (la && lb) {
-        const int f = (int)(tid >> (B - 2)) & 3;  // bit 0 flips the lower of the two positions
-        return a < b ? f : ((f & 1) << 1) | (f >> 1);
-    }
-    if (la) return (int)(tid >> (B - 1)) & 1;
-    if (lb) return ((int)(tid >> (B - 1)) & 1) << 1;
-    return 0;
-}
-__device__ __forceinline__ uint32_t flip_bits(int s, int a, int b) {
-    return ((s & 1) ? 1u << a : 0u) | ((s & 2) ? 1u << b : 0u);
-}
-
-// a x + b y for real a, b and complex x, y
-template <typename R, typename C>
-__device__ __forceinline__ C rmix(R a, C x, R b, C y) {
-    C z;
-    z.x = fma(a, x.x, b * y.x);
-    z.y = fma(a, x.y, b * y.y);
-    return z;
-}
-
 // U^dag op on both tiles; dco: 16 shared-memory slots for diagonal tables
 template <typename R>
 __device__ __forceinline__ void dual_apply(const DevOp& op, typename CT<R>::T* P, typename CT<R>::T* Q, int T,
@@ -549,7 +516,7 @@ __device__ __forceinline__ void res_apply(const DevOp& op, typename CT<R>::T* ps
             psi[j] = cmul(dco[m], psi[j]);
         }
     } else {
-        sweep_op<R, uint32_t>(op, psi, N, op.lb, tid, nthr);
+        sweep_op_spread<R>(op, psi, N, tid, nthr);
     }
 }
 
