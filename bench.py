@@ -22,6 +22,7 @@ import math
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -97,8 +98,10 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv") \
-            if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else f"/tmp/smoq_clocks_{os.getpid()}.csv"
+        # the raw samples go to $SMOQ_CLOCKS_DIR when set (kept as evidence), else to a temp file
+        d = os.environ.get("SMOQ_CLOCKS_DIR")
+        self.path = os.path.join(d, f"clocks_rank{device}.csv") if d and os.path.isdir(d) else \
+            os.path.join(tempfile.gettempdir(), f"smoq_clocks_{os.getpid()}_{device}.csv")
 
     def start(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
