@@ -882,13 +882,32 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
     VCK(cudaMallocAsync((void**)&d_epart, eblocks * sizeof(double), ctx->stream));
     w.owned.push_back(d_epart);
 
+    // the next parameter set is prepared on a host thread while this one runs
+    const int tb = smoq_internal_tile_bits(ctx, dtype), lbits = smoq_internal_low_bits(ctx, dtype);
+    auto theta_of = [&](int b) { return theta ? theta + (size_t)b * n_params : nullptr; };
+    std::unique_ptr<GradPlan> cur(new GradPlan), nxt;
+    std::thread ahead;
+    struct Joiner {
+        std::thread& t;
+        ~Joiner() {
+            if (t.joinable()) t.join();
+        }
+    } joiner{ahead};
+    const bool use_pre = pre && batch == 1;
+    if (!use_pre) plan_gradient(N, dtype, tb, lbits, ops, n, theta_of(0), grads != nullptr, *cur);
     for (int b = 0; b < batch; ++b) {
-        const double* th = theta ? theta + (size_t)b * n_params : nullptr;
-        GradPlan own;
-        GradPlan& gp = (pre && batch == 1) ? *pre : own;
-        if (&gp == &own)
-            plan_gradient(N, dtype, smoq_internal_tile_bits(ctx, dtype), smoq_internal_low_bits(ctx, dtype), ops, n,
-                          th, grads != nullptr, gp);
+        if (b > 0) {
+            ahead.join();
+            cur.swap(nxt);
+        }
+        if (b + 1 < batch) {
+            nxt.reset(new GradPlan);
+            GradPlan* np = nxt.get();
+            const double* th1 = theta_of(b + 1);
+            const bool want_grad = grads != nullptr;
+            ahead = std::thread([=]() { plan_gradient(N, dtype, tb, lbits, ops, n, th1, want_grad, *np); });
+        }
+        GradPlan& gp = use_pre ? *pre : *cur;
         if (gp.status) return smoq_internal_fail(ctx, gp.status, gp.error.c_str());
         double E = 0;
         if (smoq_status s = forward_and_h(ctx, w, gp.ir, ht, d_terms, d_epart, eblocks, &E)) return s;
