@@ -798,6 +798,33 @@ static smoq_status forward_and_h(smoq_ctx* ctx, Work& w, const std::vector<GateI
     return SMOQ_OK;
 }
 
+// The backward program of a circuit: for k = n-1 .. 0, [the measurement of
+// G_k when gate k is parameterised] then U_k^dag.  inner_param[m] = the
+// parameter of measurement m.  False (with err) for a parameterised gate type
+// that has no generator.
+static bool build_backward(const std::vector<GateIR>& ir, const smoq_op* ops, int n, std::vector<GateIR>& back,
+                           std::vector<int>& inner_param, std::string& err) {
+    back.reserve(2 * (size_t)n);
+    for (int k = n - 1; k >= 0; --k) {
+        if (ops[k].param >= 0) {
+            back.emplace_back();
+            GateIR& gi = back.back();
+            gi.nq = ir[k].nq;
+            for (int t = 0; t < gi.nq; ++t) gi.q[t] = ir[k].q[t];
+            if (!generator(ops[k].type, gi)) {
+                err = "adjoint gradient: parameterised gate type has no generator";
+                return false;
+            }
+            gi.special = OPK_INNER;
+            gi.aux2 = (int64_t)inner_param.size();
+            inner_param.push_back(ops[k].param);
+        }
+        back.emplace_back();
+        dagger_into(ir[k], back.back());
+    }
+    return true;
+}
+
 // Host-only preparation of one parameter set: the gate IR and, for a gradient,
 // the backward program planned into fused tile passes.  Touches no context
 // state, so the many-circuit call prepares several circuits on host threads.
@@ -815,26 +842,10 @@ static void plan_gradient(int N, smoq_dtype dtype, int tile_bits, int low_bits, 
         return;
     }
     if (!grad) return;
-    // the backward program: for k = n-1 .. 0: [inner(G_k)] then U_k^dag
     std::vector<GateIR> back;
-    back.reserve(2 * (size_t)n);
-    for (int k = n - 1; k >= 0; --k) {
-        if (ops[k].param >= 0) {
-            back.emplace_back();
-            GateIR& gi = back.back();
-            gi.nq = gp.ir[k].nq;
-            for (int t = 0; t < gi.nq; ++t) gi.q[t] = gp.ir[k].q[t];
-            if (!generator(ops[k].type, gi)) {
-                gp.status = SMOQ_ERR_UNSUPPORTED;
-                gp.error = "adjoint gradient: parameterised gate type has no generator";
-                return;
-            }
-            gi.special = OPK_INNER;
-            gi.aux2 = (int64_t)gp.inner_param.size();
-            gp.inner_param.push_back(ops[k].param);
-        }
-        back.emplace_back();
-        dagger_into(gp.ir[k], back.back());
+    if (!build_backward(gp.ir, ops, n, back, gp.inner_param, gp.error)) {
+        gp.status = SMOQ_ERR_UNSUPPORTED;
+        return;
     }
     if (gp.inner_param.empty()) return;
     // tiles for two states in shared memory: one qubit narrower than the single-state passes
@@ -1074,25 +1085,10 @@ static smoq_status run_resident(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vqe_
         r.fwd_n = (int32_t)ops.size() - r.fwd_off;
         r.bwd_off = (int32_t)ops.size();
         if (J.grad) {
-            // the backward program, as vqe_run builds it
             std::vector<GateIR> back;
-            back.reserve(2 * (size_t)J.n);
-            for (int k = J.n - 1; k >= 0; --k) {
-                if (J.ops[k].param >= 0) {
-                    back.emplace_back();
-                    GateIR& gi = back.back();
-                    gi.nq = ir[k].nq;
-                    for (int t = 0; t < gi.nq; ++t) gi.q[t] = ir[k].q[t];
-                    if (!generator(J.ops[k].type, gi))
-                        return job_fail(smoq_internal_fail(ctx, SMOQ_ERR_UNSUPPORTED,
-                                                           "adjoint gradient: parameterised gate type has no generator"));
-                    gi.special = OPK_INNER;
-                    gi.aux2 = (int64_t)inner_param[u].size();
-                    inner_param[u].push_back(J.ops[k].param);
-                }
-                back.emplace_back();
-                dagger_into(ir[k], back.back());
-            }
+            std::string err;
+            if (!build_backward(ir, J.ops, J.n, back, inner_param[u], err))
+                return job_fail(smoq_internal_fail(ctx, SMOQ_ERR_UNSUPPORTED, err.c_str()));
             if (!inner_param[u].empty())
                 if (smoq_status s = whole_state_ops(ctx, back, J.N, dtype, true, ops)) return job_fail(s);
         }
