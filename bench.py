@@ -192,6 +192,17 @@ def cpu_baseline_sample(n_gates=12, N=N_QUBITS):
     return len(sample) / dt, dt
 
 
+def cpu_model():
+    """the host CPU's model name (for the CPU baseline's record)"""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip() + f" ({os.cpu_count()} logical cores)"
+    except OSError:
+        pass
+    return None
+
+
 def reference_arm(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -210,7 +221,7 @@ def reference_arm(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "config": {"workload": WORKLOAD, "N": N_QUBITS, "dtype_reference": "complex128",
                        "sample": f"first {n_gates} gates of one Strang step at N=28 per step"},
-            "cpu_baseline": {"value": v, "unit": "gate-apps/s", "cores": 1, "kind": "port",
+            "cpu_baseline": {"value": v, "unit": "gate-apps/s", "cores": 1, "kind": "port", "cpu_model": cpu_model(),
                              "sample": f"{n_gates} of the 218 gate applications of one step at N=28, complex128, "
                                        "single thread (the reference's kernels are single-threaded per state)"},
             "e2e": {"value": v, "unit": "gate-apps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -223,19 +234,19 @@ def _events(torch, stream):
     return e0, e1
 
 
-def vqe_workload(args):
+def vqe_measure(ctx, steps, warmup, B=8):
     """VQE gradient throughput on the gradient configuration: TFIM N=24, 12 layers of
     [Ry all; Rz all; CZ ladder] (852 gates, 576 parameters).  Batched complex64
-    adjoint gradients against the plain complex128 path (one kernel per gate,
-    per-term reductions, parameter-shift gradient); the plain path is timed on
-    one parameter's two shifted energies and scaled to 576 parameters."""
+    adjoint gradients (B parameter sets per call) against the complex128 adjoint
+    and the plain complex128 path (one kernel per gate, one reduction per
+    Hamiltonian term, parameter-shift gradient: 2 x 576 energies per gradient);
+    the plain path is timed on one parameter's two shifted energies and scaled to
+    576 parameters.  Energy error: complex64 against complex128 of the same
+    parameters."""
     import torch
     import pysmoq as S
-    ctx = S.Context(0)
-    if args.engine >= 0:
-        ctx.set_option(S._lib.OPT_ENGINE, args.engine)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
-    N, L, B = 24, 12, 8
+    N, L = 24, 12
     ops, idx = [], 1
     for _ in range(L):
         rot, idx = S.single_qubit_rotation_layer(N, idx, gates=("ry", "rz"))
@@ -246,16 +257,16 @@ def vqe_workload(args):
     H = S.PauliSum.tfim(N)
     res = {}
     for name, dt in (("c64", S.C64), ("c128", S.C128)):
-        for _ in range(max(1, args.warmup)):
+        for _ in range(max(1, warmup)):
             S.energy_and_gradient(ctx, circ, H, thetas[:1], dtype=dt)
         e0, e1 = _events(torch, stream)
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             E, G = S.energy_and_gradient(ctx, circ, H, thetas, dtype=dt)
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1)
-        res[name] = (B * args.steps / (ms * 1e-3), E, G)
+        res[name] = (B * steps / (ms * 1e-3), E, G)
 
     def plain_energy(theta):
         st = S.CuState(ctx, N, S.C128, basis=0)
@@ -278,19 +289,33 @@ def vqe_workload(args):
     pair_ms = e0.elapsed_time(e1)
     plain_gps = 1.0 / (P * pair_ms * 1e-3)
     ps0 = (ep - em) / 2
-    err_e = float(np.max(np.abs(res["c64"][1] - res["c128"][1])))
-    err_g = float(np.max(np.abs(res["c64"][2] - res["c128"][2])))
-    line = {"metric": "vqe_gradients_per_s", "value": res["c64"][0], "unit": "gradients/s", "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * B / res["c64"][0],
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
-            "config": {"workload": "vqe_tfim_n24_hea12_576params", "N": N, "layers": L, "params": P,
-                       "gates": len(ops), "batch": B, "gradient": "adjoint"},
+    return {"workload": "vqe_tfim_n24_hea12_576params", "N": N, "layers": L, "params": P, "gates": len(ops),
+            "batch": B, "calls": steps, "gradient": "adjoint",
+            "c64_adjoint_gradients_per_s": res["c64"][0],
             "c128_adjoint_gradients_per_s": res["c128"][0],
             "plain_c128_ps_gradients_per_s": plain_gps,
-            "plain_c128_sample": "two shifted energies of one parameter, one kernel per gate; scaled to 576 parameters",
-            "speedup_c64_adjoint_vs_plain_c128": res["c64"][0] / plain_gps,
-            "energy_abs_err_c64_vs_c128": err_e, "grad_max_abs_err_c64_vs_c128": err_g,
-            "plain_ps_vs_adjoint_param0": abs(ps0 - res["c128"][2][0, 0])}
+            "plain_c128_sample": "two shifted energies of one parameter, one kernel per gate and one reduction per "
+                                 "term; scaled to 576 parameters",
+            "speedup_c64_adjoint_vs_plain_c128_ps": res["c64"][0] / plain_gps,
+            "speedup_c64_adjoint_vs_c128_adjoint": res["c64"][0] / res["c128"][0],
+            "energy_abs_err_c64_vs_c128": float(np.max(np.abs(res["c64"][1] - res["c128"][1]))),
+            "grad_max_abs_err_c64_vs_c128": float(np.max(np.abs(res["c64"][2] - res["c128"][2]))),
+            "plain_ps_vs_adjoint_param0": float(abs(ps0 - res["c128"][2][0, 0]))}
+
+
+def vqe_workload(args):
+    """the VQE gradient figures as their own line (see vqe_measure)"""
+    import pysmoq as S
+    ctx = S.Context(0)
+    if args.engine >= 0:
+        ctx.set_option(S._lib.OPT_ENGINE, args.engine)
+    r = vqe_measure(ctx, args.steps, args.warmup)
+    line = {"metric": "vqe_gradients_per_s", "value": r["c64_adjoint_gradients_per_s"], "unit": "gradients/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * r["batch"] / r["c64_adjoint_gradients_per_s"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {k: r[k] for k in ("workload", "N", "layers", "params", "gates", "batch", "gradient")}}
+    line.update({k: v for k, v in r.items() if k not in line["config"]})
     print(json.dumps(line))
     ctx.close()
     return 0
@@ -535,6 +560,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-vqe", action="store_true", help="skip the VQE gradient sub-record of the default line")
     # smaller cases of the same kernel (profiling, sweeps); the defaults are the workload
     ap.add_argument("--n-qubits", type=int, default=N_QUBITS)
     ap.add_argument("--trotter-steps", type=int, default=STEPS)
@@ -679,7 +705,14 @@ def main():
         r, t = cpu_baseline_sample(12)
         cpu = {"value": r, "unit": "gate-apps/s", "cores": 1, "kind": "port",
                "sample": f"first 12 of the 218 gate applications of one Strang step at N=28, complex128, "
-                         f"single thread, {t:.1f} s (oracle restating the reference's loops)"}
+                         f"single thread, {t:.1f} s (oracle restating the reference's loops)",
+               "cpu_model": cpu_model()}
+
+    # the gradient figures of the metric's second half (VQE gradients/s, complex64
+    # adjoint against the plain complex128 path, energy error), every rank
+    vqe = None
+    if not args.no_vqe and N == N_QUBITS:
+        vqe = vqe_measure(ctx, steps=2, warmup=1)
 
     if rank == 0:
         line = {"metric": "gate_apps_per_s", "value": value, "unit": "gate-apps/s", "n_gpus": ws,
@@ -701,7 +734,8 @@ def main():
                 "e2e": {"value": e2e_value, "unit": "gate-apps/s", "h2d_bytes_per_step": int(hp.nbytes),
                         "d2h_bytes_per_step": int(8 * N * (tsteps // RECORD_EVERY + 1))},
                 "gpu_launches": int(launches),
-                "clocks": clk}
+                "clocks": clk,
+                "vqe": vqe}
         print(json.dumps(line))
     st.close()
     plan.close()

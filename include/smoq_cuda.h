@@ -101,6 +101,10 @@ void* smoq_state_device_ptr(smoq_state* st);
 /* host <-> device copies of the whole batch in the state's own dtype */
 smoq_status smoq_state_upload(smoq_state* st, const void* host, size_t bytes);
 smoq_status smoq_state_download(smoq_state* st, void* host, size_t bytes);
+/* amplitudes [first, first + count) of the batch (state-major: state b starts at
+ * b * 2^N) into host memory: a window of a state too large to copy whole,
+ * like reading ψ[first+1 : first+count] of the reference's Vector{ComplexF64} */
+smoq_status smoq_state_download_range(smoq_state* st, uint64_t first, uint64_t count, void* host);
 /* make_initial_psi (utils/cpu/cpuQuantumStatePreparation.jl:1211): every
  * state of the batch becomes the basis state |index> */
 smoq_status smoq_state_set_basis(smoq_state* st, uint64_t index);
@@ -149,11 +153,36 @@ enum {
     SMOQ_G_SDG, SMOQ_G_T, SMOQ_G_TDG, SMOQ_G_CZ, SMOQ_G_CNOT, SMOQ_G_RXX, SMOQ_G_RYY,
     SMOQ_G_RZZ, SMOQ_G_CRY, SMOQ_G_CCZ, SMOQ_G_TOFFOLI, SMOQ_G_U1, SMOQ_G_U2
 };
+/* operations beyond the gates, for smoq_apply_circuit_mcwf (the NOISE, MEASURE,
+ * RESET, TRACE and analog types of GATE_TYPES' neighbours,
+ * cpuVariationalQuantumCircuitBuilder.jl:82-94).  Each acts on q[0] alone: the
+ * reference's noise/measure/reset ops on several qubits loop over them in order
+ * (apply_channel_*!, cpuQuantumChannelKrausOperators.jl:426-556;
+ * projective_measurement!, cpuQuantumStateMeasurements.jl:319; reset_state!,
+ * :555), so a caller lists one op per qubit in that order. */
+enum {
+    SMOQ_N_DEPOLARIZING = 32,     /* angle = p: X, Y, Z with p/3 each (_apply_depolarizing_single! :285) */
+    SMOQ_N_AMPLITUDE_DAMPING,     /* angle = gamma (_apply_amplitude_damping_single! :350) */
+    SMOQ_N_DEPHASING,             /* angle = p: Z with (1 - sqrt(1 - p)) / 2 (_apply_dephasing_single! :262) */
+    SMOQ_N_BIT_FLIP,              /* angle = p: X with p (_apply_bit_flip_single! :321) */
+    SMOQ_N_PHASE_FLIP,            /* angle = p: Z with p (_apply_phase_flip_single! :337) */
+    SMOQ_N_PHASE_DAMPING,         /* as SMOQ_N_DEPHASING (apply_noise_mcwf!, Executor.jl:199) */
+    SMOQ_N_THERMAL_RELAXATION,    /* no effect on a pure state (apply_noise_mcwf! has no branch for it) */
+    SMOQ_M_MEASURE_Z = 48,        /* projective measurement, outcome recorded (_measure_z_single! :224) */
+    SMOQ_M_MEASURE_X,             /* H, measure Z, H (projective_measurement! :319) */
+    SMOQ_M_MEASURE_Y,             /* S^dag, H, measure Z, H, S */
+    SMOQ_R_RESET,                 /* measure Z, then force q[0] to q[1] = 0 :zero, 1 :one, 2 :plus,
+                                     3 :minus (reset_state! :555, _force_qubit_state! :584) */
+    SMOQ_T_TRACE_OUT,             /* no effect on a pure state (apply_trace_out_psi!, Executor.jl:231) */
+    SMOQ_L_LINDBLAD_STEP          /* no effect (apply_lindblad_mcwf!, Executor.jl:242, a stub) */
+};
 typedef struct {
-    int32_t type;     /* SMOQ_G_* */
+    int32_t type;     /* SMOQ_G_*, or (smoq_apply_circuit_mcwf only) SMOQ_N_* / SMOQ_M_* / SMOQ_R_* / ... */
     int32_t q[3];     /* 0-based qubits */
     int32_t param;    /* -1: fixed `angle`; >= 0: theta[param] (CircuitOperation.param_idx - 1) */
-    int32_t pad;
+    int32_t if_outcome; /* CircuitOperation.if_outcome: 0 always; k > 0 only where the trajectory's
+                         measurement k (1-based, in execution order) gave 1 (smoq_apply_circuit_mcwf
+                         only; the gate-only calls require 0) */
     double angle;
     double U[32];     /* SMOQ_G_U1 / SMOQ_G_U2 (convention 0), column-major interleaved */
 } smoq_op;
@@ -165,6 +194,26 @@ smoq_status smoq_apply_sequence(smoq_state* st, const smoq_op* ops, int n, const
 /* the same, one launch per gate (the plain, unfused path) */
 smoq_status smoq_apply_sequence_unfused(smoq_state* st, const smoq_op* ops, int n,
                                         const double* theta);
+/* apply_circuit! (cpuVariationalQuantumCircuitExecutor.jl:95) on pure states for
+ * any circuit: gates, noise channels unravelled stochastically (apply_noise_mcwf!,
+ * :187), projective measurements (apply_measure_psi!, :210), resets
+ * (apply_reset_psi!, :220) and classical conditions (if_outcome, :103-105).
+ * Every state of st is one trajectory.  Stochastic op i of trajectory b draws
+ * u = the 53-bit uniform of Philox4x32-10 with key = seed and counter
+ * (i, 0x80000000, traj_offset + b) (i = the op's index in `ops`), and uses it
+ * where the reference calls rand().  Runs of gates between stochastic ops are
+ * fused into tile passes as in smoq_apply_sequence; a Pauli noise op costs one
+ * pass over the trajectories that drew a Pauli; amplitude damping, measurement
+ * and reset cost one FP64 reduction and one pass.  Amplitude damping jumps with
+ * sigma- (the |1> amplitude REPLACES the |0> one): the reference's
+ * `psi[i_ground] += psi[i]` (cpuQuantumChannelKrausOperators.jl:367) is not
+ * followed, since only the replacing jump unravels the reference's own Kraus
+ * channel (:145-180).  A measurement with if_outcome != 0 is UNSUPPORTED (the
+ * reference's measure() cannot build one).  outcomes (host, may be NULL):
+ * batch * n_meas values, outcomes[b * n_meas + m] = result of measurement m of
+ * trajectory b, n_meas = the number of SMOQ_M_* ops in `ops`. */
+smoq_status smoq_apply_circuit_mcwf(smoq_state* st, const smoq_op* ops, int n, const double* theta,
+                                    uint64_t seed, uint64_t traj_offset, int32_t* outcomes);
 
 /* ----------------------------------- observables: utils/cpu/cpuQuantumStateObservables.jl */
 /* each writes `batch` doubles to the host array out (one per state) */
@@ -198,8 +247,10 @@ smoq_status smoq_expect_zstrings(smoq_state* st, const uint64_t* zmasks, int nob
  * nobs <= 32, batch <= 65535 and batch * nobs <= 65536 (the fixed scratch of
  * 512 KiB per GPU); larger requests return SMOQ_ERR_BADINPUT with a message
  * in errbuf (may be NULL).  The first call on each device looks up the
- * scratch array's device address (make it before any stream capture); calls
- * that can overlap on one device race on the shared scratch. */
+ * scratch array's device address (make it before any stream capture), and
+ * the first call after the device's CUDA context changed (cudaDeviceReset)
+ * looks it up again; calls that can overlap on one device race on the shared
+ * scratch. */
 smoq_status smoq_expect_zstrings_noalloc(const void* psi, int N, smoq_dtype dtype, int batch,
                                          const uint64_t* zmasks, int nobs, double* out, void* stream,
                                          char* errbuf, size_t errlen);
@@ -299,7 +350,11 @@ typedef struct {           /* one Pauli-sum term: coef * prod of letters */
  * sweep, then an uncompute sweep in reverse); replaces the gradient backends
  * of calculate_gradients (cpuVariationalQuantumCircuitGradients.jl:88) for
  * gate-only circuits whose parameterised gates are RX/RY/RZ/RXX/RYY/RZZ.
- * energies[b], grads[b * n_params + p] are host arrays. */
+ * energies[b], grads[b * n_params + p] are host arrays.  The energy is
+ * <phi|H|phi> / <phi|phi> with both sums in FP64 over the computed state phi
+ * (exactly <phi|H|phi> for a unitary circuit; for complex64 the division
+ * removes the norm drift of a deep circuit), and the gradient is divided by
+ * the same <phi|phi>. */
 smoq_status smoq_energy_grad(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* ops, int n,
                              int n_params, const smoq_pauli_term* H, int nterms, int batch,
                              const double* theta, double* energies, double* grads);

@@ -112,6 +112,32 @@ _sig("so_qrc_run", [C.c_int, C.POINTER(TrotterGate), C.c_int, C.c_int, C.c_int, 
                     C.c_uint64, C.c_uint64, _dp, _dp, C.c_int])
 _sig("so_qrc_dm_run", [C.c_int, C.POINTER(TrotterGate), C.c_int, C.c_int, C.c_int, C.c_int, _cp, _dp, C.c_int, _dp])
 _sig("so_expect_pauli_rho", [_cp, C.c_uint64, C.c_uint64, C.c_int], C.c_double)
+for _n in ("dephasing", "depolarizing", "bit_flip", "phase_flip", "amplitude_damping"):
+    _sig(f"so_noise_{_n}_u", [_cp, C.c_double, C.c_int, C.c_int, C.c_double])
+_sig("so_measure_z_u", [_cp, C.c_int, C.c_int, C.c_double], C.c_int)
+_sig("so_reset_u", [_cp, C.c_int, C.c_int, C.c_int, C.c_double])
+_sig("so_circuit_draw", [C.c_uint64, C.c_uint32, C.c_uint64], C.c_double)
+_sig("so_apply_circuit_mcwf", [_cp, C.POINTER(Op), C.c_int, _dp, C.c_int, C.c_uint64, C.c_uint64,
+                               C.POINTER(C.c_int)], C.c_int)
+_sig("so_set_threads", [C.c_int])
+_sig("so_get_threads", [], C.c_int)
+
+
+class threads:
+    """with threads(n): the oracle's per-state loops use n threads inside the
+    block (default 1, the reference's single-threaded loops)"""
+
+    def __init__(self, n=None):
+        self.n = n or os.cpu_count() or 1
+
+    def __enter__(self):
+        self.old = L.so_get_threads()
+        L.so_set_threads(int(self.n))
+        return self
+
+    def __exit__(self, *exc):
+        L.so_set_threads(self.old)
+        return False
 
 
 def zero_state(N, index=0):
@@ -264,16 +290,59 @@ def trotter_step(psi, arr, n, N):
     return psi
 
 
+(N_DEPOLARIZING, N_AMPLITUDE_DAMPING, N_DEPHASING, N_BIT_FLIP, N_PHASE_FLIP, N_PHASE_DAMPING,
+ N_THERMAL_RELAXATION) = range(32, 39)
+M_MEASURE_Z, M_MEASURE_X, M_MEASURE_Y, R_RESET, T_TRACE_OUT, L_LINDBLAD_STEP = range(48, 54)
+CIRCUIT_CODES = dict(GATE_CODES, depolarizing=N_DEPOLARIZING, amplitude_damping=N_AMPLITUDE_DAMPING,
+                     dephasing=N_DEPHASING, bit_flip=N_BIT_FLIP, phase_flip=N_PHASE_FLIP,
+                     phase_damping=N_PHASE_DAMPING, thermal_relaxation=N_THERMAL_RELAXATION,
+                     measure_z=M_MEASURE_Z, measure_x=M_MEASURE_X, measure_y=M_MEASURE_Y, reset=R_RESET,
+                     trace_out=T_TRACE_OUT, lindblad_step=L_LINDBLAD_STEP)
+RESET_TARGETS = {"zero": 0, "one": 1, "plus": 2, "minus": 3}
+
+
 def make_ops(ops):
-    """ops: list of (name, [1-based qubits], param (1-based or 0), angle)"""
+    """ops: list of (name, [1-based qubits], param (1-based or 0), angle[, if_outcome]);
+    noise ops carry p (gamma) in angle, a reset its target code in qubits[1]"""
     arr = (Op * max(1, len(ops)))()
-    for t, (name, qs, param, angle) in enumerate(ops):
-        arr[t].type = GATE_CODES[name]
+    for t, op in enumerate(ops):
+        name, qs, param, angle = op[:4]
+        arr[t].type = CIRCUIT_CODES[name]
         for k, q in enumerate(qs):
             arr[t].q[k] = q
         arr[t].param = param
         arr[t].angle = angle
+        arr[t].pad = op[4] if len(op) > 4 else 0
     return arr
+
+
+def apply_circuit_mcwf(psi, ops_arr, n, theta, N, seed, traj):
+    """one trajectory of a noisy circuit; returns the measurement outcomes"""
+    th = np.ascontiguousarray(theta, dtype=np.float64)
+    out = np.zeros(max(1, n), dtype=np.int32)
+    m = L.so_apply_circuit_mcwf(_p(psi), ops_arr, n, th.ctypes.data_as(_dp), N, seed, traj,
+                                out.ctypes.data_as(C.POINTER(C.c_int)))
+    return out[:m]
+
+
+def circuit_draw(seed, op_index, traj):
+    return L.so_circuit_draw(seed, op_index, traj)
+
+
+def noise_u(kind, psi, p, k, N, u):
+    """one noise unravelling with the draw u (kind: dephasing, depolarizing, bit_flip,
+    phase_flip, amplitude_damping)"""
+    getattr(L, f"so_noise_{kind}_u")(_p(psi), p, k, N, u)
+    return psi
+
+
+def measure_z_u(psi, k, N, u):
+    return L.so_measure_z_u(_p(psi), k, N, u)
+
+
+def reset_u(psi, k, target, N, u):
+    L.so_reset_u(_p(psi), k, RESET_TARGETS.get(target, target), N, u)
+    return psi
 
 
 def apply_circuit(psi, ops_arr, n, theta, N):

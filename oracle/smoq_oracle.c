@@ -21,6 +21,60 @@ static inline C ld(const double* m, int idx) { return m[2 * idx] + I_ * m[2 * id
 /* column-major element (r, c) of an n x n matrix */
 static inline C mat(const double* m, int n, int r, int c) { return ld(m, c * n + r); }
 
+/* ---- threads over the amplitudes of ONE state ----
+ * so_set_threads (default 1 = the reference's single-threaded loops).  Only
+ * the parity tests at the measured sizes (N = 24..30) raise it, so that the
+ * same loops finish in seconds.  run_range splits [0, 2^N) into contiguous
+ * ranges, one per thread, and calls the loop body on each.  Every gate loop
+ * below writes each amplitude from exactly one iteration (a pair or quartet
+ * is updated by the iteration of its lowest index, the others skip), so the
+ * split gives the same state; an observable's FP64 sum is the sum of the
+ * ranges' partial sums in range order. */
+static int so_nthreads = 1;
+void so_set_threads(int n) { so_nthreads = n < 1 ? 1 : (n > 256 ? 256 : n); }
+int so_get_threads(void) { return so_nthreads; }
+typedef void (*range_fn)(int64_t lo, int64_t hi, const void* a, double* acc);
+typedef struct {
+    range_fn fn;
+    const void* a;
+    int64_t lo, hi;
+    double acc;
+} range_job;
+static void* range_worker(void* p) {
+    range_job* j = (range_job*)p;
+    j->acc = 0;
+    j->fn(j->lo, j->hi, j->a, &j->acc);
+    return NULL;
+}
+static double run_range(int64_t dim, range_fn fn, const void* a) {
+    int nt = so_nthreads;
+    if (nt > dim / 4096) nt = (int)(dim / 4096);
+    if (nt <= 1) {
+        double acc = 0;
+        fn(0, dim, a, &acc);
+        return acc;
+    }
+    range_job jobs[256];
+    pthread_t th[256];
+    int started[256];
+    for (int t = 0; t < nt; t++) {
+        jobs[t].fn = fn;
+        jobs[t].a = a;
+        jobs[t].lo = dim / nt * t;
+        jobs[t].hi = t == nt - 1 ? dim : dim / nt * (t + 1);
+        jobs[t].acc = 0;
+    }
+    for (int t = 1; t < nt; t++) started[t] = pthread_create(&th[t], NULL, range_worker, &jobs[t]) == 0;
+    range_worker(&jobs[0]);
+    for (int t = 1; t < nt; t++) {
+        if (started[t]) pthread_join(th[t], NULL);
+        else range_worker(&jobs[t]);  /* no thread: run the range here */
+    }
+    double acc = 0;
+    for (int t = 0; t < nt; t++) acc += jobs[t].acc;
+    return acc;
+}
+
 double so_wtime(void) {
     struct timespec ts;
     clock_gettime(CLOCK_MONOTONIC, &ts);
@@ -30,35 +84,56 @@ double so_wtime(void) {
 /* ========================================================================
  * Single-qubit gates -- utils/cpu/cpuQuantumChannelGates.jl
  * ======================================================================== */
-void so_apply_rx_psi(C* psi, int k, double theta, int N) { /* :142-161 */
-    double c = cos(theta / 2), s = sin(theta / 2);
-    C is = -I_ * s;
-    int64_t step = 1LL << (k - 1), dim = 1LL << N;
-    for (int64_t i = 0; i < dim; i++) {
-        if (((i >> (k - 1)) & 1) == 0) {
-            int64_t j = i + step;
+typedef struct {
+    C* psi;
+    int k;
+    int64_t step;
+    double c, s;
+    C is, ph[2];
+} rot_args;
+static void rx_range(int64_t lo, int64_t hi, const void* p, double* acc) {
+    const rot_args* A = (const rot_args*)p;
+    C* psi = A->psi;
+    for (int64_t i = lo; i < hi; i++) {
+        if (((i >> (A->k - 1)) & 1) == 0) {
+            int64_t j = i + A->step;
             C a = psi[i], b = psi[j];
-            psi[i] = c * a + is * b;
-            psi[j] = is * a + c * b;
+            psi[i] = A->c * a + A->is * b;
+            psi[j] = A->is * a + A->c * b;
         }
     }
+    (void)acc;
+}
+void so_apply_rx_psi(C* psi, int k, double theta, int N) { /* :142-161 */
+    rot_args A = {psi, k, 1LL << (k - 1), cos(theta / 2), sin(theta / 2), 0, {0, 0}};
+    A.is = -I_ * A.s;
+    run_range(1LL << N, rx_range, &A);
+}
+static void ry_range(int64_t lo, int64_t hi, const void* p, double* acc) {
+    const rot_args* A = (const rot_args*)p;
+    C* psi = A->psi;
+    for (int64_t i = lo; i < hi; i++) {
+        if (((i >> (A->k - 1)) & 1) == 0) {
+            int64_t j = i + A->step;
+            C a = psi[i], b = psi[j];
+            psi[i] = A->c * a - A->s * b;
+            psi[j] = A->s * a + A->c * b;
+        }
+    }
+    (void)acc;
 }
 void so_apply_ry_psi(C* psi, int k, double theta, int N) { /* :172-190 */
-    double c = cos(theta / 2), s = sin(theta / 2);
-    int64_t step = 1LL << (k - 1), dim = 1LL << N;
-    for (int64_t i = 0; i < dim; i++) {
-        if (((i >> (k - 1)) & 1) == 0) {
-            int64_t j = i + step;
-            C a = psi[i], b = psi[j];
-            psi[i] = c * a - s * b;
-            psi[j] = s * a + c * b;
-        }
-    }
+    rot_args A = {psi, k, 1LL << (k - 1), cos(theta / 2), sin(theta / 2), 0, {0, 0}};
+    run_range(1LL << N, ry_range, &A);
+}
+static void rz_range(int64_t lo, int64_t hi, const void* p, double* acc) {
+    const rot_args* A = (const rot_args*)p;
+    for (int64_t i = lo; i < hi; i++) A->psi[i] *= A->ph[(i >> (A->k - 1)) & 1];
+    (void)acc;
 }
 void so_apply_rz_psi(C* psi, int k, double theta, int N) { /* :201-212 */
-    C ph[2] = {cexp(-I_ * theta / 2), cexp(I_ * theta / 2)};
-    int64_t dim = 1LL << N;
-    for (int64_t i = 0; i < dim; i++) psi[i] *= ph[(i >> (k - 1)) & 1];
+    rot_args A = {psi, k, 0, 0, 0, 0, {cexp(-I_ * theta / 2), cexp(I_ * theta / 2)}};
+    run_range(1LL << N, rz_range, &A);
 }
 void so_apply_hadamard_psi(C* psi, int k, int N) { /* :222-238 */
     double s = 1 / sqrt(2.0);
@@ -140,12 +215,22 @@ void so_apply_cnot_psi(C* psi, int control, int target, int N) { /* :870-882 */
         }
     }
 }
-void so_apply_cz_psi(C* psi, int qi, int qj, int N) { /* :889-900 (branchless sign) */
-    int64_t dim = 1LL << N;
-    for (int64_t idx = 0; idx < dim; idx++) {
-        int bi = (idx >> (qi - 1)) & 1, bj = (idx >> (qj - 1)) & 1;
-        psi[idx] *= (double)(1 - 2 * (bi & bj));
+typedef struct {
+    C* psi;
+    int qi, qj;
+    C same, diff;
+} pair_args;
+static void cz_range(int64_t lo, int64_t hi, const void* p, double* acc) {
+    const pair_args* A = (const pair_args*)p;
+    for (int64_t idx = lo; idx < hi; idx++) {
+        int bi = (idx >> (A->qi - 1)) & 1, bj = (idx >> (A->qj - 1)) & 1;
+        A->psi[idx] *= (double)(1 - 2 * (bi & bj));
     }
+    (void)acc;
+}
+void so_apply_cz_psi(C* psi, int qi, int qj, int N) { /* :889-900 (branchless sign) */
+    pair_args A = {psi, qi, qj, 0, 0};
+    run_range(1LL << N, cz_range, &A);
 }
 void so_apply_cry_psi(C* psi, int control, int target, double theta, int N) { /* :914-943 */
     double c = cos(theta / 2), s = sin(theta / 2);
@@ -183,13 +268,17 @@ void so_apply_ryy_psi(C* psi, int qi, int qj, double theta, int N) { /* :1039 */
     C is = -I_ * s, isn = I_ * s;
     rpp_quartet(psi, qi, qj, isn, is, is, isn, c, N);
 }
-void so_apply_rzz_psi(C* psi, int qi, int qj, double theta, int N) { /* :1084-1100 */
-    C same = cexp(-I_ * theta / 2), diff = cexp(I_ * theta / 2);
-    int64_t dim = 1LL << N;
-    for (int64_t idx = 0; idx < dim; idx++) {
-        int bi = (idx >> (qi - 1)) & 1, bj = (idx >> (qj - 1)) & 1;
-        psi[idx] *= (bi == bj) ? same : diff;
+static void rzz_range(int64_t lo, int64_t hi, const void* p, double* acc) {
+    const pair_args* A = (const pair_args*)p;
+    for (int64_t idx = lo; idx < hi; idx++) {
+        int bi = (idx >> (A->qi - 1)) & 1, bj = (idx >> (A->qj - 1)) & 1;
+        A->psi[idx] *= (bi == bj) ? A->same : A->diff;
     }
+    (void)acc;
+}
+void so_apply_rzz_psi(C* psi, int qi, int qj, double theta, int N) { /* :1084-1100 */
+    pair_args A = {psi, qi, qj, cexp(-I_ * theta / 2), cexp(I_ * theta / 2)};
+    run_range(1LL << N, rzz_range, &A);
 }
 
 /* ========================================================================
@@ -226,32 +315,59 @@ double so_population_excited_psi(const C* psi, int k, int N) { /* :784-796 */
 /* ========================================================================
  * Generic bitwise gates
  * ======================================================================== */
-void so_apply_one_qubit_gate(C* psi, const double* U, int qubit, int N) {
-    /* cpuQuantumChannelUnitaryEvolutionTrotter.jl:77-99 */
-    int64_t dim = 1LL << N, step = 1LL << (qubit - 1);
-    C u00 = mat(U, 2, 0, 0), u01 = mat(U, 2, 0, 1), u10 = mat(U, 2, 1, 0), u11 = mat(U, 2, 1, 1);
-    for (int64_t b = 0; b < dim; b++) {
+typedef struct {
+    C* psi;
+    int64_t s1, s2;
+    C u[4][4];
+} gate_args;
+static void one_qubit_range(int64_t lo, int64_t hi, const void* p, double* acc) {
+    const gate_args* A = (const gate_args*)p;
+    C* psi = A->psi;
+    const int64_t step = A->s1;
+    for (int64_t b = lo; b < hi; b++) {
         if ((b & step) == 0) {
             C a0 = psi[b], a1 = psi[b + step];
-            psi[b] = u00 * a0 + u01 * a1;
-            psi[b + step] = u10 * a0 + u11 * a1;
+            psi[b] = A->u[0][0] * a0 + A->u[0][1] * a1;
+            psi[b + step] = A->u[1][0] * a0 + A->u[1][1] * a1;
         }
     }
+    (void)acc;
 }
-static void two_qubit_core(C* psi, const C u[4][4], int q1, int q2, int N) {
+void so_apply_one_qubit_gate(C* psi, const double* U, int qubit, int N) {
+    /* cpuQuantumChannelUnitaryEvolutionTrotter.jl:77-99 */
+    gate_args A;
+    A.psi = psi;
+    A.s1 = 1LL << (qubit - 1);
+    A.s2 = 0;
+    for (int r = 0; r < 2; r++)
+        for (int c = 0; c < 2; c++) A.u[r][c] = mat(U, 2, r, c);
+    run_range(1LL << N, one_qubit_range, &A);
+}
+static void two_qubit_range(int64_t lo, int64_t hi, const void* p, double* acc) {
     /* cpuQuantumChannelUnitaryEvolutionTrotter.jl:123-139: basis order
      * |00>, |q1=1>, |q2=1>, |11> with q1 < q2 */
-    int64_t dim = 1LL << N, s1 = 1LL << (q1 - 1), s2 = 1LL << (q2 - 1);
-    for (int64_t b = 0; b < dim; b++) {
+    const gate_args* A = (const gate_args*)p;
+    C* psi = A->psi;
+    const int64_t s1 = A->s1, s2 = A->s2;
+    for (int64_t b = lo; b < hi; b++) {
         if ((b & s1) == 0 && (b & s2) == 0) {
             int64_t i0 = b, i1 = b + s1, i2 = b + s2, i3 = b + s1 + s2;
             C a[4] = {psi[i0], psi[i1], psi[i2], psi[i3]};
             C o[4];
             for (int r = 0; r < 4; r++)
-                o[r] = u[r][0] * a[0] + u[r][1] * a[1] + u[r][2] * a[2] + u[r][3] * a[3];
+                o[r] = A->u[r][0] * a[0] + A->u[r][1] * a[1] + A->u[r][2] * a[2] + A->u[r][3] * a[3];
             psi[i0] = o[0]; psi[i1] = o[1]; psi[i2] = o[2]; psi[i3] = o[3];
         }
     }
+    (void)acc;
+}
+static void two_qubit_core(C* psi, const C u[4][4], int q1, int q2, int N) {
+    gate_args A;
+    A.psi = psi;
+    A.s1 = 1LL << (q1 - 1);
+    A.s2 = 1LL << (q2 - 1);
+    memcpy(A.u, u, sizeof(A.u));
+    run_range(1LL << N, two_qubit_range, &A);
 }
 void so_apply_two_qubit_gate(C* psi, const double* U, int q1, int q2, int N) {
     /* :107-142 -- if q1 > q2 the qubits are swapped, U is NOT permuted */
@@ -278,11 +394,21 @@ void so_apply_2qubit_gate_ru(C* psi, const double* U, int q1, int q2, int N) {
  * Observables -- utils/cpu/cpuQuantumStateObservables.jl
  * ======================================================================== */
 static inline double abs2(C z) { return creal(z) * creal(z) + cimag(z) * cimag(z); }
-double so_expect_z(const C* psi, int k, int N) { /* :201-210 */
-    int64_t dim = 1LL << N;
+typedef struct {
+    const C* psi;
+    int64_t xmask, zmask;
+    C iy;
+} obs_args;
+static void zstring_range(int64_t lo, int64_t hi, const void* p, double* acc) {
+    const obs_args* A = (const obs_args*)p;
     double r = 0;
-    for (int64_t i = 0; i < dim; i++) r += abs2(psi[i]) * (double)(1 - 2 * ((i >> (k - 1)) & 1));
-    return r;
+    for (int64_t i = lo; i < hi; i++) r += abs2(A->psi[i]) * (double)(1 - 2 * (__builtin_popcountll(i & A->zmask) & 1));
+    *acc = r;
+}
+double so_expect_z(const C* psi, int k, int N) { /* :201-210 */
+    /* sum_i |psi_i|^2 (1 - 2 bit_k(i)): the Z string of the one bit */
+    obs_args A = {psi, 0, 1LL << (k - 1), 0};
+    return run_range(1LL << N, zstring_range, &A);
 }
 double so_expect_x(const C* psi, int k, int N) { /* :230-240 */
     int64_t dim = 1LL << N, step = 1LL << (k - 1);
@@ -299,13 +425,10 @@ double so_expect_y(const C* psi, int k, int N) { /* :256-267 (code sign: +2 Im) 
     return r;
 }
 double so_expect_zz(const C* psi, int i, int j, int N) { /* :341-352 */
-    int64_t dim = 1LL << N;
-    double r = 0;
-    for (int64_t s = 0; s < dim; s++) {
-        int bi = (s >> (i - 1)) & 1, bj = (s >> (j - 1)) & 1;
-        r += abs2(psi[s]) * (double)(1 - 2 * (bi ^ bj));
-    }
-    return r;
+    /* sum_s |psi_s|^2 (1 - 2 (bit_i xor bit_j)): the Z string of the two bits */
+    obs_args A = {psi, 0, (1LL << (i - 1)) | (1LL << (j - 1)), 0};
+    if (i == j) return so_norm2(psi, N);
+    return run_range(1LL << N, zstring_range, &A);
 }
 static double corr_pairs(const C* psi, int i, int j, int N, double s0011) {
     int64_t dim = 1LL << N, si = 1LL << (i - 1), sj = 1LL << (j - 1);
@@ -322,10 +445,8 @@ double so_expect_xx(const C* psi, int i, int j, int N) { return corr_pairs(psi, 
 double so_expect_yy(const C* psi, int i, int j, int N) { return corr_pairs(psi, i, j, N, -1.0); } /* :427 */
 
 double so_norm2(const C* psi, int N) {
-    int64_t dim = 1LL << N;
-    double r = 0;
-    for (int64_t i = 0; i < dim; i++) r += abs2(psi[i]);
-    return r;
+    obs_args A = {psi, 0, 0, 0};
+    return run_range(1LL << N, zstring_range, &A);
 }
 
 /* Pauli string expectation.  Z-only strings: _expect_pauli_Z_string (:900).
@@ -337,6 +458,17 @@ double so_norm2(const C* psi, int N) {
  *     <P> = sum_i conj(psi_i) * phase(i) * psi_{i ^ flipmask}
  * which equals _expect_X/_expect_XX/_expect_YY (:230/:385/:427) on 1- and
  * 2-body strings, where the reference is self-consistent. */
+/* Re sum_i conj(psi_{i ^ xmask}) i^{ny} (-1)^{popc(i & zmask)} psi_i over a range */
+static void mixed_range(int64_t lo, int64_t hi, const void* p, double* acc) {
+    const obs_args* A = (const obs_args*)p;
+    C r = 0;
+    for (int64_t i = lo; i < hi; i++) {
+        int64_t j = i ^ A->xmask;
+        double sg = (double)(1 - 2 * (__builtin_popcountll(i & A->zmask) & 1));
+        r += conj(A->psi[j]) * A->iy * sg * A->psi[i];
+    }
+    *acc = creal(r);
+}
 double so_expect_pauli_string(const C* psi, int n, const char* ops, const int* qubits, int N) {
     int64_t dim = 1LL << N, xmask = 0, zmask = 0;
     int ny = 0;
@@ -347,22 +479,12 @@ double so_expect_pauli_string(const C* psi, int n, const char* ops, const int* q
         else if (o == 'Y' || o == 'y') { xmask |= b; zmask |= b; ny++; }
         else if (o == 'Z' || o == 'z') zmask |= b;
     }
-    if (xmask == 0) { /* :900-930 */
-        double r = 0;
-        for (int64_t i = 0; i < dim; i++)
-            r += abs2(psi[i]) * (double)(1 - 2 * (__builtin_popcountll(i & zmask) & 1));
-        return r;
-    }
+    obs_args A = {psi, xmask, zmask, 1};
+    if (xmask == 0) /* :900-930 */
+        return run_range(dim, zstring_range, &A);
     /* P|i> = i^{ny} (-1)^{popc(i & zmask)} |i ^ xmask>  with Y = i X Z */
-    C iy = 1;
-    for (int t = 0; t < ny; t++) iy *= I_;
-    C acc = 0;
-    for (int64_t i = 0; i < dim; i++) {
-        int64_t j = i ^ xmask;
-        double sg = (double)(1 - 2 * (__builtin_popcountll(i & zmask) & 1));
-        acc += conj(psi[j]) * iy * sg * psi[i];
-    }
-    return creal(acc);
+    for (int t = 0; t < ny; t++) A.iy *= I_;
+    return run_range(dim, mixed_range, &A);
 }
 
 /* ========================================================================
@@ -823,12 +945,12 @@ int64_t so_measure_all(so_cplx* psi, int N, uint64_t seed, uint64_t stream) {
     return idx;
 }
 /* _measure_z_single! (:224), k 1-based */
-int so_measure_qubit(so_cplx* psi, int k, int N, uint64_t seed, uint64_t stream) {
+int so_measure_z_u(so_cplx* psi, int k, int N, double u) { /* _measure_z_single! :224-255, rand() = u */
     int64_t dim = 1LL << N, mask = 1LL << (k - 1);
     double prob_0 = 0;
     for (int64_t i = 0; i < dim; i++)
         if ((i & mask) == 0) prob_0 += abs2(psi[i]);
-    int outcome = shot_u(seed, 0, stream) < prob_0 ? 0 : 1;
+    int outcome = u < prob_0 ? 0 : 1;
     double norm_sq = 0;
     for (int64_t i = 0; i < dim; i++) {
         int bit = (int)((i >> (k - 1)) & 1);
@@ -838,6 +960,176 @@ int so_measure_qubit(so_cplx* psi, int k, int N, uint64_t seed, uint64_t stream)
     double f = 1.0 / sqrt(norm_sq);
     for (int64_t i = 0; i < dim; i++) psi[i] *= f;
     return outcome;
+}
+int so_measure_qubit(so_cplx* psi, int k, int N, uint64_t seed, uint64_t stream) {
+    return so_measure_z_u(psi, k, N, shot_u(seed, 0, stream));
+}
+
+/* ========================================================================
+ * Circuits with noise, measurements, resets and classical conditions: the
+ * pure-state branch of apply_circuit! (cpuVariationalQuantumCircuitExecutor.jl:95-146).
+ * Each restated routine takes the uniform u that the reference draws with rand().
+ * ======================================================================== */
+static void pauli_x_bit(C* psi, int k, int N) { /* the X loops of :287-296 / :322-331 */
+    int64_t mask = 1LL << (k - 1), dim = 1LL << N;
+    for (int64_t i = 0; i < dim; i++) {
+        if ((i & mask) == 0) {
+            int64_t j = i | mask;
+            C t = psi[i]; psi[i] = psi[j]; psi[j] = t;
+        }
+    }
+}
+static void pauli_z_bit(C* psi, int k, int N) { /* the Z loops of :271-279 / :307-315 / :338-345 */
+    int64_t dim = 1LL << N;
+    for (int64_t i = 0; i < dim; i++)
+        if (((i >> (k - 1)) & 1) == 1) psi[i] = -psi[i];
+}
+/* utils/cpu/cpuQuantumChannelKrausOperators.jl:262-282 */
+void so_noise_dephasing_u(C* psi, double p, int k, int N, double u) {
+    if (p == 0.0) return;                                   /* p ≈ 0.0 */
+    double q = (1.0 - sqrt(1.0 - p)) / 2.0;
+    if (u < q) pauli_z_bit(psi, k, N);
+}
+/* :285-318 */
+void so_noise_depolarizing_u(C* psi, double p, int k, int N, double u) {
+    double r = u;
+    if (r < p / 3) {
+        pauli_x_bit(psi, k, N);
+    } else if (r < 2 * p / 3) {
+        int64_t mask = 1LL << (k - 1), dim = 1LL << N;
+        for (int64_t i = 0; i < dim; i++) {
+            if ((i & mask) == 0) {
+                int64_t j = i | mask;
+                C a = psi[i], b = psi[j];
+                psi[i] = -I_ * b;
+                psi[j] = I_ * a;
+            }
+        }
+    } else if (r < p) {
+        pauli_z_bit(psi, k, N);
+    }
+}
+/* :321-334 */
+void so_noise_bit_flip_u(C* psi, double p, int k, int N, double u) {
+    if (u < p) pauli_x_bit(psi, k, N);
+}
+/* :337-347 */
+void so_noise_phase_flip_u(C* psi, double p, int k, int N, double u) {
+    if (u < p) pauli_z_bit(psi, k, N);
+}
+/* :350-386.  The jump follows the sigma- operator, psi[i_ground] = psi[i]
+ * (apply_sigma_minus_psi!, cpuQuantumChannelGates.jl:746), not the line
+ * `psi[i_ground+1] += psi[i+1]` of :367: only the replacing jump unravels the
+ * same file's Kraus channel (:145-180) that the trajectory mean must match. */
+void so_noise_amplitude_damping_u(C* psi, double gamma, int k, int N, double u) {
+    int64_t mask = 1LL << (k - 1), dim = 1LL << N;
+    double pop_1 = 0.0;
+    for (int64_t i = 0; i < dim; i++)
+        if ((i & mask) != 0) pop_1 += abs2(psi[i]);
+    double p_jump = gamma * pop_1;
+    if (u < p_jump && pop_1 > 1e-12) {
+        for (int64_t i = 0; i < dim; i++) {
+            if ((i & mask) != 0) {
+                int64_t i_ground = i ^ mask;
+                psi[i_ground] = psi[i];
+                psi[i] = 0.0;
+            }
+        }
+    } else {
+        double s = sqrt(1 - gamma);
+        for (int64_t i = 0; i < dim; i++)
+            if ((i & mask) != 0) psi[i] *= s;
+    }
+    double nrm = 0;
+    for (int64_t i = 0; i < dim; i++) nrm += abs2(psi[i]);
+    nrm = sqrt(nrm);
+    if (nrm > 1e-12)
+        for (int64_t i = 0; i < dim; i++) psi[i] /= nrm;
+}
+/* _normalize! (cpuQuantumStateMeasurements.jl:629-635) */
+static void normalize_1e15(C* psi, int N) {
+    int64_t dim = 1LL << N;
+    double ns = 0;
+    for (int64_t i = 0; i < dim; i++) ns += abs2(psi[i]);
+    if (ns > 1e-15) {
+        double f = sqrt(ns);
+        for (int64_t i = 0; i < dim; i++) psi[i] /= f;
+    }
+}
+/* _force_qubit_state! (cpuQuantumStateMeasurements.jl:584-627): target 0 :zero, 1 :one, 2 :plus, 3 :minus */
+static void force_qubit_state(C* psi, int k, int target, int N) {
+    int64_t dim = 1LL << N, mask = 1LL << (k - 1);
+    if (target == 0 || target == 2) {
+        for (int64_t i = 0; i < dim; i++) {
+            if ((i & mask) != 0) {
+                int64_t j = i ^ mask;
+                psi[j] += psi[i];
+                psi[i] = 0;
+            }
+        }
+    } else {
+        for (int64_t i = 0; i < dim; i++) {
+            if ((i & mask) == 0) {
+                int64_t j = i ^ mask;
+                psi[j] += psi[i];
+                psi[i] = 0;
+            }
+        }
+    }
+    normalize_1e15(psi, N);
+    if (target >= 2) so_apply_hadamard_psi(psi, k, N);
+}
+/* reset_state! (cpuQuantumStateMeasurements.jl:555-567): measure in Z, then force */
+void so_reset_u(C* psi, int k, int target, int N, double u) {
+    so_measure_z_u(psi, k, N, u);
+    force_qubit_state(psi, k, target, N);
+}
+/* the draw of stochastic op `op_index` of trajectory `traj` (the CUDA library's rule) */
+double so_circuit_draw(uint64_t seed, uint32_t op_index, uint64_t traj) {
+    uint32_t ctr[4] = {op_index, 0x80000000u, (uint32_t)traj, (uint32_t)(traj >> 32)};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t w[4];
+    so_philox4x32_10(ctr, key, w);
+    return so_u01_from_words(w[0], w[1]);
+}
+int so_apply_circuit_mcwf(C* psi, const so_op* ops, int n, const double* theta, int N, uint64_t seed,
+                          uint64_t traj, int* outcomes) {
+    int nout = 0;
+    for (int t = 0; t < n; t++) {
+        const so_op* o = ops + t;
+        const int cond = o->pad;                   /* CircuitOperation.if_outcome */
+        if (cond > 0 && (cond > nout || outcomes[cond - 1] != 1)) continue;   /* Executor.jl:103-105 */
+        const int k = o->q[0];
+        switch (o->type) {                         /* apply_operation! :124-140, apply_noise_mcwf! :187-201 */
+        case SO_N_DEPOLARIZING: so_noise_depolarizing_u(psi, o->angle, k, N, so_circuit_draw(seed, t, traj)); break;
+        case SO_N_AMPLITUDE_DAMPING:
+            so_noise_amplitude_damping_u(psi, o->angle, k, N, so_circuit_draw(seed, t, traj));
+            break;
+        case SO_N_DEPHASING:
+        case SO_N_PHASE_DAMPING: so_noise_dephasing_u(psi, o->angle, k, N, so_circuit_draw(seed, t, traj)); break;
+        case SO_N_BIT_FLIP: so_noise_bit_flip_u(psi, o->angle, k, N, so_circuit_draw(seed, t, traj)); break;
+        case SO_N_PHASE_FLIP: so_noise_phase_flip_u(psi, o->angle, k, N, so_circuit_draw(seed, t, traj)); break;
+        case SO_N_THERMAL_RELAXATION: case SO_T_TRACE_OUT: case SO_L_LINDBLAD_STEP: break;
+        case SO_M_MEASURE_Z:                       /* projective_measurement! :319-345 */
+            outcomes[nout++] = so_measure_z_u(psi, k, N, so_circuit_draw(seed, t, traj));
+            break;
+        case SO_M_MEASURE_X:
+            so_apply_hadamard_psi(psi, k, N);
+            outcomes[nout++] = so_measure_z_u(psi, k, N, so_circuit_draw(seed, t, traj));
+            so_apply_hadamard_psi(psi, k, N);
+            break;
+        case SO_M_MEASURE_Y:
+            so_apply_sdagger_psi(psi, k, N);
+            so_apply_hadamard_psi(psi, k, N);
+            outcomes[nout++] = so_measure_z_u(psi, k, N, so_circuit_draw(seed, t, traj));
+            so_apply_hadamard_psi(psi, k, N);
+            so_apply_s_psi(psi, k, N);
+            break;
+        case SO_R_RESET: so_reset_u(psi, k, o->q[1], N, so_circuit_draw(seed, t, traj)); break;
+        default: so_apply_circuit(psi, o, 1, theta, N); break;   /* gates: apply_gate_psi! :146 */
+        }
+    }
+    return nout;
 }
 
 /* ========================================================================

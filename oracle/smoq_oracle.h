@@ -162,12 +162,50 @@ double so_expect_zz_rho(const so_cplx* rho, int i, int j, int N);
 
 /* timing helper for the CPU baseline */
 double so_wtime(void);
+/* threads over the amplitudes of one state in the generic 2x2/4x4, Rx/Ry/Rz,
+ * CZ/Rzz and Z-string/Pauli-string loops (default 1 = the reference's
+ * single-threaded loops; the parity tests at the measured sizes raise it).
+ * States are unchanged by the split; FP64 observable sums change only their
+ * summation order. */
+void so_set_threads(int n);
+int so_get_threads(void);
+/* threads over the amplitudes of one state in the gate and observable loops
+ * (default 1 = the reference's single-threaded loops; the parity tests at the
+ * measured sizes raise it); results are unchanged up to the summation order of
+ * the FP64 observable sums */
+void so_set_threads(int n);
+int so_get_threads(void);
 
 /* ---- Born sampling / projective Z measurement: utils/cpu/cpuQuantumStateMeasurements.jl ---- */
 /* u from Philox4x32-10, counter (shot, stream), key seed (the CUDA library's draws) */
 void so_sample(const so_cplx* psi, int N, int64_t nshots, uint64_t seed, uint64_t stream, int64_t* out); /* :203 */
 int64_t so_measure_all(so_cplx* psi, int N, uint64_t seed, uint64_t stream);                             /* :484 */
 int so_measure_qubit(so_cplx* psi, int k, int N, uint64_t seed, uint64_t stream);                         /* :224 */
+int so_measure_z_u(so_cplx* psi, int k, int N, double u);       /* :224 with rand() = u */
+
+/* ---- noise unravelings (utils/cpu/cpuQuantumChannelKrausOperators.jl), reset and the
+ * pure-state circuit executor with them (cpuVariationalQuantumCircuitExecutor.jl:95-201).
+ * u is the uniform the reference draws with rand(). */
+enum { SO_N_DEPOLARIZING = 32, SO_N_AMPLITUDE_DAMPING, SO_N_DEPHASING, SO_N_BIT_FLIP, SO_N_PHASE_FLIP,
+       SO_N_PHASE_DAMPING, SO_N_THERMAL_RELAXATION,
+       SO_M_MEASURE_Z = 48, SO_M_MEASURE_X, SO_M_MEASURE_Y, SO_R_RESET, SO_T_TRACE_OUT, SO_L_LINDBLAD_STEP };
+void so_noise_dephasing_u(so_cplx* psi, double p, int k, int N, double u);        /* :262 */
+void so_noise_depolarizing_u(so_cplx* psi, double p, int k, int N, double u);     /* :285 */
+void so_noise_bit_flip_u(so_cplx* psi, double p, int k, int N, double u);         /* :321 */
+void so_noise_phase_flip_u(so_cplx* psi, double p, int k, int N, double u);       /* :337 */
+/* :350, with the sigma- jump (psi_0 = psi_1), not the `+=` of :367 */
+void so_noise_amplitude_damping_u(so_cplx* psi, double gamma, int k, int N, double u);
+/* reset_state! (cpuQuantumStateMeasurements.jl:555): target 0 :zero, 1 :one, 2 :plus, 3 :minus */
+void so_reset_u(so_cplx* psi, int k, int target, int N, double u);
+/* the uniform of stochastic op `op_index` of trajectory `traj`: Philox4x32-10,
+ * key seed, counter (op_index, 0x80000000, traj) */
+double so_circuit_draw(uint64_t seed, uint32_t op_index, uint64_t traj);
+/* apply_circuit! for one trajectory: ops with 1-based qubits, gates as in
+ * so_apply_circuit and the SO_N_/SO_M_/SO_R_/... types above; per op: pad =
+ * if_outcome, angle = p (gamma), q[1] = the reset target.  outcomes receives the
+ * measurement results in order; returns their number. */
+int so_apply_circuit_mcwf(so_cplx* psi, const so_op* ops, int n, const double* theta, int N, uint64_t seed,
+                          uint64_t traj, int* outcomes);
 
 /* ---- quantum reservoir computing, bitwise MCWF path ----
  * utils/cpu/cpuQRCSimulationMonteCarloWaveFunction.jl:451 (_run_traj_loop_bitwise!),

@@ -372,6 +372,17 @@ smoq_status smoq_state_download(smoq_state* st, void* host, size_t bytes) {
     return sync_check(st->ctx);
 }
 
+smoq_status smoq_state_download_range(smoq_state* st, uint64_t first, uint64_t count, void* host) {
+    if (check_state(st) || (!host && count)) return SMOQ_ERR_BADINPUT;
+    const uint64_t total = (uint64_t)st->batch << st->N;
+    if (first > total || count > total - first) return fail(st->ctx, SMOQ_ERR_BADINPUT, "download range out of bounds");
+    if (!count) return SMOQ_OK;
+    const size_t amp = st->amp_bytes();
+    CK(st->ctx, cudaMemcpyAsync(host, (const char*)st->ptr + first * amp, count * amp, cudaMemcpyDeviceToHost,
+                                st->ctx->stream));
+    return sync_check(st->ctx);
+}
+
 smoq_status smoq_state_set_basis(smoq_state* st, uint64_t index) {
     if (check_state(st)) return SMOQ_ERR_BADINPUT;
     if (st->N < 64 && index >= (1ull << st->N)) return fail(st->ctx, SMOQ_ERR_BADINPUT, "basis index out of range");
@@ -525,7 +536,12 @@ static smoq_status ops_to_ir(smoq_state* st, int N, const smoq_op* ops, int n, c
             case SMOQ_G_CCZ: case SMOQ_G_TOFFOLI: nq = 3; break;
             default: nq = 1;
         }
-        if (o.type < 0 || o.type > SMOQ_G_U2) return fail(ctx, SMOQ_ERR_BADINPUT, "unknown op type");
+        if (o.type < 0 || o.type > SMOQ_G_U2)
+            return fail(ctx, SMOQ_ERR_BADINPUT,
+                        o.type >= SMOQ_N_DEPOLARIZING ? "noise, measurement and reset ops need smoq_apply_circuit_mcwf"
+                                                      : "unknown op type");
+        if (o.if_outcome != 0)
+            return fail(ctx, SMOQ_ERR_BADINPUT, "a conditional op (if_outcome) needs smoq_apply_circuit_mcwf");
         for (int t = 0; t < nq; ++t) {
             if (o.q[t] < 0 || o.q[t] >= N) return fail(ctx, SMOQ_ERR_BADINPUT, "op qubit out of range");
             for (int u = 0; u < t; ++u)

@@ -38,26 +38,6 @@ struct DJump {
     double gamma;
 };
 
-// Philox4x32-10 (Salmon et al., SC'11), the same rounds as the oracle's
-__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
-#pragma unroll
-    for (int r = 0; r < 10; ++r) {
-        const uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
-        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
-        const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
-        c[0] = n0;
-        c[1] = lo1;
-        c[2] = n2;
-        c[3] = lo0;
-        k0 += 0x9E3779B9u;
-        k1 += 0xBB67AE85u;
-    }
-}
-__device__ __forceinline__ double u01(uint32_t hi, uint32_t lo) {
-    const uint64_t a = hi >> 5, b = lo >> 6;
-    return (double)(a * 67108864ull + b) * (1.0 / 9007199254740992.0);
-}
-
 __global__ void mcwf_decide_kernel(int B, int64_t tiles_per_state, int npop, const double* partials,
                                    const DJump* ops, int nops, double dt, uint64_t seed, uint64_t traj_offset,
                                    uint64_t step, int32_t* jump, double* scale, int32_t* counts) {
@@ -69,8 +49,8 @@ __global__ void mcwf_decide_kernel(int B, int64_t tiles_per_state, int npop, con
     for (int64_t t = 0; t < tiles_per_state; ++t) nrm += p[t * (1 + npop)];
     const uint64_t tr = traj_offset + (uint64_t)b;
     uint32_t c[4] = {(uint32_t)step, (uint32_t)(step >> 32), (uint32_t)tr, (uint32_t)(tr >> 32)};
-    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
-    const double uj = u01(c[0], c[1]), uc = u01(c[2], c[3]);
+    philox10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const double uj = u01_53(c[0], c[1]), uc = u01_53(c[2], c[3]);
     const double dp = 1.0 - nrm;
     int chosen = -1;
     double new_norm = nrm;

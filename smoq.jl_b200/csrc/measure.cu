@@ -28,25 +28,10 @@ namespace smoq {
 
 constexpr int SAMPLE_CHUNK = 256;  // amplitudes per first-level chunk (8 per lane)
 
-__device__ __forceinline__ void philox_rounds(uint32_t c[4], uint32_t k0, uint32_t k1) {
-#pragma unroll
-    for (int r = 0; r < 10; ++r) {
-        const uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
-        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
-        const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
-        c[0] = n0;
-        c[1] = lo1;
-        c[2] = n2;
-        c[3] = lo0;
-        k0 += 0x9E3779B9u;
-        k1 += 0xBB67AE85u;
-    }
-}
 __device__ __forceinline__ double shot_uniform(uint64_t seed, uint64_t shot, uint64_t stream) {
     uint32_t c[4] = {(uint32_t)shot, (uint32_t)(shot >> 32), (uint32_t)stream, (uint32_t)(stream >> 32)};
-    philox_rounds(c, (uint32_t)seed, (uint32_t)(seed >> 32));
-    const uint64_t a = c[0] >> 5, b = c[1] >> 6;
-    return (double)(a * 67108864ull + b) * (1.0 / 9007199254740992.0);
+    philox10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    return u01_53(c[0], c[1]);
 }
 
 // sums[c] = sum of |psi|^2 over chunk c (chunks of all states, state-major)

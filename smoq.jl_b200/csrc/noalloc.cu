@@ -20,7 +20,12 @@
 // host looks up the array's device address with cudaGetSymbolAddress and
 // passes that address to the kernels.  The lookup happens inside the first
 // call made on each device; make that first call before any stream capture
-// starts, because the lookup can load the library's device code.
+// starts, because the lookup can load the library's device code.  The
+// address is remembered together with the CUDA context that was current
+// when it was looked up: after cudaDeviceReset the runtime makes a new
+// primary context, the library's device code is loaded again (possibly at
+// another address), and the next call sees the new context and looks the
+// address up again instead of reusing the stale one.
 //
 // All calls on one device share the array.  Every slot the finishing kernel
 // reads is written by the first kernel of the same call, so nothing carries
@@ -43,7 +48,33 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxPartials];
 
 std::mutex g_setup_mu;
+// per device: the scratch array's device address and the CUDA context it
+// belongs to (the address is only valid in that context)
 double* g_partials_addr[kMaxDevices] = {};
+void* g_partials_ctx[kMaxDevices] = {};
+
+// cuCtxGetCurrent through the runtime's driver entry-point table (the library
+// does not link libcuda itself); null when the driver does not provide it
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn fn = []() -> CtxGetCurrentFn {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            (void)cudaGetLastError();
+            return nullptr;
+        }
+        return reinterpret_cast<CtxGetCurrentFn>(p);
+    }();
+    return fn;
+}
+void* current_context() {
+    void* c = nullptr;
+    if (CtxGetCurrentFn f = ctx_get_current())
+        if (f(&c) != 0) c = nullptr;
+    return c;
+}
 
 struct NoAllocMasks {
     uint64_t m[kNoAllocMaxObs];
@@ -129,8 +160,10 @@ extern "C" smoq_status smoq_expect_zstrings_noalloc(const void* psi, int N, smoq
     double* partials = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_setup_mu);
-        if (!g_partials_addr[dev]) {
-            // set-up, once per device, with that device current
+        // set-up, once per device (and again if that device's context changed,
+        // e.g. after cudaDeviceReset), with that device current
+        void* cur = current_context();
+        if (!g_partials_addr[dev] || !cur || cur != g_partials_ctx[dev]) {
             double* p = nullptr;
             cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_partials);
             if (e != cudaSuccess || !p) {
@@ -140,6 +173,10 @@ extern "C" smoq_status smoq_expect_zstrings_noalloc(const void* psi, int N, smoq
                 return SMOQ_ERR_CUDA;
             }
             g_partials_addr[dev] = p;
+            // the lookup made the primary context current if nothing was; a null
+            // context here (no driver entry point) leaves the address un-cached,
+            // so every call looks it up again
+            g_partials_ctx[dev] = current_context();
         }
         partials = g_partials_addr[dev];
     }

@@ -44,14 +44,16 @@ struct HamTerm {
     int32_t pad;
 };
 
-// lambda_k = sum_t c_t i^{ny} (-1)^{popc((k ^ x) & z)} phi_{k ^ x}; partial
-// sums of conj(phi_k) lambda_k (real part) per block
+// lambda_k = sum_t c_t i^{ny} (-1)^{popc((k ^ x) & z)} phi_{k ^ x}; per block
+// the FP64 partial sums of Re(conj(phi_k) lambda_k) (partials[blockIdx.x])
+// and of |phi_k|^2 (partials[gridDim.x + blockIdx.x]), so the caller can
+// divide the energy by the norm of the state it was measured on
 template <typename R>
 __global__ void __launch_bounds__(256) ham_apply_kernel(const typename CT<R>::T* phi, typename CT<R>::T* lam, int N,
                                                         const HamTerm* terms, int nterms, double* partials) {
     using C = typename CT<R>::T;
     const int64_t len = (int64_t)1 << N;
-    double acc = 0;
+    double acc = 0, nrm = 0;
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < len; k += (int64_t)gridDim.x * blockDim.x) {
         double lr = 0, li = 0;
         for (int t = 0; t < nterms; ++t) {
@@ -73,15 +75,19 @@ __global__ void __launch_bounds__(256) ham_apply_kernel(const typename CT<R>::T*
         lam[k] = o;
         const C f = phi[k];
         acc += (double)f.x * lr + (double)f.y * li;  // Re(conj(phi) lambda)
+        nrm += (double)f.x * f.x + (double)f.y * f.y;
     }
-    __shared__ double red[8];
-    for (int d = 16; d > 0; d >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, d);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __shared__ double red[2][8];
+    for (int d = 16; d > 0; d >>= 1) {
+        acc += __shfl_down_sync(0xffffffffu, acc, d);
+        nrm += __shfl_down_sync(0xffffffffu, nrm, d);
+    }
+    if ((threadIdx.x & 31) == 0) red[0][threadIdx.x >> 5] = acc, red[1][threadIdx.x >> 5] = nrm;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 2) {
         double s = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-        partials[blockIdx.x] = s;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
+        partials[threadIdx.x * gridDim.x + blockIdx.x] = s;
     }
 }
 
@@ -496,7 +502,8 @@ struct ResArgs {
     const ResJob* jobs;
     const DevOp* ops;
     const HamTerm* terms;
-    double* energy;  // [njobs]
+    double* energy;  // [njobs], <phi|H|phi> / <phi|phi>
+    double* norm2;   // [njobs], <phi|phi>
     double* cols;    // [columns of all jobs], zeroed
     int32_t njobs;
 };
@@ -525,7 +532,7 @@ __global__ void __launch_bounds__(256) vqe_resident_kernel(const ResArgs A) {
     using C = typename CT<R>::T;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ C dco[16];
-    __shared__ double red[8];
+    __shared__ double red[2][8];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int j = blockIdx.x; j < A.njobs; j += gridDim.x) {
         const ResJob J = A.jobs[j];
@@ -543,8 +550,8 @@ __global__ void __launch_bounds__(256) vqe_resident_kernel(const ResArgs A) {
             res_apply<R>(A.ops[J.fwd_off + o], P, J.N, dco);
             __syncthreads();
         }
-        // lambda = H phi and Re <phi|lambda> (the pull rule of ham_apply_kernel)
-        double acc = 0;
+        // lambda = H phi, Re <phi|lambda> and <phi|phi> (the pull rule of ham_apply_kernel)
+        double acc = 0, nrm = 0;
         for (uint32_t k = tid; k < dim; k += blockDim.x) {
             double lr = 0, li = 0;
             for (int t = 0; t < J.nterms; ++t) {
@@ -566,14 +573,20 @@ __global__ void __launch_bounds__(256) vqe_resident_kernel(const ResArgs A) {
             Q[k] = o;
             const C f = P[k];
             acc += (double)f.x * lr + (double)f.y * li;
+            nrm += (double)f.x * f.x + (double)f.y * f.y;
         }
-        for (int d = 16; d > 0; d >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
-        if (lane == 0) red[warp] = acc;
+        for (int d = 16; d > 0; d >>= 1) {
+            acc += __shfl_xor_sync(0xffffffffu, acc, d);
+            nrm += __shfl_xor_sync(0xffffffffu, nrm, d);
+        }
+        if (lane == 0) red[0][warp] = acc, red[1][warp] = nrm;
         __syncthreads();
         if (tid == 0) {
-            double e = 0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) e += red[w];
-            A.energy[j] = e;
+            // E = <phi|H|phi> / <phi|phi>; the host divides the gradient columns by <phi|phi>
+            double e = 0, n = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) e += red[0][w], n += red[1][w];
+            A.energy[j] = e / n;
+            A.norm2[j] = n;
         }
         adj_program<R>(A.ops + J.bwd_off, J.bwd_n, P, Q, J.N, 0, dco, [&](R a, int col) {
             double x = (double)a;
@@ -770,9 +783,12 @@ static smoq_status check_vqe_args(smoq_ctx* ctx, int N, smoq_dtype dtype, const 
     return SMOQ_OK;
 }
 
-// forward state into w.phi, lambda = H phi into w.lam; returns E
+// forward state into w.phi, lambda = H phi into w.lam; returns
+// E = <phi|H|phi> / <phi|phi> and the FP64 <phi|phi> it divided by (a unitary
+// circuit keeps the norm at 1 in exact arithmetic; dividing removes the
+// complex64 norm drift of a deep circuit from the energy at first order)
 static smoq_status forward_and_h(smoq_ctx* ctx, Work& w, const std::vector<GateIR>& ir, const std::vector<HamTerm>& ht,
-                                 HamTerm* d_terms, double* d_epart, int eblocks, double* E) {
+                                 HamTerm* d_terms, double* d_epart, int eblocks, double* E, double* nrm2) {
     VCK(launch_set_basis(&w.phi, 0));
     if (!ir.empty()) {
         void* h = nullptr;
@@ -789,12 +805,14 @@ static smoq_status forward_and_h(smoq_ctx* ctx, Work& w, const std::vector<GateI
                                                                    w.phi.N, d_terms, (int)ht.size(), d_epart);
     ctx->launches++;
     VCK(cudaGetLastError());
-    std::vector<double> ep(eblocks);
-    VCK(cudaMemcpyAsync(ep.data(), d_epart, eblocks * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<double> ep(2 * (size_t)eblocks);
+    VCK(cudaMemcpyAsync(ep.data(), d_epart, ep.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     VCK(cudaStreamSynchronize(ctx->stream));
-    double e = 0;
-    for (double x : ep) e += x;
-    *E = e;
+    double e = 0, n = 0;
+    for (int k = 0; k < eblocks; ++k) e += ep[k], n += ep[eblocks + k];
+    if (!(n > 0)) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "VQE: the circuit's state has zero norm");
+    *E = e / n;
+    *nrm2 = n;
     return SMOQ_OK;
 }
 
@@ -889,8 +907,8 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
     VCK(cudaMemcpyAsync(d_terms, ht.data(), ht.size() * sizeof(HamTerm), cudaMemcpyHostToDevice, ctx->stream));
     const int64_t len = (int64_t)1 << N;
     const int eblocks = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, (int64_t)ctx->num_sms * 8));
-    double* d_epart;
-    VCK(cudaMallocAsync((void**)&d_epart, eblocks * sizeof(double), ctx->stream));
+    double* d_epart;  // energy partials, then norm partials
+    VCK(cudaMallocAsync((void**)&d_epart, 2 * (size_t)eblocks * sizeof(double), ctx->stream));
     w.owned.push_back(d_epart);
 
     // the next parameter set is prepared on a host thread while this one runs
@@ -920,8 +938,8 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
         }
         GradPlan& gp = use_pre ? *pre : *cur;
         if (gp.status) return smoq_internal_fail(ctx, gp.status, gp.error.c_str());
-        double E = 0;
-        if (smoq_status s = forward_and_h(ctx, w, gp.ir, ht, d_terms, d_epart, eblocks, &E)) return s;
+        double E = 0, nrm2 = 1;
+        if (smoq_status s = forward_and_h(ctx, w, gp.ir, ht, d_terms, d_epart, eblocks, &E, &nrm2)) return s;
         energies[b] = E;
         if (!grads) continue;
         double* g = grads + (size_t)b * n_params;
@@ -996,7 +1014,9 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
                                           ("device bounds check failed at site " + std::to_string(herr >> 8)).c_str());
             return smoq_internal_fail(ctx, SMOQ_ERR_TIMEOUT, "a bounded device wait ran out");
         }
-        for (int32_t c = 0; c < ncols; ++c) g[inner_param[c]] += colsum[c];
+        // the gradient of <phi|H|phi> / <phi|phi>: the norm is constant in theta for a
+        // unitary circuit, so the raw adjoint sums are divided by the same <phi|phi>
+        for (int32_t c = 0; c < ncols; ++c) g[inner_param[c]] += colsum[c] / nrm2;
     }
     return SMOQ_OK;
 }
@@ -1114,7 +1134,7 @@ static smoq_status run_resident(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vqe_
                  b_terms = al(terms.size() * sizeof(HamTerm)), b_e = al((size_t)n * 8),
                  b_c = al((size_t)std::max(1, ncols) * 8);
     char* buf = nullptr;
-    VCK(cudaMallocAsync((void**)&buf, b_jobs + b_ops + b_terms + b_e + b_c, ctx->stream));
+    VCK(cudaMallocAsync((void**)&buf, b_jobs + b_ops + b_terms + 2 * b_e + b_c, ctx->stream));
     std::unique_ptr<char, std::function<void(char*)>> hold(buf, [ctx](char* q) { cudaFreeAsync(q, ctx->stream); });
     ResArgs A;
     char* c = buf;
@@ -1128,6 +1148,8 @@ static smoq_status run_resident(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vqe_
     VCK(cudaMemcpyAsync(c, terms.data(), terms.size() * sizeof(HamTerm), cudaMemcpyHostToDevice, ctx->stream));
     c += b_terms;
     A.energy = (double*)c;
+    c += b_e;
+    A.norm2 = (double*)c;
     c += b_e;
     A.cols = (double*)c;
     VCK(cudaMemsetAsync(c, 0, (size_t)std::max(1, ncols) * 8, ctx->stream));
@@ -1145,8 +1167,9 @@ static smoq_status run_resident(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vqe_
     else vqe_resident_kernel<double><<<grid, 256, smem, ctx->stream>>>(A);
     ctx->launches++;
     VCK(cudaGetLastError());
-    std::vector<double> e(n), cols((size_t)std::max(1, ncols));
+    std::vector<double> e(n), nrm(n), cols((size_t)std::max(1, ncols));
     VCK(cudaMemcpyAsync(e.data(), A.energy, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    VCK(cudaMemcpyAsync(nrm.data(), A.norm2, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream));
     VCK(cudaMemcpyAsync(cols.data(), A.cols, cols.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
     VCK(cudaStreamSynchronize(ctx->stream));
     for (size_t u = 0; u < idx.size(); ++u) {
@@ -1154,7 +1177,8 @@ static smoq_status run_resident(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vqe_
         J.energy[0] = e[u];
         if (!J.grad) continue;
         for (int p = 0; p < J.n_params; ++p) J.grad[p] = 0.0;
-        for (size_t k = 0; k < inner_param[u].size(); ++k) J.grad[inner_param[u][k]] += cols[rj[u].col_off + k];
+        for (size_t k = 0; k < inner_param[u].size(); ++k)
+            J.grad[inner_param[u][k]] += cols[rj[u].col_off + k] / nrm[u];
     }
     return SMOQ_OK;
 }
@@ -1252,7 +1276,9 @@ extern "C" smoq_status smoq_apply_pauli_sum(smoq_state* in, smoq_state* out, con
     const int eblocks = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, (int64_t)ctx->num_sms * 8));
     void* buf = nullptr;
     const size_t tbytes = ht.size() * sizeof(HamTerm);
-    VCK(cudaMallocAsync(&buf, ((tbytes + 15) / 16) * 16 + (size_t)eblocks * in->batch * sizeof(double), ctx->stream));
+    // per state: eblocks energy partials, then eblocks norm partials (unused here)
+    VCK(cudaMallocAsync(&buf, ((tbytes + 15) / 16) * 16 + 2 * (size_t)eblocks * in->batch * sizeof(double),
+                        ctx->stream));
     HamTerm* d_terms = (HamTerm*)buf;
     double* d_part = (double*)((char*)buf + ((tbytes + 15) / 16) * 16);
     VCK(cudaMemcpyAsync(d_terms, ht.data(), tbytes, cudaMemcpyHostToDevice, ctx->stream));
@@ -1262,16 +1288,16 @@ extern "C" smoq_status smoq_apply_pauli_sum(smoq_state* in, smoq_state* out, con
         char* dst = (char*)out->ptr + (size_t)b * len * amp;
         if (in->dtype == SMOQ_C64)
             ham_apply_kernel<float><<<eblocks, 256, 0, ctx->stream>>>((const float2*)src, (float2*)dst, N, d_terms,
-                                                                      nterms, d_part + (size_t)b * eblocks);
+                                                                      nterms, d_part + 2 * (size_t)b * eblocks);
         else
             ham_apply_kernel<double><<<eblocks, 256, 0, ctx->stream>>>((const double2*)src, (double2*)dst, N,
-                                                                       d_terms, nterms, d_part + (size_t)b * eblocks);
+                                                                       d_terms, nterms, d_part + 2 * (size_t)b * eblocks);
         ctx->launches++;
     }
     cudaError_t e = cudaGetLastError();
     std::vector<double> part;
     if (e == cudaSuccess && expect) {
-        part.resize((size_t)eblocks * in->batch);
+        part.resize(2 * (size_t)eblocks * in->batch);
         e = cudaMemcpyAsync(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
     }
     cudaFreeAsync(buf, ctx->stream);
@@ -1280,7 +1306,7 @@ extern "C" smoq_status smoq_apply_pauli_sum(smoq_state* in, smoq_state* out, con
     if (expect)
         for (int b = 0; b < in->batch; ++b) {
             double s = 0;
-            for (int k = 0; k < eblocks; ++k) s += part[(size_t)b * eblocks + k];
+            for (int k = 0; k < eblocks; ++k) s += part[2 * (size_t)b * eblocks + k];
             expect[b] = s;
         }
     return SMOQ_OK;

@@ -129,6 +129,13 @@ class CuState:
         ck(lib.smoq_state_download(self.h, out.ctypes.data_as(C.c_void_p), out.nbytes), self.ctx.h, "download")
         return out if self.batch == 1 else out.reshape(self.batch, -1)
 
+    def download_range(self, first: int, count: int) -> np.ndarray:
+        """amplitudes [first, first + count) of the batch (state b starts at b * 2^N)"""
+        out = np.empty(count, dtype=self.np_dtype)
+        ck(lib.smoq_state_download_range(self.h, first, count, out.ctypes.data_as(C.c_void_p)), self.ctx.h,
+           "download_range")
+        return out
+
     def copy_from(self, other: "CuState"):
         ck(lib.smoq_state_copy(self.h, other.h), self.ctx.h, "copy")
 
@@ -501,21 +508,81 @@ _GATE_CODES = {"rx": _lib.G_RX, "ry": _lib.G_RY, "rz": _lib.G_RZ, "h": _lib.G_H,
                "rzz": _lib.G_RZZ, "cry": _lib.G_CRY, "ccz": _lib.G_CCZ, "toffoli": _lib.G_TOFFOLI}
 
 
+_NOISE_CODES = {"depolarizing": _lib.N_DEPOLARIZING, "amplitude_damping": _lib.N_AMPLITUDE_DAMPING,
+                "dephasing": _lib.N_DEPHASING, "bit_flip": _lib.N_BIT_FLIP, "phase_flip": _lib.N_PHASE_FLIP,
+                "phase_damping": _lib.N_PHASE_DAMPING, "thermal_relaxation": _lib.N_THERMAL_RELAXATION}
+_MEASURE_CODES = {"measure_z": _lib.M_MEASURE_Z, "measure_x": _lib.M_MEASURE_X, "measure_y": _lib.M_MEASURE_Y,
+                  "measure": _lib.M_MEASURE_Z}
+_OTHER_CODES = {"reset": _lib.R_RESET, "trace_out": _lib.T_TRACE_OUT, "lindblad_step": _lib.L_LINDBLAD_STEP}
+_RESET_TARGETS = {"zero": 0, "one": 1, "plus": 2, "minus": 3}
+
+
 @dataclass
-class CircuitOperation:  # cpuVariationalQuantumCircuitBuilder.jl:120 (gate subset)
+class CircuitOperation:  # cpuVariationalQuantumCircuitBuilder.jl:120
     type: str
     qubits: List[int]
     param_idx: int = 0
     fixed_angle: float = 0.0
+    p: float = 0.0                 # noise probability or rate
+    target_state: str = "none"     # reset target: zero, one, plus, minus
+    basis: str = "z"               # measurement basis
+    if_outcome: int = 0            # 0 always; k > 0 only if the trajectory's outcome k (1-based) is 1
+
+    @property
+    def is_gate(self) -> bool:
+        return self.type in _GATE_CODES
 
 
-def gate(type: str, qubits, param_idx: int = 0, angle: float = 0.0) -> CircuitOperation:
+def gate(type: str, qubits, param_idx: int = 0, angle: float = 0.0, if_outcome: int = 0) -> CircuitOperation:
     """gate (cpuVariationalQuantumCircuitBuilder.jl:172)"""
     t = type.lower().lstrip(":")
     if t not in _GATE_CODES:
         raise SmoqError(_lib.SMOQ_ERR_BADINPUT, f"Unknown gate type: {type}")
     q = [qubits] if isinstance(qubits, int) else list(qubits)
-    return CircuitOperation(t, q, param_idx, angle)
+    return CircuitOperation(t, q, param_idx, angle, if_outcome=if_outcome)
+
+
+def noise(type: str, qubits, p: float = 0.0, if_outcome: int = 0) -> CircuitOperation:
+    """noise (cpuVariationalQuantumCircuitBuilder.jl:192): a channel unravelled per trajectory"""
+    t = type.lower().lstrip(":")
+    if t not in _NOISE_CODES:
+        raise SmoqError(_lib.SMOQ_ERR_BADINPUT, f"Unknown noise type: {type}")
+    q = [qubits] if isinstance(qubits, int) else list(qubits)
+    return CircuitOperation(t, q, p=float(p), if_outcome=if_outcome)
+
+
+def measure(qubits, basis: str = "z") -> CircuitOperation:
+    """measure (cpuVariationalQuantumCircuitBuilder.jl:210): projective, one outcome per qubit"""
+    b = basis.lower().lstrip(":")
+    if b not in ("x", "y", "z"):
+        raise SmoqError(_lib.SMOQ_ERR_BADINPUT, f"Unknown basis: {basis}. Use :z, :x, :y")
+    q = [qubits] if isinstance(qubits, int) else list(qubits)
+    return CircuitOperation("measure_" + b, q, basis=b)
+
+
+def reset(qubits, target_state: str = "zero", if_outcome: int = 0) -> CircuitOperation:
+    """reset (cpuVariationalQuantumCircuitBuilder.jl:229)"""
+    t = target_state.lower().lstrip(":")
+    if t not in _RESET_TARGETS:
+        raise SmoqError(_lib.SMOQ_ERR_BADINPUT, f"Unknown reset target: {target_state}")
+    q = [qubits] if isinstance(qubits, int) else list(qubits)
+    return CircuitOperation("reset", q, target_state=t, if_outcome=if_outcome)
+
+
+def trace_out(qubits) -> CircuitOperation:
+    """trace_out (cpuVariationalQuantumCircuitBuilder.jl:261): no effect on a pure state"""
+    return CircuitOperation("trace_out", [qubits] if isinstance(qubits, int) else list(qubits))
+
+
+def lindblad_step(qubits) -> CircuitOperation:
+    """lindblad_step (cpuVariationalQuantumCircuitBuilder.jl:245): the reference's pure-state executor skips it"""
+    return CircuitOperation("lindblad_step", [qubits] if isinstance(qubits, int) else list(qubits))
+
+
+@dataclass
+class CircuitResult:  # cpuVariationalQuantumCircuitBuilder.jl:150
+    state: "CuState"
+    outcomes: np.ndarray   # [outcomes] (batch 1) or [batch, outcomes]: 0/1 in execution order
 
 
 @dataclass
@@ -562,27 +629,115 @@ def repeat_layer(layer_fn, L: int, N: int, param_offset: int = 1):
     return all_ops, idx
 
 
+def _c_ops(ops: Sequence[CircuitOperation]):
+    """one smoq_op per gate, and one per qubit of a noise / measure / reset op (the
+    reference loops over those qubits in order)"""
+    out = []
+    for op in ops:
+        if op.type in _GATE_CODES:
+            out.append((_GATE_CODES[op.type], [q - 1 for q in op.qubits], op.param_idx - 1 if op.param_idx > 0 else -1,
+                        op.fixed_angle, op.if_outcome))
+            continue
+        code = _NOISE_CODES.get(op.type, _MEASURE_CODES.get(op.type, _OTHER_CODES.get(op.type)))
+        if code is None:
+            raise SmoqError(_lib.SMOQ_ERR_BADINPUT, f"Unknown operation type: {op.type}")
+        for q in op.qubits:
+            qs = [q - 1, _RESET_TARGETS[op.target_state]] if op.type == "reset" else [q - 1]
+            out.append((code, qs, -1, op.p, op.if_outcome))
+    arr = (SmoqOp * max(1, len(out)))()
+    for t, (code, qs, param, angle, cond) in enumerate(out):
+        arr[t].type = code
+        for k, q in enumerate(qs):
+            arr[t].q[k] = q
+        arr[t].param = param
+        arr[t].angle = angle
+        arr[t].if_outcome = cond
+    return arr, len(out)
+
+
 def circuit_to_c_ops(ops: Sequence[CircuitOperation]):
-    arr = (SmoqOp * max(1, len(ops)))()
-    for t, op in enumerate(ops):
-        arr[t].type = _GATE_CODES[op.type]
-        for k, q in enumerate(op.qubits):
-            arr[t].q[k] = q - 1
-        arr[t].param = op.param_idx - 1 if op.param_idx > 0 else -1
-        arr[t].angle = op.fixed_angle
-    return arr
+    return _c_ops(ops)[0]
 
 
-def apply_circuit(psi: CuState, circuit: ParameterizedCircuit, theta, fused: bool = True):
-    """apply_circuit! (cpuVariationalQuantumCircuitExecutor.jl:95) for gate-only circuits."""
+def count_measurements(ops: Sequence[CircuitOperation]) -> int:
+    return sum(len(op.qubits) for op in ops if op.type in _MEASURE_CODES)
+
+
+def apply_circuit(psi: CuState, circuit: ParameterizedCircuit, theta, fused: bool = True, seed: int = 1234,
+                  traj_offset: int = 0):
+    """apply_circuit! (cpuVariationalQuantumCircuitExecutor.jl:95).  Gate-only circuits run as
+    fused tile passes (fused=True) or one kernel per gate and return psi.  Circuits with noise,
+    measurements, resets or classical conditions run every state of psi as one trajectory
+    (draws from Philox4x32-10, key seed, counter (op index, 0x80000000, traj_offset + b)) and
+    return a CircuitResult with the measurement outcomes."""
     if psi.N != circuit.N:
         raise SmoqError(_lib.SMOQ_ERR_BADINPUT, "State dimension mismatch")
     th = np.ascontiguousarray(theta, dtype=np.float64)
     if th.size < circuit.n_params:
         raise SmoqError(_lib.SMOQ_ERR_BADINPUT, "Not enough parameters")
-    arr = circuit_to_c_ops(circuit.operations)
-    fn = lib.smoq_apply_sequence if fused else lib.smoq_apply_sequence_unfused
-    ck(fn(psi.h, arr, len(circuit.operations), dptr(th)), psi.ctx.h, "apply_circuit")
+    arr, n = _c_ops(circuit.operations)
+    if all(op.is_gate and op.if_outcome == 0 for op in circuit.operations):
+        fn = lib.smoq_apply_sequence if fused else lib.smoq_apply_sequence_unfused
+        ck(fn(psi.h, arr, n, dptr(th)), psi.ctx.h, "apply_circuit")
+        return psi
+    nm = count_measurements(circuit.operations)
+    out = np.zeros(max(1, psi.batch * nm), dtype=np.int32)
+    ck(lib.smoq_apply_circuit_mcwf(psi.h, arr, n, dptr(th), seed, traj_offset,
+                                   out.ctypes.data_as(C.POINTER(C.c_int32))), psi.ctx.h, "apply_circuit")
+    oc = out[:psi.batch * nm].reshape(psi.batch, nm)
+    return CircuitResult(psi, oc[0] if psi.batch == 1 else oc)
+
+
+def _channel(kind, psi: CuState, p: float, qubits, N: int, seed: int, traj_offset: int):
+    _n(psi, N)
+    qs = [qubits] if isinstance(qubits, int) else list(qubits)
+    circ = ParameterizedCircuit(N, [noise(kind, qs, p=p)])
+    apply_circuit(psi, circ, np.zeros(1), seed=seed, traj_offset=traj_offset)
+    return psi
+
+
+def apply_channel_dephasing(psi, p, qubits, N, seed=1234, traj_offset=0):
+    """apply_channel_dephasing! (cpuQuantumChannelKrausOperators.jl:426), pure-state unravelling"""
+    return _channel("dephasing", psi, p, qubits, N, seed, traj_offset)
+
+
+def apply_channel_depolarizing(psi, p, qubits, N, seed=1234, traj_offset=0):
+    """apply_channel_depolarizing! (cpuQuantumChannelKrausOperators.jl:458)"""
+    return _channel("depolarizing", psi, p, qubits, N, seed, traj_offset)
+
+
+def apply_channel_amplitude_damping(psi, gamma, qubits, N, seed=1234, traj_offset=0):
+    """apply_channel_amplitude_damping! (cpuQuantumChannelKrausOperators.jl:492)"""
+    return _channel("amplitude_damping", psi, gamma, qubits, N, seed, traj_offset)
+
+
+def apply_channel_bit_flip(psi, p, qubits, N, seed=1234, traj_offset=0):
+    """apply_channel_bit_flip! (cpuQuantumChannelKrausOperators.jl:524)"""
+    return _channel("bit_flip", psi, p, qubits, N, seed, traj_offset)
+
+
+def apply_channel_phase_flip(psi, p, qubits, N, seed=1234, traj_offset=0):
+    """apply_channel_phase_flip! (cpuQuantumChannelKrausOperators.jl:556)"""
+    return _channel("phase_flip", psi, p, qubits, N, seed, traj_offset)
+
+
+def projective_measurement(psi: CuState, qubits, basis: str, N: int, seed: int = 1234, traj_offset: int = 0):
+    """projective_measurement! (cpuQuantumStateMeasurements.jl:319): (outcomes, psi)"""
+    _n(psi, N)
+    r = apply_circuit(psi, ParameterizedCircuit(N, [measure(qubits, basis)]), np.zeros(1), seed=seed,
+                      traj_offset=traj_offset)
+    return r.outcomes, psi
+
+
+def reset_state(psi: CuState, qubits, targets, N: int, seed: int = 1234, traj_offset: int = 0):
+    """reset_state! (cpuQuantumStateMeasurements.jl:555): targets a symbol or one per qubit"""
+    _n(psi, N)
+    qs = [qubits] if isinstance(qubits, int) else list(qubits)
+    ts = [targets] * len(qs) if isinstance(targets, str) else list(targets)
+    if len(ts) != len(qs):
+        raise SmoqError(_lib.SMOQ_ERR_BADINPUT, "Must specify target for each qubit")
+    apply_circuit(psi, ParameterizedCircuit(N, [reset([q], t) for q, t in zip(qs, ts)]), np.zeros(1), seed=seed,
+                  traj_offset=traj_offset)
     return psi
 
 

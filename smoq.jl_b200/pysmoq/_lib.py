@@ -22,8 +22,14 @@ C64, C128 = 0, 1
  OPT_ENGINE, OPT_JIT_BUFFERS, OPT_JIT_PACKED, OPT_JIT_GROUPS, OPT_JIT_STAGE_BITS, OPT_VQE_RESIDENT) = range(1, 13)
 
 
+# operations of smoq_apply_circuit_mcwf beyond the gates (one qubit each)
+(N_DEPOLARIZING, N_AMPLITUDE_DAMPING, N_DEPHASING, N_BIT_FLIP, N_PHASE_FLIP, N_PHASE_DAMPING,
+ N_THERMAL_RELAXATION) = range(32, 39)
+M_MEASURE_Z, M_MEASURE_X, M_MEASURE_Y, R_RESET, T_TRACE_OUT, L_LINDBLAD_STEP = range(48, 54)
+
+
 class SmoqOp(C.Structure):
-    _fields_ = [("type", C.c_int32), ("q", C.c_int32 * 3), ("param", C.c_int32), ("pad", C.c_int32),
+    _fields_ = [("type", C.c_int32), ("q", C.c_int32 * 3), ("param", C.c_int32), ("if_outcome", C.c_int32),
                 ("angle", C.c_double), ("U", C.c_double * 32)]
 
 
@@ -90,6 +96,7 @@ _SIGS = {
     "smoq_state_destroy": [_vp],
     "smoq_state_upload": [_vp, _vp, C.c_size_t],
     "smoq_state_download": [_vp, _vp, C.c_size_t],
+    "smoq_state_download_range": [_vp, C.c_uint64, C.c_uint64, _vp],
     "smoq_state_set_basis": [_vp, C.c_uint64],
     "smoq_state_copy": [_vp, _vp],
     "smoq_apply_rx": [_vp, C.c_int, C.c_double],
@@ -117,6 +124,8 @@ _SIGS = {
     "smoq_apply_u2": [_vp, C.c_int, C.c_int, _dp, C.c_int],
     "smoq_apply_sequence": [_vp, C.POINTER(SmoqOp), C.c_int, _dp],
     "smoq_apply_sequence_unfused": [_vp, C.POINTER(SmoqOp), C.c_int, _dp],
+    "smoq_apply_circuit_mcwf": [_vp, C.POINTER(SmoqOp), C.c_int, _dp, C.c_uint64, C.c_uint64,
+                                C.POINTER(C.c_int32)],
     "smoq_expect_x": [_vp, C.c_int, _dp],
     "smoq_expect_y": [_vp, C.c_int, _dp],
     "smoq_expect_z": [_vp, C.c_int, _dp],

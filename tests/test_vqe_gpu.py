@@ -144,8 +144,10 @@ def test_gradient_configuration_n24(ctx):
     H = S.PauliSum(tfim_terms(N))
     e128, g128 = S.energy_and_gradient(ctx, circ, H, theta, dtype=S.C128)
     e64, g64 = S.energy_and_gradient(ctx, circ, H, theta, dtype=S.C64)
-    assert abs(e64[0] - e128[0]) < 1e-4, abs(e64[0] - e128[0])
-    assert np.max(np.abs(g64[0] - g128[0])) < 1e-4
+    print(f"N=24 energy c64-c128 {abs(e64[0] - e128[0]):.2e}, gradient {np.max(np.abs(g64[0] - g128[0])):.2e}")
+    # the batched complex64 target: energy error <= 1e-6 against complex128
+    assert abs(e64[0] - e128[0]) <= 1e-6, abs(e64[0] - e128[0])
+    assert np.max(np.abs(g64[0] - g128[0])) < 1e-5
     idx = np.linspace(0, 575, 16).astype(int)
     shifted = np.repeat(theta[None, :], 32, axis=0)
     for k, p in enumerate(idx):

@@ -72,6 +72,22 @@ def test_noalloc_matches_existing_entry_point_twice(ctx):
     assert np.max(np.abs(got2 - want2)) < 1e-12
 
 
+def test_noalloc_fills_its_fixed_scratch_exactly(ctx):
+    """2048 states x 32 observables = 65536 partial sums: one block per state,
+    the last partial at the array's final slot"""
+    rng = np.random.default_rng(202)
+    N, B = 6, 2048
+    a = S.CuState(ctx, N, S.C64, B, basis=None)
+    a.upload(np.stack([D.random_state(N, rng) for _ in range(B)]).astype(np.complex64))
+    masks = [int(m) for m in rng.integers(0, 1 << N, size=32)]
+    want = S.expect_zstrings(a, masks)
+    out, p = device_out(ctx, B * len(masks))
+    s, msg = call_noalloc(ctx, a, masks, p)
+    assert s == 0, msg
+    got = read_out(out, B * len(masks)).reshape(B, -1)
+    assert np.max(np.abs(got - want)) < 1e-12
+
+
 def test_noalloc_rejects_sizes_beyond_its_fixed_scratch(ctx):
     a = S.CuState(ctx, 6, S.C128, 1)
     out, p = device_out(ctx, 64)
