@@ -245,7 +245,7 @@ def vqe_measure(ctx, steps, warmup, B=8):
     parameters."""
     import torch
     import pysmoq as S
-    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", torch.cuda.current_device()))
     N, L = 24, 12
     ops, idx = [], 1
     for _ in range(L):
@@ -561,6 +561,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-vqe", action="store_true", help="skip the VQE gradient sub-record of the default line")
+    ap.add_argument("--autotune", type=int, default=0, help="time the compiled pass kernels' variants per pass (1)")
     # smaller cases of the same kernel (profiling, sweeps); the defaults are the workload
     ap.add_argument("--n-qubits", type=int, default=N_QUBITS)
     ap.add_argument("--trotter-steps", type=int, default=STEPS)
@@ -620,6 +621,8 @@ def main():
         ctx.set_option(S._lib.OPT_JIT_GROUPS, args.jit_groups)
     if args.jit_stage_bits != 4:
         ctx.set_option(S._lib.OPT_JIT_STAGE_BITS, args.jit_stage_bits)
+    if args.autotune:
+        ctx.set_option(S._lib.OPT_AUTOTUNE, 1)
     N = args.n_qubits
     tsteps = args.trotter_steps
     gate_apps = tsteps * 2 * (N + 3 * (N - 1))
@@ -665,6 +668,9 @@ def main():
 
     for _ in range(args.warmup):
         rec = device_step()
+    tune = ctx.tune_report() if args.autotune else ""
+    if tune:
+        sys.stderr.write(tune)
     ctx.reset_counters()
     clocks = Clocks(local)
     clocks.start()
@@ -724,6 +730,8 @@ def main():
                            "record_every": RECORD_EVERY, "gate_apps_per_step": gate_apps,
                            "state_bytes": (1 << N) * 8, "l2_policy": "inputs larger than L2 (2 GiB state)",
                            "parallelism": "replicas" if ws > 1 else "single_gpu",
+                           "autotune": bool(args.autotune),
+                           "tuned_passes": tune.count("->") if args.autotune else 0,
                            "tile_passes_per_step": passes, "hbm_gbs_effective":
                                2.0 * (1 << N) * 8 * passes / (ms / args.steps * 1e-3) / 1e9},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -75,9 +75,14 @@ enum {
     SMOQ_OPT_JIT_STAGE_BITS = 11, /* compiled pass kernels: tile bits per register stage, 4 (default) or 5
                                      (32-amplitude stages: fewer shared-memory round trips per pass;
                                      needs 2 groups per thread and scalar arithmetic) */
-    SMOQ_OPT_VQE_RESIDENT = 12    /* smoq_energy_grad_jobs: 1 (default) = circuits of N <= 13 (complex64)
+    SMOQ_OPT_VQE_RESIDENT = 12,   /* smoq_energy_grad_jobs: 1 (default) = circuits of N <= 13 (complex64)
                                      or N <= 12 (complex128) run together in one launch, each in one
                                      CTA's shared memory; 0 = every circuit through the tiled passes */
+    SMOQ_OPT_AUTOTUNE = 13        /* No counterpart in the reference.  1 = when a reusable complex64
+                                     program (a Trotter plan) is first run, time each compiled pass
+                                     kernel's variants (register groups per thread x CTAs per SM) on
+                                     a scratch state and keep the fastest; choices are cached per
+                                     (GPU, pass program), in the file SMOQ_TUNE_CACHE names if set */
 };
 smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long value);
 /* launches: kernels launched by this context; tile_passes/tile_ms/tile_bytes:
@@ -85,6 +90,9 @@ smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long value);
 smoq_status smoq_ctx_counters(smoq_ctx* ctx, long long* launches, long long* tile_passes,
                               double* tile_ms, double* tile_bytes);
 smoq_status smoq_ctx_reset_counters(smoq_ctx* ctx);
+/* No counterpart in the reference: the autotuner's per-pass timings (ms per
+ * launch of each variant) and choices so far, as text */
+smoq_status smoq_ctx_tune_report(smoq_ctx* ctx, char* buf, int len);
 /* the library's build identification, e.g. "smoq_cuda sm_100a" */
 const char* smoq_version(void);
 /* 1 when the plan compiler (engine 3) can run: NVRTC could be loaded */
@@ -358,6 +366,26 @@ typedef struct {           /* one Pauli-sum term: coef * prod of letters */
 smoq_status smoq_energy_grad(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* ops, int n,
                              int n_params, const smoq_pauli_term* H, int nterms, int batch,
                              const double* theta, double* energies, double* grads);
+/* Energy and adjoint gradient of a NOISY circuit along fixed trajectories: the
+ * ops of smoq_apply_circuit_mcwf (noise, measurements, resets, if_outcome) with
+ * its draws (trajectory t = traj_offset + 0 .. n_traj-1, from |0...0>).  With
+ * the draws fixed, each trajectory is a product of unitaries, drawn Paulis and
+ * normalised branch maps K (amplitude damping, collapse, reset); the gradient
+ * is the path-wise dE/dtheta of E = <psi_T|H|psi_T> (branches held fixed):
+ * lambda runs backwards through U^dag, and through a branch map as
+ * K^T (lambda - Re<psi'|lambda> psi').  A branch map cannot be uncomputed, so
+ * the forward pass stores the state in front of every checkpoint_every-th
+ * branch op and the backward pass restores the nearest one, replaying the
+ * recorded steps; memory: ceil(branch ops / checkpoint_every) + 2 states.  The
+ * reference's gradients treat noise as identity (cpuVQCEnzymeWrapper.jl:160-170,
+ * behind calculate_gradients, cpuVariationalQuantumCircuitGradients.jl:88);
+ * this differentiates the trajectories the noise produced, whose mean is the
+ * gradient of the mean energy.  energies[t] (host) and grads[t * n_params + p]
+ * (host, may be NULL); parameterised gates RX/RY/RZ/RXX/RYY/RZZ/CRY. */
+smoq_status smoq_energy_grad_mcwf(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* ops, int n, int n_params,
+                                  const smoq_pauli_term* H, int nterms, const double* theta, uint64_t seed,
+                                  uint64_t traj_offset, int n_traj, int checkpoint_every, double* energies,
+                                  double* grads);
 /* energy only (forward + reduction), same arguments */
 smoq_status smoq_energy(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* ops, int n,
                         int n_params, const smoq_pauli_term* H, int nterms, int batch,

@@ -3,11 +3,17 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <functional>
 #include <map>
 #include <memory>
+#include <mutex>
+#include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 #include "smoq_internal.h"
 #include "k_common.cuh"
@@ -155,6 +161,192 @@ struct EventPair {
     double bytes;
 };
 
+// ================================================================ autotuner
+// For every compiled pass of a reusable program (engine 3) the tuner times the
+// kernel variants -- 16-amplitude register groups per thread (2 or 1) x CTAs
+// per SM (the register budget's default, or one more) -- on a zeroed scratch
+// state of the program's size with CUDA events on the context's stream, and
+// keeps the fastest.  The variants apply the same literal FMA sequence to every
+// amplitude, so the choice changes the timing, never the result.  Choices are
+// cached per (GPU, pass program) for the life of the process and, when the
+// environment variable SMOQ_TUNE_CACHE names a file, across processes (one
+// line per pass program: key, variant).  Passes whose ops read per-state
+// runtime data (MCWF scales, decay tables, jumps) or carry an epilogue keep
+// the default variant.
+namespace {
+struct TuneVariant {
+    int groups, minb_add;
+};
+const TuneVariant kTuneVariants[] = {{2, 0}, {2, 1}, {1, 0}, {1, 1}};
+constexpr int kTuneVariantCount = 4;
+std::mutex g_tune_mu;
+std::map<uint64_t, int> g_tune;
+bool g_tune_loaded = false;
+
+uint64_t device_hash(int device) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
+    }
+    uint64_t h = 1469598103934665603ull;
+    for (const char* c = prop.name; *c; ++c) h = (h ^ (unsigned char)*c) * 1099511628211ull;
+    return (h ^ (uint64_t)prop.multiProcessorCount) * 1099511628211ull;
+}
+
+void tune_cache_load_locked() {
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* path = std::getenv("SMOQ_TUNE_CACHE");
+    if (!path || !*path) return;
+    std::ifstream f(path);
+    std::string key;
+    int v;
+    while (f >> key >> v)
+        if (v >= 0 && v < kTuneVariantCount) g_tune[std::strtoull(key.c_str(), nullptr, 16)] = v;
+}
+
+void tune_cache_store_locked(uint64_t key, int v) {
+    g_tune[key] = v;
+    const char* path = std::getenv("SMOQ_TUNE_CACHE");
+    if (!path || !*path) return;
+    std::ofstream f(path, std::ios::app);
+    char k[32];
+    std::snprintf(k, sizeof k, "%016llx", (unsigned long long)key);
+    f << k << " " << v << "\n";
+}
+
+bool tunable(const Pass& p) {
+    if (!p.jit || p.epilogue) return false;
+    for (const DevOp& op : p.ops)
+        if (op.kind == OPK_STATESCALE || op.kind == OPK_REALTAB || op.kind == OPK_JUMP) return false;
+    return true;
+}
+}  // namespace
+
+static smoq_status autotune_program(smoq_ctx* ctx, DevProgram& P, int N) {
+    std::vector<size_t> todo;
+    for (size_t i = 0; i < P.passes.size(); ++i)
+        if (tunable(P.passes[i]) && !P.passes[i].ops.empty()) todo.push_back(i);
+    if (todo.empty()) return SMOQ_OK;
+    const uint64_t dh = device_hash(ctx->device);
+    // the cached choices first
+    std::vector<uint64_t> keys(P.passes.size(), 0);
+    std::vector<size_t> fresh;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        tune_cache_load_locked();
+        for (size_t i : todo) {
+            keys[i] = jit_pass_key(P.passes[i], ctx->jit_buffers, ctx->jit_packed != 0) ^ dh;
+            auto it = g_tune.find(keys[i]);
+            if (it == g_tune.end()) {
+                fresh.push_back(i);
+                continue;
+            }
+            const TuneVariant& v = kTuneVariants[it->second];
+            std::string why;
+            if (const JitKernel* k = jit_pass_kernel(P.passes[i], ctx->jit_buffers, ctx->jit_packed != 0, v.groups, why,
+                                                     v.minb_add))
+                P.passes[i].jit = k;
+        }
+    }
+    if (fresh.empty()) return SMOQ_OK;
+    // scratch state: only when it fits twice over with a GiB to spare
+    const size_t bytes = (size_t)8 << N;
+    size_t free_b = 0, total_b = 0;
+    CK(ctx, cudaMemGetInfo(&free_b, &total_b));
+    if (free_b < 2 * bytes + ((size_t)1 << 30)) {
+        ctx->tune_report += "autotune skipped: no room for a scratch state\n";
+        return SMOQ_OK;
+    }
+    // compile every variant of every fresh pass on host threads (NVRTC is thread-safe per program)
+    std::vector<const JitKernel*> ks(fresh.size() * kTuneVariantCount, nullptr);
+    {
+        std::vector<std::thread> pool;
+        std::mutex next_mu;
+        size_t next = 0;
+        auto work = [&]() {
+            for (;;) {
+                size_t j;
+                {
+                    std::lock_guard<std::mutex> lk(next_mu);
+                    if (next >= ks.size()) return;
+                    j = next++;
+                }
+                const TuneVariant& v = kTuneVariants[j % kTuneVariantCount];
+                std::string why;
+                ks[j] = jit_pass_kernel(P.passes[fresh[j / kTuneVariantCount]], ctx->jit_buffers,
+                                        ctx->jit_packed != 0, v.groups, why, v.minb_add);
+            }
+        };
+        const size_t nt = std::max<size_t>(1, std::min<size_t>(ks.size(), std::thread::hardware_concurrency()));
+        for (size_t t = 1; t < nt; ++t) pool.emplace_back(work);
+        work();
+        for (std::thread& t : pool) t.join();
+    }
+    void* scratch = nullptr;
+    CK(ctx, cudaMallocAsync(&scratch, bytes, ctx->stream));
+    std::unique_ptr<void, std::function<void(void*)>> hold(scratch, [ctx](void* q) { cudaFreeAsync(q, ctx->stream); });
+    CK(ctx, cudaMemsetAsync(scratch, 0, bytes, ctx->stream));
+    cudaEvent_t e0, e1;
+    CK(ctx, cudaEventCreate(&e0));
+    CK(ctx, cudaEventCreate(&e1));
+    std::ostringstream rep;
+    for (size_t f = 0; f < fresh.size(); ++f) {
+        Pass& p = P.passes[fresh[f]];
+        TileArgs a;
+        a.psi = scratch;
+        a.state_len = (int64_t)1 << N;
+        a.tiles_per_state = (int64_t)1 << (N - p.g.T);
+        a.ntiles = a.tiles_per_state;
+        a.ops = P.d_ops + P.offs[fresh[f]];
+        a.nops = (int32_t)p.ops.size();
+        a.err = ctx->d_err;
+        a.g = p.g;
+        a.ep.partials = nullptr;
+        a.ep.npop = 0;
+        int best = -1;
+        float best_ms = 0;
+        rep << "pass " << fresh[f] << " (T " << p.g.T << ", L " << p.g.L << ", " << p.ops.size() << " ops):";
+        for (int v = 0; v < kTuneVariantCount; ++v) {
+            const JitKernel* k = ks[f * kTuneVariantCount + v];
+            if (!k) continue;
+            cudaError_t e = launch_jit(ctx, a, k, false);  // warm-up
+            cudaEventRecord(e0, ctx->stream);
+            for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = launch_jit(ctx, a, k, false);
+            cudaEventRecord(e1, ctx->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            if (e != cudaSuccess) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return cuda_fail(ctx, e, "autotune launch");
+            }
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms /= 3;
+            rep << " v" << v << " " << ms;
+            if (best < 0 || ms < best_ms) best = v, best_ms = ms;
+        }
+        rep << " -> v" << best << "\n";
+        if (best >= 0) {
+            p.jit = ks[f * kTuneVariantCount + best];
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            tune_cache_store_locked(keys[fresh[f]], best);
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    int32_t herr = 0;
+    CK(ctx, cudaMemcpy(&herr, ctx->d_err, sizeof(herr), cudaMemcpyDeviceToHost));
+    if (herr) {
+        CK(ctx, cudaMemset(ctx->d_err, 0, sizeof(int32_t)));
+        return fail(ctx, SMOQ_ERR_TIMEOUT, "autotune: a bounded device wait ran out");
+    }
+    ctx->tune_report += rep.str();
+    return SMOQ_OK;
+}
+
 static smoq_status run_program(smoq_ctx* ctx, smoq_state* st, const DevProgram& P, const Epilogue* ep,
                                std::vector<EventPair>* timing) {
     for (size_t i = 0; i < P.passes.size(); ++i) {
@@ -284,8 +476,16 @@ smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long v) {
             ctx->jit_buffers = (int)v;
             break;
         case SMOQ_OPT_VQE_RESIDENT: ctx->vqe_resident = v != 0; break;
+        case SMOQ_OPT_AUTOTUNE: ctx->autotune = v != 0; break;
         default: return fail(ctx, SMOQ_ERR_BADINPUT, "unknown option");
     }
+    return SMOQ_OK;
+}
+
+smoq_status smoq_ctx_tune_report(smoq_ctx* ctx, char* buf, int len) {
+    if (!ctx || !buf || len < 1) return SMOQ_ERR_BADINPUT;
+    std::strncpy(buf, ctx->tune_report.c_str(), (size_t)len - 1);
+    buf[len - 1] = 0;
     return SMOQ_OK;
 }
 
@@ -906,6 +1106,8 @@ static smoq_status get_block(smoq_plan* P, int nsteps, smoq_plan::Block** out) {
         return fail(P->ctx, SMOQ_ERR_BADINPUT, ex.what());
     }
     if (smoq_status s = upload_program(P->ctx, B->prog)) return s;
+    if (P->ctx->autotune && P->dtype == SMOQ_C64)
+        if (smoq_status s = autotune_program(P->ctx, B->prog, P->N)) return s;
     for (auto& p : B->prog.passes)
         if (!p.ops.empty()) B->kernels++;
     *out = B.get();

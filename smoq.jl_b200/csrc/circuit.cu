@@ -41,16 +41,7 @@ smoq_status smoq_internal_ops_to_ir(int N, const smoq_op* ops, int n, const doub
 namespace smoq {
 namespace {
 
-constexpr uint32_t kCircuitTag = 0x80000000u;  // counter word 1 of every circuit draw
 constexpr int kCircThreads = 256;
-
-enum BranchKind : int32_t { BR_AMPDAMP = 0, BR_MEASURE = 1, BR_RESET = 2 };
-
-__device__ __forceinline__ double circuit_draw(uint64_t seed, uint32_t op_index, uint64_t traj) {
-    uint32_t c[4] = {op_index, kCircuitTag, (uint32_t)traj, (uint32_t)(traj >> 32)};
-    philox10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
-    return u01_53(c[0], c[1]);
-}
 
 // the trajectory's condition: if_outcome slot `cond` (0-based, -1 = always)
 __device__ __forceinline__ bool cond_met(const int32_t* outcomes, int n_meas, int64_t b, int cond) {
@@ -65,20 +56,6 @@ struct PauliNoise {
     double p;
 };
 
-// code of the Pauli a trajectory applies: 0 I, 1 X, 2 Y, 3 Z
-__device__ __forceinline__ int pauli_code(const PauliNoise& nz, double u) {
-    switch (nz.type) {
-        case SMOQ_N_DEPOLARIZING:  // cpuQuantumChannelKrausOperators.jl:285-318
-            return u < nz.p / 3 ? 1 : (u < 2 * nz.p / 3 ? 2 : (u < nz.p ? 3 : 0));
-        case SMOQ_N_BIT_FLIP:      // :321-334
-            return u < nz.p ? 1 : 0;
-        case SMOQ_N_PHASE_FLIP:    // :337-347
-            return u < nz.p ? 3 : 0;
-        default:                   // dephasing / phase damping, :262-282: Z with q = (1 - sqrt(1 - p)) / 2
-            return u < (1.0 - sqrt(1.0 - nz.p)) / 2.0 ? 3 : 0;
-    }
-}
-
 template <typename R>
 __global__ void __launch_bounds__(kCircThreads) pauli_noise_kernel(typename CT<R>::T* psi, int N, PauliNoise nz,
                                                                    uint64_t seed, uint64_t traj0,
@@ -86,7 +63,7 @@ __global__ void __launch_bounds__(kCircThreads) pauli_noise_kernel(typename CT<R
     using C = typename CT<R>::T;
     const int64_t b = blockIdx.y;
     if (!cond_met(outcomes, n_meas, b, nz.cond)) return;
-    const int code = pauli_code(nz, circuit_draw(seed, nz.op_index, traj0 + (uint64_t)b));
+    const int code = pauli_code(nz.type, nz.p, circuit_draw(seed, nz.op_index, traj0 + (uint64_t)b));
     if (code == 0) return;
     C* s = psi + (b << N);
     const uint64_t npairs = (uint64_t)1 << (N - 1), bit = (uint64_t)1 << nz.q;
@@ -151,50 +128,6 @@ struct Branch {
     double gamma;        // amplitude damping
 };
 
-// The branch of one trajectory from its halves s0 = sum_{bit q = 0} |psi|^2,
-// s1 = sum_{bit q = 1} |psi|^2 and its draw u, as the real 2x2 map K on the
-// qubit's pairs (a0, a1) -> (K00 a0 + K01 a1, K10 a0 + K11 a1), the reference's
-// renormalisation included; *outcome = the recorded bit (measurements) or -1.
-__device__ __forceinline__ void branch_map(const Branch& br, double s0, double s1, double u, double K[4],
-                                           int* outcome) {
-    K[0] = 1, K[1] = 0, K[2] = 0, K[3] = 1;
-    *outcome = -1;
-    if (br.kind == BR_AMPDAMP) {
-        // _apply_amplitude_damping_single! (cpuQuantumChannelKrausOperators.jl:350-386):
-        // jump with probability gamma * pop_1 (and pop_1 > 1e-12), else damp |1> by
-        // sqrt(1 - gamma); then divide by the norm when it exceeds 1e-12
-        if (u < br.gamma * s1 && s1 > 1e-12) {
-            const double n = sqrt(s1);           // the jumped state's norm: sigma- keeps |psi_1|
-            K[0] = 0, K[1] = n > 1e-12 ? 1.0 / n : 1.0, K[3] = 0;
-        } else {
-            const double d = sqrt(1.0 - br.gamma), n = sqrt(s0 + (1.0 - br.gamma) * s1);
-            const double f = n > 1e-12 ? 1.0 / n : 1.0;
-            K[0] = f, K[3] = d * f;
-        }
-        return;
-    }
-    // _measure_z_single! (cpuQuantumStateMeasurements.jl:224-255): outcome 0 iff
-    // u < P(0) = s0; keep that half, divide by its norm
-    const int m = u < s0 ? 0 : 1;
-    const double f = 1.0 / sqrt(m ? s1 : s0);
-    if (br.kind == BR_MEASURE) {
-        *outcome = m;
-        K[0] = m ? 0.0 : f;
-        K[3] = m ? f : 0.0;
-        return;
-    }
-    // reset_state! (:555): the measurement, then _force_qubit_state! (:584-632):
-    // the kept amplitude moves to the target's half; :plus / :minus add a Hadamard
-    K[0] = K[1] = K[2] = K[3] = 0;
-    const double h = f * 0.70710678118654752440;
-    switch (br.target) {
-        case 0: K[m] = f; break;                       // row 0 takes column m
-        case 1: K[2 + m] = f; break;                   // row 1 takes column m
-        case 2: K[m] = h, K[2 + m] = h; break;         // (|0> + |1>) / sqrt 2
-        default: K[m] = h, K[2 + m] = -h; break;       // (|0> - |1>) / sqrt 2
-    }
-}
-
 template <typename R>
 __global__ void __launch_bounds__(kCircThreads) branch_kernel(typename CT<R>::T* psi, int N, Branch br,
                                                               const double* partials, uint64_t seed,
@@ -210,7 +143,7 @@ __global__ void __launch_bounds__(kCircThreads) branch_kernel(typename CT<R>::T*
         for (int k = 0; k < br.nblk; ++k) s0 += p[2 * k], s1 += p[2 * k + 1];
         double K[4];
         int m;
-        branch_map(br, s0, s1, circuit_draw(seed, br.op_index, traj0 + (uint64_t)b), K, &m);
+        branch_map(br.kind, br.target, br.gamma, s0, s1, circuit_draw(seed, br.op_index, traj0 + (uint64_t)b), K, &m);
         for (int k = 0; k < 4; ++k) sK[k] = K[k];
         if (blockIdx.x == 0 && m >= 0) outcomes[b * n_meas + br.out_slot] = m;
     }

@@ -662,13 +662,15 @@ struct Gen {
 };
 
 // full source of the kernels for one pass
-std::string generate(const Pass& p, bool need_epi, int nbuf, bool packed, int groups, std::string& err) {
+std::string generate(const Pass& p, bool need_epi, int nbuf, bool packed, int groups, int minb_add, std::string& err) {
     const int N = p.g.N;
     const TileGeom& g = p.g;
     const int T = g.T;
     // G register groups of 16 amplitudes per thread, NT = 2^(T-4) / G threads
-    // register budget: 128 per thread with two groups, 64 with one
-    const int G = packed ? 2 : groups, NT = 1 << (T - 4 - (G - 1)), MINB = 65536 / (NT * (G == 2 ? 128 : 64));
+    // register budget: 128 per thread with two groups, 64 with one; minb_add asks
+    // for that many more CTAs per SM (a tighter register cap, at most 32 a thread)
+    const int G = packed ? 2 : groups, NT = 1 << (T - 4 - (G - 1));
+    const int MINB = std::min(65536 / (NT * (G == 2 ? 128 : 64)) + std::max(0, minb_add), 65536 / (NT * 32));
     Gen gen(p, G, NT);
     std::ostringstream& o = gen.o;
     o << kPrelude;
@@ -856,6 +858,13 @@ std::string generate(const Pass& p, bool need_epi, int nbuf, bool packed, int gr
 std::mutex g_mu;
 std::map<std::string, std::unique_ptr<JitKernel>> g_cache;
 
+// FNV-1a of a kernel source: the key of a pass program in the tuning cache
+uint64_t fnv1a(const std::string& s) {
+    uint64_t h = 1469598103934665603ull;
+    for (unsigned char c : s) h = (h ^ c) * 1099511628211ull;
+    return h;
+}
+
 }  // namespace
 
 namespace {
@@ -907,7 +916,7 @@ bool jit_check_pass(const Pass& p, int nbuf, bool packed, int groups, std::strin
         err = "jit: only stage-scheduled passes of tile width 12-13";
         return false;
     }
-    const std::string src = generate(p, p.epilogue, nbuf, packed, groups, err);
+    const std::string src = generate(p, p.epilogue, nbuf, packed, groups, 0, err);
     if (src.empty()) return false;
     std::vector<char> cubin;
     if (!compile_cubin(src, cubin, err, info)) return false;
@@ -917,18 +926,24 @@ bool jit_check_pass(const Pass& p, int nbuf, bool packed, int groups, std::strin
 
 // Compile (or fetch) the kernel of a stage-scheduled complex64 pass and load
 // it into the current device.  Returns nullptr and fills `err` on failure.
-const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, int groups, std::string& err) {
+const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, int groups, std::string& err, int minb_add) {
     if (!p.staged || (p.g.T != 12 && p.g.T != 13)) {
         err = "jit: only stage-scheduled passes of tile width 12-13";
         return nullptr;
     }
-    std::string src = generate(p, p.epilogue, nbuf, packed, groups, err);
+    std::string src = generate(p, p.epilogue, nbuf, packed, groups, minb_add, err);
     if (src.empty()) return nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        auto it = g_cache.find(src);
+        if (it != g_cache.end()) return it->second.get();
+    }
+    // compile outside the lock: several host threads may compile different passes at once
+    std::vector<char> cubin;
+    if (!compile_cubin(src, cubin, err)) return nullptr;
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_cache.find(src);
     if (it != g_cache.end()) return it->second.get();
-    std::vector<char> cubin;
-    if (!compile_cubin(src, cubin, err)) return nullptr;
     std::unique_ptr<JitKernel> k(new JitKernel());
     cudaLibrary_t lib = nullptr;
     cudaError_t e = cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
@@ -965,6 +980,12 @@ const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, int group
 }
 
 bool jit_available() { return nvrtc().ok; }
+
+uint64_t jit_pass_key(const Pass& p, int nbuf, bool packed) {
+    std::string err;
+    const std::string src = generate(p, p.epilogue, nbuf, packed, 2, 0, err);
+    return src.empty() ? 0 : fnv1a(src);
+}
 
 cudaError_t launch_jit(smoq_ctx* ctx, const TileArgs& a, const JitKernel* k, bool epi) {
     const void* fn = k->fn[epi ? 1 : 0];

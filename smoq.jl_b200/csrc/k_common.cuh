@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "smoq_internal.h"
+#include "circuit_common.cuh"
 
 namespace smoq {
 
@@ -122,28 +123,8 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 }
 
 // ------------------------------------------------------------ random numbers
-// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): the published rounds and
-// constants, the same as the oracle's so_philox4x32_10.  c is the counter (in
-// place: it becomes the four output words), (k0, k1) the key.
-__device__ __forceinline__ void philox10(uint32_t c[4], uint32_t k0, uint32_t k1) {
-#pragma unroll
-    for (int r = 0; r < 10; ++r) {
-        const uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
-        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
-        const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
-        c[0] = n0;
-        c[1] = lo1;
-        c[2] = n2;
-        c[3] = lo0;
-        k0 += 0x9E3779B9u;
-        k1 += 0xBB67AE85u;
-    }
-}
-// 53-bit uniform in [0, 1): 27 bits of hi, 26 bits of lo (so_u01_from_words)
-__device__ __forceinline__ double u01_53(uint32_t hi, uint32_t lo) {
-    const uint64_t a = hi >> 5, b = lo >> 6;
-    return (double)(a * 67108864ull + b) * (1.0 / 9007199254740992.0);
-}
+// philox10 / u01_53 (Philox4x32-10 and its 53-bit uniform) live in
+// circuit_common.cuh with the other per-trajectory rules.
 
 // ------------------------------------------------------------ op application
 // Apply one fused op to the amplitude array `psi` indexed by I.  `bits` are

@@ -102,6 +102,15 @@ struct TileArgs {
     Epilogue ep;
 };
 
+// One Pauli-sum term on the device: coef * i^ny * X^x Z^z (ny = popcount(x & z),
+// the Y letters: Y = i X Z)
+struct HamTerm {
+    double coef;
+    uint64_t x, z;
+    int32_t ny;
+    int32_t pad;
+};
+
 // ----------------------------------------------------------------------------
 // Host-side gate IR consumed by the planner.
 // ----------------------------------------------------------------------------
@@ -163,7 +172,11 @@ void schedule_regtile(Pass& p);
 void schedule_stages(Pass& p, int amp_bytes, int K = 4);
 void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op);
 // jit.cpp: compile (or fetch from the process cache) the kernel of a staged complex64 pass
-const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, int groups, std::string& err);
+// (minb_add: that many more CTAs per SM than the default register budget allows)
+const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, int groups, std::string& err,
+                                 int minb_add = 0);
+// the tuning-cache key of a staged pass program (hash of its default kernel source)
+uint64_t jit_pass_key(const Pass& p, int nbuf, bool packed);
 // jit.cpp: generate and compile a staged complex64 pass without a GPU (plan checks)
 bool jit_check_pass(const Pass& p, int nbuf, bool packed, int groups, std::string& err, size_t* cubin_bytes,
                     std::string* info);
@@ -204,6 +217,8 @@ struct smoq_ctx {
     int jit_groups = 2;                // compiled pass kernels: 16-amplitude register groups per thread
     int jit_stage_bits = 4;            // compiled pass kernels: tile bits per register stage (4 or 5)
     bool vqe_resident = true;          // many-circuit VQE: small circuits in one shared-memory launch
+    bool autotune = false;             // time the compiled kernels' variants per pass at plan upload
+    std::string tune_report;           // the tuner's per-pass timings and choices
     long long launches = 0;            // kernels launched by this ctx
     long long tile_passes = 0;
     double tile_ms = 0;                // summed tile-pass time when kernel_timing
@@ -244,5 +259,9 @@ cudaError_t stage_kernels_init(smoq_ctx* ctx);
 cudaError_t launch_stage(smoq_ctx* ctx, const TileArgs& a, int dtype, bool epi);
 cudaError_t launch_jit(smoq_ctx* ctx, const TileArgs& a, const JitKernel* k, bool epi);
 cudaError_t vqe_kernels_init(smoq_ctx* ctx);
+// lam = H psi for one state (vqe.cu); per block the FP64 partials of Re<psi|lam>
+// (d_part[blk]) and <psi|psi> (d_part[eblocks + blk])
+cudaError_t launch_ham_apply(smoq_ctx* ctx, const smoq_state* st, void* lam, const HamTerm* d_terms, int nterms,
+                             double* d_part, int eblocks);
 cudaError_t qrc_kernels_init(smoq_ctx* ctx);
 }  // namespace smoq

@@ -37,13 +37,6 @@
 
 namespace smoq {
 
-struct HamTerm {
-    double coef;
-    uint64_t x, z;
-    int32_t ny;
-    int32_t pad;
-};
-
 // lambda_k = sum_t c_t i^{ny} (-1)^{popc((k ^ x) & z)} phi_{k ^ x}; per block
 // the FP64 partial sums of Re(conj(phi_k) lambda_k) (partials[blockIdx.x])
 // and of |phi_k|^2 (partials[gridDim.x + blockIdx.x]), so the caller can
@@ -89,6 +82,18 @@ __global__ void __launch_bounds__(256) ham_apply_kernel(const typename CT<R>::T*
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
         partials[threadIdx.x * gridDim.x + blockIdx.x] = s;
     }
+}
+
+cudaError_t launch_ham_apply(smoq_ctx* ctx, const smoq_state* st, void* lam, const HamTerm* d_terms, int nterms,
+                             double* d_part, int eblocks) {
+    if (st->dtype == SMOQ_C64)
+        ham_apply_kernel<float><<<eblocks, 256, 0, ctx->stream>>>((const float2*)st->ptr, (float2*)lam, st->N, d_terms,
+                                                                  nterms, d_part);
+    else
+        ham_apply_kernel<double><<<eblocks, 256, 0, ctx->stream>>>((const double2*)st->ptr, (double2*)lam, st->N,
+                                                                   d_terms, nterms, d_part);
+    ctx->launches++;
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- backward sweep

@@ -80,6 +80,12 @@ class Context:
     def reset_counters(self):
         ck(lib.smoq_ctx_reset_counters(self.h), self.h)
 
+    def tune_report(self) -> str:
+        """the autotuner's per-pass variant timings (ms per launch) and choices"""
+        buf = C.create_string_buffer(1 << 16)
+        ck(lib.smoq_ctx_tune_report(self.h, buf, len(buf)), self.h)
+        return buf.value.decode()
+
     @property
     def stream(self) -> int:
         return lib.smoq_ctx_stream(self.h)

@@ -19,7 +19,8 @@ C64, C128 = 0, 1
  G_CRY, G_CCZ, G_TOFFOLI, G_U1, G_U2) = range(21)
 
 (OPT_TILE_BITS_C64, OPT_TILE_BITS_C128, OPT_LOW_BITS_C64, OPT_LOW_BITS_C128, OPT_USE_GRAPHS, OPT_KERNEL_TIMING,
- OPT_ENGINE, OPT_JIT_BUFFERS, OPT_JIT_PACKED, OPT_JIT_GROUPS, OPT_JIT_STAGE_BITS, OPT_VQE_RESIDENT) = range(1, 13)
+ OPT_ENGINE, OPT_JIT_BUFFERS, OPT_JIT_PACKED, OPT_JIT_GROUPS, OPT_JIT_STAGE_BITS, OPT_VQE_RESIDENT,
+ OPT_AUTOTUNE) = range(1, 14)
 
 
 # operations of smoq_apply_circuit_mcwf beyond the gates (one qubit each)
@@ -91,6 +92,7 @@ _SIGS = {
     "smoq_ctx_set_option": [_vp, C.c_int, C.c_longlong],
     "smoq_ctx_counters": [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), _dp, _dp],
     "smoq_ctx_reset_counters": [_vp],
+    "smoq_ctx_tune_report": [_vp, C.c_char_p, C.c_int],
     "smoq_state_create": [_vp, C.c_int, C.c_int, C.c_int, C.POINTER(_vp)],
     "smoq_state_wrap": [_vp, _vp, C.c_int, C.c_int, C.c_int, C.POINTER(_vp)],
     "smoq_state_destroy": [_vp],
@@ -166,6 +168,8 @@ _SIGS = {
                                  C.POINTER(SmoqPassInfo), C.c_int, C.POINTER(SmoqFusedOpInfo), C.c_int, _ip, _ip],
     "smoq_energy": [_vp, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, C.c_int, C.POINTER(SmoqPauliTerm),
                     C.c_int, C.c_int, _dp, _dp],
+    "smoq_energy_grad_mcwf": [_vp, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, C.c_int, C.POINTER(SmoqPauliTerm),
+                              C.c_int, _dp, C.c_uint64, C.c_uint64, C.c_int, C.c_int, _dp, _dp],
 }
 
 for _name, _args in _SIGS.items():
