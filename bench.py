@@ -150,7 +150,6 @@ def measured_peak():
 
 
 ENGINE_KERNELS = {0: ("tile_pass_kernel<float>", "tile_pass_xxz_n28_c64.json"),
-                  1: ("regtile_kernel<float>", None),
                   2: ("stage_kernel<float>", None),
                   3: ("smoq_pass_e0 (compiled per pass)", "compiled_pass_xxz_n28_c64.json")}
 
@@ -512,10 +511,6 @@ def bandwidth_workload(args):
     ctx = S.Context(0)
     if args.engine >= 0:
         ctx.set_option(S._lib.OPT_ENGINE, args.engine)
-    if args.jit_packed:
-        ctx.set_option(S._lib.OPT_JIT_PACKED, args.jit_packed)
-    if args.jit_stage_bits != 4:
-        ctx.set_option(S._lib.OPT_JIT_STAGE_BITS, args.jit_stage_bits)
     peak, peak_kind = measured_peak()
     out = {}
     for N, dt, name in ((32, S.C64, "n32_c64"), (31, S.C128, "n31_c128")):
@@ -561,7 +556,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-vqe", action="store_true", help="skip the VQE gradient sub-record of the default line")
-    ap.add_argument("--autotune", type=int, default=0, help="time the compiled pass kernels' variants per pass (1)")
+    ap.add_argument("--autotune", type=int, default=-1,
+                    help="compiled pass kernels: per-pass variant tuning (-1 library default = on, 0 off, 1 on)")
     # smaller cases of the same kernel (profiling, sweeps); the defaults are the workload
     ap.add_argument("--n-qubits", type=int, default=N_QUBITS)
     ap.add_argument("--trotter-steps", type=int, default=STEPS)
@@ -569,9 +565,7 @@ def main():
     ap.add_argument("--low-bits", type=int, default=0, help="complex64 contiguous low qubits per tile segment (0 = default)")
     ap.add_argument("--engine", type=int, default=-1, help="fused-pass engine (-1 = library default)")
     ap.add_argument("--jit-buffers", type=int, default=1, help="compiled pass kernels: tile buffers per CTA (1, 2)")
-    ap.add_argument("--jit-packed", type=int, default=0, help="compiled pass kernels: FP32x2 arithmetic (1) or scalar (0)")
     ap.add_argument("--jit-groups", type=int, default=2, help="compiled pass kernels: register groups per thread (1, 2)")
-    ap.add_argument("--jit-stage-bits", type=int, default=4, help="compiled pass kernels: bits per register stage (4, 5)")
     ap.add_argument("--trajectories", type=int, default=4096, help="qrc workload: trajectories")
     ap.add_argument("--inputs", type=int, default=100, help="qrc workload: length of the input series")
     ap.add_argument("--workload", default="trotter", choices=["trotter", "vqe", "vqe_jobs", "mcwf", "bandwidth", "qrc"],
@@ -615,14 +609,10 @@ def main():
         ctx.set_option(S._lib.OPT_ENGINE, args.engine)
     if args.jit_buffers != 1:
         ctx.set_option(S._lib.OPT_JIT_BUFFERS, args.jit_buffers)
-    if args.jit_packed:
-        ctx.set_option(S._lib.OPT_JIT_PACKED, args.jit_packed)
     if args.jit_groups != 2:
         ctx.set_option(S._lib.OPT_JIT_GROUPS, args.jit_groups)
-    if args.jit_stage_bits != 4:
-        ctx.set_option(S._lib.OPT_JIT_STAGE_BITS, args.jit_stage_bits)
-    if args.autotune:
-        ctx.set_option(S._lib.OPT_AUTOTUNE, 1)
+    if args.autotune >= 0:
+        ctx.set_option(S._lib.OPT_AUTOTUNE, args.autotune)
     N = args.n_qubits
     tsteps = args.trotter_steps
     gate_apps = tsteps * 2 * (N + 3 * (N - 1))
@@ -668,7 +658,7 @@ def main():
 
     for _ in range(args.warmup):
         rec = device_step()
-    tune = ctx.tune_report() if args.autotune else ""
+    tune = ctx.tune_report()
     if tune:
         sys.stderr.write(tune)
     ctx.reset_counters()
@@ -730,8 +720,9 @@ def main():
                            "record_every": RECORD_EVERY, "gate_apps_per_step": gate_apps,
                            "state_bytes": (1 << N) * 8, "l2_policy": "inputs larger than L2 (2 GiB state)",
                            "parallelism": "replicas" if ws > 1 else "single_gpu",
-                           "autotune": bool(args.autotune),
-                           "tuned_passes": tune.count("->") if args.autotune else 0,
+                           "autotune": args.autotune != 0,
+                           "tuned_variants": {v: tune.count("-> " + v) for v in ("v0", "v1", "v2", "v3", "v4", "v5")
+                                              if tune.count("-> " + v)},
                            "tile_passes_per_step": passes, "hbm_gbs_effective":
                                2.0 * (1 << N) * 8 * passes / (ms / args.steps * 1e-3) / 1e9},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

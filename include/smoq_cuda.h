@@ -60,29 +60,25 @@ enum {
     SMOQ_OPT_USE_GRAPHS = 5,      /* capture Trotter blocks as CUDA graphs (default 1) */
     SMOQ_OPT_KERNEL_TIMING = 6,   /* bracket fused passes with CUDA events (default 0) */
     SMOQ_OPT_ENGINE = 7           /* fused-pass engine: -1 auto (default), 0 shared-memory sweeps,
-                                     1 register tiles, 2 stage sweeps (4-bit register stages, tile
-                                     widths 12-13), 3 compiled pass kernels (engine 2's schedule,
-                                     each complex64 pass compiled with NVRTC at upload; needs
-                                     libnvrtc).  Auto: reusable complex64 programs (Trotter plans,
-                                     MCWF) run engine 3 when NVRTC loads, everything else engine 0 */,
+                                     2 stage sweeps (4-bit register stages, tile widths 12-13),
+                                     3 compiled pass kernels (engine 2's schedule, each complex64 pass
+                                     compiled with NVRTC at upload; needs libnvrtc).  Auto: reusable
+                                     complex64 programs (Trotter plans, MCWF) run engine 3 when NVRTC
+                                     loads, everything else engine 0 */,
     SMOQ_OPT_JIT_BUFFERS = 8,     /* compiled pass kernels: tile buffers per CTA, 1 (default) or 2 (the next
                                      tile's bulk load runs under the current tile's stages) */
-    SMOQ_OPT_JIT_PACKED = 9       /* compiled pass kernels: 0 (default) = scalar FP32; 1 = FP32x2 arithmetic,
-                                     a thread's two register groups as one 64-bit pair (more registers
-                                     per thread; measured slower on B200) */,
     SMOQ_OPT_JIT_GROUPS = 10,     /* compiled pass kernels: 16-amplitude register groups per thread, 2
                                      (default; 2^(T-5) threads) or 1 (2^(T-4) threads) */
-    SMOQ_OPT_JIT_STAGE_BITS = 11, /* compiled pass kernels: tile bits per register stage, 4 (default) or 5
-                                     (32-amplitude stages: fewer shared-memory round trips per pass;
-                                     needs 2 groups per thread and scalar arithmetic) */
     SMOQ_OPT_VQE_RESIDENT = 12,   /* smoq_energy_grad_jobs: 1 (default) = circuits of N <= 13 (complex64)
                                      or N <= 12 (complex128) run together in one launch, each in one
                                      CTA's shared memory; 0 = every circuit through the tiled passes */
-    SMOQ_OPT_AUTOTUNE = 13        /* No counterpart in the reference.  1 = when a reusable complex64
-                                     program (a Trotter plan) is first run, time each compiled pass
-                                     kernel's variants (register groups per thread x CTAs per SM) on
-                                     a scratch state and keep the fastest; choices are cached per
-                                     (GPU, pass program), in the file SMOQ_TUNE_CACHE names if set */
+    SMOQ_OPT_AUTOTUNE = 13        /* No counterpart in the reference.  1 (default) = when a reusable
+                                     complex64 program (a Trotter plan) of N >= 20 is first run, time
+                                     each compiled pass kernel's variants (register groups per thread,
+                                     CTAs per SM, one or two tile buffers) on a scratch state and keep
+                                     the fastest (the variants compute bit-identical results); choices
+                                     are cached per (GPU, pass program), across processes in the file
+                                     SMOQ_TUNE_CACHE names if set; 0 = the SMOQ_OPT_JIT_* settings */
 };
 smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long value);
 /* launches: kernels launched by this context; tile_passes/tile_ms/tile_bytes:
@@ -421,6 +417,21 @@ smoq_status smoq_energy_grad_jobs(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vq
  * the building block of Chebyshev and Lanczos.  in and out: same shape, not aliased. */
 smoq_status smoq_apply_pauli_sum(smoq_state* in, smoq_state* out, const smoq_pauli_term* H, int nterms,
                                  double* expect);
+/* apply_hamiltonian_bitwise!(psi_out, psi_in, params::HamiltonianParams)
+ * (cpuQuantumChannelUnitaryEvolutionChebyshev.jl:55): out = H in for the
+ * HamiltonianParams (cpuHamiltonianBuilder.jl:69) given as its x_bonds and
+ * y_bonds, rows (i, j, Jxx, Jyy, Jzz) of CouplingTerm (:42), and fields, rows
+ * (idx, hx, hy, hz) of FieldTerm (:51), with 0-based sites; terms with a zero
+ * coefficient are skipped as the reference skips them.  The Y field is the
+ * Pauli Y of construct_sparse_hamiltonian (cpuHamiltonianBuilder.jl:297) and
+ * apply_Y! (cpuQuantumStateLanczos.jl:84); the reference's pull loop
+ * (Chebyshev.jl:142) applies its transpose, -hy Y.  in, out: same shape, not aliased. */
+smoq_status smoq_apply_hamiltonian_bitwise(smoq_state* out, smoq_state* in, const double* x_bonds, int nx,
+                                           const double* y_bonds, int ny, const double* fields, int nf);
+/* apply_H_xxz!(psi, out, N, Jx, Jy, Jz, h) (cpuQuantumStateLanczos.jl:157): out = Jx sum X_i X_{i+1}
+ * + Jy sum Y_i Y_{i+1} + Jz sum Z_i Z_{i+1} + h sum X_i on the open chain; apply_H_ising!
+ * (:220) is Jx = Jy = 0 */
+smoq_status smoq_apply_h_xxz(smoq_state* psi, smoq_state* out, double Jx, double Jy, double Jz, double h);
 
 /* ------------------------------------------------------- density matrices */
 /* A density matrix of N qubits (N <= 16) is a smoq_state of 2N qubits holding
@@ -465,11 +476,11 @@ smoq_status smoq_measure_qubit(smoq_state* st, int q, unsigned long long seed, u
 /* ------------------------------------------------- host-only introspection */
 /* No counterpart in the reference.  Runs the fused-pass planner (host code,
  * no GPU or context needed) on a gate sequence exactly as
- * smoq_apply_sequence would and reports, per pass, the tile geometry and the
- * fused ops (kind = 0 dense 2x2, 1 dense 4x4, 2 parity 4x4, 3 monomial,
- * 4 diagonal, 8 register-tile layout change; coefficients as the kernels read
- * them), scheduled for the default register-tile engine.  Counts are written
- * even when the output arrays are too small (NULL arrays allowed). */
+ * smoq_apply_sequence would with `engine` (0, 2 or 3) and reports, per pass,
+ * the tile geometry and the fused ops (kind = 0 dense 2x2, 1 dense 4x4,
+ * 2 parity 4x4, 3 monomial, 4 diagonal, 10 stage header of engines 2-3;
+ * coefficients as the kernels read them).  Counts are written even when the
+ * output arrays are too small (NULL arrays allowed). */
 typedef struct {
     int32_t T, L, H, nops;
     int32_t hb[24];
@@ -477,18 +488,18 @@ typedef struct {
 typedef struct {
     int32_t kind, nq;
     int32_t lb[4], gb[4];
-    int32_t perm[8];       /* monomial permutation; kind 8 (register layout): register / warp bits */
-    int32_t slot[4];       /* register-tile placement of each qubit: type << 8 | index */
-    int32_t mode;          /* 1 = applied through shared memory */
+    int32_t perm[8];       /* monomial permutation; stage header (kind 10): the stage's 4 tile bits,
+                              then the lane bit rotating each */
+    int32_t slot[4];       /* engines 2-3: the stage position of each qubit */
+    int32_t mode;          /* unused */
     double c[32];          /* 16 interleaved complex coefficients */
 } smoq_fused_op_info;
 /* Host-only check of the plan compiler (engine 3): plans `ops` as smoq_apply_sequence
  * would with engine 3 and compiles every complex64 pass kernel with NVRTC, without a GPU
  * and without loading them.  flags: 1 = return the compiler's register/spill report in msg,
- * 2 = two tile buffers per CTA (SMOQ_OPT_JIT_BUFFERS 2), 4 = FP32x2 arithmetic (SMOQ_OPT_JIT_PACKED 1),
- * 8 = one register group per thread (SMOQ_OPT_JIT_GROUPS 1), 16 = 5-bit stages (SMOQ_OPT_JIT_STAGE_BITS 5).  *n_compiled = kernels compiled; msg
- * gets "ok" (or the report) or the first error.  SMOQ_ERR_UNSUPPORTED when NVRTC is not
- * available. */
+ * 2 = two tile buffers per CTA (SMOQ_OPT_JIT_BUFFERS 2), 8 = one register group per thread
+ * (SMOQ_OPT_JIT_GROUPS 1).  *n_compiled = kernels compiled; msg gets "ok" (or the report)
+ * or the first error.  SMOQ_ERR_UNSUPPORTED when NVRTC is not available. */
 smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops, int n,
                                     const double* theta, int flags, int* n_compiled, char* msg, int msg_len);
 smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tile_bits, int low_bits, int engine,

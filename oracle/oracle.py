@@ -119,6 +119,8 @@ _sig("so_reset_u", [_cp, C.c_int, C.c_int, C.c_int, C.c_double])
 _sig("so_circuit_draw", [C.c_uint64, C.c_uint32, C.c_uint64], C.c_double)
 _sig("so_apply_circuit_mcwf", [_cp, C.POINTER(Op), C.c_int, _dp, C.c_int, C.c_uint64, C.c_uint64,
                                C.POINTER(C.c_int)], C.c_int)
+_sig("so_apply_hamiltonian_bitwise", [_cp, _cp, _dp, C.c_int, _dp, C.c_int, _dp, C.c_int, C.c_int])
+_sig("so_apply_H_xxz", [_cp, _cp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double])
 _sig("so_set_threads", [C.c_int])
 _sig("so_get_threads", [], C.c_int)
 
@@ -323,6 +325,36 @@ def apply_circuit_mcwf(psi, ops_arr, n, theta, N, seed, traj):
     m = L.so_apply_circuit_mcwf(_p(psi), ops_arr, n, th.ctypes.data_as(_dp), N, seed, traj,
                                 out.ctypes.data_as(C.POINTER(C.c_int)))
     return out[:m]
+
+
+def noisy_energy(ops_arr, n, theta, N, terms, seed, traj):
+    """<psi_T|H|psi_T> of one trajectory of a noisy circuit from |0...0>"""
+    coef, s = pauli_strings(terms, N)
+    psi = zero_state(N, 0)
+    apply_circuit_mcwf(psi, ops_arr, n, theta, N, seed, traj)
+    return L.so_pauli_sum_expect(_p(psi), len(terms), coef.ctypes.data_as(_dp), s, N)
+
+
+def _rows(rows, width):
+    a = np.ascontiguousarray(np.asarray(rows, dtype=np.float64).reshape(-1, width))
+    return a, a.shape[0]
+
+
+def apply_hamiltonian_bitwise(psi_in, x_bonds, y_bonds, fields, N):
+    """out = H psi_in for bond rows (i, j, Jxx, Jyy, Jzz) and field rows (idx, hx, hy, hz), 1-based"""
+    out = np.zeros_like(psi_in)
+    xb, nx = _rows(x_bonds if len(x_bonds) else np.zeros((0, 5)), 5)
+    yb, ny = _rows(y_bonds if len(y_bonds) else np.zeros((0, 5)), 5)
+    fb, nf = _rows(fields if len(fields) else np.zeros((0, 4)), 4)
+    L.so_apply_hamiltonian_bitwise(_p(out), _p(psi_in), xb.ctypes.data_as(_dp), nx, yb.ctypes.data_as(_dp), ny,
+                                   fb.ctypes.data_as(_dp), nf, N)
+    return out
+
+
+def apply_H_xxz(psi, N, Jx, Jy, Jz, h):
+    out = np.zeros_like(psi)
+    L.so_apply_H_xxz(_p(psi), _p(out), N, Jx, Jy, Jz, h)
+    return out
 
 
 def circuit_draw(seed, op_index, traj):

@@ -637,6 +637,92 @@ void so_grad_finite_difference(const so_op* ops, int n, const double* theta, int
 }
 
 /* ========================================================================
+ * H|psi> -- the matrix-free Hamiltonian applications of the Chebyshev and
+ * Lanczos integrators
+ * ======================================================================== */
+/* apply_hamiltonian_bitwise! (cpuQuantumChannelUnitaryEvolutionChebyshev.jl:55-148),
+ * the pull loop: for every row k, the x bonds, then the y bonds (ZZ from k
+ * itself, XX and YY from k with both bits flipped), then the fields (Z from k,
+ * X and Y from k with the bit flipped).  Bond rows (i, j, Jxx, Jyy, Jzz) and
+ * field rows (idx, hx, hy, hz) with 1-based sites, as CouplingTerm / FieldTerm
+ * (cpuHamiltonianBuilder.jl:42,51).  The Y field follows the Y of
+ * construct_sparse_hamiltonian (cpuHamiltonianBuilder.jl:297: -i on rows with
+ * the bit clear) and of apply_Y! (cpuQuantumStateLanczos.jl:84-94); the pull
+ * loop's `phase_y = (val == 0) ? 1im : -1im` (Chebyshev.jl:142) is the
+ * transpose, i.e. -hy Y. */
+static C bond_pull(const C* in, int64_t k, const double* b) {
+    int bit_i = (int)b[0] - 1, bit_j = (int)b[1] - 1;
+    int64_t mask_flip = (1LL << bit_i) | (1LL << bit_j);
+    int val_i = (int)((k >> bit_i) & 1), val_j = (int)((k >> bit_j) & 1);
+    C acc = 0;
+    if (b[4] != 0.0) acc += b[4] * (val_i == val_j ? 1.0 : -1.0) * in[k];
+    int64_t k_flip = k ^ mask_flip;
+    if (b[2] != 0.0) acc += b[2] * in[k_flip];
+    if (b[3] != 0.0) acc += b[3] * (val_i == val_j ? -1.0 : 1.0) * in[k_flip];
+    return acc;
+}
+void so_apply_hamiltonian_bitwise(C* out, const C* in, const double* x_bonds, int nx, const double* y_bonds, int ny,
+                                  const double* fields, int nf, int N) {
+    int64_t dim = 1LL << N;
+    for (int64_t k = 0; k < dim; k++) {
+        C acc = 0;
+        for (int t = 0; t < nx; t++) acc += bond_pull(in, k, x_bonds + 5 * t);
+        for (int t = 0; t < ny; t++) acc += bond_pull(in, k, y_bonds + 5 * t);
+        for (int t = 0; t < nf; t++) {
+            const double* f = fields + 4 * t;
+            int bit_idx = (int)f[0] - 1;
+            int64_t mask = 1LL << bit_idx;
+            int val = (int)((k >> bit_idx) & 1);
+            if (f[3] != 0.0) acc += f[3] * (val == 0 ? 1.0 : -1.0) * in[k];
+            int64_t k_flip = k ^ mask;
+            if (f[1] != 0.0) acc += f[1] * in[k_flip];
+            if (f[2] != 0.0) acc += f[2] * (val == 0 ? -I_ : I_) * in[k_flip];
+        }
+        out[k] = acc;
+    }
+}
+/* apply_H_xxz! (cpuQuantumStateLanczos.jl:157-205): out = Jx sum X_i X_{i+1} +
+ * Jy sum Y_i Y_{i+1} + Jz sum Z_i Z_{i+1} + h sum X_i, term by term through a
+ * temporary as the reference accumulates (apply_XX! :98, apply_YY! :118,
+ * apply_ZZ! :86, apply_X! :70) */
+void so_apply_H_xxz(const C* psi, C* out, int N, double Jx, double Jy, double Jz, double h) {
+    int64_t dim = 1LL << N;
+    C* temp = (C*)calloc(dim, sizeof(C));
+    for (int64_t s = 0; s < dim; s++) out[s] = 0;
+    for (int pass = 0; pass < 4; pass++) {
+        double J = pass == 0 ? Jx : pass == 1 ? Jy : pass == 2 ? Jz : h;
+        if (J == 0.0) continue;
+        for (int i = 1; i <= (pass == 3 ? N : N - 1); i++) {
+            for (int64_t s = 0; s < dim; s++) temp[s] = 0;
+            if (pass == 3) {
+                int64_t step = 1LL << (i - 1);
+                for (int64_t a = 0; a < dim; a++)
+                    if (((a >> (i - 1)) & 1) == 0) { temp[a] += psi[a + step]; temp[a + step] += psi[a]; }
+            } else if (pass == 2) {
+                for (int64_t a = 0; a < dim; a++) {
+                    int bi = (int)((a >> (i - 1)) & 1), bj = (int)((a >> i) & 1);
+                    temp[a] += (double)(1 - 2 * (bi ^ bj)) * psi[a];
+                }
+            } else {
+                int64_t si = 1LL << (i - 1), sj = 1LL << i;
+                double sg = pass == 1 ? -1.0 : 1.0;
+                for (int64_t a = 0; a < dim; a++) {
+                    if (((a >> (i - 1)) & 1) == 0 && ((a >> i) & 1) == 0) {
+                        int64_t s00 = a, s01 = a + sj, s10 = a + si, s11 = a + si + sj;
+                        temp[s00] += sg * psi[s11];
+                        temp[s01] += psi[s10];
+                        temp[s10] += psi[s01];
+                        temp[s11] += sg * psi[s00];
+                    }
+                }
+            }
+            for (int64_t s = 0; s < dim; s++) out[s] += J * temp[s];
+        }
+    }
+    free(temp);
+}
+
+/* ========================================================================
  * Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
  * easy as 1, 2, 3", SC'11): 10 rounds of the 4x32 S-box with multipliers
  * 0xD2511F53 / 0xCD9E8D57 and Weyl key increments 0x9E3779B9 / 0xBB67AE85,

@@ -130,6 +130,15 @@ void so_grad_finite_difference(const so_op* ops, int n, const double* theta, int
                                int nterms, const double* coef, const char* paulis,
                                double eps, const int* which, int nwhich, double* grad);
 
+/* ---- H|psi> of the Chebyshev / Lanczos integrators ---- */
+/* apply_hamiltonian_bitwise! (cpuQuantumChannelUnitaryEvolutionChebyshev.jl:55): bond rows
+ * (i, j, Jxx, Jyy, Jzz), field rows (idx, hx, hy, hz), 1-based sites; the Y field as
+ * construct_sparse_hamiltonian (cpuHamiltonianBuilder.jl:297), see the .c file */
+void so_apply_hamiltonian_bitwise(so_cplx* out, const so_cplx* in, const double* x_bonds, int nx,
+                                  const double* y_bonds, int ny, const double* fields, int nf, int N);
+/* apply_H_xxz! (cpuQuantumStateLanczos.jl:157) */
+void so_apply_H_xxz(const so_cplx* psi, so_cplx* out, int N, double Jx, double Jy, double Jz, double h);
+
 /* ---- counter-based RNG (Philox4x32-10, Salmon et al., SC'11) ---- */
 void so_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 double so_u01_from_words(uint32_t hi, uint32_t lo);

@@ -11,7 +11,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "lib", "libsmoq_cuda.so")
-SOURCES = ["capi.cu", "k_kernels.cu", "k_regtile.cu", "k_stage.cu", "planner.cpp", "mcwf.cu", "vqe.cu", "noalloc.cu", "measure.cu", "dm.cu", "qrc.cu", "circuit.cu", "noisy_grad.cu", "jit.cpp"]
+SOURCES = ["capi.cu", "k_kernels.cu", "k_stage.cu", "planner.cpp", "mcwf.cu", "vqe.cu", "noalloc.cu", "measure.cu", "dm.cu", "qrc.cu", "circuit.cu", "noisy_grad.cu", "jit.cpp"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC"]
 OBJDIR = os.path.join(PKG, "_build")

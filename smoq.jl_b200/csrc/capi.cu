@@ -102,20 +102,15 @@ static int engine_for(smoq_ctx* ctx, bool reusable, int dtype) {
     return (reusable && dtype == SMOQ_C64 && jit_available()) ? 3 : 0;
 }
 
-// plan a gate list into fused passes; with the register engine every pass
-// wide enough for it gets a register-tile schedule
+// plan a gate list into fused passes; with the stage engines every pass of
+// tile width 12 (13 for complex64) gets a stage schedule
 static std::vector<Pass> plan_for(int engine, const std::vector<GateIR>& ir, int N, int dtype, int tbits, int lbits,
-                                  int epilogue_special = -1, int stage_bits = 4) {
+                                  int epilogue_special = -1) {
     std::vector<Pass> pl = plan_passes(ir, N, tbits, lbits, epilogue_special, dtype == SMOQ_C64 ? 1 : 0);
-    if (engine == 1)
-        for (Pass& p : pl)
-            if (p.g.T >= RT_MIN_T && p.g.T - RT_MIN_T <= (dtype == SMOQ_C64 ? 5 : 4)) schedule_regtile(p);
     if (engine == 2 || engine == 3)
         for (Pass& p : pl)
             if (p.g.T == 12 || (p.g.T == 13 && dtype == SMOQ_C64)) {
-                // 5-bit stages exist only in compiled complex64 kernels
-                const bool k5 = engine == 3 && dtype == SMOQ_C64 && stage_bits == 5;
-                schedule_stages(p, dtype == SMOQ_C64 ? 8 : 16, k5 ? 5 : 4);
+                schedule_stages(p, dtype == SMOQ_C64 ? 8 : 16);
                 p.want_jit = engine == 3 && p.staged && dtype == SMOQ_C64;
             }
     return pl;
@@ -139,7 +134,7 @@ static smoq_status upload_program(smoq_ctx* ctx, DevProgram& P) {
     for (Pass& p : P.passes) {
         if (!p.want_jit || p.jit) continue;
         std::string why;
-        p.jit = jit_pass_kernel(p, ctx->jit_buffers, ctx->jit_packed != 0, ctx->jit_groups, why);
+        p.jit = jit_pass_kernel(p, ctx->jit_buffers, ctx->jit_groups, why);
         if (!p.jit) return fail(ctx, SMOQ_ERR_UNSUPPORTED, "compiled pass kernel: " + why);
     }
     std::vector<DevOp> all;
@@ -163,11 +158,14 @@ struct EventPair {
 
 // ================================================================ autotuner
 // For every compiled pass of a reusable program (engine 3) the tuner times the
-// kernel variants -- 16-amplitude register groups per thread (2 or 1) x CTAs
-// per SM (the register budget's default, or one more) -- on a zeroed scratch
-// state of the program's size with CUDA events on the context's stream, and
-// keeps the fastest.  The variants apply the same literal FMA sequence to every
-// amplitude, so the choice changes the timing, never the result.  Choices are
+// kernel variants -- 16-amplitude register groups per thread (2 or 1), CTAs per
+// SM (the register budget's default, or one more), and one tile buffer per CTA
+// or two (the next tile's bulk load in flight under the current tile's stages)
+// -- on a zeroed scratch state of the program's size with CUDA events on the
+// context's stream, and keeps the fastest.  The variants apply the same literal
+// FMA sequence to every amplitude, so the choice changes the timing, never the
+// result.  States below 2^20 amplitudes are not tuned (their passes take
+// microseconds).  Choices are
 // cached per (GPU, pass program) for the life of the process and, when the
 // environment variable SMOQ_TUNE_CACHE names a file, across processes (one
 // line per pass program: key, variant).  Passes whose ops read per-state
@@ -175,10 +173,11 @@ struct EventPair {
 // the default variant.
 namespace {
 struct TuneVariant {
-    int groups, minb_add;
+    int groups, minb_add, nbuf;
 };
-const TuneVariant kTuneVariants[] = {{2, 0}, {2, 1}, {1, 0}, {1, 1}};
-constexpr int kTuneVariantCount = 4;
+const TuneVariant kTuneVariants[] = {{2, 0, 1}, {2, 1, 1}, {1, 0, 1}, {1, 1, 1}, {2, 0, 2}, {1, 0, 2}};
+constexpr int kTuneVariantCount = 6;
+constexpr int kTuneMinN = 20;
 std::mutex g_tune_mu;
 std::map<uint64_t, int> g_tune;
 bool g_tune_loaded = false;
@@ -225,6 +224,7 @@ bool tunable(const Pass& p) {
 }  // namespace
 
 static smoq_status autotune_program(smoq_ctx* ctx, DevProgram& P, int N) {
+    if (N < kTuneMinN) return SMOQ_OK;
     std::vector<size_t> todo;
     for (size_t i = 0; i < P.passes.size(); ++i)
         if (tunable(P.passes[i]) && !P.passes[i].ops.empty()) todo.push_back(i);
@@ -237,7 +237,7 @@ static smoq_status autotune_program(smoq_ctx* ctx, DevProgram& P, int N) {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         tune_cache_load_locked();
         for (size_t i : todo) {
-            keys[i] = jit_pass_key(P.passes[i], ctx->jit_buffers, ctx->jit_packed != 0) ^ dh;
+            keys[i] = jit_pass_key(P.passes[i], 1) ^ dh;
             auto it = g_tune.find(keys[i]);
             if (it == g_tune.end()) {
                 fresh.push_back(i);
@@ -245,8 +245,7 @@ static smoq_status autotune_program(smoq_ctx* ctx, DevProgram& P, int N) {
             }
             const TuneVariant& v = kTuneVariants[it->second];
             std::string why;
-            if (const JitKernel* k = jit_pass_kernel(P.passes[i], ctx->jit_buffers, ctx->jit_packed != 0, v.groups, why,
-                                                     v.minb_add))
+            if (const JitKernel* k = jit_pass_kernel(P.passes[i], v.nbuf, v.groups, why, v.minb_add))
                 P.passes[i].jit = k;
         }
     }
@@ -275,8 +274,7 @@ static smoq_status autotune_program(smoq_ctx* ctx, DevProgram& P, int N) {
                 }
                 const TuneVariant& v = kTuneVariants[j % kTuneVariantCount];
                 std::string why;
-                ks[j] = jit_pass_kernel(P.passes[fresh[j / kTuneVariantCount]], ctx->jit_buffers,
-                                        ctx->jit_packed != 0, v.groups, why, v.minb_add);
+                ks[j] = jit_pass_kernel(P.passes[fresh[j / kTuneVariantCount]], v.nbuf, v.groups, why, v.minb_add);
             }
         };
         const size_t nt = std::max<size_t>(1, std::min<size_t>(ks.size(), std::thread::hardware_concurrency()));
@@ -406,7 +404,6 @@ smoq_status smoq_ctx_create(int device, smoq_ctx** out) {
     if (cudaMalloc(&ctx->d_err, sizeof(int32_t)) != cudaSuccess) return SMOQ_ERR_OOM;
     if (cudaMemset(ctx->d_err, 0, sizeof(int32_t)) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (tile_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
-    if (regtile_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (stage_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (vqe_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (qrc_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
@@ -459,13 +456,8 @@ smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long v) {
         case SMOQ_OPT_USE_GRAPHS: ctx->use_graphs = v != 0; break;
         case SMOQ_OPT_KERNEL_TIMING: ctx->kernel_timing = v != 0; break;
         case SMOQ_OPT_ENGINE:
-            if (v < -1 || v > 3) return fail(ctx, SMOQ_ERR_BADINPUT, "engine must be -1 (auto), 0, 1, 2 or 3");
+            if (v < -1 || v > 3 || v == 1) return fail(ctx, SMOQ_ERR_BADINPUT, "engine must be -1 (auto), 0, 2 or 3");
             ctx->engine = (int)v;
-            break;
-        case SMOQ_OPT_JIT_PACKED: ctx->jit_packed = v != 0; break;
-        case SMOQ_OPT_JIT_STAGE_BITS:
-            if (v != 4 && v != 5) return fail(ctx, SMOQ_ERR_BADINPUT, "compiled-kernel stage bits must be 4 or 5");
-            ctx->jit_stage_bits = (int)v;
             break;
         case SMOQ_OPT_JIT_GROUPS:
             if (v != 1 && v != 2) return fail(ctx, SMOQ_ERR_BADINPUT, "compiled-kernel register groups must be 1 or 2");
@@ -776,7 +768,7 @@ smoq_status smoq_apply_sequence(smoq_state* st, const smoq_op* ops, int n, const
     DevProgram P;
     try {
         P.passes = plan_for(engine_for(ctx, false, st->dtype), ir, st->N, st->dtype, tile_bits(ctx, st->dtype),
-                            low_bits(ctx, st->dtype), -1, ctx->jit_stage_bits);
+                            low_bits(ctx, st->dtype), -1);
     } catch (const std::exception& ex) {
         return fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
     }
@@ -806,7 +798,11 @@ smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tbits, int lbit
     if (smoq_status s = ops_to_ir(nullptr, N, ops, n, theta, ir)) return s;
     std::vector<Pass> pl;
     try {
-        pl = plan_for(3, ir, N, dtype, tbits, lbits, -1, (flags & 16) ? 5 : 4);
+        if (flags & ~(1 | 2 | 8)) {
+            say("unknown flag");
+            return SMOQ_ERR_BADINPUT;
+        }
+        pl = plan_for(3, ir, N, dtype, tbits, lbits, -1);
     } catch (const std::exception& e) {
         say(e.what());
         return SMOQ_ERR_BADINPUT;
@@ -815,8 +811,7 @@ smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tbits, int lbit
     for (const Pass& p : pl) {
         if (!p.want_jit) continue;
         std::string why, info;
-        if (!jit_check_pass(p, (flags & 2) ? 2 : 1, (flags & 4) != 0, (flags & 8) ? 1 : 2, why, nullptr,
-                            verbose ? &info : nullptr)) {
+        if (!jit_check_pass(p, (flags & 2) ? 2 : 1, (flags & 8) ? 1 : 2, why, nullptr, verbose ? &info : nullptr)) {
             say(why);
             return why.rfind("NVRTC (", 0) == 0 ? SMOQ_ERR_UNSUPPORTED : SMOQ_ERR_BADINPUT;
         }
@@ -832,7 +827,7 @@ smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tbits, int lbi
                                      smoq_fused_op_info* fused, int max_fused, int* n_passes, int* n_fused) {
     if (N < 1 || N > 40 || n < 0 || (n > 0 && !ops) || !n_passes || !n_fused) return SMOQ_ERR_BADINPUT;
     if (dtype != SMOQ_C64 && dtype != SMOQ_C128) return SMOQ_ERR_BADINPUT;
-    if (engine < 0 || engine > 3) return SMOQ_ERR_BADINPUT;
+    if (engine < 0 || engine > 3 || engine == 1) return SMOQ_ERR_BADINPUT;
     std::vector<GateIR> ir;
     if (smoq_status s = ops_to_ir(nullptr, N, ops, n, theta, ir)) return s;
     std::vector<Pass> pl;
@@ -865,7 +860,6 @@ smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tbits, int lbi
                 }
                 for (int r = 0; r < 8; ++r) fi.perm[r] = op.perm[r];
                 for (int t = 0; t < 4; ++t) fi.slot[t] = op.slot[t];
-                fi.mode = op.mode;
                 for (int k = 0; k < 16; ++k) {
                     fi.c[2 * k] = op.cd[k].x;
                     fi.c[2 * k + 1] = op.cd[k].y;
@@ -1101,7 +1095,7 @@ static smoq_status get_block(smoq_plan* P, int nsteps, smoq_plan::Block** out) {
     for (int s = 0; s < nsteps; ++s) all.insert(all.end(), P->step.begin(), P->step.end());
     try {
         B->prog.passes = plan_for(engine_for(P->ctx, true, P->dtype), all, P->N, P->dtype, tile_bits(P->ctx, P->dtype),
-                                  low_bits(P->ctx, P->dtype), -1, P->ctx->jit_stage_bits);
+                                  low_bits(P->ctx, P->dtype), -1);
     } catch (const std::exception& ex) {
         return fail(P->ctx, SMOQ_ERR_BADINPUT, ex.what());
     }
@@ -1334,7 +1328,7 @@ smoq_status smoq_internal_prepare(smoq_ctx* ctx, smoq_state* st, const std::vect
     std::unique_ptr<DevProgram> P(new DevProgram());
     try {
         P->passes = plan_for(engine_for(ctx, reusable, st->dtype), gates, st->N, st->dtype, tile_bits(ctx, st->dtype),
-                             low_bits(ctx, st->dtype), epilogue_special, ctx->jit_stage_bits);
+                             low_bits(ctx, st->dtype), epilogue_special);
     } catch (const std::exception& ex) {
         return fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
     }

@@ -158,16 +158,6 @@ __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.comm
 __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-// packed pairs: lane 0 = the thread's group 0, lane 1 = its group 1 (FP32x2 arithmetic)
-__device__ __forceinline__ u64 pk(float a, float b) { u64 r; asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b)); return r; }
-__device__ __forceinline__ void up(u64 v, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
-__device__ __forceinline__ u64 mul2(u64 a, u64 b) { u64 d; asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; }
-__device__ __forceinline__ u64 add2(u64 a, u64 b) { u64 d; asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d; }
-__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
-    u64 d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
 )PRE";
 
 // ------------------------------------------------------------ code helpers
@@ -263,220 +253,7 @@ struct Gen {
     const Pass& p;
     int G, NT;
     std::ostringstream o;
-    std::vector<uint64_t> kc;          // packed constants (c, c), emitted as __constant__ KC[]
-    std::map<uint64_t, int> kidx;
     explicit Gen(const Pass& pass, int g, int nt) : p(pass), G(g), NT(nt) {}
-
-    // ------------------------------------------------------------ packed (FP32x2)
-    // Registers P_r / Q_r hold the real / imaginary parts of stage element r of
-    // the thread's two groups as one 64-bit pair; every op runs once on the pair.
-    std::string K(float c) {
-        uint32_t b;
-        std::memcpy(&b, &c, 4);
-        const uint64_t v = ((uint64_t)b << 32) | b;
-        auto it = kidx.find(v);
-        int i;
-        if (it == kidx.end()) {
-            i = (int)kc.size();
-            kc.push_back(v);
-            kidx[v] = i;
-        } else {
-            i = it->second;
-        }
-        return "KC[" + std::to_string(i) + "]";
-    }
-    // sum of k * x over the terms (k != 0), as nested mul2/fma2/add2
-    std::string chain(const std::vector<std::pair<float, std::string>>& terms) {
-        std::string acc;
-        for (const auto& t : terms) {
-            if (t.first == 0.f) continue;
-            if (acc.empty()) acc = t.first == 1.f ? t.second : "mul2(" + K(t.first) + ", " + t.second + ")";
-            else if (t.first == 1.f) acc = "add2(" + acc + ", " + t.second + ")";
-            else acc = "fma2(" + K(t.first) + ", " + t.second + ", " + acc + ")";
-        }
-        return acc.empty() ? std::string("0ull") : acc;
-    }
-    std::string Pn(int r) { return "P" + std::to_string(r); }
-    std::string Qn(int r) { return "Q" + std::to_string(r); }
-
-    void stage_packed(const int* S, const int* rl, const std::vector<int>& members) {
-        const uint32_t gstep = deposit_value(S, 4, (uint32_t)NT);
-        uint32_t off[16];
-        for (int r = 0; r < 16; ++r) {
-            off[r] = 0;
-            for (int q = 0; q < 4; ++q)
-                if ((r >> q) & 1) off[r] |= 1u << S[q];
-        }
-        bool rotated = false;
-        for (int q = 0; q < 4; ++q) rotated |= rl[q] >= 0;
-        o << "    {  // stage S = {" << S[0] << "," << S[1] << "," << S[2] << "," << S[3] << "}, FP32x2\n";
-        o << "        const u32 g0 = " << deposit_expr(S, 4, "tid") << ";\n";
-        if (rotated) {
-            o << "        const u32 ga = g0";
-            for (int q = 0; q < 4; ++q)
-                if (rl[q] >= 0) o << " ^ (((tid >> " << rl[q] << ") & 1u) << " << S[q] << ")";
-            o << ";\n";
-        }
-        auto addr = [&](int r, int j) {
-            const uint32_t c = off[r] | (j ? gstep : 0u);
-            return rotated ? "ga ^ " + std::to_string(c) + "u" : "g0 + " + std::to_string(c) + "u";
-        };
-        o << "        u64";
-        for (int r = 0; r < 16; ++r) o << (r ? ", " : " ") << Pn(r) << ", " << Qn(r);
-        o << ";\n";
-        for (int r = 0; r < 16; ++r)
-            o << "        { const cf a = tile[" << addr(r, 0) << "], b = tile[" << addr(r, 1) << "]; " << Pn(r)
-              << " = pk(a.x, b.x); " << Qn(r) << " = pk(a.y, b.y); }\n";
-        if (rotated) unrotate_packed(rl);
-        bool scal = false;
-        for (int m : members) scal |= member_packed(m, S, gstep, off, scal);
-        if (scal) {
-            o << "        { const u64 kr = pk(sc.x, sc.x), ki = pk(sc.y, sc.y), kn = pk(-sc.y, -sc.y);\n";
-            for (int r = 0; r < 16; ++r)
-                o << "          { const u64 p = " << Pn(r) << ", q = " << Qn(r) << "; " << Pn(r)
-                  << " = fma2(kn, q, mul2(kr, p)); " << Qn(r) << " = fma2(ki, p, mul2(kr, q)); }\n";
-            o << "        }\n";
-        }
-        if (rotated) unrotate_packed(rl);
-        for (int r = 0; r < 16; ++r)
-            o << "        { float p0, p1, q0, q1; up(" << Pn(r) << ", p0, p1); up(" << Qn(r) << ", q0, q1); tile["
-              << addr(r, 0) << "] = cf{p0, q0}; tile[" << addr(r, 1) << "] = cf{p1, q1}; }\n";
-        o << "    }\n    __syncthreads();\n";
-    }
-
-    void unrotate_packed(const int* rl) {
-        for (int q = 0; q < 4; ++q) {
-            if (rl[q] < 0) continue;
-            o << "        { const bool s = (tid >> " << rl[q] << ") & 1u;\n";
-            for (int r = 0; r < 16; ++r) {
-                if ((r >> q) & 1) continue;
-                const int k = r | (1 << q);
-                for (auto nm : {&Gen::Pn, &Gen::Qn}) {
-                    const std::string A = (this->*nm)(r), B = (this->*nm)(k);
-                    o << "          { const u64 t = s ? " << B << " : " << A << "; " << B << " = s ? " << A << " : " << B
-                      << "; " << A << " = t; }\n";
-                }
-            }
-            o << "        }\n";
-        }
-    }
-
-    // complex literal times element r (both groups)
-    void cmul_lit_packed(int r, float re, float im) {
-        o << "        { const u64 p = " << Pn(r) << ", q = " << Qn(r) << "; " << Pn(r) << " = "
-          << chain({{re, "p"}, {-im, "q"}}) << "; " << Qn(r) << " = " << chain({{re, "q"}, {im, "p"}}) << "; }\n";
-    }
-
-    bool member_packed(int m, const int* S, uint32_t gstep, const uint32_t* off, bool have_scal) {
-        const DevOp& op = p.ops[m];
-        auto spos = [&](int lb) {
-            for (int q = 0; q < 4; ++q)
-                if (S[q] == lb) return q;
-            return -1;
-        };
-        auto open_scal = [&]() {
-            if (!have_scal) o << "        cf sc = cf{1.f, 0.f};\n";
-        };
-        if (op.kind == OPK_STATESCALE) {
-            open_scal();
-            o << "        sc = cscale(sc, (float)((const double*)a.ops[" << m << "].aux)[b]);\n";
-            return true;
-        }
-        if (op.kind == OPK_REALTAB) {
-            for (int r = 0; r < 16; ++r)
-                o << "        { const u64 f = pk(realtab(a.ops[" << m << "], base, g0 | " << off[r]
-                  << "u), realtab(a.ops[" << m << "], base, g0 | " << (off[r] | gstep) << "u)); " << Pn(r)
-                  << " = mul2(f, " << Pn(r) << "); " << Qn(r) << " = mul2(f, " << Qn(r) << "); }\n";
-            return false;
-        }
-        if (op.kind == OPK_DIAG) {
-            int pos[4] = {-1, -1, -1, -1};
-            bool any_tile_nonstage = false, any_off = false, any_stage = false;
-            for (int t = 0; t < op.nq; ++t) {
-                if (op.lb[t] >= 0) {
-                    pos[t] = spos(op.lb[t]);
-                    if (pos[t] < 0) any_tile_nonstage = true;
-                    else any_stage = true;
-                } else {
-                    any_off = true;
-                }
-            }
-            std::ostringstream rt;
-            rt << "0u";
-            for (int t = 0; t < op.nq; ++t)
-                if (op.lb[t] < 0) rt << " | ((u32)((base >> " << op.gb[t] << ") & 1ull) << " << t << ")";
-            if (!any_stage && !any_tile_nonstage) {
-                open_scal();
-                o << "        sc = cmul(sc, a.ops[" << m << "].c[" << rt.str() << "]);\n";
-                return true;
-            }
-            if (!any_tile_nonstage && !any_off) {
-                for (int r = 0; r < 16; ++r) {
-                    int mi = 0;
-                    for (int t = 0; t < op.nq; ++t) mi |= ((r >> pos[t]) & 1) << t;
-                    const float re = op.cf[mi].x, im = op.cf[mi].y;
-                    if (re == 1.f && im == 0.f) continue;
-                    cmul_lit_packed(r, re, im);
-                }
-                return false;
-            }
-            o << "        { const u32 g1 = g0 | " << gstep << "u;\n";
-            for (int j = 0; j < 2; ++j) {
-                o << "          const u32 mr" << j << " = " << rt.str();
-                for (int t = 0; t < op.nq; ++t)
-                    if (op.lb[t] >= 0 && pos[t] < 0)
-                        o << " | ((((g" << j << ") >> " << op.lb[t] << ") & 1u) << " << t << ")";
-                o << ";\n";
-            }
-            for (int r = 0; r < 16; ++r) {
-                int mi = 0;
-                for (int t = 0; t < op.nq; ++t)
-                    if (pos[t] >= 0) mi |= ((r >> pos[t]) & 1) << t;
-                o << "          { const cf c0 = a.ops[" << m << "].c[mr0 | " << mi << "u], c1 = a.ops[" << m
-                  << "].c[mr1 | " << mi << "u];\n"
-                  << "            const u64 kr = pk(c0.x, c1.x), ki = pk(c0.y, c1.y), kn = pk(-c0.y, -c1.y);\n"
-                  << "            const u64 p = " << Pn(r) << ", q = " << Qn(r) << "; " << Pn(r)
-                  << " = fma2(kn, q, mul2(kr, p)); " << Qn(r) << " = fma2(ki, p, mul2(kr, q)); }\n";
-            }
-            o << "        }\n";
-            return false;
-        }
-        int pos[3] = {-1, -1, -1};
-        for (int t = 0; t < op.nq; ++t) pos[t] = spos(op.lb[t]);
-        const int dim = 1 << op.nq;
-        const std::vector<CplxF> M = op_matrix_f(op);
-        int pmask = 0;
-        for (int t = 0; t < op.nq; ++t) pmask |= 1 << pos[t];
-        for (int e = 0; e < 16; ++e) {
-            if (e & pmask) continue;
-            int ix[8];
-            for (int c = 0; c < dim; ++c) {
-                int r = e;
-                for (int t = 0; t < op.nq; ++t)
-                    if ((c >> t) & 1) r |= 1 << pos[t];
-                ix[c] = r;
-            }
-            o << "        {";
-            for (int c = 0; c < dim; ++c)
-                o << " const u64 p" << c << " = " << Pn(ix[c]) << ", q" << c << " = " << Qn(ix[c]) << ";";
-            o << "\n";
-            for (int r = 0; r < dim; ++r) {
-                std::vector<std::pair<float, std::string>> re, im;
-                for (int c = 0; c < dim; ++c) {
-                    const CplxF k = M[r * dim + c];
-                    const std::string pc = "p" + std::to_string(c), qc = "q" + std::to_string(c);
-                    re.push_back({k.re, pc});
-                    re.push_back({-k.im, qc});
-                    im.push_back({k.re, qc});
-                    im.push_back({k.im, pc});
-                }
-                o << "          " << Pn(ix[r]) << " = " << chain(re) << ";\n";
-                o << "          " << Qn(ix[r]) << " = " << chain(im) << ";\n";
-            }
-            o << "        }\n";
-        }
-        return false;
-    }
 
     std::string v(int i) { return "v" + std::to_string(i); }
 
@@ -662,19 +439,18 @@ struct Gen {
 };
 
 // full source of the kernels for one pass
-std::string generate(const Pass& p, bool need_epi, int nbuf, bool packed, int groups, int minb_add, std::string& err) {
+std::string generate(const Pass& p, bool need_epi, int nbuf, int groups, int minb_add, std::string& err) {
     const int N = p.g.N;
     const TileGeom& g = p.g;
     const int T = g.T;
     // G register groups of 16 amplitudes per thread, NT = 2^(T-4) / G threads
     // register budget: 128 per thread with two groups, 64 with one; minb_add asks
     // for that many more CTAs per SM (a tighter register cap, at most 32 a thread)
-    const int G = packed ? 2 : groups, NT = 1 << (T - 4 - (G - 1));
+    const int G = groups, NT = 1 << (T - 4 - (G - 1));
     const int MINB = std::min(65536 / (NT * (G == 2 ? 128 : 64)) + std::max(0, minb_add), 65536 / (NT * 32));
     Gen gen(p, G, NT);
     std::ostringstream& o = gen.o;
     o << kPrelude;
-    o << "/*KCONST*/\n";
     o << "static_assert(sizeof(DevOp) == " << sizeof(DevOp) << ", \"DevOp layout\");\n";
     o << "static_assert(sizeof(TileArgs) == " << sizeof(TileArgs) << ", \"TileArgs layout\");\n";
     o << "#define NT " << NT << "\n#define TB " << T << "\n#define LB " << g.L << "\n#define HB " << g.H << "\n";
@@ -776,24 +552,12 @@ std::string generate(const Pass& p, bool need_epi, int nbuf, bool packed, int gr
             }
             members.push_back((int)o_i + 1);
             o_i += 2;
-        } else if (h.nq == 5) {
-            // 5-bit stage: bits in perm[0..4], rotation lanes of positions 0..3 in lb[0..3]
-            if (packed || G != 2) {
-                err = "jit: 5-bit stages need scalar arithmetic and two groups per thread";
-                return "";
-            }
-            kb = 5;
-            for (int q = 0; q < 5; ++q) S[q] = h.perm[q];
-            for (int q = 0; q < 4; ++q) rl[q] = h.lb[q];
-            for (int k = 1; k <= (int)h.aux2; ++k) members.push_back((int)(o_i + k));
-            o_i += 1 + (size_t)h.aux2;
         } else {
             for (int q = 0; q < 4; ++q) S[q] = h.perm[q], rl[q] = h.perm[4 + q];
             for (int k = 1; k <= (int)h.aux2; ++k) members.push_back((int)(o_i + k));
             o_i += 1 + (size_t)h.aux2;
         }
-        if (packed) gen.stage_packed(S, rl, members);
-        else gen.stage(S, kb, rl, members);
+        gen.stage(S, kb, rl, members);
     }
     o << "    if (EPI) {\n"
          "        constexpr int nb = NT == 128 ? 7 : NT == 256 ? 8 : 9;\n"
@@ -844,15 +608,7 @@ std::string generate(const Pass& p, bool need_epi, int nbuf, bool packed, int gr
     if (need_epi)
         o << "extern \"C\" __global__ void __launch_bounds__(NT, " << MINB
           << ") smoq_pass_e1(const TileArgs a) { body<true>(a); }\n";
-    std::string src = o.str();
-    std::ostringstream kt;
-    kt << "__constant__ u64 KC[" << std::max<size_t>(1, gen.kc.size()) << "] = {";
-    if (gen.kc.empty()) kt << "0ull";
-    for (size_t k = 0; k < gen.kc.size(); ++k) kt << (k ? ", " : "") << gen.kc[k] << "ull";
-    kt << "};";
-    const size_t at = src.find("/*KCONST*/");
-    src.replace(at, 10, kt.str());
-    return src;
+    return o.str();
 }
 
 std::mutex g_mu;
@@ -910,13 +666,13 @@ bool compile_cubin(const std::string& src, std::vector<char>& cubin, std::string
 
 // Generate and compile a staged complex64 pass without loading it (host only);
 // `info` (optional) receives the compiler's resource report.
-bool jit_check_pass(const Pass& p, int nbuf, bool packed, int groups, std::string& err, size_t* cubin_bytes,
+bool jit_check_pass(const Pass& p, int nbuf, int groups, std::string& err, size_t* cubin_bytes,
                     std::string* info) {
     if (!p.staged || (p.g.T != 12 && p.g.T != 13)) {
         err = "jit: only stage-scheduled passes of tile width 12-13";
         return false;
     }
-    const std::string src = generate(p, p.epilogue, nbuf, packed, groups, 0, err);
+    const std::string src = generate(p, p.epilogue, nbuf, groups, 0, err);
     if (src.empty()) return false;
     std::vector<char> cubin;
     if (!compile_cubin(src, cubin, err, info)) return false;
@@ -926,12 +682,12 @@ bool jit_check_pass(const Pass& p, int nbuf, bool packed, int groups, std::strin
 
 // Compile (or fetch) the kernel of a stage-scheduled complex64 pass and load
 // it into the current device.  Returns nullptr and fills `err` on failure.
-const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, int groups, std::string& err, int minb_add) {
+const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, int groups, std::string& err, int minb_add) {
     if (!p.staged || (p.g.T != 12 && p.g.T != 13)) {
         err = "jit: only stage-scheduled passes of tile width 12-13";
         return nullptr;
     }
-    std::string src = generate(p, p.epilogue, nbuf, packed, groups, minb_add, err);
+    std::string src = generate(p, p.epilogue, nbuf, groups, minb_add, err);
     if (src.empty()) return nullptr;
     {
         std::lock_guard<std::mutex> lk(g_mu);
@@ -951,7 +707,7 @@ const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, int group
         err = std::string("cudaLibraryLoadData: ") + cudaGetErrorString(e);
         return nullptr;
     }
-    k->threads = 1 << (p.g.T - 4 - ((packed ? 2 : groups) - 1));
+    k->threads = 1 << (p.g.T - 4 - (groups - 1));
     k->smem = (size_t)(nbuf == 2 ? 16 : 8) << p.g.T;
     const char* names[2] = {"smoq_pass_e0", "smoq_pass_e1"};
     for (int v = 0; v < (p.epilogue ? 2 : 1); ++v) {
@@ -981,9 +737,9 @@ const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, int group
 
 bool jit_available() { return nvrtc().ok; }
 
-uint64_t jit_pass_key(const Pass& p, int nbuf, bool packed) {
+uint64_t jit_pass_key(const Pass& p, int nbuf) {
     std::string err;
-    const std::string src = generate(p, p.epilogue, nbuf, packed, 2, 0, err);
+    const std::string src = generate(p, p.epilogue, nbuf, 2, 0, err);
     return src.empty() ? 0 : fnv1a(src);
 }
 

@@ -509,11 +509,6 @@ cudaError_t launch_tile_pass(smoq_ctx* ctx, smoq_state* st, const Pass& p, const
     const size_t smem = tile_max_smem((int)st->amp_bytes(), p.g.T);
     cudaError_t e;
     const bool epi = ep && ep->partials;
-    if (p.regtile) {
-        e = launch_regtile(ctx, a, st->dtype, epi);
-        ctx->launches++;
-        return e;
-    }
     if (p.jit) {
         e = launch_jit(ctx, a, p.jit, epi);
         ctx->launches++;

@@ -518,19 +518,6 @@ std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, in
     return passes;
 }
 
-// ----------------------------------------------------------------------------
-// Register-tile scheduling.  In the register engine a tile of 2^T amplitudes
-// lives in the registers of 256 threads: tile-local bits 0..4 are the lane
-// index (ops on them exchange values with warp shuffles), KR = T - 8 bits are
-// register bits (ops on them stay inside a thread), and 3 bits are the warp
-// index.  A non-diagonal op may only touch lane and register bits, so the
-// schedule changes the register/warp assignment (an OPK_LAYOUT op: one
-// round trip of the tile through shared memory) when the next op needs a
-// warp bit, choosing the new register bits from the ops that follow.  Ops
-// that cannot fit (3-qubit non-diagonal ops when KR < 3) run through shared
-// memory (mode 1).  Diagonal and special ops read any bit from the element's
-// tile index and never force a layout change.
-// ----------------------------------------------------------------------------
 // Exchange the roles of a 2-qubit op's qubits 0 and 1 (matrix index bits
 // swapped: local index 1 <-> 2), in every encoding the kernels read.
 static void swap_qubit_roles(DevOp& op) {
@@ -565,111 +552,6 @@ static void swap_qubit_roles(DevOp& op) {
     }
 }
 
-void schedule_regtile(Pass& p) {
-    const int T = p.g.T;
-    const int KR = T - RT_MIN_T;
-    if (KR < 0) return;  // tile too small for the register engine
-    std::vector<DevOp> in = std::move(p.ops);
-    auto needs = [&](const DevOp& op) {
-        std::vector<int> v;
-        if (op.kind == OPK_DIAG || op.kind == OPK_STATESCALE || op.kind == OPK_REALTAB) return v;
-        for (int t = 0; t < op.nq; ++t)
-            if (op.lb[t] >= RT_LANE_BITS) v.push_back(op.lb[t]);
-        return v;
-    };
-    auto contains = [](const std::vector<int>& s, int b) {
-        for (int x : s)
-            if (x == b) return true;
-        return false;
-    };
-    // choose register bits starting at op i: bits needed soonest first
-    auto choose = [&](size_t i) {
-        std::vector<int> R;
-        for (size_t k = i; k < in.size() && (int)R.size() < KR; ++k) {
-            std::vector<int> nd = needs(in[k]);
-            if ((int)nd.size() > KR) continue;
-            int extra = 0;
-            for (int b : nd)
-                if (!contains(R, b)) ++extra;
-            if ((int)R.size() + extra > KR) break;
-            for (int b : nd)
-                if (!contains(R, b)) R.push_back(b);
-        }
-        for (int b = RT_LANE_BITS; b < T && (int)R.size() < KR; ++b)
-            if (!contains(R, b)) R.push_back(b);
-        // ascending register bits: a chain of neighbour bonds then always maps
-        // to the same few (P, P+1) register pairs, i.e. the same few code paths
-        std::sort(R.begin(), R.end());
-        return R;
-    };
-    auto layout_op = [&](const std::vector<int>& R) {
-        DevOp op;
-        std::memset(&op, 0, sizeof(op));
-        op.kind = OPK_LAYOUT;
-        for (int k = 0; k < KR; ++k) op.perm[k] = R[k];
-        int w = 0;
-        for (int b = RT_LANE_BITS; b < T; ++b)
-            if (!contains(R, b)) op.perm[5 + w++] = b;
-        return op;
-    };
-    std::vector<int> R = choose(0);
-    std::vector<DevOp> out;
-    out.push_back(layout_op(R));
-    for (size_t i = 0; i < in.size(); ++i) {
-        DevOp op = in[i];
-        std::vector<int> nd = needs(op);
-        bool fits = true;
-        for (int b : nd)
-            if (!contains(R, b)) fits = false;
-        const bool three_dense = op.kind != OPK_DIAG && op.nq > 2;
-        op.mode = 0;
-        if (three_dense) {
-            op.mode = 1;  // 3-qubit permutations (Toffoli) go through shared memory
-        } else if (!fits) {
-            if ((int)nd.size() <= KR) {
-                R = choose(i);
-                out.push_back(layout_op(R));
-            } else {
-                op.mode = 1;
-            }
-        }
-        // slots under the current layout
-        const DevOp& lay = out.back().kind == OPK_LAYOUT ? out.back() : out.front();
-        (void)lay;
-        for (int t = 0; t < 4; ++t) op.slot[t] = SLOT_OFF << 8;
-        for (int t = 0; t < op.nq; ++t) {
-            const int b = op.lb[t];
-            if (b < 0) {
-                op.slot[t] = SLOT_OFF << 8;
-            } else if (b < RT_LANE_BITS) {
-                op.slot[t] = (SLOT_LANE << 8) | b;
-            } else {
-                int k = -1;
-                for (int j = 0; j < KR; ++j)
-                    if (R[j] == b) k = j;
-                if (k >= 0) {
-                    op.slot[t] = (SLOT_REG << 8) | k;
-                } else {
-                    int w = 0, kw = -1;
-                    for (int bb = RT_LANE_BITS; bb < T; ++bb)
-                        if (!contains(R, bb)) {
-                            if (bb == b) kw = w;
-                            ++w;
-                        }
-                    op.slot[t] = (SLOT_WARP << 8) | kw;
-                }
-            }
-        }
-        // canonical register pairs: the op's qubit 0 on the lower register bit
-        if (op.mode == 0 && op.nq == 2 && op.kind != OPK_DIAG && (op.slot[0] >> 8) == SLOT_REG &&
-            (op.slot[1] >> 8) == SLOT_REG && (op.slot[0] & 255) > (op.slot[1] & 255))
-            swap_qubit_roles(op);
-        out.push_back(op);
-    }
-    p.ops = std::move(out);
-    p.regtile = true;
-}
-
 // ----------------------------------------------------------------------------
 // Stage-sweep scheduling (engine 2).  The tile stays in shared memory; the
 // pass's op list is cut into stages of consecutive ops whose non-diagonal
@@ -683,13 +565,13 @@ void schedule_regtile(Pass& p) {
 // always hit distinct banks.  The kernel folds the rotation into per-thread
 // coefficients, once per op.
 // ----------------------------------------------------------------------------
-void schedule_stages(Pass& p, int amp_bytes, int K) {
+void schedule_stages(Pass& p, int amp_bytes) {
     const int T = p.g.T;
-    if (K != 5) K = 4;
+    constexpr int K = 4;
     if (T < 12 || T > 13) return;
     const int LB = amp_bytes == 8 ? 4 : 3;
     for (const DevOp& op : p.ops)  // adjoint partials and layout ops belong to other kernels
-        if (op.kind == OPK_INNER || op.kind == OPK_LAYOUT || op.kind == OPK_JUMP || op.kind == OPK_STAGE) return;
+        if (op.kind == OPK_INNER || op.kind == OPK_JUMP || op.kind == OPK_STAGE) return;
     std::vector<DevOp> in = std::move(p.ops);
     // 1- and 2-qubit permutations run as dense matrices on the stage registers
     for (DevOp& op : in) {
@@ -734,9 +616,7 @@ void schedule_stages(Pass& p, int amp_bytes, int K) {
         for (int k = 0; k < 4; ++k) h.lb[k] = -1;
         for (int k = 0; k < K; ++k) {
             h.perm[k] = S[k];
-            const int lane = S[k] < LB ? c + a++ : -1;
-            if (K == 4) h.perm[4 + k] = lane;
-            else if (k < 4) h.lb[k] = lane;  // 5-bit stage: bits in perm[0..4], lanes in lb[0..3]
+            h.perm[4 + k] = S[k] < LB ? c + a++ : -1;
         }
         return h;
     };

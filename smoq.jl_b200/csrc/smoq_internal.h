@@ -35,21 +35,15 @@ enum OpKind : int32_t {
     OPK_STAGE = 10,   // stage-sweep engine: header of a stage; perm[0..3] = the stage's 4
                       // tile bits (ascending), perm[4..7] = lane bit feeding the rotation of
                       // each stage bit (-1 none), aux2 = number of member ops that follow;
-                      // nq = 0 marks a single op applied by a plain shared-memory sweep;
-                      // nq = 5 a 5-bit stage (compiled kernels only): perm[0..4] = bits,
-                      // lb[0..3] = rotation lanes
+                      // nq = 0 marks a single op applied by a plain shared-memory sweep
     OPK_INNER = 9,    // adjoint sweep: Im<lambda|G|phi> on 1-2 tile bits, accumulated into
                       // partials column perm[0]; G is a signed monomial: row r holds i^slot[r]
                       // at column perm[1 + r] (slot[r] = INNER_ZERO: an all-zero row);
                       // flags: INNER_DIAGG (G real diagonal), INNER_PRE (cd/cf hold a dense
                       // 2^nq x 2^nq matrix applied to both states first), INNER_PREDIAG
                       // (that matrix is diagonal)
-    OPK_LAYOUT = 8,   // register-tile layout change: perm[0..KR-1] = register bits,
-                      // perm[5..7] = warp bits (tile-local bit positions)
 };
 
-// Placement of an op qubit in the register-tile engine: slot = type << 8 | index
-enum SlotType : int32_t { SLOT_LANE = 0, SLOT_REG = 1, SLOT_WARP = 2, SLOT_OFF = 3 };
 
 // OPK_INNER encoding details
 enum InnerBits : int32_t { INNER_ZERO = 4, INNER_DIAGG = 1, INNER_PRE = 2, INNER_PREDIAG = 8 };
@@ -62,8 +56,8 @@ struct alignas(16) DevOp {
     int32_t nq;         // 1..3 qubits (OPK_DIAG: 0..4)
     int32_t lb[4];      // tile-local bit of qubit t, -1 when the qubit is not a tile bit
     int32_t gb[4];      // global bit of qubit t
-    int32_t slot[4];    // register-tile placement of qubit t (SlotType << 8 | index)
-    int32_t mode;       // register-tile engine: 0 = in registers, 1 = through shared memory
+    int32_t slot[4];    // stage engines: stage position of qubit t; OPK_INNER: the i^k codes
+    int32_t mode;       // unused (kept: the compiled kernels mirror this layout)
     int32_t flags;      // OPK_PARITY2: bit 0 even block diagonal, bit 1 odd block diagonal
     int32_t pad0[2];
     int32_t perm[8];    // OPK_MONO: out[r] = ph[r] * in[perm[r]]
@@ -148,38 +142,25 @@ struct Pass {
     TileGeom g;
     std::vector<DevOp> ops;
     bool epilogue = false;
-    bool regtile = false;   // scheduled for the register-tile engine (ops[0] is OPK_LAYOUT)
     bool staged = false;    // scheduled for the stage-sweep engine (OPK_STAGE headers)
     bool want_jit = false;  // engine 3: compile this staged pass to its own kernel at upload
     const JitKernel* jit = nullptr;
 };
 
-// register-tile engine geometry: 256 threads = 8 warps x 32 lanes; lanes hold
-// tile-local bits 0..4, 3 warp bits, KR = T - 8 register bits per thread
-constexpr int RT_THREADS = 256;
-constexpr int RT_LANE_BITS = 5;
-constexpr int RT_WARP_BITS = 3;
-constexpr int RT_MIN_T = 8;
-
 // planner.cpp
 std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, int Lmin,
                               int epilogue_after_special = -1, int Lreq = 0);
-// turn a planned pass into a register-tile program (layout ops + slots)
-void schedule_regtile(Pass& p);
-// turn a planned pass into stage sweeps (engines 2, 3); amp_bytes selects the bank
-// geometry; K = 4 bits per stage, or 5 (engine 3 only: header bits in perm[0..4],
-// rotation lanes of positions 0..3 in lb[0..3])
-void schedule_stages(Pass& p, int amp_bytes, int K = 4);
+// turn a planned pass into stage sweeps of 4 tile bits (engines 2, 3); amp_bytes
+// selects the bank geometry
+void schedule_stages(Pass& p, int amp_bytes);
 void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op);
 // jit.cpp: compile (or fetch from the process cache) the kernel of a staged complex64 pass
 // (minb_add: that many more CTAs per SM than the default register budget allows)
-const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, bool packed, int groups, std::string& err,
-                                 int minb_add = 0);
+const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, int groups, std::string& err, int minb_add = 0);
 // the tuning-cache key of a staged pass program (hash of its default kernel source)
-uint64_t jit_pass_key(const Pass& p, int nbuf, bool packed);
+uint64_t jit_pass_key(const Pass& p, int nbuf);
 // jit.cpp: generate and compile a staged complex64 pass without a GPU (plan checks)
-bool jit_check_pass(const Pass& p, int nbuf, bool packed, int groups, std::string& err, size_t* cubin_bytes,
-                    std::string* info);
+bool jit_check_pass(const Pass& p, int nbuf, int groups, std::string& err, size_t* cubin_bytes, std::string* info);
 // jit.cpp: NVRTC could be loaded
 bool jit_available();
 
@@ -209,15 +190,12 @@ struct smoq_ctx {
     int use_graphs = 1;
     int engine = -1;                   // fused passes: -1 = auto, 0 = shared-memory sweeps, 1 = register
                                        // tiles, 2 = stage sweeps, 3 = compiled pass kernels
-    int rt_occ[2][2][8] = {};          // CTAs per SM of the register-tile kernel [dtype][epilogue][KR]
     int st_occ[2][2][2] = {};          // CTAs per SM of the stage kernel [dtype][epilogue][GP-1]
     int kernel_timing = 0;             // bracket tile passes with events
     int jit_buffers = 1;               // compiled pass kernels: tile buffers per CTA (1 or 2)
-    int jit_packed = 0;                // compiled pass kernels: FP32x2 arithmetic on group pairs
     int jit_groups = 2;                // compiled pass kernels: 16-amplitude register groups per thread
-    int jit_stage_bits = 4;            // compiled pass kernels: tile bits per register stage (4 or 5)
     bool vqe_resident = true;          // many-circuit VQE: small circuits in one shared-memory launch
-    bool autotune = false;             // time the compiled kernels' variants per pass at plan upload
+    bool autotune = true;              // time the compiled kernels' variants per pass at plan upload
     std::string tune_report;           // the tuner's per-pass timings and choices
     long long launches = 0;            // kernels launched by this ctx
     long long tile_passes = 0;
@@ -253,8 +231,6 @@ cudaError_t launch_convert(smoq_state* dst, smoq_state* src);
 size_t diag_reduce_scratch_doubles(smoq_state* st, int nobs);
 size_t tile_max_smem(int amp_bytes, int T);
 cudaError_t tile_kernels_init(smoq_ctx* ctx);
-cudaError_t regtile_kernels_init(smoq_ctx* ctx);
-cudaError_t launch_regtile(smoq_ctx* ctx, const TileArgs& a, int dtype, bool epi);
 cudaError_t stage_kernels_init(smoq_ctx* ctx);
 cudaError_t launch_stage(smoq_ctx* ctx, const TileArgs& a, int dtype, bool epi);
 cudaError_t launch_jit(smoq_ctx* ctx, const TileArgs& a, const JitKernel* k, bool epi);

@@ -495,7 +495,9 @@ __global__ void __launch_bounds__(1024) adj_colsum_kernel(const double* part, in
 // ---------------------------------------------------------------- many small circuits, one launch
 // A circuit whose two states (phi, lambda) fit one CTA's shared memory runs
 // entirely there: forward program, lambda = H phi and the energy, then the
-// backward program; one CTA per circuit, persistent over the job list.
+// backward program; one CTA per circuit.  The CTAs are persistent and take
+// circuits off a device work queue (an atomic counter over the jobs, sorted by
+// cost, largest first), so uneven circuits balance across the SMs.
 struct ResJob {
     int32_t N;
     int32_t fwd_off, fwd_n;  // forward ops (whole-state tile)
@@ -510,6 +512,8 @@ struct ResArgs {
     double* energy;  // [njobs], <phi|H|phi> / <phi|phi>
     double* norm2;   // [njobs], <phi|phi>
     double* cols;    // [columns of all jobs], zeroed
+    const int32_t* order;  // the queue: job indices, largest cost first
+    int32_t* next;         // queue head, zeroed
     int32_t njobs;
 };
 
@@ -538,8 +542,13 @@ __global__ void __launch_bounds__(256) vqe_resident_kernel(const ResArgs A) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ C dco[16];
     __shared__ double red[2][8];
+    __shared__ int32_t s_job;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int j = blockIdx.x; j < A.njobs; j += gridDim.x) {
+    for (;;) {
+        if (tid == 0) s_job = atomicAdd(A.next, 1);
+        __syncthreads();  // (the job's last barrier keeps thread 0 from overwriting s_job early)
+        if (s_job >= A.njobs) break;
+        const int j = A.order[s_job];
         const ResJob J = A.jobs[j];
         const uint32_t dim = 1u << J.N;
         C* P = reinterpret_cast<C*>(smem_raw);
@@ -1138,8 +1147,15 @@ static smoq_status run_resident(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vqe_
     const size_t b_jobs = al(rj.size() * sizeof(ResJob)), b_ops = al(std::max<size_t>(1, ops.size()) * sizeof(DevOp)),
                  b_terms = al(terms.size() * sizeof(HamTerm)), b_e = al((size_t)n * 8),
                  b_c = al((size_t)std::max(1, ncols) * 8);
+    // the queue order: estimated cost (ops x amplitudes), largest first
+    std::vector<int32_t> order(rj.size());
+    for (size_t u = 0; u < rj.size(); ++u) order[u] = (int32_t)u;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+        return ((int64_t)rj[a].fwd_n + rj[a].bwd_n + 1) << rj[a].N > ((int64_t)rj[b].fwd_n + rj[b].bwd_n + 1) << rj[b].N;
+    });
+    const size_t b_q = al((order.size() + 1) * sizeof(int32_t));
     char* buf = nullptr;
-    VCK(cudaMallocAsync((void**)&buf, b_jobs + b_ops + b_terms + 2 * b_e + b_c, ctx->stream));
+    VCK(cudaMallocAsync((void**)&buf, b_jobs + b_ops + b_terms + 2 * b_e + b_c + b_q, ctx->stream));
     std::unique_ptr<char, std::function<void(char*)>> hold(buf, [ctx](char* q) { cudaFreeAsync(q, ctx->stream); });
     ResArgs A;
     char* c = buf;
@@ -1158,6 +1174,12 @@ static smoq_status run_resident(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vqe_
     c += b_e;
     A.cols = (double*)c;
     VCK(cudaMemsetAsync(c, 0, (size_t)std::max(1, ncols) * 8, ctx->stream));
+    c += b_c;
+    A.next = (int32_t*)c;
+    A.order = (const int32_t*)c + 1;
+    VCK(cudaMemsetAsync(c, 0, sizeof(int32_t), ctx->stream));
+    VCK(cudaMemcpyAsync(c + sizeof(int32_t), order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                        ctx->stream));
     A.njobs = n;
     const size_t amp = dtype == SMOQ_C64 ? 8 : 16;
     const size_t smem = 2 * amp << nmax;
@@ -1224,9 +1246,10 @@ extern "C" smoq_status smoq_energy_grad_jobs(smoq_ctx* ctx, smoq_dtype dtype, co
     // (half the host threads, at most 8: the planning is memory-bound on 4 KB gates)
     const size_t nthreads = std::max<size_t>(1, std::min<size_t>(8, std::thread::hardware_concurrency() / 2));
     const size_t chunk = 4 * nthreads;
-    for (size_t c0 = 0; c0 < large.size(); c0 += chunk) {
+    // plans of the chunk of large circuits starting at c0, on host threads (no CUDA calls)
+    auto plan_chunk = [&, dtype](size_t c0, std::vector<GradPlan>& plans) {
         const size_t nc = std::min(chunk, large.size() - c0);
-        std::vector<GradPlan> plans(nc);
+        plans.assign(nc, GradPlan());
         std::atomic<size_t> next(0);
         auto work = [&]() {
             for (size_t i; (i = next++) < nc;) {
@@ -1238,6 +1261,20 @@ extern "C" smoq_status smoq_energy_grad_jobs(smoq_ctx* ctx, smoq_dtype dtype, co
         for (size_t t = 1; t < std::min(nthreads, nc); ++t) pool.emplace_back(work);
         work();
         for (std::thread& t : pool) t.join();
+    };
+    // the next chunk is planned while the GPU runs this one
+    std::vector<GradPlan> plans, next_plans;
+    std::thread ahead;
+    struct Joiner {
+        std::thread& t;
+        ~Joiner() {
+            if (t.joinable()) t.join();
+        }
+    } joiner{ahead};
+    if (!large.empty()) plan_chunk(0, plans);
+    for (size_t c0 = 0; c0 < large.size(); c0 += chunk) {
+        const size_t nc = plans.size();
+        if (c0 + chunk < large.size()) ahead = std::thread([&, c0]() { plan_chunk(c0 + chunk, next_plans); });
         for (size_t i = 0; i < nc; ++i) {
             const int j = large[c0 + i];
             const smoq_vqe_job& J = jobs[j];
@@ -1248,8 +1285,78 @@ extern "C" smoq_status smoq_energy_grad_jobs(smoq_ctx* ctx, smoq_dtype dtype, co
                 return smoq_internal_fail(ctx, s, why.c_str());
             }
         }
+        if (ahead.joinable()) ahead.join();
+        plans.swap(next_plans);
     }
     return SMOQ_OK;
+}
+
+// ---------------------------------------------------------------- HamiltonianParams -> Pauli terms
+// apply_hamiltonian_bitwise! (cpuQuantumChannelUnitaryEvolutionChebyshev.jl:55) sums, per row,
+// the bonds' ZZ, XX, YY and the fields' Z, X, Y terms with nonzero coefficients
+static void params_to_terms(const double* x_bonds, int nx, const double* y_bonds, int ny, const double* fields,
+                            int nf, std::vector<smoq_pauli_term>& t) {
+    auto add = [&](double c, uint64_t x, uint64_t z) {
+        if (c == 0.0) return;
+        smoq_pauli_term p;
+        p.coef = c;
+        p.xmask = x;
+        p.zmask = z;
+        t.push_back(p);
+    };
+    for (int set = 0; set < 2; ++set) {
+        const double* rows = set ? y_bonds : x_bonds;
+        for (int r = 0; r < (set ? ny : nx); ++r) {
+            const double* b = rows + 5 * r;
+            const uint64_t m = (1ull << (int)b[0]) | (1ull << (int)b[1]);
+            add(b[4], 0, m);   // ZZ
+            add(b[2], m, 0);   // XX
+            add(b[3], m, m);   // YY
+        }
+    }
+    for (int r = 0; r < nf; ++r) {
+        const double* f = fields + 4 * r;
+        const uint64_t m = 1ull << (int)f[0];
+        add(f[3], 0, m);   // Z
+        add(f[1], m, 0);   // X
+        add(f[2], m, m);   // Y
+    }
+}
+
+extern "C" smoq_status smoq_apply_pauli_sum(smoq_state* in, smoq_state* out, const smoq_pauli_term* H, int nterms,
+                                            double* expect);
+
+extern "C" smoq_status smoq_apply_hamiltonian_bitwise(smoq_state* out, smoq_state* in, const double* x_bonds, int nx,
+                                                      const double* y_bonds, int ny, const double* fields, int nf) {
+    if (!in || !out || !in->ctx) return SMOQ_ERR_BADINPUT;
+    if (nx < 0 || ny < 0 || nf < 0 || (nx && !x_bonds) || (ny && !y_bonds) || (nf && !fields))
+        return smoq_internal_fail(in->ctx, SMOQ_ERR_BADINPUT, "apply_hamiltonian_bitwise: bad term arrays");
+    for (int r = 0; r < nx + ny; ++r) {
+        const double* b = r < nx ? x_bonds + 5 * r : y_bonds + 5 * (r - nx);
+        if (b[0] < 0 || b[0] >= in->N || b[1] < 0 || b[1] >= in->N || (int)b[0] == (int)b[1])
+            return smoq_internal_fail(in->ctx, SMOQ_ERR_BADINPUT, "apply_hamiltonian_bitwise: bond site out of range");
+    }
+    for (int r = 0; r < nf; ++r)
+        if (fields[4 * r] < 0 || fields[4 * r] >= in->N)
+            return smoq_internal_fail(in->ctx, SMOQ_ERR_BADINPUT, "apply_hamiltonian_bitwise: field site out of range");
+    std::vector<smoq_pauli_term> t;
+    params_to_terms(x_bonds, nx, y_bonds, ny, fields, nf, t);
+    if (t.empty()) {  // H = 0
+        smoq_pauli_term z;
+        z.coef = 0.0;
+        z.xmask = z.zmask = 0;
+        t.push_back(z);
+    }
+    return smoq_apply_pauli_sum(in, out, t.data(), (int)t.size(), nullptr);
+}
+
+extern "C" smoq_status smoq_apply_h_xxz(smoq_state* psi, smoq_state* out, double Jx, double Jy, double Jz, double h) {
+    if (!psi) return SMOQ_ERR_BADINPUT;
+    const int N = psi->N;
+    std::vector<double> bonds, fields;
+    for (int i = 0; i + 1 < N; ++i) bonds.insert(bonds.end(), {(double)i, (double)(i + 1), Jx, Jy, Jz});
+    for (int i = 0; i < N; ++i) fields.insert(fields.end(), {(double)i, h, 0.0, 0.0});
+    return smoq_apply_hamiltonian_bitwise(out, psi, bonds.data(), N - 1, nullptr, 0, fields.data(), N);
 }
 
 // ---------------------------------------------------------------- H psi

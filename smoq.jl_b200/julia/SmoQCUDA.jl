@@ -16,7 +16,11 @@ export CuContext, CuState, apply_rx_psi!, apply_ry_psi!, apply_rz_psi!, apply_ha
        expect_local, expect_corr, get_expectation_pauli_string, get_norm, normalize_state!,
        TrotterPlan, evolve_trotter_psi!, apply_fast_trotter_step_cpu!, energy_and_gradient,
        energy_and_gradient_jobs, lindblad_mcwf_batched!, apply_hamiltonian_bitwise!, sample_bitstrings,
-       projective_measurement_all!, measure_z_single!, set_engine!, run_mcwf_simulation
+       projective_measurement_all!, measure_z_single!, set_engine!, run_mcwf_simulation,
+       apply_gate!, apply_2qubit_gate!, apply_one_qubit_gate_bitwise_cpu!, apply_two_qubit_gate_bitwise_cpu!,
+       apply_circuit!, apply_channel_dephasing!, apply_channel_depolarizing!, apply_channel_amplitude_damping!,
+       apply_channel_bit_flip!, apply_channel_phase_flip!, projective_measurement!, reset_state!,
+       VQECost, calculate_gradients, apply_H_xxz!, apply_H_ising!, energy_and_gradient_noisy
 
 const lib = joinpath(@__DIR__, "..", "lib", "libsmoq_cuda.so")
 const SMOQ_C64 = Cint(0)
@@ -56,6 +60,21 @@ mutable struct CuState
     end
 end
 
+# host <-> device: CuState(ctx, psi::Vector{ComplexF64}) uploads, Vector(psi) downloads
+function CuState(ctx::CuContext, ψ::Vector{ComplexF64})
+    N = trailing_zeros(length(ψ))
+    length(ψ) == 1 << N || error("State dimension mismatch")
+    s = CuState(ctx, N)
+    check(ccall((:smoq_state_upload, lib), Cint, (Ptr{Cvoid}, Ptr{ComplexF64}, Csize_t), s.h, ψ, sizeof(ψ)), ctx)
+    s
+end
+function Base.Vector(ψ::CuState)
+    out = Vector{ComplexF64}(undef, ψ.batch << ψ.N)
+    check(ccall((:smoq_state_download, lib), Cint, (Ptr{Cvoid}, Ptr{ComplexF64}, Csize_t), ψ.h, out, sizeof(out)),
+          ψ.ctx)
+    out
+end
+
 # ---------------------------------------------------------------- gates
 for (jl, c) in ((:apply_rx_psi!, :smoq_apply_rx), (:apply_ry_psi!, :smoq_apply_ry), (:apply_rz_psi!, :smoq_apply_rz))
     @eval $jl(ψ::CuState, k::Int, θ::Float64, N::Int) =
@@ -83,6 +102,26 @@ for (jl, c) in ((:apply_ccz_psi!, :smoq_apply_ccz), (:apply_toffoli_psi!, :smoq_
     @eval $jl(ψ::CuState, a::Int, b::Int, t::Int, N::Int) =
         (check(ccall(($(QuoteNode(c)), lib), Cint, (Ptr{Cvoid}, Cint, Cint, Cint), ψ.h, a - 1, b - 1, t - 1), ψ.ctx); ψ)
 end
+
+# generic matrices.  apply_gate!(psi, U, qubit, N) (RandomUnitaries.jl:230) and
+# apply_one_qubit_gate_bitwise_cpu!(psi, U, qubit, N) (Trotter.jl:77): U a 2x2 Matrix{ComplexF64};
+# apply_2qubit_gate! (RandomUnitaries.jl:317) conjugates U by SWAP when q1 > q2 (convention 1);
+# apply_two_qubit_gate_bitwise_cpu! (Trotter.jl:107) swaps the qubits and keeps U (convention 0)
+function _u1(ψ::CuState, U::Matrix{ComplexF64}, q::Int)
+    size(U) == (2, 2) || error("U must be 2x2")
+    check(ccall((:smoq_apply_u1, lib), Cint, (Ptr{Cvoid}, Cint, Ptr{ComplexF64}), ψ.h, q - 1, U), ψ.ctx)
+    ψ
+end
+function _u2(ψ::CuState, U::Matrix{ComplexF64}, q1::Int, q2::Int, convention::Int)
+    size(U) == (4, 4) || error("U must be 4x4")
+    check(ccall((:smoq_apply_u2, lib), Cint, (Ptr{Cvoid}, Cint, Cint, Ptr{ComplexF64}, Cint),
+                ψ.h, q1 - 1, q2 - 1, U, convention), ψ.ctx)
+    ψ
+end
+apply_gate!(ψ::CuState, U::Matrix{ComplexF64}, qubit::Int, N::Int) = _u1(ψ, U, qubit)
+apply_one_qubit_gate_bitwise_cpu!(ψ::CuState, U::Matrix{ComplexF64}, qubit::Int, N::Int) = _u1(ψ, U, qubit)
+apply_2qubit_gate!(ψ::CuState, U::Matrix{ComplexF64}, q1::Int, q2::Int, N::Int) = _u2(ψ, U, q1, q2, 1)
+apply_two_qubit_gate_bitwise_cpu!(ψ::CuState, U::Matrix{ComplexF64}, q1::Int, q2::Int, N::Int) = _u2(ψ, U, q1, q2, 0)
 
 # --------------------------------------------------------- observables
 function _out(f, ψ::CuState, args...)
@@ -163,9 +202,110 @@ struct COp
     type::Int32
     q::NTuple{3,Int32}
     param::Int32
-    pad::Int32
+    if_outcome::Int32
     angle::Float64
     U::NTuple{32,Float64}
+end
+
+# the CircuitOperation symbols (cpuVariationalQuantumCircuitBuilder.jl:82-94) -> smoq_op types
+const GATE_CODE = Dict(:rx => 0, :ry => 1, :rz => 2, :h => 3, :x => 4, :y => 5, :z => 6, :s => 7, :sdg => 8,
+                       :t => 9, :tdg => 10, :cz => 11, :cnot => 12, :cx => 12, :rxx => 13, :ryy => 14, :rzz => 15,
+                       :cry => 16, :ccz => 17, :toffoli => 18)
+const NOISE_CODE = Dict(:depolarizing => 32, :amplitude_damping => 33, :dephasing => 34, :bit_flip => 35,
+                        :phase_flip => 36, :phase_damping => 37, :thermal_relaxation => 38)
+const MEASURE_CODE = Dict(:measure_z => 48, :measure_x => 49, :measure_y => 50, :measure => 48)
+const OTHER_CODE = Dict(:reset => 51, :trace_out => 52, :lindblad_step => 53)
+const RESET_TARGET = Dict(:zero => 0, :one => 1, :plus => 2, :minus => 3)
+const NOU = ntuple(_ -> 0.0, 32)
+
+"the reference's CircuitOperation list (any object with its fields) as smoq_op records:
+one record per gate, one per qubit of a noise / measure / reset op"
+function c_ops(operations)
+    out = COp[]
+    for op in operations
+        t = op.type
+        if haskey(GATE_CODE, t)
+            q = ntuple(k -> k <= length(op.qubits) ? Int32(op.qubits[k] - 1) : Int32(0), 3)
+            push!(out, COp(GATE_CODE[t], q, op.param_idx > 0 ? op.param_idx - 1 : -1, op.if_outcome,
+                           op.fixed_angle, NOU))
+        else
+            code = get(NOISE_CODE, t, get(MEASURE_CODE, t, get(OTHER_CODE, t, -1)))
+            code < 0 && error("Unknown operation type: $t")
+            for q in op.qubits
+                q2 = t === :reset ? RESET_TARGET[op.target_state] : 0
+                push!(out, COp(code, (Int32(q - 1), Int32(q2), Int32(0)), -1, op.if_outcome, op.p, NOU))
+            end
+        end
+    end
+    out
+end
+n_measurements(operations) = sum((length(op.qubits) for op in operations if haskey(MEASURE_CODE, op.type)); init=0)
+
+"""apply_circuit!(ψ::CuState, circuit, θ) -- cpuVariationalQuantumCircuitExecutor.jl:95.
+`circuit` is the reference's ParameterizedCircuit (fields N, operations).  Gate-only
+circuits run as fused tile passes; circuits with noise, measurements, resets or
+if_outcome conditions run every state of ψ as one trajectory (Philox draws, key seed,
+counter (op index, 0x80000000, traj_offset + b)).  Returns (state = ψ, outcomes), the
+fields of the reference's CircuitResult; outcomes is a Vector (one trajectory) or a
+Matrix (outcome, trajectory)."""
+function apply_circuit!(ψ::CuState, circuit, θ::Vector{Float64}; seed::UInt64=UInt64(1234),
+                        traj_offset::UInt64=UInt64(0))
+    ψ.N == circuit.N || error("State dimension mismatch")
+    length(θ) >= circuit.n_params || error("Not enough parameters")
+    ops = c_ops(circuit.operations)
+    plain = all(op -> haskey(GATE_CODE, op.type) && op.if_outcome == 0, circuit.operations)
+    if plain
+        check(ccall((:smoq_apply_sequence, lib), Cint, (Ptr{Cvoid}, Ptr{COp}, Cint, Ptr{Float64}),
+                    ψ.h, ops, length(ops), θ), ψ.ctx)
+        return (state = ψ, outcomes = Int[])
+    end
+    nm = n_measurements(circuit.operations)
+    out = Matrix{Int32}(undef, max(nm, 1), ψ.batch)
+    check(ccall((:smoq_apply_circuit_mcwf, lib), Cint,
+                (Ptr{Cvoid}, Ptr{COp}, Cint, Ptr{Float64}, UInt64, UInt64, Ptr{Int32}),
+                ψ.h, ops, length(ops), θ, seed, traj_offset, out), ψ.ctx)
+    o = Int.(out[1:nm, :])
+    (state = ψ, outcomes = ψ.batch == 1 ? vec(o) : o)
+end
+
+# the public channels on pure states (cpuQuantumChannelKrausOperators.jl:426-556):
+# one stochastic unravelling per state of ψ
+for (jl, t) in ((:apply_channel_dephasing!, :dephasing), (:apply_channel_depolarizing!, :depolarizing),
+                (:apply_channel_amplitude_damping!, :amplitude_damping), (:apply_channel_bit_flip!, :bit_flip),
+                (:apply_channel_phase_flip!, :phase_flip))
+    @eval function $jl(ψ::CuState, p::Float64, qubits::Vector{Int}, N::Int; seed::UInt64=UInt64(1234),
+                       traj_offset::UInt64=UInt64(0))
+        ops = [COp($(NOISE_CODE[t]), (Int32(q - 1), Int32(0), Int32(0)), -1, 0, p, NOU) for q in qubits]
+        check(ccall((:smoq_apply_circuit_mcwf, lib), Cint,
+                    (Ptr{Cvoid}, Ptr{COp}, Cint, Ptr{Float64}, UInt64, UInt64, Ptr{Int32}),
+                    ψ.h, ops, length(ops), C_NULL, seed, traj_offset, C_NULL), ψ.ctx)
+        ψ
+    end
+end
+
+"projective_measurement!(ψ, qubits, basis, N) -- cpuQuantumStateMeasurements.jl:319: (outcomes, ψ)"
+function projective_measurement!(ψ::CuState, qubits::Vector{Int}, basis::Symbol, N::Int; seed::UInt64=UInt64(1234),
+                                 traj_offset::UInt64=UInt64(0))
+    code = get(MEASURE_CODE, Symbol("measure_", basis), -1)
+    code < 0 && error("Unknown basis: $basis. Use :z, :x, :y, or provide Vector/Matrix.")
+    ops = [COp(code, (Int32(q - 1), Int32(0), Int32(0)), -1, 0, 0.0, NOU) for q in qubits]
+    out = Matrix{Int32}(undef, length(qubits), ψ.batch)
+    check(ccall((:smoq_apply_circuit_mcwf, lib), Cint,
+                (Ptr{Cvoid}, Ptr{COp}, Cint, Ptr{Float64}, UInt64, UInt64, Ptr{Int32}),
+                ψ.h, ops, length(ops), C_NULL, seed, traj_offset, out), ψ.ctx)
+    (ψ.batch == 1 ? Int.(vec(out)) : Int.(out)), ψ
+end
+
+"reset_state!(ψ, qubits, target_states, N) -- cpuQuantumStateMeasurements.jl:555"
+function reset_state!(ψ::CuState, qubits::Vector{Int}, targets, N::Int; seed::UInt64=UInt64(1234),
+                      traj_offset::UInt64=UInt64(0))
+    ts = targets isa Symbol ? fill(targets, length(qubits)) : targets
+    length(ts) == length(qubits) || error("Must specify target for each qubit")
+    ops = [COp(51, (Int32(q - 1), Int32(RESET_TARGET[t]), Int32(0)), -1, 0, 0.0, NOU) for (q, t) in zip(qubits, ts)]
+    check(ccall((:smoq_apply_circuit_mcwf, lib), Cint,
+                (Ptr{Cvoid}, Ptr{COp}, Cint, Ptr{Float64}, UInt64, UInt64, Ptr{Int32}),
+                ψ.h, ops, length(ops), C_NULL, seed, traj_offset, C_NULL), ψ.ctx)
+    ψ
 end
 
 "θ: n_params × batch; returns (energies, grads::Matrix)"
@@ -181,11 +321,67 @@ function energy_and_gradient(ctx::CuContext, N::Int, ops::Vector{COp}, n_params:
     E, G
 end
 
-# ChainRulesCore (Manifest.toml:254, 1.26.0) -- the adjoint behind an rrule:
-#   function ChainRulesCore.rrule(::typeof(vqe_energy), θ)
-#       E, G = energy_and_gradient(ctx, N, ops, length(θ), H, reshape(θ, :, 1))
-#       return E[1], Δ -> (NoTangent(), Δ .* G[:, 1])
-#   end
+"""VQECost(ctx, circuit, H; dtype): the VQE cost θ -> <0|U(θ)^dag H U(θ)|0> of the
+reference's cost closures (scripts_variational_quantum_circuits/demo_vqe_dm_vs_mcwf.jl:189-202)
+as a callable object; H is a Vector of (coef, Dict(qubit => :X/:Y/:Z)) terms."""
+struct VQECost
+    ctx::CuContext
+    N::Int
+    ops::Vector{COp}
+    n_params::Int
+    H::Vector{CPauliTerm}
+    dtype::Cint
+end
+function pauli_terms(H)
+    map(H) do (c, letters)
+        x = UInt64(0); z = UInt64(0)
+        for (q, P) in letters
+            b = UInt64(1) << (q - 1)
+            (P === :X || P === :Y) && (x |= b)
+            (P === :Z || P === :Y) && (z |= b)
+        end
+        CPauliTerm(c, x, z)
+    end
+end
+VQECost(ctx::CuContext, circuit, H; dtype=SMOQ_C128) =
+    VQECost(ctx, circuit.N, c_ops(circuit.operations), circuit.n_params, pauli_terms(H), dtype)
+(c::VQECost)(θ::AbstractVector{<:Real}) =
+    energy_and_gradient(c.ctx, c.N, c.ops, c.n_params, c.H, reshape(Float64.(θ), :, 1); dtype=c.dtype)[1][1]
+
+"""calculate_gradients(cost::VQECost, θ) -- cpuVariationalQuantumCircuitGradients.jl:88 with the
+adjoint method as the backend (one forward sweep, one uncompute sweep) instead of Enzyme or the
+parameter shift; returns the gradient vector."""
+calculate_gradients(c::VQECost, θ::Vector{Float64}) =
+    vec(energy_and_gradient(c.ctx, c.N, c.ops, c.n_params, c.H, reshape(θ, :, 1); dtype=c.dtype)[2])
+
+# ChainRulesCore.rrule for the cost: reverse-mode AD (Zygote, a dependency of the reference's
+# Project.toml, which loads ChainRulesCore 1.26.0, Manifest.toml:254) calls the adjoint kernels
+# instead of differentiating through the gate loops.
+import Zygote
+const ChainRulesCore = Zygote.ChainRulesCore
+function ChainRulesCore.rrule(c::VQECost, θ::AbstractVector{<:Real})
+    E, G = energy_and_gradient(c.ctx, c.N, c.ops, c.n_params, c.H, reshape(Float64.(θ), :, 1); dtype=c.dtype)
+    vqe_cost_pullback(ΔE) = (ChainRulesCore.NoTangent(), ΔE .* G[:, 1])
+    return E[1], vqe_cost_pullback
+end
+
+"""energy_and_gradient_noisy(ctx, circuit, H, θ; seed, traj_offset, n_traj, checkpoint_every)
+-- the path-wise adjoint gradient of a noisy circuit along fixed trajectories
+(smoq_energy_grad_mcwf): returns (energies[n_traj], grads[n_params, n_traj])."""
+function energy_and_gradient_noisy(ctx::CuContext, circuit, H, θ::Vector{Float64}; seed::UInt64=UInt64(1234),
+                                   traj_offset::UInt64=UInt64(0), n_traj::Int=1, checkpoint_every::Int=1,
+                                   dtype=SMOQ_C128)
+    ops = c_ops(circuit.operations)
+    terms = pauli_terms(H)
+    E = Vector{Float64}(undef, n_traj)
+    G = Matrix{Float64}(undef, max(circuit.n_params, 1), n_traj)
+    check(ccall((:smoq_energy_grad_mcwf, lib), Cint,
+                (Ptr{Cvoid}, Cint, Cint, Ptr{COp}, Cint, Cint, Ptr{CPauliTerm}, Cint, Ptr{Float64}, UInt64, UInt64,
+                 Cint, Cint, Ptr{Float64}, Ptr{Float64}),
+                ctx.h, circuit.N, dtype, ops, length(ops), circuit.n_params, terms, length(terms), θ, seed,
+                traj_offset, n_traj, checkpoint_every, E, G), ctx)
+    E, G[1:circuit.n_params, :]
+end
 
 # ------------------------------------------------ many circuits (C4b)
 struct CVqeJob
@@ -239,7 +435,27 @@ function lindblad_mcwf_batched!(ψ::CuState, plan::TrotterPlan, jumps::Vector{CJ
 end
 
 # ------------------------------------------------ H ψ, sampling, measurement
-"apply_hamiltonian_bitwise!(ψ_out, ψ_in, params) -- Chebyshev.jl:55, for a Pauli sum; returns <ψ_in|H|ψ_in>"
+"""apply_hamiltonian_bitwise!(ψ_out, ψ_in, params::HamiltonianParams) -- Chebyshev.jl:55:
+ψ_out = H ψ_in for the reference's HamiltonianParams (fields x_bonds, y_bonds of CouplingTerm
+(i, j, Jxx, Jyy, Jzz) and fields of FieldTerm (idx, hx, hy, hz), 1-based sites)"""
+function apply_hamiltonian_bitwise!(ψout::CuState, ψin::CuState, params)
+    rows(bs) = isempty(bs) ? Float64[] : reduce(vcat, [[b.i - 1, b.j - 1, b.Jxx, b.Jyy, b.Jzz] for b in bs])
+    xb = rows(params.x_bonds); yb = rows(params.y_bonds)
+    fb = isempty(params.fields) ? Float64[] : reduce(vcat, [[f.idx - 1, f.hx, f.hy, f.hz] for f in params.fields])
+    check(ccall((:smoq_apply_hamiltonian_bitwise, lib), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Float64}, Cint, Ptr{Float64}, Cint, Ptr{Float64}, Cint),
+                ψout.h, ψin.h, xb, length(params.x_bonds), yb, length(params.y_bonds), fb, length(params.fields)),
+          ψin.ctx)
+    ψout
+end
+"apply_H_xxz!(ψ, out, N, Jx, Jy, Jz, h) -- cpuQuantumStateLanczos.jl:157"
+apply_H_xxz!(ψ::CuState, out::CuState, N::Int, Jx::Float64, Jy::Float64, Jz::Float64, h::Float64) =
+    (check(ccall((:smoq_apply_h_xxz, lib), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Cdouble, Cdouble, Cdouble, Cdouble),
+                 ψ.h, out.h, Jx, Jy, Jz, h), ψ.ctx); out)
+"apply_H_ising!(ψ, out, N, J, h) -- cpuQuantumStateLanczos.jl:220"
+apply_H_ising!(ψ::CuState, out::CuState, N::Int, J::Float64, h::Float64) = apply_H_xxz!(ψ, out, N, 0.0, 0.0, J, h)
+
+"apply_hamiltonian_bitwise! for a Pauli sum; returns <ψ_in|H|ψ_in>"
 function apply_hamiltonian_bitwise!(ψout::CuState, ψin::CuState, H::Vector{CPauliTerm})
     e = Vector{Float64}(undef, ψin.batch)
     check(ccall((:smoq_apply_pauli_sum, lib), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{CPauliTerm}, Cint, Ptr{Float64}),
@@ -299,8 +515,8 @@ function run_mcwf_simulation(psi0, H_params, gates::TrotterPlan, padded_u::Vecto
     permutedims(reshape(X, n_ops, T))   # X[k, f], as the reference's Matrix (T x n_ops)
 end
 
-"fused-pass engine: -1 auto (default), 0 shared-memory sweeps, 1 register tiles, 2 stage
-sweeps, 3 compiled pass kernels"
+"fused-pass engine: -1 auto (default), 0 shared-memory sweeps, 2 stage sweeps, 3 compiled
+pass kernels"
 set_engine!(ctx::CuContext, e::Integer) =
     check(ccall((:smoq_ctx_set_option, lib), Cint, (Ptr{Cvoid}, Cint, Clonglong), ctx.h, 7, e), ctx)
 

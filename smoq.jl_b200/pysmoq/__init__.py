@@ -822,13 +822,40 @@ class PauliSum:
         return arr
 
 
-def apply_hamiltonian_bitwise(psi_out: CuState, psi_in: CuState, H: PauliSum):
-    """apply_hamiltonian_bitwise!(psi_out, psi_in, params): psi_out = H psi_in; returns
-    Re <psi_in|H|psi_in> (per state)."""
+def apply_pauli_sum(psi_out: CuState, psi_in: CuState, H: PauliSum):
+    """psi_out = H psi_in for a Pauli sum; returns Re <psi_in|H|psi_in> (per state)."""
     e = np.empty(psi_in.batch)
     ck(lib.smoq_apply_pauli_sum(psi_in.h, psi_out.h, H.c_terms(), len(H.terms), dptr(e)), psi_in.ctx.h,
-       "apply_hamiltonian_bitwise")
+       "apply_pauli_sum")
     return e[0] if psi_in.batch == 1 else e
+
+
+def apply_hamiltonian_bitwise(psi_out: CuState, psi_in: CuState, params):
+    """apply_hamiltonian_bitwise!(psi_out, psi_in, params::HamiltonianParams)
+    (cpuQuantumChannelUnitaryEvolutionChebyshev.jl:55): psi_out = H psi_in.  `params` is a
+    HamiltonianParams (1-based sites, as the reference's), or a PauliSum (then the
+    return value is Re <psi_in|H|psi_in> per state)."""
+    if isinstance(params, PauliSum):
+        return apply_pauli_sum(psi_out, psi_in, params)
+    xb = np.array([[b.i - 1, b.j - 1, b.Jxx, b.Jyy, b.Jzz] for b in params.x_bonds], dtype=np.float64).reshape(-1)
+    yb = np.array([[b.i - 1, b.j - 1, b.Jxx, b.Jyy, b.Jzz] for b in params.y_bonds], dtype=np.float64).reshape(-1)
+    fb = np.array([[f.idx - 1, f.hx, f.hy, f.hz] for f in params.fields], dtype=np.float64).reshape(-1)
+    ck(lib.smoq_apply_hamiltonian_bitwise(psi_out.h, psi_in.h, dptr(xb), len(params.x_bonds), dptr(yb),
+                                          len(params.y_bonds), dptr(fb), len(params.fields)),
+       psi_in.ctx.h, "apply_hamiltonian_bitwise")
+    return psi_out
+
+
+def apply_H_xxz(psi: CuState, out: CuState, N: int, Jx: float, Jy: float, Jz: float, h: float):
+    """apply_H_xxz! (cpuQuantumStateLanczos.jl:157)"""
+    _n(psi, N)
+    ck(lib.smoq_apply_h_xxz(psi.h, out.h, Jx, Jy, Jz, h), psi.ctx.h, "apply_H_xxz")
+    return out
+
+
+def apply_H_ising(psi: CuState, out: CuState, N: int, J: float, h: float):
+    """apply_H_ising! (cpuQuantumStateLanczos.jl:220)"""
+    return apply_H_xxz(psi, out, N, 0.0, 0.0, J, h)
 
 
 def energy(ctx: Context, circuit: ParameterizedCircuit, H: PauliSum, theta, dtype: int = C128):
@@ -851,6 +878,24 @@ def energy_and_gradient(ctx: Context, circuit: ParameterizedCircuit, H: PauliSum
     ck(lib.smoq_energy_grad(ctx.h, circuit.N, dtype, ops, len(circuit.operations), circuit.n_params, H.c_terms(),
                             len(H.terms), B, dptr(th), dptr(e), dptr(g)), ctx.h, "energy_grad")
     return e, g
+
+
+def energy_and_gradient_noisy(ctx: Context, circuit: ParameterizedCircuit, H: PauliSum, theta, seed: int = 1234,
+                              traj_offset: int = 0, n_traj: int = 1, checkpoint_every: int = 1, dtype: int = C128,
+                              gradient: bool = True):
+    """Energy and path-wise adjoint gradient of a noisy circuit along the trajectories
+    traj_offset .. traj_offset + n_traj - 1 (the draws of apply_circuit with the same seed),
+    from |0...0>.  Returns (energies[n_traj], grads[n_traj, P])."""
+    th = np.ascontiguousarray(theta, dtype=np.float64).reshape(-1)
+    if th.size < circuit.n_params:
+        raise SmoqError(_lib.SMOQ_ERR_BADINPUT, "Not enough parameters")
+    arr, n = _c_ops(circuit.operations)
+    e = np.empty(n_traj)
+    g = np.empty((n_traj, max(1, circuit.n_params))) if gradient else None
+    ck(lib.smoq_energy_grad_mcwf(ctx.h, circuit.N, dtype, arr, n, circuit.n_params, H.c_terms(), len(H.terms),
+                                 dptr(th), seed, traj_offset, n_traj, checkpoint_every, dptr(e), dptr(g)),
+       ctx.h, "energy_grad_mcwf")
+    return e, (g[:, :circuit.n_params] if gradient else None)
 
 
 def energy_and_gradient_jobs(ctx: Context, jobs, dtype: int = C128, gradient: bool = True):
@@ -878,7 +923,7 @@ def energy_and_gradient_jobs(ctx: Context, jobs, dtype: int = C128, gradient: bo
 
 # ------------------------------------------------------ planner introspection
 def debug_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtype: int = C128, tile_bits: int = 12,
-               low_bits: int = 4, engine: int = 1):
+               low_bits: int = 4, engine: int = 0):
     """Host-only view of how smoq_apply_sequence splits `ops` into tile passes
     (as scheduled for fused-pass `engine`).
     Returns a list of passes: {"T","L","H","hb","ops":[{"kind","nq","lb","gb","perm","c"}]}."""

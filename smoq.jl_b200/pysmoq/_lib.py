@@ -19,8 +19,8 @@ C64, C128 = 0, 1
  G_CRY, G_CCZ, G_TOFFOLI, G_U1, G_U2) = range(21)
 
 (OPT_TILE_BITS_C64, OPT_TILE_BITS_C128, OPT_LOW_BITS_C64, OPT_LOW_BITS_C128, OPT_USE_GRAPHS, OPT_KERNEL_TIMING,
- OPT_ENGINE, OPT_JIT_BUFFERS, OPT_JIT_PACKED, OPT_JIT_GROUPS, OPT_JIT_STAGE_BITS, OPT_VQE_RESIDENT,
- OPT_AUTOTUNE) = range(1, 14)
+ OPT_ENGINE, OPT_JIT_BUFFERS) = range(1, 9)
+OPT_JIT_GROUPS, OPT_VQE_RESIDENT, OPT_AUTOTUNE = 10, 12, 13
 
 
 # operations of smoq_apply_circuit_mcwf beyond the gates (one qubit each)
@@ -153,6 +153,8 @@ _SIGS = {
                          C.c_int, C.c_int, _dp, _dp, _dp],
     "smoq_jit_available": [],
     "smoq_apply_pauli_sum": [_vp, _vp, C.POINTER(SmoqPauliTerm), C.c_int, _dp],
+    "smoq_apply_hamiltonian_bitwise": [_vp, _vp, _dp, C.c_int, _dp, C.c_int, _dp, C.c_int],
+    "smoq_apply_h_xxz": [_vp, _vp, C.c_double, C.c_double, C.c_double, C.c_double],
     "smoq_dm_plan_create": [_vp, C.c_int, C.c_int, C.POINTER(SmoqTrotterGate), C.c_int, C.POINTER(SmoqJumpOp),
                             C.c_int, C.c_double, C.POINTER(C.c_void_p)],
     "smoq_dm_expect_zstrings": [_vp, C.c_int, C.POINTER(C.c_uint64), C.c_int, _dp],

@@ -72,11 +72,11 @@ def test_tile_width_variations(ctx, tile_bits):
         ctx.set_option(S._lib.OPT_LOW_BITS_C128, 4)
 
 
-@pytest.mark.parametrize("engine", [0, 1])
+@pytest.mark.parametrize("engine", [0, 2])
 @pytest.mark.parametrize("N,tile_bits", [(9, 8), (12, 9), (16, 10), (18, 13), (20, 11)])
-def test_both_engines_and_register_widths(ctx, engine, N, tile_bits):
-    """shared-memory sweeps (engine 0) and register tiles (engine 1, every register
-    width KR = tile_bits - 8) give the oracle's state on a benchmark circuit"""
+def test_engines_and_tile_widths(ctx, engine, N, tile_bits):
+    """shared-memory sweeps (engine 0) at every tile width and stage sweeps (engine 2,
+    on the passes of tile width 12-13) give the oracle's state on a benchmark circuit"""
     lines = json.load(open(os.path.join(GOLD, "circuits.json")))[str(N - N % 2)]
     g_ops, o_ops = circuit_ops(lines[:600])
     g_ops = [op for op in g_ops if max(op.qubits) <= N]

@@ -105,3 +105,37 @@ def test_pauli_sum_apply_matches_dense(ctx, dtype, tol):
     e = S.apply_hamiltonian_bitwise(b, a, H)
     assert np.max(np.abs(b.download() - Hd @ psi)) < tol * 10
     assert abs(e - np.real(np.vdot(psi, Hd @ psi))) < tol * 10
+
+
+@pytest.mark.parametrize("N,dtype,tol", [(10, S.C128, 1e-12), (15, S.C128, 1e-12), (15, S.C64, 5e-6)])
+def test_apply_hamiltonian_bitwise_vs_oracle(ctx, N, dtype, tol):
+    """apply_hamiltonian_bitwise! at the reference's interface (HamiltonianParams: a 2-rail
+    grid with x and y bonds, anisotropic couplings, random fields with X, Y and Z parts)
+    and apply_H_xxz! / apply_H_ising!, against the oracle's restatement of their loops"""
+    import oracle as O
+    rng = np.random.default_rng(N)
+    Nx, Ny = (N + 1) // 2, 2
+    N = Nx * Ny if Nx * Ny <= N else N
+    params = S.build_hamiltonian_parameters(Nx, Ny, (1.0, 0.7, -0.4), (0.3, 0.0, 0.9), (0.0, 0.0, 0.0))
+    for f in params.fields:
+        f.hx, f.hy, f.hz = (float(v) for v in rng.normal(size=3))
+    params.N = Nx * Ny
+    N = params.N
+    psi = rand_state(N, 31)
+    cast = np.complex128 if dtype == S.C128 else np.complex64
+    a = S.CuState(ctx, N, dtype, basis=None)
+    a.upload(psi.astype(cast))
+    b = S.CuState(ctx, N, dtype, basis=0)
+    S.apply_hamiltonian_bitwise(b, a, params)
+    rows = lambda bonds: [[t.i, t.j, t.Jxx, t.Jyy, t.Jzz] for t in bonds]
+    want = O.apply_hamiltonian_bitwise(psi.astype(cast).astype(np.complex128), rows(params.x_bonds),
+                                       rows(params.y_bonds), [[f.idx, f.hx, f.hy, f.hz] for f in params.fields], N)
+    scale = np.max(np.abs(want))
+    assert np.max(np.abs(b.download() - want)) < tol * scale
+    for Jx, Jy, Jz, h in ((1.0, 1.0, 0.5, 0.3), (0.0, 0.0, -1.0, -1.0)):
+        if Jx == 0.0:
+            S.apply_H_ising(a, b, N, Jz, h)
+        else:
+            S.apply_H_xxz(a, b, N, Jx, Jy, Jz, h)
+        want = O.apply_H_xxz(psi.astype(cast).astype(np.complex128), N, Jx, Jy, Jz, h)
+        assert np.max(np.abs(b.download() - want)) < tol * np.max(np.abs(want))

@@ -335,3 +335,30 @@ def test_dm_superoperator_algebra_matches_dense_lindblad():
             got = np.asfortranarray(rho0.copy())
             O.dm_dissipator(got, (ty, q, gamma), dt, N)
             assert np.max(np.abs(got - want)) < 1e-13, (ty, q)
+
+
+def test_oracle_hamiltonian_apply_vs_dense_and_lanczos():
+    """the oracle's restatement of apply_hamiltonian_bitwise! equals the dense
+    Pauli sum (Y the Pauli Y, as construct_sparse_hamiltonian builds it,
+    cpuHamiltonianBuilder.jl:297), and equals its restatement of apply_H_xxz!
+    (cpuQuantumStateLanczos.jl:157) for the same chain"""
+    import dense_ref as Dr
+    N = 6
+    rng = np.random.default_rng(9)
+    psi = Dr.random_state(N, rng)
+    xb = [[i, i + 1, *rng.normal(size=3)] for i in range(1, N)]
+    yb = [[1, 4, 0.2, -0.6, 0.4]]
+    fields = [[i, *rng.normal(size=3)] for i in range(1, N + 1)]
+    Hd = np.zeros((1 << N, 1 << N), complex)
+    pm = {"X": Dr.X, "Y": Dr.Y, "Z": Dr.Z}
+    for i, j, jx, jy, jz in xb + yb:
+        for P, c in (("X", jx), ("Y", jy), ("Z", jz)):
+            Hd += c * Dr.embed({int(i): pm[P], int(j): pm[P]}, N)
+    for k, hx, hy, hz in fields:
+        for P, c in (("X", hx), ("Y", hy), ("Z", hz)):
+            Hd += c * Dr.embed({int(k): pm[P]}, N)
+    got = O.apply_hamiltonian_bitwise(psi, xb, yb, fields, N)
+    assert np.max(np.abs(got - Hd @ psi)) < 1e-13
+    chain = O.apply_hamiltonian_bitwise(psi, [[i, i + 1, 1.0, 0.8, 0.5] for i in range(1, N)], [],
+                                        [[i, 0.3, 0.0, 0.0] for i in range(1, N + 1)], N)
+    assert np.max(np.abs(chain - O.apply_H_xxz(psi, N, 1.0, 0.8, 0.5, 0.3))) < 1e-13

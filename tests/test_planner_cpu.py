@@ -53,7 +53,7 @@ def op_matrix(op):
 def replay(plan, N, psi):
     for p in plan:
         for op in p["ops"]:
-            if op["kind"] in (8, 10):  # layout change / stage header: no arithmetic
+            if op["kind"] == 10:  # stage header: no arithmetic
                 continue
             psi = apply_local(psi, op_matrix(op), op["gb"][:op["nq"]], N)
     return psi

@@ -261,27 +261,6 @@ def test_compiled_two_tile_buffers(ctx, tb64):
         ctx.set_option(S._lib.OPT_JIT_BUFFERS, 1)
 
 
-def test_compiled_fp32x2_arithmetic(ctx):
-    """engine 3 with FP32x2 arithmetic (SMOQ_OPT_JIT_PACKED): random circuit on a
-    random state equals the oracle"""
-    N, seed = 14, 11
-    g_ops, o_ops = random_circuit(N, 200, seed)
-    rng = np.random.default_rng(seed)
-    psi = rng.normal(size=1 << N) + 1j * rng.normal(size=1 << N)
-    psi /= np.linalg.norm(psi)
-    want = psi.copy()
-    O.apply_circuit(want, O.make_ops(o_ops), len(o_ops), np.zeros(1), N)
-    ctx.set_option(S._lib.OPT_JIT_PACKED, 1)
-    try:
-        with engine(ctx, 3):
-            st = S.CuState(ctx, N, S.C64, basis=None)
-            st.upload(psi.astype(np.complex64))
-            S.apply_circuit(st, S.ParameterizedCircuit(N, g_ops), np.zeros(1))
-            assert rel(st.download().astype(complex), want) < 5e-5
-    finally:
-        ctx.set_option(S._lib.OPT_JIT_PACKED, 0)
-
-
 @pytest.mark.parametrize("tb64", [12, 13])
 def test_compiled_one_group_per_thread(ctx, tb64):
     """engine 3 with one 16-amplitude register group per thread (SMOQ_OPT_JIT_GROUPS 1):
@@ -312,35 +291,3 @@ def test_compiled_one_group_per_thread(ctx, tb64):
             assert rel(s2.download().astype(complex), ref) < 1e-4
     finally:
         ctx.set_option(S._lib.OPT_JIT_GROUPS, 2)
-
-
-@pytest.mark.parametrize("tb64", [12, 13])
-def test_compiled_five_bit_stages(ctx, tb64):
-    """engine 3 with 32-amplitude register stages (SMOQ_OPT_JIT_STAGE_BITS 5): random
-    circuit with every gate kind and a Strang XXZ sweep equal the oracle"""
-    N, seed = 15, 13
-    g_ops, o_ops = random_circuit(N, 200, seed)
-    rng = np.random.default_rng(seed)
-    psi = rng.normal(size=1 << N) + 1j * rng.normal(size=1 << N)
-    psi /= np.linalg.norm(psi)
-    want = psi.copy()
-    O.apply_circuit(want, O.make_ops(o_ops), len(o_ops), np.zeros(1), N)
-    ctx.set_option(S._lib.OPT_JIT_STAGE_BITS, 5)
-    try:
-        with engine(ctx, 3, tb64=tb64):
-            st = S.CuState(ctx, N, S.C64, basis=None)
-            st.upload(psi.astype(np.complex64))
-            S.apply_circuit(st, S.ParameterizedCircuit(N, g_ops), np.zeros(1))
-            assert rel(st.download().astype(complex), want) < 5e-5
-            arr, n, gl = xxz(17, 0.05)
-            neel = sum(1 << (k - 1) for k in range(1, 18, 2))
-            ref = O.zero_state(17, neel)
-            both = O.make_gates(gl + gl[::-1])
-            for _ in range(3):
-                O.trotter_step(ref, both, 2 * n, 17)
-            plan = S.TrotterPlan(ctx, 17, [S.FastTrotterGate(i, U) for i, U in gl], order=2, dtype=S.C64)
-            s2 = S.CuState(ctx, 17, S.C64, basis=neel)
-            plan.step(s2, 3)
-            assert rel(s2.download().astype(complex), ref) < 1e-4
-    finally:
-        ctx.set_option(S._lib.OPT_JIT_STAGE_BITS, 4)
