@@ -302,6 +302,57 @@ def vqe_measure(ctx, steps, warmup, B=8):
             "plain_ps_vs_adjoint_param0": float(abs(ps0 - res["c128"][2][0, 0]))}
 
 
+# The reference's own expectation-value benchmark
+# (SmoQ.jl_benchmarks/benchmark_expectation_values/bench_smoq.jl:17-37, 82-85): 4 brickwork
+# layers [H on even qubits; Ry(ANGLES_RY[q]) on all; CNOT on (q, q+1) for odd q; S on odd
+# qubits; Rx(ANGLES_RX[q]) on all; CZ on (q, q+1) for even q] from |0...0>, then <X>, <Y>, <Z>
+# of every qubit and <XX>, <YY>, <ZZ> of every bond, complex128.  Its published wall times
+# (timing_smoq.txt:10-14, a laptop, single-threaded kernels).
+PUBLISHED_EXPECTATION_S = {20: 0.483826, 24: 11.048547}
+_ANG_RY = [np.pi / d for d in (4, 3, 6, 5, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23, 24, 25, 26)]
+_ANG_RX = [np.pi / d for d in (5, 7, 4, 9, 3, 11, 6, 13, 8, 10, 12, 14, 15, 17, 16, 19, 18, 20, 21, 22, 23, 24, 25, 26)]
+
+
+def published_comparison(ctx, runs=5):
+    """the reference's expectation benchmark at N=20 and N=24 on the GPU, CUDA events around
+    circuit + 6N-3 observables (the observables come back to the host inside the region);
+    against the reference's own published seconds"""
+    import torch
+    import pysmoq as S
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", torch.cuda.current_device()))
+    out = {}
+    for N, ref_s in PUBLISHED_EXPECTATION_S.items():
+        g = S.gate
+        ops = []
+        for _ in range(4):
+            ops += [g("h", q) for q in range(2, N + 1, 2)]
+            ops += [g("ry", q, angle=_ANG_RY[q - 1]) for q in range(1, N + 1)]
+            ops += [g("cnot", [q, q + 1]) for q in range(1, N, 2)]
+            ops += [g("s", q) for q in range(1, N + 1, 2)]
+            ops += [g("rx", q, angle=_ANG_RX[q - 1]) for q in range(1, N + 1)]
+            ops += [g("cz", [q, q + 1]) for q in range(2, N, 2)]
+        circ = S.ParameterizedCircuit(N, ops)
+        st = S.CuState(ctx, N, S.C128, basis=0)
+        times = []
+        for r in range(runs + 1):
+            e0, e1 = _events(torch, stream)
+            e0.record(stream)
+            st.set_basis(0)
+            S.apply_circuit(st, circ, np.zeros(1))
+            obs = S.measure_all_observables_state_vector(st, N, 1)
+            e1.record(stream)
+            e1.synchronize()
+            if r:  # the first run plans and warms up
+                times.append(e0.elapsed_time(e1) * 1e-3)
+        st.close()
+        t = float(np.median(times))
+        out[f"n{N}"] = {"gpu_s": t, "reference_published_s": ref_s, "speedup": ref_s / t, "gates": len(ops),
+                        "observables": int(obs.size)}
+    return {"workload": "reference expectation benchmark: 4 brickwork layers + all X/Y/Z and XX/YY/ZZ, complex128",
+            "source": "SmoQ.jl_benchmarks/benchmark_expectation_values/timing_smoq.txt:10-14 (laptop)",
+            "runs": out}
+
+
 def vqe_workload(args):
     """the VQE gradient figures as their own line (see vqe_measure)"""
     import pysmoq as S
@@ -502,16 +553,31 @@ def qrc_workload(args):
     return 0
 
 
+# FP32 instructions per amplitude of a fused op, by kind (dense 2x2: 2 complex
+# multiply-adds per output amplitude, dense 4x4: 4, parity 4x4: 2, monomial and
+# diagonal: 1 complex multiply; 4 FP32 FMA-pipe instructions each)
+_FP32_PER_AMP = {0: 8, 1: 16, 2: 8, 3: 4, 4: 4}
+
+
+def plan_fp32_per_amp(S, N, ops, dtype, engine):
+    """sum over the planned passes of the FP32 instructions per amplitude (host planner)"""
+    tb, lb = (13, 5) if dtype == S.C64 else (12, 4)
+    plan = S.debug_plan(N, ops, dtype=dtype, tile_bits=tb, low_bits=lb, engine=max(0, engine))
+    return sum(_FP32_PER_AMP.get(o["kind"], 0) for p in plan for o in p["ops"]), len(plan)
+
+
 def bandwidth_workload(args):
     """32 GiB single-state sweeps: N=32 complex64 and N=31 complex128, 20 layers of
     [Rx, Ry, Rz on every qubit (seeded angles); Rzz on a seeded random perfect
-    matching], fused passes; every pass timed with CUDA events."""
+    matching], fused passes; every pass timed with CUDA events.  Reported against
+    the HBM roofline (2 state sizes per pass) and the FP32 roofline (the planned
+    ops' FMA-pipe instructions per amplitude; 148 SMs x 128 lanes x the clock)."""
+    import time as _t
     import torch
     import pysmoq as S
-    ctx = S.Context(0)
-    if args.engine >= 0:
-        ctx.set_option(S._lib.OPT_ENGINE, args.engine)
     peak, peak_kind = measured_peak()
+    sm_mhz = 1965.0
+    fp32_peak = 148 * 128 * sm_mhz * 1e6  # FMA-pipe instructions / s
     out = {}
     for N, dt, name in ((32, S.C64, "n32_c64"), (31, S.C128, "n31_c128")):
         rng = np.random.default_rng(SEED)
@@ -523,28 +589,41 @@ def bandwidth_workload(args):
             ops += [S.gate("rzz", [int(perm[2 * i]), int(perm[2 * i + 1])], angle=float(rng.uniform(0, 2 * np.pi)))
                     for i in range(N // 2)]
         circ = S.ParameterizedCircuit(N, ops)
-        st = S.CuState(ctx, N, dt, basis=0)
-        S.apply_circuit(st, circ, np.zeros(1))  # warm-up (plans, first touch)
-        ctx.set_option(S._lib.OPT_KERNEL_TIMING, 1)
-        ctx.reset_counters()
-        st.set_basis(0)
-        S.apply_circuit(st, circ, np.zeros(1))
-        c = ctx.counters()
-        ctx.set_option(S._lib.OPT_KERNEL_TIMING, 0)
-        masks = [1 << q for q in range(N)] + [3 << q for q in range(N - 1)]
-        obs = S.expect_zstrings(st, masks[:32])
-        gbs = c["tile_bytes"] / (c["tile_ms"] * 1e-3) / 1e9
-        out[name] = {"gates": len(ops), "passes": c["tile_passes"], "ms": c["tile_ms"],
-                     "gate_apps_per_s": len(ops) / (c["tile_ms"] * 1e-3), "hbm_gbs": gbs, "frac": gbs / peak,
-                     "norm": float(S.get_norm(st)), "z1": float(obs[0, 0])}
-        st.close()
-    line = {"metric": "hbm_gbs_per_sweep", "value": out["n32_c64"]["hbm_gbs"], "unit": "GB/s", "n_gpus": 1,
+        engines = [args.engine] if args.engine >= 0 else ([-1, 3] if dt == S.C64 and S.jit_available() else [-1])
+        for eng in engines:
+            ctx = S.Context(0)
+            if eng >= 0:
+                ctx.set_option(S._lib.OPT_ENGINE, eng)
+            st = S.CuState(ctx, N, dt, basis=0)
+            t0 = _t.perf_counter()
+            S.apply_circuit(st, circ, np.zeros(1))  # first call: plans (and compiles, engine 3), first touch
+            first_s = _t.perf_counter() - t0
+            ctx.set_option(S._lib.OPT_KERNEL_TIMING, 1)
+            ctx.reset_counters()
+            st.set_basis(0)
+            S.apply_circuit(st, circ, np.zeros(1))
+            c = ctx.counters()
+            ctx.set_option(S._lib.OPT_KERNEL_TIMING, 0)
+            masks = [1 << q for q in range(N)] + [3 << q for q in range(N - 1)]
+            obs = S.expect_zstrings(st, masks[:32])
+            gbs = c["tile_bytes"] / (c["tile_ms"] * 1e-3) / 1e9
+            eng_run = eng if eng >= 0 else 0   # one-shot sequences: auto = shared-memory sweeps
+            instr, npass = plan_fp32_per_amp(S, N, ops, dt, eng_run)
+            fp32_rate = instr * float(1 << N) / (c["tile_ms"] * 1e-3)
+            out[f"{name}_engine{eng_run}"] = {
+                "gates": len(ops), "passes": c["tile_passes"], "ms": c["tile_ms"], "first_call_s": first_s,
+                "gate_apps_per_s": len(ops) / (c["tile_ms"] * 1e-3), "hbm_gbs": gbs, "hbm_frac": gbs / peak,
+                "fp32_instr_per_amp": instr, "fp32_frac": fp32_rate / fp32_peak,
+                "norm": float(S.get_norm(st)), "z1": float(obs[0, 0])}
+            st.close()
+            ctx.close()
+    head = out.get("n32_c64_engine0") or next(iter(out.values()))
+    line = {"metric": "hbm_gbs_per_sweep", "value": head["hbm_gbs"], "unit": "GB/s", "n_gpus": 1,
             "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "c64", "data": "synthetic",
             "config": {"workload": "random_rxryrz_rzz_depth20_32GiB", "engine": args.engine},
-            "peak": peak, "peak_kind": peak_kind, "runs": out}
+            "peak": peak, "peak_kind": peak_kind, "fp32_peak_instr_per_s": fp32_peak, "runs": out}
     print(json.dumps(line))
-    ctx.close()
     return 0
 
 
@@ -661,6 +740,12 @@ def main():
     tune = ctx.tune_report()
     if tune:
         sys.stderr.write(tune)
+    # the plan's fused-pass geometry: the autotuner's choice, else the options
+    geom = (args.tile_bits or 13, args.low_bits or 5, None)
+    for line in tune.splitlines():
+        if line.startswith("-> geometry tile"):
+            w = line.split()
+            geom = (int(w[3]), int(w[5]), None if w[7] == "-1" else int(w[7]))
     ctx.reset_counters()
     clocks = Clocks(local)
     clocks.start()
@@ -709,6 +794,9 @@ def main():
     vqe = None
     if not args.no_vqe and N == N_QUBITS:
         vqe = vqe_measure(ctx, steps=2, warmup=1)
+    published = None
+    if not args.no_vqe and N == N_QUBITS and rank == 0:
+        published = published_comparison(ctx)
 
     if rank == 0:
         line = {"metric": "gate_apps_per_s", "value": value, "unit": "gate-apps/s", "n_gpus": ws,
@@ -716,7 +804,8 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
                 "data": "synthetic",
                 "config": {"workload": workload, "N": N, "dt": DT, "trotter_steps": tsteps,
-                           "tile_bits_c64": args.tile_bits or 13, "low_bits_c64": args.low_bits or 5, "engine": eng,
+                           "tile_bits_c64": geom[0], "low_bits_c64": geom[1], "fusion_depth": geom[2],
+                           "engine": eng,
                            "record_every": RECORD_EVERY, "gate_apps_per_step": gate_apps,
                            "state_bytes": (1 << N) * 8, "l2_policy": "inputs larger than L2 (2 GiB state)",
                            "parallelism": "replicas" if ws > 1 else "single_gpu",
@@ -734,7 +823,8 @@ def main():
                         "d2h_bytes_per_step": int(8 * N * (tsteps // RECORD_EVERY + 1))},
                 "gpu_launches": int(launches),
                 "clocks": clk,
-                "vqe": vqe}
+                "vqe": vqe,
+                "published_comparison": published}
         print(json.dumps(line))
     st.close()
     plan.close()

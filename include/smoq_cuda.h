@@ -64,7 +64,9 @@ enum {
                                      3 compiled pass kernels (engine 2's schedule, each complex64 pass
                                      compiled with NVRTC at upload; needs libnvrtc).  Auto: reusable
                                      complex64 programs (Trotter plans, MCWF) run engine 3 when NVRTC
-                                     loads, everything else engine 0 */,
+                                     loads, everything else engine 0.  The complex64 backward passes of
+                                     smoq_energy_grad run compiled adjoint kernels under auto and 3,
+                                     the shared-memory adjoint kernel under 0 and 2 */,
     SMOQ_OPT_JIT_BUFFERS = 8,     /* compiled pass kernels: tile buffers per CTA, 1 (default) or 2 (the next
                                      tile's bulk load runs under the current tile's stages) */
     SMOQ_OPT_JIT_GROUPS = 10,     /* compiled pass kernels: 16-amplitude register groups per thread, 2
@@ -72,13 +74,19 @@ enum {
     SMOQ_OPT_VQE_RESIDENT = 12,   /* smoq_energy_grad_jobs: 1 (default) = circuits of N <= 13 (complex64)
                                      or N <= 12 (complex128) run together in one launch, each in one
                                      CTA's shared memory; 0 = every circuit through the tiled passes */
-    SMOQ_OPT_AUTOTUNE = 13        /* No counterpart in the reference.  1 (default) = when a reusable
-                                     complex64 program (a Trotter plan) of N >= 20 is first run, time
-                                     each compiled pass kernel's variants (register groups per thread,
-                                     CTAs per SM, one or two tile buffers) on a scratch state and keep
-                                     the fastest (the variants compute bit-identical results); choices
-                                     are cached per (GPU, pass program), across processes in the file
-                                     SMOQ_TUNE_CACHE names if set; 0 = the SMOQ_OPT_JIT_* settings */
+    SMOQ_OPT_AUTOTUNE = 13,       /* No counterpart in the reference.  1 (default) = when a reusable
+                                     complex64 program (a Trotter plan) of N >= 20 is first run on the
+                                     compiled pass kernels, (a) time its block with each candidate
+                                     geometry -- tile width, low bits, fusion depth -- on a scratch
+                                     state and keep the fastest for the plan, then (b) time each
+                                     compiled pass kernel's variants (register groups per thread, CTAs
+                                     per SM, one or two tile buffers; bit-identical results) and keep
+                                     the fastest; choices are cached per (GPU, program), across
+                                     processes in the file SMOQ_TUNE_CACHE names if set; 0 = the
+                                     options' settings */
+    SMOQ_OPT_FUSION_DEPTH = 14    /* No counterpart in the reference.  Max fused ops per pass: a longer
+                                     pass is split into consecutive passes of the same tile (0 =
+                                     default, as many as fit) */
 };
 smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long value);
 /* launches: kernels launched by this context; tile_passes/tile_ms/tile_bytes:
@@ -358,7 +366,11 @@ typedef struct {           /* one Pauli-sum term: coef * prod of letters */
  * <phi|H|phi> / <phi|phi> with both sums in FP64 over the computed state phi
  * (exactly <phi|H|phi> for a unitary circuit; for complex64 the division
  * removes the norm drift of a deep circuit), and the gradient is divided by
- * the same <phi|phi>. */
+ * the same <phi|phi>.  complex64 backward passes of tile width 12 run as
+ * compiled kernels (NVRTC; SMOQ_OPT_ENGINE auto or 3): 4-qubit register stages
+ * on both states with the generator measurements in between, the gate
+ * coefficients passed per launch, so the compile of a circuit's first parameter
+ * set serves every later one. */
 smoq_status smoq_energy_grad(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* ops, int n,
                              int n_params, const smoq_pauli_term* H, int nterms, int batch,
                              const double* theta, double* energies, double* grads);
@@ -473,6 +485,15 @@ smoq_status smoq_measure_all(smoq_state* st, unsigned long long seed, unsigned l
 smoq_status smoq_measure_qubit(smoq_state* st, int q, unsigned long long seed, unsigned long long stream,
                                int* outcome);
 
+/* No counterpart in the reference: the failure path of the bounded device
+ * waits, for tests.  Launches one block whose mbarrier wait (the wait every
+ * tile kernel uses for its bulk copies) can never complete -- the barrier
+ * expects bytes no copy delivers -- so the wait gives up after limit_ns
+ * (1 us .. 100 ms), records the timeout and returns; nothing is left in
+ * flight.  Returns SMOQ_ERR_TIMEOUT, as a tile kernel's timed-out wait would,
+ * and leaves the context usable. */
+smoq_status smoq_debug_wait_timeout(smoq_ctx* ctx, uint64_t limit_ns);
+
 /* ------------------------------------------------- host-only introspection */
 /* No counterpart in the reference.  Runs the fused-pass planner (host code,
  * no GPU or context needed) on a gate sequence exactly as
@@ -497,11 +518,25 @@ typedef struct {
 /* Host-only check of the plan compiler (engine 3): plans `ops` as smoq_apply_sequence
  * would with engine 3 and compiles every complex64 pass kernel with NVRTC, without a GPU
  * and without loading them.  flags: 1 = return the compiler's register/spill report in msg,
- * 2 = two tile buffers per CTA (SMOQ_OPT_JIT_BUFFERS 2), 8 = one register group per thread
- * (SMOQ_OPT_JIT_GROUPS 1).  *n_compiled = kernels compiled; msg gets "ok" (or the report)
- * or the first error.  SMOQ_ERR_UNSUPPORTED when NVRTC is not available. */
+ * 2 = two tile buffers per CTA (SMOQ_OPT_JIT_BUFFERS 2), 4 = run-time coefficients (the form
+ * the complex64 forward of smoq_energy_grad compiles: gate coefficients passed per launch),
+ * 8 = one register group per thread (SMOQ_OPT_JIT_GROUPS 1), 16 = the generated source of the
+ * first pass in msg (nothing compiled).  *n_compiled = kernels compiled; msg gets "ok" (or the
+ * report) or the first error.  SMOQ_ERR_UNSUPPORTED when NVRTC is not available. */
 smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops, int n,
                                     const double* theta, int flags, int* n_compiled, char* msg, int msg_len);
+/* Host-only check of the compiled adjoint kernels of smoq_energy_grad (complex64):
+ * builds the backward program of `ops` (measurements of the parameterised gates'
+ * generators interleaved with the inverse gates), plans it into tile passes of width
+ * tile_bits - 1, stage-schedules every pass the compiled adjoint kernel takes and
+ * compiles those kernels with NVRTC, without a GPU and without loading them.
+ * *n_passes = backward passes, *n_compiled = passes compiled for the compiled kernel
+ * (the rest run on the shared-memory adjoint kernel).  flags: 1 = the compiler's
+ * register/spill report in msg, 2 = the generated source of the first such pass in
+ * msg (nothing compiled).  SMOQ_ERR_UNSUPPORTED when NVRTC is not available. */
+smoq_status smoq_debug_compile_adjoint(int N, const smoq_op* ops, int n, int n_params, const double* theta,
+                                       int tile_bits, int low_bits, int flags, int* n_passes, int* n_compiled,
+                                       char* msg, int msg_len);
 smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tile_bits, int low_bits, int engine,
                                      const smoq_op* ops, int n, const double* theta, smoq_pass_info* passes, int max_passes,
                                      smoq_fused_op_info* fused, int max_fused, int* n_passes, int* n_fused);

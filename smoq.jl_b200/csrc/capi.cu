@@ -102,16 +102,50 @@ static int engine_for(smoq_ctx* ctx, bool reusable, int dtype) {
     return (reusable && dtype == SMOQ_C64 && jit_available()) ? 3 : 0;
 }
 
+// the fusion depth: a pass with more than `cap` fused ops becomes consecutive
+// passes of the same tile geometry (the ops keep their order, and every op of a
+// pass acts on that pass's tile, so the split changes nothing but the count)
+static void cap_fusion_depth(std::vector<Pass>& pl, int cap) {
+    if (cap <= 0) return;
+    std::vector<Pass> out;
+    for (Pass& p : pl) {
+        if ((int)p.ops.size() <= cap) {
+            out.push_back(std::move(p));
+            continue;
+        }
+        for (size_t i = 0; i < p.ops.size(); i += (size_t)cap) {
+            Pass q;
+            q.g = p.g;
+            q.ops.assign(p.ops.begin() + i, p.ops.begin() + std::min(p.ops.size(), i + (size_t)cap));
+            q.epilogue = p.epilogue && i + (size_t)cap >= p.ops.size();
+            out.push_back(std::move(q));
+        }
+    }
+    pl.swap(out);
+}
+
 // plan a gate list into fused passes; with the stage engines every pass of
 // tile width 12 (13 for complex64) gets a stage schedule
+// rtc: the compiled kernels read their coefficients at run time (a variational
+// circuit: one compile per circuit structure serves every parameter set)
 static std::vector<Pass> plan_for(int engine, const std::vector<GateIR>& ir, int N, int dtype, int tbits, int lbits,
-                                  int epilogue_special = -1) {
+                                  int epilogue_special = -1, int max_ops = 0, bool rtc = false) {
     std::vector<Pass> pl = plan_passes(ir, N, tbits, lbits, epilogue_special, dtype == SMOQ_C64 ? 1 : 0);
+    cap_fusion_depth(pl, max_ops);
     if (engine == 2 || engine == 3)
         for (Pass& p : pl)
             if (p.g.T == 12 || (p.g.T == 13 && dtype == SMOQ_C64)) {
                 schedule_stages(p, dtype == SMOQ_C64 ? 8 : 16);
                 p.want_jit = engine == 3 && p.staged && dtype == SMOQ_C64;
+                if (p.want_jit && rtc) {
+                    p.rtc = true;
+                    jit_rtc_block(p, p.coefs);
+                    // (a block beyond the parameter space: the stage-sweep engine runs the pass)
+                    if (sizeof(TileArgs) + sizeof(float2) * p.coefs.size() > kMaxKernelParamBytes) {
+                        p.rtc = p.want_jit = false;
+                        p.coefs.clear();
+                    }
+                }
             }
     return pl;
 }
@@ -131,6 +165,13 @@ struct DevProgram {
 }  // namespace
 
 static smoq_status upload_program(smoq_ctx* ctx, DevProgram& P) {
+    std::vector<JitRequest> reqs;
+    for (Pass& p : P.passes) {
+        if (p.want_jit && !p.jit && p.rtc)  // a known structure: no source generated
+            p.jit = jit_pass_find(p, ctx->jit_buffers, ctx->jit_groups, 0);
+        if (p.want_jit && !p.jit) reqs.push_back(JitRequest{&p, ctx->jit_buffers, ctx->jit_groups, 0});
+    }
+    if (reqs.size() > 1) jit_precompile(reqs);
     for (Pass& p : P.passes) {
         if (!p.want_jit || p.jit) continue;
         std::string why;
@@ -258,29 +299,20 @@ static smoq_status autotune_program(smoq_ctx* ctx, DevProgram& P, int N) {
         ctx->tune_report += "autotune skipped: no room for a scratch state\n";
         return SMOQ_OK;
     }
-    // compile every variant of every fresh pass on host threads (NVRTC is thread-safe per program)
+    // compile every variant of every fresh pass with NVRTC on host threads, then load them here
     std::vector<const JitKernel*> ks(fresh.size() * kTuneVariantCount, nullptr);
     {
-        std::vector<std::thread> pool;
-        std::mutex next_mu;
-        size_t next = 0;
-        auto work = [&]() {
-            for (;;) {
-                size_t j;
-                {
-                    std::lock_guard<std::mutex> lk(next_mu);
-                    if (next >= ks.size()) return;
-                    j = next++;
-                }
-                const TuneVariant& v = kTuneVariants[j % kTuneVariantCount];
-                std::string why;
-                ks[j] = jit_pass_kernel(P.passes[fresh[j / kTuneVariantCount]], v.nbuf, v.groups, why, v.minb_add);
-            }
-        };
-        const size_t nt = std::max<size_t>(1, std::min<size_t>(ks.size(), std::thread::hardware_concurrency()));
-        for (size_t t = 1; t < nt; ++t) pool.emplace_back(work);
-        work();
-        for (std::thread& t : pool) t.join();
+        std::vector<JitRequest> reqs;
+        for (size_t j = 0; j < ks.size(); ++j) {
+            const TuneVariant& v = kTuneVariants[j % kTuneVariantCount];
+            reqs.push_back(JitRequest{&P.passes[fresh[j / kTuneVariantCount]], v.nbuf, v.groups, v.minb_add});
+        }
+        jit_precompile(reqs);
+        for (size_t j = 0; j < ks.size(); ++j) {
+            const TuneVariant& v = kTuneVariants[j % kTuneVariantCount];
+            std::string why;
+            ks[j] = jit_pass_kernel(P.passes[fresh[j / kTuneVariantCount]], v.nbuf, v.groups, why, v.minb_add);
+        }
     }
     void* scratch = nullptr;
     CK(ctx, cudaMallocAsync(&scratch, bytes, ctx->stream));
@@ -290,6 +322,7 @@ static smoq_status autotune_program(smoq_ctx* ctx, DevProgram& P, int N) {
     CK(ctx, cudaEventCreate(&e0));
     CK(ctx, cudaEventCreate(&e1));
     std::ostringstream rep;
+    const long long launches0 = ctx->launches;
     for (size_t f = 0; f < fresh.size(); ++f) {
         Pass& p = P.passes[fresh[f]];
         TileArgs a;
@@ -309,9 +342,10 @@ static smoq_status autotune_program(smoq_ctx* ctx, DevProgram& P, int N) {
         for (int v = 0; v < kTuneVariantCount; ++v) {
             const JitKernel* k = ks[f * kTuneVariantCount + v];
             if (!k) continue;
-            cudaError_t e = launch_jit(ctx, a, k, false);  // warm-up
+            const float2* kc = p.rtc ? p.coefs.data() : nullptr;
+            cudaError_t e = launch_jit(ctx, a, k, false, kc);  // warm-up
             cudaEventRecord(e0, ctx->stream);
-            for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = launch_jit(ctx, a, k, false);
+            for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = launch_jit(ctx, a, k, false, kc);
             cudaEventRecord(e1, ctx->stream);
             if (e == cudaSuccess) e = cudaEventSynchronize(e1);
             if (e != cudaSuccess) {
@@ -334,6 +368,7 @@ static smoq_status autotune_program(smoq_ctx* ctx, DevProgram& P, int N) {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    ctx->launches = launches0;  // the timing launches are not the caller's work
     CK(ctx, cudaStreamSynchronize(ctx->stream));
     int32_t herr = 0;
     CK(ctx, cudaMemcpy(&herr, ctx->d_err, sizeof(herr), cudaMemcpyDeviceToHost));
@@ -434,6 +469,14 @@ smoq_status smoq_ctx_synchronize(smoq_ctx* ctx) {
 
 void* smoq_ctx_stream(smoq_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
+smoq_status smoq_debug_wait_timeout(smoq_ctx* ctx, uint64_t limit_ns) {
+    if (!ctx) return SMOQ_ERR_BADINPUT;
+    if (limit_ns < 1000 || limit_ns > 100000000ull)
+        return fail(ctx, SMOQ_ERR_BADINPUT, "wait limit must be in 1 us .. 100 ms");
+    CK(ctx, launch_wait_timeout_probe(ctx, limit_ns));
+    return sync_check(ctx);
+}
+
 smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long v) {
     if (!ctx) return SMOQ_ERR_BADINPUT;
     switch (option) {
@@ -469,6 +512,10 @@ smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long v) {
             break;
         case SMOQ_OPT_VQE_RESIDENT: ctx->vqe_resident = v != 0; break;
         case SMOQ_OPT_AUTOTUNE: ctx->autotune = v != 0; break;
+        case SMOQ_OPT_FUSION_DEPTH:
+            if (v < 0 || v > 1000000) return fail(ctx, SMOQ_ERR_BADINPUT, "fusion depth must be >= 0");
+            ctx->fusion_depth = (int)v;
+            break;
         default: return fail(ctx, SMOQ_ERR_BADINPUT, "unknown option");
     }
     return SMOQ_OK;
@@ -768,7 +815,7 @@ smoq_status smoq_apply_sequence(smoq_state* st, const smoq_op* ops, int n, const
     DevProgram P;
     try {
         P.passes = plan_for(engine_for(ctx, false, st->dtype), ir, st->N, st->dtype, tile_bits(ctx, st->dtype),
-                            low_bits(ctx, st->dtype), -1);
+                            low_bits(ctx, st->dtype), -1, ctx->fusion_depth);
     } catch (const std::exception& ex) {
         return fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
     }
@@ -798,11 +845,11 @@ smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tbits, int lbit
     if (smoq_status s = ops_to_ir(nullptr, N, ops, n, theta, ir)) return s;
     std::vector<Pass> pl;
     try {
-        if (flags & ~(1 | 2 | 8)) {
+        if (flags & ~(1 | 2 | 4 | 8 | 16)) {
             say("unknown flag");
             return SMOQ_ERR_BADINPUT;
         }
-        pl = plan_for(3, ir, N, dtype, tbits, lbits, -1);
+        pl = plan_for(3, ir, N, dtype, tbits, lbits, -1, 0, (flags & 4) != 0);
     } catch (const std::exception& e) {
         say(e.what());
         return SMOQ_ERR_BADINPUT;
@@ -811,6 +858,15 @@ smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tbits, int lbit
     for (const Pass& p : pl) {
         if (!p.want_jit) continue;
         std::string why, info;
+        if (flags & 16) {  // the generated source of the first compiled pass
+            if (!jit_pass_source(p, (flags & 2) ? 2 : 1, (flags & 8) ? 1 : 2, info, why)) {
+                say(why);
+                return SMOQ_ERR_BADINPUT;
+            }
+            *n_compiled = 1;
+            say(info);
+            return SMOQ_OK;
+        }
         if (!jit_check_pass(p, (flags & 2) ? 2 : 1, (flags & 8) ? 1 : 2, why, nullptr, verbose ? &info : nullptr)) {
             say(why);
             return why.rfind("NVRTC (", 0) == 0 ? SMOQ_ERR_UNSUPPORTED : SMOQ_ERR_BADINPUT;
@@ -1070,6 +1126,11 @@ struct smoq_plan {
     int dtype = SMOQ_C64;
     int order = 1;
     std::vector<GateIR> step;  // gates of one step (order 2: list + reversed list)
+    // the fused-pass geometry of the plan's blocks: tile width, low bits and the
+    // fusion depth (max fused ops per pass, 0 = as many as fit); the context's
+    // defaults, or the autotuner's choice made when the first block is built
+    int tbits = 0, lbits = 0, max_ops = 0;
+    bool geometry_chosen = false;
     struct Block {
         DevProgram prog;
         cudaGraphExec_t gexec = nullptr;
@@ -1083,6 +1144,8 @@ struct smoq_plan {
     std::map<int, std::unique_ptr<Block>> blocks;  // keyed by steps per block
 };
 
+static smoq_status choose_geometry(smoq_plan* P, const std::vector<GateIR>& all);
+
 static smoq_status get_block(smoq_plan* P, int nsteps, smoq_plan::Block** out) {
     auto it = P->blocks.find(nsteps);
     if (it != P->blocks.end()) {
@@ -1093,9 +1156,16 @@ static smoq_status get_block(smoq_plan* P, int nsteps, smoq_plan::Block** out) {
     std::vector<GateIR> all;
     all.reserve(P->step.size() * nsteps);
     for (int s = 0; s < nsteps; ++s) all.insert(all.end(), P->step.begin(), P->step.end());
+    if (!P->geometry_chosen) {
+        P->tbits = tile_bits(P->ctx, P->dtype);
+        P->lbits = low_bits(P->ctx, P->dtype);
+        P->max_ops = P->ctx->fusion_depth;
+        if (smoq_status s = choose_geometry(P, all)) return s;
+        P->geometry_chosen = true;
+    }
     try {
-        B->prog.passes = plan_for(engine_for(P->ctx, true, P->dtype), all, P->N, P->dtype, tile_bits(P->ctx, P->dtype),
-                                  low_bits(P->ctx, P->dtype), -1);
+        B->prog.passes = plan_for(engine_for(P->ctx, true, P->dtype), all, P->N, P->dtype, P->tbits, P->lbits, -1,
+                                  P->max_ops);
     } catch (const std::exception& ex) {
         return fail(P->ctx, SMOQ_ERR_BADINPUT, ex.what());
     }
@@ -1107,6 +1177,114 @@ static smoq_status get_block(smoq_plan* P, int nsteps, smoq_plan::Block** out) {
     *out = B.get();
     P->blocks[nsteps] = std::move(B);
     return SMOQ_OK;
+}
+
+// Plan-level autotuning (reusable complex64 programs of N >= 20 on the compiled
+// pass kernels, when SMOQ_OPT_AUTOTUNE is on): the block is planned with each
+// candidate geometry -- tile width, low bits, fusion depth -- compiled, and run
+// once on a zeroed scratch state; the fastest geometry is kept for every block of
+// the plan and cached per (GPU, N, gate pattern).  Every candidate computes the
+// same evolution (fusion regroups the same gates).
+namespace {
+struct PlanGeometry {
+    int tbits, lbits, max_ops;
+};
+const PlanGeometry kGeometries[] = {{13, 5, 0}, {13, 4, 0}, {12, 5, 0}, {12, 4, 0}, {13, 5, 12}};
+std::map<uint64_t, int> g_geometry;  // guarded by g_tune_mu
+}  // namespace
+
+static smoq_status choose_geometry(smoq_plan* P, const std::vector<GateIR>& all) {
+    smoq_ctx* ctx = P->ctx;
+    if (!ctx->autotune || P->dtype != SMOQ_C64 || P->N < kTuneMinN || engine_for(ctx, true, P->dtype) != 3)
+        return SMOQ_OK;
+    // key: device, N and the gate pattern (qubits, diagonal or not) of the block
+    uint64_t key = device_hash(ctx->device) ^ 0x9E3779B97F4A7C15ull;
+    auto mix = [&key](uint64_t v) { key = (key ^ v) * 1099511628211ull; };
+    mix((uint64_t)P->N);
+    for (const GateIR& g : all) {
+        mix((uint64_t)g.nq | ((uint64_t)g.diag << 8));
+        for (int t = 0; t < g.nq; ++t) mix((uint64_t)g.q[t]);
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        tune_cache_load_locked();
+        auto it = g_geometry.find(key);
+        if (it == g_geometry.end()) {
+            auto jt = g_tune.find(key);  // geometry choices share the cache file (key, candidate index)
+            if (jt != g_tune.end()) it = g_geometry.emplace(key, jt->second).first;
+        }
+        if (it != g_geometry.end() && it->second >= 0 && it->second < (int)(sizeof(kGeometries) / sizeof(kGeometries[0]))) {
+            const PlanGeometry& G = kGeometries[it->second];
+            P->tbits = G.tbits, P->lbits = G.lbits, P->max_ops = G.max_ops;
+            return SMOQ_OK;
+        }
+    }
+    const size_t bytes = (size_t)8 << P->N;
+    size_t free_b = 0, total_b = 0;
+    CK(ctx, cudaMemGetInfo(&free_b, &total_b));
+    if (free_b < 2 * bytes + ((size_t)1 << 30)) {
+        ctx->tune_report += "geometry tuning skipped: no room for a scratch state\n";
+        return SMOQ_OK;
+    }
+    void* scratch = nullptr;
+    CK(ctx, cudaMallocAsync(&scratch, bytes, ctx->stream));
+    std::unique_ptr<void, std::function<void(void*)>> hold(scratch, [ctx](void* q) { cudaFreeAsync(q, ctx->stream); });
+    CK(ctx, cudaMemsetAsync(scratch, 0, bytes, ctx->stream));
+    smoq_state st;
+    st.ctx = ctx;
+    st.N = P->N;
+    st.dtype = SMOQ_C64;
+    st.batch = 1;
+    st.ptr = scratch;
+    st.owned = false;
+    cudaEvent_t e0, e1;
+    CK(ctx, cudaEventCreate(&e0));
+    CK(ctx, cudaEventCreate(&e1));
+    std::ostringstream rep;
+    int best = -1;
+    float best_ms = 0;
+    const long long launches0 = ctx->launches, passes0 = ctx->tile_passes;
+    for (int c = 0; c < (int)(sizeof(kGeometries) / sizeof(kGeometries[0])); ++c) {
+        const PlanGeometry& G = kGeometries[c];
+        DevProgram prog;
+        try {
+            prog.passes = plan_for(3, all, P->N, P->dtype, G.tbits, G.lbits, -1, G.max_ops);
+        } catch (const std::exception&) {
+            continue;  // a geometry the planner cannot use for this circuit
+        }
+        CK(ctx, cudaStreamSynchronize(ctx->stream));
+        if (upload_program(ctx, prog) != SMOQ_OK) continue;
+        smoq_status s = run_program(ctx, &st, prog, nullptr, nullptr);  // warm-up
+        cudaEventRecord(e0, ctx->stream);
+        if (!s) s = run_program(ctx, &st, prog, nullptr, nullptr);
+        cudaEventRecord(e1, ctx->stream);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (s || e != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return s ? s : cuda_fail(ctx, e, "geometry tuning");
+        }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        rep << "geometry tile " << G.tbits << " low " << G.lbits << " depth " << (G.max_ops ? G.max_ops : -1) << ": "
+            << prog.passes.size() << " passes, " << ms << " ms\n";
+        if (best < 0 || ms < best_ms) best = c, best_ms = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->launches = launches0;  // the tuning runs are not the caller's work
+    ctx->tile_passes = passes0;
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if (best >= 0) {
+        const PlanGeometry& G = kGeometries[best];
+        P->tbits = G.tbits, P->lbits = G.lbits, P->max_ops = G.max_ops;
+        rep << "-> geometry tile " << G.tbits << " low " << G.lbits << " depth " << (G.max_ops ? G.max_ops : -1) << "\n";
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_geometry[key] = best;
+        tune_cache_store_locked(key, best);
+    }
+    ctx->tune_report += rep.str();
+    return sync_check(ctx);
 }
 
 static smoq_status run_block(smoq_plan* P, smoq_state* st, smoq_plan::Block* B, std::vector<EventPair>* timing) {
@@ -1324,11 +1502,13 @@ smoq_status smoq_internal_plan_step(smoq_plan* plan, std::vector<GateIR>& out, i
 
 // plan + upload a gate program for `st` (no launch); the handle owns it
 smoq_status smoq_internal_prepare(smoq_ctx* ctx, smoq_state* st, const std::vector<GateIR>& gates,
-                                  int epilogue_special, bool reusable, void** handle) {
+                                  int epilogue_special, bool reusable, void** handle, bool variational) {
     std::unique_ptr<DevProgram> P(new DevProgram());
+    // a variational circuit's complex64 forward: compiled kernels with run-time coefficients
+    const bool rtc = variational && st->dtype == SMOQ_C64 && ctx->engine < 0 && jit_available();
     try {
-        P->passes = plan_for(engine_for(ctx, reusable, st->dtype), gates, st->N, st->dtype, tile_bits(ctx, st->dtype),
-                             low_bits(ctx, st->dtype), epilogue_special);
+        P->passes = plan_for(rtc ? 3 : engine_for(ctx, reusable, st->dtype), gates, st->N, st->dtype,
+                             tile_bits(ctx, st->dtype), low_bits(ctx, st->dtype), epilogue_special, 0, rtc);
     } catch (const std::exception& ex) {
         return fail(ctx, SMOQ_ERR_BADINPUT, ex.what());
     }

@@ -25,6 +25,9 @@
 #include <stddef.h>
 
 #include <algorithm>
+#include <atomic>
+#include <set>
+#include <thread>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -205,26 +208,37 @@ struct CplxF {
     float re, im;
 };
 
-// dense matrix (row-major, dim x dim) of a non-diagonal op, in float
-std::vector<CplxF> op_matrix_f(const DevOp& op) {
+// dense matrix (row-major, dim x dim) of a non-diagonal op, in float; idx[k] = the
+// op's coefficient slot of entry k (-1: a zero of the op kind's structure)
+std::vector<CplxF> op_matrix_f(const DevOp& op, std::vector<int>* idx = nullptr) {
     const int dim = 1 << op.nq;
     std::vector<CplxF> M(dim * dim, CplxF{0.f, 0.f});
-    auto c = [&](int i) { return CplxF{op.cf[i].x, op.cf[i].y}; };
+    std::vector<int> I(dim * dim, -1);
+    auto set = [&](int k, int i) { M[k] = CplxF{op.cf[i].x, op.cf[i].y}, I[k] = i; };
     switch (op.kind) {
         case OPK_DENSE1:
         case OPK_DENSE2:
-            for (int k = 0; k < dim * dim; ++k) M[k] = c(k);
+            for (int k = 0; k < dim * dim; ++k) set(k, k);
             break;
         case OPK_PARITY2:
-            M[0 * 4 + 0] = c(0), M[0 * 4 + 3] = c(1), M[3 * 4 + 0] = c(2), M[3 * 4 + 3] = c(3);
-            M[1 * 4 + 1] = c(4), M[1 * 4 + 2] = c(5), M[2 * 4 + 1] = c(6), M[2 * 4 + 2] = c(7);
+            set(0 * 4 + 0, 0), set(0 * 4 + 3, 1), set(3 * 4 + 0, 2), set(3 * 4 + 3, 3);
+            set(1 * 4 + 1, 4), set(1 * 4 + 2, 5), set(2 * 4 + 1, 6), set(2 * 4 + 2, 7);
             break;
         case OPK_MONO:
-            for (int r = 0; r < dim; ++r) M[r * dim + op.perm[r]] = c(r);
+            for (int r = 0; r < dim; ++r) set(r * dim + op.perm[r], r);
             break;
         default: break;
     }
+    if (idx) idx->swap(I);
     return M;
+}
+
+// 0, +-1 and +-i: coefficients a compiled kernel keeps as literals even when it
+// reads the others at run time (the entries a gate's structure fixes: CZ, CNOT, X)
+bool trivial_coef(CplxF k) {
+    const bool re01 = k.re == 0.f || k.re == 1.f || k.re == -1.f;
+    const bool im01 = k.im == 0.f || k.im == 1.f || k.im == -1.f;
+    return re01 && im01 && (k.re == 0.f || k.im == 0.f);
 }
 
 // "a*x + ..." real part and imaginary part of sum_c M[c] * x_c
@@ -249,13 +263,50 @@ void cmac_terms(const std::vector<std::pair<CplxF, std::string>>& terms, std::st
     im = fi ? "0.f" : i.str();
 }
 
+// ------------------------------------------------------ run-time coefficients
+// With p.rtc, the op coefficients other than 0, +-1, +-i travel as a kernel
+// parameter block (one complex64 per (op, coefficient slot) pair, in this order);
+// the compiled code reads them as constant-bank operands.  The kernel source then
+// depends on the circuit's gates and qubits, not on its angles, and one compiled
+// kernel serves every parameter set of a variational circuit.
+std::vector<std::pair<int, int>> rtc_list(const Pass& p) {
+    std::vector<std::pair<int, int>> out;
+    for (size_t m = 0; m < p.ops.size(); ++m) {
+        const DevOp& op = p.ops[m];
+        std::set<int> need;
+        if (op.kind == OPK_DIAG) {
+            bool on_tile = true;
+            for (int t = 0; t < op.nq; ++t) on_tile &= op.lb[t] >= 0;
+            if (!on_tile) continue;  // the mixed and off-tile forms index a.ops[m].c at run time
+            for (int k = 0; k < (1 << op.nq); ++k)
+                if (!trivial_coef(CplxF{op.cf[k].x, op.cf[k].y})) need.insert(k);
+        } else if (op.kind == OPK_DENSE1 || op.kind == OPK_DENSE2 || op.kind == OPK_PARITY2 || op.kind == OPK_MONO) {
+            std::vector<int> I;
+            const std::vector<CplxF> M = op_matrix_f(op, &I);
+            for (size_t k = 0; k < M.size(); ++k)
+                if (I[k] >= 0 && !trivial_coef(M[k])) need.insert(I[k]);
+        }
+        for (int i : need) out.push_back({(int)m, i});
+    }
+    return out;
+}
+
 struct Gen {
     const Pass& p;
     int G, NT;
     std::ostringstream o;
-    explicit Gen(const Pass& pass, int g, int nt) : p(pass), G(g), NT(nt) {}
+    std::map<std::pair<int, int>, int> kslot;  // run-time coefficient (op, slot) -> parameter index
+    explicit Gen(const Pass& pass, int g, int nt) : p(pass), G(g), NT(nt) {
+        if (p.rtc) {
+            const auto l = rtc_list(p);
+            for (size_t k = 0; k < l.size(); ++k) kslot[l[k]] = (int)k;
+        }
+    }
 
-    std::string v(int i) { return "v" + std::to_string(i); }
+    // register names: v<i> for the single-state kernels and phi of the adjoint
+    // kernels, w<i> for lambda; scn: the stage scalar of that register set
+    std::string vp = "v", scn = "sc";
+    std::string v(int i) { return vp + std::to_string(i); }
 
     // one stage: S sorted 4 tile bits, rl[q] lane bit of the rotation at stage
     // position q (-1 none), members = indices into p.ops
@@ -297,7 +348,7 @@ struct Gen {
         bool scal = false;
         for (int m : members) scal |= member(m, S, gstep, scal);
         if (scal)
-            for (int i = 0; i < nreg; ++i) o << "        " << v(i) << " = cmul(sc, " << v(i) << ");\n";
+            for (int i = 0; i < nreg; ++i) o << "        " << v(i) << " = cmul(" << scn << ", " << v(i) << ");\n";
         if (rotated) unrotate(rl);  // conditional swaps are involutions
         for (int i = 0; i < nreg; ++i) {
             const uint32_t c = off[i & (R - 1)] | ((i >> KB) ? gstep : 0u);
@@ -322,6 +373,201 @@ struct Gen {
         }
     }
 
+    // ------------------------------------------------------------ adjoint (dual)
+    // One stage of the compiled adjoint kernel: the same 16-amplitude groups of
+    // phi (tile, registers v<i>) and lambda (tlam, w<i>).  U^dag members act on
+    // both register sets (the same literal code twice); an OPK_INNER member adds
+    // Im<lambda|G|phi> over the thread's registers, at its place in the op order,
+    // to its warp's row of the partials.
+    void stage_dual(const int* S, const int* rl, const std::vector<int>& members) {
+        KB = 4;
+        GS = (G << 4) >> KB;
+        const int R = 1 << KB;
+        const uint32_t gstep = GS > 1 ? deposit_value(S, KB, (uint32_t)NT) : 0u;
+        uint32_t off[16];
+        for (int r = 0; r < R; ++r) {
+            off[r] = 0;
+            for (int q = 0; q < KB; ++q)
+                if ((r >> q) & 1) off[r] |= 1u << S[q];
+        }
+        bool rotated = false;
+        for (int q = 0; q < KB; ++q) rotated |= rl[q] >= 0;
+        o << "    {  // stage S = {" << S[0] << "," << S[1] << "," << S[2] << "," << S[3] << "}, phi and lambda\n";
+        o << "        const u32 g0 = " << deposit_expr(S, KB, "tid") << ";\n";
+        if (rotated) {
+            o << "        const u32 ga = g0";
+            for (int q = 0; q < KB; ++q)
+                if (rl[q] >= 0) o << " ^ (((tid >> " << rl[q] << ") & 1u) << " << S[q] << ")";
+            o << ";\n";
+        }
+        const int nreg = GS * R;
+        const char* sets[2][3] = {{"v", "tile", "sc"}, {"w", "tlam", "scw"}};
+        for (auto& st : sets) {
+            vp = st[0];
+            for (int i = 0; i < nreg; ++i) {
+                const uint32_t c = off[i & (R - 1)] | ((i >> KB) ? gstep : 0u);
+                o << "        cf " << v(i) << " = " << st[1] << (rotated ? "[ga ^ " : "[g0 + ") << c << "u];\n";
+            }
+            if (rotated) unrotate(rl);
+        }
+        bool scal[2] = {false, false};
+        o << "        cf sc = cf{1.f, 0.f}, scw = cf{1.f, 0.f};\n";
+        std::vector<int> cols;  // the stage's measurements, reduced together at its end
+        bool writes = false;
+        for (int m : members) {
+            if (p.ops[m].kind == OPK_INNER) {
+                inner(m, S, (int)cols.size());
+                cols.push_back(p.ops[m].perm[0]);
+                continue;
+            }
+            writes = true;
+            for (int k = 0; k < 2; ++k) {  // the op on both register sets
+                vp = sets[k][0];
+                scn = sets[k][2];
+                scal[k] |= member(m, S, gstep, true);
+            }
+        }
+        for (size_t c0 = 0; c0 < cols.size(); c0 += 8)
+            reduce_measurements(cols, c0, std::min<size_t>(cols.size(), c0 + 8));
+        // after a stage that only read (no barrier at its end), other threads may
+        // still be reading what this stage's stores overwrite
+        if (writes && pending_reads) o << "        __syncthreads();\n";
+        for (int k = 0; k < 2 && writes; ++k) {
+            vp = sets[k][0];
+            if (scal[k])
+                for (int i = 0; i < nreg; ++i) o << "        " << v(i) << " = cmul(" << sets[k][2] << ", " << v(i) << ");\n";
+            if (rotated) unrotate(rl);
+            for (int i = 0; i < nreg; ++i) {
+                const uint32_t c = off[i & (R - 1)] | ((i >> KB) ? gstep : 0u);
+                o << "        " << sets[k][1] << (rotated ? "[ga ^ " : "[g0 + ") << c << "u] = " << v(i) << ";\n";
+            }
+        }
+        vp = "v";
+        scn = "sc";
+        // a stage that only measured leaves the tiles as they were: the next stage
+        // may read them without a barrier (a writing stage waits before its stores)
+        o << (writes ? "    }\n    __syncthreads();\n" : "    }\n");
+        pending_reads = !writes;
+    }
+    bool pending_reads = false;
+
+    // warp sums of measurements cols[c0..c1) (at most 8, accumulators m<c0>..): a
+    // transposed butterfly -- each exchange step halves the values a lane carries
+    // and doubles the lanes it sums over -- then a plain butterfly; lane L ends with
+    // the sum of value ((L >> 4) & 1) * h0 + ((L >> 3) & 1) * h1 + ..., and the
+    // lanes with the remaining low bits 0 add it to the warp's row of the partials
+    // (with s transposed steps: value (L >> (5 - s)) & (2^s - 1))
+    void reduce_measurements(const std::vector<int>& cols, size_t c0, size_t c1) {
+        const int n = (int)(c1 - c0);
+        int P = 1, steps = 0;
+        while (P < n) P <<= 1, ++steps;
+        o << "        {  // warp sums of " << n << " measurements\n";
+        o << "          const u32 lane = tid & 31u;\n";
+        for (int i = 0; i < P; ++i)
+            o << "          float r" << i << " = " << (i < n ? "m" + std::to_string(c0 + i) : std::string("0.f")) << ";\n";
+        int count = P, d = 16;
+        for (int s = 0; s < steps; ++s, d >>= 1) {
+            const int half = count >> 1;
+            o << "          { const bool up = (lane & " << d << "u) != 0;\n";
+            for (int i = 0; i < half; ++i)
+                o << "            { const float snd = up ? r" << i << " : r" << (i + half) << "; r" << i << " = (up ? r"
+                  << (i + half) << " : r" << i << ") + __shfl_xor_sync(0xffffffffu, snd, " << d << "); }\n";
+            o << "          }\n";
+            count = half;
+        }
+        for (; d > 0; d >>= 1) o << "          r0 += __shfl_xor_sync(0xffffffffu, r0, " << d << ");\n";
+        // lane bits 4, 3, ... (one per transposed step) name the value it holds
+        const int low = 5 - steps;
+        o << "          if ((lane & " << ((1u << low) - 1) << "u) == 0u) {\n";
+        o << "            const u32 k = (lane >> " << low << ") & " << (P - 1) << "u;\n";
+        o << "            const int col = ";
+        for (int i = 0; i < n; ++i) o << "k == " << i << "u ? " << cols[c0 + i] << " : ";
+        o << "-1;\n";
+        o << "            const i64 row = (i64)blockIdx.x * (NT / 32) + (tid >> 5);\n"
+             "            if (col >= 0 && row < A.n_rows && col < A.n_cols) atomicAdd(&A.partials[row * A.n_cols + col], (double)r0);\n"
+             "          }\n"
+             "        }\n";
+    }
+
+    // Im<lambda|G|phi> of one measurement over the thread's registers: row r of the
+    // signed monomial G holds i^slot[r] at column perm[1 + r] (INNER_ZERO: a zero row);
+    // with conj(l) p = a + i b, Im(i^k conj(l) p) = b, a, -b, -a for k = 0..3
+    void inner(int m, const int* S, int idx) {
+        const DevOp& op = p.ops[m];
+        int pos[2] = {-1, -1};
+        int pmask = 0;
+        for (int t = 0; t < op.nq; ++t) {
+            for (int q = 0; q < KB; ++q)
+                if (S[q] == op.lb[t]) pos[t] = q;
+            pmask |= 1 << pos[t];
+        }
+        const int dim = 1 << op.nq;
+        auto reg_of = [&](int j, int e, int loc) {
+            int r = e;
+            for (int t = 0; t < op.nq; ++t)
+                if ((loc >> t) & 1) r |= 1 << pos[t];
+            return (j << KB) + r;
+        };
+        const std::string acc = "m" + std::to_string(idx);
+        o << "        float " << acc << " = 0.f;  // measurement column " << op.perm[0] << "\n";
+        for (int j = 0; j < GS; ++j)
+            for (int e = 0; e < (1 << KB); ++e) {
+                if (e & pmask) continue;
+                for (int r = 0; r < dim; ++r) {
+                    const int code = op.slot[r];
+                    if (code == INNER_ZERO) continue;
+                    const std::string l = "w" + std::to_string(reg_of(j, e, r));
+                    const std::string q = "v" + std::to_string(reg_of(j, e, op.perm[1 + r]));
+                    const std::string a = "(" + l + ".x * " + q + ".x + " + l + ".y * " + q + ".y)";
+                    const std::string b = "(" + l + ".x * " + q + ".y - " + l + ".y * " + q + ".x)";
+                    o << "        " << acc << ((code & 2) ? " -= " : " += ") << ((code & 1) ? a : b) << ";\n";
+                }
+            }
+    }
+
+    // the parameter-block operand of op m's coefficient slot i
+    std::string kname(int m, int i) const {
+        const auto it = kslot.find({m, i});
+        if (it == kslot.end()) throw std::logic_error("jit: coefficient not in the parameter block");
+        return "K.k[" + std::to_string(it->second) + "]";
+    }
+
+    // row r of op m's matrix times x0..x(dim-1): literals for the trivial entries,
+    // named coefficient registers for the rest (real-only when the entry is real)
+    void cmac_rt(int m, const std::vector<int>& I, int r, int dim, const std::vector<CplxF>& M, std::string& re,
+                 std::string& im) {
+        std::vector<std::pair<CplxF, std::string>> lit;
+        std::ostringstream rr, ii;
+        bool first = true;
+        for (int c = 0; c < dim; ++c) {
+            const CplxF k = M[r * dim + c];
+            const std::string x = "x" + std::to_string(c);
+            if (k.re == 0.f && k.im == 0.f) continue;
+            if (trivial_coef(k)) {
+                lit.push_back({k, x});
+                continue;
+            }
+            const std::string kn = kname(m, I[r * dim + c]);
+            if (!first) rr << " + ", ii << " + ";
+            first = false;
+            if (k.im == 0.f) {
+                rr << kn << ".x * " << x << ".x";
+                ii << kn << ".x * " << x << ".y";
+            } else {
+                rr << "(" << kn << ".x * " << x << ".x - " << kn << ".y * " << x << ".y)";
+                ii << "(" << kn << ".x * " << x << ".y + " << kn << ".y * " << x << ".x)";
+            }
+        }
+        std::string lr, li;
+        cmac_terms(lit, lr, li);
+        if (first) {
+            re = lr, im = li;
+            return;
+        }
+        re = rr.str() + (lr == "0.f" ? "" : " + " + lr);
+        im = ii.str() + (li == "0.f" ? "" : " + " + li);
+    }
+
     // emits one member op; returns true when it multiplied into the stage scalar
     bool member(int m, const int* S, uint32_t gstep, bool have_scal) {
         const DevOp& op = p.ops[m];
@@ -331,11 +577,11 @@ struct Gen {
             return -1;
         };
         auto open_scal = [&]() {
-            if (!have_scal) o << "        cf sc = cf{1.f, 0.f};\n";
+            if (!have_scal) o << "        cf " << scn << " = cf{1.f, 0.f};\n";
         };
         if (op.kind == OPK_STATESCALE) {
             open_scal();
-            o << "        sc = cscale(sc, (float)((const double*)a.ops[" << m << "].aux)[b]);\n";
+            o << "        " << scn << " = cscale(" << scn << ", (float)((const double*)a.ops[" << m << "].aux)[b]);\n";
             return true;
         }
         if (op.kind == OPK_REALTAB) {
@@ -368,7 +614,7 @@ struct Gen {
                 if (op.lb[t] < 0) rt << " | ((u32)((base >> " << op.gb[t] << ") & 1ull) << " << t << ")";
             if (!any_stage && !any_tile_nonstage) {
                 open_scal();
-                o << "        sc = cmul(sc, a.ops[" << m << "].c[" << rt.str() << "]);\n";
+                o << "        " << scn << " = cmul(" << scn << ", a.ops[" << m << "].c[" << rt.str() << "]);\n";
                 return true;
             }
             if (!any_tile_nonstage && !any_off) {
@@ -378,6 +624,10 @@ struct Gen {
                     for (int t = 0; t < op.nq; ++t) mi |= ((i >> pos[t]) & 1) << t;
                     const float re = op.cf[mi].x, im = op.cf[mi].y;
                     if (re == 1.f && im == 0.f) continue;
+                    if (p.rtc && !trivial_coef(CplxF{re, im})) {
+                        o << "        " << v(i) << " = cmul(" << kname(m, mi) << ", " << v(i) << ");\n";
+                        continue;
+                    }
                     std::string r, q;
                     cmac_terms({{CplxF{re, im}, v(i)}}, r, q);
                     o << "        " << v(i) << " = cf{" << r << ", " << q << "};\n";
@@ -405,7 +655,8 @@ struct Gen {
         int pos[3] = {-1, -1, -1};
         for (int t = 0; t < op.nq; ++t) pos[t] = spos(op.lb[t]);
         const int dim = 1 << op.nq;
-        const std::vector<CplxF> M = op_matrix_f(op);
+        std::vector<int> I;
+        const std::vector<CplxF> M = op_matrix_f(op, &I);
         int pmask = 0;
         for (int t = 0; t < op.nq; ++t) pmask |= 1 << pos[t];
         for (int j = 0; j < GS; ++j) {
@@ -428,7 +679,8 @@ struct Gen {
                         if (k.re != 0.f || k.im != 0.f) terms.push_back({k, "x" + std::to_string(c)});
                     }
                     std::string re, im;
-                    cmac_terms(terms, re, im);
+                    if (p.rtc) cmac_rt(m, I, r, dim, M, re, im);
+                    else cmac_terms(terms, re, im);
                     o << "          " << v(ix[r]) << " = cf{" << re << ", " << im << "};\n";
                 }
                 o << "        }\n";
@@ -453,6 +705,14 @@ std::string generate(const Pass& p, bool need_epi, int nbuf, int groups, int min
     o << kPrelude;
     o << "static_assert(sizeof(DevOp) == " << sizeof(DevOp) << ", \"DevOp layout\");\n";
     o << "static_assert(sizeof(TileArgs) == " << sizeof(TileArgs) << ", \"TileArgs layout\");\n";
+    if (p.rtc) {  // the run-time coefficients: a second kernel parameter
+        const size_t nk = std::max<size_t>(1, gen.kslot.size());
+        if (sizeof(TileArgs) + 8 * nk > kMaxKernelParamBytes) {
+            err = "jit: the pass has more run-time coefficients than a kernel parameter block holds";
+            return "";
+        }
+        o << "struct Coefs { cf k[" << nk << "]; };\n";
+    }
     o << "#define NT " << NT << "\n#define TB " << T << "\n#define LB " << g.L << "\n#define HB " << g.H << "\n";
     o << "#define NSHIFT " << (N - T) << "\n";
     // tile geometry as literals
@@ -483,7 +743,8 @@ std::string generate(const Pass& p, bool need_epi, int nbuf, int groups, int min
          "    for (u32 s = threadIdx.x; s < (1u << HB); s += NT)\n"
          "        bulk_g2s(buf + ((u64)s << LB), gs + seg_off(base, s), 8u << LB, bar);\n"
          "}\n";
-    o << "template <bool EPI>\n__device__ __forceinline__ void body(const TileArgs& a) {\n"
+    o << "template <bool EPI>\n__device__ __forceinline__ void body(const TileArgs& a"
+      << (p.rtc ? ", const Coefs& K" : "") << ") {\n"
          "    extern __shared__ __align__(128) unsigned char smem_raw[];\n"
          "    cf* const buf0 = (cf*)smem_raw;\n"
          "    __shared__ __align__(8) u64 bars[2];\n"
@@ -603,16 +864,136 @@ std::string generate(const Pass& p, bool need_epi, int nbuf, int groups, int min
          "    }\n"
          "    bulk_wait0();\n"
          "}\n";
-    o << "extern \"C\" __global__ void __launch_bounds__(NT, " << MINB
-      << ") smoq_pass_e0(const TileArgs a) { body<false>(a); }\n";
+    const char* params = p.rtc ? "(const TileArgs a, const Coefs K)" : "(const TileArgs a)";
+    const char* args = p.rtc ? "(a, K)" : "(a)";
+    o << "extern \"C\" __global__ void __launch_bounds__(NT, " << MINB << ") smoq_pass_e0" << params
+      << " { body<false>" << args << "; }\n";
     if (need_epi)
-        o << "extern \"C\" __global__ void __launch_bounds__(NT, " << MINB
-          << ") smoq_pass_e1(const TileArgs a) { body<true>(a); }\n";
+        o << "extern \"C\" __global__ void __launch_bounds__(NT, " << MINB << ") smoq_pass_e1" << params
+          << " { body<true>" << args << "; }\n";
+    return o.str();
+}
+
+// full source of the compiled adjoint kernel of one backward pass: the tile pair
+// (phi, lambda) in shared memory by bulk copy, then the pass's stages on both
+// register sets, measurements added to the warps' partial rows, then both tiles back
+std::string generate_adjoint(const Pass& p, std::string& err) {
+    const int N = p.g.N;
+    const TileGeom& g = p.g;
+    const int T = g.T;
+    // one 16-amplitude group of each state per thread; 2 CTAs per SM (128 registers
+    // a thread: the two register sets plus a stage's run-time coefficients)
+    const int G = 1, NT = 1 << (T - 4);
+    const int MINB = std::max(1, 65536 / (NT * 128));
+    for (const DevOp& op : p.ops)
+        if (op.kind == OPK_REALTAB || op.kind == OPK_STATESCALE || op.kind == OPK_JUMP) {
+            err = "jit: op kind not supported by the adjoint kernel";
+            return "";
+        }
+    Gen gen(p, G, NT);
+    std::ostringstream& o = gen.o;
+    o << kPrelude;
+    o << "static_assert(sizeof(DevOp) == " << sizeof(DevOp) << ", \"DevOp layout\");\n";
+    o << "static_assert(sizeof(TileArgs) == " << sizeof(TileArgs) << ", \"TileArgs layout\");\n";
+    o << "struct AdjArgs { TileArgs a; void* lam; double* partials; i64 n_rows; int n_cols; };\n";
+    o << "static_assert(sizeof(AdjArgs) == " << sizeof(AdjArgs) << ", \"AdjArgs layout\");\n";
+    const size_t nk = gen.kslot.size();
+    if (sizeof(AdjArgs) + 8 * std::max<size_t>(1, nk) > kMaxKernelParamBytes) {
+        err = "jit: the pass has more run-time coefficients than a kernel parameter block holds";
+        return "";
+    }
+    o << "struct Coefs { cf k[" << std::max<size_t>(1, nk) << "]; };\n";
+    o << "#define NT " << NT << "\n#define TB " << T << "\n#define LB " << g.L << "\n#define HB " << g.H << "\n";
+    o << "#define NSHIFT " << (N - T) << "\n";
+    o << "__device__ __forceinline__ u64 tile_base(i64 t, i64& b) {\n"
+         "    b = t >> NSHIFT;\n"
+         "    u64 base = (u64)(t & ((1ll << NSHIFT) - 1)) << LB;\n";
+    for (int m = 0; m < g.H; ++m) o << "    base = ins0(base, " << g.hb[m] << ");\n";
+    o << "    return base;\n}\n";
+    o << "__device__ __forceinline__ u64 seg_off(u64 base, u32 s) {\n    u64 off = base;\n";
+    for (int m = 0; m < g.H; ++m) o << "    off |= (u64)((s >> " << m << ") & 1u) << " << g.hb[m] << ";\n";
+    o << "    return off;\n}\n";
+    o << "extern \"C\" __global__ void __launch_bounds__(NT, " << MINB << ") smoq_adj_e0(const AdjArgs A, const Coefs K) {\n"
+         "    const TileArgs& a = A.a;\n"
+         "    extern __shared__ __align__(128) unsigned char smem_raw[];\n"
+         "    cf* const tile = (cf*)smem_raw;\n"
+         "    cf* const tlam = tile + (1u << TB);\n"
+         "    __shared__ __align__(8) u64 bar;\n"
+         "    const u32 tid = threadIdx.x;\n"
+         "    const u32 seg_bytes = 8u << LB;\n"
+         "    if (tid == 0) { mbar_init(&bar, 1); fence_mbar_init(); }\n"
+         "    __syncthreads();\n"
+         "    u32 phase = 0;\n"
+         "    for (i64 t = blockIdx.x; t < a.ntiles; t += gridDim.x) {\n"
+         "    i64 b;\n"
+         "    const u64 base = tile_base(t, b);\n"
+         "    cf* gs = (cf*)a.psi + b * a.state_len;\n"
+         "    cf* gl = (cf*)A.lam + b * a.state_len;\n"
+         "    if (tid == 0) mbar_arrive_expect_tx(&bar, 16u << TB);\n"
+         "    for (u32 s = tid; s < (1u << HB); s += NT) {\n"
+         "        bulk_g2s(tile + ((u64)s << LB), gs + seg_off(base, s), seg_bytes, &bar);\n"
+         "        bulk_g2s(tlam + ((u64)s << LB), gl + seg_off(base, s), seg_bytes, &bar);\n"
+         "    }\n"
+         "    const bool ok = mbar_wait_bounded(&bar, phase, a.err);\n"
+         "    if (!__syncthreads_and(ok)) { mbar_wait_bounded(&bar, phase, nullptr); return; }\n"
+         "    phase ^= 1;\n";
+    const int LBk = 4;
+    size_t o_i = 0;
+    while (o_i < p.ops.size()) {
+        const DevOp& h = p.ops[o_i];
+        if (h.kind != OPK_STAGE) {
+            err = "jit: adjoint pass program is not stage-scheduled";
+            return "";
+        }
+        std::vector<int> members;
+        int S[4], rl[4] = {-1, -1, -1, -1};
+        if (h.nq == 0) {
+            // one wide op: its 3 bits + one pad bit (bank-neutral first)
+            const DevOp& op = p.ops[o_i + 1];
+            std::vector<int> sv;
+            for (int t = 0; t < op.nq; ++t) sv.push_back(op.lb[t]);
+            for (int bb = LBk; (int)sv.size() < 4 && bb < T; ++bb)
+                if (std::find(sv.begin(), sv.end(), bb) == sv.end()) sv.push_back(bb);
+            for (int bb = 0; (int)sv.size() < 4 && bb < T; ++bb)
+                if (std::find(sv.begin(), sv.end(), bb) == sv.end()) sv.push_back(bb);
+            std::sort(sv.begin(), sv.end());
+            int cfree = 0;
+            for (int bb = 0; bb < LBk; ++bb)
+                if (std::find(sv.begin(), sv.end(), bb) == sv.end()) ++cfree;
+            int aa = 0;
+            for (int q = 0; q < 4; ++q) {
+                S[q] = sv[q];
+                rl[q] = sv[q] < LBk ? cfree + aa++ : -1;
+            }
+            members.push_back((int)o_i + 1);
+            o_i += 2;
+        } else {
+            for (int q = 0; q < 4; ++q) S[q] = h.perm[q], rl[q] = h.perm[4 + q];
+            for (int k = 1; k <= (int)h.aux2; ++k) members.push_back((int)(o_i + k));
+            o_i += 1 + (size_t)h.aux2;
+        }
+        gen.stage_dual(S, rl, members);
+    }
+    o << "    fence_proxy_async_smem();\n"
+         "    __syncthreads();\n"
+         "    for (u32 s = tid; s < (1u << HB); s += NT) {\n"
+         "        bulk_s2g(gs + seg_off(base, s), tile + ((u64)s << LB), seg_bytes);\n"
+         "        bulk_s2g(gl + seg_off(base, s), tlam + ((u64)s << LB), seg_bytes);\n"
+         "    }\n"
+         "    bulk_commit();\n"
+         "    bulk_wait_read0();\n"
+         "    __syncthreads();\n"
+         "    }\n"
+         "    bulk_wait0();\n"
+         "}\n";
     return o.str();
 }
 
 std::mutex g_mu;
-std::map<std::string, std::unique_ptr<JitKernel>> g_cache;
+std::map<std::string, std::unique_ptr<JitKernel>> g_cache;   // loaded kernels, by source
+std::map<std::string, std::vector<char>> g_cubins;           // compiled, not loaded yet
+// loaded run-time-coefficient kernels by pass signature (+ kernel variant)
+std::map<std::vector<int32_t>, const JitKernel*> g_by_sig;
 
 // FNV-1a of a kernel source: the key of a pass program in the tuning cache
 uint64_t fnv1a(const std::string& s) {
@@ -664,6 +1045,22 @@ bool compile_cubin(const std::string& src, std::vector<char>& cubin, std::string
 }
 }  // namespace
 
+const JitKernel* jit_pass_find(const Pass& p, int nbuf, int groups, int minb_add) {
+    if (!p.rtc || !p.staged) return nullptr;
+    std::vector<int32_t> key = jit_pass_signature(p);
+    key.insert(key.end(), {-2, nbuf, groups, minb_add});
+    return jit_sig_find(key);
+}
+
+bool jit_pass_source(const Pass& p, int nbuf, int groups, std::string& src, std::string& err) {
+    if (!p.staged || (p.g.T != 12 && p.g.T != 13)) {
+        err = "jit: only stage-scheduled passes of tile width 12-13";
+        return false;
+    }
+    src = generate(p, p.epilogue, nbuf, groups, 0, err);
+    return !src.empty();
+}
+
 // Generate and compile a staged complex64 pass without loading it (host only);
 // `info` (optional) receives the compiler's resource report.
 bool jit_check_pass(const Pass& p, int nbuf, int groups, std::string& err, size_t* cubin_bytes,
@@ -680,23 +1077,23 @@ bool jit_check_pass(const Pass& p, int nbuf, int groups, std::string& err, size_
     return true;
 }
 
-// Compile (or fetch) the kernel of a stage-scheduled complex64 pass and load
-// it into the current device.  Returns nullptr and fills `err` on failure.
-const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, int groups, std::string& err, int minb_add) {
-    if (!p.staged || (p.g.T != 12 && p.g.T != 13)) {
-        err = "jit: only stage-scheduled passes of tile width 12-13";
-        return nullptr;
-    }
-    std::string src = generate(p, p.epilogue, nbuf, groups, minb_add, err);
-    if (src.empty()) return nullptr;
+namespace {
+// the loaded kernel of a generated source: from the process cache, from a cubin
+// that jit_precompile left, or compiled here; then loaded into the current device
+const JitKernel* load_source(const std::string& src, int threads, size_t smem, int nfn, const char* const* names,
+                             std::string& err) {
+    std::vector<char> cubin;
     {
         std::lock_guard<std::mutex> lk(g_mu);
         auto it = g_cache.find(src);
         if (it != g_cache.end()) return it->second.get();
+        auto ct = g_cubins.find(src);  // compiled ahead by jit_precompile
+        if (ct != g_cubins.end()) {
+            cubin.swap(ct->second);
+            g_cubins.erase(ct);
+        }
     }
-    // compile outside the lock: several host threads may compile different passes at once
-    std::vector<char> cubin;
-    if (!compile_cubin(src, cubin, err)) return nullptr;
+    if (cubin.empty() && !compile_cubin(src, cubin, err)) return nullptr;
     std::lock_guard<std::mutex> lk(g_mu);
     auto it = g_cache.find(src);
     if (it != g_cache.end()) return it->second.get();
@@ -707,10 +1104,9 @@ const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, int groups, std::strin
         err = std::string("cudaLibraryLoadData: ") + cudaGetErrorString(e);
         return nullptr;
     }
-    k->threads = 1 << (p.g.T - 4 - (groups - 1));
-    k->smem = (size_t)(nbuf == 2 ? 16 : 8) << p.g.T;
-    const char* names[2] = {"smoq_pass_e0", "smoq_pass_e1"};
-    for (int v = 0; v < (p.epilogue ? 2 : 1); ++v) {
+    k->threads = threads;
+    k->smem = smem;
+    for (int v = 0; v < nfn; ++v) {
         cudaKernel_t kern = nullptr;
         if ((e = cudaLibraryGetKernel(&kern, lib, names[v])) != cudaSuccess) {
             err = std::string("cudaLibraryGetKernel: ") + cudaGetErrorString(e);
@@ -731,11 +1127,181 @@ const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, int groups, std::strin
         k->per_sm[v] = per_sm < 1 ? 1 : per_sm;
     }
     const JitKernel* out = k.get();
-    g_cache.emplace(std::move(src), std::move(k));
+    g_cache.emplace(src, std::move(k));
     return out;
+}
+}  // namespace
+
+// Compile (or fetch) the kernel of a stage-scheduled complex64 pass and load
+// it into the current device.  Returns nullptr and fills `err` on failure.  A
+// run-time-coefficient pass is looked up by its signature first (no source is
+// generated for a later parameter set of the same circuit).
+const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, int groups, std::string& err, int minb_add) {
+    if (!p.staged || (p.g.T != 12 && p.g.T != 13)) {
+        err = "jit: only stage-scheduled passes of tile width 12-13";
+        return nullptr;
+    }
+    std::vector<int32_t> key;
+    if (p.rtc) {
+        key = jit_pass_signature(p);
+        key.insert(key.end(), {-2, nbuf, groups, minb_add});
+        if (const JitKernel* k = jit_sig_find(key)) return k;
+    }
+    std::string src = generate(p, p.epilogue, nbuf, groups, minb_add, err);
+    if (src.empty()) return nullptr;
+    static const char* const names[2] = {"smoq_pass_e0", "smoq_pass_e1"};
+    const JitKernel* k = load_source(src, 1 << (p.g.T - 4 - (groups - 1)), (size_t)(nbuf == 2 ? 16 : 8) << p.g.T,
+                                     p.epilogue ? 2 : 1, names, err);
+    if (k && p.rtc) {
+        const_cast<JitKernel*>(k)->rtc = true;
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_by_sig.emplace(key, k);
+    }
+    return k;
+}
+
+// the adjoint kernel of a staged backward pass (tile width 12: two 32 KB tiles)
+static bool adjoint_ok(const Pass& p, std::string& err) {
+    if (!p.staged || p.g.T != 12) {
+        err = "jit: the adjoint kernel takes stage-scheduled passes of tile width 12";
+        return false;
+    }
+    return true;
+}
+
+void jit_rtc_block(const Pass& p, std::vector<float2>& out) {
+    out.clear();
+    if (p.rtc)
+        for (const auto& mi : rtc_list(p)) out.push_back(p.ops[mi.first].cf[mi.second]);
+    if (out.empty()) out.push_back(make_float2(0.f, 0.f));  // (the block has at least one entry)
+}
+
+namespace {
+
+// class of a coefficient as the run-time-coefficient generator sees it: the
+// literals 0, 1, -1, i, -i; a parameter-block entry read as real or as complex
+int32_t coef_class(float2 c) {
+    const CplxF k{c.x, c.y};
+    if (trivial_coef(k)) return 1 + (int32_t)(k.re + 1.f) * 3 + (int32_t)(k.im + 1.f);
+    return k.im == 0.f ? 20 : 21;
+}
+}  // namespace
+
+// Everything the generators read from a run-time-coefficient pass: its tile
+// geometry, and per op the kind, qubits, codes and flags and the class of each
+// coefficient (never its value).  Two passes with equal signatures get the same
+// kernel source (for the same kernel variant).
+std::vector<int32_t> jit_pass_signature(const Pass& p) {
+    std::vector<int32_t> s{p.g.N, p.g.T, p.g.L, p.g.H, p.rtc ? 1 : 0, p.staged ? 1 : 0, p.epilogue ? 1 : 0};
+    for (int m = 0; m < p.g.H; ++m) s.push_back(p.g.hb[m]);
+    for (const DevOp& op : p.ops) {
+        s.insert(s.end(), {op.kind, op.nq, op.flags, (int32_t)op.aux2});
+        s.insert(s.end(), op.lb, op.lb + 4);
+        s.insert(s.end(), op.gb, op.gb + 4);
+        s.insert(s.end(), op.slot, op.slot + 4);
+        s.insert(s.end(), op.perm, op.perm + 8);
+        for (int k = 0; k < 16; ++k) {
+            if (p.rtc) s.push_back(coef_class(op.cf[k]));
+            else {  // (literal coefficients: the values themselves)
+                int32_t b[2];
+                std::memcpy(b, &op.cf[k], sizeof b);
+                s.insert(s.end(), b, b + 2);
+            }
+        }
+    }
+    return s;
+}
+
+const JitKernel* jit_sig_find(const std::vector<int32_t>& sig) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    const auto it = g_by_sig.find(sig);
+    return it == g_by_sig.end() ? nullptr : it->second;
+}
+
+std::string jit_adjoint_source(const Pass& p, std::string& err) {
+    if (!adjoint_ok(p, err)) return std::string();
+    return generate_adjoint(p, err);
+}
+
+const JitKernel* jit_adjoint_load(const Pass& p, const std::string& src, const std::vector<int32_t>& sig,
+                                  std::string& err) {
+    if (const JitKernel* k = jit_sig_find(sig)) return k;
+    if (!adjoint_ok(p, err)) return nullptr;
+    if (src.empty()) {
+        err = "jit: no adjoint kernel source";
+        return nullptr;
+    }
+    static const char* const names[1] = {"smoq_adj_e0"};
+    const JitKernel* k = load_source(src, 1 << (p.g.T - 4), (size_t)16 << p.g.T, 1, names, err);
+    if (k) {
+        const_cast<JitKernel*>(k)->rtc = p.rtc;
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_by_sig.emplace(sig, k);
+    }
+    return k;
+}
+
+bool jit_check_adjoint(const Pass& p, std::string& err, std::string* info, std::string* source) {
+    if (!adjoint_ok(p, err)) return false;
+    const std::string src = generate_adjoint(p, err);
+    if (src.empty()) return false;
+    if (source) {
+        *source = src;
+        return true;
+    }
+    std::vector<char> cubin;
+    return compile_cubin(src, cubin, err, info);
 }
 
 bool jit_available() { return nvrtc().ok; }
+
+// NVRTC on host threads for every request whose kernel is neither loaded nor
+// compiled yet; the cubins wait in g_cubins until jit_pass_kernel loads them on
+// the calling thread (the worker threads make no CUDA calls)
+void jit_precompile(const std::vector<JitRequest>& reqs) {
+    if (!nvrtc().ok) return;
+    std::vector<std::string> srcs;
+    for (const JitRequest& r : reqs) {
+        if (!r.p || !r.p->staged || (r.p->g.T != 12 && r.p->g.T != 13)) continue;
+        std::string err;
+        std::string src = generate(*r.p, r.p->epilogue, r.nbuf, r.groups, r.minb_add, err);
+        if (!src.empty()) srcs.push_back(std::move(src));
+    }
+    std::vector<const std::string*> ptr;
+    for (const std::string& x : srcs) ptr.push_back(&x);
+    jit_precompile_sources(ptr);
+}
+
+void jit_precompile_sources(const std::vector<const std::string*>& srcs) {
+    if (!nvrtc().ok) return;
+    std::vector<std::string> todo;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        std::set<std::string> seen;
+        for (const std::string* src : srcs) {
+            if (!src || src->empty() || g_cache.count(*src) || g_cubins.count(*src) || !seen.insert(*src).second)
+                continue;
+            todo.push_back(*src);
+        }
+    }
+    if (todo.empty()) return;
+    std::vector<std::vector<char>> out(todo.size());
+    std::atomic<size_t> next(0);
+    auto work = [&]() {
+        for (size_t i; (i = next++) < todo.size();) {
+            std::string err;
+            if (!compile_cubin(todo[i], out[i], err)) out[i].clear();  // jit_pass_kernel reports the error
+        }
+    };
+    const size_t nt = std::max<size_t>(1, std::min<size_t>(todo.size(), std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < nt; ++t) pool.emplace_back(work);
+    work();
+    for (std::thread& t : pool) t.join();
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (size_t i = 0; i < todo.size(); ++i)
+        if (!out[i].empty()) g_cubins.emplace(std::move(todo[i]), std::move(out[i]));
+}
 
 uint64_t jit_pass_key(const Pass& p, int nbuf) {
     std::string err;
@@ -743,13 +1309,13 @@ uint64_t jit_pass_key(const Pass& p, int nbuf) {
     return src.empty() ? 0 : fnv1a(src);
 }
 
-cudaError_t launch_jit(smoq_ctx* ctx, const TileArgs& a, const JitKernel* k, bool epi) {
+cudaError_t launch_jit(smoq_ctx* ctx, const TileArgs& a, const JitKernel* k, bool epi, const float2* coefs) {
     const void* fn = k->fn[epi ? 1 : 0];
-    if (!fn) return cudaErrorInvalidValue;
+    if (!fn || (k->rtc && !coefs)) return cudaErrorInvalidValue;
     int64_t grid = (int64_t)ctx->num_sms * k->per_sm[epi ? 1 : 0];
     if (grid > a.ntiles) grid = a.ntiles;
     TileArgs args = a;
-    void* params[] = {&args};
+    void* params[] = {&args, const_cast<float2*>(coefs)};
     return cudaLaunchKernel(fn, dim3((unsigned)grid), dim3((unsigned)k->threads), params, k->smem, ctx->stream);
 }
 

@@ -90,11 +90,12 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 // (a legitimate tile copy completes in microseconds) or 2^22 polls, whichever
 // comes first, records DEVERR_TIMEOUT and returns false.
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int32_t* err) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int32_t* err,
+                                                  uint64_t limit_ns = kWaitLimitNs) {
     const uint64_t t0 = globaltimer_ns();
     for (int it = 0; it < (1 << 22); ++it) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 63) == 63 && globaltimer_ns() - t0 > kWaitLimitNs) break;
+        if ((it & 63) == 63 && globaltimer_ns() - t0 > limit_ns) break;
     }
     if (err) atomicExch(err, DEVERR_TIMEOUT);
     return false;

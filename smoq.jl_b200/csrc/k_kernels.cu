@@ -220,6 +220,31 @@ __global__ void __launch_bounds__(256) direct_op_kernel(typename CT<R>::T* psi, 
         sweep_op<R, uint64_t>(op, psi + b * len, N, op.gb, tid, nthr);
 }
 
+// --------------------------------------------------------------- failure path
+// A wait that nothing completes: the barrier's one arrival comes with an
+// expectation of 16 bytes that no copy delivers, so the bounded wait of the
+// tile kernels (mbar_wait_bounded) runs out after limit_ns, records
+// DEVERR_TIMEOUT in the error word and returns.  No copy is issued, so nothing
+// is in flight when the block exits.
+__global__ void wait_timeout_probe_kernel(int32_t* err, uint64_t limit_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(&bar, 16);
+        mbar_wait_bounded(&bar, 0, err, limit_ns);
+    }
+}
+
+cudaError_t launch_wait_timeout_probe(smoq_ctx* ctx, uint64_t limit_ns) {
+    wait_timeout_probe_kernel<<<1, 32, 0, ctx->stream>>>(ctx->d_err, limit_ns);
+    ctx->launches++;
+    return cudaGetLastError();
+}
+
 // --------------------------------------------------------------- reductions
 // out_partials[(b * nblk + blk) * nobs + o] = sum over this block's amplitudes
 // of |psi|^2 * (-1)^{popc(i & zmask_o)}.  Accumulation in FP64.
@@ -510,7 +535,7 @@ cudaError_t launch_tile_pass(smoq_ctx* ctx, smoq_state* st, const Pass& p, const
     cudaError_t e;
     const bool epi = ep && ep->partials;
     if (p.jit) {
-        e = launch_jit(ctx, a, p.jit, epi);
+        e = launch_jit(ctx, a, p.jit, epi, p.rtc ? p.coefs.data() : nullptr);
         ctx->launches++;
         return e;
     }

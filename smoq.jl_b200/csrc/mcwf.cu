@@ -140,7 +140,8 @@ using namespace smoq;
 // pieces of capi.cu this file uses
 smoq_status smoq_internal_plan_step(smoq_plan* plan, std::vector<GateIR>& out, int& N, int& dtype, int& order);
 smoq_status smoq_internal_prepare(smoq_ctx* ctx, smoq_state* st, const std::vector<GateIR>& gates,
-                                  int epilogue_special, bool reusable, void** prog_handle);
+                                  int epilogue_special, bool reusable, void** prog_handle,
+                                  bool variational = false);
 smoq_status smoq_internal_rerun(smoq_ctx* ctx, smoq_state* st, void* prog_handle, const Epilogue* ep);
 void smoq_internal_free_prog(void* prog_handle);
 smoq_status smoq_internal_fail(smoq_ctx* ctx, smoq_status s, const char* msg);

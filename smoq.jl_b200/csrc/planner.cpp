@@ -565,13 +565,17 @@ static void swap_qubit_roles(DevOp& op) {
 // always hit distinct banks.  The kernel folds the rotation into per-thread
 // coefficients, once per op.
 // ----------------------------------------------------------------------------
-void schedule_stages(Pass& p, int amp_bytes) {
+void schedule_stages(Pass& p, int amp_bytes, bool allow_inner) {
     const int T = p.g.T;
     constexpr int K = 4;
     if (T < 12 || T > 13) return;
     const int LB = amp_bytes == 8 ? 4 : 3;
-    for (const DevOp& op : p.ops)  // adjoint partials and layout ops belong to other kernels
-        if (op.kind == OPK_INNER || op.kind == OPK_JUMP || op.kind == OPK_STAGE) return;
+    // adjoint measurements only for the compiled adjoint kernels, and only plain ones
+    // (a U^dag folded into a measurement belongs to the shared-memory adjoint kernel)
+    for (const DevOp& op : p.ops)
+        if ((op.kind == OPK_INNER && (!allow_inner || (op.flags & (INNER_PRE | INNER_PREDIAG)))) ||
+            op.kind == OPK_JUMP || op.kind == OPK_STAGE)
+            return;
     std::vector<DevOp> in = std::move(p.ops);
     // 1- and 2-qubit permutations run as dense matrices on the stage registers
     for (DevOp& op : in) {
@@ -648,6 +652,10 @@ void schedule_stages(Pass& p, int amp_bytes) {
         out.push_back(h);
         for (size_t k = i; k < j; ++k) {
             DevOp op = in[k];
+            if (op.kind == OPK_INNER) {  // its slot[] holds the generator's i^k codes: keep them
+                out.push_back(op);
+                continue;
+            }
             for (int t = 0; t < 4; ++t) op.slot[t] = -1;
             if (op.kind != OPK_DIAG && op.kind != OPK_STATESCALE && op.kind != OPK_REALTAB) {
                 for (int t = 0; t < op.nq; ++t)

@@ -105,6 +105,16 @@ struct HamTerm {
     int32_t pad;
 };
 
+// Arguments of the adjoint backward pass over the tile pair (phi, lambda); the
+// compiled adjoint kernels (jit.cpp) mirror this layout
+struct AdjArgs {
+    TileArgs a;        // a.psi = phi
+    void* lam;
+    double* partials;  // [n_rows][n_cols]: row = CTA x warps + warp, column = measurement
+    int64_t n_rows;
+    int32_t n_cols;
+};
+
 // ----------------------------------------------------------------------------
 // Host-side gate IR consumed by the planner.
 // ----------------------------------------------------------------------------
@@ -136,6 +146,7 @@ struct JitKernel {
     int threads = 0;
     int per_sm[2] = {1, 1};
     size_t smem = 0;
+    bool rtc = false;  // takes the run-time coefficient block as its second parameter
 };
 
 struct Pass {
@@ -144,6 +155,9 @@ struct Pass {
     bool epilogue = false;
     bool staged = false;    // scheduled for the stage-sweep engine (OPK_STAGE headers)
     bool want_jit = false;  // engine 3: compile this staged pass to its own kernel at upload
+    bool rtc = false;       // compiled kernel reads the op coefficients at run time: its
+                            // source depends on the circuit's structure, not its angles
+    std::vector<float2> coefs;  // with rtc: the coefficient block of this pass's launches
     const JitKernel* jit = nullptr;
 };
 
@@ -152,15 +166,50 @@ std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, in
                               int epilogue_after_special = -1, int Lreq = 0);
 // turn a planned pass into stage sweeps of 4 tile bits (engines 2, 3); amp_bytes
 // selects the bank geometry
-void schedule_stages(Pass& p, int amp_bytes);
+void schedule_stages(Pass& p, int amp_bytes, bool allow_inner = false);
 void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op);
 // jit.cpp: compile (or fetch from the process cache) the kernel of a staged complex64 pass
 // (minb_add: that many more CTAs per SM than the default register budget allows)
 const JitKernel* jit_pass_kernel(const Pass& p, int nbuf, int groups, std::string& err, int minb_add = 0);
+// one kernel variant of a staged pass, for jit_precompile
+struct JitRequest {
+    const Pass* p;
+    int nbuf, groups, minb_add;
+};
+// jit.cpp: compile the requested kernels with NVRTC on host threads (no CUDA
+// calls there); a later jit_pass_kernel of the same variant only loads it
+void jit_precompile(const std::vector<JitRequest>& reqs);
+// jit.cpp: the compiled kernel of a staged ADJOINT pass (complex64): U^dag ops on the
+// tile pair (phi, lambda) and the OPK_INNER measurements in 4-bit register stages
+std::string jit_adjoint_source(const Pass& p, std::string& err);
+// compile generated sources with NVRTC on host threads (no CUDA calls) for a later load
+void jit_precompile_sources(const std::vector<const std::string*>& srcs);
+// the structural signature of a staged pass (equal signatures: equal kernel sources)
+std::vector<int32_t> jit_pass_signature(const Pass& p);
+// the loaded kernel of a signature, or nullptr
+const JitKernel* jit_sig_find(const std::vector<int32_t>& sig);
+// load the adjoint kernel of `p` from its source (compiled ahead, or compiled here)
+// and file it under its signature
+const JitKernel* jit_adjoint_load(const Pass& p, const std::string& src, const std::vector<int32_t>& sig,
+                                  std::string& err);
+// jit.cpp: the run-time coefficient block of a pass compiled with rtc (the kernel's
+// second parameter, in the order the generated code indexes it)
+void jit_rtc_block(const Pass& p, std::vector<float2>& out);
+// the kernel parameter space of a launch (CUDA 12.1+ on Volta and later)
+constexpr size_t kMaxKernelParamBytes = 32764;
+// jit.cpp: generate and compile the adjoint kernel of a staged backward pass without
+// loading it (host only); `info` (optional) receives the compiler's resource report;
+// with `source` the generated source is returned there instead of being compiled
+bool jit_check_adjoint(const Pass& p, std::string& err, std::string* info, std::string* source = nullptr);
 // the tuning-cache key of a staged pass program (hash of its default kernel source)
 uint64_t jit_pass_key(const Pass& p, int nbuf);
 // jit.cpp: generate and compile a staged complex64 pass without a GPU (plan checks)
 bool jit_check_pass(const Pass& p, int nbuf, int groups, std::string& err, size_t* cubin_bytes, std::string* info);
+// jit.cpp: the loaded kernel of a run-time-coefficient pass with this signature and
+// variant, or nullptr (no source generated)
+const JitKernel* jit_pass_find(const Pass& p, int nbuf, int groups, int minb_add);
+// jit.cpp: the generated source of a staged complex64 pass (host only)
+bool jit_pass_source(const Pass& p, int nbuf, int groups, std::string& src, std::string& err);
 // jit.cpp: NVRTC could be loaded
 bool jit_available();
 
@@ -195,7 +244,8 @@ struct smoq_ctx {
     int jit_buffers = 1;               // compiled pass kernels: tile buffers per CTA (1 or 2)
     int jit_groups = 2;                // compiled pass kernels: 16-amplitude register groups per thread
     bool vqe_resident = true;          // many-circuit VQE: small circuits in one shared-memory launch
-    bool autotune = true;              // time the compiled kernels' variants per pass at plan upload
+    bool autotune = true;              // tune plan geometry and compiled-kernel variants at plan upload
+    int fusion_depth = 0;              // max fused ops per pass (0 = as many as fit)
     std::string tune_report;           // the tuner's per-pass timings and choices
     long long launches = 0;            // kernels launched by this ctx
     long long tile_passes = 0;
@@ -226,6 +276,8 @@ cudaError_t launch_diag_reduce(smoq_ctx* ctx, smoq_state* st, const uint64_t* zm
 cudaError_t launch_pauli_reduce(smoq_ctx* ctx, smoq_state* st, uint64_t xmask, uint64_t zmask,
                                 int ny, double* d_out);
 cudaError_t launch_set_basis(smoq_state* st, uint64_t index);
+// a bounded mbarrier wait that nothing completes (the failure path's test)
+cudaError_t launch_wait_timeout_probe(smoq_ctx* ctx, uint64_t limit_ns);
 cudaError_t launch_scale(smoq_state* st, const double* d_scale_per_state, double scalar);
 cudaError_t launch_convert(smoq_state* dst, smoq_state* src);
 size_t diag_reduce_scratch_doubles(smoq_state* st, int nobs);
@@ -233,7 +285,8 @@ size_t tile_max_smem(int amp_bytes, int T);
 cudaError_t tile_kernels_init(smoq_ctx* ctx);
 cudaError_t stage_kernels_init(smoq_ctx* ctx);
 cudaError_t launch_stage(smoq_ctx* ctx, const TileArgs& a, int dtype, bool epi);
-cudaError_t launch_jit(smoq_ctx* ctx, const TileArgs& a, const JitKernel* k, bool epi);
+cudaError_t launch_jit(smoq_ctx* ctx, const TileArgs& a, const JitKernel* k, bool epi,
+                       const float2* coefs = nullptr);
 cudaError_t vqe_kernels_init(smoq_ctx* ctx);
 // lam = H psi for one state (vqe.cu); per block the FP64 partials of Re<psi|lam>
 // (d_part[blk]) and <psi|psi> (d_part[eblocks + blk])

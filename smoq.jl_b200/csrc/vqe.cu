@@ -315,14 +315,6 @@ __device__ __forceinline__ R inner_pairs(const DevOp& op, typename CT<R>::T* P, 
     return acc;
 }
 
-struct AdjArgs {
-    TileArgs a;      // a.psi = phi
-    void* lam;
-    double* partials;  // [n_rows][n_cols]: row = CTA x warps + warp, column = measurement
-    int64_t n_rows;
-    int32_t n_cols;
-};
-
 // warp sum of one measurement, added to this warp's row of the partials
 template <typename R>
 __device__ __forceinline__ void inner_flush(R acc, const AdjArgs& A, int col) {
@@ -619,7 +611,8 @@ smoq_status smoq_internal_fail(smoq_ctx* ctx, smoq_status s, const char* msg);
 smoq_status smoq_internal_cuda(smoq_ctx* ctx, cudaError_t e, const char* where);
 smoq_status smoq_internal_ops_to_ir(int N, const smoq_op* ops, int n, const double* theta, std::vector<GateIR>& out);
 smoq_status smoq_internal_prepare(smoq_ctx* ctx, smoq_state* st, const std::vector<GateIR>& gates,
-                                  int epilogue_special, bool reusable, void** prog_handle);
+                                  int epilogue_special, bool reusable, void** prog_handle,
+                                  bool variational = false);
 smoq_status smoq_internal_rerun(smoq_ctx* ctx, smoq_state* st, void* prog_handle, const Epilogue* ep);
 void smoq_internal_free_prog(void* prog_handle);
 int smoq_internal_tile_bits(smoq_ctx* ctx, int dtype);
@@ -806,7 +799,7 @@ static smoq_status forward_and_h(smoq_ctx* ctx, Work& w, const std::vector<GateI
     VCK(launch_set_basis(&w.phi, 0));
     if (!ir.empty()) {
         void* h = nullptr;
-        if (smoq_status s = smoq_internal_prepare(ctx, &w.phi, ir, -1, false, &h)) return s;
+        if (smoq_status s = smoq_internal_prepare(ctx, &w.phi, ir, -1, false, &h, true)) return s;
         std::unique_ptr<void, void (*)(void*)> hold(h, smoq_internal_free_prog);
         if (smoq_status s = smoq_internal_rerun(ctx, &w.phi, h, nullptr)) return s;
         VCK(cudaStreamSynchronize(ctx->stream));  // the program is freed at scope exit
@@ -863,12 +856,21 @@ static bool build_backward(const std::vector<GateIR>& ir, const smoq_op* ops, in
 struct GradPlan {
     std::vector<GateIR> ir;
     std::vector<Pass> passes;    // the backward passes, measurements fused
+    std::vector<Pass> staged;    // per pass: its stage schedule when the compiled adjoint
+                                 // kernel runs it (staged[i].staged false: the shared-memory kernel)
+    std::vector<std::vector<int32_t>> sig;   // ... that kernel's signature
+    std::vector<std::string> src;            // ... and source (empty when it is loaded already)
+    std::vector<std::vector<float2>> coefs;  // ... and its run-time coefficients
     std::vector<int> inner_param;  // measurement -> parameter
     smoq_status status = SMOQ_OK;
     std::string error;
 };
+// jit (1, 2): complex64 backward passes of tile width 12 get the compiled adjoint
+// kernel (4-bit register stages on both states, coefficients read at run time, so
+// the NVRTC compile of the first parameter set serves all later ones); with jit = 1
+// they are compiled here, on the planning thread, and loaded by the caller
 static void plan_gradient(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops, int n,
-                          const double* th, bool grad, GradPlan& gp) {
+                          const double* th, bool grad, GradPlan& gp, int jit = 0) {
     if ((gp.status = smoq_internal_ops_to_ir(N, ops, n, th, gp.ir))) {
         gp.error = "bad op list";
         return;
@@ -888,6 +890,38 @@ static void plan_gradient(int N, smoq_dtype dtype, int tile_bits, int low_bits, 
         gp.status = SMOQ_ERR_BADINPUT;
         gp.error = ex.what();
         return;
+    }
+    gp.staged.assign(gp.passes.size(), Pass());
+    gp.src.assign(gp.passes.size(), std::string());
+    gp.sig.assign(gp.passes.size(), std::vector<int32_t>());
+    gp.coefs.assign(gp.passes.size(), std::vector<float2>());
+    if (jit && dtype == SMOQ_C64) {
+        std::vector<const std::string*> todo;
+        for (size_t i = 0; i < gp.passes.size(); ++i) {
+            Pass q = gp.passes[i];  // (before the measurements are fused)
+            q.rtc = true;
+            schedule_stages(q, 8, true);
+            if (!q.staged || q.g.T != 12) continue;
+            std::vector<float2> blk;  // the coefficients must fit the kernel parameter space
+            jit_rtc_block(q, blk);
+            if (sizeof(AdjArgs) + sizeof(float2) * blk.size() > kMaxKernelParamBytes) continue;
+            std::vector<int32_t> sig = jit_pass_signature(q);
+            if (jit == 1 && jit_sig_find(sig)) {  // a later parameter set of a known circuit
+                gp.staged[i] = std::move(q);
+                gp.sig[i] = std::move(sig);
+                gp.coefs[i] = std::move(blk);
+                continue;
+            }
+            std::string err;
+            std::string src = jit_adjoint_source(q, err);
+            if (src.empty()) continue;  // (an op the compiled kernel does not take)
+            gp.staged[i] = std::move(q);
+            gp.sig[i] = std::move(sig);
+            gp.src[i] = std::move(src);
+            gp.coefs[i] = std::move(blk);
+            todo.push_back(&gp.src[i]);
+        }
+        if (jit == 1) jit_precompile_sources(todo);
     }
     for (Pass& p : gp.passes)
         if ((gp.status = fuse_measurements(p.ops, gp.error))) return;
@@ -927,6 +961,7 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
 
     // the next parameter set is prepared on a host thread while this one runs
     const int tb = smoq_internal_tile_bits(ctx, dtype), lbits = smoq_internal_low_bits(ctx, dtype);
+    const int jit = (ctx->engine == 3 || (ctx->engine < 0 && jit_available())) ? 1 : 0;
     auto theta_of = [&](int b) { return theta ? theta + (size_t)b * n_params : nullptr; };
     std::unique_ptr<GradPlan> cur(new GradPlan), nxt;
     std::thread ahead;
@@ -937,7 +972,7 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
         }
     } joiner{ahead};
     const bool use_pre = pre && batch == 1;
-    if (!use_pre) plan_gradient(N, dtype, tb, lbits, ops, n, theta_of(0), grads != nullptr, *cur);
+    if (!use_pre) plan_gradient(N, dtype, tb, lbits, ops, n, theta_of(0), grads != nullptr, *cur, jit);
     for (int b = 0; b < batch; ++b) {
         if (b > 0) {
             ahead.join();
@@ -948,7 +983,7 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
             GradPlan* np = nxt.get();
             const double* th1 = theta_of(b + 1);
             const bool want_grad = grads != nullptr;
-            ahead = std::thread([=]() { plan_gradient(N, dtype, tb, lbits, ops, n, th1, want_grad, *np); });
+            ahead = std::thread([=]() { plan_gradient(N, dtype, tb, lbits, ops, n, th1, want_grad, *np, jit); });
         }
         GradPlan& gp = use_pre ? *pre : *cur;
         if (gp.status) return smoq_internal_fail(ctx, gp.status, gp.error.c_str());
@@ -963,19 +998,32 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
         std::vector<Pass>& passes = gp.passes;
         std::vector<size_t> opoff(passes.size() + 1, 0);
         std::vector<int64_t> grid(passes.size(), 0);
+        std::vector<const JitKernel*> kern(passes.size(), nullptr);
         std::vector<DevOp> all;
-        int64_t max_grid = 1;
+        int64_t max_rows = 1;
         for (size_t i = 0; i < passes.size(); ++i) {
+            const int64_t ntiles = (int64_t)1 << (N - passes[i].g.T);
+            if (gp.staged[i].staged) {  // the compiled adjoint kernel of this pass
+                std::string why;
+                kern[i] = jit_adjoint_load(gp.staged[i], gp.src[i], gp.sig[i], why);
+                if (!kern[i]) return smoq_internal_fail(ctx, SMOQ_ERR_UNSUPPORTED, ("compiled adjoint kernel: " + why).c_str());
+                const std::vector<DevOp>& so = gp.staged[i].ops;
+                opoff[i + 1] = opoff[i] + so.size();
+                all.insert(all.end(), so.begin(), so.end());
+                grid[i] = std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)ctx->num_sms * kern[i]->per_sm[0]));
+                max_rows = std::max(max_rows, grid[i] * (kern[i]->threads / 32));
+                continue;
+            }
             opoff[i + 1] = opoff[i] + passes[i].ops.size();
             all.insert(all.end(), passes[i].ops.begin(), passes[i].ops.end());
             const size_t smem = (size_t)2 * w.phi.amp_bytes() << passes[i].g.T;
             if (smem > kAdjMaxSmem) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "adjoint tile too wide");
-            grid[i] = adj_grid(ctx, dtype, (int64_t)1 << (N - passes[i].g.T), smem);
-            max_grid = std::max(max_grid, grid[i]);
+            grid[i] = adj_grid(ctx, dtype, ntiles, smem);
+            max_rows = std::max(max_rows, grid[i] * (kAdjThreads / 32));
         }
         // partials: one row per warp of the widest launch, one column per measurement
         const int32_t ncols = (int32_t)inner_param.size();
-        const int64_t nrows = max_grid * (kAdjThreads / 32);
+        const int64_t nrows = max_rows;
         double *d_part, *d_sum;
         DevOp* d_ops;
         VCK(cudaMallocAsync((void**)&d_part, (size_t)nrows * ncols * sizeof(double), ctx->stream));
@@ -992,7 +1040,7 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
             A.a.tiles_per_state = (int64_t)1 << (N - p.g.T);
             A.a.ntiles = A.a.tiles_per_state;
             A.a.ops = d_ops + opoff[i];
-            A.a.nops = (int32_t)p.ops.size();
+            A.a.nops = (int32_t)(opoff[i + 1] - opoff[i]);
             A.a.err = ctx->d_err;
             A.a.g = p.g;
             A.a.ep.partials = nullptr;
@@ -1002,6 +1050,14 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
             A.n_rows = nrows;
             A.n_cols = ncols;
             const size_t smem = (size_t)2 * w.phi.amp_bytes() << p.g.T;
+            if (kern[i]) {
+                void* params[] = {&A, gp.coefs[i].data()};  // (the angles of this parameter set)
+                VCK(cudaLaunchKernel(kern[i]->fn[0], dim3((unsigned)grid[i]), dim3((unsigned)kern[i]->threads), params,
+                                     kern[i]->smem, ctx->stream));
+                ctx->launches++;
+                ctx->tile_passes++;
+                continue;
+            }
             // (the kernels' shared-memory limit is set once per context, vqe_kernels_init:
             // setting it per launch would race between contexts driven from several threads)
             if (dtype == SMOQ_C64) adj_tile_kernel<float><<<(unsigned)grid[i], kAdjThreads, smem, ctx->stream>>>(A);
@@ -1032,6 +1088,53 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
         // unitary circuit, so the raw adjoint sums are divided by the same <phi|phi>
         for (int32_t c = 0; c < ncols; ++c) g[inner_param[c]] += colsum[c] / nrm2;
     }
+    return SMOQ_OK;
+}
+
+extern "C" smoq_status smoq_debug_compile_adjoint(int N, const smoq_op* ops, int n, int n_params, const double* theta,
+                                                  int tile_bits, int low_bits, int flags, int* n_passes,
+                                                  int* n_compiled, char* msg, int msg_len) {
+    if (N < 1 || N > 34 || n < 0 || (n > 0 && !ops) || n_params < 0 || (n_params > 0 && !theta) || !n_passes ||
+        !n_compiled || tile_bits < 7 || tile_bits > 14 || (flags & ~3))
+        return SMOQ_ERR_BADINPUT;
+    for (int i = 0; i < n; ++i)
+        if (ops[i].param >= n_params) return SMOQ_ERR_BADINPUT;
+    auto say = [&](const std::string& m) {
+        if (msg && msg_len > 0) {
+            std::strncpy(msg, m.c_str(), (size_t)msg_len - 1);
+            msg[msg_len - 1] = 0;
+        }
+    };
+    *n_passes = *n_compiled = 0;
+    if (!jit_available()) {
+        say("NVRTC not available");
+        return SMOQ_ERR_UNSUPPORTED;
+    }
+    GradPlan gp;
+    plan_gradient(N, SMOQ_C64, tile_bits, low_bits, ops, n, theta, true, gp, 2);
+    if (gp.status) {
+        say(gp.error);
+        return gp.status;
+    }
+    *n_passes = (int)gp.passes.size();
+    std::string report;
+    for (size_t i = 0; i < gp.staged.size(); ++i) {
+        const Pass& q = gp.staged[i];
+        if (!q.staged) continue;
+        std::string why, info;
+        if (flags & 2) {  // the generated source of the first compiled pass
+            *n_compiled = 1;
+            say(gp.src[i]);
+            return SMOQ_OK;
+        }
+        if (!jit_check_adjoint(q, why, (flags & 1) ? &info : nullptr)) {
+            say(why);
+            return SMOQ_ERR_BADINPUT;
+        }
+        report += info;
+        ++*n_compiled;
+    }
+    say((flags & 1) ? report : std::string("ok"));
     return SMOQ_OK;
 }
 

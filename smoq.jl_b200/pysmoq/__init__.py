@@ -951,20 +951,42 @@ def debug_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtype: int =
 
 
 def debug_compile_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtype: int = C64, tile_bits: int = 13,
-                       low_bits: int = 5, verbose: bool = False, buffers: int = 1, packed: bool = False,
-                       groups: int = 2, stage_bits: int = 4):
+                       low_bits: int = 5, verbose: bool = False, buffers: int = 1, groups: int = 2,
+                       rtc: bool = False, source: bool = False):
     """Host-only: plan `ops` for the plan compiler (engine 3) and compile every pass
     kernel with NVRTC (no GPU, nothing loaded).  Returns (status, n_compiled, message);
-    with verbose the message is the compiler's register/spill report."""
+    with verbose the message is the compiler's register/spill report.  rtc: the
+    run-time-coefficient form (a variational forward); source: the message is the
+    generated source of the first pass (nothing compiled)."""
     arr = circuit_to_c_ops(ops)
     th = np.ascontiguousarray(theta if theta is not None else np.zeros(1), dtype=np.float64)
     n = C.c_int()
-    msg = C.create_string_buffer(1 << 16)
-    flags = (1 if verbose else 0) | (2 if buffers == 2 else 0) | (4 if packed else 0) | (8 if groups == 1 else 0) \
-        | (16 if stage_bits == 5 else 0)
+    size = 1 << (22 if source else 16)
+    msg = C.create_string_buffer(size)
+    flags = (1 if verbose else 0) | (2 if buffers == 2 else 0) | (4 if rtc else 0) | (8 if groups == 1 else 0) \
+        | (16 if source else 0)
     st = lib.smoq_debug_compile_plan(N, dtype, tile_bits, low_bits, arr, len(ops), dptr(th), flags, C.byref(n),
-                                     msg, 1 << 16)
+                                     msg, size)
     return st, n.value, msg.value.decode(errors="replace")
+
+
+def debug_compile_adjoint(circuit: "ParameterizedCircuit", theta, tile_bits: int = 13, low_bits: int = 5,
+                          verbose: bool = False, source: bool = False):
+    """Host-only: build the backward program of a variational circuit as
+    energy_and_gradient does (complex64), stage-schedule its passes for the compiled
+    adjoint kernel and compile those kernels with NVRTC (no GPU, nothing loaded).
+    Returns (status, n_passes, n_compiled, message); with verbose the message is the
+    compiler's register/spill report, with source the generated CUDA source of the first
+    compiled pass (nothing compiled)."""
+    arr = circuit_to_c_ops(circuit.operations)
+    th = np.ascontiguousarray(theta, dtype=np.float64)
+    npass, ncomp = C.c_int(), C.c_int()
+    size = 1 << 22
+    msg = C.create_string_buffer(size)
+    st = lib.smoq_debug_compile_adjoint(circuit.N, arr, len(circuit.operations), circuit.n_params,
+                                        dptr(th), tile_bits, low_bits, (1 if verbose else 0) | (2 if source else 0),
+                                        C.byref(npass), C.byref(ncomp), msg, size)
+    return st, npass.value, ncomp.value, msg.value.decode(errors="replace")
 
 
 def jit_available() -> bool:

@@ -20,7 +20,7 @@ C64, C128 = 0, 1
 
 (OPT_TILE_BITS_C64, OPT_TILE_BITS_C128, OPT_LOW_BITS_C64, OPT_LOW_BITS_C128, OPT_USE_GRAPHS, OPT_KERNEL_TIMING,
  OPT_ENGINE, OPT_JIT_BUFFERS) = range(1, 9)
-OPT_JIT_GROUPS, OPT_VQE_RESIDENT, OPT_AUTOTUNE = 10, 12, 13
+OPT_JIT_GROUPS, OPT_VQE_RESIDENT, OPT_AUTOTUNE, OPT_FUSION_DEPTH = 10, 12, 13, 14
 
 
 # operations of smoq_apply_circuit_mcwf beyond the gates (one qubit each)
@@ -93,6 +93,7 @@ _SIGS = {
     "smoq_ctx_counters": [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), _dp, _dp],
     "smoq_ctx_reset_counters": [_vp],
     "smoq_ctx_tune_report": [_vp, C.c_char_p, C.c_int],
+    "smoq_debug_wait_timeout": [_vp, C.c_uint64],
     "smoq_state_create": [_vp, C.c_int, C.c_int, C.c_int, C.POINTER(_vp)],
     "smoq_state_wrap": [_vp, _vp, C.c_int, C.c_int, C.c_int, C.POINTER(_vp)],
     "smoq_state_destroy": [_vp],
@@ -166,6 +167,8 @@ _SIGS = {
     "smoq_qrc_run": [_vp, C.POINTER(SmoqQrcParams), _dp, _dp, C.c_int, C.c_int64, _dp, _dp],
     "smoq_debug_compile_plan": [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, _dp, C.c_int, _ip,
                                 C.c_char_p, C.c_int],
+    "smoq_debug_compile_adjoint": [C.c_int, C.POINTER(SmoqOp), C.c_int, C.c_int, _dp, C.c_int, C.c_int, C.c_int,
+                                   _ip, _ip, C.c_char_p, C.c_int],
     "smoq_debug_plan_sequence": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, _dp,
                                  C.POINTER(SmoqPassInfo), C.c_int, C.POINTER(SmoqFusedOpInfo), C.c_int, _ip, _ip],
     "smoq_energy": [_vp, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, C.c_int, C.POINTER(SmoqPauliTerm),

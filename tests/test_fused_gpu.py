@@ -201,3 +201,37 @@ def test_trotter_full_size_properties(ctx):
         st.close()
         plan.close()
     assert np.max(np.abs(res[S.C64] - res[S.C128])) < 1e-5
+
+
+@pytest.mark.parametrize("depth", [1, 3, 7])
+def test_fusion_depth_cap_keeps_the_state(ctx, depth):
+    """SMOQ_OPT_FUSION_DEPTH splits passes longer than `depth` fused ops into
+    consecutive passes of the same tile: a benchmark circuit (one-shot, engine 0)
+    and a Strang Trotter plan (compiled kernels) still equal the oracle"""
+    N = 16
+    lines = json.load(open(os.path.join(GOLD, "circuits.json")))[str(N)]
+    g_ops, o_ops = circuit_ops(lines[:400])
+    want = O.zero_state(N)
+    O.apply_circuit(want, O.make_ops(o_ops), len(o_ops), np.zeros(1), N)
+    ctx.set_option(S._lib.OPT_FUSION_DEPTH, depth)
+    try:
+        st = S.CuState(ctx, N, S.C128)
+        S.apply_circuit(st, S.ParameterizedCircuit(N, g_ops), np.zeros(1))
+        assert rel(st.download(), want) < 1e-12
+        st.close()
+        h = np.random.default_rng(5).uniform(-1, 1, size=N)
+        arr, n = O.precompute_trotter_gates([(i, i + 1, 1.0, 1.0, 0.5) for i in range(1, N)],
+                                            [(i, 0.0, 0.0, float(h[i - 1])) for i in range(1, N + 1)], 0.025)
+        gl = O.gates_to_list(arr, n)
+        ref = O.zero_state(N, 0b1010101010101010)
+        both = O.make_gates(gl + gl[::-1])
+        for _ in range(3):
+            O.trotter_step(ref, both, 2 * n, N)
+        plan = S.TrotterPlan(ctx, N, [S.FastTrotterGate(i, U) for i, U in gl], order=2, dtype=S.C64)
+        s2 = S.CuState(ctx, N, S.C64, basis=0b1010101010101010)
+        plan.step(s2, 3)
+        assert rel(s2.download().astype(complex), ref) < 1e-5
+        s2.close()
+        plan.close()
+    finally:
+        ctx.set_option(S._lib.OPT_FUSION_DEPTH, 0)

@@ -121,3 +121,17 @@ def test_measure_all_observables_ladder(ctx, L, rails, dtype, tol):
             want += [O.expect_corr(psi, i, j, N, pp) for pp in ("xx", "yy", "zz")]
         assert got.shape == (2, len(want))
         assert np.max(np.abs(got[b] - np.array(want))) < tol
+
+
+def test_bounded_wait_times_out_and_the_context_survives(ctx):
+    """the failure path of the tile kernels' bounded waits: a wait that nothing
+    completes gives up after its limit and the call returns SMOQ_ERR_TIMEOUT with
+    the reason; the next calls on the same context still compute"""
+    from pysmoq import _lib as L
+    assert L.lib.smoq_debug_wait_timeout(ctx.h, 2_000_000) == L.SMOQ_ERR_TIMEOUT
+    assert b"bounded device wait" in L.lib.smoq_last_error(ctx.h)
+    st = S.CuState(ctx, 12, S.C128, basis=0)
+    S.apply_rx_psi(st, 3, 0.8, 12)
+    assert abs(S.expect_local(st, 3, 12, "z") - np.cos(0.8)) < 1e-12
+    assert L.lib.smoq_debug_wait_timeout(ctx.h, 10) == L.SMOQ_ERR_BADINPUT   # limit below 1 us
+    st.close()

@@ -237,3 +237,75 @@ def test_plan_compiler_generates_valid_kernels(built, N, tile_bits):
     spills = [int(m) for m in re.findall(r"(\d+) bytes spill stores", msg)]
     assert len(spills) == n, msg          # one compiler report per kernel
     assert max(spills) <= 64, msg
+
+
+@pytest.mark.parametrize("N", [16, 24])
+def test_run_time_coefficient_forward_kernels(built, N):
+    """the compiled forward passes of a variational circuit with the coefficients
+    passed per launch (host only): they compile without spills beyond a few bytes,
+    and a second parameter set gives the same kernel source"""
+    import pysmoq as S
+    import re
+    rng = np.random.default_rng(N)
+    ops, idx = [], 1
+    for layer in range(6):
+        rot, idx = S.single_qubit_rotation_layer(N, idx, gates=("ry", "rz"))
+        ops += rot + S.entangling_layer(N, "chain", "cz")
+        ops.append(S.gate("rxx", [1 + layer, N - layer], param_idx=idx)); idx += 1
+        ops.append(S.gate("toffoli", [2, 5 + layer, N]))
+    th = [rng.uniform(0, 2 * np.pi, size=idx - 1) for _ in range(2)]
+    st, n, msg = S.debug_compile_plan(N, ops, theta=th[0], rtc=True, verbose=True)
+    if st == 5:
+        pytest.skip("NVRTC not available: " + msg)
+    assert st == 0, msg
+    spills = [int(m) for m in re.findall(r"(\d+) bytes spill stores", msg)]
+    assert n >= 1 and len(spills) == n and max(spills) <= 64, msg
+    srcs = [S.debug_compile_plan(N, ops, theta=t, rtc=True, source=True) for t in th]
+    assert srcs[0][0] == 0 and "Coefs K" in srcs[0][2] and srcs[0][2] == srcs[1][2]
+    lit = [S.debug_compile_plan(N, ops, theta=t, source=True) for t in th]
+    assert "Coefs" not in lit[0][2] and lit[0][2] != lit[1][2]   # literal form: the angles are in the source
+
+
+@pytest.mark.parametrize("N,L,kinds", [(24, 6, ("ry", "rz")), (16, 4, ("rx", "ry", "rz")), (14, 3, "mixed")])
+def test_compiled_adjoint_kernels_compile(built, N, L, kinds):
+    """the compiled adjoint kernels of smoq_energy_grad (host only): every backward pass
+    of tile width 12 of a variational circuit is stage-scheduled and compiles with
+    NVRTC, with at most a few bytes of spills; the angles do not enter the source"""
+    import pysmoq as S
+    import re
+    rng = np.random.default_rng(N)
+    ops, idx = [], 1
+    for layer in range(L):
+        if kinds == "mixed":
+            for q in range(1, N + 1):
+                t = str(rng.choice(["rx", "ry", "rz", "h", "t"]))
+                if t in ("h", "t"):
+                    ops.append(S.gate(t, q))
+                else:
+                    ops.append(S.gate(t, q, param_idx=idx))
+                    idx += 1
+            for q in range(1, N):
+                t = str(rng.choice(["cz", "cnot", "rxx", "ryy", "rzz", "cry"]))
+                if t in ("cz", "cnot"):
+                    ops.append(S.gate(t, [q, q + 1]))
+                else:
+                    ops.append(S.gate(t, [q, 1 + (q + 2 * layer) % N if 1 + (q + 2 * layer) % N != q else q + 1],
+                                      param_idx=idx))
+                    idx += 1
+        else:
+            rot, idx = S.single_qubit_rotation_layer(N, idx, gates=kinds)
+            ops += rot + S.entangling_layer(N, "chain", "cz")
+    circ = S.ParameterizedCircuit(N, ops)
+    theta = rng.uniform(0, 2 * np.pi, size=circ.n_params)
+    st, npass, ncomp, msg = S.debug_compile_adjoint(circ, theta, verbose=True)
+    if st == 5:
+        pytest.skip("NVRTC not available: " + msg)
+    assert st == 0, msg
+    assert npass >= 1 and ncomp == npass, (npass, ncomp)
+    spills = [int(m) for m in re.findall(r"(\d+) bytes spill stores", msg)]
+    assert len(spills) == ncomp and max(spills) <= 64, msg
+    # another parameter set of the same circuit: the same kernel source
+    srcs = [S.debug_compile_adjoint(circ, th, source=True)
+            for th in (theta, rng.uniform(0, 2 * np.pi, size=circ.n_params))]
+    assert srcs[0][0] == 0 and srcs[1][0] == 0
+    assert "smoq_adj_e0" in srcs[0][3] and srcs[0][3] == srcs[1][3]

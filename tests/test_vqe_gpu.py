@@ -241,3 +241,75 @@ def test_jobs_in_one_launch_equal_the_tiled_path(built, dtype, tol):
     arr = O.make_ops(oo)
     fd = O.grad(arr, len(oo), theta, circ.N, raw[4], method="fd", eps=1e-5)
     assert np.max(np.abs(g1[4] - fd)) < (1e-7 if dtype == S.C128 else 1e-4)
+
+
+@pytest.mark.parametrize("N,seed", [(13, 21), (17, 22), (20, 23)])
+def test_compiled_adjoint_matches_shared_memory_adjoint(ctx, N, seed):
+    """complex64 forward and backward passes run as compiled kernels with run-time
+    coefficients (engine auto) or as shared-memory sweeps (engine 0): every
+    parameterised type, fixed 1-3 qubit gates (Toffoli, CCZ: single-op stages)
+    between; both agree, and both agree with the oracle's complex128 gradient; a
+    second parameter set reuses the compiled kernels (their source holds no angle)
+    and still matches"""
+    if not S.jit_available():
+        pytest.skip("NVRTC not available")
+    rng = np.random.default_rng(seed)
+    g = S.gate
+    ops, p = [], 1
+    for _ in range(4 * N):
+        kind = rng.integers(0, 6)
+        q = [int(x) + 1 for x in rng.choice(N, 3, replace=False)]
+        if kind == 0:
+            ops.append(g(str(rng.choice(["rx", "ry", "rz"])), q[0], param_idx=p)); p += 1
+        elif kind == 1:
+            ops.append(g(str(rng.choice(["rxx", "ryy", "rzz", "cry"])), q[:2], param_idx=p)); p += 1
+        elif kind == 2:
+            ops.append(g(str(rng.choice(["h", "s", "t", "x"])), q[0]))
+        elif kind == 3:
+            ops.append(g(str(rng.choice(["cnot", "cz"])), q[:2]))
+        elif kind == 4:
+            ops.append(g(str(rng.choice(["toffoli", "ccz"])), q))
+        else:
+            ops.append(g("ry", q[0], param_idx=p))
+            ops.append(g("rzz", q[:2], param_idx=p + 1)); p += 2
+    circ = S.ParameterizedCircuit(N, ops)
+    terms = [(0.9, {1: "X", N: "Y"}), (-0.6, {3: "Z", N - 1: "Z"}), (0.5, {N // 2: "Y"}), (-0.4, {5: "Z"})]
+    H = S.PauliSum(terms)
+    oo = oracle_ops(circ)
+    arr = O.make_ops(oo)
+    for k in range(2):
+        theta = rng.uniform(-3, 3, size=circ.n_params)
+        ctx.set_option(S._lib.OPT_ENGINE, -1)
+        ctx.reset_counters()
+        e_c, g_c = S.energy_and_gradient(ctx, circ, H, theta, dtype=S.C64)
+        ctx.set_option(S._lib.OPT_ENGINE, 0)
+        try:
+            e_s, g_s = S.energy_and_gradient(ctx, circ, H, theta, dtype=S.C64)
+        finally:
+            ctx.set_option(S._lib.OPT_ENGINE, -1)
+        e_ref = O.energy(arr, len(oo), theta, N, terms)
+        fd = O.grad(arr, len(oo), theta, N, terms, method="fd", eps=1e-5)
+        print(f"N={N} set {k}: compiled vs shared-memory adjoint {np.max(np.abs(g_c[0] - g_s[0])):.2e}, "
+              f"vs oracle {np.max(np.abs(g_c[0] - fd)):.2e}")
+        assert abs(e_c[0] - e_s[0]) < 2e-6      # (complex64 forwards of different fusion)
+        assert np.max(np.abs(g_c[0] - g_s[0])) < 2e-5
+        assert abs(e_c[0] - e_ref) < 1e-5 and np.max(np.abs(g_c[0] - fd)) < 1e-4
+
+
+def test_compiled_adjoint_batch_and_special_angles(ctx):
+    """a batch of complex64 parameter sets through one compiled kernel per pass
+    (each set equals its own call), and angles that make coefficients 0 or +-1
+    (theta = 0, pi: another kernel source) against the complex128 gradient"""
+    N, L = 15, 3
+    circ, _ = hea(N, L)
+    H = S.PauliSum(tfim_terms(N))
+    rng = np.random.default_rng(9)
+    thetas = rng.uniform(0, 2 * np.pi, size=(3, circ.n_params))
+    thetas[2, ::3] = 0.0
+    thetas[2, 1::5] = np.pi
+    e, g = S.energy_and_gradient(ctx, circ, H, thetas, dtype=S.C64)
+    for b in range(3):
+        e1, g1 = S.energy_and_gradient(ctx, circ, H, thetas[b], dtype=S.C64)
+        assert abs(e[b] - e1[0]) < 1e-9 and np.max(np.abs(g[b] - g1[0])) < 1e-9
+        e2, g2 = S.energy_and_gradient(ctx, circ, H, thetas[b], dtype=S.C128)
+        assert abs(e[b] - e2[0]) < 1e-5 and np.max(np.abs(g[b] - g2[0])) < 1e-4
