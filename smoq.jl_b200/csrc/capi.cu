@@ -450,6 +450,8 @@ smoq_status smoq_ctx_create(int device, smoq_ctx** out) {
 
 smoq_status smoq_ctx_destroy(smoq_ctx* ctx) {
     if (!ctx) return SMOQ_ERR_BADINPUT;
+    for (smoq_ctx* w : ctx->workers) smoq_ctx_destroy(w);
+    ctx->workers.clear();
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->d_scratch) cudaFree(ctx->d_scratch);
@@ -1501,6 +1503,26 @@ smoq_status smoq_internal_plan_step(smoq_plan* plan, std::vector<GateIR>& out, i
 }
 
 // plan + upload a gate program for `st` (no launch); the handle owns it
+// the passes of a one-use gate program (host only: reads the context's options,
+// touches nothing else, so a planning thread may call it); throws on bad input.
+// variational: a variational circuit's complex64 forward, compiled kernels with
+// run-time coefficients
+std::vector<Pass> smoq_internal_plan(smoq_ctx* ctx, int N, int dtype, const std::vector<GateIR>& gates,
+                                     bool variational) {
+    const bool rtc = variational && dtype == SMOQ_C64 && ctx->engine < 0 && jit_available();
+    return plan_for(rtc ? 3 : engine_for(ctx, false, dtype), gates, N, dtype, tile_bits(ctx, dtype),
+                    low_bits(ctx, dtype), -1, 0, rtc);
+}
+
+// upload planned passes (kernels resolved, ops on the device); the handle owns them
+smoq_status smoq_internal_prepare_planned(smoq_ctx* ctx, std::vector<Pass>&& passes, void** handle) {
+    std::unique_ptr<DevProgram> P(new DevProgram());
+    P->passes = std::move(passes);
+    if (smoq_status s = upload_program(ctx, *P)) return s;
+    *handle = P.release();
+    return SMOQ_OK;
+}
+
 smoq_status smoq_internal_prepare(smoq_ctx* ctx, smoq_state* st, const std::vector<GateIR>& gates,
                                   int epilogue_special, bool reusable, void** handle, bool variational) {
     std::unique_ptr<DevProgram> P(new DevProgram());

@@ -237,8 +237,8 @@ struct smoq_ctx {
     int low_bits_c64 = 5;
     int low_bits_c128 = 4;
     int use_graphs = 1;
-    int engine = -1;                   // fused passes: -1 = auto, 0 = shared-memory sweeps, 1 = register
-                                       // tiles, 2 = stage sweeps, 3 = compiled pass kernels
+    int engine = -1;                   // fused passes: -1 = auto, 0 = shared-memory sweeps,
+                                       // 2 = stage sweeps, 3 = compiled pass kernels
     int st_occ[2][2][2] = {};          // CTAs per SM of the stage kernel [dtype][epilogue][GP-1]
     int kernel_timing = 0;             // bracket tile passes with events
     int jit_buffers = 1;               // compiled pass kernels: tile buffers per CTA (1 or 2)
@@ -253,6 +253,7 @@ struct smoq_ctx {
     double tile_bytes = 0;             // algorithmic bytes of the timed tile passes
     int num_sms = 148;
     int tile_occ[2][2][16] = {};       // CTAs per SM of tile_pass_kernel [dtype][epilogue][T]
+    std::vector<smoq_ctx*> workers;    // worker contexts of the many-circuit VQE call
 };
 
 struct smoq_state {

@@ -27,8 +27,10 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <future>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -613,6 +615,9 @@ smoq_status smoq_internal_ops_to_ir(int N, const smoq_op* ops, int n, const doub
 smoq_status smoq_internal_prepare(smoq_ctx* ctx, smoq_state* st, const std::vector<GateIR>& gates,
                                   int epilogue_special, bool reusable, void** prog_handle,
                                   bool variational = false);
+std::vector<Pass> smoq_internal_plan(smoq_ctx* ctx, int N, int dtype, const std::vector<GateIR>& gates,
+                                     bool variational);
+smoq_status smoq_internal_prepare_planned(smoq_ctx* ctx, std::vector<Pass>&& passes, void** handle);
 smoq_status smoq_internal_rerun(smoq_ctx* ctx, smoq_state* st, void* prog_handle, const Epilogue* ep);
 void smoq_internal_free_prog(void* prog_handle);
 int smoq_internal_tile_bits(smoq_ctx* ctx, int dtype);
@@ -793,13 +798,19 @@ static smoq_status check_vqe_args(smoq_ctx* ctx, int N, smoq_dtype dtype, const 
 // forward state into w.phi, lambda = H phi into w.lam; returns
 // E = <phi|H|phi> / <phi|phi> and the FP64 <phi|phi> it divided by (a unitary
 // circuit keeps the norm at 1 in exact arithmetic; dividing removes the
-// complex64 norm drift of a deep circuit from the energy at first order)
+// complex64 norm drift of a deep circuit from the energy at first order).
+// compiled: the forward runs compiled kernels with run-time coefficients (one
+// compile per circuit structure, for repeated calls on one circuit); fwd: the
+// forward passes when a planning thread made them already (moved from)
 static smoq_status forward_and_h(smoq_ctx* ctx, Work& w, const std::vector<GateIR>& ir, const std::vector<HamTerm>& ht,
-                                 HamTerm* d_terms, double* d_epart, int eblocks, double* E, double* nrm2) {
+                                 HamTerm* d_terms, double* d_epart, int eblocks, double* E, double* nrm2,
+                                 bool compiled, std::vector<Pass>* fwd = nullptr) {
     VCK(launch_set_basis(&w.phi, 0));
     if (!ir.empty()) {
         void* h = nullptr;
-        if (smoq_status s = smoq_internal_prepare(ctx, &w.phi, ir, -1, false, &h, true)) return s;
+        if (smoq_status s = fwd ? smoq_internal_prepare_planned(ctx, std::move(*fwd), &h)
+                                : smoq_internal_prepare(ctx, &w.phi, ir, -1, false, &h, compiled))
+            return s;
         std::unique_ptr<void, void (*)(void*)> hold(h, smoq_internal_free_prog);
         if (smoq_status s = smoq_internal_rerun(ctx, &w.phi, h, nullptr)) return s;
         VCK(cudaStreamSynchronize(ctx->stream));  // the program is freed at scope exit
@@ -855,6 +866,8 @@ static bool build_backward(const std::vector<GateIR>& ir, const smoq_op* ops, in
 // state, so the many-circuit call prepares several circuits on host threads.
 struct GradPlan {
     std::vector<GateIR> ir;
+    std::vector<Pass> fwd;       // the forward passes, when planned ahead (fwd_ready)
+    bool fwd_ready = false;
     std::vector<Pass> passes;    // the backward passes, measurements fused
     std::vector<Pass> staged;    // per pass: its stage schedule when the compiled adjoint
                                  // kernel runs it (staged[i].staged false: the shared-memory kernel)
@@ -869,11 +882,22 @@ struct GradPlan {
 // kernel (4-bit register stages on both states, coefficients read at run time, so
 // the NVRTC compile of the first parameter set serves all later ones); with jit = 1
 // they are compiled here, on the planning thread, and loaded by the caller
+// fwd_ctx: also plan the forward (on fwd_ctx's options; a variational forward with jit 1)
 static void plan_gradient(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops, int n,
-                          const double* th, bool grad, GradPlan& gp, int jit = 0) {
+                          const double* th, bool grad, GradPlan& gp, int jit = 0, smoq_ctx* fwd_ctx = nullptr) {
     if ((gp.status = smoq_internal_ops_to_ir(N, ops, n, th, gp.ir))) {
         gp.error = "bad op list";
         return;
+    }
+    if (fwd_ctx && !gp.ir.empty()) {
+        try {
+            gp.fwd = smoq_internal_plan(fwd_ctx, N, dtype, gp.ir, jit == 1);
+            gp.fwd_ready = true;
+        } catch (const std::exception& ex) {
+            gp.status = SMOQ_ERR_BADINPUT;
+            gp.error = ex.what();
+            return;
+        }
     }
     if (!grad) return;
     std::vector<GateIR> back;
@@ -963,32 +987,36 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
     const int tb = smoq_internal_tile_bits(ctx, dtype), lbits = smoq_internal_low_bits(ctx, dtype);
     const int jit = (ctx->engine == 3 || (ctx->engine < 0 && jit_available())) ? 1 : 0;
     auto theta_of = [&](int b) { return theta ? theta + (size_t)b * n_params : nullptr; };
-    std::unique_ptr<GradPlan> cur(new GradPlan), nxt;
-    std::thread ahead;
-    struct Joiner {
-        std::thread& t;
-        ~Joiner() {
-            if (t.joinable()) t.join();
-        }
-    } joiner{ahead};
     const bool use_pre = pre && batch == 1;
-    if (!use_pre) plan_gradient(N, dtype, tb, lbits, ops, n, theta_of(0), grads != nullptr, *cur, jit);
+    // Parameter sets are planned (forward and backward) on host threads, up to
+    // `window` sets ahead of the one the GPU runs; each plan holds one set's gate IR
+    // and pass lists and is freed once its set ran
+    const int window = std::max(1, std::min(batch, (int)std::min<unsigned>(8, std::thread::hardware_concurrency())));
+    std::vector<std::unique_ptr<GradPlan>> plans(batch);
+    std::vector<std::future<void>> planned(batch);  // (declared after `plans`: joined first)
+    const bool want_grad = grads != nullptr;
+    auto start = [&](int b) {
+        plans[b].reset(new GradPlan);
+        GradPlan* np = plans[b].get();
+        const double* th = theta_of(b);
+        planned[b] = std::async(std::launch::async,
+                                [=]() { plan_gradient(N, dtype, tb, lbits, ops, n, th, want_grad, *np, jit, ctx); });
+    };
+    // set 0 alone first: a new circuit structure is compiled once, by its planning
+    if (!use_pre) start(0);
     for (int b = 0; b < batch; ++b) {
-        if (b > 0) {
-            ahead.join();
-            cur.swap(nxt);
+        if (!use_pre) {
+            planned[b].get();
+            if (b > 0) plans[b - 1].reset();
+            for (int k = b == 0 ? 1 : b + window; k <= b + window && k < batch; ++k) start(k);
         }
-        if (b + 1 < batch) {
-            nxt.reset(new GradPlan);
-            GradPlan* np = nxt.get();
-            const double* th1 = theta_of(b + 1);
-            const bool want_grad = grads != nullptr;
-            ahead = std::thread([=]() { plan_gradient(N, dtype, tb, lbits, ops, n, th1, want_grad, *np, jit); });
-        }
-        GradPlan& gp = use_pre ? *pre : *cur;
+        GradPlan& gp = use_pre ? *pre : *plans[b];
         if (gp.status) return smoq_internal_fail(ctx, gp.status, gp.error.c_str());
         double E = 0, nrm2 = 1;
-        if (smoq_status s = forward_and_h(ctx, w, gp.ir, ht, d_terms, d_epart, eblocks, &E, &nrm2)) return s;
+        // (the many-circuit call keeps its distinct circuits off the compiler)
+        if (smoq_status s = forward_and_h(ctx, w, gp.ir, ht, d_terms, d_epart, eblocks, &E, &nrm2, jit && !use_pre,
+                                          gp.fwd_ready ? &gp.fwd : nullptr))
+            return s;
         energies[b] = E;
         if (!grads) continue;
         double* g = grads + (size_t)b * n_params;
@@ -1314,83 +1342,97 @@ static smoq_status run_resident(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vqe_
 }
 
 // ---------------------------------------------------------------- many circuits
-// Independent VQE jobs (each its own circuit, size and Hamiltonian), run in
-// submission order on the context's stream; each job's passes fill the GPU by
-// themselves from N of about 16 up (smaller states leave most SMs idle).
+// Worker contexts of a context (own stream and error word, the parent's options):
+// the many-circuit call runs its larger circuits on them from host threads, so the
+// small grids of several circuits share the GPU
+static smoq_status job_workers(smoq_ctx* ctx, size_t k) {
+    while (ctx->workers.size() < k) {
+        smoq_ctx* w = nullptr;
+        if (smoq_status s = smoq_ctx_create(ctx->device, &w)) return s;
+        ctx->workers.push_back(w);
+    }
+    for (smoq_ctx* w : ctx->workers) {
+        w->tile_bits_c64 = ctx->tile_bits_c64;
+        w->tile_bits_c128 = ctx->tile_bits_c128;
+        w->low_bits_c64 = ctx->low_bits_c64;
+        w->low_bits_c128 = ctx->low_bits_c128;
+        w->engine = ctx->engine;
+        w->jit_buffers = ctx->jit_buffers;
+        w->jit_groups = ctx->jit_groups;
+        w->autotune = ctx->autotune;
+        w->fusion_depth = ctx->fusion_depth;
+        w->kernel_timing = 0;
+    }
+    return SMOQ_OK;
+}
+
+// Independent VQE jobs (each its own circuit, size and Hamiltonian).  Circuits
+// whose two states fit one CTA's shared memory run in one launch off a device
+// work queue (run_resident); the others are taken off a host queue by up to 8
+// worker threads, each planning a circuit and running it on its own worker
+// context's stream, while the calling thread runs the resident launch.
 extern "C" smoq_status smoq_energy_grad_jobs(smoq_ctx* ctx, smoq_dtype dtype, const smoq_vqe_job* jobs, int njobs) {
     if (!ctx) return SMOQ_ERR_BADINPUT;
     if (njobs < 0 || (njobs > 0 && !jobs)) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "bad job list");
     for (int j = 0; j < njobs; ++j)
         if (!jobs[j].energy) return smoq_internal_fail(ctx, SMOQ_ERR_BADINPUT, "job without energy output");
-    // circuits whose two states fit one CTA's shared memory: all in one launch
-    std::vector<int> small;
-    for (int j = 0; j < njobs; ++j)
-        if (ctx->vqe_resident && jobs[j].N >= 1 && jobs[j].N <= (dtype == SMOQ_C64 ? kResMaxN64 : kResMaxN128))
-            small.push_back(j);
-    if (!small.empty())
-        if (smoq_status s = run_resident(ctx, dtype, jobs, small)) return s;
-    // the others: validated here, prepared on host threads a chunk at a time (the
-    // prepared gate IR takes 4 KB a gate), run on the GPU in submission order
-    std::vector<int> large;
-    size_t next_small = 0;
+    std::vector<int> small, large;
     for (int j = 0; j < njobs; ++j) {
-        if (next_small < small.size() && small[next_small] == j) {
-            ++next_small;
+        const smoq_vqe_job& J = jobs[j];
+        if (ctx->vqe_resident && J.N >= 1 && J.N <= (dtype == SMOQ_C64 ? kResMaxN64 : kResMaxN128)) {
+            small.push_back(j);
             continue;
         }
-        const smoq_vqe_job& J = jobs[j];
         if (smoq_status s = check_vqe_args(ctx, J.N, dtype, J.ops, J.n, J.n_params, J.H, J.nterms, 1, J.theta)) {
             const std::string why = "job " + std::to_string(j) + ": " + smoq_last_error(ctx);
             return smoq_internal_fail(ctx, s, why.c_str());
         }
         large.push_back(j);
     }
+    const size_t nworkers =
+        std::min(large.size(), std::max<size_t>(1, std::min<size_t>(8, std::thread::hardware_concurrency() / 2)));
+    if (nworkers > 0)
+        if (smoq_status s = job_workers(ctx, nworkers)) return smoq_internal_fail(ctx, s, "worker context");
     const int tb = smoq_internal_tile_bits(ctx, dtype), lb = smoq_internal_low_bits(ctx, dtype);
-    // (half the host threads, at most 8: the planning is memory-bound on 4 KB gates)
-    const size_t nthreads = std::max<size_t>(1, std::min<size_t>(8, std::thread::hardware_concurrency() / 2));
-    const size_t chunk = 4 * nthreads;
-    // plans of the chunk of large circuits starting at c0, on host threads (no CUDA calls)
-    auto plan_chunk = [&, dtype](size_t c0, std::vector<GradPlan>& plans) {
-        const size_t nc = std::min(chunk, large.size() - c0);
-        plans.assign(nc, GradPlan());
-        std::atomic<size_t> next(0);
-        auto work = [&]() {
-            for (size_t i; (i = next++) < nc;) {
-                const smoq_vqe_job& J = jobs[large[c0 + i]];
-                plan_gradient(J.N, dtype, tb, lb, J.ops, J.n, J.theta, J.grad != nullptr, plans[i]);
-            }
-        };
-        std::vector<std::thread> pool;
-        for (size_t t = 1; t < std::min(nthreads, nc); ++t) pool.emplace_back(work);
-        work();
-        for (std::thread& t : pool) t.join();
-    };
-    // the next chunk is planned while the GPU runs this one
-    std::vector<GradPlan> plans, next_plans;
-    std::thread ahead;
-    struct Joiner {
-        std::thread& t;
-        ~Joiner() {
-            if (t.joinable()) t.join();
+    std::atomic<size_t> next(0);
+    std::atomic<bool> failed(false);
+    std::mutex mu;
+    smoq_status first = SMOQ_OK;
+    std::string why;
+    std::vector<long long> launches0(nworkers);
+    for (size_t w = 0; w < nworkers; ++w) launches0[w] = ctx->workers[w]->launches;
+    auto work = [&](size_t w) {
+        smoq_ctx* wc = ctx->workers[w];
+        if (cudaSetDevice(ctx->device) != cudaSuccess) {
+            std::lock_guard<std::mutex> lk(mu);
+            if (first == SMOQ_OK) first = SMOQ_ERR_CUDA, why = "worker thread: cudaSetDevice failed";
+            failed = true;
+            return;
         }
-    } joiner{ahead};
-    if (!large.empty()) plan_chunk(0, plans);
-    for (size_t c0 = 0; c0 < large.size(); c0 += chunk) {
-        const size_t nc = plans.size();
-        if (c0 + chunk < large.size()) ahead = std::thread([&, c0]() { plan_chunk(c0 + chunk, next_plans); });
-        for (size_t i = 0; i < nc; ++i) {
-            const int j = large[c0 + i];
-            const smoq_vqe_job& J = jobs[j];
-            const smoq_status s = vqe_run(ctx, J.N, dtype, J.ops, J.n, J.n_params, J.H, J.nterms, 1, J.theta, J.energy,
-                                          J.grad, &plans[i]);
+        for (size_t i; !failed && (i = next++) < large.size();) {
+            const smoq_vqe_job& J = jobs[large[i]];
+            GradPlan gp;  // (host planning overlaps the other workers' GPU work)
+            plan_gradient(J.N, dtype, tb, lb, J.ops, J.n, J.theta, J.grad != nullptr, gp, 0, wc);
+            const smoq_status s =
+                vqe_run(wc, J.N, dtype, J.ops, J.n, J.n_params, J.H, J.nterms, 1, J.theta, J.energy, J.grad, &gp);
             if (s != SMOQ_OK) {
-                const std::string why = "job " + std::to_string(j) + ": " + smoq_last_error(ctx);
-                return smoq_internal_fail(ctx, s, why.c_str());
+                std::lock_guard<std::mutex> lk(mu);
+                if (first == SMOQ_OK) {
+                    first = s;
+                    why = "job " + std::to_string(large[i]) + ": " + smoq_last_error(wc);
+                }
+                failed = true;
             }
         }
-        if (ahead.joinable()) ahead.join();
-        plans.swap(next_plans);
-    }
+    };
+    std::vector<std::thread> pool;
+    for (size_t w = 0; w < nworkers; ++w) pool.emplace_back(work, w);
+    smoq_status rs = SMOQ_OK;
+    if (!small.empty()) rs = run_resident(ctx, dtype, jobs, small);
+    for (std::thread& t : pool) t.join();
+    for (size_t w = 0; w < nworkers; ++w) ctx->launches += ctx->workers[w]->launches - launches0[w];
+    if (rs != SMOQ_OK) return rs;
+    if (first != SMOQ_OK) return smoq_internal_fail(ctx, first, why.c_str());
     return SMOQ_OK;
 }
 

@@ -313,3 +313,27 @@ def test_compiled_adjoint_batch_and_special_angles(ctx):
         assert abs(e[b] - e1[0]) < 1e-9 and np.max(np.abs(g[b] - g1[0])) < 1e-9
         e2, g2 = S.energy_and_gradient(ctx, circ, H, thetas[b], dtype=S.C128)
         assert abs(e[b] - e2[0]) < 1e-5 and np.max(np.abs(g[b] - g2[0])) < 1e-4
+
+
+def test_many_circuits_on_worker_streams(ctx):
+    """larger circuits of the many-circuit call run on worker contexts from host
+    threads, concurrently with the resident launch of the small ones: every job equals
+    its own single-circuit call (complex128), and a bad job is reported by its index"""
+    rng = np.random.default_rng(31)
+    jobs = []
+    for j in range(14):
+        N = int(rng.integers(14, 17)) if j % 2 == 0 else int(rng.integers(6, 12))
+        circ, theta = hea(N, int(rng.integers(1, 4)), seed=200 + j)
+        jobs.append((circ, S.PauliSum(tfim_terms(N)), theta))
+    e, g = S.energy_and_gradient_jobs(ctx, jobs, dtype=S.C128)
+    for j, (circ, H, theta) in enumerate(jobs):
+        e1, g1 = S.energy_and_gradient(ctx, circ, H, theta, dtype=S.C128)
+        assert abs(e[j] - e1[0]) < 1e-11 and np.max(np.abs(g[j] - g1[0])) < 1e-10, j
+    bad = list(jobs)
+    circ, H, theta = bad[4]
+    bad[4] = (S.ParameterizedCircuit(circ.N, circ.operations + [S.gate("ry", 1, param_idx=circ.n_params + 1)],
+                                     n_params=circ.n_params), H, theta)
+    with pytest.raises(S.SmoqError, match="job 4"):
+        S.energy_and_gradient_jobs(ctx, bad, dtype=S.C128)
+    e2, _ = S.energy_and_gradient_jobs(ctx, jobs, dtype=S.C128)   # the context still works
+    assert np.max(np.abs(e2 - e)) < 1e-12
