@@ -86,7 +86,8 @@ enum {
                                      options' settings */
     SMOQ_OPT_FUSION_DEPTH = 14    /* No counterpart in the reference.  Max fused ops per pass: a longer
                                      pass is split into consecutive passes of the same tile (0 =
-                                     default, as many as fit) */
+                                     default, as many as fit); applies to gate sequences, plans and
+                                     the forward and backward passes of smoq_energy_grad */
 };
 smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long value);
 /* launches: kernels launched by this context; tile_passes/tile_ms/tile_bytes:

@@ -78,7 +78,7 @@ static smoq_status sync_check(smoq_ctx* ctx) {
     int32_t h = 0;
     CK(ctx, cudaMemcpy(&h, ctx->d_err, sizeof(h), cudaMemcpyDeviceToHost));
     if (h != 0) {
-        CK(ctx, cudaMemset(ctx->d_err, 0, sizeof(int32_t)));
+        CK(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(int32_t), ctx->stream));
         if (h == DEVERR_TIMEOUT) return fail(ctx, SMOQ_ERR_TIMEOUT, "a bounded device wait ran out");
         if ((h & 255) == DEVERR_BOUNDS)
             return fail(ctx, SMOQ_ERR_CUDA, "device bounds check failed at site " + std::to_string(h >> 8));
@@ -135,8 +135,10 @@ static std::vector<Pass> plan_for(int engine, const std::vector<GateIR>& ir, int
     if (engine == 2 || engine == 3)
         for (Pass& p : pl)
             if (p.g.T == 12 || (p.g.T == 13 && dtype == SMOQ_C64)) {
-                schedule_stages(p, dtype == SMOQ_C64 ? 8 : 16);
-                p.want_jit = engine == 3 && p.staged && dtype == SMOQ_C64;
+                // literal compiled kernels: rotations split into diagonals the kernel folds
+                const bool jit = engine == 3 && dtype == SMOQ_C64;
+                schedule_stages(p, dtype == SMOQ_C64 ? 8 : 16, false, jit && !rtc);
+                p.want_jit = jit && p.staged;
                 if (p.want_jit && rtc) {
                     p.rtc = true;
                     jit_rtc_block(p, p.coefs);
@@ -188,7 +190,9 @@ static smoq_status upload_program(smoq_ctx* ctx, DevProgram& P) {
     P.nops = all.size();
     if (all.empty()) return SMOQ_OK;
     CK(ctx, cudaMalloc(&P.d_ops, all.size() * sizeof(DevOp)));
-    CK(ctx, cudaMemcpy(P.d_ops, all.data(), all.size() * sizeof(DevOp), cudaMemcpyHostToDevice));
+    // on the context's (non-blocking) stream: a cudaMemcpy from pageable memory may
+    // return before its DMA lands, and nothing would order it before the passes
+    CK(ctx, cudaMemcpyAsync(P.d_ops, all.data(), all.size() * sizeof(DevOp), cudaMemcpyHostToDevice, ctx->stream));
     return SMOQ_OK;
 }
 
@@ -373,7 +377,7 @@ static smoq_status autotune_program(smoq_ctx* ctx, DevProgram& P, int N) {
     int32_t herr = 0;
     CK(ctx, cudaMemcpy(&herr, ctx->d_err, sizeof(herr), cudaMemcpyDeviceToHost));
     if (herr) {
-        CK(ctx, cudaMemset(ctx->d_err, 0, sizeof(int32_t)));
+        CK(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(int32_t), ctx->stream));
         return fail(ctx, SMOQ_ERR_TIMEOUT, "autotune: a bounded device wait ran out");
     }
     ctx->tune_report += rep.str();
@@ -437,7 +441,9 @@ smoq_status smoq_ctx_create(int device, smoq_ctx** out) {
     ctx->num_sms = prop.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (cudaMalloc(&ctx->d_err, sizeof(int32_t)) != cudaSuccess) return SMOQ_ERR_OOM;
-    if (cudaMemset(ctx->d_err, 0, sizeof(int32_t)) != cudaSuccess) return SMOQ_ERR_CUDA;
+    if (cudaMemsetAsync(ctx->d_err, 0, sizeof(int32_t), ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return SMOQ_ERR_CUDA;
     if (tile_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (stage_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
     if (vqe_kernels_init(ctx.get()) != cudaSuccess) return SMOQ_ERR_CUDA;
@@ -1511,8 +1517,10 @@ std::vector<Pass> smoq_internal_plan(smoq_ctx* ctx, int N, int dtype, const std:
                                      bool variational) {
     const bool rtc = variational && dtype == SMOQ_C64 && ctx->engine < 0 && jit_available();
     return plan_for(rtc ? 3 : engine_for(ctx, false, dtype), gates, N, dtype, tile_bits(ctx, dtype),
-                    low_bits(ctx, dtype), -1, 0, rtc);
+                    low_bits(ctx, dtype), -1, ctx->fusion_depth, rtc);
 }
+
+void smoq_internal_cap_fusion_depth(std::vector<Pass>& pl, int cap) { cap_fusion_depth(pl, cap); }
 
 // upload planned passes (kernels resolved, ops on the device); the handle owns them
 smoq_status smoq_internal_prepare_planned(smoq_ctx* ctx, std::vector<Pass>&& passes, void** handle) {

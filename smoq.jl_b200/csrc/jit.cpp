@@ -29,6 +29,7 @@
 #include <set>
 #include <thread>
 #include <cmath>
+#include <complex>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -346,7 +347,52 @@ struct Gen {
         }
         if (rotated) unrotate(rl);
         bool scal = false;
-        for (int m : members) scal |= member(m, S, gstep, scal);
+        // Literal diagonals whose qubits are stage bits fold into one pending phase per
+        // stage pattern (computed here in FP64); it commutes with every diagonal member
+        // and with matrix members on other stage bits, and is applied before a matrix
+        // member on its bits and at the stage's end.  (Run-time coefficients: no folding.)
+        std::vector<std::complex<double>> pend(R, 1.0);
+        int psup = 0;  // stage positions the pending phase depends on
+        auto flush = [&]() {
+            if (!psup) return;
+            for (int i = 0; i < nreg; ++i) {
+                const std::complex<double> z = pend[i & (R - 1)];
+                if (z == std::complex<double>(1.0, 0.0)) continue;
+                std::string re, im;
+                cmac_terms({{CplxF{(float)z.real(), (float)z.imag()}, v(i)}}, re, im);
+                o << "        " << v(i) << " = cf{" << re << ", " << im << "};\n";
+            }
+            std::fill(pend.begin(), pend.end(), std::complex<double>(1.0, 0.0));
+            psup = 0;
+        };
+        auto stage_pos = [&](int lb) {
+            for (int q = 0; q < KB; ++q)
+                if (S[q] == lb) return q;
+            return -1;
+        };
+        for (int m : members) {
+            const DevOp& op = p.ops[m];
+            int pm = 0;
+            bool on_stage = op.nq >= 1;
+            for (int t = 0; t < op.nq; ++t) {
+                const int q = op.lb[t] >= 0 ? stage_pos(op.lb[t]) : -1;
+                if (q < 0) on_stage = false;
+                else pm |= 1 << q;
+            }
+            if (!p.rtc && op.kind == OPK_DIAG && on_stage) {
+                for (int r = 0; r < R; ++r) {
+                    int mi = 0;
+                    for (int t = 0; t < op.nq; ++t) mi |= ((r >> stage_pos(op.lb[t])) & 1) << t;
+                    pend[r] *= std::complex<double>(op.cd[mi].x, op.cd[mi].y);
+                }
+                psup |= pm;
+                continue;
+            }
+            const bool diagonal = op.kind == OPK_DIAG || op.kind == OPK_STATESCALE || op.kind == OPK_REALTAB;
+            if (!diagonal && (pm & psup)) flush();
+            scal |= member(m, S, gstep, scal);
+        }
+        flush();
         if (scal)
             for (int i = 0; i < nreg; ++i) o << "        " << v(i) << " = cmul(" << scn << ", " << v(i) << ");\n";
         if (rotated) unrotate(rl);  // conditional swaps are involutions

@@ -553,6 +553,112 @@ static void swap_qubit_roles(DevOp& op) {
 }
 
 // ----------------------------------------------------------------------------
+// Rotation splitting for the compiled pass kernels.  A unitary 2x2 block
+// [[p, q], [r, t]] equals diag(1, l2) . [[c, -is], [-is, c]] . diag(r1, r2) with
+// c = |p|, s = |q|, r1 = p / c, r2 = i q / s, l2 = t / (c r2) (unitarity gives the
+// fourth entry).  The middle factor has one real and one imaginary coefficient per
+// row: half the FP32 work of a general complex block.  The two diagonal factors sit
+// on the op's own qubits, which the stage schedule keeps on stage bits, so the
+// compiled kernel folds them with the stage's other diagonals into one literal
+// phase per register.
+namespace {
+struct BlockSplit {
+    cd r1, r2, l2;
+    double c, s;
+};
+// false: the block is not reproduced to 1e-12 (not unitary): keep the op
+bool split_block(cd p, cd q, cd r, cd t, BlockSplit& o) {
+    const cd I(0.0, 1.0);
+    const double c = std::abs(p), s = std::abs(q);
+    if (s < 1e-13) o = BlockSplit{p, t, 1.0, 1.0, 0.0};               // diagonal block
+    else if (c < 1e-13) o = BlockSplit{1.0, I * q, I * r, 0.0, 1.0};  // anti-diagonal block
+    else {
+        o.c = c;
+        o.s = s;
+        o.r1 = p / c;
+        o.r2 = I * q / s;
+        o.l2 = t / (c * o.r2);
+    }
+    const cd P = o.c * o.r1, Q = -I * o.s * o.r2, R = -I * o.s * o.l2 * o.r1, T = o.c * o.l2 * o.r2;
+    return std::abs(P - p) + std::abs(Q - q) + std::abs(R - r) + std::abs(T - t) < 1e-12;
+}
+
+bool genuine(const BlockSplit& b) { return b.c > 1e-13 && b.s > 1e-13; }
+
+DevOp diag_of(const DevOp& like, const cd* v, int n) {
+    DevOp d = like;
+    d.kind = OPK_DIAG;
+    d.flags = DIAG_STAGED;
+    for (int k = 0; k < 16; ++k) {
+        d.cd[k] = make_double2(0.0, 0.0);
+        d.cf[k] = make_float2(0.f, 0.f);
+    }
+    for (int k = 0; k < n; ++k) {
+        d.cd[k] = make_double2(v[k].real(), v[k].imag());
+        d.cf[k] = make_float2((float)v[k].real(), (float)v[k].imag());
+    }
+    return d;
+}
+
+bool is_one(cd z) { return std::abs(z - cd(1.0, 0.0)) < 1e-15; }
+
+// DENSE1 / PARITY2 ops with a genuine complex rotation become R-diagonal, rotation,
+// L-diagonal (the L-diagonal left out when it is the identity)
+std::vector<DevOp> split_rotations(std::vector<DevOp> in) {
+    const cd I(0.0, 1.0);
+    std::vector<DevOp> out;
+    out.reserve(in.size() * 2);
+    for (const DevOp& op : in) {
+        auto c = [&](int k) { return cd(op.cd[k].x, op.cd[k].y); };
+        bool real = true;
+        for (int k = 0; k < 8; ++k) real &= op.cd[k].y == 0.0;
+        if (op.kind == OPK_DENSE1 && !(op.flags & OPF_REAL) && !real) {
+            BlockSplit b;
+            if (split_block(c(0), c(1), c(2), c(3), b) && genuine(b)) {
+                const cd rd[2] = {b.r1, b.r2}, ld[2] = {1.0, b.l2};
+                out.push_back(diag_of(op, rd, 2));
+                DevOp m = op;
+                const cd v[4] = {b.c, -I * b.s, -I * b.s, b.c};
+                for (int k = 0; k < 4; ++k) {
+                    m.cd[k] = make_double2(v[k].real(), v[k].imag());
+                    m.cf[k] = make_float2((float)v[k].real(), (float)v[k].imag());
+                }
+                m.flags = 0;
+                out.push_back(m);
+                if (!is_one(b.l2)) out.push_back(diag_of(op, ld, 2));
+                continue;
+            }
+        }
+        if (op.kind == OPK_PARITY2 && !real) {
+            BlockSplit e, o;
+            if (split_block(c(0), c(1), c(2), c(3), e) && split_block(c(4), c(5), c(6), c(7), o) &&
+                (genuine(e) || genuine(o))) {
+                // local index 0 = 00, 1 = 01, 2 = 10, 3 = 11: even block (0, 3), odd block (1, 2)
+                const cd rd[4] = {e.r1, o.r1, o.r2, e.r2}, ld[4] = {1.0, 1.0, o.l2, e.l2};
+                out.push_back(diag_of(op, rd, 4));
+                DevOp m = op;
+                const cd v[8] = {e.c, -I * e.s, -I * e.s, e.c, o.c, -I * o.s, -I * o.s, o.c};
+                for (int k = 0; k < 16; ++k) {
+                    m.cd[k] = make_double2(0.0, 0.0);
+                    m.cf[k] = make_float2(0.f, 0.f);
+                }
+                for (int k = 0; k < 8; ++k) {
+                    m.cd[k] = make_double2(v[k].real(), v[k].imag());
+                    m.cf[k] = make_float2((float)v[k].real(), (float)v[k].imag());
+                }
+                m.flags = (e.s == 0.0 ? 1 : 0) | (o.s == 0.0 ? 2 : 0);
+                out.push_back(m);
+                if (!is_one(e.l2) || !is_one(o.l2)) out.push_back(diag_of(op, ld, 4));
+                continue;
+            }
+        }
+        out.push_back(op);
+    }
+    return out;
+}
+}  // namespace
+
+// ----------------------------------------------------------------------------
 // Stage-sweep scheduling (engine 2).  The tile stays in shared memory; the
 // pass's op list is cut into stages of consecutive ops whose non-diagonal
 // qubits fit in 4 tile bits S.  A stage is one conflict-free sweep: every
@@ -565,7 +671,7 @@ static void swap_qubit_roles(DevOp& op) {
 // always hit distinct banks.  The kernel folds the rotation into per-thread
 // coefficients, once per op.
 // ----------------------------------------------------------------------------
-void schedule_stages(Pass& p, int amp_bytes, bool allow_inner) {
+void schedule_stages(Pass& p, int amp_bytes, bool allow_inner, bool split) {
     const int T = p.g.T;
     constexpr int K = 4;
     if (T < 12 || T > 13) return;
@@ -594,10 +700,13 @@ void schedule_stages(Pass& p, int amp_bytes, bool allow_inner) {
         }
         op.kind = op.nq == 1 ? OPK_DENSE1 : OPK_DENSE2;
     }
+    if (split) in = split_rotations(std::move(in));
     std::vector<DevOp> out;
     auto needs = [](const DevOp& op) {
         std::vector<int> v;
-        if (op.kind == OPK_DIAG || op.kind == OPK_STATESCALE || op.kind == OPK_REALTAB) return v;
+        if ((op.kind == OPK_DIAG && !(op.flags & DIAG_STAGED)) || op.kind == OPK_STATESCALE ||
+            op.kind == OPK_REALTAB)
+            return v;
         for (int t = 0; t < op.nq; ++t) v.push_back(op.lb[t]);
         return v;
     };

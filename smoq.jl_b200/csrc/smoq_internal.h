@@ -50,6 +50,9 @@ enum InnerBits : int32_t { INNER_ZERO = 4, INNER_DIAGG = 1, INNER_PRE = 2, INNER
 // OPK_DENSE1 / OPK_DENSE2 flag: every coefficient is real (Ry, CZ products): a
 // kernel may multiply with real scalars, half the FMAs of complex coefficients
 enum DenseBits : int32_t { OPF_REAL = 4 };
+// OPK_DIAG flag: a diagonal split off a rotation (split_rotations): the stage schedule
+// keeps its qubits on stage bits, so a compiled kernel folds it into literal phases
+enum DiagFlagBits : int32_t { DIAG_STAGED = 16 };
 
 struct alignas(16) DevOp {
     int32_t kind;
@@ -166,7 +169,7 @@ std::vector<Pass> plan_passes(const std::vector<GateIR>& gates, int N, int T, in
                               int epilogue_after_special = -1, int Lreq = 0);
 // turn a planned pass into stage sweeps of 4 tile bits (engines 2, 3); amp_bytes
 // selects the bank geometry
-void schedule_stages(Pass& p, int amp_bytes, bool allow_inner = false);
+void schedule_stages(Pass& p, int amp_bytes, bool allow_inner = false, bool split = false);
 void build_devop(const GateIR& gt, const TileGeom* g, DevOp& op);
 // jit.cpp: compile (or fetch from the process cache) the kernel of a staged complex64 pass
 // (minb_add: that many more CTAs per SM than the default register budget allows)

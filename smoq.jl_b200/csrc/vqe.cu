@@ -618,6 +618,7 @@ smoq_status smoq_internal_prepare(smoq_ctx* ctx, smoq_state* st, const std::vect
 std::vector<Pass> smoq_internal_plan(smoq_ctx* ctx, int N, int dtype, const std::vector<GateIR>& gates,
                                      bool variational);
 smoq_status smoq_internal_prepare_planned(smoq_ctx* ctx, std::vector<Pass>&& passes, void** handle);
+void smoq_internal_cap_fusion_depth(std::vector<Pass>& pl, int cap);
 smoq_status smoq_internal_rerun(smoq_ctx* ctx, smoq_state* st, void* prog_handle, const Epilogue* ep);
 void smoq_internal_free_prog(void* prog_handle);
 int smoq_internal_tile_bits(smoq_ctx* ctx, int dtype);
@@ -882,9 +883,11 @@ struct GradPlan {
 // kernel (4-bit register stages on both states, coefficients read at run time, so
 // the NVRTC compile of the first parameter set serves all later ones); with jit = 1
 // they are compiled here, on the planning thread, and loaded by the caller
-// fwd_ctx: also plan the forward (on fwd_ctx's options; a variational forward with jit 1)
+// fwd_ctx: also plan the forward (on fwd_ctx's options; a variational forward with jit 1);
+// max_ops: at most that many fused ops per backward pass (0: as many as fit)
 static void plan_gradient(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops, int n,
-                          const double* th, bool grad, GradPlan& gp, int jit = 0, smoq_ctx* fwd_ctx = nullptr) {
+                          const double* th, bool grad, GradPlan& gp, int jit = 0, smoq_ctx* fwd_ctx = nullptr,
+                          int max_ops = 0) {
     if ((gp.status = smoq_internal_ops_to_ir(N, ops, n, th, gp.ir))) {
         gp.error = "bad op list";
         return;
@@ -910,6 +913,7 @@ static void plan_gradient(int N, smoq_dtype dtype, int tile_bits, int low_bits, 
     const int T = std::max(tile_bits - 1, 6);
     try {
         gp.passes = plan_passes(back, N, T, low_bits, -1, dtype == SMOQ_C64 ? 1 : 0);
+        smoq_internal_cap_fusion_depth(gp.passes, max_ops);
     } catch (const std::exception& ex) {
         gp.status = SMOQ_ERR_BADINPUT;
         gp.error = ex.what();
@@ -995,12 +999,13 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
     std::vector<std::unique_ptr<GradPlan>> plans(batch);
     std::vector<std::future<void>> planned(batch);  // (declared after `plans`: joined first)
     const bool want_grad = grads != nullptr;
+    const int depth = ctx->fusion_depth;
     auto start = [&](int b) {
         plans[b].reset(new GradPlan);
         GradPlan* np = plans[b].get();
         const double* th = theta_of(b);
         planned[b] = std::async(std::launch::async,
-                                [=]() { plan_gradient(N, dtype, tb, lbits, ops, n, th, want_grad, *np, jit, ctx); });
+                                [=]() { plan_gradient(N, dtype, tb, lbits, ops, n, th, want_grad, *np, jit, ctx, depth); });
     };
     // set 0 alone first: a new circuit structure is compiled once, by its planning
     if (!use_pre) start(0);
@@ -1106,7 +1111,7 @@ static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op
         int32_t herr = 0;
         VCK(cudaMemcpy(&herr, ctx->d_err, sizeof(herr), cudaMemcpyDeviceToHost));
         if (herr) {
-            VCK(cudaMemset(ctx->d_err, 0, sizeof(int32_t)));
+            VCK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int32_t), ctx->stream));
             if ((herr & 255) == DEVERR_BOUNDS)
                 return smoq_internal_fail(ctx, SMOQ_ERR_CUDA,
                                           ("device bounds check failed at site " + std::to_string(herr >> 8)).c_str());
@@ -1412,7 +1417,7 @@ extern "C" smoq_status smoq_energy_grad_jobs(smoq_ctx* ctx, smoq_dtype dtype, co
         for (size_t i; !failed && (i = next++) < large.size();) {
             const smoq_vqe_job& J = jobs[large[i]];
             GradPlan gp;  // (host planning overlaps the other workers' GPU work)
-            plan_gradient(J.N, dtype, tb, lb, J.ops, J.n, J.theta, J.grad != nullptr, gp, 0, wc);
+            plan_gradient(J.N, dtype, tb, lb, J.ops, J.n, J.theta, J.grad != nullptr, gp, 0, wc, wc->fusion_depth);
             const smoq_status s =
                 vqe_run(wc, J.N, dtype, J.ops, J.n, J.n_params, J.H, J.nterms, 1, J.theta, J.energy, J.grad, &gp);
             if (s != SMOQ_OK) {

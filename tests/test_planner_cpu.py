@@ -309,3 +309,46 @@ def test_compiled_adjoint_kernels_compile(built, N, L, kinds):
             for th in (theta, rng.uniform(0, 2 * np.pi, size=circ.n_params))]
     assert srcs[0][0] == 0 and srcs[1][0] == 0
     assert "smoq_adj_e0" in srcs[0][3] and srcs[0][3] == srcs[1][3]
+
+
+def xxz_strang(S, N, seed=42, dt=0.05):
+    rng = np.random.default_rng(seed)
+    h = rng.uniform(-1, 1, size=N)
+    s1 = [S.gate("rz", [i + 1], angle=2 * h[i] * dt / 2) for i in range(N)]
+    for i in range(1, N):
+        s1 += [S.gate("rxx", [i, i + 1], angle=dt), S.gate("ryy", [i, i + 1], angle=dt),
+               S.gate("rzz", [i, i + 1], angle=dt / 2)]
+    ops = s1 + s1[::-1]
+    return ops, [(op.type, op.qubits, 0, op.fixed_angle) for op in ops]
+
+
+@pytest.mark.parametrize("N", [13, 16, 20])
+def test_compiled_plan_splits_rotations_exactly(built, N):
+    """engine 3 (literal compiled kernels): every complex 2x2 rotation block of a
+    1-qubit or parity op is split into diagonal . [[c, -is], [-is, c]] . diagonal;
+    the split program replays to the oracle's state (1e-12), keeps the stage
+    schedule well formed, and the XXZ bonds' rotations have only real and
+    imaginary coefficients"""
+    import pysmoq as S
+    ops, o = xxz_strang(S, N)
+    g2, o2 = circuit(N - N % 2, 300)
+    for gates, oo in ((ops + ops, o + o), (g2, o2)):
+        plan = S.debug_plan(N, gates, dtype=S.C64, tile_bits=13, low_bits=5, engine=3)
+        staged = [p for p in plan if p["T"] == 13]
+        assert staged
+        check_stages(staged, 4)
+        want = O.zero_state(N, 0b0101010101010101 & ((1 << N) - 1))
+        O.apply_circuit(want, O.make_ops(oo), len(oo), np.zeros(1), N)
+        got = replay(plan, N, O.zero_state(N, 0b0101010101010101 & ((1 << N) - 1)))
+        assert np.max(np.abs(got - want)) < 1e-12
+    plan = S.debug_plan(N, ops, dtype=S.C64, tile_bits=13, low_bits=5, engine=3)
+    par = [op for p in plan if p["T"] == 13 for op in p["ops"] if op["kind"] == 2]
+    assert par
+    for op in par:
+        c = op["c"][:8]
+        for blk in (c[0:4], c[4:8]):
+            assert abs(blk[0].imag) < 1e-15 and abs(blk[3].imag) < 1e-15 and abs(blk[0] - blk[3]) < 1e-15
+            assert abs(blk[1].real) < 1e-15 and abs(blk[2].real) < 1e-15 and abs(blk[1] - blk[2]) < 1e-15
+    # engine 2 keeps the fused ops whole
+    plan2 = S.debug_plan(N, ops, dtype=S.C64, tile_bits=13, low_bits=5, engine=2)
+    assert sum(len(p["ops"]) for p in plan2) < sum(len(p["ops"]) for p in plan)
