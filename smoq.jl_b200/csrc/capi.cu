@@ -158,10 +158,12 @@ struct DevProgram {
     std::vector<Pass> passes;
     std::vector<size_t> offs;  // first op of each pass in d_ops
     DevOp* d_ops = nullptr;
+    cudaStream_t s = nullptr;  // the stream d_ops was allocated on (stream-ordered free:
+                               // cudaFree would wait for every stream of the device)
     size_t nops = 0;
     int epi_pass = -1;
     ~DevProgram() {
-        if (d_ops) cudaFree(d_ops);
+        if (d_ops) cudaFreeAsync(d_ops, s);
     }
 };
 }  // namespace
@@ -189,7 +191,10 @@ static smoq_status upload_program(smoq_ctx* ctx, DevProgram& P) {
     }
     P.nops = all.size();
     if (all.empty()) return SMOQ_OK;
-    CK(ctx, cudaMalloc(&P.d_ops, all.size() * sizeof(DevOp)));
+    if (P.d_ops) CK(ctx, cudaFreeAsync(P.d_ops, P.s));  // (a program uploaded again)
+    P.d_ops = nullptr;
+    P.s = ctx->stream;
+    CK(ctx, cudaMallocAsync((void**)&P.d_ops, all.size() * sizeof(DevOp), ctx->stream));
     // on the context's (non-blocking) stream: a cudaMemcpy from pageable memory may
     // return before its DMA lands, and nothing would order it before the passes
     CK(ctx, cudaMemcpyAsync(P.d_ops, all.data(), all.size() * sizeof(DevOp), cudaMemcpyHostToDevice, ctx->stream));

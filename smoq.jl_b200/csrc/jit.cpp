@@ -351,20 +351,24 @@ struct Gen {
         // stage pattern (computed here in FP64); it commutes with every diagonal member
         // and with matrix members on other stage bits, and is applied before a matrix
         // member on its bits and at the stage's end.  (Run-time coefficients: no folding.)
-        std::vector<std::complex<double>> pend(R, 1.0);
-        int psup = 0;  // stage positions the pending phase depends on
-        auto flush = [&]() {
-            if (!psup) return;
+        // A matrix member leaves alone the stage patterns whose local index k has row and
+        // column e_k (an identity row: the even rows of a split XXZ rotation): only the
+        // other patterns take their pending phase before it.
+        const std::complex<double> one(1.0, 0.0);
+        std::vector<std::complex<double>> pend(R, one);
+        auto flush_where = [&](const std::vector<bool>& need) {
             for (int i = 0; i < nreg; ++i) {
-                const std::complex<double> z = pend[i & (R - 1)];
-                if (z == std::complex<double>(1.0, 0.0)) continue;
+                const int r = i & (R - 1);
+                if (!need[r] || pend[r] == one) continue;
+                const std::complex<double> z = pend[r];
                 std::string re, im;
                 cmac_terms({{CplxF{(float)z.real(), (float)z.imag()}, v(i)}}, re, im);
                 o << "        " << v(i) << " = cf{" << re << ", " << im << "};\n";
             }
-            std::fill(pend.begin(), pend.end(), std::complex<double>(1.0, 0.0));
-            psup = 0;
+            for (int r = 0; r < R; ++r)
+                if (need[r]) pend[r] = one;
         };
+        auto flush = [&]() { flush_where(std::vector<bool>(R, true)); };
         auto stage_pos = [&](int lb) {
             for (int q = 0; q < KB; ++q)
                 if (S[q] == lb) return q;
@@ -385,11 +389,32 @@ struct Gen {
                     for (int t = 0; t < op.nq; ++t) mi |= ((r >> stage_pos(op.lb[t])) & 1) << t;
                     pend[r] *= std::complex<double>(op.cd[mi].x, op.cd[mi].y);
                 }
-                psup |= pm;
                 continue;
             }
             const bool diagonal = op.kind == OPK_DIAG || op.kind == OPK_STATESCALE || op.kind == OPK_REALTAB;
-            if (!diagonal && (pm & psup)) flush();
+            if (!diagonal) {
+                const int dim = 1 << op.nq;
+                std::vector<bool> iso(dim, false);
+                if (!p.rtc && on_stage) {
+                    const std::vector<CplxF> M = op_matrix_f(op);
+                    for (int k = 0; k < dim; ++k) {
+                        bool e = M[k * dim + k].re == 1.f && M[k * dim + k].im == 0.f;
+                        for (int j = 0; j < dim && e; ++j)
+                            if (j != k) {
+                                const CplxF a = M[k * dim + j], b = M[j * dim + k];
+                                e = a.re == 0.f && a.im == 0.f && b.re == 0.f && b.im == 0.f;
+                            }
+                        iso[k] = e;
+                    }
+                }
+                std::vector<bool> need(R, true);
+                for (int r = 0; r < R && on_stage; ++r) {
+                    int k = 0;
+                    for (int t = 0; t < op.nq; ++t) k |= ((r >> stage_pos(op.lb[t])) & 1) << t;
+                    need[r] = !iso[k];
+                }
+                if (pm) flush_where(need);
+            }
             scal |= member(m, S, gstep, scal);
         }
         flush();
