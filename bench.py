@@ -371,7 +371,20 @@ def vqe_workload(args):
     return 0
 
 
+def lib_trotter_gates(S, N, bonds, fields, dt):
+    """the library's closed-form Trotter gates (smoq_precompute_trotter_gates) of bonds
+    (i, j, Jxx, Jyy, Jzz) and fields (idx, hx, hy, hz), 1-based sites"""
+    params = S.HamiltonianParams(N, [S.CouplingTerm(*b) for b in bonds], [],
+                                 [S.FieldTerm(*f) for f in fields])
+    return S.precompute_trotter_gates_bitwise(params, dt)
+
+
 def vqe_jobs_workload(args):
+    print(json.dumps(vqe_jobs_line(args)))
+    return 0
+
+
+def vqe_jobs_line(args):
     """Batched uneven circuits: 256 circuits, N ~ U{10..20}, depth ~ U{4..16} layers of
     [Ry all; Rz all; CZ ladder] (seeded), TFIM H = -sum ZZ - sum X each, one energy +
     adjoint gradient per circuit, through smoq_energy_grad_jobs.  metric =
@@ -415,12 +428,17 @@ def vqe_jobs_workload(args):
             "c128_gradients_per_s": res["c128"][0],
             "param_gradients_per_s_c64": nparams * args.steps / res["c64"][3],
             "energy_abs_err_c64_vs_c128": err_e, "grad_max_abs_err_c64_vs_c128": err_g}
-    print(json.dumps(line))
     ctx.close()
+    return line
     return 0
 
 
 def mcwf_workload(args):
+    print(json.dumps(mcwf_line(args)))
+    return 0
+
+
+def mcwf_line(args):
     """Batched MCWF: TFIM N=16 (J = h = 1, first-order Trotter, 31 gates per step),
     jumps sqrt(0.1) sigma- and sqrt(0.05) sigma_z on every qubit, dt = 0.01, 500
     steps, 4096 trajectories from |0...0>, complex64 amplitudes with FP64 norms and
@@ -430,15 +448,13 @@ def mcwf_workload(args):
     a trajectory subset."""
     import torch
     import pysmoq as S
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
     ctx = S.Context(0)
     if args.engine >= 0:
         ctx.set_option(S._lib.OPT_ENGINE, args.engine)
     N, dt, steps, B, rec = 16, 0.01, 500, 4096, 10
-    arr, n = O.precompute_trotter_gates([(i, i + 1, 0.0, 0.0, 1.0) for i in range(1, N)],
-                                        [(i, 1.0, 0.0, 0.0) for i in range(1, N + 1)], dt)
-    gates = [S.FastTrotterGate(idx, U) for idx, U in O.gates_to_list(arr, n)]
+    bonds = [(i, i + 1, 0.0, 0.0, 1.0) for i in range(1, N)]
+    fields = [(i, 1.0, 0.0, 0.0) for i in range(1, N + 1)]
+    gates = lib_trotter_gates(S, N, bonds, fields, dt)
     jumps = [S.JumpOperator("sigma_minus", q, 0.1) for q in range(1, N + 1)] + \
             [S.JumpOperator("sigma_z", q, 0.05) for q in range(1, N + 1)]
     plan = S.TrotterPlan(ctx, N, gates, order=1, dtype=S.C64)
@@ -458,6 +474,9 @@ def mcwf_workload(args):
     value = B * steps * args.steps / (ms * 1e-3)
     cpu = None
     if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        arr, n = O.precompute_trotter_gates(bonds, fields, dt)
         ncpu = os.cpu_count() or 1
         ntr = 2 * ncpu
         oj = [(0, q, 0.1) for q in range(1, N + 1)] + [(2, q, 0.05) for q in range(1, N + 1)]
@@ -477,14 +496,18 @@ def mcwf_workload(args):
             "reference_published": "N=16 1000 trajectories x 200 steps (dephasing only, dt 0.05) 397.29 s "
                                    "= 503 trajectory-steps/s on a laptop (output.log:449)",
             "cpu_baseline": cpu}
-    print(json.dumps(line))
     st.close()
     plan.close()
     ctx.close()
-    return 0
+    return line
 
 
 def qrc_workload(args):
+    print(json.dumps(qrc_line(args)))
+    return 0
+
+
+def qrc_line(args):
     """Quantum reservoir computing, the bitwise MCWF loop: two XXZ rails of L=6
     qubits (N=12; rail bonds Jxx = Jyy = 1, Jzz = 0.5; rungs 0.7, 0.7, 0.3; x field
     0.5 and seeded z fields), dt = 0.1, 5 Trotter steps per input, 100 seeded
@@ -495,16 +518,13 @@ def qrc_workload(args):
     (complex128, trajectories over all host cores) on a trajectory subset."""
     import torch
     import pysmoq as S
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
     ctx = S.Context(0)
     L, T, B, sub, dt = 6, args.inputs, args.trajectories, 5, 0.1
     rng = np.random.default_rng(2026)
     bonds = [(r * L + s + 1, r * L + s + 2, 1.0, 1.0, 0.5) for r in range(2) for s in range(L - 1)]
     bonds += [(s + 1, L + s + 1, 0.7, 0.7, 0.3) for s in range(L)]
     fields = [(q + 1, 0.5, 0.0, float(rng.uniform(-1, 1))) for q in range(2 * L)]
-    arr, n = O.precompute_trotter_gates(bonds, fields, dt)
-    gates = [S.FastTrotterGate(idx, U) for idx, U in O.gates_to_list(arr, n)]
+    gates = lib_trotter_gates(S, 2 * L, bonds, fields, dt)
     u = rng.uniform(0, 1, T)
     padded = np.concatenate([np.zeros(L), u])
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
@@ -528,6 +548,9 @@ def qrc_workload(args):
         plan.close()
     cpu = None
     if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        arr, n = O.precompute_trotter_gates(bonds, fields, dt)
         ncpu = os.cpu_count() or 1
         ntr, ti = 4 * ncpu, min(20, T)
         t0 = time.perf_counter()
@@ -548,9 +571,8 @@ def qrc_workload(args):
             "c128_trajectory_inputs_per_s": res["c128"][0],
             "feature_mean_abs_diff_c64_vs_c128": float(np.mean(np.abs(X64 - X128))),
             "gpu_launches": args.steps, "cpu_baseline": cpu}
-    print(json.dumps(line))
     ctx.close()
-    return 0
+    return line
 
 
 # FP32 instructions per amplitude of a fused op, by kind (dense 2x2: 2 complex
@@ -635,6 +657,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-vqe", action="store_true", help="skip the VQE gradient sub-record of the default line")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the short C4b / MCWF / QRC sub-records of the default line")
     ap.add_argument("--autotune", type=int, default=-1,
                     help="compiled pass kernels: per-pass variant tuning (-1 library default = on, 0 off, 1 on)")
     # smaller cases of the same kernel (profiling, sweeps); the defaults are the workload
@@ -797,6 +821,23 @@ def main():
     published = None
     if not args.no_vqe and N == N_QUBITS and rank == 0:
         published = published_comparison(ctx)
+    # short runs of the other workloads (one timed step each, no CPU baselines), so the
+    # default line carries their figures too; the full runs are --workload vqe_jobs,
+    # mcwf and qrc
+    extras = None
+    if rank == 0 and ws == 1 and not args.no_extras and N == N_QUBITS:
+        extras = {}
+        sub = argparse.Namespace(steps=1, warmup=1, engine=-1, no_cpu_baseline=True, trajectories=4096,
+                                 inputs=100)
+        keep = ("metric", "value", "unit", "ms_per_step", "c128_gradients_per_s", "energy_abs_err_c64_vs_c128",
+                "c128_trajectory_inputs_per_s", "e2e", "jumps_per_trajectory_mean")
+        for name, fn in (("vqe_jobs", vqe_jobs_line), ("mcwf", mcwf_line), ("qrc", qrc_line)):
+            try:
+                r = fn(sub)
+                extras[name] = {k: r[k] for k in keep if k in r}
+                extras[name]["workload"] = r["config"]["workload"]
+            except Exception as ex:  # a sub-record never costs the headline line
+                extras[name] = {"error": f"{type(ex).__name__}: {ex}"}
 
     if rank == 0:
         line = {"metric": "gate_apps_per_s", "value": value, "unit": "gate-apps/s", "n_gpus": ws,
@@ -824,7 +865,8 @@ def main():
                 "gpu_launches": int(launches),
                 "clocks": clk,
                 "vqe": vqe,
-                "published_comparison": published}
+                "published_comparison": published,
+                "other_workloads": extras}
         print(json.dumps(line))
     st.close()
     plan.close()

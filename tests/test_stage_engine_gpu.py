@@ -158,22 +158,30 @@ def test_strang_trotter(ctx, eng, N, dtype, tb64, tol):
 
 
 def test_engines_agree_on_trotter_n22(ctx):
-    """N=22 complex64 XXZ: the stage engine and the shared-memory engine agree
-    to FP32 rounding after 10 Strang steps"""
+    """N=22 complex64 XXZ, 10 Strang steps (about 4,000 fused-op applications per
+    amplitude): the shared-memory, stage and compiled engines each stay within FP32
+    rounding of the complex128 result of the same plan (max |d psi| < 5e-6, relative
+    L2 < 2e-6), and within 5e-6 of one another.  The compiled engine splits rotations
+    and folds diagonals, so its roundings come in another order than engine 0's."""
     N = 22
     _, _, gl = xxz(N, 0.05)
     gates = [S.FastTrotterGate(i, U) for i, U in gl]
     out = {}
-    for e in (0, 2, 3):
+    for e, dt in ((0, S.C128), (0, S.C64), (2, S.C64), (3, S.C64)):
         with engine(ctx, e):
-            plan = S.TrotterPlan(ctx, N, gates, order=2, dtype=S.C64)
-            st = S.CuState(ctx, N, S.C64, basis=5)
+            plan = S.TrotterPlan(ctx, N, gates, order=2, dtype=dt)
+            st = S.CuState(ctx, N, dt, basis=5)
             plan.step(st, 10)
-            out[e] = st.download()
+            out[(e, dt)] = st.download().astype(complex)
             st.close()
             plan.close()
-    assert np.max(np.abs(out[0] - out[2])) < 2e-6
-    assert np.max(np.abs(out[0] - out[3])) < 2e-6
+    ref = out[(0, S.C128)]
+    for e in (0, 2, 3):
+        d = out[(e, S.C64)] - ref
+        print(f"N=22 engine {e} c64 vs c128: max {np.max(np.abs(d)):.2e}, rel L2 {rel(out[(e, S.C64)], ref):.2e}")
+        assert np.max(np.abs(d)) < 5e-6 and rel(out[(e, S.C64)], ref) < 2e-6
+    assert np.max(np.abs(out[(0, S.C64)] - out[(2, S.C64)])) < 5e-6
+    assert np.max(np.abs(out[(0, S.C64)] - out[(3, S.C64)])) < 5e-6
 
 
 def test_mcwf_trajectory_exact(ctx, eng):
