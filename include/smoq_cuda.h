@@ -406,10 +406,13 @@ smoq_status smoq_energy(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* o
  * Threads.@threads loop).  Each job is one circuit with one parameter vector;
  * grad may be NULL (energy only).  Circuits whose two states fit one CTA's
  * shared memory (N <= 13 complex64, N <= 12 complex128) run together in one
- * launch, one CTA per circuit (SMOQ_OPT_VQE_RESIDENT); the others run in
- * submission order on the context's stream; the call returns when all are
- * done.  The first failing job's status is returned, with its index in the
- * message. */
+ * launch, one CTA per circuit, off a device work queue (SMOQ_OPT_VQE_RESIDENT);
+ * the others are taken off a host queue by up to 8 worker threads, each planning
+ * a circuit and running it on a worker context of its own (own stream and error
+ * word, the context's options; created on first use and kept until the context
+ * is destroyed), so the small grids of several circuits share the GPU.  The
+ * call returns when all jobs are done.  The first failing job's status is
+ * returned, with its index in the message. */
 typedef struct {
     int N;                        /* qubits of this circuit */
     const smoq_op* ops;           /* its gate list */
