@@ -575,17 +575,45 @@ def qrc_line(args):
     return line
 
 
-# FP32 instructions per amplitude of a fused op, by kind (dense 2x2: 2 complex
-# multiply-adds per output amplitude, dense 4x4: 4, parity 4x4: 2, monomial and
-# diagonal: 1 complex multiply; 4 FP32 FMA-pipe instructions each)
-_FP32_PER_AMP = {0: 8, 1: 16, 2: 8, 3: 4, 4: 4}
+def _op_fp32_per_amp(o):
+    """FP32 FMA-pipe instructions per amplitude of one fused op, from its matrix: per
+    output amplitude each nonzero coefficient costs 4 (general complex), 2 (real or
+    imaginary) or 0 (+-1, +-i: a copy or a swap of parts)"""
+    c, k, nq = o["c"], o["kind"], o["nq"]
+    dim = 1 << nq
+    if k in (5, 6):                       # per-state scale, real byte tables: 2 real multiplies
+        return 2.0
+    M = np.zeros((dim, dim), complex)
+    if k == 0:
+        M = c[:4].reshape(2, 2)
+    elif k == 1:
+        M = c[:16].reshape(4, 4)
+    elif k == 2:
+        M[0, 0], M[0, 3], M[3, 0], M[3, 3] = c[0], c[1], c[2], c[3]
+        M[1, 1], M[1, 2], M[2, 1], M[2, 2] = c[4], c[5], c[6], c[7]
+    elif k == 3:
+        for r in range(dim):
+            M[r, o["perm"][r]] = c[r]
+    elif k == 4:
+        M = np.diag(c[:dim])
+    else:
+        return 0.0
+
+    def cost(z):
+        if z == 0:
+            return 0
+        if (z.imag == 0 and abs(z.real) == 1) or (z.real == 0 and abs(z.imag) == 1):
+            return 0
+        return 2 if (z.imag == 0 or z.real == 0) else 4
+    return sum(cost(z) for z in M.reshape(-1)) / dim
 
 
 def plan_fp32_per_amp(S, N, ops, dtype, engine):
-    """sum over the planned passes of the FP32 instructions per amplitude (host planner)"""
+    """sum over the planned passes of the FP32 instructions per amplitude (host planner;
+    for engine 3 an upper bound: the compiled kernels fold the stage diagonals)"""
     tb, lb = (13, 5) if dtype == S.C64 else (12, 4)
     plan = S.debug_plan(N, ops, dtype=dtype, tile_bits=tb, low_bits=lb, engine=max(0, engine))
-    return sum(_FP32_PER_AMP.get(o["kind"], 0) for p in plan for o in p["ops"]), len(plan)
+    return sum(_op_fp32_per_amp(o) for p in plan for o in p["ops"]), len(plan)
 
 
 def bandwidth_workload(args):

@@ -541,6 +541,11 @@ smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tile_bits, int 
 smoq_status smoq_debug_compile_adjoint(int N, const smoq_op* ops, int n, int n_params, const double* theta,
                                        int tile_bits, int low_bits, int flags, int* n_passes, int* n_compiled,
                                        char* msg, int msg_len);
+/* Host-only view of the autotuner's geometry rule: ms[c] = the timed run of
+ * candidate c (< 0: not plannable), candidate 0 the default geometry.  Returns the
+ * candidate kept: the fastest, unless the default is within 2% of it (one timed
+ * run each: smaller differences are noise); -1 when none was plannable. */
+int smoq_debug_pick_geometry(const float* ms, int n);
 smoq_status smoq_debug_plan_sequence(int N, smoq_dtype dtype, int tile_bits, int low_bits, int engine,
                                      const smoq_op* ops, int n, const double* theta, smoq_pass_info* passes, int max_passes,
                                      smoq_fused_op_info* fused, int max_fused, int* n_passes, int* n_fused);

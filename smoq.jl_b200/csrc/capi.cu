@@ -842,6 +842,7 @@ smoq_status smoq_apply_sequence(smoq_state* st, const smoq_op* ops, int n, const
     return sync_check(ctx);
 }
 
+
 smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tbits, int lbits, const smoq_op* ops, int n,
                                    const double* theta, int flags, int* n_compiled, char* msg, int msg_len) {
     const bool verbose = (flags & 1) != 0;
@@ -1196,13 +1197,26 @@ static smoq_status get_block(smoq_plan* P, int nsteps, smoq_plan::Block** out) {
 // pass kernels, when SMOQ_OPT_AUTOTUNE is on): the block is planned with each
 // candidate geometry -- tile width, low bits, fusion depth -- compiled, and run
 // once on a zeroed scratch state; the fastest geometry is kept for every block of
-// the plan and cached per (GPU, N, gate pattern).  Every candidate computes the
-// same evolution (fusion regroups the same gates).
+// the plan and cached per (GPU, N, gate pattern).  The first candidate is the
+// default: another one replaces it only when it is faster by more than
+// kGeometryMargin (one timed run per candidate: smaller differences are noise).
+// Every candidate computes the same evolution (fusion regroups the same gates).
 namespace {
 struct PlanGeometry {
     int tbits, lbits, max_ops;
 };
 const PlanGeometry kGeometries[] = {{13, 5, 0}, {13, 4, 0}, {12, 5, 0}, {12, 4, 0}, {13, 5, 12}};
+constexpr float kGeometryMargin = 0.02f;
+
+// the candidate kept: the fastest, unless the default (candidate 0) is within the
+// margin of it; ms[c] < 0: candidate c could not be planned (-1: none could)
+int pick_geometry(const float* ms, int n) {
+    int best = -1;
+    for (int c = 0; c < n; ++c)
+        if (ms[c] >= 0 && (best < 0 || ms[c] < ms[best])) best = c;
+    if (best > 0 && ms[0] >= 0 && ms[best] > (1.0f - kGeometryMargin) * ms[0]) best = 0;
+    return best;
+}
 std::map<uint64_t, int> g_geometry;  // guarded by g_tune_mu
 }  // namespace
 
@@ -1254,10 +1268,11 @@ static smoq_status choose_geometry(smoq_plan* P, const std::vector<GateIR>& all)
     CK(ctx, cudaEventCreate(&e0));
     CK(ctx, cudaEventCreate(&e1));
     std::ostringstream rep;
-    int best = -1;
-    float best_ms = 0;
+    constexpr int ng = (int)(sizeof(kGeometries) / sizeof(kGeometries[0]));
+    float times[ng];
+    for (int c = 0; c < ng; ++c) times[c] = -1.0f;
     const long long launches0 = ctx->launches, passes0 = ctx->tile_passes;
-    for (int c = 0; c < (int)(sizeof(kGeometries) / sizeof(kGeometries[0])); ++c) {
+    for (int c = 0; c < ng; ++c) {
         const PlanGeometry& G = kGeometries[c];
         DevProgram prog;
         try {
@@ -1281,8 +1296,9 @@ static smoq_status choose_geometry(smoq_plan* P, const std::vector<GateIR>& all)
         cudaEventElapsedTime(&ms, e0, e1);
         rep << "geometry tile " << G.tbits << " low " << G.lbits << " depth " << (G.max_ops ? G.max_ops : -1) << ": "
             << prog.passes.size() << " passes, " << ms << " ms\n";
-        if (best < 0 || ms < best_ms) best = c, best_ms = ms;
+        times[c] = ms;
     }
+    const int best = pick_geometry(times, ng);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     ctx->launches = launches0;  // the tuning runs are not the caller's work
@@ -1587,3 +1603,9 @@ smoq_status smoq_internal_plan_step(smoq_plan* P, smoq_ctx** ctx, int* N, int* d
     return SMOQ_OK;
 }
 int smoq_internal_low_bits(smoq_ctx* ctx, int dtype) { return low_bits(ctx, dtype); }
+
+// host-only view of the geometry rule (pick_geometry)
+extern "C" int smoq_debug_pick_geometry(const float* ms, int n) {
+    if (!ms || n < 1 || n > 64) return -1;
+    return pick_geometry(ms, n);
+}

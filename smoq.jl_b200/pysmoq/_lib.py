@@ -169,6 +169,7 @@ _SIGS = {
                                 C.c_char_p, C.c_int],
     "smoq_debug_compile_adjoint": [C.c_int, C.POINTER(SmoqOp), C.c_int, C.c_int, _dp, C.c_int, C.c_int, C.c_int,
                                    _ip, _ip, C.c_char_p, C.c_int],
+    "smoq_debug_pick_geometry": [C.POINTER(C.c_float), C.c_int],
     "smoq_debug_plan_sequence": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, _dp,
                                  C.POINTER(SmoqPassInfo), C.c_int, C.POINTER(SmoqFusedOpInfo), C.c_int, _ip, _ip],
     "smoq_energy": [_vp, C.c_int, C.c_int, C.POINTER(SmoqOp), C.c_int, C.c_int, C.POINTER(SmoqPauliTerm),

@@ -352,3 +352,22 @@ def test_compiled_plan_splits_rotations_exactly(built, N):
     # engine 2 keeps the fused ops whole
     plan2 = S.debug_plan(N, ops, dtype=S.C64, tile_bits=13, low_bits=5, engine=2)
     assert sum(len(p["ops"]) for p in plan2) < sum(len(p["ops"]) for p in plan)
+
+
+def test_autotuner_geometry_rule(built):
+    """the plan autotuner keeps its default geometry (candidate 0) unless another
+    candidate's timed run is faster by more than 2% (one run each: smaller
+    differences are noise); unplannable candidates (< 0) never win"""
+    import ctypes as C
+    import pysmoq as S
+
+    def pick(ms):
+        a = (C.c_float * len(ms))(*ms)
+        return S.lib.smoq_debug_pick_geometry(a, len(ms))
+    assert pick([53.46, 53.12, 53.74, 65.90, 59.29]) == 0      # 0.6% faster: noise, keep the default
+    assert pick([62.0, 55.0, 67.9, 77.2, 67.2]) == 1           # 11% faster: switch
+    assert pick([10.0, 9.85, 9.82, 12.0]) == 0                 # within 2% of the default
+    assert pick([10.0, 9.7, 9.79, 12.0]) == 1                  # 3% faster
+    assert pick([-1.0, 20.0, 18.0]) == 2                       # no default run: the fastest
+    assert pick([-1.0, -1.0]) == -1
+    assert pick([5.0]) == 0
