@@ -603,7 +603,7 @@ DevOp diag_of(const DevOp& like, const cd* v, int n) {
 bool is_one(cd z) { return std::abs(z - cd(1.0, 0.0)) < 1e-15; }
 
 // DENSE1 / PARITY2 ops with a genuine complex rotation become R-diagonal, rotation,
-// L-diagonal (the L-diagonal left out when it is the identity)
+// L-diagonal (a diagonal factor that is the identity is left out)
 std::vector<DevOp> split_rotations(std::vector<DevOp> in) {
     const cd I(0.0, 1.0);
     std::vector<DevOp> out;
@@ -616,7 +616,7 @@ std::vector<DevOp> split_rotations(std::vector<DevOp> in) {
             BlockSplit b;
             if (split_block(c(0), c(1), c(2), c(3), b) && genuine(b)) {
                 const cd rd[2] = {b.r1, b.r2}, ld[2] = {1.0, b.l2};
-                out.push_back(diag_of(op, rd, 2));
+                if (!is_one(b.r1) || !is_one(b.r2)) out.push_back(diag_of(op, rd, 2));
                 DevOp m = op;
                 const cd v[4] = {b.c, -I * b.s, -I * b.s, b.c};
                 for (int k = 0; k < 4; ++k) {
@@ -635,7 +635,8 @@ std::vector<DevOp> split_rotations(std::vector<DevOp> in) {
                 (genuine(e) || genuine(o))) {
                 // local index 0 = 00, 1 = 01, 2 = 10, 3 = 11: even block (0, 3), odd block (1, 2)
                 const cd rd[4] = {e.r1, o.r1, o.r2, e.r2}, ld[4] = {1.0, 1.0, o.l2, e.l2};
-                out.push_back(diag_of(op, rd, 4));
+                if (!is_one(e.r1) || !is_one(e.r2) || !is_one(o.r1) || !is_one(o.r2))
+                    out.push_back(diag_of(op, rd, 4));
                 DevOp m = op;
                 const cd v[8] = {e.c, -I * e.s, -I * e.s, e.c, o.c, -I * o.s, -I * o.s, o.c};
                 for (int k = 0; k < 16; ++k) {
