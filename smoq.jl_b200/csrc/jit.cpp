@@ -485,21 +485,35 @@ struct Gen {
         o << "        cf sc = cf{1.f, 0.f}, scw = cf{1.f, 0.f};\n";
         std::vector<int> cols;  // the stage's measurements, reduced together at its end
         bool writes = false;
+        size_t reduced = 0;  // measurements [0, reduced) are summed already
         for (int m : members) {
             if (p.ops[m].kind == OPK_INNER) {
                 inner(m, S, (int)cols.size());
                 cols.push_back(p.ops[m].perm[0]);
+                // a group of kMeasGroup is reduced at once: at most that many FP32
+                // accumulators stay live beside the two register sets
+                if (cols.size() - reduced == (size_t)kMeasGroup) {
+                    reduce_measurements(cols, reduced, cols.size());
+                    reduced = cols.size();
+                }
                 continue;
             }
             writes = true;
-            for (int k = 0; k < 2; ++k) {  // the op on both register sets
+            // the op on both register sets, emitted statement by statement in
+            // alternation: a coefficient's two uses (phi, lambda) are adjacent
+            std::string code[2];
+            for (int k = 0; k < 2; ++k) {
                 vp = sets[k][0];
                 scn = sets[k][2];
+                std::ostringstream keep(std::move(o));
+                o = std::ostringstream();
                 scal[k] |= member(m, S, gstep, true);
+                code[k] = o.str();
+                o = std::move(keep);
             }
+            interleave(code[0], code[1]);
         }
-        for (size_t c0 = 0; c0 < cols.size(); c0 += 8)
-            reduce_measurements(cols, c0, std::min<size_t>(cols.size(), c0 + 8));
+        if (reduced < cols.size()) reduce_measurements(cols, reduced, cols.size());
         // after a stage that only read (no barrier at its end), other threads may
         // still be reading what this stage's stores overwrite
         if (writes && pending_reads) o << "        __syncthreads();\n";
@@ -521,6 +535,37 @@ struct Gen {
         pending_reads = !writes;
     }
     bool pending_reads = false;
+    static constexpr int kMeasGroup = 4;
+
+    // top-level statements of generated code: a line at the stage's indent, or a
+    // block from such a line opening "{" to the matching closing line
+    static std::vector<std::string> statements(const std::string& code) {
+        std::vector<std::string> out;
+        std::istringstream in(code);
+        std::string line, cur;
+        int depth = 0;
+        while (std::getline(in, line)) {
+            cur += line + "\n";
+            for (char ch : line) depth += ch == '{' ? 1 : ch == '}' ? -1 : 0;
+            if (depth <= 0) {
+                out.push_back(cur);
+                cur.clear();
+                depth = 0;
+            }
+        }
+        if (!cur.empty()) out.push_back(cur);
+        return out;
+    }
+    // the two sets' code for one op, statement by statement in alternation (they
+    // have the same statements, register names aside); else one after the other
+    void interleave(const std::string& a, const std::string& b) {
+        const std::vector<std::string> sa = statements(a), sb = statements(b);
+        if (sa.size() != sb.size()) {
+            o << a << b;
+            return;
+        }
+        for (size_t i = 0; i < sa.size(); ++i) o << sa[i] << sb[i];
+    }
 
     // warp sums of measurements cols[c0..c1) (at most 8, accumulators m<c0>..): a
     // transposed butterfly -- each exchange step halves the values a lane carries

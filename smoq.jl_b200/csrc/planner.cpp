@@ -305,7 +305,10 @@ static void diag_of(const GateIR& g, cd* d) {
 //  * a pending 2x2 that is flushed (end of pass, or a diagonal on a non-tile
 //    qubit) is folded into the last 2-qubit op on its qubit when nothing
 //    after that op touched the qubit;
-//  * consecutive diagonal ops merge into one phase table (up to 4 qubits).
+//  * a diagonal op merges into an earlier diagonal op (one phase table, up to 4
+//    qubits) when every op in between commutes with it: diagonal ops, measurements
+//    of a diagonal generator, and ops on other qubits (a backward program's Rz^dag
+//    ops join the CZ tables across the Z measurements between them).
 struct Fuser {
     const TileGeom* g;
     std::vector<GateIR> ops;
@@ -362,11 +365,45 @@ struct Fuser {
         A = r;
         return true;
     }
+    // does op o commute with the diagonal d?
+    static bool commutes_with_diag(const GateIR& o, const GateIR& d) {
+        if (o.special == OPK_REALTAB || o.special == OPK_STATESCALE) return true;  // diagonal
+        bool diag = o.diag && !o.special;
+        if (o.special == OPK_INNER) {  // a measurement: its generator's matrix is in m
+            const int dim = 1 << o.nq;
+            diag = true;
+            for (int r = 0; r < dim && diag; ++r)
+                for (int c = 0; c < dim; ++c)
+                    if (r != c && std::abs(o.m[r * dim + c]) != 0.0) diag = false;
+        } else if (o.special) {
+            return false;
+        }
+        if (diag) return true;
+        for (int t = 0; t < o.nq; ++t)
+            for (int u = 0; u < d.nq; ++u)
+                if (o.q[t] == d.q[u]) return false;
+        return true;
+    }
     void push(const GateIR& gt) {
-        if (gt.diag && !gt.special && !ops.empty() && ops.back().diag && !ops.back().special &&
-            merge_diag(ops.back(), gt)) {
-            touch((int)ops.size() - 1);
-            return;
+        if (gt.diag && !gt.special) {
+            int seen = 0;
+            for (int i = (int)ops.size() - 1; i >= 0 && seen < 64; --i, ++seen) {
+                GateIR& e = ops[i];
+                if (e.diag && !e.special) {
+                    // (a look-back merge only builds tables on tile qubits: a table
+                    // with an off-tile qubit is indexed per register at run time)
+                    bool tile_only = true;
+                    for (int t = 0; t < e.nq; ++t) tile_only &= is_tile(e.q[t]);
+                    for (int t = 0; t < gt.nq; ++t) tile_only &= is_tile(gt.q[t]);
+                    if ((i == (int)ops.size() - 1 || tile_only) && merge_diag(e, gt)) {
+                        // (ops after i that touched these qubits keep their later mark)
+                        for (int t = 0; t < e.nq; ++t) last_touch[e.q[t]] = std::max(last_touch[e.q[t]], i);
+                        return;
+                    }
+                    continue;  // diagonals commute: look further back for room
+                }
+                if (!commutes_with_diag(e, gt)) break;
+            }
         }
         ops.push_back(gt);
         touch((int)ops.size() - 1);
@@ -672,6 +709,8 @@ std::vector<DevOp> split_rotations(std::vector<DevOp> in) {
 // always hit distinct banks.  The kernel folds the rotation into per-thread
 // coefficients, once per op.
 // ----------------------------------------------------------------------------
+constexpr int kMaxBackwardStageOps = 24;
+
 void schedule_stages(Pass& p, int amp_bytes, bool allow_inner, bool split) {
     const int T = p.g.T;
     constexpr int K = 4;
@@ -752,6 +791,9 @@ void schedule_stages(Pass& p, int amp_bytes, bool allow_inner, bool split) {
         size_t j = i;
         for (; j < in.size(); ++j) {
             if (in[j].kind != OPK_DIAG && in[j].nq > 2) break;
+            // a backward stage holds two register sets: its length is capped, so the
+            // compiled kernel's straight-line code per stage stays within registers
+            if (allow_inner && (int)(j - i) >= kMaxBackwardStageOps) break;
             std::vector<int> U = S;
             for (int b : needs(in[j]))
                 if (!contains(U, b)) U.push_back(b);
