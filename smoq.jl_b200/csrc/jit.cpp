@@ -437,7 +437,7 @@ struct Gen {
             for (int i = 0; i < (GS << KB); ++i) {
                 if ((i >> q) & 1) continue;
                 const int k = i | (1 << q);
-                o << "          { const cf t = s ? " << v(k) << " : " << v(i) << "; " << v(k) << " = s ? " << v(i)
+                o << "          { const auto t = s ? " << v(k) << " : " << v(i) << "; " << v(k) << " = s ? " << v(i)
                   << " : " << v(k) << "; " << v(i) << " = t; }\n";
             }
             o << "        }\n";
@@ -472,17 +472,19 @@ struct Gen {
             o << ";\n";
         }
         const int nreg = GS * R;
-        const char* sets[2][3] = {{"v", "tile", "sc"}, {"w", "tlam", "scw"}};
-        for (auto& st : sets) {
-            vp = st[0];
-            for (int i = 0; i < nreg; ++i) {
-                const uint32_t c = off[i & (R - 1)] | ((i >> KB) ? gstep : 0u);
-                o << "        cf " << v(i) << " = " << st[1] << (rotated ? "[ga ^ " : "[g0 + ") << c << "u];\n";
-            }
-            if (rotated) unrotate(rl);
+        for (int i = 0; i < nreg; ++i) {
+            const uint32_t c = off[i & (R - 1)] | ((i >> KB) ? gstep : 0u);
+            const std::string at = std::string(rotated ? "[ga ^ " : "[g0 + ") + std::to_string(c) + "u]";
+            o << "        float2 P" << i << ", Q" << i << ";\n        { const cf f = tile" << at << ", l = tlam" << at
+              << "; P" << i << " = make_float2(f.x, l.x); Q" << i << " = make_float2(f.y, l.y); }\n";
         }
-        bool scal[2] = {false, false};
-        o << "        cf sc = cf{1.f, 0.f}, scw = cf{1.f, 0.f};\n";
+        if (rotated)
+            for (const char* pre : {"P", "Q"}) {
+                vp = pre;
+                unrotate(rl);
+            }
+        bool scal = false;
+        o << "        cf sc = cf{1.f, 0.f};\n";
         std::vector<int> cols;  // the stage's measurements, reduced together at its end
         bool writes = false;
         size_t reduced = 0;  // measurements [0, reduced) are summed already
@@ -499,32 +501,26 @@ struct Gen {
                 continue;
             }
             writes = true;
-            // the op on both register sets, emitted statement by statement in
-            // alternation: a coefficient's two uses (phi, lambda) are adjacent
-            std::string code[2];
-            for (int k = 0; k < 2; ++k) {
-                vp = sets[k][0];
-                scn = sets[k][2];
-                std::ostringstream keep(std::move(o));
-                o = std::ostringstream();
-                scal[k] |= member(m, S, gstep, true);
-                code[k] = o.str();
-                o = std::move(keep);
-            }
-            interleave(code[0], code[1]);
+            scal |= member_packed(m, S);
         }
         if (reduced < cols.size()) reduce_measurements(cols, reduced, cols.size());
         // after a stage that only read (no barrier at its end), other threads may
         // still be reading what this stage's stores overwrite
         if (writes && pending_reads) o << "        __syncthreads();\n";
-        for (int k = 0; k < 2 && writes; ++k) {
-            vp = sets[k][0];
-            if (scal[k])
-                for (int i = 0; i < nreg; ++i) o << "        " << v(i) << " = cmul(" << sets[k][2] << ", " << v(i) << ");\n";
-            if (rotated) unrotate(rl);
+        if (writes) {
+            if (scal)
+                for (int i = 0; i < nreg; ++i)
+                    emit_pmul("P" + std::to_string(i), "Q" + std::to_string(i), "sc.x", false, "sc.y", "        ");
+            if (rotated)
+                for (const char* pre : {"P", "Q"}) {
+                    vp = pre;
+                    unrotate(rl);
+                }
             for (int i = 0; i < nreg; ++i) {
                 const uint32_t c = off[i & (R - 1)] | ((i >> KB) ? gstep : 0u);
-                o << "        " << sets[k][1] << (rotated ? "[ga ^ " : "[g0 + ") << c << "u] = " << v(i) << ";\n";
+                const std::string at = std::string(rotated ? "[ga ^ " : "[g0 + ") + std::to_string(c) + "u]";
+                o << "        tile" << at << " = cf{P" << i << ".x, Q" << i << ".x}; tlam" << at << " = cf{P" << i
+                  << ".y, Q" << i << ".y};\n";
             }
         }
         vp = "v";
@@ -537,34 +533,149 @@ struct Gen {
     bool pending_reads = false;
     static constexpr int kMeasGroup = 4;
 
-    // top-level statements of generated code: a line at the stage's indent, or a
-    // block from such a line opening "{" to the matching closing line
-    static std::vector<std::string> statements(const std::string& code) {
-        std::vector<std::string> out;
-        std::istringstream in(code);
-        std::string line, cur;
-        int depth = 0;
-        while (std::getline(in, line)) {
-            cur += line + "\n";
-            for (char ch : line) depth += ch == '{' ? 1 : ch == '}' ? -1 : 0;
-            if (depth <= 0) {
-                out.push_back(cur);
-                cur.clear();
-                depth = 0;
-            }
-        }
-        if (!cur.empty()) out.push_back(cur);
-        return out;
+    // ------------------------------------------------- packed adjoint registers
+    // The adjoint stage keeps both states in float2 pairs: P<i> = (phi_i.x, lambda_i.x),
+    // Q<i> = (phi_i.y, lambda_i.y).  A U^dag op multiplies both states by the same
+    // coefficients, so each real multiply-add is one packed __ffma2_rn for the two.
+    static std::string splat(const std::string& e) { return "make_float2(" + e + ", " + e + ")"; }
+    struct PTerm {
+        std::string c;  // scalar coefficient expression
+        bool one;       // the coefficient is exactly 1 (no multiply)
+        std::string x;  // float2 operand
+    };
+    static std::string chain(const std::vector<PTerm>& t) {
+        if (t.empty()) return "make_float2(0.f, 0.f)";
+        std::string acc = t[0].one ? t[0].x : "__fmul2_rn(" + splat(t[0].c) + ", " + t[0].x + ")";
+        for (size_t i = 1; i < t.size(); ++i) acc = "__ffma2_rn(" + splat(t[i].c) + ", " + t[i].x + ", " + acc + ")";
+        return acc;
     }
-    // the two sets' code for one op, statement by statement in alternation (they
-    // have the same statements, register names aside); else one after the other
-    void interleave(const std::string& a, const std::string& b) {
-        const std::vector<std::string> sa = statements(a), sb = statements(b);
-        if (sa.size() != sb.size()) {
-            o << a << b;
+    // (P, Q) of a register times the complex k = (re, im) given as expressions
+    // (empty: a zero part; re_one: re is exactly 1)
+    void emit_pmul(const std::string& P, const std::string& Q, const std::string& re, bool re_one,
+                   const std::string& im, const std::string& ind) {
+        std::vector<PTerm> tp, tq;
+        if (!re.empty()) tp.push_back({re, re_one, "pa"}), tq.push_back({re, re_one, "qa"});
+        if (!im.empty()) tp.push_back({"-(" + im + ")", false, "qa"}), tq.push_back({im, false, "pa"});
+        o << ind << "{ const float2 pa = " << P << ", qa = " << Q << "; " << P << " = " << chain(tp) << "; " << Q
+          << " = " << chain(tq) << "; }\n";
+    }
+    // coefficient parts of entry k (op m, coefficient slot idx): literals, or the
+    // parameter block under run-time coefficients
+    void coef_parts(int m, int idx, CplxF k, std::string& re, bool& re_one, std::string& im) {
+        re_one = false;
+        if (p.rtc && !trivial_coef(k)) {
+            const std::string kn = kname(m, idx);
+            re = k.re == 0.f ? "" : kn + ".x";
+            im = k.im == 0.f ? "" : kn + ".y";
             return;
         }
-        for (size_t i = 0; i < sa.size(); ++i) o << sa[i] << sb[i];
+        re = k.re == 0.f ? "" : flit(k.re);
+        im = k.im == 0.f ? "" : flit(k.im);
+        re_one = k.re == 1.f;
+    }
+    // one U^dag member of the adjoint stage on the packed registers; returns true when
+    // it multiplied into the stage scalar sc (a phase on off-tile bits, both states)
+    bool member_packed(int m, const int* S) {
+        const DevOp& op = p.ops[m];
+        const int R = 1 << KB;
+        auto spos = [&](int lb) {
+            for (int q = 0; q < KB; ++q)
+                if (S[q] == lb) return q;
+            return -1;
+        };
+        auto P = [](int i) { return "P" + std::to_string(i); };
+        auto Q = [](int i) { return "Q" + std::to_string(i); };
+        if (op.kind == OPK_DIAG) {
+            int pos[4] = {-1, -1, -1, -1};
+            bool any_tile_nonstage = false, any_off = false, any_stage = false;
+            for (int t = 0; t < op.nq; ++t) {
+                if (op.lb[t] >= 0) {
+                    pos[t] = spos(op.lb[t]);
+                    if (pos[t] < 0) any_tile_nonstage = true;
+                    else any_stage = true;
+                } else {
+                    any_off = true;
+                }
+            }
+            std::ostringstream rt;
+            rt << "0u";
+            for (int t = 0; t < op.nq; ++t)
+                if (op.lb[t] < 0) rt << " | ((u32)((base >> " << op.gb[t] << ") & 1ull) << " << t << ")";
+            if (!any_stage && !any_tile_nonstage) {
+                o << "        sc = cmul(sc, a.ops[" << m << "].c[" << rt.str() << "]);\n";
+                return true;
+            }
+            if (!any_tile_nonstage && !any_off) {
+                for (int i = 0; i < (GS << KB); ++i) {
+                    int mi = 0;
+                    for (int t = 0; t < op.nq; ++t) mi |= ((i >> pos[t]) & 1) << t;
+                    const CplxF k{op.cf[mi].x, op.cf[mi].y};
+                    if (k.re == 1.f && k.im == 0.f) continue;
+                    std::string re, im;
+                    bool one;
+                    coef_parts(m, mi, k, re, one, im);
+                    emit_pmul(P(i), Q(i), re, one, im, "        ");
+                }
+                return false;
+            }
+            for (int j = 0; j < GS; ++j) {
+                o << "        { const u32 gj = g0 | " << (j ? deposit_value(S, KB, (uint32_t)NT) : 0u)
+                  << "u; (void)gj; const u32 mr = " << rt.str();
+                for (int t = 0; t < op.nq; ++t)
+                    if (op.lb[t] >= 0 && pos[t] < 0) o << " | (((gj >> " << op.lb[t] << ") & 1u) << " << t << ")";
+                o << ";\n";
+                for (int r = 0; r < R; ++r) {
+                    int mi = 0;
+                    for (int t = 0; t < op.nq; ++t)
+                        if (pos[t] >= 0) mi |= ((r >> pos[t]) & 1) << t;
+                    o << "          { const cf z = a.ops[" << m << "].c[mr | " << mi << "u];\n";
+                    emit_pmul(P((j << KB) + r), Q((j << KB) + r), "z.x", false, "z.y", "            ");
+                    o << "          }\n";
+                }
+                o << "        }\n";
+            }
+            return false;
+        }
+        // matrix op on stage positions
+        int pos[3] = {-1, -1, -1};
+        for (int t = 0; t < op.nq; ++t) pos[t] = spos(op.lb[t]);
+        const int dim = 1 << op.nq;
+        std::vector<int> I;
+        const std::vector<CplxF> M = op_matrix_f(op, &I);
+        int pmask = 0;
+        for (int t = 0; t < op.nq; ++t) pmask |= 1 << pos[t];
+        for (int j = 0; j < GS; ++j)
+            for (int e = 0; e < R; ++e) {
+                if (e & pmask) continue;
+                int ix[8];
+                for (int c = 0; c < dim; ++c) {
+                    int r = e;
+                    for (int t = 0; t < op.nq; ++t)
+                        if ((c >> t) & 1) r |= 1 << pos[t];
+                    ix[c] = (j << KB) + r;
+                }
+                o << "        {";
+                for (int c = 0; c < dim; ++c)
+                    o << " const float2 xp" << c << " = " << P(ix[c]) << ", xq" << c << " = " << Q(ix[c]) << ";";
+                o << "\n";
+                for (int r = 0; r < dim; ++r) {
+                    std::vector<PTerm> tp, tq;
+                    for (int c = 0; c < dim; ++c) {
+                        const CplxF k = M[r * dim + c];
+                        if (k.re == 0.f && k.im == 0.f) continue;
+                        std::string re, im;
+                        bool one;
+                        coef_parts(m, I[r * dim + c], k, re, one, im);
+                        const std::string xp = "xp" + std::to_string(c), xq = "xq" + std::to_string(c);
+                        if (!re.empty()) tp.push_back({re, one, xp}), tq.push_back({re, one, xq});
+                        if (!im.empty()) tp.push_back({"-(" + im + ")", false, xq}), tq.push_back({im, false, xp});
+                    }
+                    o << "          " << P(ix[r]) << " = " << chain(tp) << "; " << Q(ix[r]) << " = " << chain(tq)
+                      << ";\n";
+                }
+                o << "        }\n";
+            }
+        return false;
     }
 
     // warp sums of measurements cols[c0..c1) (at most 8, accumulators m<c0>..): a
@@ -632,10 +743,13 @@ struct Gen {
                 for (int r = 0; r < dim; ++r) {
                     const int code = op.slot[r];
                     if (code == INNER_ZERO) continue;
-                    const std::string l = "w" + std::to_string(reg_of(j, e, r));
-                    const std::string q = "v" + std::to_string(reg_of(j, e, op.perm[1 + r]));
-                    const std::string a = "(" + l + ".x * " + q + ".x + " + l + ".y * " + q + ".y)";
-                    const std::string b = "(" + l + ".x * " + q + ".y - " + l + ".y * " + q + ".x)";
+                    // lambda = (P.y, Q.y), phi = (P.x, Q.x) of the packed registers
+                    const std::string li = std::to_string(reg_of(j, e, r));
+                    const std::string qi = std::to_string(reg_of(j, e, op.perm[1 + r]));
+                    const std::string lx = "P" + li + ".y", ly = "Q" + li + ".y";
+                    const std::string qx = "P" + qi + ".x", qy = "Q" + qi + ".x";
+                    const std::string a = "(" + lx + " * " + qx + " + " + ly + " * " + qy + ")";
+                    const std::string b = "(" + lx + " * " + qy + " - " + ly + " * " + qx + ")";
                     o << "        " << acc << ((code & 2) ? " -= " : " += ") << ((code & 1) ? a : b) << ";\n";
                 }
             }
