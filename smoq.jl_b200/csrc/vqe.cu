@@ -42,50 +42,35 @@ namespace smoq {
 // lambda_k = sum_t c_t i^{ny} (-1)^{popc((k ^ x) & z)} phi_{k ^ x}; per block
 // the FP64 partial sums of Re(conj(phi_k) lambda_k) (partials[blockIdx.x])
 // and of |phi_k|^2 (partials[gridDim.x + blockIdx.x]), so the caller can
-// divide the energy by the norm of the state it was measured on.  A block takes
-// chunks of 2^CB consecutive amplitudes into shared memory: a term whose X mask
-// lies inside the chunk reads its partner there, the others read it from global
-// memory (coalesced: a fixed X mask keeps consecutive k consecutive).
+// divide the energy by the norm of the state it was measured on
 template <typename R>
 __global__ void __launch_bounds__(256) ham_apply_kernel(const typename CT<R>::T* phi, typename CT<R>::T* lam, int N,
                                                         const HamTerm* terms, int nterms, double* partials) {
     using C = typename CT<R>::T;
-    constexpr int CB = sizeof(R) == 4 ? 12 : 11;  // 32 KB of amplitudes
-    __shared__ C chunk[1 << CB];
-    const int cb = N < CB ? N : CB;
-    const uint32_t csize = 1u << cb;
-    const int64_t nchunks = ((int64_t)1 << N) >> cb;
+    const int64_t len = (int64_t)1 << N;
     double acc = 0, nrm = 0;
-    for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
-        const int64_t k0 = ch << cb;
-        __syncthreads();  // (the previous chunk's readers are done)
-        for (uint32_t i = threadIdx.x; i < csize; i += blockDim.x) chunk[i] = phi[k0 + i];
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < csize; i += blockDim.x) {
-            const int64_t k = k0 + i;
-            double lr = 0, li = 0;
-            for (int t = 0; t < nterms; ++t) {
-                const uint64_t x = terms[t].x;
-                const uint64_t j = (uint64_t)k ^ x;
-                const C p = (x >> cb) == 0 ? chunk[i ^ (uint32_t)x] : phi[j];
-                double s = terms[t].coef * ((__popcll(j & terms[t].z) & 1) ? -1.0 : 1.0);
-                const int yk = terms[t].ny & 3;
-                double pr = p.x, pi = p.y;
-                // multiply by i^yk
-                if (yk == 1) { const double tr = -pi; pi = pr; pr = tr; }
-                else if (yk == 2) { pr = -pr; pi = -pi; }
-                else if (yk == 3) { const double tr = pi; pi = -pr; pr = tr; }
-                lr += s * pr;
-                li += s * pi;
-            }
-            C o;
-            o.x = (R)lr;
-            o.y = (R)li;
-            lam[k] = o;
-            const C f = chunk[i];
-            acc += (double)f.x * lr + (double)f.y * li;  // Re(conj(phi) lambda)
-            nrm += (double)f.x * f.x + (double)f.y * f.y;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < len; k += (int64_t)gridDim.x * blockDim.x) {
+        double lr = 0, li = 0;
+        for (int t = 0; t < nterms; ++t) {
+            const uint64_t j = (uint64_t)k ^ terms[t].x;
+            const C p = phi[j];
+            double s = terms[t].coef * ((__popcll(j & terms[t].z) & 1) ? -1.0 : 1.0);
+            const int yk = terms[t].ny & 3;
+            double pr = p.x, pi = p.y;
+            // multiply by i^yk
+            if (yk == 1) { const double tr = -pi; pi = pr; pr = tr; }
+            else if (yk == 2) { pr = -pr; pi = -pi; }
+            else if (yk == 3) { const double tr = pi; pi = -pr; pr = tr; }
+            lr += s * pr;
+            li += s * pi;
         }
+        C o;
+        o.x = (R)lr;
+        o.y = (R)li;
+        lam[k] = o;
+        const C f = phi[k];
+        acc += (double)f.x * lr + (double)f.y * li;  // Re(conj(phi) lambda)
+        nrm += (double)f.x * f.x + (double)f.y * f.y;
     }
     __shared__ double red[2][8];
     for (int d = 16; d > 0; d >>= 1) {
