@@ -921,7 +921,7 @@ struct Gen {
 };
 
 // full source of the kernels for one pass
-std::string generate(const Pass& p, bool need_epi, int nbuf, int groups, int minb_add, std::string& err) {
+std::string generate_impl(const Pass& p, bool need_epi, int nbuf, int groups, int minb_add, std::string& err) {
     const int N = p.g.N;
     const TileGeom& g = p.g;
     const int T = g.T;
@@ -1107,7 +1107,7 @@ std::string generate(const Pass& p, bool need_epi, int nbuf, int groups, int min
 // full source of the compiled adjoint kernel of one backward pass: the tile pair
 // (phi, lambda) in shared memory by bulk copy, then the pass's stages on both
 // register sets, measurements added to the warps' partial rows, then both tiles back
-std::string generate_adjoint(const Pass& p, std::string& err) {
+std::string generate_adjoint_impl(const Pass& p, std::string& err) {
     const int N = p.g.N;
     const TileGeom& g = p.g;
     const int T = g.T;
@@ -1217,6 +1217,25 @@ std::string generate_adjoint(const Pass& p, std::string& err) {
          "    bulk_wait0();\n"
          "}\n";
     return o.str();
+}
+
+// the generators' failures (an inconsistent pass program) come back as errors,
+// never as exceptions through the C ABI
+std::string generate(const Pass& p, bool need_epi, int nbuf, int groups, int minb_add, std::string& err) {
+    try {
+        return generate_impl(p, need_epi, nbuf, groups, minb_add, err);
+    } catch (const std::exception& ex) {
+        err = ex.what();
+        return std::string();
+    }
+}
+std::string generate_adjoint(const Pass& p, std::string& err) {
+    try {
+        return generate_adjoint_impl(p, err);
+    } catch (const std::exception& ex) {
+        err = ex.what();
+        return std::string();
+    }
 }
 
 std::mutex g_mu;

@@ -885,9 +885,8 @@ struct GradPlan {
 // they are compiled here, on the planning thread, and loaded by the caller
 // fwd_ctx: also plan the forward (on fwd_ctx's options; a variational forward with jit 1);
 // max_ops: at most that many fused ops per backward pass (0: as many as fit)
-static void plan_gradient(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops, int n,
-                          const double* th, bool grad, GradPlan& gp, int jit = 0, smoq_ctx* fwd_ctx = nullptr,
-                          int max_ops = 0) {
+static void plan_gradient_impl(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops, int n,
+                               const double* th, bool grad, GradPlan& gp, int jit, smoq_ctx* fwd_ctx, int max_ops) {
     if ((gp.status = smoq_internal_ops_to_ir(N, ops, n, th, gp.ir))) {
         gp.error = "bad op list";
         return;
@@ -953,6 +952,17 @@ static void plan_gradient(int N, smoq_dtype dtype, int tile_bits, int low_bits, 
     }
     for (Pass& p : gp.passes)
         if ((gp.status = fuse_measurements(p.ops, gp.error))) return;
+}
+// (planning threads and the C entry points: a failure is a status, never an exception)
+static void plan_gradient(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops, int n,
+                          const double* th, bool grad, GradPlan& gp, int jit = 0, smoq_ctx* fwd_ctx = nullptr,
+                          int max_ops = 0) {
+    try {
+        plan_gradient_impl(N, dtype, tile_bits, low_bits, ops, n, th, grad, gp, jit, fwd_ctx, max_ops);
+    } catch (const std::exception& ex) {
+        gp.status = SMOQ_ERR_BADINPUT;
+        gp.error = ex.what();
+    }
 }
 
 static smoq_status vqe_run(smoq_ctx* ctx, int N, smoq_dtype dtype, const smoq_op* ops, int n, int n_params,
