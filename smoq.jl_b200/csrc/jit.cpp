@@ -815,6 +815,7 @@ struct Gen {
             return true;
         }
         if (op.kind == OPK_REALTAB) {
+            if (op.aux2 == 0) return false;  // no tables: a marker op (the epilogue's anchor)
             for (int i = 0; i < (GS << KB); ++i) {
                 uint32_t c = (i >> KB) ? gstep : 0u;
                 for (int q = 0; q < KB; ++q)

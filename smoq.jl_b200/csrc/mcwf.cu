@@ -38,9 +38,12 @@ struct DJump {
     double gamma;
 };
 
+constexpr int kJumpRows = 256;  // block rows of the jump kernel (jumpers per step: typically dozens)
+
 __global__ void mcwf_decide_kernel(int B, int64_t tiles_per_state, int npop, const double* partials,
                                    const DJump* ops, int nops, double dt, uint64_t seed, uint64_t traj_offset,
-                                   uint64_t step, int32_t* jump, double* scale, int32_t* counts) {
+                                   uint64_t step, int32_t* jump, double* scale, int32_t* counts,
+                                   int32_t* jumpers, int32_t* njump) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= B) return;
     // FP64 sums over this trajectory's tiles, in tile order
@@ -80,20 +83,28 @@ __global__ void mcwf_decide_kernel(int B, int64_t tiles_per_state, int npop, con
             }
             new_norm = (ops[chosen].type == 0 || ops[chosen].type == 1) ? chosen_ev : nrm;
             counts[b] += 1;
+            jumpers[atomicAdd(njump, 1)] = b;  // (the list order does not matter)
         }
     }
     jump[b] = chosen;
     scale[b] = 1.0 / sqrt(new_norm);
 }
 
+// the chosen jump applied to the trajectories on the step's jumper list: block row y
+// takes list entries y, y + gridDim.y, ... (a few dozen jumpers per step among
+// thousands of trajectories: the grid stays small)
 template <typename R>
-__global__ void mcwf_jump_kernel(typename CT<R>::T* psi, int N, const int32_t* jump, const DJump* ops) {
+__global__ void mcwf_jump_kernel(typename CT<R>::T* psi, int N, const int32_t* jump, const DJump* ops,
+                                 const int32_t* jumpers, const int32_t* njump, int B) {
     using C = typename CT<R>::T;
-    const int b = blockIdx.y;
+    const int nj = *njump;
+    for (int e = blockIdx.y; e < nj; e += gridDim.y) {
+    const int b = jumpers[e];
+    if (b < 0 || b >= B) continue;
     const int o = jump[b];
-    if (o < 0) return;
+    if (o < 0) continue;
     const int64_t len = (int64_t)1 << N;
-    C* s = psi + b * len;
+    C* s = psi + (int64_t)b * len;
     const int q = ops[o].qubit, ty = ops[o].type;
     const uint64_t m = 1ull << q;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < (len >> 1);
@@ -112,6 +123,7 @@ __global__ void mcwf_jump_kernel(typename CT<R>::T* psi, int N, const int32_t* j
             s[i0] = c;
             s[i1] = a;
         }
+    }
     }
 }
 
@@ -242,6 +254,9 @@ extern "C" smoq_status smoq_mcwf_run(smoq_plan* plan, smoq_state* st, const smoq
     MCK(buf.alloc(&d_scale, B));
     MCK(buf.alloc(&d_jump, B));
     MCK(buf.alloc(&d_counts, B));
+    int32_t *d_jumpers, *d_njump;
+    MCK(buf.alloc(&d_jumpers, B));
+    MCK(buf.alloc(&d_njump, 1));
     MCK(buf.alloc(&d_ops, dj.size()));
     MCK(buf.alloc(&d_rec, (size_t)nrec * B * nobs));
     MCK(buf.alloc(&d_mean, (size_t)nrec * nobs));
@@ -260,10 +275,29 @@ extern "C" smoq_status smoq_mcwf_run(smoq_plan* plan, smoq_state* st, const smoq
     sc.diag = true;
     prog.push_back(sc);
     prog.insert(prog.end(), step.begin(), step.end());
+    // The no-jump decay is a product of one-qubit real diagonals (diag(bq, a) per
+    // qubit, times fu).  The compiled complex64 kernels fold such diagonals into their
+    // stage phases, so there they enter as diagonal gates and the table op stays only
+    // as a marker that keeps the norm and population epilogue in the step's last
+    // pass; the other engines apply the byte tables in one sweep.
+    const bool fold_decay = st->dtype == SMOQ_C64 && (ctx->engine == 3 || (ctx->engine < 0 && jit_available()));
+    if (fold_decay) {
+        double g = fu;
+        for (int q = 0; q < N; ++q) {
+            if (a[q] == 1.0 && bq[q] == 1.0) continue;
+            const cd m[4] = {bq[q] * g, 0.0, 0.0, a[q] * g};
+            g = 1.0;
+            prog.push_back(gate_1q(q, m));
+        }
+        if (g != 1.0) {  // (no population decay: the uniform factor alone)
+            const cd m[4] = {g, 0.0, 0.0, g};
+            prog.push_back(gate_1q(0, m));
+        }
+    }
     GateIR dec;
     dec.special = OPK_REALTAB;
     dec.aux = d_tabs;
-    dec.aux2 = ntab;
+    dec.aux2 = fold_decay ? 0 : ntab;
     dec.diag = true;
     prog.push_back(dec);
 
@@ -305,14 +339,17 @@ extern "C" smoq_status smoq_mcwf_run(smoq_plan* plan, smoq_state* st, const smoq
     int r = 1;
     for (int s = 0; s < steps; ++s) {
         if (smoq_status e = smoq_internal_rerun(ctx, st, handle, &ep)) return e;
+        MCK(cudaMemsetAsync(d_njump, 0, sizeof(int32_t), ctx->stream));
         mcwf_decide_kernel<<<(B + 127) / 128, 128, 0, ctx->stream>>>(B, tps, ep.npop, d_part, d_ops, nops, dt, seed,
                                                                      traj_offset, (uint64_t)s, d_jump, d_scale,
-                                                                     d_counts);
-        dim3 jg(jump_grid, B);
+                                                                     d_counts, d_jumpers, d_njump);
+        dim3 jg(jump_grid, std::min(B, kJumpRows));
         if (dtype == SMOQ_C64)
-            mcwf_jump_kernel<float><<<jg, 256, 0, ctx->stream>>>((float2*)st->ptr, N, d_jump, d_ops);
+            mcwf_jump_kernel<float><<<jg, 256, 0, ctx->stream>>>((float2*)st->ptr, N, d_jump, d_ops, d_jumpers,
+                                                                 d_njump, B);
         else
-            mcwf_jump_kernel<double><<<jg, 256, 0, ctx->stream>>>((double2*)st->ptr, N, d_jump, d_ops);
+            mcwf_jump_kernel<double><<<jg, 256, 0, ctx->stream>>>((double2*)st->ptr, N, d_jump, d_ops, d_jumpers,
+                                                                  d_njump, B);
         ctx->launches += 2;
         MCK(cudaGetLastError());
         if ((s + 1) % record_every == 0) {
