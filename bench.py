@@ -233,6 +233,52 @@ def _events(torch, stream):
     return e0, e1
 
 
+def default_geometry_record(S, local, N, gates, neel, tsteps, gate_apps, steps, peak):
+    """The headline evolution on a second context whose plan keeps the default fused-pass
+    geometry (tile 13, low bits 5; SMOQ_OPT_AUTOTUNE 2: the per-pass kernel variants are
+    still tuned): gate-apps/s over `steps` evolutions and the per-pass HBM fraction, beside
+    the geometry the autotuner chose for the headline (fewer passes, more gates each)."""
+    import torch
+    ctx = S.Context(local)
+    try:
+        ctx.set_option(S._lib.OPT_TILE_BITS_C64, 13)
+        ctx.set_option(S._lib.OPT_LOW_BITS_C64, 5)
+        ctx.set_option(S._lib.OPT_AUTOTUNE, 2)
+        plan = S.TrotterPlan(ctx, N, gates, order=2, dtype=S.C64)
+        st = S.CuState(ctx, N, S.C64, basis=None)
+        stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+
+        def step():
+            st.set_basis(neel)
+            return plan.run(st, tsteps, RECORD_EVERY)
+        for _ in range(2):
+            step()
+        ctx.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        ctx.set_option(S._lib.OPT_USE_GRAPHS, 0)
+        ctx.set_option(S._lib.OPT_KERNEL_TIMING, 1)
+        ctx.reset_counters()
+        step()
+        ctx.synchronize()
+        kc = ctx.counters()
+        avg_ms = kc["tile_ms"] / max(1, kc["tile_passes"])
+        achieved = kc["tile_bytes"] / max(1, kc["tile_passes"]) / (avg_ms * 1e-3) / 1e9
+        st.close()
+        plan.close()
+        return {"tile_bits_c64": 13, "low_bits_c64": 5, "autotune": "variants only",
+                "value": gate_apps * steps / (ms * 1e-3), "unit": "gate-apps/s", "ms_per_step": ms / steps,
+                "tile_passes_per_step": kc["tile_passes"], "avg_launch_ms": avg_ms,
+                "roofline_achieved_gbs": achieved, "roofline_frac": achieved / peak}
+    finally:
+        ctx.close()
+
+
 def vqe_measure(ctx, steps, warmup, B=8):
     """VQE gradient throughput on the gradient configuration: TFIM N=24, 12 layers of
     [Ry all; Rz all; CZ ladder] (852 gates, 576 parameters).  Batched complex64
@@ -829,6 +875,12 @@ def main():
     # e2e through the C ABI with host buffers
     e2e_ms = timed(e2e_step, args.steps)
 
+    # the same evolution with the default geometry, when the autotuner chose another
+    default_geom = None
+    if rank == 0 and ws == 1 and not args.tile_bits and not args.low_bits and args.autotune != 0 \
+            and geom != (13, 5, None):
+        default_geom = default_geometry_record(S, local, N, gates, neel, tsteps, gate_apps, args.steps, peak)
+
     per_rank_apps = gate_apps * args.steps
     value = whole_job_rate(per_rank_apps, ws, ms)
     e2e_value = whole_job_rate(per_rank_apps, ws, e2e_ms)
@@ -892,6 +944,7 @@ def main():
                         "d2h_bytes_per_step": int(8 * N * (tsteps // RECORD_EVERY + 1))},
                 "gpu_launches": int(launches),
                 "clocks": clk,
+                "default_geometry": default_geom,
                 "vqe": vqe,
                 "published_comparison": published,
                 "other_workloads": extras}

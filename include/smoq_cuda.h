@@ -82,8 +82,8 @@ enum {
                                      compiled pass kernel's variants (register groups per thread, CTAs
                                      per SM, one or two tile buffers; bit-identical results) and keep
                                      the fastest; choices are cached per (GPU, program), across
-                                     processes in the file SMOQ_TUNE_CACHE names if set; 0 = the
-                                     options' settings */
+                                     processes in the file SMOQ_TUNE_CACHE names if set; 2 = (b) only,
+                                     with the geometry the options set; 0 = the options' settings */
     SMOQ_OPT_FUSION_DEPTH = 14    /* No counterpart in the reference.  Max fused ops per pass: a longer
                                      pass is split into consecutive passes of the same tile (0 =
                                      default, as many as fit); applies to gate sequences, plans and
@@ -525,7 +525,8 @@ typedef struct {
  * 2 = two tile buffers per CTA (SMOQ_OPT_JIT_BUFFERS 2), 4 = run-time coefficients (the form
  * the complex64 forward of smoq_energy_grad compiles: gate coefficients passed per launch),
  * 8 = one register group per thread (SMOQ_OPT_JIT_GROUPS 1), 16 = the generated source of the
- * first pass in msg (nothing compiled).  *n_compiled = kernels compiled; msg gets "ok" (or the
+ * first pass in msg (nothing compiled; with 32, the sources of every pass one after another,
+ * *n_compiled = their count).  *n_compiled = kernels compiled; msg gets "ok" (or the
  * report) or the first error.  SMOQ_ERR_UNSUPPORTED when NVRTC is not available. */
 smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops, int n,
                                     const double* theta, int flags, int* n_compiled, char* msg, int msg_len);

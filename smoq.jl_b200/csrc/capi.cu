@@ -524,7 +524,11 @@ smoq_status smoq_ctx_set_option(smoq_ctx* ctx, int option, long long v) {
             ctx->jit_buffers = (int)v;
             break;
         case SMOQ_OPT_VQE_RESIDENT: ctx->vqe_resident = v != 0; break;
-        case SMOQ_OPT_AUTOTUNE: ctx->autotune = v != 0; break;
+        case SMOQ_OPT_AUTOTUNE:
+            if (v < 0 || v > 2) return fail(ctx, SMOQ_ERR_BADINPUT, "autotune must be 0, 1 or 2");
+            ctx->autotune = v != 0;
+            ctx->tune_geometry = v == 1;
+            break;
         case SMOQ_OPT_FUSION_DEPTH:
             if (v < 0 || v > 1000000) return fail(ctx, SMOQ_ERR_BADINPUT, "fusion depth must be >= 0");
             ctx->fusion_depth = (int)v;
@@ -859,7 +863,7 @@ smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tbits, int lbit
     if (smoq_status s = ops_to_ir(nullptr, N, ops, n, theta, ir)) return s;
     std::vector<Pass> pl;
     try {
-        if (flags & ~(1 | 2 | 4 | 8 | 16)) {
+        if (flags & ~(1 | 2 | 4 | 8 | 16 | 32)) {
             say("unknown flag");
             return SMOQ_ERR_BADINPUT;
         }
@@ -872,13 +876,15 @@ smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tbits, int lbit
     for (const Pass& p : pl) {
         if (!p.want_jit) continue;
         std::string why, info;
-        if (flags & 16) {  // the generated source of the first compiled pass
+        if (flags & 16) {  // the generated source of the first compiled pass (32: of every pass)
             if (!jit_pass_source(p, (flags & 2) ? 2 : 1, (flags & 8) ? 1 : 2, info, why)) {
                 say(why);
                 return SMOQ_ERR_BADINPUT;
             }
-            *n_compiled = 1;
-            say(info);
+            ++*n_compiled;
+            report += info;
+            if (flags & 32) continue;
+            say(report);
             return SMOQ_OK;
         }
         if (!jit_check_pass(p, (flags & 2) ? 2 : 1, (flags & 8) ? 1 : 2, why, nullptr, verbose ? &info : nullptr)) {
@@ -888,7 +894,7 @@ smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tbits, int lbit
         report += info;
         ++*n_compiled;
     }
-    say(verbose ? report : std::string("ok"));
+    say(verbose || (flags & 16) ? report : std::string("ok"));
     return SMOQ_OK;
 }
 
@@ -1222,7 +1228,8 @@ std::map<uint64_t, int> g_geometry;  // guarded by g_tune_mu
 
 static smoq_status choose_geometry(smoq_plan* P, const std::vector<GateIR>& all) {
     smoq_ctx* ctx = P->ctx;
-    if (!ctx->autotune || P->dtype != SMOQ_C64 || P->N < kTuneMinN || engine_for(ctx, true, P->dtype) != 3)
+    if (!ctx->autotune || !ctx->tune_geometry || P->dtype != SMOQ_C64 || P->N < kTuneMinN ||
+        engine_for(ctx, true, P->dtype) != 3)
         return SMOQ_OK;
     // key: device, N and the gate pattern (qubits, diagonal or not) of the block
     uint64_t key = device_hash(ctx->device) ^ 0x9E3779B97F4A7C15ull;

@@ -368,13 +368,27 @@ struct Gen {
             for (int r = 0; r < R; ++r)
                 if (need[r]) pend[r] = one;
         };
-        auto flush = [&]() { flush_where(std::vector<bool>(R, true)); };
         auto stage_pos = [&](int lb) {
             for (int q = 0; q < KB; ++q)
                 if (S[q] == lb) return q;
             return -1;
         };
-        for (int m : members) {
+        // The phase a pattern still has pending at the stage's end goes, where that costs
+        // less, into the row of the last member that mixes the pattern instead of a flush
+        // at the end: a dry run of the members (its code discarded) finds those members
+        // and the final phases; the second run emits.
+        Absorb ab;
+        ab.last.assign(R, -1);
+        ab.taken.assign(R, false);
+        std::ostringstream kept = std::move(o);
+        for (int run = 0; run < 2; ++run) {
+            ab.dry = run == 0;
+            if (ab.dry) o = std::ostringstream();
+            else o = std::move(kept);
+            std::fill(pend.begin(), pend.end(), one);
+            scal = false;
+            for (size_t at = 0; at < members.size(); ++at) {
+            const int m = members[at];
             const DevOp& op = p.ops[m];
             int pm = 0;
             bool on_stage = op.nq >= 1;
@@ -392,6 +406,12 @@ struct Gen {
                 continue;
             }
             const bool diagonal = op.kind == OPK_DIAG || op.kind == OPK_STATESCALE || op.kind == OPK_REALTAB;
+            if (!diagonal && !p.rtc && on_stage) {
+                member_through(m, (int)at, S, gstep, pend, ab);
+                continue;
+            }
+            if (!diagonal && pm && ab.dry)  // a flushing member: what it mixes is not absorbed
+                std::fill(ab.last.begin(), ab.last.end(), -2);
             if (!diagonal) {
                 const int dim = 1 << op.nq;
                 std::vector<bool> iso(dim, false);
@@ -416,8 +436,14 @@ struct Gen {
                 if (pm) flush_where(need);
             }
             scal |= member(m, S, gstep, scal);
+            }
+            if (ab.dry) ab.fin = pend;
         }
-        flush();
+        {
+            std::vector<bool> rest(R);
+            for (int r = 0; r < R; ++r) rest[r] = !ab.taken[r];
+            flush_where(rest);
+        }
         if (scal)
             for (int i = 0; i < nreg; ++i) o << "        " << v(i) << " = cmul(" << scn << ", " << v(i) << ");\n";
         if (rotated) unrotate(rl);  // conditional swaps are involutions
@@ -427,6 +453,139 @@ struct Gen {
             else o << "        tile[g0 + " << c << "u] = " << v(i) << ";\n";
         }
         o << "    }\n    __syncthreads();\n";
+    }
+
+    // FP32 multiplies one coefficient costs per output amplitude: none for 0, +-1, +-i
+    // (a copy or a swap of parts), 2 for a real or imaginary one, 4 for a general one
+    static int coef_cost(CplxF k) {
+        if (trivial_coef(k)) return 0;
+        return (k.re == 0.f || k.im == 0.f) ? 2 : 4;
+    }
+
+    // What the dry run of a stage's members learns: per stage pattern the position of
+    // the last member that mixes it (-2: a member that flushes) and the phases pending
+    // at the stage's end; the emitting run marks the patterns whose final phase went into
+    // a member row (taken), which the end of the stage then skips.
+    struct Absorb {
+        bool dry = true;
+        std::vector<int> last;
+        std::vector<std::complex<double>> fin;
+        std::vector<bool> taken;
+    };
+
+    // A literal matrix member on stage bits under the stage's pending phases P (one per
+    // stage pattern).  For each pattern of the other stage bits (the "rest") it takes the
+    // cheaper of two exact forms: apply the pending phases of the member's non-identity
+    // rows first (a flush), then M; or leave every phase pending and apply P^-1 M P, the
+    // member moved through the phases (entry (r, c) times p_c / p_r: M's diagonal stays as
+    // it is, so a split rotation's real cosines stay real, and the flush disappears).
+    // Where this member is the last to mix a pattern, the pattern's phase at the stage's
+    // end may go into the member's row for it (row times that phase) instead of a flush
+    // at the end, when the row costs less than the row plus the flush.  Coefficients are
+    // formed in FP64 and rounded once.
+    void member_through(int m, int at, const int* S, uint32_t gstep, std::vector<std::complex<double>>& pend,
+                        Absorb& ab) {
+        using cd = std::complex<double>;
+        const DevOp& op = p.ops[m];
+        const int dim = 1 << op.nq, R = 1 << KB;
+        int pos[3] = {-1, -1, -1}, pmask = 0;
+        for (int t = 0; t < op.nq; ++t) {
+            for (int q = 0; q < KB; ++q)
+                if (S[q] == op.lb[t]) pos[t] = q;
+            pmask |= 1 << pos[t];
+        }
+        const std::vector<CplxF> M = op_matrix_f(op);
+        const cd one(1.0, 0.0);
+        auto rnd = [](cd z) { return CplxF{(float)z.real(), (float)z.imag()}; };
+        std::vector<bool> iso(dim, false);  // rows and columns e_k: the member leaves pattern k alone
+        for (int k = 0; k < dim; ++k) {
+            bool e = M[k * dim + k].re == 1.f && M[k * dim + k].im == 0.f;
+            for (int j = 0; j < dim && e; ++j)
+                if (j != k) {
+                    const CplxF a = M[k * dim + j], b = M[j * dim + k];
+                    e = a.re == 0.f && a.im == 0.f && b.re == 0.f && b.im == 0.f;
+                }
+            iso[k] = e;
+        }
+        for (int e = 0; e < R; ++e) {
+            if (e & pmask) continue;
+            int pat[8];
+            for (int c = 0; c < dim; ++c) {
+                pat[c] = e;
+                for (int t = 0; t < op.nq; ++t)
+                    if ((c >> t) & 1) pat[c] |= 1 << pos[t];
+            }
+            // the moved-through member, its cost, and the flush form's cost
+            std::vector<cd> Mt(dim * dim);
+            int cost_through = 0, cost_flush = 0;
+            // a zero pending factor (a projector) has no P^-1; near-zero ones take the
+            // flush form too (no FP32 coefficients scaled by their inverse)
+            bool invertible = true;
+            for (int c = 0; c < dim; ++c) invertible &= std::abs(pend[pat[c]]) > 1e-6;
+            for (int r = 0; r < dim && invertible; ++r)
+                for (int c = 0; c < dim; ++c) {
+                    const CplxF k = M[r * dim + c];
+                    cost_flush += coef_cost(k);
+                    cd ratio = pend[pat[c]] / pend[pat[r]];
+                    if (std::abs(ratio - one) < 1e-15) ratio = one;
+                    Mt[r * dim + c] = cd(k.re, k.im) * ratio;
+                    cost_through += coef_cost(rnd(Mt[r * dim + c]));
+                }
+            for (int c = 0; c < dim; ++c)
+                if (!iso[c] && pend[pat[c]] != one) cost_flush += coef_cost(rnd(pend[pat[c]]));
+            if (!invertible) cost_through = cost_flush + 1;  // the flush form
+            const bool through = cost_through <= cost_flush;
+            // the rows to emit (FP64), with the final phases of the patterns this member
+            // mixes last folded in where that is cheaper
+            std::vector<cd> A(dim * dim);
+            for (int k = 0; k < dim * dim; ++k) A[k] = through ? Mt[k] : cd(M[k].re, M[k].im);
+            for (int r = 0; r < dim; ++r) {
+                if (iso[r]) continue;
+                if (ab.dry) {
+                    ab.last[pat[r]] = at;
+                    continue;
+                }
+                const cd f = ab.fin[pat[r]];
+                if (ab.last[pat[r]] != at || f == one) continue;
+                int cost_row = coef_cost(rnd(f)), cost_abs = 0;
+                for (int c = 0; c < dim; ++c) {
+                    cost_row += coef_cost(rnd(A[r * dim + c]));
+                    cost_abs += coef_cost(rnd(A[r * dim + c] * f));
+                }
+                if (cost_abs > cost_row) continue;
+                for (int c = 0; c < dim; ++c) A[r * dim + c] *= f;
+                ab.taken[pat[r]] = true;
+            }
+            for (int j = 0; j < GS; ++j) {
+                int ix[8];
+                for (int c = 0; c < dim; ++c) ix[c] = (j << KB) + pat[c];
+                if (!through)
+                    for (int c = 0; c < dim; ++c) {
+                        const cd z = pend[pat[c]];
+                        if (iso[c] || z == one) continue;
+                        std::string re, im;
+                        cmac_terms({{rnd(z), v(ix[c])}}, re, im);
+                        o << "        " << v(ix[c]) << " = cf{" << re << ", " << im << "};\n";
+                    }
+                o << "        {";
+                for (int c = 0; c < dim; ++c) o << " const cf x" << c << " = " << v(ix[c]) << ";";
+                o << "\n";
+                for (int r = 0; r < dim; ++r) {
+                    std::vector<std::pair<CplxF, std::string>> terms;
+                    for (int c = 0; c < dim; ++c) {
+                        const CplxF k = rnd(A[r * dim + c]);
+                        if (k.re != 0.f || k.im != 0.f) terms.push_back({k, "x" + std::to_string(c)});
+                    }
+                    std::string re, im;
+                    cmac_terms(terms, re, im);
+                    o << "          " << v(ix[r]) << " = cf{" << re << ", " << im << "};\n";
+                }
+                o << "        }\n";
+            }
+            if (!through)
+                for (int c = 0; c < dim; ++c)
+                    if (!iso[c]) pend[pat[c]] = one;
+        }
     }
 
     // registers loaded at stage bits r ^ rot -> canonical order (and back)

@@ -248,6 +248,7 @@ struct smoq_ctx {
     int jit_groups = 2;                // compiled pass kernels: 16-amplitude register groups per thread
     bool vqe_resident = true;          // many-circuit VQE: small circuits in one shared-memory launch
     bool autotune = true;              // tune plan geometry and compiled-kernel variants at plan upload
+    bool tune_geometry = true;         // ... the geometry too (else the options' tile width, low bits, depth)
     int fusion_depth = 0;              // max fused ops per pass (0 = as many as fit)
     std::string tune_report;           // the tuner's per-pass timings and choices
     long long launches = 0;            // kernels launched by this ctx

@@ -952,19 +952,21 @@ def debug_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtype: int =
 
 def debug_compile_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtype: int = C64, tile_bits: int = 13,
                        low_bits: int = 5, verbose: bool = False, buffers: int = 1, groups: int = 2,
-                       rtc: bool = False, source: bool = False):
+                       rtc: bool = False, source: bool = False, all_sources: bool = False):
     """Host-only: plan `ops` for the plan compiler (engine 3) and compile every pass
     kernel with NVRTC (no GPU, nothing loaded).  Returns (status, n_compiled, message);
     with verbose the message is the compiler's register/spill report.  rtc: the
     run-time-coefficient form (a variational forward); source: the message is the
-    generated source of the first pass (nothing compiled)."""
+    generated source of the first pass (nothing compiled); all_sources: the sources of
+    every pass, one after another."""
     arr = circuit_to_c_ops(ops)
     th = np.ascontiguousarray(theta if theta is not None else np.zeros(1), dtype=np.float64)
     n = C.c_int()
-    size = 1 << (22 if source else 16)
+    source = source or all_sources
+    size = 1 << (26 if all_sources else 22 if source else 16)
     msg = C.create_string_buffer(size)
     flags = (1 if verbose else 0) | (2 if buffers == 2 else 0) | (4 if rtc else 0) | (8 if groups == 1 else 0) \
-        | (16 if source else 0)
+        | (16 if source else 0) | (32 if all_sources else 0)
     st = lib.smoq_debug_compile_plan(N, dtype, tile_bits, low_bits, arr, len(ops), dptr(th), flags, C.byref(n),
                                      msg, size)
     return st, n.value, msg.value.decode(errors="replace")

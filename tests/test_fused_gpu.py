@@ -235,3 +235,41 @@ def test_fusion_depth_cap_keeps_the_state(ctx, depth):
         plan.close()
     finally:
         ctx.set_option(S._lib.OPT_FUSION_DEPTH, 0)
+
+
+def test_autotune_modes_geometry_and_variants():
+    """SMOQ_OPT_AUTOTUNE on a Trotter plan of N = 20 (compiled kernels): 1 times the
+    candidate geometries and then the pass variants; 2 keeps the geometry the options
+    set (here low bits 4) and tunes only the variants; both evolve to the oracle's
+    state; values outside 0..2 are refused"""
+    if not S.jit_available():
+        pytest.skip("NVRTC not available")
+    N = 20
+    h = np.random.default_rng(11).uniform(-1, 1, size=N)
+    arr, n = O.precompute_trotter_gates([(i, i + 1, 1.0, 1.0, 0.5) for i in range(1, N)],
+                                        [(i, 0.0, 0.0, float(h[i - 1])) for i in range(1, N + 1)], 0.025)
+    gl = O.gates_to_list(arr, n)
+    ref = O.zero_state(N, 0b10101010101010101010)
+    both = O.make_gates(gl + gl[::-1])
+    for _ in range(2):
+        O.trotter_step(ref, both, 2 * n, N)
+    reports = {}
+    for mode in (1, 2):
+        c = S.Context(0)
+        try:
+            with pytest.raises(S.SmoqError):
+                c.set_option(S._lib.OPT_AUTOTUNE, 3)
+            c.set_option(S._lib.OPT_AUTOTUNE, mode)
+            if mode == 2:
+                c.set_option(S._lib.OPT_LOW_BITS_C64, 4)
+            plan = S.TrotterPlan(c, N, [S.FastTrotterGate(i, U) for i, U in gl], order=2, dtype=S.C64)
+            st = S.CuState(c, N, S.C64, basis=0b10101010101010101010)
+            plan.step(st, 2)
+            assert rel(st.download().astype(complex), ref) < 1e-5
+            reports[mode] = c.tune_report()
+            st.close()
+            plan.close()
+        finally:
+            c.close()
+    assert "-> geometry" in reports[1] and reports[1].count("geometry tile") >= 2
+    assert "geometry" not in reports[2] and "-> v" in reports[2]
