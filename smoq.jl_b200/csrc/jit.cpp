@@ -1080,6 +1080,35 @@ struct Gen {
     }
 };
 
+// The tile's high qubits hb[0..H) (ascending) as runs of consecutive bit positions:
+// the generated address code moves a run with one shift and mask instead of one
+// bit at a time.
+std::vector<std::pair<int, int>> high_runs(const TileGeom& g) {  // (first m, length)
+    std::vector<std::pair<int, int>> runs;
+    for (int m = 0; m < g.H; ++m) {
+        if (!runs.empty() && g.hb[m] == g.hb[runs.back().first] + runs.back().second) ++runs.back().second;
+        else runs.push_back({m, 1});
+    }
+    return runs;
+}
+// "var |= bits of src deposited at the high positions" lines
+std::string deposit_high(const TileGeom& g, const char* var, const char* src) {
+    std::ostringstream o;
+    for (const auto& r : high_runs(g))
+        o << "    " << var << " |= (u64)((" << src << " >> " << r.first << ") & " << ((1u << r.second) - 1)
+          << "u) << " << g.hb[r.first] << ";\n";
+    return o.str();
+}
+// "base = base with zero bits inserted at the high positions" lines (ascending runs)
+std::string insert_high_zeros(const TileGeom& g) {
+    std::ostringstream o;
+    for (const auto& r : high_runs(g)) {
+        const int p = g.hb[r.first], k = r.second;
+        o << "    base = ((base >> " << p << ") << " << (p + k) << ") | (base & ((1ull << " << p << ") - 1));\n";
+    }
+    return o.str();
+}
+
 // full source of the kernels for one pass
 std::string generate_impl(const Pass& p, bool need_epi, int nbuf, int groups, int minb_add, std::string& err) {
     const int N = p.g.N;
@@ -1109,15 +1138,15 @@ std::string generate_impl(const Pass& p, bool need_epi, int nbuf, int groups, in
     o << "__device__ __forceinline__ u64 tile_base(i64 t, i64& b) {\n"
          "    b = t >> NSHIFT;\n"
          "    u64 base = (u64)(t & ((1ll << NSHIFT) - 1)) << LB;\n";
-    for (int m = 0; m < g.H; ++m) o << "    base = ins0(base, " << g.hb[m] << ");\n";
+    o << insert_high_zeros(g);
     o << "    return base;\n}\n";
     o << "__device__ __forceinline__ u64 seg_off(u64 base, u32 s) {\n    u64 off = base;\n";
-    for (int m = 0; m < g.H; ++m) o << "    off |= (u64)((s >> " << m << ") & 1u) << " << g.hb[m] << ";\n";
+    o << deposit_high(g, "off", "s");
     o << "    return off;\n}\n";
     o << "__device__ __forceinline__ float realtab(const DevOp& op, u64 base, u32 j) {\n"
          "    u64 gi = base | (j & ((1u << LB) - 1));\n"
          "    const u32 h = j >> LB;\n";
-    for (int m = 0; m < g.H; ++m) o << "    gi |= (u64)((h >> " << m << ") & 1u) << " << g.hb[m] << ";\n";
+    o << deposit_high(g, "gi", "h");
     o << "    const double* tab = (const double*)op.aux;\n"
          "    double f = 1.0;\n"
          "    for (int k = 0; k < (int)op.aux2; ++k) f *= tab[k * 256 + ((gi >> (8 * k)) & 255)];\n"
@@ -1298,10 +1327,10 @@ std::string generate_adjoint_impl(const Pass& p, std::string& err) {
     o << "__device__ __forceinline__ u64 tile_base(i64 t, i64& b) {\n"
          "    b = t >> NSHIFT;\n"
          "    u64 base = (u64)(t & ((1ll << NSHIFT) - 1)) << LB;\n";
-    for (int m = 0; m < g.H; ++m) o << "    base = ins0(base, " << g.hb[m] << ");\n";
+    o << insert_high_zeros(g);
     o << "    return base;\n}\n";
     o << "__device__ __forceinline__ u64 seg_off(u64 base, u32 s) {\n    u64 off = base;\n";
-    for (int m = 0; m < g.H; ++m) o << "    off |= (u64)((s >> " << m << ") & 1u) << " << g.hb[m] << ";\n";
+    o << deposit_high(g, "off", "s");
     o << "    return off;\n}\n";
     o << "extern \"C\" __global__ void __launch_bounds__(NT, " << MINB << ") smoq_adj_e0(const AdjArgs A, const Coefs K) {\n"
          "    const TileArgs& a = A.a;\n"
