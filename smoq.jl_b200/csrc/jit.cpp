@@ -1162,6 +1162,17 @@ std::string generate_impl(const Pass& p, bool need_epi, int nbuf, int groups, in
          "    for (u32 s = threadIdx.x; s < (1u << HB); s += NT)\n"
          "        bulk_g2s(buf + ((u64)s << LB), gs + seg_off(base, s), 8u << LB, bar);\n"
          "}\n";
+    // a hint to bring tile t's segments into L2 while the current tile's stages run
+    // (the one-buffer kernels: the next bulk load then reads L2); t is a valid tile,
+    // so every segment lies inside the state, 16-byte aligned, a multiple of 16 bytes
+    o << "__device__ __forceinline__ void prefetch_tile(const TileArgs& a, i64 t) {\n"
+         "    i64 b;\n"
+         "    const u64 base = tile_base(t, b);\n"
+         "    const cf* gs = (const cf*)a.psi + b * a.state_len;\n"
+         "    for (u32 s = threadIdx.x; s < (1u << HB); s += NT)\n"
+         "        asm volatile(\"cp.async.bulk.prefetch.L2.global [%0], %1;\" ::\"l\"(gs + seg_off(base, s)), "
+         "\"r\"(8u << LB) : \"memory\");\n"
+         "}\n";
     o << "template <bool EPI>\n__device__ __forceinline__ void body(const TileArgs& a"
       << (p.rtc ? ", const Coefs& K" : "") << ") {\n"
          "    extern __shared__ __align__(128) unsigned char smem_raw[];\n"
@@ -1200,6 +1211,7 @@ std::string generate_impl(const Pass& p, bool need_epi, int nbuf, int groups, in
              "    const bool ok = mbar_wait_bounded(&bars[0], phases & 1, a.err);\n"
              "    if (!__syncthreads_and(ok)) { mbar_wait_bounded(&bars[0], phases & 1, nullptr); return; }\n"
              "    phases ^= 1;\n"
+             "    if (t + gridDim.x < a.ntiles) prefetch_tile(a, t + gridDim.x);\n"
              "    (void)cur; (void)k;\n";
     // stages
     const int LBk = 4;  // complex64 bank boundary
