@@ -314,6 +314,17 @@ struct Gen {
     // current stage: KB bits, GS register groups of 2^KB amplitudes per thread
     int KB = 4, GS = 2;
 
+    // What the dry run of a stage's members learns: per stage pattern the position of
+    // the last member that mixes it (-2: a member that flushes) and the phases pending
+    // at the stage's end; the emitting run marks the patterns whose final phase went into
+    // a member row (taken), which the end of the stage then skips.
+    struct Absorb {
+        bool dry = true;
+        std::vector<int> last;
+        std::vector<std::complex<double>> fin;
+        std::vector<bool> taken;
+    };
+
     // one stage: S sorted KB tile bits, rl[q] lane bit of the rotation at stage
     // position q (-1 none), members = indices into p.ops
     void stage(const int* S, int k_bits, const int* rl, const std::vector<int>& members) {
@@ -388,54 +399,36 @@ struct Gen {
             std::fill(pend.begin(), pend.end(), one);
             scal = false;
             for (size_t at = 0; at < members.size(); ++at) {
-            const int m = members[at];
-            const DevOp& op = p.ops[m];
-            int pm = 0;
-            bool on_stage = op.nq >= 1;
-            for (int t = 0; t < op.nq; ++t) {
-                const int q = op.lb[t] >= 0 ? stage_pos(op.lb[t]) : -1;
-                if (q < 0) on_stage = false;
-                else pm |= 1 << q;
-            }
-            if (!p.rtc && op.kind == OPK_DIAG && on_stage) {
-                for (int r = 0; r < R; ++r) {
-                    int mi = 0;
-                    for (int t = 0; t < op.nq; ++t) mi |= ((r >> stage_pos(op.lb[t])) & 1) << t;
-                    pend[r] *= std::complex<double>(op.cd[mi].x, op.cd[mi].y);
+                const int m = members[at];
+                const DevOp& op = p.ops[m];
+                int pm = 0;
+                bool on_stage = op.nq >= 1;
+                for (int t = 0; t < op.nq; ++t) {
+                    const int q = op.lb[t] >= 0 ? stage_pos(op.lb[t]) : -1;
+                    if (q < 0) on_stage = false;
+                    else pm |= 1 << q;
                 }
-                continue;
-            }
-            const bool diagonal = op.kind == OPK_DIAG || op.kind == OPK_STATESCALE || op.kind == OPK_REALTAB;
-            if (!diagonal && !p.rtc && on_stage) {
-                member_through(m, (int)at, S, gstep, pend, ab);
-                continue;
-            }
-            if (!diagonal && pm && ab.dry)  // a flushing member: what it mixes is not absorbed
-                std::fill(ab.last.begin(), ab.last.end(), -2);
-            if (!diagonal) {
-                const int dim = 1 << op.nq;
-                std::vector<bool> iso(dim, false);
-                if (!p.rtc && on_stage) {
-                    const std::vector<CplxF> M = op_matrix_f(op);
-                    for (int k = 0; k < dim; ++k) {
-                        bool e = M[k * dim + k].re == 1.f && M[k * dim + k].im == 0.f;
-                        for (int j = 0; j < dim && e; ++j)
-                            if (j != k) {
-                                const CplxF a = M[k * dim + j], b = M[j * dim + k];
-                                e = a.re == 0.f && a.im == 0.f && b.re == 0.f && b.im == 0.f;
-                            }
-                        iso[k] = e;
+                if (!p.rtc && op.kind == OPK_DIAG && on_stage) {
+                    for (int r = 0; r < R; ++r) {
+                        int mi = 0;
+                        for (int t = 0; t < op.nq; ++t) mi |= ((r >> stage_pos(op.lb[t])) & 1) << t;
+                        pend[r] *= std::complex<double>(op.cd[mi].x, op.cd[mi].y);
                     }
+                    continue;
                 }
-                std::vector<bool> need(R, true);
-                for (int r = 0; r < R && on_stage; ++r) {
-                    int k = 0;
-                    for (int t = 0; t < op.nq; ++t) k |= ((r >> stage_pos(op.lb[t])) & 1) << t;
-                    need[r] = !iso[k];
+                const bool diagonal =
+                    op.kind == OPK_DIAG || op.kind == OPK_STATESCALE || op.kind == OPK_REALTAB;
+                if (!diagonal && !p.rtc && on_stage) {
+                    member_through(m, (int)at, S, gstep, pend, ab);
+                    continue;
                 }
-                if (pm) flush_where(need);
-            }
-            scal |= member(m, S, gstep, scal);
+                // any other matrix member takes every pending phase first (with run-time
+                // coefficients nothing is pending), and nothing it mixes is absorbed
+                if (!diagonal && pm) {
+                    if (ab.dry) std::fill(ab.last.begin(), ab.last.end(), -2);
+                    flush_where(std::vector<bool>(R, true));
+                }
+                scal |= member(m, S, gstep, scal);
             }
             if (ab.dry) ab.fin = pend;
         }
@@ -461,17 +454,6 @@ struct Gen {
         if (trivial_coef(k)) return 0;
         return (k.re == 0.f || k.im == 0.f) ? 2 : 4;
     }
-
-    // What the dry run of a stage's members learns: per stage pattern the position of
-    // the last member that mixes it (-2: a member that flushes) and the phases pending
-    // at the stage's end; the emitting run marks the patterns whose final phase went into
-    // a member row (taken), which the end of the stage then skips.
-    struct Absorb {
-        bool dry = true;
-        std::vector<int> last;
-        std::vector<std::complex<double>> fin;
-        std::vector<bool> taken;
-    };
 
     // A literal matrix member on stage bits under the stage's pending phases P (one per
     // stage pattern).  For each pattern of the other stage bits (the "rest") it takes the
