@@ -16,7 +16,7 @@ export CuContext, CuState, apply_rx_psi!, apply_ry_psi!, apply_rz_psi!, apply_ha
        expect_local, expect_corr, get_expectation_pauli_string, get_norm, normalize_state!,
        TrotterPlan, evolve_trotter_psi!, apply_fast_trotter_step_cpu!, energy_and_gradient,
        energy_and_gradient_jobs, lindblad_mcwf_batched!, apply_hamiltonian_bitwise!, sample_bitstrings,
-       projective_measurement_all!, measure_z_single!, set_engine!, run_mcwf_simulation,
+       projective_measurement_all!, measure_z_single!, set_engine!, set_option!, run_mcwf_simulation,
        apply_gate!, apply_2qubit_gate!, apply_one_qubit_gate_bitwise_cpu!, apply_two_qubit_gate_bitwise_cpu!,
        apply_circuit!, apply_channel_dephasing!, apply_channel_depolarizing!, apply_channel_amplitude_damping!,
        apply_channel_bit_flip!, apply_channel_phase_flip!, projective_measurement!, reset_state!,
@@ -519,5 +519,18 @@ end
 pass kernels"
 set_engine!(ctx::CuContext, e::Integer) =
     check(ccall((:smoq_ctx_set_option, lib), Cint, (Ptr{Cvoid}, Cint, Clonglong), ctx.h, 7, e), ctx)
+
+# the context options of smoq_cuda.h (SMOQ_OPT_*) by name
+const OPTIONS = Dict(:tile_bits_c64 => 1, :tile_bits_c128 => 2, :low_bits_c64 => 3, :low_bits_c128 => 4,
+                     :use_graphs => 5, :kernel_timing => 6, :engine => 7, :jit_buffers => 8, :jit_groups => 10,
+                     :vqe_resident => 12, :autotune => 13, :fusion_depth => 14)
+
+"set a context option by name, e.g. `set_option!(ctx, :autotune, 2)` (tune the compiled
+pass kernels' variants only, keeping the geometry the tile/low-bits/fusion-depth options
+set; 1 = also time the candidate geometries, 0 = off)"
+function set_option!(ctx::CuContext, name::Symbol, value::Integer)
+    haskey(OPTIONS, name) || error("Unknown option: $name")
+    check(ccall((:smoq_ctx_set_option, lib), Cint, (Ptr{Cvoid}, Cint, Clonglong), ctx.h, OPTIONS[name], value), ctx)
+end
 
 end # module
