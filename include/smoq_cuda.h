@@ -526,7 +526,8 @@ typedef struct {
  * the complex64 forward of smoq_energy_grad compiles: gate coefficients passed per launch),
  * 8 = one register group per thread (SMOQ_OPT_JIT_GROUPS 1), 16 = the generated source of the
  * first pass in msg (nothing compiled; with 32, the sources of every pass one after another,
- * *n_compiled = their count).  *n_compiled = kernels compiled; msg gets "ok" (or the
+ * *n_compiled = their count, and with 4 as well each source is followed by a line "//@coefs"
+ * and its run-time coefficient block as hex floats, re im per entry).  *n_compiled = kernels compiled; msg gets "ok" (or the
  * report) or the first error.  SMOQ_ERR_UNSUPPORTED when NVRTC is not available. */
 smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tile_bits, int low_bits, const smoq_op* ops, int n,
                                     const double* theta, int flags, int* n_compiled, char* msg, int msg_len);

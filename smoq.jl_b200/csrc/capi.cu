@@ -883,6 +883,15 @@ smoq_status smoq_debug_compile_plan(int N, smoq_dtype dtype, int tbits, int lbit
             }
             ++*n_compiled;
             report += info;
+            if (p.rtc && (flags & 32)) {  // the pass's run-time coefficient block, after its source
+                report += "\n//@coefs";
+                char num[80];
+                for (const float2& c : p.coefs) {
+                    std::snprintf(num, sizeof num, " %a %a", (double)c.x, (double)c.y);
+                    report += num;
+                }
+                report += "\n";
+            }
             if (flags & 32) continue;
             say(report);
             return SMOQ_OK;

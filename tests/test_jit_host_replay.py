@@ -29,6 +29,7 @@ typedef unsigned long long u64;
 struct cf { float x, y; };
 struct HostOp { cf c[16]; };          // the coefficients a mixed diagonal reads at run time
 struct HostArgs { const HostOp* ops; };
+struct HostCoefs { const cf* k; };    // a run-time-coefficient kernel's parameter block
 static inline cf cmul(cf a, cf b) { return cf{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
 static inline cf cscale(cf a, float s) { return cf{a.x * s, a.y * s}; }
 """
@@ -37,19 +38,29 @@ _STAGE = re.compile(r"\n    \{  // stage S = \{[^\n]*\n(.*?)\n    \}\n    __sync
 
 
 def host_library(src, tmp_path, name):
-    """one host function per generated kernel source: run_<k>(tile, ops, base) applies
-    that kernel's stage blocks, thread by thread, to one tile (ops: the pass's fused ops'
-    complex64 coefficients, in the pass's op order; base: the tile's first amplitude index)"""
+    """one host function per generated kernel source: run_<k>(tile, ops, base, coefs)
+    applies that kernel's stage blocks, thread by thread, to one tile (ops: the pass's
+    fused ops' complex64 coefficients, in the pass's op order; base: the tile's first
+    amplitude index; coefs: the run-time coefficient block of a run-time-coefficient
+    kernel).  Returns the library and each kernel's coefficient block (or None)."""
     kernels = [s for s in src.split("\ntypedef unsigned int u32;") if "// stage S" in s]
     body = [_HOST_PRELUDE]
+    blocks_k = []
     for k, ks in enumerate(kernels):
         nt = int(re.search(r"#define NT (\d+)", ks).group(1))
         blocks = _STAGE.findall(ks)
         assert blocks, "no stage blocks in a compiled pass"
-        for b in blocks:  # the stage blocks use the tile, tid, literals, a.ops[m].c and base
+        for b in blocks:  # the stage blocks use the tile, tid, literals, a.ops[m].c, K.k[i] and base
             assert len(re.findall(r"\ba\.", b)) == len(re.findall(r"\ba\.ops\[", b)), b[:200]
-        body.append(f'extern "C" void run_{k}(cf* tile, const HostOp* ops, u64 base) {{\n'
-                    f'  const HostArgs a{{ops}};\n  (void)base;\n')
+        m = re.search(r"//@coefs([^\n]*)", ks)
+        if m:
+            v = [float.fromhex(x) for x in m.group(1).split()]
+            blocks_k.append(np.array(v[0::2], np.float32) + 1j * np.array(v[1::2], np.float32))
+        else:
+            assert "K.k[" not in ks
+            blocks_k.append(None)
+        body.append(f'extern "C" void run_{k}(cf* tile, const HostOp* ops, u64 base, const cf* kc) {{\n'
+                    f'  const HostArgs a{{ops}};\n  const HostCoefs K{{kc}};\n  (void)base; (void)K;\n')
         for b in blocks:
             body.append(f"  for (u32 tid = 0; tid < {nt}u; ++tid) {{\n{b}\n  }}\n")
         body.append("}\n")
@@ -57,7 +68,7 @@ def host_library(src, tmp_path, name):
     so = tmp_path / f"{name}.so"
     cpp.write_text("".join(body))
     subprocess.run(["g++", "-O1", "-ffp-contract=off", "-shared", "-fPIC", "-o", str(so), str(cpp)], check=True)
-    return C.CDLL(str(so)), len(kernels)
+    return C.CDLL(str(so)), blocks_k
 
 
 def random_gates(N, n, seed):
@@ -104,8 +115,12 @@ CASES = {"xxz_n13": (13, 5), "bench_circuit_n12": (12, 5), "random_n13": (13, 5)
          "xxz_n18_low5": (18, 5), "xxz_n18_low4": (18, 4), "random_n16": (16, 5)}
 
 
+@pytest.mark.parametrize("rtc", [False, True], ids=["literal", "run_time_coefficients"])
 @pytest.mark.parametrize("case", list(CASES))
-def test_generated_stage_code_replays_on_host(built, tmp_path, case):
+def test_generated_stage_code_replays_on_host(built, tmp_path, case, rtc):
+    """literal kernels (Trotter plans, MCWF) and the run-time-coefficient form (the
+    complex64 forward of smoq_energy_grad: coefficients read from the launch's
+    parameter block) of the same program"""
     import pysmoq as S
     N, low = CASES[case]
     if case.startswith("xxz"):
@@ -115,18 +130,21 @@ def test_generated_stage_code_replays_on_host(built, tmp_path, case):
         g, o = circuit(N, 400)
     else:
         g, o = random_gates(N, 240, 7)
-    st, n, src = S.debug_compile_plan(N, g, tile_bits=13, low_bits=low, all_sources=True)
+    st, n, src = S.debug_compile_plan(N, g, tile_bits=13, low_bits=low, all_sources=True, rtc=rtc)
     if st == 5:
         pytest.skip("NVRTC not available: " + src)
     assert st == 0 and n >= 1, src[:500]
-    lib, nk = host_library(src, tmp_path, case)
-    assert nk == n
+    lib, coefs = host_library(src, tmp_path, case)
+    nk = len(coefs)
+    assert nk == n and all((c is not None) == rtc for c in coefs)
     rng = np.random.default_rng(3)
     psi0 = rng.normal(size=1 << N) + 1j * rng.normal(size=1 << N)
     psi0 /= np.linalg.norm(psi0)
     want = psi0.astype(np.complex128).copy()
     O.apply_circuit(want, O.make_ops(o), len(o), np.zeros(1), N)
-    plan = S.debug_plan(N, g, dtype=S.C64, tile_bits=13, low_bits=low, engine=3)
+    # the passes' op tables (for the ops that read coefficients at run time): the
+    # run-time-coefficient form schedules like engine 2 (no rotation split)
+    plan = S.debug_plan(N, g, dtype=S.C64, tile_bits=13, low_bits=low, engine=2 if rtc else 3)
     assert len(plan) == nk
     psi = psi0.astype(np.complex64)
     for k, p in enumerate(plan):
@@ -136,11 +154,13 @@ def test_generated_stage_code_replays_on_host(built, tmp_path, case):
         off, bases = tile_offsets(N, p["L"], p["hb"])
         assert len(off) == 1 << p["T"] and len(bases) << p["T"] == 1 << N
         run = getattr(lib, f"run_{k}")
+        kc = coefs[k] if coefs[k] is not None else np.zeros(1, np.complex64)
         for base in bases:
             idx = base | off
             tile = np.ascontiguousarray(psi[idx])
-            run(tile.ctypes.data_as(C.c_void_p), cf.ctypes.data_as(C.c_void_p), C.c_uint64(base))
+            run(tile.ctypes.data_as(C.c_void_p), cf.ctypes.data_as(C.c_void_p), C.c_uint64(base),
+                kc.ctypes.data_as(C.c_void_p))
             psi[idx] = tile
     err = np.linalg.norm(psi.astype(np.complex128) - want) / np.linalg.norm(want)
-    print(case, "relative L2", err)
+    print(case, rtc, "relative L2", err)
     assert err < 2e-6, err   # FP32 rounding over the circuit: measured 4e-7 to 6e-7
