@@ -879,7 +879,10 @@ def main():
     default_geom = None
     if rank == 0 and ws == 1 and not args.tile_bits and not args.low_bits and args.autotune != 0 \
             and geom != (13, 5, None):
-        default_geom = default_geometry_record(S, local, N, gates, neel, tsteps, gate_apps, args.steps, peak)
+        try:
+            default_geom = default_geometry_record(S, local, N, gates, neel, tsteps, gate_apps, args.steps, peak)
+        except Exception as ex:  # a sub-record never costs the headline line
+            default_geom = {"error": f"{type(ex).__name__}: {ex}"}
 
     per_rank_apps = gate_apps * args.steps
     value = whole_job_rate(per_rank_apps, ws, ms)
