@@ -900,10 +900,16 @@ def main():
     # adjoint against the plain complex128 path, energy error), every rank
     vqe = None
     if not args.no_vqe and N == N_QUBITS:
-        vqe = vqe_measure(ctx, steps=2, warmup=1)
+        try:  # (no collectives inside: a rank that fails here fails alone)
+            vqe = vqe_measure(ctx, steps=2, warmup=1)
+        except Exception as ex:  # a sub-record never costs the headline line
+            vqe = {"error": f"{type(ex).__name__}: {ex}"}
     published = None
     if not args.no_vqe and N == N_QUBITS and rank == 0:
-        published = published_comparison(ctx)
+        try:
+            published = published_comparison(ctx)
+        except Exception as ex:
+            published = {"error": f"{type(ex).__name__}: {ex}"}
     # short runs of the other workloads (one timed step each, no CPU baselines), so the
     # default line carries their figures too; the full runs are --workload vqe_jobs,
     # mcwf and qrc
