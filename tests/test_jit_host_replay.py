@@ -115,33 +115,19 @@ CASES = {"xxz_n13": (13, 5), "bench_circuit_n12": (12, 5), "random_n13": (13, 5)
          "xxz_n18_low5": (18, 5), "xxz_n18_low4": (18, 4), "random_n16": (16, 5)}
 
 
-@pytest.mark.parametrize("rtc", [False, True], ids=["literal", "run_time_coefficients"])
-@pytest.mark.parametrize("case", list(CASES))
-def test_generated_stage_code_replays_on_host(built, tmp_path, case, rtc):
-    """literal kernels (Trotter plans, MCWF) and the run-time-coefficient form (the
-    complex64 forward of smoq_energy_grad: coefficients read from the launch's
-    parameter block) of the same program"""
-    import pysmoq as S
-    N, low = CASES[case]
-    if case.startswith("xxz"):
-        g, o = xxz_strang(S, N)
-        g, o = g + g + g, o + o + o   # three Strang steps: the merged half steps fold across
-    elif case.startswith("bench"):
-        g, o = circuit(N, 400)
-    else:
-        g, o = random_gates(N, 240, 7)
-    st, n, src = S.debug_compile_plan(N, g, tile_bits=13, low_bits=low, all_sources=True, rtc=rtc)
+def replay(S, N, g, low, tmp_path, name, rtc=False, groups=2):
+    """the state after every compiled pass of `g`, run on the host from a seeded random
+    state (complex64), and that initial state"""
+    st, n, src = S.debug_compile_plan(N, g, tile_bits=13, low_bits=low, all_sources=True, rtc=rtc, groups=groups)
     if st == 5:
         pytest.skip("NVRTC not available: " + src)
     assert st == 0 and n >= 1, src[:500]
-    lib, coefs = host_library(src, tmp_path, case)
+    lib, coefs = host_library(src, tmp_path, name)
     nk = len(coefs)
     assert nk == n and all((c is not None) == rtc for c in coefs)
     rng = np.random.default_rng(3)
     psi0 = rng.normal(size=1 << N) + 1j * rng.normal(size=1 << N)
     psi0 /= np.linalg.norm(psi0)
-    want = psi0.astype(np.complex128).copy()
-    O.apply_circuit(want, O.make_ops(o), len(o), np.zeros(1), N)
     # the passes' op tables (for the ops that read coefficients at run time): the
     # run-time-coefficient form schedules like engine 2 (no rotation split)
     plan = S.debug_plan(N, g, dtype=S.C64, tile_bits=13, low_bits=low, engine=2 if rtc else 3)
@@ -161,6 +147,44 @@ def test_generated_stage_code_replays_on_host(built, tmp_path, case, rtc):
             run(tile.ctypes.data_as(C.c_void_p), cf.ctypes.data_as(C.c_void_p), C.c_uint64(base),
                 kc.ctypes.data_as(C.c_void_p))
             psi[idx] = tile
+    return psi, psi0
+
+
+def case_gates(S, case):
+    N, low = CASES[case]
+    if case.startswith("xxz"):
+        g, o = xxz_strang(S, N)
+        g, o = g + g + g, o + o + o   # three Strang steps: the merged half steps fold across
+    elif case.startswith("bench"):
+        g, o = circuit(N, 400)
+    else:
+        g, o = random_gates(N, 240, 7)
+    return N, low, g, o
+
+
+@pytest.mark.parametrize("rtc", [False, True], ids=["literal", "run_time_coefficients"])
+@pytest.mark.parametrize("case", list(CASES))
+def test_generated_stage_code_replays_on_host(built, tmp_path, case, rtc):
+    """literal kernels (Trotter plans, MCWF) and the run-time-coefficient form (the
+    complex64 forward of smoq_energy_grad: coefficients read from the launch's
+    parameter block) of the same program"""
+    import pysmoq as S
+    N, low, g, o = case_gates(S, case)
+    psi, psi0 = replay(S, N, g, low, tmp_path, case, rtc=rtc)
+    want = psi0.astype(np.complex128).copy()
+    O.apply_circuit(want, O.make_ops(o), len(o), np.zeros(1), N)
     err = np.linalg.norm(psi.astype(np.complex128) - want) / np.linalg.norm(want)
     print(case, rtc, "relative L2", err)
     assert err < 2e-6, err   # FP32 rounding over the circuit: measured 4e-7 to 6e-7
+
+
+@pytest.mark.parametrize("case", ["xxz_n18_low4", "random_n16"])
+def test_register_group_variants_are_bit_identical(built, tmp_path, case):
+    """the autotuner's register-group variants (two 16-amplitude groups per thread, or one
+    with twice the threads) apply the same literal arithmetic to every amplitude: the
+    host replays of both give the same bits"""
+    import pysmoq as S
+    N, low, g, _ = case_gates(S, case)
+    two, _ = replay(S, N, g, low, tmp_path, case + "_g2", groups=2)
+    one, _ = replay(S, N, g, low, tmp_path, case + "_g1", groups=1)
+    assert np.array_equal(two.view(np.uint32), one.view(np.uint32))
