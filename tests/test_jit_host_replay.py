@@ -188,3 +188,21 @@ def test_register_group_variants_are_bit_identical(built, tmp_path, case):
     two, _ = replay(S, N, g, low, tmp_path, case + "_g2", groups=2)
     one, _ = replay(S, N, g, low, tmp_path, case + "_g1", groups=1)
     assert np.array_equal(two.view(np.uint32), one.view(np.uint32))
+
+
+def test_bench_program_multiply_count(built):
+    """the generated arithmetic of three Strang steps of the N=28 XXZ bench program
+    (tile 13, low bits 5; 19 compiled passes): FP32 multiplies, counted as the literal
+    coefficient terms of the stage code.  Flushing the pending phases before every member
+    gave 23,920; moving members through the phases and absorbing the final phases into
+    member rows gives 18,640.  A regression to flushing shows here, not in the parity
+    tests (both forms are exact)."""
+    import pysmoq as S
+    g, _ = xxz_strang(S, 28)
+    st, n, src = S.debug_compile_plan(28, g + g + g, tile_bits=13, low_bits=5, all_sources=True)
+    if st == 5:
+        pytest.skip("NVRTC not available: " + src)
+    assert st == 0 and n == 19, (st, n)
+    stages = "".join(_STAGE.findall(src))
+    mults = len(re.findall(r"\* [vx]\d", stages))
+    assert mults <= 19000, mults
