@@ -67,7 +67,7 @@ def host_library(src, tmp_path, name):
     cpp = tmp_path / f"{name}.cpp"
     so = tmp_path / f"{name}.so"
     cpp.write_text("".join(body))
-    subprocess.run(["g++", "-O1", "-ffp-contract=off", "-shared", "-fPIC", "-o", str(so), str(cpp)], check=True)
+    subprocess.run(["g++", "-O0", "-ffp-contract=off", "-shared", "-fPIC", "-o", str(so), str(cpp)], check=True)
     return C.CDLL(str(so)), blocks_k
 
 
