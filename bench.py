@@ -947,7 +947,12 @@ def main():
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": ncu_traffic(eng), "peak_kind": peak_kind,
                              "kernel": ENGINE_KERNELS[eng][0], "avg_launch_ms": avg_ms,
-                             "algorithmic_bytes_per_launch": bytes_per_launch},
+                             "algorithmic_bytes_per_launch": bytes_per_launch,
+                             # per pass launch: with the autotuner's geometry a pass may carry
+                             # more gates (fewer passes per evolution); the same kernels' fraction
+                             # at the default geometry, measured in this run, sits beside it
+                             "geometry": f"tile {geom[0]}, low bits {geom[1]}",
+                             "default_geometry_frac": (default_geom or {}).get("roofline_frac")},
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": "gate-apps/s", "h2d_bytes_per_step": int(hp.nbytes),
                         "d2h_bytes_per_step": int(8 * N * (tsteps // RECORD_EVERY + 1))},
