@@ -958,7 +958,8 @@ def debug_compile_plan(N: int, ops: Sequence[CircuitOperation], theta=None, dtyp
     with verbose the message is the compiler's register/spill report.  rtc: the
     run-time-coefficient form (a variational forward); source: the message is the
     generated source of the first pass (nothing compiled); all_sources: the sources of
-    every pass, one after another."""
+    every pass, one after another (with rtc each followed by a "//@coefs" line: the pass's
+    run-time coefficient block as hex floats, re im per entry)."""
     arr = circuit_to_c_ops(ops)
     th = np.ascontiguousarray(theta if theta is not None else np.zeros(1), dtype=np.float64)
     n = C.c_int()
